@@ -1,0 +1,39 @@
+// Host-side entry points of the surface builder library (grid environment and patch builders).
+// Exported with C linkage from libnsgpu; the public declarations live in include/nsgpu.h.
+#pragma once
+#include <stdint.h>
+
+#include "../ns_types.h"
+
+#define NSG_OK 0
+#define NSG_ERR_ARG (-1)
+#define NSG_ERR_EMPTY (-2)
+#define NSG_ERR_IO (-3)
+#define NSG_ERR_CAPACITY (-4)
+#define NSG_ERR_CUDA (-5)
+#define NSG_ERR_NOMEM (-6)
+#define NSG_ERR_STATE (-7)
+#define NSG_ERR_GEOMETRY (-8)
+#define NSG_ERR_TIMEOUT (-9)
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+int nsg_grid_build(const double* atoms_xyzr, int64_t n_atoms, double scale, double perfil, NsGrid* out);
+double nsg_randnum(int64_t* seed);
+int nsg_jitter_atoms(double* atoms_xyzr, int64_t n_atoms, double displacement, int64_t* seed);
+int64_t nsg_read_xyzr(const char* path, double* out, int64_t capacity);
+
+// Host-owned patch set produced by a patch builder.
+typedef struct NsPatchSet NsPatchSet;
+
+int nsg_ses_build(const double* atoms_xyzr, int64_t n_atoms, double probe_radius, int n_threads,
+                  NsPatchSet** out);
+int nsg_patchset_info(const NsPatchSet* ps, int64_t* n_patches, int64_t* n_pool, int64_t counts[5]);
+int nsg_patchset_export(const NsPatchSet* ps, double* f64, int32_t* i32, double* pool, int8_t* pool_flag);
+void nsg_patchset_free(NsPatchSet* ps);
+
+#ifdef __cplusplus
+}
+#endif

@@ -1,0 +1,72 @@
+// Shared plain-old-data layouts of the grid-ray-casting surface builder.
+// Included by the host patch builders, the C-ABI layer and the sm_100a kernels,
+// so it must stay C/C++/CUDA neutral (no STL, no torch).
+#pragma once
+#include <stdint.h>
+
+#ifdef __CUDACC__
+#define NS_HD __host__ __device__ __forceinline__
+#else
+#define NS_HD inline
+#endif
+
+// Patch kinds.  They mirror the reference cell classes:
+//   POINT      -> PointCell  (exposed atom sphere, clipped by neighbour spheres)
+//   EDGE_REG   -> EdgeCell REGULAR_EDGE_CELL  (torus sector bounded by plane pairs)
+//   EDGE_SING  -> EdgeCell SINGULAR_EDGE_CELL (full torus)
+//   FACE_REG   -> FacetCell REGULAR_FACE_CELL (re-entrant probe patch, 3 trimming planes)
+//   FACE_SING  -> FacetCell SINGULAR_FACE_CELL (probe patch, 4 trimming planes)
+// (src/ConnollySurface.h:31-167, cell type tags src/Surface.h).
+enum NsPatchKind {
+  NS_POINT = 0,
+  NS_EDGE_REG = 1,
+  NS_EDGE_SING = 2,
+  NS_FACE_REG = 3,
+  NS_FACE_SING = 4
+};
+
+// Per-patch double record (NS_PATCH_F64 doubles per patch).
+//   [0..2] bounding-sphere centre, [3] bounding-sphere radius
+//          POINT: atom centre / radius; EDGE: clipping sphere; FACE: probe sphere
+//   [4..6] torus centre (EDGE only)
+//   [7]    torus major radius (EDGE only)
+//   [8]    spindle self-intersection radius, < 0 when the torus is not spindle (EDGE)
+//   [9..17] inverse torus frame rotation, row major (EDGE)
+//   [18..19] unused
+#define NS_PATCH_F64 20
+// Per-patch int record (NS_PATCH_I32 ints per patch): kind, first pool entry, pool entry count, unused.
+#define NS_PATCH_I32 4
+
+// Pool entries are 4 doubles.
+//   POINT: clipping sphere (cx, cy, cz, r^2); a point strictly inside any of them is infeasible.
+//   FACE : plane (a, b, c, d); a point with a*x+b*y+c*z+d > 0 is infeasible.
+//   EDGE : plane pairs (2 consecutive entries).  pool_flag[first entry of the pair] = 1 for an
+//          acute pair (feasible iff both tests <= 0), 0 for an obtuse pair (feasible iff either
+//          test <= 0).  A point is feasible if any pair accepts it; a pair-less EDGE accepts all.
+
+// Status codes of the status map (src/DelphiShared.h:22-33).
+#define NS_STATUS_INSIDE (-1)
+#define NS_STATUS_TEMPORARY_OUT 2
+#define NS_STATUS_OUT 3
+#define NS_STATUS_FIRST_CAV 4
+
+// Tolerances of the reference (src/Surface.h:285-291).
+#define NS_EPS_INT 1e-8
+#define NS_DELTA 1e-10
+
+// Edge directions of marching-cubes vertices.
+#define NS_X_DIR 0
+#define NS_Y_DIR 1
+#define NS_Z_DIR 2
+
+typedef struct NsGrid {
+  int64_t nx, ny, nz;
+  double xmin, ymin, zmin;
+  double xmax, ymax, zmax;
+  double scale, side, hside, A;
+  double rmaxdim;
+  double baricenter[3];
+} NsGrid;
+
+// Grid coordinate of node i along an axis: min + i*side (src/DelphiShared.cpp:1155-1162).
+NS_HD double ns_coord(double vmin, double side, int64_t i) { return vmin + (double)i * side; }

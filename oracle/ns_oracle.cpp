@@ -1,0 +1,802 @@
+// ORACLE — test infrastructure only.  CPU restatement of the reference's grid ray-casting surface
+// path, used by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg as the checker.
+// It is never linked into, called by or loaded from the product library.
+//
+// Restates, for the patch-based ray tracer of an SES patch set:
+//   * per-patch ray casting     ConnollySurface::getPatchIntersectionData
+//                               (src/ConnollySurface.cpp:4319-4590), raySphere (src/tools.cpp:833-861),
+//                               rayTorus (src/tools.cpp:907-1098), quarticEqSolutions
+//                               (src/tools.cpp:525-639), realCubicSolution (src/tools.cpp:350-391),
+//                               ConnollySurface::isFeasible (src/ConnollySurface.cpp:4769-5019)
+//   * pixel binning and sort    countPixelIntersections / copyPatchIntersections /
+//                               reorderPatchIntersections (src/Surface.cpp:4941-5095)
+//   * interval fill             setVerticesAndGridsWithIntersectionData (src/Surface.cpp:5101-6251)
+//                               with NEW_INTERSECTION_FILTERING: a ray with an odd hit count is
+//                               skipped (the emptiness test precedes the closure test, :5279-5287)
+//   * volume                    src/Surface.cpp:1680-1684
+//   * cavities                  getCavitiesWithBilevelStatusMap (src/Surface.cpp:1994-2126),
+//                               floodFillWithBilevelStatusMap2 (:4284-4554), fillCavities (:2355-2484)
+//   * vertex assembly           assembleVerticesList (src/Surface.cpp:7415-7667)
+//   * marching cubes            triangulateSurface / getVertices / triangulationKernel / getTriangles
+//                               (src/Surface.cpp:9909-10300, 8002-8327, 9075-9318, 14526-14780)
+// Single-threaded by default so that volume and area are summed in the reference's serial order.
+// Compile without FMA contraction (-ffp-contract=off) so that every operation rounds as written.
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <array>
+#include <atomic>
+#include <deque>
+#include <stack>
+#include <string>
+#include <thread>
+#include <utility>
+#include <vector>
+
+#include "../nanoshaper_b200/csrc/mc_cases.h"
+#include "../nanoshaper_b200/csrc/ns_types.h"
+
+namespace {
+
+inline double rintp(double x) { return floor(x + 0.5); }
+
+struct Patches {
+  int64_t n;
+  const double* f64;
+  const int32_t* i32;
+  const double* pool;
+  const int8_t* flag;
+  double probe;
+};
+
+// raySphere (src/tools.cpp:833-861)
+bool ray_sphere(const double* orig, const double* dir, const double* c, double r, double* t1, double* t2) {
+  double temp[3], A, B, C;
+  A = dir[0] * dir[0] + dir[1] * dir[1] + dir[2] * dir[2];
+  temp[0] = orig[0] - c[0]; temp[1] = orig[1] - c[1]; temp[2] = orig[2] - c[2];
+  B = temp[0] * dir[0] + temp[1] * dir[1] + temp[2] * dir[2];
+  C = temp[0] * temp[0] + temp[1] * temp[1] + temp[2] * temp[2] - r * r;
+  double det = B * B - A * C;
+  if (det < 0.) return false;
+  det = sqrt(det);
+  *t1 = (-B - det) / A;
+  *t2 = (-B + det) / A;
+  if (*t2 < *t1) { double tt = *t1; *t1 = *t2; *t2 = tt; }
+  return true;
+}
+
+// realCubicSolution (src/tools.cpp:350-391)
+double real_cubic(double b, double c, double d) {
+  double p = -(1.0 / 3.0) * b * b + c;
+  double q = (2. / 27.) * b * b * b - (1. / 3.) * b * c + d;
+  double D3p = (1. / 27.) * p * p * p;
+  double D3 = D3p + 0.25 * q * q;
+  if (fabs(c) < b * b * 1.E-6 && fabs(d) < fabs(b) * 1.E-6) {
+    return c / b - b - d / (b * b);
+  } else if (fabs(d / c) < 4.E-4) {
+    double ratio = d / c;
+    if (D3 <= 0.) {
+      return 0.5 * (ratio - b + sqrt((b - ratio) * (b - ratio) - 4. * (c - ratio * (b - ratio))));
+    } else {
+      double eps = -ratio * ratio * (b - ratio) / (3. * ratio * ratio - 2. * b * ratio + c);
+      return eps - ratio;
+    }
+  } else {
+    if (D3 >= 0.) {
+      double radD3 = sqrt(D3);
+      double A = cbrt(radD3 - 0.5 * q);
+      double psu3A = cbrt(radD3 + 0.5 * q);
+      return A - psu3A - (1. / 3.) * b;
+    } else {
+      double Aarg = acos(-0.5 * q / sqrt(-D3p));
+      return 2. * sqrt(-(1. / 3.) * p) * cos((1. / 3.) * Aarg) - (1. / 3.) * b;
+    }
+  }
+}
+
+// quarticEqSolutions (src/tools.cpp:525-639)
+void quartic(double roots[4], double b, double c, double d, double e, int* num_sol) {
+  double b_2 = 0.5 * b;
+  double b_4 = 0.25 * b;
+  double p = c - 1.5 * (b_2 * b_2);
+  double q = d + b_2 * (b_2 * b_2 - c);
+  double r = e + b_4 * (b_4 * (c - 3.0 * b_4 * b_4) - d);
+  double f = p * p - 4. * r;
+  double delta = 4. * f * (4. * r * (p * p) - p * (q * q) - 16. * (r * r)) + (q * q) * (128. * p * r - 27. * (q * q));
+  bool change_variant = false;
+  if (e != 0. && (fabs(p) > 3.E+3 || fabs(r) > 3.E+3 || fabs(q) > 3.E+3 || fabs(delta) > 1.E+14)) {
+    double dsu2e = 0.5 * d / e;
+    change_variant = true;
+    p = -1.5 * dsu2e * dsu2e + c / e;
+    q = dsu2e * (dsu2e * dsu2e - c / e) + b / e;
+    r = dsu2e * (-3. / 16. * (dsu2e * dsu2e * dsu2e) + 0.25 * dsu2e * (c / e) - 0.5 * b / e) + 1. / e;
+    f = p * p - 4. * r;
+    delta = 4. * f * (4. * r * (p * p) - p * (q * q) - 16. * (r * r)) + (q * q) * (128. * p * r - 27. * (q * q));
+  }
+  if (delta < 0. || (delta == 0. && (p >= 0. || f < 0.)))
+    *num_sol = 2;
+  else if ((p < 0. && f > 0.) || (delta == 0. && p == 0. && r == 0.))
+    *num_sol = 4;
+  else {
+    *num_sol = 0;
+    return;
+  }
+  double m = real_cubic(p, 0.25 * (p * p) - r, (-0.125) * (q * q));
+  if (m <= 0) {
+    *num_sol = 0;
+    return;
+  }
+  double coeff;
+  if (*num_sol >= 2) {
+    double sol_delta_min, sol_delta_max, p1, p2, p3;
+    if (m < 1.E-14) {
+      p1 = p + p;
+      p2 = (q * q) / f;
+      p3 = 2. * sqrt(f);
+      sol_delta_max = p3 - p1 - p2;
+      coeff = 2. * fabs(q) / f;
+    } else {
+      p1 = -2. * (p + m);
+      p2 = sqrt(2. * (q * q) / m);
+      sol_delta_max = p1 + p2;
+      coeff = sqrt(2. * m);
+    }
+    roots[0] = 0.5 * (((q >= 0.) ? -coeff : coeff) - sqrt(sol_delta_max));
+    roots[1] = 0.5 * (((q >= 0.) ? -coeff : coeff) + sqrt(sol_delta_max));
+    if (*num_sol == 4) {
+      if (m < 1.E-14)
+        sol_delta_min = -p1 - p2 - p3;
+      else
+        sol_delta_min = p1 - p2;
+      roots[2] = 0.5 * (((q >= 0.) ? coeff : -coeff) - sqrt(sol_delta_min));
+      roots[3] = 0.5 * (((q >= 0.) ? coeff : -coeff) + sqrt(sol_delta_min));
+    }
+  }
+  if (change_variant) {
+    for (int i = 0; i < *num_sol; i++) roots[i] = 1. / (roots[i] - 0.25 * d / e);
+  } else {
+    for (int i = 0; i < *num_sol; i++) roots[i] -= 0.25 * b;
+  }
+}
+
+// rayTorus with the analytical solver (src/tools.cpp:907-1098)
+bool ray_torus(const double* invrot, const double* tc, const double* sc, double probe, double major,
+               double radius, int vc, const double* orig, const double* dir, double t[4], int& numInt) {
+  double roots[4], pp[3], temp[3], orig1[3];
+  double ray_dir = dir[vc];
+  orig1[0] = orig[0]; orig1[1] = orig[1]; orig1[2] = orig[2];
+  orig1[vc] += t[0] * ray_dir;
+  temp[0] = orig1[0] - tc[0]; temp[1] = orig1[1] - tc[1]; temp[2] = orig1[2] - tc[2];
+  for (int i = 0; i < 3; i++) pp[i] = invrot[3 * i + 0] * temp[0] + invrot[3 * i + 1] * temp[1] + invrot[3 * i + 2] * temp[2];
+  double r2 = probe * probe;
+  double R2 = major * major;
+  double pd = pp[0] * invrot[0 * 3 + vc] + pp[1] * invrot[1 * 3 + vc] + pp[2] * invrot[2 * 3 + vc];
+  double p2 = pp[0] * pp[0] + pp[1] * pp[1] + pp[2] * pp[2];
+  double coeff = p2 - r2 - R2;
+  double B = 4 * pd;
+  double C = 2 * coeff + 4 * pd * pd + 4 * R2 * invrot[2 * 3 + vc] * invrot[2 * 3 + vc];
+  double D = 4 * pd * coeff + 8 * R2 * pp[2] * invrot[2 * 3 + vc];
+  double E = coeff * coeff - 4 * R2 * (r2 - pp[2] * pp[2]);
+  int numroots;
+  quartic(roots, B, C, D, E, &numroots);
+  if (numroots == 0) return false;
+  double t0 = t[0];
+  numInt = 0;
+  for (int i = 0; i < numroots; i++) {
+    if (roots[i] < 0) continue;
+    double point[3] = {orig1[0], orig1[1], orig1[2]};
+    point[vc] += roots[i];
+    double dd = (sc[0] - point[0]) * (sc[0] - point[0]) + (sc[1] - point[1]) * (sc[1] - point[1]) +
+                (sc[2] - point[2]) * (sc[2] - point[2]);
+    if (dd < radius * radius) t[numInt++] = t0 + roots[i] / ray_dir;
+  }
+  return numInt != 0;
+}
+
+inline double dist2(const double* a, const double* b) {
+  return (a[0] - b[0]) * (a[0] - b[0]) + (a[1] - b[1]) * (a[1] - b[1]) + (a[2] - b[2]) * (a[2] - b[2]);
+}
+inline double plane_test(const double* w, const double* p) { return (w[0] * p[0] + w[1] * p[1] + w[2] * p[2]) + w[3]; }
+
+// isFeasible (src/ConnollySurface.cpp:4769-5019) over the patch-set encoding.
+bool feasible(const Patches& P, int64_t it, const double* p) {
+  const int32_t* ir = P.i32 + NS_PATCH_I32 * it;
+  const double* fr = P.f64 + NS_PATCH_F64 * it;
+  int kind = ir[0];
+  const double* pool = P.pool + 4 * (int64_t)ir[1];
+  const int8_t* flg = P.flag + ir[1];
+  int cnt = ir[2];
+  if (kind == NS_FACE_REG || kind == NS_FACE_SING) {
+    for (int q = 0; q < cnt; q++)
+      if (plane_test(pool + 4 * q, p) > 0) return false;
+    return true;
+  }
+  if (kind == NS_POINT) {
+    for (int q = 0; q < cnt; q++) {
+      double dd = dist2(pool + 4 * q, p);
+      dd -= pool[4 * q + 3];
+      if (dd < 0) return false;
+    }
+    return true;
+  }
+  double r = fr[8];
+  if (r >= 0.) {
+    double dd = dist2(fr + 4, p);
+    if (dd < r * r) return false;
+  }
+  if (cnt == 0) return true;
+  for (int q = 0; q + 1 < cnt; q += 2) {
+    double t0 = plane_test(pool + 4 * q, p);
+    if (flg[q]) {
+      if (t0 > 0) continue;
+      if (plane_test(pool + 4 * (q + 1), p) > 0) continue;
+      return true;
+    } else {
+      if (t0 <= 0) return true;
+      if (plane_test(pool + 4 * (q + 1), p) <= 0) return true;
+    }
+  }
+  return false;
+}
+
+struct Hit {
+  int64_t pixel;
+  double t;
+};
+
+struct Oracle {
+  NsGrid g;
+  Patches P;
+  int flags;
+  double cav_vol;
+  int nthreads;
+  int panels[2];
+  int numPanels;
+  int64_t NMAX;
+  // products
+  std::vector<int64_t> pix_off;  // pixel -> first hit
+  std::vector<double> pix_t;
+  std::vector<int32_t> status;
+  std::vector<uint32_t> bits;
+  double volPanel[3] = {0, 0, 0};
+  int flagsum = 0;
+  double volume = 0;
+  std::vector<double> vert;        // analytic vertices before assembly: x y z
+  std::vector<int32_t> vert_edge;  // ix iy iz dir
+  std::vector<double> vlist;       // assembled vertex list
+  std::vector<int32_t> vkey;       // edge of every assembled vertex (ix iy iz dir)
+  std::vector<int32_t> tris;
+  double area = 0;
+  int ncav = 0;
+  std::vector<double> cav_size;
+  std::vector<int32_t> cav_filled;
+  std::vector<int64_t> ray_hits;  // per pixel id: number of hits (for tests)
+  int64_t n_hits = 0;
+
+  double X(int64_t i) const { return ns_coord(g.xmin, g.side, i); }
+  double Y(int64_t i) const { return ns_coord(g.ymin, g.side, i); }
+  double Z(int64_t i) const { return ns_coord(g.zmin, g.side, i); }
+  double coord(int d, int64_t i) const { return d == 0 ? X(i) : (d == 1 ? Y(i) : Z(i)); }
+  int64_t Nd(int d) const { return d == 0 ? g.nx : (d == 1 ? g.ny : g.nz); }
+  double mind(int d) const { return d == 0 ? g.xmin : (d == 1 ? g.ymin : g.zmin); }
+  double maxd(int d) const { return d == 0 ? g.xmax : (d == 1 ? g.ymax : g.zmax); }
+
+  void trace_patch(int64_t it, std::vector<Hit>& out) const {
+    const int32_t* ir = P.i32 + NS_PATCH_I32 * it;
+    const double* fr = P.f64 + NS_PATCH_F64 * it;
+    int kind = ir[0];
+    const double* sc = fr;
+    double radius = fr[3];
+    bool doTorus = (kind == NS_EDGE_REG || kind == NS_EDGE_SING);
+    double down[3] = {sc[0] - radius, sc[1] - radius, sc[2] - radius};
+    double up[3] = {sc[0] + radius, sc[1] + radius, sc[2] + radius};
+    const double dacc = NS_DELTA;
+    // CELL_CULLING
+    for (int d = 0; d < 3; d++) if (down[d] > maxd(d) + NS_EPS_INT) return;
+    for (int d = 0; d < 3; d++) if (up[d] < mind(d) - (g.hside - dacc + NS_EPS_INT)) return;
+    int64_t i_start[3], i_end[3];
+    for (int d = 0; d < 3; d++) {
+      i_start[d] = (int64_t)rintp(fmax(0., down[d] - mind(d)) * g.scale);
+      i_end[d] = (int64_t)rintp(fmax(0., up[d] - mind(d)) * g.scale);
+      if (i_end[d] >= Nd(d)) i_end[d] = Nd(d) - 1;
+    }
+    int64_t pixels[3] = {1 + i_end[0] - i_start[0], 1 + i_end[1] - i_start[1], 1 + i_end[2] - i_start[2]};
+    for (int phase = 0; phase < 2; phase++) {
+      if (panels[phase] == 0) continue;
+      double delta = (phase == 0) ? 0. : dacc - g.hside;
+      for (int panel = 0; panel < panels[phase]; panel++) {
+        int fd, ld, vc;
+        if (panel == 0) { fd = 1; ld = 2; vc = 0; }
+        else if (panel == 1) { fd = 0; ld = 1; vc = 2; }
+        else { fd = 0; ld = 2; vc = 1; }
+        double pa[3], dir[3] = {0., 0., 0.};
+        pa[vc] = coord(vc, 0) + delta;
+        double ray_dir = coord(vc, Nd(vc) - 1) - coord(vc, 0);
+        dir[vc] = ray_dir;
+        int64_t npix = pixels[fd] * pixels[ld];
+        for (int64_t rp = 0; rp < npix; rp++) {
+          int64_t n = rp / pixels[fd];
+          int64_t m = rp - n * pixels[fd];
+          n += i_start[ld];
+          m += i_start[fd];
+          pa[fd] = coord(fd, m) + delta;
+          if (pa[fd] < down[fd] || pa[fd] > up[fd]) continue;
+          pa[ld] = coord(ld, n) + delta;
+          if (pa[ld] < down[ld] || pa[ld] > up[ld]) continue;
+          double dx = sc[fd] - pa[fd];
+          double dy = sc[ld] - pa[ld];
+          if (dx * dx + dy * dy > radius * radius) continue;
+          double t[4];
+          if (!ray_sphere(pa, dir, sc, radius, &t[0], &t[1])) continue;
+          int numInt = 0;
+          if (!doTorus) numInt = 2;
+          else ray_torus(fr + 9, fr + 4, sc, P.probe, fr[7], radius, vc, pa, dir, t, numInt);
+          for (int i = 0; i < numInt; i++) {
+            double ip[3] = {pa[0], pa[1], pa[2]};
+            ip[vc] += t[i] * ray_dir;
+            if (!feasible(P, it, ip)) continue;
+            int64_t pid = (n * NMAX + m) * numPanels + (panels[0] * phase + panel);
+            out.push_back({pid, t[i]});
+          }
+        }
+      }
+    }
+  }
+
+  void trace() {
+    std::vector<std::vector<Hit>> per(std::max(1, nthreads));
+    auto work = [&](int tid) {
+      for (int64_t it = tid; it < P.n; it += std::max(1, nthreads)) trace_patch(it, per[tid]);
+    };
+    if (nthreads <= 1) work(0);
+    else {
+      std::vector<std::thread> th;
+      for (int t = 0; t < nthreads; t++) th.emplace_back(work, t);
+      for (auto& x : th) x.join();
+    }
+    int64_t npix = NMAX * NMAX * numPanels;
+    pix_off.assign(npix + 1, 0);
+    for (auto& v : per)
+      for (auto& h : v) pix_off[h.pixel + 1]++;
+    for (int64_t i = 0; i < npix; i++) pix_off[i + 1] += pix_off[i];
+    n_hits = pix_off[npix];
+    pix_t.resize(n_hits);
+    std::vector<int64_t> fill(pix_off.begin(), pix_off.end() - 1);
+    for (auto& v : per)
+      for (auto& h : v) pix_t[fill[h.pixel]++] = h.t;
+    for (int64_t i = 0; i < npix; i++)
+      std::sort(pix_t.begin() + pix_off[i], pix_t.begin() + pix_off[i + 1]);
+  }
+
+  // 32x compressed bit grid accessors (src/tools.h:1364-1413); bit = 1 means outside.
+  bool rbit(int64_t i, int64_t j, int64_t k) const {
+    int64_t f = (k * g.ny + j) * g.nx + i;
+    return (bits[f >> 5] >> (f & 31)) & 1u;
+  }
+  void clear_bit(int64_t i, int64_t j, int64_t k) {
+    int64_t f = (k * g.ny + j) * g.nx + i;
+    if ((f >> 5) < (int64_t)bits.size()) bits[f >> 5] &= ~(1u << (f & 31));
+  }
+
+  // Pairs of a ray's sorted hits under NEW_INTERSECTION_FILTERING (src/Surface.cpp:5262-5282).
+  void pairs_of(int64_t id, std::vector<std::pair<int64_t, int64_t>>& pr) const {
+    pr.clear();
+    int64_t s = pix_off[id], vsize = pix_off[id + 1] - s;
+    if (vsize == 0 || (vsize & 1)) return;
+    for (int64_t i = 0; i < vsize; i += 2)
+      if (fabs(pix_t[s + i + 1] - pix_t[s + i]) >= NS_EPS_INT) pr.push_back({s + i, s + i + 1});
+  }
+
+  void fill_panel(int panel) {
+    int64_t na, nb;
+    if (panel == 0) { na = g.nz; nb = g.ny; }
+    else if (panel == 1) { na = g.ny; nb = g.nx; }
+    else { na = g.nz; nb = g.nx; }
+    std::vector<std::pair<int64_t, int64_t>> pr;
+    // phase 0: status map along x (only panel 0 when the status map is built)
+    if (panels[0] > 0 && panel == 0) {
+      flagsum++;
+      double pa[3], pb[3];
+      pa[0] = X(0); pb[0] = X(g.nx - 1);
+      for (int64_t n = 0; n < na; n++) {
+        pa[2] = Z(n);
+        for (int64_t m = 0; m < nb; m++) {
+          int64_t id = (n * NMAX + m) * numPanels + panel;
+          pairs_of(id, pr);
+          if (pr.empty()) continue;
+          pa[1] = Y(m);
+          double dir = pb[0] - pa[0];
+          double lvi = 0.0;
+          for (auto& q : pr) {
+            double lim1 = pa[0] + dir * pix_t[q.first];
+            double lim2 = pa[0] + dir * pix_t[q.second];
+            lvi += lim2 - lim1;
+            int64_t i1 = (int64_t)rintp((lim1 - g.xmin) * g.scale);
+            int64_t i2 = (int64_t)rintp((lim2 - g.xmin) * g.scale);
+            i1 = i1 < 0 ? 0 : (i1 >= g.nx ? g.nx - 1 : i1);
+            i2 = i2 < 0 ? 0 : (i2 >= g.nx ? g.nx - 1 : i2);
+            if (i2 < i1) continue;
+            for (int64_t ix = i1; ix <= i2; ix++) {
+              double xx = X(ix);
+              if (xx <= lim2 && xx >= lim1) status[(n * g.ny + m) * g.nx + ix] = NS_STATUS_INSIDE;
+            }
+          }
+          volPanel[panel] += lvi;
+        }
+      }
+    }
+    if (!(flags & 2)) return;  // accurate triangulation rays
+    flagsum++;
+    double delta = NS_DELTA - g.hside;
+    int vc = panel == 0 ? 0 : (panel == 1 ? 2 : 1);
+    double pa[3], pb[3];
+    pa[vc] = coord(vc, 0) + delta;
+    pb[vc] = coord(vc, Nd(vc) - 1) + delta;
+    for (int64_t n = 0; n < na; n++) {
+      if (panel == 0) pa[2] = Z(n) + delta;
+      else if (panel == 1) pa[1] = Y(n) + delta;
+      else pa[2] = Z(n) + delta;
+      for (int64_t m = 0; m < nb; m++) {
+        int64_t id = (n * NMAX + m) * numPanels + (panels[0] + panel);
+        pairs_of(id, pr);
+        if (pr.empty()) continue;
+        if (panel == 0) pa[1] = Y(m) + delta;
+        else pa[0] = X(m) + delta;
+        double dir = pb[vc] - pa[vc];
+        double lvi = 0.0;
+        for (auto& q : pr) {
+          double lim1 = pa[vc] + dir * pix_t[q.first];
+          double lim2 = pa[vc] + dir * pix_t[q.second];
+          lvi += lim2 - lim1;
+          int64_t a = (int64_t)rintp((lim1 - mind(vc)) * g.scale);
+          int64_t b = (int64_t)rintp((lim2 - mind(vc)) * g.scale);
+          if (b <= a) continue;
+          double v1[3] = {pa[0], pa[1], pa[2]}, v2[3] = {pa[0], pa[1], pa[2]};
+          v1[vc] = lim1;
+          v2[vc] = lim2;
+          int32_t e1[4], e2[4];
+          if (panel == 0) {
+            for (int64_t i = a + 1; i <= b; i++) clear_bit(i, m, n);
+            int32_t t1[4] = {(int32_t)a, (int32_t)m, (int32_t)n, NS_X_DIR};
+            int32_t t2[4] = {(int32_t)b, (int32_t)m, (int32_t)n, NS_X_DIR};
+            memcpy(e1, t1, sizeof e1); memcpy(e2, t2, sizeof e2);
+          } else if (panel == 1) {
+            for (int64_t k = a + 1; k <= b; k++) clear_bit(m, n, k);
+            int32_t t1[4] = {(int32_t)m, (int32_t)n, (int32_t)a, NS_Z_DIR};
+            int32_t t2[4] = {(int32_t)m, (int32_t)n, (int32_t)b, NS_Z_DIR};
+            memcpy(e1, t1, sizeof e1); memcpy(e2, t2, sizeof e2);
+          } else {
+            for (int64_t j = a + 1; j <= b; j++) clear_bit(m, j, n);
+            int32_t t1[4] = {(int32_t)m, (int32_t)a, (int32_t)n, NS_Y_DIR};
+            int32_t t2[4] = {(int32_t)m, (int32_t)b, (int32_t)n, NS_Y_DIR};
+            memcpy(e1, t1, sizeof e1); memcpy(e2, t2, sizeof e2);
+          }
+          vert.insert(vert.end(), v1, v1 + 3);
+          vert_edge.insert(vert_edge.end(), e1, e1 + 4);
+          vert.insert(vert.end(), v2, v2 + 3);
+          vert_edge.insert(vert_edge.end(), e2, e2 + 4);
+        }
+        volPanel[panel] += lvi;
+      }
+    }
+  }
+
+  // Flood fill of one 6-connected region of value idold with idnew, in the scanline order of
+  // floodFillWithBilevelStatusMap2; returns the visited nodes in fill order.
+  void flood(int64_t si, int64_t sj, int64_t sk, int idold, int idnew, std::vector<int64_t>* nodes) {
+    auto S = [&](int64_t i, int64_t j, int64_t k) -> int32_t& { return status[(k * g.ny + j) * g.nx + i]; };
+    std::deque<std::array<int64_t, 3>> zq;
+    zq.push_back({si, sj, sk});
+    while (!zq.empty()) {
+      auto tr = zq.front();
+      zq.pop_front();
+      int64_t i = tr[0], j = tr[1], k = tr[2];
+      if (S(i, j, k) == idnew) continue;
+      std::stack<std::pair<int64_t, int64_t>> xy;
+      xy.push({i, j});
+      while (!xy.empty()) {
+        auto d = xy.top();
+        xy.pop();
+        i = d.first;
+        j = d.second;
+        bool spanLeft = false, spanRight = false;
+        int64_t i1 = i;
+        while (i1 >= 0 && S(i1, j, k) == idold) i1--;
+        i1++;
+        while (i1 < g.nx) {
+          if (S(i1, j, k) != idold) break;
+          S(i1, j, k) = idnew;
+          if (nodes) nodes->push_back((k * g.ny + j) * g.nx + i1);
+          if (k < g.nz - 1 && S(i1, j, k + 1) == idold) zq.push_back({i1, j, k + 1});
+          if (k > 0 && S(i1, j, k - 1) == idold) zq.push_back({i1, j, k - 1});
+          if (!spanLeft && j > 0) {
+            if (S(i1, j - 1, k) == idold) { xy.push({i1, j - 1}); spanLeft = true; }
+          } else if (spanLeft && j > 0) {
+            if (S(i1, j - 1, k) != idold) spanLeft = false;
+          }
+          if (!spanRight && j < g.ny - 1) {
+            if (S(i1, j + 1, k) == idold) { xy.push({i1, j + 1}); spanRight = true; }
+          } else if (spanRight && j < g.ny - 1) {
+            if (S(i1, j + 1, k) != idold) spanRight = false;
+          }
+          i1++;
+        }
+      }
+    }
+  }
+
+  void cavities() {
+    int id = NS_STATUS_TEMPORARY_OUT;
+    int times = 0;
+    std::vector<std::vector<int64_t>> cav_nodes;
+    // search cursors: the scan restarts from the beginning in the reference; since nodes only
+    // ever leave the TEMPORARY_OUT state, resuming from the last hit position is equivalent.
+    int64_t cur_up = 0, cur_dn = 0;
+    const int64_t plane = g.nx * g.ny;
+    const int64_t total = plane * g.nz;
+    while (true) {
+      int64_t found = -1;
+      if (times % 2 == 0) {
+        for (int64_t s = cur_up; s < total; s++)
+          if (status[s] == NS_STATUS_TEMPORARY_OUT) { found = s; break; }
+        if (found >= 0) cur_up = found;
+      } else {
+        for (int64_t s = cur_dn; s < total; s++) {
+          int64_t k = g.nz - 1 - s / plane;
+          int64_t f = k * plane + (s % plane);
+          if (status[f] == NS_STATUS_TEMPORARY_OUT) { found = f; cur_dn = s; break; }
+        }
+      }
+      times++;
+      if (found < 0) break;
+      id++;
+      int64_t k = found / plane, j = (found % plane) / g.nx, i = found % g.nx;
+      std::vector<int64_t> nodes;
+      flood(i, j, k, NS_STATUS_TEMPORARY_OUT, id, id >= NS_STATUS_FIRST_CAV ? &nodes : nullptr);
+      if (id >= NS_STATUS_FIRST_CAV) cav_nodes.push_back(std::move(nodes));
+    }
+    ncav = id - NS_STATUS_OUT;
+    double cubeVol = g.side * g.side * g.side;
+    cav_size.assign(cav_nodes.size(), 0);
+    cav_filled.assign(cav_nodes.size(), 0);
+    for (size_t c = 0; c < cav_nodes.size(); c++) {
+      double cv = cav_nodes[c].size() * cubeVol;
+      cav_size[c] = cv;
+      if (cv <= cav_vol) {
+        cav_filled[c] = 1;
+        if (flags & 2)
+          for (int64_t f : cav_nodes[c]) {
+            int64_t k = f / plane, j = (f % plane) / g.nx, i = f % g.nx;
+            for (int dk = 0; dk < 2; dk++)
+              for (int dj = 0; dj < 2; dj++)
+                for (int di = 0; di < 2; di++) clear_bit(i + di, j + dj, k + dk);
+          }
+      }
+    }
+  }
+
+  std::vector<int32_t> idx[3];  // edge -> vertex index, dense per direction
+  int64_t IX(int64_t i, int64_t j, int64_t k) const { return (k * g.ny + j) * g.nx + i; }
+
+  // Dangling-vertex removal and first-vertex-per-edge wins (assembleVerticesList).
+  void assemble() {
+    vlist.clear();
+    vkey.clear();
+    int64_t tot = g.nx * g.ny * g.nz;
+    for (int d = 0; d < 3; d++) idx[d].assign(tot, -1);
+    size_t nv = vert_edge.size() / 4;
+    for (size_t v = 0; v < nv; v++) {
+      const int32_t* e = &vert_edge[4 * v];
+      bool a = rbit(e[0], e[1], e[2]);
+      bool b;
+      if (e[3] == NS_X_DIR) b = rbit(e[0] + 1, e[1], e[2]);
+      else if (e[3] == NS_Y_DIR) b = rbit(e[0], e[1] + 1, e[2]);
+      else b = rbit(e[0], e[1], e[2] + 1);
+      if (a == b) continue;
+      int32_t& slot = idx[e[3]][IX(e[0], e[1], e[2])];
+      if (slot != -1) continue;
+      slot = (int32_t)(vlist.size() / 3);
+      vlist.insert(vlist.end(), &vert[3 * v], &vert[3 * v] + 3);
+      vkey.insert(vkey.end(), e, e + 4);
+    }
+  }
+
+  void triangulate() {
+    int64_t tot = g.nx * g.ny * g.nz;
+    std::vector<char> active(tot, 0);
+    auto cube = [&](int64_t i, int64_t j, int64_t k) {
+      int c = 0;
+      if (!rbit(i, j, k)) c |= 1;
+      if (!rbit(i + 1, j, k)) c |= 2;
+      if (!rbit(i + 1, j + 1, k)) c |= 4;
+      if (!rbit(i, j + 1, k)) c |= 8;
+      if (!rbit(i, j, k + 1)) c |= 16;
+      if (!rbit(i + 1, j, k + 1)) c |= 32;
+      if (!rbit(i + 1, j + 1, k + 1)) c |= 64;
+      if (!rbit(i, j + 1, k + 1)) c |= 128;
+      return c;
+    };
+    static const int ec[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6}, {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
+    auto emask = [&](int c) {
+      int m = 0;
+      for (int e = 0; e < 12; e++)
+        if (((c >> ec[e][0]) & 1) != ((c >> ec[e][1]) & 1)) m |= 1 << e;
+      return m;
+    };
+    // pass 1: active cubes and midpoint vertices for own edges 5, 6, 10 (getVertices)
+    for (int64_t k = 1; k < g.nz - 1; k++)
+      for (int64_t j = 1; j < g.ny - 1; j++)
+        for (int64_t i = 1; i < g.nx - 1; i++) {
+          int c = cube(i, j, k);
+          int m = emask(c);
+          if (m == 0) continue;
+          active[IX(i, j, k)] = 1;
+          if (m & 32) {
+            int32_t& s = idx[NS_Y_DIR][IX(i + 1, j, k + 1)];
+            if (s == -1) {
+              double p[3] = {X(i + 1) - g.hside, Y(j), Z(k + 1) - g.hside};
+              s = (int32_t)(vlist.size() / 3);
+              vlist.insert(vlist.end(), p, p + 3);
+              int32_t e[4] = {(int32_t)(i + 1), (int32_t)j, (int32_t)(k + 1), NS_Y_DIR};
+              vkey.insert(vkey.end(), e, e + 4);
+            }
+          }
+          if (m & 64) {
+            int32_t& s = idx[NS_X_DIR][IX(i, j + 1, k + 1)];
+            if (s == -1) {
+              double p[3] = {X(i), Y(j + 1) - g.hside, Z(k + 1) - g.hside};
+              s = (int32_t)(vlist.size() / 3);
+              vlist.insert(vlist.end(), p, p + 3);
+              int32_t e[4] = {(int32_t)i, (int32_t)(j + 1), (int32_t)(k + 1), NS_X_DIR};
+              vkey.insert(vkey.end(), e, e + 4);
+            }
+          }
+          if (m & 1024) {
+            int32_t& s = idx[NS_Z_DIR][IX(i + 1, j + 1, k)];
+            if (s == -1) {
+              double p[3] = {X(i + 1) - g.hside, Y(j + 1) - g.hside, Z(k)};
+              s = (int32_t)(vlist.size() / 3);
+              vlist.insert(vlist.end(), p, p + 3);
+              int32_t e[4] = {(int32_t)(i + 1), (int32_t)(j + 1), (int32_t)k, NS_Z_DIR};
+              vkey.insert(vkey.end(), e, e + 4);
+            }
+          }
+        }
+    // pass 2: triangles and Heron area (triangulationKernel / getTriangles)
+    area = 0;
+    for (int64_t k = 1; k < g.nz - 1; k++)
+      for (int64_t j = 1; j < g.ny - 1; j++)
+        for (int64_t i = 1; i < g.nx - 1; i++) {
+          if (!active[IX(i, j, k)]) continue;
+          int c = cube(i, j, k);
+          int m = emask(c);
+          int vl[12];
+          for (int e = 0; e < 12; e++) vl[e] = -1;
+          const int64_t ek[12][4] = {{i, j, k, 0}, {i + 1, j, k, 1}, {i, j + 1, k, 0}, {i, j, k, 1},
+                                     {i, j, k + 1, 0}, {i + 1, j, k + 1, 1}, {i, j + 1, k + 1, 0}, {i, j, k + 1, 1},
+                                     {i, j, k, 2}, {i + 1, j, k, 2}, {i + 1, j + 1, k, 2}, {i, j + 1, k, 2}};
+          for (int e = 0; e < 12; e++)
+            if (m & (1 << e)) vl[e] = idx[ek[e][3]][IX(ek[e][0], ek[e][1], ek[e][2])];
+          const char* cs = kNsMcCases[c];
+          for (int q = 0; cs[q]; q += 3) {
+            int a = vl[cs[q] <= '9' ? cs[q] - '0' : cs[q] - 'a' + 10];
+            int b = vl[cs[q + 1] <= '9' ? cs[q + 1] - '0' : cs[q + 1] - 'a' + 10];
+            int cc = vl[cs[q + 2] <= '9' ? cs[q + 2] - '0' : cs[q + 2] - 'a' + 10];
+            if (a == -1 || b == -1 || cc == -1) continue;
+            const double* A = &vlist[3 * (int64_t)a];
+            const double* B = &vlist[3 * (int64_t)b];
+            const double* Cc = &vlist[3 * (int64_t)cc];
+            double da = sqrt((A[0] - B[0]) * (A[0] - B[0]) + (A[1] - B[1]) * (A[1] - B[1]) + (A[2] - B[2]) * (A[2] - B[2]));
+            double db = sqrt((A[0] - Cc[0]) * (A[0] - Cc[0]) + (A[1] - Cc[1]) * (A[1] - Cc[1]) + (A[2] - Cc[2]) * (A[2] - Cc[2]));
+            double dc = sqrt((B[0] - Cc[0]) * (B[0] - Cc[0]) + (B[1] - Cc[1]) * (B[1] - Cc[1]) + (B[2] - Cc[2]) * (B[2] - Cc[2]));
+            double ttt = (da + db + dc) * (db + dc - da) * (dc + da - db) * (da + db - dc);
+            if (ttt > 0) area += 0.25 * sqrt(ttt);
+            tris.push_back(cc);
+            tris.push_back(b);
+            tris.push_back(a);
+          }
+        }
+  }
+
+  void run() {
+    NMAX = std::max(g.nx, std::max(g.ny, g.nz));
+    panels[0] = (flags & 1) ? 1 : 0;
+    panels[1] = (flags & 2) ? 3 : 0;
+    numPanels = panels[0] + panels[1];
+    if (flags & 1) status.assign(g.nx * g.ny * g.nz, NS_STATUS_TEMPORARY_OUT);
+    if (flags & 2) {
+      int64_t cnx = (g.nx + 31) >> 5;
+      bits.assign(cnx * g.ny * g.nz, ~0u);
+    }
+    if (P.n > 0 && numPanels > 0) trace();
+    else {
+      pix_off.assign(NMAX * NMAX * std::max(1, numPanels) + 1, 0);
+    }
+    int np = (flags & 2) ? 3 : ((flags & 1) ? 1 : 0);
+    for (int panel = 0; panel < np; panel++) fill_panel(panel);
+    volume = flagsum ? g.A * (volPanel[0] + volPanel[1] + volPanel[2]) / flagsum : 0;
+    if ((flags & 4) && (flags & 1)) cavities();
+    if (flags & 2) {
+      assemble();
+      if (flags & 8) triangulate();
+    }
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+// flags: 1 status map, 2 accurate-triangulation rays + insideness, 4 cavity detection/filling,
+//        8 marching cubes.
+void* nso_run(const NsGrid* g, int64_t n_patches, const double* f64, const int32_t* i32, const double* pool,
+              const int8_t* pool_flag, double probe, int flags, double cav_vol, int nthreads) {
+  Oracle* o = new Oracle();
+  o->g = *g;
+  o->P = {n_patches, f64, i32, pool, pool_flag, probe};
+  o->flags = flags;
+  o->cav_vol = cav_vol;
+  o->nthreads = nthreads;
+  o->run();
+  return o;
+}
+
+double nso_scalar(void* h, const char* what) {
+  Oracle* o = (Oracle*)h;
+  std::string w(what);
+  if (w == "volume") return o->volume;
+  if (w == "area") return o->area;
+  if (w == "ncav") return o->ncav;
+  if (w == "n_hits") return (double)o->n_hits;
+  if (w == "vol_panel0") return o->volPanel[0];
+  if (w == "vol_panel1") return o->volPanel[1];
+  if (w == "vol_panel2") return o->volPanel[2];
+  return NAN;
+}
+
+int64_t nso_size(void* h, const char* what) {
+  Oracle* o = (Oracle*)h;
+  std::string w(what);
+  if (w == "status") return (int64_t)o->status.size();
+  if (w == "bits") return (int64_t)o->bits.size();
+  if (w == "verts") return (int64_t)o->vlist.size();
+  if (w == "vkeys") return (int64_t)o->vkey.size();
+  if (w == "tris") return (int64_t)o->tris.size();
+  if (w == "cav_size") return (int64_t)o->cav_size.size();
+  if (w == "pix_off") return (int64_t)o->pix_off.size();
+  if (w == "pix_t") return (int64_t)o->pix_t.size();
+  return -1;
+}
+
+int nso_copy(void* h, const char* what, void* dst) {
+  Oracle* o = (Oracle*)h;
+  std::string w(what);
+  if (w == "status") memcpy(dst, o->status.data(), o->status.size() * 4);
+  else if (w == "bits") memcpy(dst, o->bits.data(), o->bits.size() * 4);
+  else if (w == "verts") memcpy(dst, o->vlist.data(), o->vlist.size() * 8);
+  else if (w == "vkeys") memcpy(dst, o->vkey.data(), o->vkey.size() * 4);
+  else if (w == "tris") memcpy(dst, o->tris.data(), o->tris.size() * 4);
+  else if (w == "cav_size") memcpy(dst, o->cav_size.data(), o->cav_size.size() * 8);
+  else if (w == "cav_filled") memcpy(dst, o->cav_filled.data(), o->cav_filled.size() * 4);
+  else if (w == "pix_off") memcpy(dst, o->pix_off.data(), o->pix_off.size() * 8);
+  else if (w == "pix_t") memcpy(dst, o->pix_t.data(), o->pix_t.size() * 8);
+  else return -1;
+  return 0;
+}
+
+void nso_free(void* h) { delete (Oracle*)h; }
+
+// Individual math restatements, exposed for the known-answer tests.
+int nso_ray_sphere(const double* orig, const double* dir, const double* c, double r, double* t) {
+  return ray_sphere(orig, dir, c, r, &t[0], &t[1]) ? 1 : 0;
+}
+int nso_quartic(double b, double c, double d, double e, double* roots) {
+  int n = 0;
+  quartic(roots, b, c, d, e, &n);
+  return n;
+}
+double nso_real_cubic(double b, double c, double d) { return real_cubic(b, c, d); }
+
+}  // extern "C"
