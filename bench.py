@@ -1,0 +1,376 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 grid ray-casting surface builder.
+
+One step = one full surface pass of one structure: ray casting of the status ray set and the
+three accurate-triangulation ray sets (hits, status map, insideness bits, volume), cavity
+detection and filling, vertex assembly and marching cubes.  ``value`` is measured with the patch
+set resident in HBM; ``e2e`` is the same pass through the C-ABI with host buffers: patch upload
+from pinned memory, the GPU pass, and the download of the status map, the mesh and the cavity
+table.  The status map (4 bytes per node) is larger than L2, so no extra flush is needed.
+
+The default workload is the large SES globule: 100,000 atoms, probe 1.4 A, grid scale 4.0,
+perfil 70 (about 1050^3 nodes).  Multiple GPUs run independent replicas (the path has no
+cross-GPU exchange).
+
+``--impl reference`` times the CPU restatement of the reference path on a bounded slab sample of
+the same workload with all host threads, and prints the same JSON line with ``impl: reference``.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "structures/s and rays/s, mixed-prec vs FP64 GPU kernel at ≤1e-5 Å hit error"
+
+WORKLOADS = {
+    # name: atoms, generator seed, probe, scale, perfil, cavity fill threshold
+    "ses_100k": dict(n=100000, seed=3, probe=1.4, scale=4.0, perfil=70.0, cav_vol=10.0),
+    "ses_10k": dict(n=10000, seed=2, probe=1.4, scale=3.0, perfil=80.0, cav_vol=10.0),
+    "ses_327": dict(n=327, seed=1, probe=1.4, scale=2.0, perfil=70.0, cav_vol=10.0),
+}
+
+STAGES = ("bin", "trace", "overflow", "cavity", "vertex", "mc")
+
+
+def load_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": d.get("hbm_gbs", 6650.0), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.out, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.out.flush()
+        rows = []
+        for line in Path(self.out.name).read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                rows.append(f)
+        os.unlink(self.out.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def make_workload(name: str):
+    from nanoshaper_b200 import generator
+    import nanoshaper_b200 as nb
+    w = WORKLOADS[name]
+    t0 = time.perf_counter()
+    atoms = generator.rsa_globule(w["n"], w["seed"])
+    t_gen = time.perf_counter() - t0
+    nb.reset_seed()
+    ds = nb.DelPhiShared(atoms, w["scale"], w["perfil"])
+    cf = nb.ConfigFile()
+    cf.add("Surface", "ses")
+    cf.add("Probe_Radius", w["probe"])
+    cf.add("Accurate_Triangulation", True)
+    cf.add("Triangulation", True)
+    surf = nb.surfaceFactory().create(cf, ds)
+    t0 = time.perf_counter()
+    surf.build()
+    t_build = time.perf_counter() - t0
+    return w, atoms, ds, surf, t_gen, t_build
+
+
+def run_reference(args, w, ds, surf) -> dict:
+    """CPU restatement of the reference path on a bounded slab sample, all host threads."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    O.build()
+    threads = os.cpu_count() or 1
+    g = ds.grid
+    rays_total = g.nz * g.ny + (g.nz * g.ny + g.ny * g.nx + g.nz * g.nx)
+    # size the slab for roughly ten seconds of work per step from a small probe run
+    t_probe, r_probe = O.time_slab(g, surf.patches, threads, 0.48, 0.50)
+    per_ray = t_probe / max(r_probe, 1)
+    frac = min(1.0, max(0.01, 10.0 / max(per_ray * rays_total, 1e-9)))
+    lo = 0.5 - frac / 2
+    hi = 0.5 + frac / 2
+    times = []
+    rays = 0
+    for _ in range(args.warmup):
+        O.time_slab(g, surf.patches, threads, lo, hi)
+    for _ in range(args.steps):
+        dt, rays = O.time_slab(g, surf.patches, threads, lo, hi)
+        times.append(dt)
+    t = max(statistics.median(times), 1e-9)
+    rays_per_s = rays / t
+    structs = rays_per_s / rays_total
+    sample = (f"ray casting (status + 3 triangulation ray sets) of the central slab "
+              f"[{lo:.3f}, {hi:.3f}) of every ray set, {rays} of {rays_total} rays; cavity detection and "
+              f"marching cubes not included; structures/s extrapolated from rays/s")
+    return {"value": structs, "rays_per_s": rays_per_s, "cores": threads, "kind": "port", "sample": sample,
+            "unit": "structures/s"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
+    ap.add_argument("--workload", default="ses_100k", choices=sorted(WORKLOADS))
+    ap.add_argument("--precision", default="fp64", choices=("fp64", "mixed"))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+    world, rank, local = dist_setup()
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        w, atoms, ds, surf, t_gen, t_build = make_workload(args.workload)
+        cb = run_reference(args, w, ds, surf)
+        g = ds.grid
+        line = {
+            "impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "structures/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "rays_per_s": cb["rays_per_s"],
+            "config": {"workload": args.workload, "atoms": w["n"], "probe": w["probe"], "scale": w["scale"],
+                       "perfil": w["perfil"], "grid": [g.nx, g.ny, g.nz], "patches": surf.patches.n},
+            "cpu_baseline": {"value": cb["value"], "unit": "structures/s", "cores": cb["cores"], "kind": cb["kind"],
+                             "sample": cb["sample"]},
+            "e2e": {"value": cb["value"], "unit": "structures/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line))
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        pg = dist
+
+    import nanoshaper_b200 as nb
+    from nanoshaper_b200 import _native as N
+    from nanoshaper_b200 import build as nbuild
+    nbuild.build()
+    L = N.lib()
+
+    w, atoms, ds, surf, t_gen, t_build = make_workload(args.workload)
+    surf.device = local
+    surf.precision = args.precision
+    g = ds.grid
+    p = surf.patches
+    ctx = surf._context().handle
+    prec = 0 if args.precision == "fp64" else 1
+    flags = N.STATUS | N.ACCURATE_TRIANGULATION
+
+    def barrier():
+        if pg is not None:
+            pg.barrier()
+        torch.cuda.synchronize()
+
+    # device-resident inputs
+    surf.upload()
+
+    def step():
+        v = ctypes.c_double()
+        N.check(L.nsg_raycast(ctx, flags, prec, ctypes.byref(v)), "raycast")
+        nc = ctypes.c_int()
+        N.check(L.nsg_cavities(ctx, w["cav_vol"], ctypes.byref(nc)), "cavities")
+        a = ctypes.c_double()
+        nv = ctypes.c_int64()
+        nt = ctypes.c_int64()
+        N.check(L.nsg_triangulate(ctx, ctypes.byref(a), ctypes.byref(nv), ctypes.byref(nt)), "triangulate")
+        return v.value, a.value, nc.value, nv.value, nt.value
+
+    # per-stage kernel times from one profiled (untimed) pass
+    N.check(L.nsg_profile(ctx, 1), "profile")
+    step()
+    stage_ms = np.zeros(8)
+    stage_calls = np.zeros(8, np.int64)
+    L.nsg_stage_times(ctx, stage_ms.ctypes.data, stage_calls.ctypes.data, 8)
+    N.check(L.nsg_profile(ctx, 0), "profile")
+    stats = surf.stats()
+
+    for _ in range(args.warmup):
+        step()
+    barrier()
+    clk = ClockSampler(local)
+    clk.start()
+    launches0 = L.nsg_launch_count(ctx)
+    N.check(L.nsg_event_record(ctx, 0), "event")
+    for _ in range(args.steps):
+        vol, area, ncav, nv, nt = step()
+    N.check(L.nsg_event_record(ctx, 1), "event")
+    ms = ctypes.c_double()
+    N.check(L.nsg_event_elapsed(ctx, 0, 1, ctypes.byref(ms)), "elapsed")
+    launches = L.nsg_launch_count(ctx) - launches0
+    barrier()
+    clocks = clk.stop()
+    ms_per_step = ms.value / args.steps
+    if pg is not None:
+        t = torch.tensor([ms_per_step], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms_per_step = float(t.item())
+
+    rays_per_struct = g.nz * g.ny + (g.nz * g.ny + g.ny * g.nx + g.nz * g.nx)
+    nodes = g.nx * g.ny * g.nz
+    structs_per_s = world * 1000.0 / ms_per_step
+    rays_per_s = structs_per_s * rays_per_struct
+    nodes_per_s = structs_per_s * nodes
+
+    # e2e through the C-ABI with pinned host buffers
+    pin = {}
+    for name in ("f64", "i32", "pool", "pool_flag"):
+        a = getattr(p, name)
+        t = torch.empty(a.nbytes, dtype=torch.uint8, pin_memory=True)
+        t.numpy()[:] = a.view(np.uint8).ravel()
+        pin[name] = t
+    status_host = torch.empty(nodes * 4, dtype=torch.uint8, pin_memory=True)
+    verts_host = torch.empty(max(nv, 1) * 24 + 4096, dtype=torch.uint8, pin_memory=True)
+    keys_host = torch.empty(max(nv, 1) * 16 + 4096, dtype=torch.uint8, pin_memory=True)
+    tris_host = torch.empty(max(nt, 1) * 12 + 4096, dtype=torch.uint8, pin_memory=True)
+    h2d = sum(t.numel() for t in pin.values())
+
+    def e2e_step():
+        N.check(L.nsg_upload_patches(ctx, p.n, pin["f64"].data_ptr(), pin["i32"].data_ptr(), len(p.pool),
+                                     pin["pool"].data_ptr(), pin["pool_flag"].data_ptr(), p.probe), "upload")
+        r = step()
+        N.check(L.nsg_download_status(ctx, status_host.data_ptr()), "download status")
+        N.check(L.nsg_download_mesh(ctx, verts_host.data_ptr(), keys_host.data_ptr(), tris_host.data_ptr()), "mesh")
+        return r
+
+    e2e_steps = max(2, min(args.steps, 5))
+    e2e_step()
+    barrier()
+    N.check(L.nsg_event_record(ctx, 2), "event")
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        r = e2e_step()
+    N.check(L.nsg_event_record(ctx, 3), "event")
+    e2e_wall = (time.perf_counter() - t0) / e2e_steps
+    e_ms = ctypes.c_double()
+    N.check(L.nsg_event_elapsed(ctx, 2, 3, ctypes.byref(e_ms)), "elapsed")
+    e2e_ms = max(e_ms.value / e2e_steps, e2e_wall * 1000.0)
+    if pg is not None:
+        t = torch.tensor([e2e_ms], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    d2h = nodes * 4 + r[3] * (24 + 16) + r[4] * 12
+
+    # roofline of the dominant stage (HBM: algorithmic bytes per launch / measured launch time)
+    peaks = load_peaks()
+    stage_times = {STAGES[i]: float(stage_ms[i]) for i in range(len(STAGES))}
+    dominant = max(stage_times, key=stage_times.get)
+    nwords = ((g.nx + 31) // 32) * g.ny * g.nz
+    ncav_nodes = nodes  # cavity pass streams the whole status map
+    alg_bytes = {
+        # status rows written (4 B/node) + bit grid (cleared by three ray sets, read+write) +
+        # per-ray interval-length words and pair records of the triangulation rays
+        "trace": 4 * nodes + 3 * 2 * 4 * nwords + 8 * rays_per_struct + 16 * nv,
+        "overflow": 4 * nodes,
+        "bin": 6 * 4 * p.n,
+        # union-find: status read (init, hook), labels write+read (init, hook, compress, stats,
+        # label), status write (label) -- 4 B each
+        "cavity": 4 * ncav_nodes * 8,
+        "vertex": 8 * 2 * nv + 40 * nv,
+        "mc": nwords * 4 * 8 + 40 * nv + 12 * nt,
+    }
+    dom_ms = stage_times[dominant] / max(int(stage_calls[STAGES.index(dominant)]), 1)
+    achieved = alg_bytes[dominant] / (dom_ms / 1000.0) / 1e9
+    roofline = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"], "traffic": None, "peak_source": peaks["source"],
+                "stage_ms": stage_times, "algorithmic_bytes": alg_bytes[dominant]}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cb = run_reference(argparse.Namespace(steps=1, warmup=0), w, ds, surf)
+            cpu = {"value": cb["value"], "unit": "structures/s", "cores": cb["cores"], "kind": cb["kind"],
+                   "sample": cb["sample"], "rays_per_s": cb["rays_per_s"]}
+        except Exception as e:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": "structures/s", "cores": 0, "kind": "port", "sample": f"failed: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": structs_per_s, "unit": "structures/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+            "precision": args.precision, "data": "synthetic",
+            "rays_per_s": rays_per_s, "nodes_per_s": nodes_per_s,
+            "config": {"workload": args.workload, "atoms": w["n"], "probe": w["probe"], "scale": w["scale"],
+                       "perfil": w["perfil"], "grid": [g.nx, g.ny, g.nz], "patches": p.n,
+                       "patch_kinds": list(p.counts), "rays_per_structure": rays_per_struct,
+                       "l2": "inputs larger than L2 (status map %.1f GB)" % (nodes * 4 / 1e9),
+                       "parallelism": f"replicas x{world}"},
+            "result": {"volume": vol, "area": area, "cavities": ncav, "vertices": nv, "triangles": nt,
+                       "overflow_rays": stats["overflow_rays"]},
+            "host": {"patch_build_s": t_build, "generator_s": t_gen},
+            "clocks": clocks,
+            "e2e": {"value": world * 1000.0 / e2e_ms, "unit": "structures/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms},
+            "gpu_launches": int(launches),
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    surf.ctx.close()
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,17 @@
+"""B200-native grid ray-casting molecular surface builder (NanoShaper-compatible interface)."""
+from .surface import (  # noqa: F401
+    ConfigFile,
+    ConnollySurface,
+    Context,
+    DelPhiShared,
+    NanoShaper,
+    PatchSet,
+    Surface,
+    SurfaceFactory,
+    build_ses_patches,
+    read_xyzr,
+    reset_seed,
+    surfaceFactory,
+)
+
+__version__ = "0.1.0"

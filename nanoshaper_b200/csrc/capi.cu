@@ -1,0 +1,787 @@
+// C-ABI of the B200 grid ray-casting surface builder (libnsgpu).
+//
+// One context per host thread: it owns a CUDA stream and grow-only device buffers; host buffers
+// are always caller-owned.  Calls return NSG_OK or a negative NSG_ERR_* code, never exit.  The
+// entry points mirror the pieces of Surface::getSurf (src/Surface.cpp:398-1692) and
+// Surface::triangulateSurface (src/Surface.cpp:9909-10526) that run once the surface patches
+// exist: ray casting with status/insideness fill and volume, cavity detection and filling, vertex
+// assembly and marching cubes.  Declarations and the reference interface each one replaces are
+// in include/nsgpu.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cub/cub.cuh>
+
+#include "host/host_api.h"
+#include "kernels/cavity.h"
+#include "kernels/mc.h"
+#include "kernels/pipeline.h"
+
+namespace {
+
+thread_local char g_last_error[512] = "";
+
+int fail(int code, const char* what, cudaError_t e = cudaSuccess) {
+  if (e != cudaSuccess)
+    snprintf(g_last_error, sizeof g_last_error, "%s: %s", what, cudaGetErrorString(e));
+  else
+    snprintf(g_last_error, sizeof g_last_error, "%s", what);
+  return code;
+}
+
+#define CK(call)                                              \
+  do {                                                        \
+    cudaError_t e_ = (call);                                  \
+    if (e_ != cudaSuccess) return fail(NSG_ERR_CUDA, #call, e_); \
+  } while (0)
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  cudaError_t ensure(size_t bytes) {
+    if (bytes <= cap) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    size_t want = std::max<size_t>(bytes, 256);
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e == cudaSuccess) cap = want;
+    return e;
+  }
+  template <class T>
+  T* as() const { return (T*)p; }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
+}  // namespace
+
+struct nsg_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  NsGrid grid{};
+  nsg::GridDev gd{};
+  bool has_grid = false;
+  // patches
+  int64_t np = 0, npool = 0;
+  double probe = 1.4;
+  DevBuf f64, i32, pool, flag, win;
+  const double* ext_f64 = nullptr;  // device-resident patch arrays bound by the caller
+  const int32_t* ext_i32 = nullptr;
+  const double* ext_pool = nullptr;
+  const int8_t* ext_flag = nullptr;
+  bool has_patches = false;
+  // binning per panel
+  DevBuf tile_cnt[3], tile_off[3], tile_list[3];
+  // trace outputs
+  DevBuf status, bits, vol_ray[4];
+  DevBuf pairs, ray_pair_off, ray_pair_cnt, cursors, ovf_rays[4], ovf_scratch, err;
+  DevBuf hits, ray_hit_off[4], ray_hit_cnt[4];
+  int64_t pair_cap = 0, hit_cap = 0;
+  int flags = 0;
+  int precision = 0;
+  double volume = 0;
+  bool have_status = false, have_bits = false;
+  // cavities
+  DevBuf labels, is_root, roots, cc_count, cc_desc, cc_label_of, cc_fill_of, nroots_d;
+  int ncav = 0;
+  std::vector<double> cav_size;
+  std::vector<int32_t> cav_filled;
+  // mesh
+  DevBuf surv_cnt, surv_off, vpos, vkey, row_act_cnt, row_mid_cnt, row_act_off, row_mid_off, act_rec, act_mid,
+      tri_cnt, tri_off, tris, cube_area, red_out;
+  int64_t n_vert = 0, n_analytic = 0, n_tri = 0, n_active = 0;
+  double area = 0;
+  DevBuf temp;  // cub temporary storage
+  int64_t last_overflow_rays = 0;
+  // timing: user events and per-stage kernel times (milliseconds, summed over calls)
+  cudaEvent_t user_ev[8] = {};
+  bool profile = false;
+  cudaEvent_t st_ev[2 * 8] = {};
+  double stage_ms[8] = {};
+  int64_t stage_calls[8] = {};
+  int64_t launches = 0;
+};
+
+namespace {
+
+nsg::PatchDev patch_dev(nsg_ctx* c) {
+  nsg::PatchDev P;
+  P.n = c->np;
+  P.f64 = c->ext_f64 ? c->ext_f64 : c->f64.as<double>();
+  P.i32 = c->ext_i32 ? c->ext_i32 : c->i32.as<int32_t>();
+  P.pool = (const double4*)(c->ext_pool ? c->ext_pool : c->pool.as<double>());
+  P.flag = c->ext_flag ? c->ext_flag : c->flag.as<int8_t>();
+  P.probe = c->probe;
+  P.win = c->win.as<int32_t>();
+  return P;
+}
+
+int64_t nwords_of(const NsGrid& g) { return ((g.nx + 31) >> 5) * g.ny * g.nz; }
+
+// Stage ids of the per-stage kernel timers.
+enum { kStageBin = 0, kStageTrace = 1, kStageOverflow = 2, kStageCavity = 3, kStageVertex = 4, kStageMC = 5,
+       kStageCount = 6 };
+
+void stage_begin(nsg_ctx* c, int id) {
+  if (!c->profile) return;
+  if (!c->st_ev[2 * id]) {
+    cudaEventCreate(&c->st_ev[2 * id]);
+    cudaEventCreate(&c->st_ev[2 * id + 1]);
+  }
+  cudaEventRecord(c->st_ev[2 * id], c->stream);
+}
+
+void stage_end(nsg_ctx* c, int id) {
+  if (!c->profile) return;
+  cudaEventRecord(c->st_ev[2 * id + 1], c->stream);
+  cudaEventSynchronize(c->st_ev[2 * id + 1]);
+  float ms = 0;
+  cudaEventElapsedTime(&ms, c->st_ev[2 * id], c->st_ev[2 * id + 1]);
+  c->stage_ms[id] += ms;
+  c->stage_calls[id]++;
+}
+
+#define LAUNCH(call)  \
+  do {                \
+    c->launches++;    \
+    CK(call);         \
+  } while (0)
+
+// Exclusive scan of n int32 (or int64) counts into n+1 int64 offsets; returns the total.
+template <class In>
+int scan_counts(nsg_ctx* c, const In* in, int64_t n, int64_t* out, int64_t* total) {
+  size_t tb = 0;
+  CK(cub::DeviceScan::ExclusiveScan(nullptr, tb, in, out, cub::Sum(), (int64_t)0, n, c->stream));
+  CK(c->temp.ensure(tb));
+  tb = c->temp.cap;
+  CK(cub::DeviceScan::ExclusiveScan(c->temp.p, tb, in, out, cub::Sum(), (int64_t)0, n, c->stream));
+  if (total) {
+    int64_t last_off = 0;
+    In last_cnt = 0;
+    if (n > 0) {
+      CK(cudaMemcpyAsync(&last_off, out + n - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaMemcpyAsync(&last_cnt, in + n - 1, sizeof(In), cudaMemcpyDeviceToHost, c->stream));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    *total = last_off + (int64_t)last_cnt;
+    CK(cudaMemcpyAsync(out + n, total, sizeof(int64_t), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  }
+  return NSG_OK;
+}
+
+int reduce_sum(nsg_ctx* c, const double* in, int64_t n, double* host_out) {
+  if (n == 0) { *host_out = 0; return NSG_OK; }
+  CK(c->red_out.ensure(sizeof(double)));
+  size_t tb = 0;
+  CK(cub::DeviceReduce::Sum(nullptr, tb, in, c->red_out.as<double>(), n, c->stream));
+  CK(c->temp.ensure(tb));
+  tb = c->temp.cap;
+  CK(cub::DeviceReduce::Sum(c->temp.p, tb, in, c->red_out.as<double>(), n, c->stream));
+  CK(cudaMemcpyAsync(host_out, c->red_out.p, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return NSG_OK;
+}
+
+int bin_panel(nsg_ctx* c, int panel) {
+  nsg::RaySet rs = nsg::make_ray_set(panel == 0 ? 0 : panel + 1, c->gd);
+  int64_t ntiles = ((rs.nb + nsg::kTileM - 1) / nsg::kTileM) * ((rs.na + nsg::kTileN - 1) / nsg::kTileN);
+  CK(c->tile_cnt[panel].ensure((ntiles + 1) * sizeof(int32_t)));
+  CK(c->tile_off[panel].ensure((ntiles + 1) * sizeof(int64_t)));
+  CK(cudaMemsetAsync(c->tile_cnt[panel].p, 0, (ntiles + 1) * sizeof(int32_t), c->stream));
+  nsg::PatchDev P = patch_dev(c);
+  LAUNCH(nsg::launch_bin_count(P, c->gd, rs, c->tile_cnt[panel].as<int32_t>(), c->stream));
+  int64_t total = 0;
+  int rc = scan_counts(c, c->tile_cnt[panel].as<int32_t>(), ntiles, c->tile_off[panel].as<int64_t>(), &total);
+  if (rc) return rc;
+  CK(c->tile_list[panel].ensure(std::max<int64_t>(total, 1) * sizeof(int32_t)));
+  CK(cudaMemsetAsync(c->tile_cnt[panel].p, 0, (ntiles + 1) * sizeof(int32_t), c->stream));
+  LAUNCH(nsg::launch_bin_fill(P, c->gd, rs, c->tile_off[panel].as<int64_t>(), c->tile_cnt[panel].as<int32_t>(),
+                          c->tile_list[panel].as<int32_t>(), c->stream));
+  return NSG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* nsg_last_error(void) { return g_last_error; }
+
+int nsg_version(void) { return 1; }
+
+int nsg_ctx_create(int device, nsg_ctx** out) {
+  if (!out) return NSG_ERR_ARG;
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) return fail(NSG_ERR_CUDA, "no CUDA device", e);
+  if (device < 0 || device >= ndev) return fail(NSG_ERR_ARG, "device index out of range");
+  CK(cudaSetDevice(device));
+  nsg_ctx* c = new nsg_ctx();
+  c->device = device;
+  e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) { delete c; return fail(NSG_ERR_CUDA, "cudaStreamCreate", e); }
+  c->own_stream = true;
+  e = nsg::mc_init_tables();
+  if (e != cudaSuccess) { cudaStreamDestroy(c->stream); delete c; return fail(NSG_ERR_CUDA, "mc tables", e); }
+  *out = c;
+  return NSG_OK;
+}
+
+int nsg_ctx_destroy(nsg_ctx* c) {
+  if (!c) return NSG_ERR_ARG;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  DevBuf* bufs[] = {&c->f64, &c->i32, &c->pool, &c->flag, &c->win, &c->status, &c->bits, &c->pairs,
+                    &c->ray_pair_off, &c->ray_pair_cnt, &c->cursors, &c->ovf_scratch, &c->err, &c->hits,
+                    &c->labels, &c->is_root, &c->roots, &c->cc_count, &c->cc_desc, &c->cc_label_of,
+                    &c->cc_fill_of, &c->nroots_d, &c->surv_cnt, &c->surv_off, &c->vpos, &c->vkey,
+                    &c->row_act_cnt, &c->row_mid_cnt, &c->row_act_off, &c->row_mid_off, &c->act_rec,
+                    &c->act_mid, &c->tri_cnt, &c->tri_off, &c->tris, &c->cube_area, &c->red_out, &c->temp};
+  for (DevBuf* b : bufs) b->release();
+  for (int i = 0; i < 3; i++) { c->tile_cnt[i].release(); c->tile_off[i].release(); c->tile_list[i].release(); }
+  for (int i = 0; i < 4; i++) {
+    c->vol_ray[i].release(); c->ovf_rays[i].release(); c->ray_hit_off[i].release(); c->ray_hit_cnt[i].release();
+  }
+  for (int i = 0; i < 8; i++)
+    if (c->user_ev[i]) cudaEventDestroy(c->user_ev[i]);
+  for (int i = 0; i < 16; i++)
+    if (c->st_ev[i]) cudaEventDestroy(c->st_ev[i]);
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return NSG_OK;
+}
+
+// Use a caller-provided stream (e.g. a framework's current stream) instead of the context's own.
+int nsg_set_stream(nsg_ctx* c, void* stream) {
+  if (!c) return NSG_ERR_ARG;
+  CK(cudaSetDevice(c->device));
+  if (c->stream) CK(cudaStreamSynchronize(c->stream));
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  c->stream = (cudaStream_t)stream;
+  c->own_stream = false;
+  return NSG_OK;
+}
+
+int nsg_set_grid(nsg_ctx* c, const NsGrid* g) {
+  if (!c || !g) return NSG_ERR_ARG;
+  if (g->nx < 3 || g->ny < 3 || g->nz < 3) return fail(NSG_ERR_ARG, "grid must have at least 3 nodes per axis");
+  if (g->nx * g->ny * g->nz >= (int64_t)1 << 31) return fail(NSG_ERR_ARG, "grid larger than 2^31 nodes");
+  c->grid = *g;
+  c->gd.n[0] = g->nx; c->gd.n[1] = g->ny; c->gd.n[2] = g->nz;
+  c->gd.mn[0] = g->xmin; c->gd.mn[1] = g->ymin; c->gd.mn[2] = g->zmin;
+  c->gd.mx[0] = g->xmax; c->gd.mx[1] = g->ymax; c->gd.mx[2] = g->zmax;
+  c->gd.scale = g->scale; c->gd.side = g->side; c->gd.hside = g->hside;
+  c->has_grid = true;
+  c->have_status = c->have_bits = false;
+  return NSG_OK;
+}
+
+static int upload_common(nsg_ctx* c, int64_t n, int64_t npool, double probe) {
+  c->np = n;
+  c->npool = npool;
+  c->probe = probe;
+  CK(c->win.ensure(std::max<int64_t>(n, 1) * 6 * sizeof(int32_t)));
+  c->has_patches = true;
+  return NSG_OK;
+}
+
+int nsg_upload_patches(nsg_ctx* c, int64_t n, const double* f64, const int32_t* i32, int64_t npool,
+                       const double* pool, const int8_t* pool_flag, double probe) {
+  if (!c || n < 0 || npool < 0 || (n > 0 && (!f64 || !i32)) || (npool > 0 && (!pool || !pool_flag)))
+    return NSG_ERR_ARG;
+  CK(cudaSetDevice(c->device));
+  CK(c->f64.ensure(std::max<int64_t>(n, 1) * NS_PATCH_F64 * sizeof(double)));
+  CK(c->i32.ensure(std::max<int64_t>(n, 1) * NS_PATCH_I32 * sizeof(int32_t)));
+  CK(c->pool.ensure(std::max<int64_t>(npool, 1) * 4 * sizeof(double)));
+  CK(c->flag.ensure(std::max<int64_t>(npool, 1)));
+  if (n) {
+    CK(cudaMemcpyAsync(c->f64.p, f64, n * NS_PATCH_F64 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->i32.p, i32, n * NS_PATCH_I32 * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
+  }
+  if (npool) {
+    CK(cudaMemcpyAsync(c->pool.p, pool, npool * 4 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->flag.p, pool_flag, npool, cudaMemcpyHostToDevice, c->stream));
+  }
+  c->ext_f64 = nullptr; c->ext_i32 = nullptr; c->ext_pool = nullptr; c->ext_flag = nullptr;
+  return upload_common(c, n, npool, probe);
+}
+
+// Binds patch arrays that already live in device memory (no copy); they must stay valid until
+// the next bind/upload or the context's destruction.
+int nsg_bind_patches_device(nsg_ctx* c, int64_t n, const double* f64, const int32_t* i32, int64_t npool,
+                            const double* pool, const int8_t* pool_flag, double probe) {
+  if (!c || n < 0 || npool < 0) return NSG_ERR_ARG;
+  CK(cudaSetDevice(c->device));
+  c->ext_f64 = f64; c->ext_i32 = i32; c->ext_pool = pool; c->ext_flag = pool_flag;
+  return upload_common(c, n, npool, probe);
+}
+
+int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
+  if (!c || !c->has_grid || !c->has_patches) return fail(NSG_ERR_STATE, "grid and patches must be set first");
+  if (precision != 0) return fail(NSG_ERR_ARG, "unsupported precision");
+  CK(cudaSetDevice(c->device));
+  const NsGrid& g = c->grid;
+  const int64_t tot = g.nx * g.ny * g.nz;
+  const bool do_status = flags & 1;
+  const bool do_mc = flags & 2;
+  const bool keep_hits = flags & 16;
+  c->flags = flags;
+  c->precision = precision;
+  nsg::PatchDev P = patch_dev(c);
+  stage_begin(c, kStageBin);
+  LAUNCH(nsg::launch_windows(P, c->win.as<int32_t>(), c->gd, c->stream));
+  for (int panel = 0; panel < 3; panel++) {
+    if (panel == 0 && !(do_status || do_mc)) continue;
+    if (panel > 0 && !do_mc) continue;
+    int rc = bin_panel(c, panel);
+    if (rc) return rc;
+  }
+  stage_end(c, kStageBin);
+  const int64_t nwords = nwords_of(g);
+  const int64_t nrays_mc = g.nz * g.ny + g.ny * g.nx + g.nz * g.nx;
+  if (do_status) CK(c->status.ensure(tot * sizeof(int32_t)));
+  if (do_mc) {
+    CK(c->bits.ensure(nwords * sizeof(uint32_t)));
+    CK(cudaMemsetAsync(c->bits.p, 0xff, nwords * sizeof(uint32_t), c->stream));
+    CK(c->ray_pair_off.ensure(nrays_mc * sizeof(int64_t)));
+    CK(c->ray_pair_cnt.ensure(nrays_mc * sizeof(int32_t)));
+    CK(cudaMemsetAsync(c->ray_pair_cnt.p, 0, nrays_mc * sizeof(int32_t), c->stream));
+    if (c->pair_cap == 0) c->pair_cap = std::max<int64_t>(4 * nrays_mc, 1 << 16);
+  }
+  CK(c->cursors.ensure(8 * sizeof(unsigned long long)));
+  CK(c->err.ensure(sizeof(int32_t)));
+  const int ovf_cap = 1 << 16;
+  for (int attempt = 0; attempt < 4; attempt++) {
+    if (do_mc) CK(c->pairs.ensure(c->pair_cap * 2 * sizeof(double)));
+    if (keep_hits) {
+      if (c->hit_cap == 0) c->hit_cap = std::max<int64_t>(8 * (nrays_mc + g.nz * g.ny), 1 << 16);
+      CK(c->hits.ensure(c->hit_cap * sizeof(double)));
+    }
+    CK(cudaMemsetAsync(c->cursors.p, 0, 8 * sizeof(unsigned long long), c->stream));
+    CK(cudaMemsetAsync(c->err.p, 0, sizeof(int32_t), c->stream));
+    if (do_mc) CK(cudaMemsetAsync(c->bits.p, 0xff, nwords * sizeof(uint32_t), c->stream));
+    unsigned long long* cur = c->cursors.as<unsigned long long>();
+    int32_t* ovf_count = (int32_t*)(cur + 4);  // 4 int32 counters
+    int sets[4], nsets = 0;
+    if (do_status) sets[nsets++] = 0;
+    if (do_mc) { sets[nsets++] = 1; sets[nsets++] = 2; sets[nsets++] = 3; }
+    nsg::TraceOut outs[4];
+    stage_begin(c, kStageTrace);
+    for (int si = 0; si < nsets; si++) {
+      int s = sets[si];
+      nsg::RaySet rs = nsg::make_ray_set(s, c->gd);
+      int panel = rs.panel;
+      int64_t nr = rs.nb * rs.na;
+      CK(c->vol_ray[s].ensure(nr * sizeof(double)));
+      CK(c->ovf_rays[s].ensure(ovf_cap * sizeof(int32_t)));
+      nsg::TraceOut o{};
+      o.status = c->status.as<int32_t>();
+      o.bits = c->bits.as<uint32_t>();
+      o.vol_ray = c->vol_ray[s].as<double>();
+      o.pairs = c->pairs.as<double>();
+      o.pair_cap = c->pair_cap;
+      o.pair_cursor = cur + 0;
+      o.ray_pair_off = c->ray_pair_off.as<int64_t>();
+      o.ray_pair_cnt = c->ray_pair_cnt.as<int32_t>();
+      o.ovf_rays = c->ovf_rays[s].as<int32_t>();
+      o.ovf_cap = ovf_cap;
+      o.ovf_count = ovf_count + s;
+      o.error_flag = c->err.as<int32_t>();
+      if (keep_hits) {
+        CK(c->ray_hit_off[s].ensure(nr * sizeof(int64_t)));
+        CK(c->ray_hit_cnt[s].ensure(nr * sizeof(int32_t)));
+        CK(cudaMemsetAsync(c->ray_hit_cnt[s].p, 0, nr * sizeof(int32_t), c->stream));
+        o.hits = c->hits.as<double>();
+        o.hit_cap = c->hit_cap;
+        o.hit_cursor = cur + 1;
+        o.ray_hit_off = c->ray_hit_off[s].as<int64_t>();
+        o.ray_hit_cnt = c->ray_hit_cnt[s].as<int32_t>();
+      }
+      outs[s] = o;
+      LAUNCH(nsg::launch_trace(P, c->gd, rs, c->tile_off[panel].as<int64_t>(), c->tile_list[panel].as<int32_t>(), o,
+                           precision, c->stream));
+    }
+    stage_end(c, kStageTrace);
+    int32_t novf[4] = {0, 0, 0, 0};
+    CK(cudaMemcpyAsync(novf, ovf_count, 4 * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    int64_t tot_ovf = 0;
+    stage_begin(c, kStageOverflow);
+    for (int si = 0; si < nsets; si++) {
+      int s = sets[si];
+      int n = std::min(novf[s], ovf_cap);
+      tot_ovf += n;
+      if (n == 0) continue;
+      nsg::RaySet rs = nsg::make_ray_set(s, c->gd);
+      CK(c->ovf_scratch.ensure((size_t)n * nsg::kOverflowCap * sizeof(double)));
+      LAUNCH(nsg::launch_trace_overflow(P, c->gd, rs, c->tile_off[rs.panel].as<int64_t>(),
+                                    c->tile_list[rs.panel].as<int32_t>(), outs[s], n, c->ovf_scratch.as<double>(),
+                                    precision, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+    }
+    stage_end(c, kStageOverflow);
+    c->last_overflow_rays = tot_ovf;
+    int32_t errflag = 0;
+    unsigned long long used[2] = {0, 0};
+    CK(cudaMemcpyAsync(&errflag, c->err.p, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(used, cur, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (errflag == 0) break;
+    if (errflag == 3) { c->pair_cap = std::max<int64_t>(2 * c->pair_cap, (int64_t)used[0] + 1024); continue; }
+    if (errflag == 2) { c->hit_cap = std::max<int64_t>(2 * c->hit_cap, (int64_t)used[1] + 1024); continue; }
+    return fail(NSG_ERR_CAPACITY, errflag == 1 ? "too many overflow rays" : "ray hit capacity exceeded");
+  }
+  // volume: A * sum of interval lengths over the ray sets / number of ray sets
+  double vsum = 0;
+  int flag_sum = 0;
+  for (int s = 0; s < 4; s++) {
+    if ((s == 0 && !do_status) || (s > 0 && !do_mc)) continue;
+    nsg::RaySet rs = nsg::make_ray_set(s, c->gd);
+    double v = 0;
+    int rc = reduce_sum(c, c->vol_ray[s].as<double>(), rs.nb * rs.na, &v);
+    if (rc) return rc;
+    vsum += v;
+    flag_sum++;
+  }
+  c->volume = flag_sum ? g.A * vsum / flag_sum : 0.0;
+  if (volume) *volume = c->volume;
+  c->have_status = do_status;
+  c->have_bits = do_mc;
+  c->n_vert = c->n_tri = 0;
+  return NSG_OK;
+}
+
+int nsg_cavities(nsg_ctx* c, double cav_vol, int* ncav_out) {
+  if (!c || !c->have_status) return fail(NSG_ERR_STATE, "cavity detection needs the status map");
+  CK(cudaSetDevice(c->device));
+  const NsGrid& g = c->grid;
+  const int64_t tot = g.nx * g.ny * g.nz;
+  CK(c->labels.ensure(tot * sizeof(int32_t)));
+  CK(c->is_root.ensure(tot));
+  stage_begin(c, kStageCavity);
+  c->launches += 3;
+  CK(nsg::cc_label(c->status.as<int32_t>(), c->labels.as<int32_t>(), c->is_root.as<uint8_t>(), g.nx, g.ny, g.nz,
+                   c->stream));
+  CK(c->nroots_d.ensure(sizeof(int32_t)));
+  size_t tb = 0;
+  CK(nsg::cc_select_roots(c->is_root.as<uint8_t>(), tot, nullptr, nullptr, nullptr, &tb, c->stream));
+  CK(c->temp.ensure(tb));
+  tb = c->temp.cap;
+  // the root list is at most the number of free nodes; size it lazily from the flag count
+  CK(c->roots.ensure(tot * sizeof(int32_t)));
+  int64_t max_roots = (int64_t)(c->roots.cap / sizeof(int32_t));
+  CK(nsg::cc_select_roots(c->is_root.as<uint8_t>(), tot, c->roots.as<int32_t>(), c->nroots_d.as<int32_t>(),
+                          c->temp.p, &tb, c->stream));
+  int32_t nroots = 0;
+  CK(cudaMemcpyAsync(&nroots, c->nroots_d.p, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (nroots > max_roots) return fail(NSG_ERR_CAPACITY, "too many free regions");
+  c->cav_size.clear();
+  c->cav_filled.clear();
+  if (nroots == 0) {
+    c->ncav = 0;
+    if (ncav_out) *ncav_out = 0;
+    return NSG_OK;
+  }
+  CK(c->cc_count.ensure(nroots * sizeof(unsigned long long)));
+  CK(c->cc_desc.ensure(nroots * sizeof(unsigned int)));
+  CK(cudaMemsetAsync(c->cc_count.p, 0, nroots * sizeof(unsigned long long), c->stream));
+  CK(cudaMemsetAsync(c->cc_desc.p, 0xff, nroots * sizeof(unsigned int), c->stream));
+  LAUNCH(nsg::cc_stats(c->labels.as<int32_t>(), c->roots.as<int32_t>(), nroots, c->cc_count.as<unsigned long long>(),
+                   c->cc_desc.as<unsigned int>(), g.nx, g.ny, g.nz, c->stream));
+  std::vector<unsigned long long> cnt(nroots);
+  std::vector<unsigned int> desc(nroots);
+  CK(cudaMemcpyAsync(cnt.data(), c->cc_count.p, nroots * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(desc.data(), c->cc_desc.p, nroots * sizeof(unsigned int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  // replay the alternating seed scan: even rounds take the region whose first node in ascending
+  // order comes first (regions are already sorted by it), odd rounds the first in descending order
+  std::vector<int32_t> by_desc(nroots);
+  for (int32_t i = 0; i < nroots; i++) by_desc[i] = i;
+  std::sort(by_desc.begin(), by_desc.end(), [&](int32_t a, int32_t b) { return desc[a] < desc[b]; });
+  std::vector<int32_t> label_of(nroots, 0);
+  std::vector<uint8_t> fill_of(nroots, 0);
+  std::vector<char> taken(nroots, 0);
+  int32_t pa = 0, pd = 0, id = NS_STATUS_TEMPORARY_OUT;
+  const double cube = g.side * g.side * g.side;
+  for (int32_t t = 0; t < nroots; t++) {
+    int32_t pick;
+    if ((t & 1) == 0) {
+      while (taken[pa]) pa++;
+      pick = pa;
+    } else {
+      while (taken[by_desc[pd]]) pd++;
+      pick = by_desc[pd];
+    }
+    taken[pick] = 1;
+    id++;
+    label_of[pick] = id;
+  }
+  c->ncav = id - NS_STATUS_OUT;
+  c->cav_size.assign(c->ncav, 0.0);
+  c->cav_filled.assign(c->ncav, 0);
+  for (int32_t r = 0; r < nroots; r++) {
+    int lab = label_of[r];
+    if (lab < NS_STATUS_FIRST_CAV) continue;
+    double v = (double)cnt[r] * cube;
+    c->cav_size[lab - NS_STATUS_FIRST_CAV] = v;
+    if (v <= cav_vol) {
+      c->cav_filled[lab - NS_STATUS_FIRST_CAV] = 1;
+      fill_of[r] = 1;
+    }
+  }
+  CK(c->cc_label_of.ensure(nroots * sizeof(int32_t)));
+  CK(c->cc_fill_of.ensure(nroots));
+  CK(cudaMemcpyAsync(c->cc_label_of.p, label_of.data(), nroots * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->cc_fill_of.p, fill_of.data(), nroots, cudaMemcpyHostToDevice, c->stream));
+  LAUNCH(nsg::cc_label_fill(c->status.as<int32_t>(), c->labels.as<int32_t>(), c->cc_label_of.as<int32_t>(),
+                        c->cc_fill_of.as<uint8_t>(), c->have_bits ? c->bits.as<uint32_t>() : nullptr, nwords_of(g),
+                        g.nx, g.ny, g.nz, c->stream));
+  stage_end(c, kStageCavity);
+  CK(cudaStreamSynchronize(c->stream));
+  if (ncav_out) *ncav_out = c->ncav;
+  c->n_vert = c->n_tri = 0;
+  return NSG_OK;
+}
+
+int nsg_triangulate(nsg_ctx* c, double* area_out, int64_t* nverts, int64_t* ntris) {
+  if (!c || !c->have_bits) return fail(NSG_ERR_STATE, "triangulation needs the accurate-triangulation rays");
+  CK(cudaSetDevice(c->device));
+  const NsGrid& g = c->grid;
+  const int64_t nwords = nwords_of(g);
+  const int64_t nrays = g.nz * g.ny + g.ny * g.nx + g.nz * g.nx;
+  CK(c->surv_cnt.ensure(nrays * sizeof(int32_t)));
+  CK(c->surv_off.ensure((nrays + 1) * sizeof(int64_t)));
+  nsg::VertArgs V{};
+  V.g = c->gd;
+  V.nrays = nrays;
+  V.ray_pair_off = c->ray_pair_off.as<int64_t>();
+  V.ray_pair_cnt = c->ray_pair_cnt.as<int32_t>();
+  V.pairs = c->pairs.as<double>();
+  V.bits = c->bits.as<uint32_t>();
+  V.nwords = nwords;
+  V.surv_cnt = c->surv_cnt.as<int32_t>();
+  V.surv_off = c->surv_off.as<int64_t>();
+  stage_begin(c, kStageVertex);
+  LAUNCH(nsg::launch_vert(V, 0, c->stream));
+  int64_t n_an = 0;
+  int rc = scan_counts(c, c->surv_cnt.as<int32_t>(), nrays, c->surv_off.as<int64_t>(), &n_an);
+  if (rc) return rc;
+  // rows of cubes
+  const int64_t nrows = (g.ny - 2) * (g.nz - 2);
+  CK(c->row_act_cnt.ensure((nrows + 1) * sizeof(int64_t)));
+  CK(c->row_mid_cnt.ensure((nrows + 1) * sizeof(int64_t)));
+  CK(c->row_act_off.ensure((nrows + 1) * sizeof(int64_t)));
+  CK(c->row_mid_off.ensure((nrows + 1) * sizeof(int64_t)));
+  // vertex buffers: analytic now, midpoints appended later (reallocation keeps analytic data)
+  nsg::MCArgs M{};
+  M.g = c->gd;
+  M.bits = c->bits.as<uint32_t>();
+  M.nwords = nwords;
+  M.surv_cnt = c->surv_cnt.as<int32_t>();
+  M.surv_off = c->surv_off.as<int64_t>();
+  M.n_analytic = n_an;
+  M.nrows = nrows;
+  M.row_act_cnt = c->row_act_cnt.as<int64_t>();
+  M.row_mid_cnt = c->row_mid_cnt.as<int64_t>();
+  // analytic vertices first (the midpoint count pass needs their edge keys)
+  CK(c->vkey.ensure(std::max<int64_t>(n_an, 1) * sizeof(int4)));
+  CK(c->vpos.ensure(std::max<int64_t>(n_an, 1) * 3 * sizeof(double)));
+  V.vpos = c->vpos.as<double>();
+  V.vkey = c->vkey.as<int4>();
+  LAUNCH(nsg::launch_vert(V, 1, c->stream));
+  stage_end(c, kStageVertex);
+  stage_begin(c, kStageMC);
+  M.vpos = c->vpos.as<double>();
+  M.vkey = c->vkey.as<int4>();
+  LAUNCH(nsg::launch_mc_rows(M, 0, c->stream));
+  int64_t n_act = 0, n_mid = 0;
+  rc = scan_counts(c, c->row_act_cnt.as<int64_t>(), nrows, c->row_act_off.as<int64_t>(), &n_act);
+  if (rc) return rc;
+  rc = scan_counts(c, c->row_mid_cnt.as<int64_t>(), nrows, c->row_mid_off.as<int64_t>(), &n_mid);
+  if (rc) return rc;
+  const int64_t n_v = n_an + n_mid;
+  if ((size_t)n_v * sizeof(int4) > c->vkey.cap) {
+    DevBuf nk, np_;
+    CK(nk.ensure(n_v * sizeof(int4)));
+    CK(np_.ensure(n_v * 3 * sizeof(double)));
+    if (n_an) {
+      CK(cudaMemcpyAsync(nk.p, c->vkey.p, n_an * sizeof(int4), cudaMemcpyDeviceToDevice, c->stream));
+      CK(cudaMemcpyAsync(np_.p, c->vpos.p, n_an * 3 * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    c->vkey.release();
+    c->vpos.release();
+    c->vkey = nk;
+    c->vpos = np_;
+  }
+  if ((size_t)n_v * 3 * sizeof(double) > c->vpos.cap) {
+    DevBuf np_;
+    CK(np_.ensure(n_v * 3 * sizeof(double)));
+    if (n_an) CK(cudaMemcpyAsync(np_.p, c->vpos.p, n_an * 3 * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->vpos.release();
+    c->vpos = np_;
+  }
+  M.vpos = c->vpos.as<double>();
+  M.vkey = c->vkey.as<int4>();
+  M.row_act_off = c->row_act_off.as<int64_t>();
+  M.row_mid_off = c->row_mid_off.as<int64_t>();
+  CK(c->act_rec.ensure(std::max<int64_t>(n_act, 1) * sizeof(int4)));
+  CK(c->act_mid.ensure(std::max<int64_t>(n_act, 1) * sizeof(int32_t)));
+  M.act_rec = c->act_rec.as<int4>();
+  M.act_mid = c->act_mid.as<int32_t>();
+  LAUNCH(nsg::launch_mc_rows(M, 1, c->stream));
+  M.n_active = n_act;
+  CK(c->tri_cnt.ensure(std::max<int64_t>(n_act, 1) * sizeof(int32_t)));
+  CK(c->tri_off.ensure((n_act + 1) * sizeof(int64_t)));
+  CK(c->cube_area.ensure(std::max<int64_t>(n_act, 1) * sizeof(double)));
+  M.tri_cnt = c->tri_cnt.as<int32_t>();
+  LAUNCH(nsg::launch_mc_tris(M, 0, c->stream));
+  int64_t n_tri = 0;
+  rc = scan_counts(c, c->tri_cnt.as<int32_t>(), n_act, c->tri_off.as<int64_t>(), &n_tri);
+  if (rc) return rc;
+  CK(c->tris.ensure(std::max<int64_t>(n_tri, 1) * 3 * sizeof(int32_t)));
+  M.tri_off = c->tri_off.as<int64_t>();
+  M.tris = c->tris.as<int32_t>();
+  M.cube_area = c->cube_area.as<double>();
+  LAUNCH(nsg::launch_mc_tris(M, 1, c->stream));
+  double area = 0;
+  rc = reduce_sum(c, c->cube_area.as<double>(), n_act, &area);
+  if (rc) return rc;
+  stage_end(c, kStageMC);
+  c->n_analytic = n_an;
+  c->n_vert = n_v;
+  c->n_tri = n_tri;
+  c->n_active = n_act;
+  c->area = area;
+  if (area_out) *area_out = area;
+  if (nverts) *nverts = n_v;
+  if (ntris) *ntris = n_tri;
+  return NSG_OK;
+}
+
+int nsg_download_status(nsg_ctx* c, int32_t* dst) {
+  if (!c || !dst || !c->have_status) return NSG_ERR_STATE;
+  const NsGrid& g = c->grid;
+  CK(cudaMemcpyAsync(dst, c->status.p, g.nx * g.ny * g.nz * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return NSG_OK;
+}
+
+int nsg_download_insideness(nsg_ctx* c, uint32_t* dst) {
+  if (!c || !dst || !c->have_bits) return NSG_ERR_STATE;
+  CK(cudaMemcpyAsync(dst, c->bits.p, nwords_of(c->grid) * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return NSG_OK;
+}
+
+int nsg_download_mesh(nsg_ctx* c, double* verts, int32_t* vkeys, int32_t* tris) {
+  if (!c) return NSG_ERR_ARG;
+  if (verts && c->n_vert)
+    CK(cudaMemcpyAsync(verts, c->vpos.p, c->n_vert * 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (vkeys && c->n_vert)
+    CK(cudaMemcpyAsync(vkeys, c->vkey.p, c->n_vert * sizeof(int4), cudaMemcpyDeviceToHost, c->stream));
+  if (tris && c->n_tri)
+    CK(cudaMemcpyAsync(tris, c->tris.p, c->n_tri * 3 * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return NSG_OK;
+}
+
+int nsg_download_cavities(nsg_ctx* c, double* sizes, int32_t* filled) {
+  if (!c) return NSG_ERR_ARG;
+  if (sizes && !c->cav_size.empty()) memcpy(sizes, c->cav_size.data(), c->cav_size.size() * sizeof(double));
+  if (filled && !c->cav_filled.empty()) memcpy(filled, c->cav_filled.data(), c->cav_filled.size() * sizeof(int32_t));
+  return NSG_OK;
+}
+
+// Per-ray sorted hit parameters of one ray set (raycast with flag 16): counts are indexed by
+// n*nb + m of the set; hits are gathered in that order into dst.
+int nsg_download_hits(nsg_ctx* c, int set, int32_t* counts, double* dst, int64_t dst_cap) {
+  if (!c || set < 0 || set > 3 || !(c->flags & 16)) return NSG_ERR_STATE;
+  nsg::RaySet rs = nsg::make_ray_set(set, c->gd);
+  int64_t nr = rs.nb * rs.na;
+  std::vector<int64_t> off(nr);
+  std::vector<int32_t> cnt(nr);
+  CK(cudaMemcpyAsync(off.data(), c->ray_hit_off[set].p, nr * sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(cnt.data(), c->ray_hit_cnt[set].p, nr * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  int64_t total = 0;
+  for (int64_t r = 0; r < nr; r++) total += cnt[r];
+  if (counts) memcpy(counts, cnt.data(), nr * sizeof(int32_t));
+  if (!dst) return (int)std::min<int64_t>(total, INT32_MAX);
+  if (total > dst_cap) return NSG_ERR_CAPACITY;
+  std::vector<double> all(c->hit_cap);
+  CK(cudaMemcpyAsync(all.data(), c->hits.p, c->hit_cap * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  int64_t o = 0;
+  for (int64_t r = 0; r < nr; r++)
+    for (int32_t q = 0; q < cnt[r]; q++) dst[o++] = all[off[r] + q];
+  return NSG_OK;
+}
+
+// Records user event `slot` (0..7) on the context's stream.
+int nsg_event_record(nsg_ctx* c, int slot) {
+  if (!c || slot < 0 || slot >= 8) return NSG_ERR_ARG;
+  CK(cudaSetDevice(c->device));
+  if (!c->user_ev[slot]) CK(cudaEventCreate(&c->user_ev[slot]));
+  CK(cudaEventRecord(c->user_ev[slot], c->stream));
+  return NSG_OK;
+}
+
+// Milliseconds between two recorded user events (waits for the second one).
+int nsg_event_elapsed(nsg_ctx* c, int slot_a, int slot_b, double* ms) {
+  if (!c || !ms || slot_a < 0 || slot_a >= 8 || slot_b < 0 || slot_b >= 8) return NSG_ERR_ARG;
+  if (!c->user_ev[slot_a] || !c->user_ev[slot_b]) return NSG_ERR_STATE;
+  CK(cudaEventSynchronize(c->user_ev[slot_b]));
+  float f = 0;
+  CK(cudaEventElapsedTime(&f, c->user_ev[slot_a], c->user_ev[slot_b]));
+  *ms = f;
+  return NSG_OK;
+}
+
+// Enables (1) / disables (0) per-stage kernel timing; enabling resets the accumulated times.
+int nsg_profile(nsg_ctx* c, int enable) {
+  if (!c) return NSG_ERR_ARG;
+  c->profile = enable != 0;
+  if (c->profile)
+    for (int i = 0; i < 8; i++) { c->stage_ms[i] = 0; c->stage_calls[i] = 0; }
+  return NSG_OK;
+}
+
+// Accumulated per-stage milliseconds and call counts: bin, trace, overflow, cavity, vertex, mc.
+int nsg_stage_times(nsg_ctx* c, double* ms, int64_t* calls, int n) {
+  if (!c) return NSG_ERR_ARG;
+  for (int i = 0; i < n && i < 8; i++) {
+    if (ms) ms[i] = c->stage_ms[i];
+    if (calls) calls[i] = c->stage_calls[i];
+  }
+  return NSG_OK;
+}
+
+// Number of this library's kernels launched since the context was created.
+int64_t nsg_launch_count(nsg_ctx* c) { return c ? c->launches : -1; }
+
+void* nsg_get_stream(nsg_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int nsg_stats(nsg_ctx* c, int64_t* out, int n) {
+  if (!c || !out) return NSG_ERR_ARG;
+  int64_t v[8] = {c->np, c->n_vert, c->n_analytic, c->n_tri, c->n_active, c->ncav, c->last_overflow_rays, c->pair_cap};
+  for (int i = 0; i < n && i < 8; i++) out[i] = v[i];
+  return NSG_OK;
+}
+
+double nsg_volume(nsg_ctx* c) { return c ? c->volume : 0.0; }
+double nsg_area(nsg_ctx* c) { return c ? c->area : 0.0; }
+
+}  // extern "C"

@@ -1,0 +1,345 @@
+// Vertex assembly and marching cubes of the SES grid ray caster.
+//
+// Vertices: every vertex-producing pair of an accurate-triangulation ray yields two analytic
+// vertices on the grid edges that contain the interval ends; a vertex is dropped when the two
+// end nodes of its edge have the same final insideness, and the first vertex of an edge wins
+// (assembleVerticesList src/Surface.cpp:7415-7667).  Vertices keep the reference order: panel 0
+// rays (z-major), panel 1 rays (y-major), panel 2 rays (z-major), pairs in ray order.  Because a
+// ray's surviving vertices are sorted along the ray, the vertex of a grid edge is found by a
+// short scan of that one ray's survivors, so no dense edge-index grids are needed.
+//
+// Marching cubes: cubes (i,j,k) in [1, N-2]^3 are classified from the 8 insideness bits; active
+// cubes add an edge-midpoint vertex to their own edges 5, 6, 10 that carry no analytic vertex,
+// in (k, j, i, edge) order, appended after the analytic ones (getVertices :8002-8327); a second
+// pass emits the case-table triangles with reversed winding and sums their Heron areas
+// (triangulationKernel :9075-9318, getTriangles :14559-14780).  Triangles with an edge without a
+// vertex are skipped, as the reference does.
+#include <cub/cub.cuh>
+
+#include "../mc_cases.h"
+#include "mc.h"
+
+namespace nsg {
+
+namespace {
+
+__constant__ int8_t c_tri[256][16];  // triangle edge lists, -1 terminated
+__constant__ uint16_t c_emask[256];  // cut-edge mask per case
+
+__device__ __forceinline__ double gcoord(const GridDev& g, int d, int64_t i) { return g.mn[d] + (double)i * g.side; }
+
+__device__ __forceinline__ int rbit(const uint32_t* __restrict__ bits, int64_t nwords, int64_t f) {
+  if (f < 0 || (f >> 5) >= nwords) return 1;
+  return (bits[f >> 5] >> (f & 31)) & 1;
+}
+
+struct RayId {
+  int panel;
+  int64_t m, n;
+};
+
+__device__ __forceinline__ RayId ray_of(const GridDev& g, int64_t r) {
+  const int64_t NX = g.n[0], NY = g.n[1], NZ = g.n[2];
+  RayId id;
+  int64_t R0 = NZ * NY, R1 = NY * NX;
+  if (r < R0) { id.panel = 0; id.n = r / NY; id.m = r - id.n * NY; }
+  else if (r < R0 + R1) { int64_t q = r - R0; id.panel = 1; id.n = q / NX; id.m = q - id.n * NX; }
+  else { int64_t q = r - R0 - R1; id.panel = 2; id.n = q / NX; id.m = q - id.n * NX; }
+  return id;
+}
+
+// Edge key (ix, iy, iz, dir) of the vertex at ray position index a.
+__device__ __forceinline__ int4 edge_key(const RayId& id, int64_t a) {
+  if (id.panel == 0) return make_int4((int)a, (int)id.m, (int)id.n, NS_X_DIR);
+  if (id.panel == 1) return make_int4((int)id.m, (int)id.n, (int)a, NS_Z_DIR);
+  return make_int4((int)id.m, (int)a, (int)id.n, NS_Y_DIR);
+}
+
+__device__ __forceinline__ bool keeps(const GridDev& g, const uint32_t* bits, int64_t nwords, int4 e) {
+  const int64_t NX = g.n[0], NY = g.n[1];
+  int64_t f = ((int64_t)e.z * NY + e.y) * NX + e.x;
+  int64_t step = e.w == NS_X_DIR ? 1 : (e.w == NS_Y_DIR ? NX : NX * NY);
+  return rbit(bits, nwords, f) != rbit(bits, nwords, f + step);
+}
+
+__global__ void k_vert(VertArgs A, int emit) {
+  const GridDev& g = A.g;
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < A.nrays; r += (int64_t)gridDim.x * blockDim.x) {
+    int np = A.ray_pair_cnt[r];
+    if (!emit) {
+      int cnt = 0;
+      if (np > 0) {
+        RayId id = ray_of(g, r);
+        int vc = id.panel == 0 ? 0 : (id.panel == 1 ? 2 : 1);
+        const double* pr = A.pairs + 2 * A.ray_pair_off[r];
+        for (int q = 0; q < 2 * np; q++) {
+          int64_t a = (int64_t)floor((pr[q] - g.mn[vc]) * g.scale + 0.5);
+          if (keeps(g, A.bits, A.nwords, edge_key(id, a))) cnt++;
+        }
+      }
+      A.surv_cnt[r] = cnt;
+      continue;
+    }
+    if (np == 0 || A.surv_cnt[r] == 0) continue;
+    RayId id = ray_of(g, r);
+    int vc = id.panel == 0 ? 0 : (id.panel == 1 ? 2 : 1);
+    const double* pr = A.pairs + 2 * A.ray_pair_off[r];
+    const double delta = NS_DELTA - g.hside;
+    double base[3];
+    if (id.panel == 0) { base[1] = gcoord(g, 1, id.m) + delta; base[2] = gcoord(g, 2, id.n) + delta; }
+    else if (id.panel == 1) { base[0] = gcoord(g, 0, id.m) + delta; base[1] = gcoord(g, 1, id.n) + delta; }
+    else { base[0] = gcoord(g, 0, id.m) + delta; base[2] = gcoord(g, 2, id.n) + delta; }
+    int64_t o = A.surv_off[r];
+    for (int q = 0; q < 2 * np; q++) {
+      int64_t a = (int64_t)floor((pr[q] - g.mn[vc]) * g.scale + 0.5);
+      int4 e = edge_key(id, a);
+      if (!keeps(g, A.bits, A.nwords, e)) continue;
+      double p[3] = {base[0], base[1], base[2]};
+      p[vc] = pr[q];
+      A.vpos[3 * o + 0] = p[0];
+      A.vpos[3 * o + 1] = p[1];
+      A.vpos[3 * o + 2] = p[2];
+      A.vkey[o] = e;
+      o++;
+    }
+  }
+}
+
+// Index of the analytic vertex on edge (dir, i, j, k), -1 if none.
+__device__ __forceinline__ int64_t analytic_vertex(const MCArgs& A, int dir, int64_t i, int64_t j, int64_t k) {
+  const GridDev& g = A.g;
+  const int64_t NX = g.n[0], NY = g.n[1], NZ = g.n[2];
+  int64_t r, e;
+  if (dir == NS_X_DIR) { r = k * NY + j; e = i; }
+  else if (dir == NS_Z_DIR) { r = NZ * NY + j * NX + i; e = k; }
+  else { r = NZ * NY + NY * NX + k * NX + i; e = j; }
+  int cnt = A.surv_cnt[r];
+  if (cnt == 0) return -1;
+  int64_t off = A.surv_off[r];
+  for (int s = 0; s < cnt; s++) {
+    int4 key = A.vkey[off + s];
+    int along = dir == NS_X_DIR ? key.x : (dir == NS_Y_DIR ? key.y : key.z);
+    if (along == e) return off + s;
+    if (along > e) break;
+  }
+  return -1;
+}
+
+__device__ __forceinline__ int cube_case(const MCArgs& A, int64_t i, int64_t j, int64_t k) {
+  const int64_t NX = A.g.n[0], NY = A.g.n[1];
+  int64_t f = (k * NY + j) * NX + i;
+  int64_t sy = NX, sz = NX * NY;
+  int c = 0;
+  if (!rbit(A.bits, A.nwords, f)) c |= 1;
+  if (!rbit(A.bits, A.nwords, f + 1)) c |= 2;
+  if (!rbit(A.bits, A.nwords, f + 1 + sy)) c |= 4;
+  if (!rbit(A.bits, A.nwords, f + sy)) c |= 8;
+  if (!rbit(A.bits, A.nwords, f + sz)) c |= 16;
+  if (!rbit(A.bits, A.nwords, f + 1 + sz)) c |= 32;
+  if (!rbit(A.bits, A.nwords, f + 1 + sy + sz)) c |= 64;
+  if (!rbit(A.bits, A.nwords, f + sy + sz)) c |= 128;
+  return c;
+}
+
+// Midpoint vertices a cube creates on its own edges 5 (y), 6 (x), 10 (z): bit 0, 1, 2.
+__device__ __forceinline__ int own_midpoints(const MCArgs& A, int64_t i, int64_t j, int64_t k, int em) {
+  int mm = 0;
+  if ((em & 32) && analytic_vertex(A, NS_Y_DIR, i + 1, j, k + 1) < 0) mm |= 1;
+  if ((em & 64) && analytic_vertex(A, NS_X_DIR, i, j + 1, k + 1) < 0) mm |= 2;
+  if ((em & 1024) && analytic_vertex(A, NS_Z_DIR, i + 1, j + 1, k) < 0) mm |= 4;
+  return mm;
+}
+
+// One warp per cube row (j, k); pass 0 counts, pass 1 emits active cubes and midpoint vertices.
+__global__ void k_mc_rows(MCArgs A, int emit) {
+  const GridDev& g = A.g;
+  const int64_t NX = g.n[0], NY = g.n[1];
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t row = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); row < A.nrows; row += warps) {
+    int64_t j = 1 + row % (NY - 2);
+    int64_t k = 1 + row / (NY - 2);
+    int64_t act_run = 0, mid_run = 0;
+    int64_t act_base = emit ? A.row_act_off[row] : 0;
+    int64_t mid_base = emit ? A.row_mid_off[row] : 0;
+    for (int64_t i0 = 1; i0 < NX - 1; i0 += 32) {
+      int64_t i = i0 + lane;
+      int act = 0, mm = 0, c = 0;
+      if (i < NX - 1) {
+        c = cube_case(A, i, j, k);
+        int em = c_emask[c];
+        if (em) {
+          act = 1;
+          mm = own_midpoints(A, i, j, k, em);
+        }
+      }
+      int nm = __popc(mm);
+      int ia = act, im = nm;
+      for (int o = 1; o < 32; o <<= 1) {
+        int va = __shfl_up_sync(0xffffffffu, ia, o);
+        int vm = __shfl_up_sync(0xffffffffu, im, o);
+        if (lane >= o) { ia += va; im += vm; }
+      }
+      int ta = __shfl_sync(0xffffffffu, ia, 31), tm = __shfl_sync(0xffffffffu, im, 31);
+      if (emit && act) {
+        int64_t slot = act_base + act_run + ia - act;
+        int64_t mbase = mid_base + mid_run + im - nm;
+        A.act_rec[slot] = make_int4((int)i, (int)j, (int)k, c | (mm << 8));
+        A.act_mid[slot] = (int32_t)(A.n_analytic + mbase);
+        int64_t v = A.n_analytic + mbase;
+        if (mm & 1) {
+          A.vpos[3 * v] = gcoord(g, 0, i + 1) - g.hside; A.vpos[3 * v + 1] = gcoord(g, 1, j);
+          A.vpos[3 * v + 2] = gcoord(g, 2, k + 1) - g.hside;
+          A.vkey[v] = make_int4((int)(i + 1), (int)j, (int)(k + 1), NS_Y_DIR);
+          v++;
+        }
+        if (mm & 2) {
+          A.vpos[3 * v] = gcoord(g, 0, i); A.vpos[3 * v + 1] = gcoord(g, 1, j + 1) - g.hside;
+          A.vpos[3 * v + 2] = gcoord(g, 2, k + 1) - g.hside;
+          A.vkey[v] = make_int4((int)i, (int)(j + 1), (int)(k + 1), NS_X_DIR);
+          v++;
+        }
+        if (mm & 4) {
+          A.vpos[3 * v] = gcoord(g, 0, i + 1) - g.hside; A.vpos[3 * v + 1] = gcoord(g, 1, j + 1) - g.hside;
+          A.vpos[3 * v + 2] = gcoord(g, 2, k);
+          A.vkey[v] = make_int4((int)(i + 1), (int)(j + 1), (int)k, NS_Z_DIR);
+        }
+      }
+      act_run += ta;
+      mid_run += tm;
+    }
+    if (!emit && lane == 0) {
+      A.row_act_cnt[row] = act_run;
+      A.row_mid_cnt[row] = mid_run;
+    }
+  }
+}
+
+// Midpoint vertex created by the cube that owns edge (dir, ex, ey, ez), -1 if none.
+__device__ __forceinline__ int64_t midpoint_vertex(const MCArgs& A, int dir, int64_t ex, int64_t ey, int64_t ez) {
+  const int64_t NX = A.g.n[0], NY = A.g.n[1], NZ = A.g.n[2];
+  int64_t oi = ex, oj = ey, ok = ez;
+  int bit;
+  if (dir == NS_Y_DIR) { oi = ex - 1; ok = ez - 1; bit = 0; }
+  else if (dir == NS_X_DIR) { oj = ey - 1; ok = ez - 1; bit = 1; }
+  else { oi = ex - 1; oj = ey - 1; bit = 2; }
+  if (oi < 1 || oj < 1 || ok < 1 || oi > NX - 2 || oj > NY - 2 || ok > NZ - 2) return -1;
+  int64_t row = (ok - 1) * (NY - 2) + (oj - 1);
+  int64_t lo = A.row_act_off[row], hi = A.row_act_off[row + 1];
+  while (lo < hi) {
+    int64_t mid = (lo + hi) >> 1;
+    if (A.act_rec[mid].x < oi) lo = mid + 1;
+    else hi = mid;
+  }
+  if (lo >= A.row_act_off[row + 1] || A.act_rec[lo].x != oi) return -1;
+  int mm = (A.act_rec[lo].w >> 8) & 7;
+  if (!(mm & (1 << bit))) return -1;
+  return A.act_mid[lo] + __popc(mm & ((1 << bit) - 1));
+}
+
+__device__ __forceinline__ int64_t edge_vertex(const MCArgs& A, int e, int64_t i, int64_t j, int64_t k) {
+  // cube edge -> grid edge (dir, ex, ey, ez)
+  int dir;
+  int64_t x = i, y = j, z = k;
+  switch (e) {
+    case 0: dir = NS_X_DIR; break;
+    case 1: dir = NS_Y_DIR; x = i + 1; break;
+    case 2: dir = NS_X_DIR; y = j + 1; break;
+    case 3: dir = NS_Y_DIR; break;
+    case 4: dir = NS_X_DIR; z = k + 1; break;
+    case 5: dir = NS_Y_DIR; x = i + 1; z = k + 1; break;
+    case 6: dir = NS_X_DIR; y = j + 1; z = k + 1; break;
+    case 7: dir = NS_Y_DIR; z = k + 1; break;
+    case 8: dir = NS_Z_DIR; break;
+    case 9: dir = NS_Z_DIR; x = i + 1; break;
+    case 10: dir = NS_Z_DIR; x = i + 1; y = j + 1; break;
+    default: dir = NS_Z_DIR; y = j + 1; break;
+  }
+  int64_t v = analytic_vertex(A, dir, x, y, z);
+  if (v >= 0) return v;
+  return midpoint_vertex(A, dir, x, y, z);
+}
+
+__device__ __forceinline__ double vdist(const double* a, const double* b) {
+  return sqrt((a[0] - b[0]) * (a[0] - b[0]) + (a[1] - b[1]) * (a[1] - b[1]) + (a[2] - b[2]) * (a[2] - b[2]));
+}
+
+// One thread per active cube; pass 0 counts triangles, pass 1 writes them and their areas.
+__global__ void k_mc_tris(MCArgs A, int emit) {
+  for (int64_t a = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; a < A.n_active; a += (int64_t)gridDim.x * blockDim.x) {
+    int4 rec = A.act_rec[a];
+    int c = rec.w & 255;
+    int64_t i = rec.x, j = rec.y, k = rec.z;
+    int64_t vl[12];
+    int em = c_emask[c];
+    for (int e = 0; e < 12; e++) vl[e] = (em >> e) & 1 ? edge_vertex(A, e, i, j, k) : -1;
+    int cnt = 0;
+    int64_t o = emit ? A.tri_off[a] : 0;
+    double area = 0.0;
+    for (int q = 0; q < 16 && c_tri[c][q] >= 0; q += 3) {
+      int64_t v0 = vl[c_tri[c][q]], v1 = vl[c_tri[c][q + 1]], v2 = vl[c_tri[c][q + 2]];
+      if (v0 < 0 || v1 < 0 || v2 < 0) continue;
+      if (emit) {
+        const double* P0 = A.vpos + 3 * v0;
+        const double* P1 = A.vpos + 3 * v1;
+        const double* P2 = A.vpos + 3 * v2;
+        double da = vdist(P0, P1), db = vdist(P0, P2), dc = vdist(P1, P2);
+        double ttt = (da + db + dc) * (db + dc - da) * (dc + da - db) * (da + db - dc);
+        if (ttt > 0) area += 0.25 * sqrt(ttt);
+        A.tris[3 * (o + cnt) + 0] = (int32_t)v2;
+        A.tris[3 * (o + cnt) + 1] = (int32_t)v1;
+        A.tris[3 * (o + cnt) + 2] = (int32_t)v0;
+      }
+      cnt++;
+    }
+    if (!emit) A.tri_cnt[a] = cnt;
+    else A.cube_area[a] = area;
+  }
+}
+
+int grid_for(int64_t n, int threads) {
+  int64_t b = (n + threads - 1) / threads;
+  return (int)(b < 148 * 32 ? (b < 1 ? 1 : b) : 148 * 32);
+}
+
+}  // namespace
+
+cudaError_t mc_init_tables() {
+  int8_t tri[256][16];
+  uint16_t em[256];
+  static const int ec[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6}, {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
+  for (int c = 0; c < 256; c++) {
+    int m = 0;
+    for (int e = 0; e < 12; e++)
+      if (((c >> ec[e][0]) & 1) != ((c >> ec[e][1]) & 1)) m |= 1 << e;
+    em[c] = (uint16_t)m;
+    const char* s = kNsMcCases[c];
+    int q = 0;
+    for (; s[q] && q < 16; q++) tri[c][q] = (int8_t)(s[q] <= '9' ? s[q] - '0' : s[q] - 'a' + 10);
+    for (; q < 16; q++) tri[c][q] = -1;
+  }
+  cudaError_t err = cudaMemcpyToSymbol(c_tri, tri, sizeof tri);
+  if (err != cudaSuccess) return err;
+  return cudaMemcpyToSymbol(c_emask, em, sizeof em);
+}
+
+cudaError_t launch_vert(const VertArgs& A, int emit, cudaStream_t s) {
+  if (A.nrays == 0) return cudaSuccess;
+  k_vert<<<grid_for(A.nrays, 256), 256, 0, s>>>(A, emit);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mc_rows(const MCArgs& A, int emit, cudaStream_t s) {
+  if (A.nrows <= 0) return cudaSuccess;
+  int64_t warps = A.nrows;
+  k_mc_rows<<<grid_for(warps * 32, 256), 256, 0, s>>>(A, emit);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mc_tris(const MCArgs& A, int emit, cudaStream_t s) {
+  if (A.n_active <= 0) return cudaSuccess;
+  k_mc_tris<<<grid_for(A.n_active, 128), 128, 0, s>>>(A, emit);
+  return cudaGetLastError();
+}
+
+}  // namespace nsg

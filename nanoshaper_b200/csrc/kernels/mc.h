@@ -1,0 +1,52 @@
+// Vertex assembly and marching-cubes kernels (mc.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "pipeline.h"
+
+namespace nsg {
+
+struct VertArgs {
+  GridDev g;
+  int64_t nrays;                 // accurate-triangulation rays of the three panels
+  const int64_t* ray_pair_off;
+  const int32_t* ray_pair_cnt;
+  const double* pairs;
+  const uint32_t* bits;
+  int64_t nwords;
+  int32_t* surv_cnt;             // surviving vertices per ray
+  const int64_t* surv_off;       // exclusive scan of surv_cnt
+  double* vpos;                  // 3 per vertex
+  int4* vkey;                    // ix, iy, iz, dir per vertex
+};
+
+struct MCArgs {
+  GridDev g;
+  const uint32_t* bits;
+  int64_t nwords;
+  const int32_t* surv_cnt;
+  const int64_t* surv_off;
+  int64_t n_analytic;
+  double* vpos;
+  int4* vkey;
+  int64_t nrows;                 // (NY-2)*(NZ-2) cube rows
+  int64_t* row_act_cnt;
+  int64_t* row_mid_cnt;
+  const int64_t* row_act_off;    // nrows+1 entries
+  const int64_t* row_mid_off;
+  int4* act_rec;                 // i, j, k, case | midpoint mask << 8
+  int32_t* act_mid;              // index of the first midpoint vertex of the cube
+  int64_t n_active;
+  int32_t* tri_cnt;
+  const int64_t* tri_off;
+  int32_t* tris;
+  double* cube_area;
+};
+
+cudaError_t mc_init_tables();
+cudaError_t launch_vert(const VertArgs& A, int emit, cudaStream_t s);
+cudaError_t launch_mc_rows(const MCArgs& A, int emit, cudaStream_t s);
+cudaError_t launch_mc_tris(const MCArgs& A, int emit, cudaStream_t s);
+
+}  // namespace nsg

@@ -1,0 +1,106 @@
+// Device-side pipeline of the SES grid ray caster: shared parameter blocks and kernel launchers.
+// Kernels live in trace.cu (patch windows, tile binning, ray tracing + interval fill),
+// cavity.cu (connected components of the status map, cavity filling) and mc.cu (vertex
+// assembly and marching cubes); capi.cu drives them.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../ns_types.h"
+
+namespace nsg {
+
+// Ray tile handled by one CTA: 32 consecutive pixels along the first panel axis (one per lane)
+// times 4 rows along the second axis (one per warp).
+constexpr int kTileM = 32;
+constexpr int kTileN = 4;
+constexpr int kTraceThreads = kTileM * kTileN;
+// Hits kept on chip per ray; rays with more hits are re-traced by the overflow path.
+constexpr int kHitCap = 32;
+// Hits per ray on the overflow path.
+constexpr int kOverflowCap = 2048;
+
+// Ray sets: 0 = status rays along x (panel 0, through grid nodes); 1..3 = accurate
+// triangulation rays of panels 0 (x), 1 (z), 2 (y), shifted by DELTA - hside.
+struct RaySet {
+  int set;      // 0..3
+  int panel;    // 0..2
+  int fd, ld, vc;  // first pixel axis (m), second pixel axis (n), ray axis
+  int64_t nb, na;  // pixel counts along m and n
+  double delta;
+  int64_t ordinal_base;  // first ray ordinal of this set in the accurate-triangulation order
+};
+
+struct GridDev {
+  int64_t n[3];
+  double mn[3];
+  double mx[3];
+  double scale, side, hside;
+};
+
+__host__ __device__ inline RaySet make_ray_set(int set, const GridDev& g) {
+  RaySet r;
+  r.set = set;
+  r.panel = set == 0 ? 0 : set - 1;
+  if (r.panel == 0) { r.fd = 1; r.ld = 2; r.vc = 0; }
+  else if (r.panel == 1) { r.fd = 0; r.ld = 1; r.vc = 2; }
+  else { r.fd = 0; r.ld = 2; r.vc = 1; }
+  r.nb = g.n[r.fd];
+  r.na = g.n[r.ld];
+  r.delta = set == 0 ? 0.0 : NS_DELTA - g.hside;
+  // accurate triangulation ray order: panel 0 rays (n over z, m over y), panel 1 (n over y,
+  // m over x), panel 2 (n over z, m over x)
+  int64_t b = 0;
+  if (r.panel >= 1) b += g.n[2] * g.n[1];
+  if (r.panel >= 2) b += g.n[1] * g.n[0];
+  r.ordinal_base = set == 0 ? 0 : b;
+  return r;
+}
+
+// Outputs of one trace launch.
+struct TraceOut {
+  int32_t* status;         // set 0: full status map rows
+  uint32_t* bits;          // sets 1..3: insideness bits (1 = outside), cleared with atomicAnd
+  double* vol_ray;         // per ray interval length sum, indexed by n*nb+m
+  // pair store (sets 1..3): lim1/lim2 of vertex-producing pairs
+  double* pairs;           // 2 doubles per pair
+  int64_t pair_cap;
+  unsigned long long* pair_cursor;
+  int64_t* ray_pair_off;   // per ray ordinal
+  int32_t* ray_pair_cnt;   // per ray ordinal
+  // overflow rays
+  int32_t* ovf_rays;       // n*nb+m of rays whose hits exceeded kHitCap
+  int32_t ovf_cap;
+  int32_t* ovf_count;
+  // optional per-ray hit dump (tests)
+  double* hits;
+  int64_t hit_cap;
+  unsigned long long* hit_cursor;
+  int64_t* ray_hit_off;    // indexed by n*nb+m
+  int32_t* ray_hit_cnt;
+  int32_t* error_flag;     // set when a device-side capacity is exceeded
+};
+
+struct PatchDev {
+  int64_t n;
+  const double* f64;
+  const int32_t* i32;
+  const double4* pool;
+  const int8_t* flag;
+  double probe;
+  const int32_t* win;  // 6 per patch: start x,y,z, end x,y,z; start = -1 when culled
+};
+
+// trace.cu
+cudaError_t launch_windows(const PatchDev& P, int32_t* win, const GridDev& g, cudaStream_t s);
+cudaError_t launch_bin_count(const PatchDev& P, const GridDev& g, const RaySet& rs, int32_t* tile_cnt,
+                             cudaStream_t s);
+cudaError_t launch_bin_fill(const PatchDev& P, const GridDev& g, const RaySet& rs, const int64_t* tile_off,
+                            int32_t* tile_cursor, int32_t* tile_list, cudaStream_t s);
+cudaError_t launch_trace(const PatchDev& P, const GridDev& g, const RaySet& rs, const int64_t* tile_off,
+                         const int32_t* tile_list, const TraceOut& out, int precision, cudaStream_t s);
+cudaError_t launch_trace_overflow(const PatchDev& P, const GridDev& g, const RaySet& rs, const int64_t* tile_off,
+                                  const int32_t* tile_list, const TraceOut& out, int n_ovf, double* scratch,
+                                  int precision, cudaStream_t s);
+
+}  // namespace nsg

@@ -1,0 +1,459 @@
+"""Host-side mirror of the reference's surface plugin interface, backed by libnsgpu.
+
+Mirrors, with the same names and argument meanings:
+  * ``ConfigFile``      -- the .prm ``key = value`` reader (src/ConfigFile/ConfigFile.{h,cpp})
+  * ``DelPhiShared``    -- the grid environment: atoms, grid construction, maps
+                           (src/DelphiShared.cpp:309-704, 1038-1201)
+  * ``Surface``         -- ``build()``, ``getSurf()``, ``triangulateSurface()`` (src/Surface.h:835-990)
+  * ``ConnollySurface`` -- the "ses" surface (src/ConnollySurface.h)
+  * ``SurfaceFactory``  -- name -> surface registry keyed by the .prm ``Surface`` key
+                           (src/SurfaceFactory.h:15-65)
+  * ``NanoShaper``      -- the library facade (src/nanoshaper.h:294-423)
+
+The ray casting, cavity detection and marching cubes run on the GPU through the C-ABI; the
+patch construction runs in host C++ inside the same library.  Errors raise instead of calling
+``exit``.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+from typing import Callable
+
+import numpy as np
+
+from . import _native as N
+
+DEFAULT_PERFIL = 80.0
+DEFAULT_SCALE = 2.0
+DEFAULT_PROBE = 1.4
+RAND_DISPLACEMENT = 1e-4
+SEED = 1234
+
+STATUS_POINT_INSIDE = -1
+STATUS_POINT_TEMPORARY_OUT = 2
+STATUS_POINT_OUT = 3
+STATUS_FIRST_CAV = 4
+
+PRECISIONS = {"fp64": 0, "mixed": 1}
+
+# Process-wide generator state of the atom jitter, like the reference's static SEED.
+_seed = ctypes.c_int64(SEED)
+
+
+def reset_seed(value: int = SEED) -> None:
+    _seed.value = value
+
+
+# --------------------------------------------------------------------------------------------
+class ConfigFile:
+    """``key = value`` configuration with ``#`` comments and an optional ``EndConfigFile`` sentry.
+
+    A value continues on the following lines until a blank line or a line holding a delimiter.
+    Unknown keys are kept and ignored by the surfaces, as in the reference.
+    """
+
+    def __init__(self, path: str | Path | None = None, text: str | None = None):
+        self.contents: dict[str, str] = {}
+        self.path = Path(path) if path is not None else None
+        if path is not None:
+            text = Path(path).read_text()
+        if text:
+            self._parse(text)
+
+    def _parse(self, text: str) -> None:
+        lines = text.splitlines()
+        i = 0
+        while i < len(lines):
+            line = lines[i].split("#", 1)[0]
+            i += 1
+            if "EndConfigFile" in line:
+                return
+            if "=" not in line:
+                continue
+            key, value = line.split("=", 1)
+            key = key.strip()
+            while i < len(lines):
+                nxt = lines[i].split("#", 1)[0]
+                if "EndConfigFile" in nxt or "=" in nxt or not nxt.strip():
+                    break
+                value += "\n" + nxt
+                i += 1
+            self.contents[key] = value.strip()
+
+    def keyExists(self, key: str) -> bool:
+        return key in self.contents
+
+    def add(self, key: str, value) -> None:
+        self.contents[key] = str(value).lower() if isinstance(value, bool) else str(value)
+
+    def read(self, key: str, default=None, type_: type | None = None):
+        if key not in self.contents:
+            if default is None:
+                raise KeyError(key)
+            return default
+        raw = self.contents[key]
+        t = type_ or (type(default) if default is not None else str)
+        if t is bool:
+            return raw.strip().upper() not in ("FALSE", "F", "NO", "N", "0", "NONE")
+        if t is int:
+            return int(float(raw.split()[0]))
+        if t is float:
+            return float(raw.split()[0])
+        return raw
+
+
+# --------------------------------------------------------------------------------------------
+def read_xyzr(path: str | Path) -> np.ndarray:
+    """Atoms of an xyzr file as an (N, 4) float64 array (x, y, z, radius)."""
+    L = N.lib()
+    n = L.nsg_read_xyzr(str(path).encode(), None, 0)
+    if n < 0:
+        raise N.NativeError(f"cannot read {path}: {N.ERRORS.get(n, n)}")
+    out = np.zeros((n, 4), np.float64)
+    n2 = L.nsg_read_xyzr(str(path).encode(), N.ptr(out), n)
+    if n2 != n:
+        raise N.NativeError(f"cannot read {path}")
+    return out
+
+
+class DelPhiShared:
+    """Grid environment: the atoms, the cubic grid and the maps produced on it."""
+
+    def __init__(self, atoms: np.ndarray, scale: float = DEFAULT_SCALE, perfil: float = DEFAULT_PERFIL,
+                 build_status: bool = True, build_eps_map: bool = False):
+        self.atoms = np.ascontiguousarray(np.asarray(atoms, np.float64).reshape(-1, 4)).copy()
+        if len(self.atoms) == 0:
+            raise ValueError("Cannot build grid with no atoms!")
+        self.buildStatus = build_status
+        self.buildEpsMap = build_eps_map
+        if build_eps_map:
+            raise NotImplementedError("epsilon maps are not built by this implementation")
+        self.grid = N.NsGrid()
+        self.buildGrid(scale, perfil)
+        self.status: np.ndarray | None = None
+        self.cavitiesSize: list[float] = []
+        self.cavitiesFlag: list[bool] = []
+
+    def buildGrid(self, scale: float, perfil: float) -> bool:
+        N.check(N.lib().nsg_grid_build(N.ptr(self.atoms), len(self.atoms), scale, perfil, ctypes.byref(self.grid)),
+                "buildGrid")
+        g = self.grid
+        self.nx, self.ny, self.nz = g.nx, g.ny, g.nz
+        self.scale, self.side, self.hside, self.A = g.scale, g.side, g.hside, g.A
+        self.xmin, self.ymin, self.zmin = g.xmin, g.ymin, g.zmin
+        self.xmax, self.ymax, self.zmax = g.xmax, g.ymax, g.zmax
+        self.rmaxdim = g.rmaxdim
+        self.x = g.xmin + np.arange(g.nx) * g.side
+        self.y = g.ymin + np.arange(g.ny) * g.side
+        self.z = g.zmin + np.arange(g.nz) * g.side
+        return True
+
+
+class PatchSet:
+    """Host copy of a patch set in the C-ABI layout (see include/nsgpu.h)."""
+
+    KINDS = ("point", "regular_edge", "singular_edge", "regular_facet", "singular_facet")
+
+    def __init__(self, f64: np.ndarray, i32: np.ndarray, pool: np.ndarray, pool_flag: np.ndarray, probe: float,
+                 counts: tuple[int, ...] = ()):
+        self.f64 = np.ascontiguousarray(f64, np.float64).reshape(-1, 20)
+        self.i32 = np.ascontiguousarray(i32, np.int32).reshape(-1, 4)
+        self.pool = np.ascontiguousarray(pool, np.float64).reshape(-1, 4)
+        self.pool_flag = np.ascontiguousarray(pool_flag, np.int8).reshape(-1)
+        self.probe = float(probe)
+        self.counts = tuple(counts) or tuple(int((self.i32[:, 0] == k).sum()) for k in range(5))
+
+    @property
+    def n(self) -> int:
+        return len(self.i32)
+
+    @classmethod
+    def from_native(cls, handle: ctypes.c_void_p, probe: float) -> "PatchSet":
+        L = N.lib()
+        n = ctypes.c_int64()
+        npool = ctypes.c_int64()
+        counts = (ctypes.c_int64 * 5)()
+        N.check(L.nsg_patchset_info(handle, ctypes.byref(n), ctypes.byref(npool), counts), "patchset_info")
+        f64 = np.zeros((n.value, 20))
+        i32 = np.zeros((n.value, 4), np.int32)
+        pool = np.zeros((npool.value, 4))
+        flag = np.zeros(npool.value, np.int8)
+        N.check(L.nsg_patchset_export(handle, N.ptr(f64), N.ptr(i32), N.ptr(pool), N.ptr(flag)), "patchset_export")
+        return cls(f64, i32, pool, flag, probe, tuple(counts))
+
+
+def build_ses_patches(atoms: np.ndarray, probe: float, threads: int = 0) -> PatchSet:
+    """SES patch set (points, tori, probe patches) of jittered atoms, built on the host."""
+    atoms = np.ascontiguousarray(atoms, np.float64)
+    h = ctypes.c_void_p()
+    rc = N.lib().nsg_ses_build(N.ptr(atoms), len(atoms), probe, threads, ctypes.byref(h))
+    if rc not in (N.NSG_OK, -8):
+        N.check(rc, "SES patch construction")
+    try:
+        ps = PatchSet.from_native(h, probe)
+        ps.degenerate = rc == -8
+        return ps
+    finally:
+        N.lib().nsg_patchset_free(h)
+
+
+# --------------------------------------------------------------------------------------------
+class Context:
+    """A libnsgpu context: a CUDA stream plus device-resident buffers on one GPU."""
+
+    def __init__(self, device: int = 0):
+        self.handle = ctypes.c_void_p()
+        N.check(N.lib().nsg_ctx_create(device, ctypes.byref(self.handle)), "context creation")
+
+    def close(self) -> None:
+        if self.handle:
+            N.lib().nsg_ctx_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Surface:
+    """Base of the GPU-backed surfaces (the reference's ``Surface`` plugin interface)."""
+
+    name = "surface"
+
+    def __init__(self, cf: ConfigFile | None = None, delphi: DelPhiShared | None = None, device: int = 0):
+        self.delphi = delphi
+        cf = cf or ConfigFile()
+        self.accurateTriangulation = cf.read("Accurate_Triangulation", False, bool)
+        self.triangulation = cf.read("Triangulation", False, bool)
+        self.probe_radius = cf.read("Probe_Radius", DEFAULT_PROBE, float)
+        self.patchBasedAlgorithm = cf.read("Patch_Based_Algorithm", True, bool)
+        self.analyticalTorus = cf.read("Analytical_Ray_Vs_Torus_Intersection", True, bool)
+        self.computeNormals = cf.read("Compute_Vertex_Normals", False, bool)
+        self.forceSerialBuild = cf.read("Force_Serial_Build", False, bool)
+        self.numThreads = cf.read("Number_thread", 0, int)
+        self.precision = cf.read("Gpu_Precision", "fp64", str).strip().lower()
+        self.randDisplacement = RAND_DISPLACEMENT
+        self.device = device
+        self.ctx: Context | None = None
+        self.patches: PatchSet | None = None
+        self.volume = None
+        self.area = None
+        self.insideness: np.ndarray | None = None
+        self.vertices: np.ndarray | None = None
+        self.vertex_edges: np.ndarray | None = None
+        self.triangles: np.ndarray | None = None
+        self.ncav = 0
+
+    # -- reference interface ---------------------------------------------------------------
+    def build(self) -> bool:
+        raise NotImplementedError
+
+    def getNumPatches(self) -> int:
+        return 0 if self.patches is None else self.patches.n
+
+    def isPatchBasedRayTracingSupported(self) -> bool:
+        return True
+
+    def _context(self) -> Context:
+        if self.ctx is None:
+            self.ctx = Context(self.device)
+        return self.ctx
+
+    def upload(self) -> None:
+        if self.patches is None or self.delphi is None:
+            raise RuntimeError("Cannot get surface without DelPhi environment and patches")
+        c = self._context().handle
+        p = self.patches
+        N.check(N.lib().nsg_set_grid(c, ctypes.byref(self.delphi.grid)), "set_grid")
+        N.check(N.lib().nsg_upload_patches(c, p.n, N.ptr(p.f64), N.ptr(p.i32), len(p.pool), N.ptr(p.pool),
+                                           N.ptr(p.pool_flag), p.probe), "upload_patches")
+
+    def getSurf(self, optimize_grids: bool = True, fill: bool = False, cav_vol: float = 0.0,
+                keep_hits: bool = False, download: bool = True) -> float:
+        """Ray casts the grid: status map, insideness bits, volume; optional cavity filling."""
+        if self.delphi is None:
+            raise RuntimeError("Cannot get surface without DelPhi environment!")
+        self.upload()
+        c = self._context().handle
+        flags = 0
+        if self.delphi.buildStatus:
+            flags |= N.STATUS
+        if self.accurateTriangulation:
+            flags |= N.ACCURATE_TRIANGULATION
+        if keep_hits:
+            flags |= N.KEEP_HITS
+        prec = PRECISIONS.get(self.precision)
+        if prec is None:
+            raise ValueError(f"unknown Gpu_Precision {self.precision}")
+        vol = ctypes.c_double()
+        N.check(N.lib().nsg_raycast(c, flags, prec, ctypes.byref(vol)), "ray casting")
+        self.volume = vol.value
+        if fill:
+            if not self.delphi.buildStatus:
+                raise RuntimeError("Cannot do cavity detection without a status map (Build_status_map = true)")
+            ncav = ctypes.c_int()
+            N.check(N.lib().nsg_cavities(c, float(cav_vol), ctypes.byref(ncav)), "cavity detection")
+            self.ncav = ncav.value
+            sizes = np.zeros(max(self.ncav, 0))
+            flagv = np.zeros(max(self.ncav, 0), np.int32)
+            if self.ncav > 0:
+                N.check(N.lib().nsg_download_cavities(c, N.ptr(sizes), N.ptr(flagv)), "download cavities")
+            self.delphi.cavitiesSize = sizes.tolist()
+            self.delphi.cavitiesFlag = [bool(f) for f in flagv]
+        if download:
+            g = self.delphi.grid
+            if self.delphi.buildStatus:
+                st = np.empty(g.nx * g.ny * g.nz, np.int32)
+                N.check(N.lib().nsg_download_status(c, N.ptr(st)), "download status")
+                self.delphi.status = st.reshape(g.nz, g.ny, g.nx)
+            if self.accurateTriangulation:
+                words = ((g.nx + 31) >> 5) * g.ny * g.nz
+                bits = np.empty(words, np.uint32)
+                N.check(N.lib().nsg_download_insideness(c, N.ptr(bits)), "download insideness")
+                self.insideness = bits
+        return self.volume
+
+    def triangulateSurface(self, outputMesh: bool = False, fileName: str = "triangulatedSurf",
+                           download: bool = True) -> float:
+        """Analytical marching cubes on the insideness grid; returns the mesh area."""
+        c = self._context().handle
+        area = ctypes.c_double()
+        nv = ctypes.c_int64()
+        nt = ctypes.c_int64()
+        N.check(N.lib().nsg_triangulate(c, ctypes.byref(area), ctypes.byref(nv), ctypes.byref(nt)), "triangulation")
+        self.area = area.value
+        if download:
+            self.vertices = np.empty((nv.value, 3))
+            self.vertex_edges = np.empty((nv.value, 4), np.int32)
+            self.triangles = np.empty((nt.value, 3), np.int32)
+            N.check(N.lib().nsg_download_mesh(c, N.ptr(self.vertices), N.ptr(self.vertex_edges),
+                                              N.ptr(self.triangles)), "download mesh")
+        if outputMesh:
+            self.saveMesh(fileName + ".off")
+        return self.area
+
+    def saveMesh(self, path: str | Path) -> None:
+        """OFF mesh file (vertices then triangles), as the reference's default output."""
+        v, t = self.vertices, self.triangles
+        with open(path, "w") as f:
+            f.write("OFF\n")
+            f.write(f"{len(v)} {len(t)} 0\n")
+            for p in v:
+                f.write(f"{p[0]:.6f} {p[1]:.6f} {p[2]:.6f}\n")
+            for q in t:
+                f.write(f"3 {q[0]} {q[1]} {q[2]}\n")
+
+    def hits(self, ray_set: int) -> tuple[np.ndarray, np.ndarray]:
+        """Per-ray sorted hit parameters of one ray set from the last keep_hits ray cast."""
+        c = self._context().handle
+        g = self.delphi.grid
+        nb, na = ((g.ny, g.nz), (g.ny, g.nz), (g.nx, g.ny), (g.nx, g.nz))[ray_set]
+        counts = np.zeros(nb * na, np.int32)
+        total = N.lib().nsg_download_hits(c, ray_set, N.ptr(counts), None, 0)
+        if total < 0:
+            N.check(total, "download hits")
+        vals = np.zeros(int(counts.sum()))
+        N.check(N.lib().nsg_download_hits(c, ray_set, N.ptr(counts), N.ptr(vals), len(vals)), "download hits")
+        return counts.reshape(na, nb), vals
+
+    def stats(self) -> dict:
+        out = np.zeros(8, np.int64)
+        N.check(N.lib().nsg_stats(self._context().handle, N.ptr(out), 8), "stats")
+        keys = ("patches", "vertices", "analytic_vertices", "triangles", "active_cubes", "cavities",
+                "overflow_rays", "pair_capacity")
+        return dict(zip(keys, out.tolist()))
+
+    # snake_case aliases
+    get_surf = getSurf
+    triangulate_surface = triangulateSurface
+
+
+class ConnollySurface(Surface):
+    """Solvent-excluded (Connolly) surface, ``Surface = ses``."""
+
+    name = "ses"
+
+    def build(self) -> bool:
+        atoms = self.delphi.atoms
+        # jitter the atoms after the grid was built (src/ConnollySurface.cpp:2484-2488)
+        if self.randDisplacement > 0:
+            N.check(N.lib().nsg_jitter_atoms(N.ptr(atoms), len(atoms), self.randDisplacement, ctypes.byref(_seed)),
+                    "jitter")
+        threads = 1 if self.forceSerialBuild else self.numThreads
+        self.patches = build_ses_patches(atoms, self.probe_radius, threads)
+        return True
+
+
+class SurfaceFactory:
+    """Surface registry keyed by the .prm ``Surface`` value."""
+
+    def __init__(self):
+        self.surfRegister: dict[str, Callable[..., Surface]] = {}
+
+    def add(self, name: str, ctor: Callable[..., Surface]) -> None:
+        self.surfRegister[name] = ctor
+
+    def create(self, conf: ConfigFile, ds: DelPhiShared, device: int = 0) -> Surface:
+        name = conf.read("Surface", "ses", str).strip()
+        if name not in self.surfRegister:
+            raise KeyError(f"{name} type is not registered!")
+        return self.surfRegister[name](conf, ds, device)
+
+    def available(self) -> list[str]:
+        return sorted(self.surfRegister)
+
+
+_factory = SurfaceFactory()
+_factory.add("ses", lambda cf, ds, dev=0: ConnollySurface(cf, ds, dev))
+
+
+def surfaceFactory() -> SurfaceFactory:
+    return _factory
+
+
+# --------------------------------------------------------------------------------------------
+class NanoShaper:
+    """Library facade: atoms + configuration in, surface volume / area / maps out."""
+
+    def __init__(self, atoms: np.ndarray, surface: str = "ses", probe: float = DEFAULT_PROBE,
+                 scale: float = DEFAULT_SCALE, perfil: float = DEFAULT_PERFIL, config: ConfigFile | None = None,
+                 device: int = 0, precision: str = "fp64"):
+        cf = config or ConfigFile()
+        if not cf.keyExists("Surface"):
+            cf.add("Surface", surface)
+        if not cf.keyExists("Probe_Radius"):
+            cf.add("Probe_Radius", probe)
+        if not cf.keyExists("Accurate_Triangulation"):
+            cf.add("Accurate_Triangulation", True)
+        if not cf.keyExists("Gpu_Precision"):
+            cf.add("Gpu_Precision", precision)
+        self.cf = cf
+        self.scale = cf.read("Grid_scale", scale, float)
+        self.perfil = cf.read("Grid_perfil", perfil, float)
+        self.ds = DelPhiShared(atoms, self.scale, self.perfil, build_status=cf.read("Build_status_map", True, bool))
+        self.surf = surfaceFactory().create(cf, self.ds, device)
+
+    def buildAnalyticalSurface(self, randDisplacement: float = -1) -> bool:
+        if randDisplacement >= 0:
+            self.surf.randDisplacement = randDisplacement
+        return self.surf.build()
+
+    def colourGrid(self, fill_cavities: bool | None = None, cav_vol: float | None = None) -> float:
+        fill = self.cf.read("Cavity_Detection_Filling", False, bool) if fill_cavities is None else fill_cavities
+        vol = self.cf.read("Conditional_Volume_Filling_Value", 11.4, float) if cav_vol is None else cav_vol
+        return self.surf.getSurf(True, fill, vol)
+
+    def triangulate(self) -> float:
+        return self.surf.triangulateSurface()
+
+    def getGridSize(self) -> list[int]:
+        return [self.ds.nx, self.ds.ny, self.ds.nz]
+
+    def getGridPointStatus(self, ix: int, iy: int, iz: int) -> int:
+        """+1 outside, -1 inside, 0 unknown (grid not computed)."""
+        if self.ds.status is None:
+            return 0
+        return -1 if self.ds.status[iz, iy, ix] == STATUS_POINT_INSIDE else 1

@@ -274,6 +274,11 @@ struct Oracle {
   std::vector<int32_t> cav_filled;
   std::vector<int64_t> ray_hits;  // per pixel id: number of hits (for tests)
   int64_t n_hits = 0;
+  // optional sample: only rays whose second pixel index n lies in [slab_lo*na, slab_hi*na)
+  double slab_lo = 0.0, slab_hi = 1.0;
+  int64_t n_lo(int64_t na) const { return (int64_t)(slab_lo * na); }
+  int64_t n_hi(int64_t na) const { return slab_hi >= 1.0 ? na : (int64_t)(slab_hi * na); }
+  int64_t rays_cast = 0;
 
   double X(int64_t i) const { return ns_coord(g.xmin, g.side, i); }
   double Y(int64_t i) const { return ns_coord(g.ymin, g.side, i); }
@@ -321,6 +326,7 @@ struct Oracle {
           int64_t m = rp - n * pixels[fd];
           n += i_start[ld];
           m += i_start[fd];
+          if (n < n_lo(Nd(ld)) || n >= n_hi(Nd(ld))) continue;
           pa[fd] = coord(fd, m) + delta;
           if (pa[fd] < down[fd] || pa[fd] > up[fd]) continue;
           pa[ld] = coord(ld, n) + delta;
@@ -400,7 +406,8 @@ struct Oracle {
       flagsum++;
       double pa[3], pb[3];
       pa[0] = X(0); pb[0] = X(g.nx - 1);
-      for (int64_t n = 0; n < na; n++) {
+      rays_cast += (n_hi(na) - n_lo(na)) * nb;
+      for (int64_t n = n_lo(na); n < n_hi(na); n++) {
         pa[2] = Z(n);
         for (int64_t m = 0; m < nb; m++) {
           int64_t id = (n * NMAX + m) * numPanels + panel;
@@ -434,7 +441,8 @@ struct Oracle {
     double pa[3], pb[3];
     pa[vc] = coord(vc, 0) + delta;
     pb[vc] = coord(vc, Nd(vc) - 1) + delta;
-    for (int64_t n = 0; n < na; n++) {
+    rays_cast += (n_hi(na) - n_lo(na)) * nb;
+    for (int64_t n = n_lo(na); n < n_hi(na); n++) {
       if (panel == 0) pa[2] = Z(n) + delta;
       else if (panel == 1) pa[1] = Y(n) + delta;
       else pa[2] = Z(n) + delta;
@@ -750,6 +758,7 @@ double nso_scalar(void* h, const char* what) {
   if (w == "area") return o->area;
   if (w == "ncav") return o->ncav;
   if (w == "n_hits") return (double)o->n_hits;
+  if (w == "rays_cast") return (double)o->rays_cast;
   if (w == "vol_panel0") return o->volPanel[0];
   if (w == "vol_panel1") return o->volPanel[1];
   if (w == "vol_panel2") return o->volPanel[2];
@@ -788,6 +797,22 @@ int nso_copy(void* h, const char* what, void* dst) {
 
 void nso_free(void* h) { delete (Oracle*)h; }
 
+// Ray casting of a slab of every ray set (rays whose second pixel index lies in
+// [slab_lo, slab_hi) of its range), used to time a bounded sample of a large workload.
+void* nso_run_slab(const NsGrid* g, int64_t n_patches, const double* f64, const int32_t* i32, const double* pool,
+                   const int8_t* pool_flag, double probe, int flags, int nthreads, double slab_lo, double slab_hi) {
+  Oracle* o = new Oracle();
+  o->g = *g;
+  o->P = {n_patches, f64, i32, pool, pool_flag, probe};
+  o->flags = flags & 3;
+  o->cav_vol = 0;
+  o->nthreads = nthreads;
+  o->slab_lo = slab_lo;
+  o->slab_hi = slab_hi;
+  o->run();
+  return o;
+}
+
 // Individual math restatements, exposed for the known-answer tests.
 int nso_ray_sphere(const double* orig, const double* dir, const double* c, double r, double* t) {
   return ray_sphere(orig, dir, c, r, &t[0], &t[1]) ? 1 : 0;
@@ -798,5 +823,12 @@ int nso_quartic(double b, double c, double d, double e, double* roots) {
   return n;
 }
 double nso_real_cubic(double b, double c, double d) { return real_cubic(b, c, d); }
+// rayTorus restatement; t[0..1] hold the clipping-sphere hits on input.
+int nso_ray_torus(const double* invrot9, const double* tc, const double* sc, double probe, double major,
+                  double radius, int panel, const double* orig, const double* dir, double* t) {
+  int vc = (panel == 0) ? 0 : ((panel == 1) ? 2 : 1);
+  int n = 0;
+  return ray_torus(invrot9, tc, sc, probe, major, radius, vc, orig, dir, t, n) ? n : 0;
+}
 
 }  // extern "C"

@@ -1,0 +1,138 @@
+"""ORACLE — test infrastructure only.  Python access to the CPU restatement in ns_oracle.cpp.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this module, as the
+checker; the product library never imports it.
+"""
+from __future__ import annotations
+
+import ctypes
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "_build" / "libnsoracle.so"
+
+STATUS = 1
+ACCURATE_TRIANGULATION = 2
+CAVITIES = 4
+TRIANGULATE = 8
+
+_lib = None
+
+
+def build() -> Path:
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build()
+        L = ctypes.CDLL(str(LIB))
+        P = ctypes.c_void_p
+        L.nso_run.restype = P
+        L.nso_run.argtypes = [P, ctypes.c_int64, P, P, P, P, ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                              ctypes.c_int]
+        L.nso_scalar.restype = ctypes.c_double
+        L.nso_scalar.argtypes = [P, ctypes.c_char_p]
+        L.nso_size.restype = ctypes.c_int64
+        L.nso_size.argtypes = [P, ctypes.c_char_p]
+        L.nso_copy.restype = ctypes.c_int
+        L.nso_copy.argtypes = [P, ctypes.c_char_p, P]
+        L.nso_free.argtypes = [P]
+        L.nso_ray_sphere.restype = ctypes.c_int
+        L.nso_ray_sphere.argtypes = [P, P, P, ctypes.c_double, P]
+        L.nso_quartic.restype = ctypes.c_int
+        L.nso_quartic.argtypes = [ctypes.c_double] * 4 + [P]
+        L.nso_real_cubic.restype = ctypes.c_double
+        L.nso_real_cubic.argtypes = [ctypes.c_double] * 3
+        L.nso_run_slab.restype = P
+        L.nso_run_slab.argtypes = [P, ctypes.c_int64, P, P, P, P, ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                   ctypes.c_double, ctypes.c_double]
+        L.nso_ray_torus.restype = ctypes.c_int
+        L.nso_ray_torus.argtypes = [P, P, P, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int, P, P, P]
+        _lib = L
+    return _lib
+
+
+class OracleResult:
+    """Products of one oracle run (arrays copied out, native handle freed)."""
+
+    def __init__(self, handle, grid):
+        L = lib()
+        self.grid = grid
+
+        def arr(name, dtype):
+            n = L.nso_size(handle, name.encode())
+            a = np.zeros(max(n, 0), dtype)
+            if n > 0:
+                L.nso_copy(handle, name.encode(), a.ctypes.data)
+            return a
+
+        self.volume = L.nso_scalar(handle, b"volume")
+        self.area = L.nso_scalar(handle, b"area")
+        self.ncav = int(L.nso_scalar(handle, b"ncav"))
+        self.n_hits = int(L.nso_scalar(handle, b"n_hits"))
+        self.status = arr("status", np.int32)
+        if len(self.status):
+            self.status = self.status.reshape(grid.nz, grid.ny, grid.nx)
+        self.bits = arr("bits", np.uint32)
+        self.vertices = arr("verts", np.float64).reshape(-1, 3)
+        self.vertex_edges = arr("vkeys", np.int32).reshape(-1, 4)
+        self.triangles = arr("tris", np.int32).reshape(-1, 3)
+        self.cav_size = arr("cav_size", np.float64)
+        n = L.nso_size(handle, b"cav_size")
+        fl = np.zeros(max(n, 0), np.int32)
+        if n > 0:
+            L.nso_copy(handle, b"cav_filled", fl.ctypes.data)
+        self.cav_filled = fl
+        self.pix_off = arr("pix_off", np.int64)
+        self.pix_t = arr("pix_t", np.float64)
+
+
+def run(grid, patches, flags: int = STATUS | ACCURATE_TRIANGULATION | CAVITIES | TRIANGULATE, cav_vol: float = 0.0,
+        threads: int = 1) -> OracleResult:
+    """Runs the CPU restatement on a grid (NsGrid ctypes struct) and a PatchSet."""
+    L = lib()
+    p = patches
+    h = L.nso_run(ctypes.byref(grid), p.n, p.f64.ctypes.data, p.i32.ctypes.data, p.pool.ctypes.data,
+                  p.pool_flag.ctypes.data, p.probe, flags, cav_vol, threads)
+    try:
+        return OracleResult(h, grid)
+    finally:
+        L.nso_free(h)
+
+
+def ray_hits(res: OracleResult, ray_set: int) -> tuple[np.ndarray, np.ndarray]:
+    """Per-ray sorted hits of one ray set, laid out like the GPU dump: (counts[na, nb], values)."""
+    g = res.grid
+    nmax = max(g.nx, g.ny, g.nz)
+    nb, na = ((g.ny, g.nz), (g.ny, g.nz), (g.nx, g.ny), (g.nx, g.nz))[ray_set]
+    npan = (len(res.pix_off) - 1) // (nmax * nmax)
+    panel_idx = ray_set if npan == 4 else ray_set - 1
+    n_idx = np.arange(na)[:, None]
+    m_idx = np.arange(nb)[None, :]
+    pid = (n_idx * nmax + m_idx) * npan + panel_idx
+    off = res.pix_off[pid]
+    cnt = res.pix_off[pid + 1] - off
+    vals = np.concatenate([res.pix_t[o:o + c] for o, c in zip(off.ravel(), cnt.ravel())]) if cnt.sum() else np.zeros(0)
+    return cnt.astype(np.int32), vals
+
+
+def time_slab(grid, patches, threads: int, slab_lo: float, slab_hi: float,
+              flags: int = STATUS | ACCURATE_TRIANGULATION) -> tuple[float, int]:
+    """Wall time (s) and number of rays of the oracle's ray casting of a slab of every ray set."""
+    import time
+    L = lib()
+    p = patches
+    t0 = time.perf_counter()
+    h = L.nso_run_slab(ctypes.byref(grid), p.n, p.f64.ctypes.data, p.i32.ctypes.data, p.pool.ctypes.data,
+                       p.pool_flag.ctypes.data, p.probe, flags, threads, slab_lo, slab_hi)
+    dt = time.perf_counter() - t0
+    rays = int(L.nso_scalar(h, b"rays_cast"))
+    L.nso_free(h)
+    return dt, rays
