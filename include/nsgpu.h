@@ -1,0 +1,137 @@
+/* libnsgpu -- B200 grid ray-casting molecular surface builder, C ABI.
+ *
+ * Drop-in boundary for the part of NanoShaper that runs once a surface's patches exist:
+ * Surface::getSurf (src/Surface.cpp:398-1692) and Surface::triangulateSurface
+ * (src/Surface.cpp:9909-10526), behind the Surface plugin interface (src/Surface.h:835-990).
+ * Plain pointers and sizes only.  Every call returns NSG_OK (0) or a negative NSG_ERR_* code and
+ * never terminates the process (the reference exits on fatal errors).  Host buffers are always
+ * owned by the caller; device buffers by the context.  One context per host thread.
+ */
+#ifndef NSGPU_H
+#define NSGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NSG_OK 0
+#define NSG_ERR_ARG (-1)
+#define NSG_ERR_EMPTY (-2)
+#define NSG_ERR_IO (-3)
+#define NSG_ERR_CAPACITY (-4)
+#define NSG_ERR_CUDA (-5)
+#define NSG_ERR_NOMEM (-6)
+#define NSG_ERR_STATE (-7)
+#define NSG_ERR_GEOMETRY (-8)
+#define NSG_ERR_TIMEOUT (-9)
+
+/* nsg_raycast flags */
+#define NSG_RAYCAST_STATUS 1            /* status map: Build_status_map = true */
+#define NSG_RAYCAST_TRIANGULATION 2     /* accurate-triangulation rays: Accurate_Triangulation = true */
+#define NSG_RAYCAST_KEEP_HITS 16        /* keep per-ray sorted hits for nsg_download_hits */
+
+/* precision of nsg_raycast */
+#define NSG_PRECISION_FP64 0
+#define NSG_PRECISION_MIXED 1
+
+/* Grid environment; replaces the grid members of DelPhiShared (src/DelphiShared.h:151-213).
+ * Node i of an axis sits at min + i*side. */
+typedef struct NsGrid {
+  int64_t nx, ny, nz;
+  double xmin, ymin, zmin;
+  double xmax, ymax, zmax;
+  double scale, side, hside, A;
+  double rmaxdim;
+  double baricenter[3];
+} NsGrid;
+
+/* Patch set layout (host builder output, ray caster input).
+ *   f64 : 20 doubles per patch: [0..2] bounding-sphere centre, [3] radius, [4..6] torus centre,
+ *         [7] torus major radius, [8] spindle self-intersection radius (<0: none),
+ *         [9..17] inverse torus frame (row major), [18..19] unused
+ *   i32 : 4 ints per patch: kind (0 point, 1 regular edge, 2 singular edge, 3 regular facet,
+ *         4 singular facet), first pool entry, pool entry count, unused
+ *   pool: 4 doubles per entry: clipping sphere (x, y, z, r^2) for points, plane (a, b, c, d)
+ *         for facets and edges (a point with a*x+b*y+c*z+d > 0 is cut away)
+ *   pool_flag: 1 byte per entry; for edges, 1 on the first plane of an acute pair.
+ * Mirrors the cell records of src/ConnollySurface.h:31-167. */
+
+typedef struct nsg_ctx nsg_ctx;
+typedef struct NsPatchSet NsPatchSet;
+
+/* ---- grid environment (host) ---- */
+/* DelPhiShared::buildGrid (src/DelphiShared.cpp:1038-1201). */
+int nsg_grid_build(const double* atoms_xyzr, int64_t n_atoms, double scale, double perfil, NsGrid* out);
+/* randnum (src/tools.cpp:64-81); *seed is the generator state (1234 initially, src/tools.h:1827). */
+double nsg_randnum(int64_t* seed);
+/* Atom jitter of buildConnollyCGAL (src/ConnollySurface.cpp:2484-2488). */
+int nsg_jitter_atoms(double* atoms_xyzr, int64_t n_atoms, double displacement, int64_t* seed);
+/* xyzr reading of DelPhiShared::loadAtoms (src/DelphiShared.cpp:309-704); out == NULL counts. */
+int64_t nsg_read_xyzr(const char* path, double* out, int64_t capacity);
+
+/* ---- patch construction (host) ---- */
+/* ConnollySurface::build / buildConnollyCGAL (src/ConnollySurface.cpp:256, 2326-3316). */
+int nsg_ses_build(const double* atoms_xyzr, int64_t n_atoms, double probe_radius, int n_threads, NsPatchSet** out);
+int nsg_patchset_info(const NsPatchSet* ps, int64_t* n_patches, int64_t* n_pool, int64_t counts[5]);
+int nsg_patchset_export(const NsPatchSet* ps, double* f64, int32_t* i32, double* pool, int8_t* pool_flag);
+void nsg_patchset_free(NsPatchSet* ps);
+
+/* ---- device context ---- */
+int nsg_version(void);
+const char* nsg_last_error(void);
+int nsg_ctx_create(int device, nsg_ctx** out);
+int nsg_ctx_destroy(nsg_ctx* ctx);
+int nsg_set_stream(nsg_ctx* ctx, void* cuda_stream);
+void* nsg_get_stream(nsg_ctx* ctx);
+/* Grid of the surface (the DelPhiShared* the reference Surface holds, src/Surface.h:572). */
+int nsg_set_grid(nsg_ctx* ctx, const NsGrid* grid);
+/* Patch set from host memory (the sesComplex of src/ConnollySurface.h). */
+int nsg_upload_patches(nsg_ctx* ctx, int64_t n, const double* f64, const int32_t* i32, int64_t n_pool,
+                       const double* pool, const int8_t* pool_flag, double probe_radius);
+/* Patch set already resident in device memory (no copy). */
+int nsg_bind_patches_device(nsg_ctx* ctx, int64_t n, const double* f64, const int32_t* i32, int64_t n_pool,
+                            const double* pool, const int8_t* pool_flag, double probe_radius);
+
+/* ---- the hot path ---- */
+/* Ray casting of Surface::getSurf: getPatchIntersectionData (src/ConnollySurface.cpp:4319-4590),
+ * pixel binning and sort (src/Surface.cpp:4766-5095), setVerticesAndGridsWithIntersectionData
+ * (src/Surface.cpp:5101-6251) and the volume (src/Surface.cpp:1680-1684). */
+int nsg_raycast(nsg_ctx* ctx, int flags, int precision, double* volume);
+/* getCavitiesWithBilevelStatusMap + fillCavities (src/Surface.cpp:1994-2126, 2355-2484). */
+int nsg_cavities(nsg_ctx* ctx, double cavity_volume, int* n_cavities);
+/* Label order of the alternating-z seed scan of getCavitiesWithBilevelStatusMap
+ * (src/Surface.cpp:2044-2116) over regions sorted by first node; host only. */
+int nsg_cavity_order(int32_t n_regions, const uint32_t* desc_key, int32_t* label_out);
+/* assembleVerticesList + triangulateSurface (src/Surface.cpp:7415-7667, 9909-10526). */
+int nsg_triangulate(nsg_ctx* ctx, double* area, int64_t* n_vertices, int64_t* n_triangles);
+
+/* ---- results into caller-owned host buffers ---- */
+/* Status map, flat int32 k*ny*nx + j*nx + i (read3DVector layout, src/tools.h:549-575). */
+int nsg_download_status(nsg_ctx* ctx, int32_t* dst);
+/* 32x-packed insideness bits, bit = 1 outside (src/tools.h:1324-1414); ceil(nx/32)*ny*nz words. */
+int nsg_download_insideness(nsg_ctx* ctx, uint32_t* dst);
+/* Vertices (3 doubles), their grid edges (ix, iy, iz, dir) and triangles (3 ints):
+ * vertList / triList of Surface (src/Surface.h). */
+int nsg_download_mesh(nsg_ctx* ctx, double* vertices, int32_t* vertex_edges, int32_t* triangles);
+/* cavitiesSize / cavitiesFlag of DelPhiShared (src/DelphiShared.h:160-213). */
+int nsg_download_cavities(nsg_ctx* ctx, double* sizes, int32_t* filled);
+/* Sorted hit parameters per ray of one ray set (tests). */
+int nsg_download_hits(nsg_ctx* ctx, int ray_set, int32_t* counts, double* dst, int64_t dst_capacity);
+
+/* ---- instrumentation ---- */
+int nsg_stats(nsg_ctx* ctx, int64_t* out, int n);
+double nsg_volume(nsg_ctx* ctx);
+double nsg_area(nsg_ctx* ctx);
+int nsg_event_record(nsg_ctx* ctx, int slot);
+int nsg_event_elapsed(nsg_ctx* ctx, int slot_a, int slot_b, double* ms);
+int nsg_profile(nsg_ctx* ctx, int enable);
+int nsg_stage_times(nsg_ctx* ctx, double* ms, int64_t* calls, int n);
+int64_t nsg_launch_count(nsg_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NSGPU_H */

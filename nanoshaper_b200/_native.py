@@ -62,6 +62,7 @@ _SIGNATURES = {
     "nsg_bind_patches_device": ([_P, _I64, _P, _P, _I64, _P, _P, _D], _INT),
     "nsg_raycast": ([_P, _INT, _INT, ctypes.POINTER(_D)], _INT),
     "nsg_cavities": ([_P, _D, ctypes.POINTER(_INT)], _INT),
+    "nsg_cavity_order": ([ctypes.c_int32, _P, _P], _INT),
     "nsg_triangulate": ([_P, ctypes.POINTER(_D), ctypes.POINTER(_I64), ctypes.POINTER(_I64)], _INT),
     "nsg_download_status": ([_P, _P], _INT),
     "nsg_download_insideness": ([_P, _P], _INT),

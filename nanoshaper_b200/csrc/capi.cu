@@ -461,6 +461,34 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
   return NSG_OK;
 }
 
+// Labels of the free regions in the order the reference's alternating scan discovers them
+// (getCavitiesWithBilevelStatusMap, src/Surface.cpp:2044-2116): regions are given sorted by
+// their first node in ascending scan order (k, j, i); desc_key[r] is region r's first node in
+// the descending-z scan.  Even rounds take the first remaining region of the ascending scan, odd
+// rounds that of the descending scan; the first region found is STATUS_POINT_OUT (3), the next
+// ones 4, 5, ...  Host-only; needs no device.
+int nsg_cavity_order(int32_t n, const uint32_t* desc_key, int32_t* label_out) {
+  if (n < 0 || (n > 0 && (!desc_key || !label_out))) return NSG_ERR_ARG;
+  std::vector<int32_t> by_desc(n);
+  for (int32_t i = 0; i < n; i++) by_desc[i] = i;
+  std::sort(by_desc.begin(), by_desc.end(), [&](int32_t a, int32_t b) { return desc_key[a] < desc_key[b]; });
+  std::vector<char> taken(n, 0);
+  int32_t pa = 0, pd = 0, id = NS_STATUS_TEMPORARY_OUT;
+  for (int32_t t = 0; t < n; t++) {
+    int32_t pick;
+    if ((t & 1) == 0) {
+      while (taken[pa]) pa++;
+      pick = pa;
+    } else {
+      while (taken[by_desc[pd]]) pd++;
+      pick = by_desc[pd];
+    }
+    taken[pick] = 1;
+    label_out[pick] = ++id;
+  }
+  return NSG_OK;
+}
+
 int nsg_cavities(nsg_ctx* c, double cav_vol, int* ncav_out) {
   if (!c || !c->have_status) return fail(NSG_ERR_STATE, "cavity detection needs the status map");
   CK(cudaSetDevice(c->device));
@@ -504,29 +532,11 @@ int nsg_cavities(nsg_ctx* c, double cav_vol, int* ncav_out) {
   CK(cudaMemcpyAsync(cnt.data(), c->cc_count.p, nroots * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaMemcpyAsync(desc.data(), c->cc_desc.p, nroots * sizeof(unsigned int), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  // replay the alternating seed scan: even rounds take the region whose first node in ascending
-  // order comes first (regions are already sorted by it), odd rounds the first in descending order
-  std::vector<int32_t> by_desc(nroots);
-  for (int32_t i = 0; i < nroots; i++) by_desc[i] = i;
-  std::sort(by_desc.begin(), by_desc.end(), [&](int32_t a, int32_t b) { return desc[a] < desc[b]; });
   std::vector<int32_t> label_of(nroots, 0);
   std::vector<uint8_t> fill_of(nroots, 0);
-  std::vector<char> taken(nroots, 0);
-  int32_t pa = 0, pd = 0, id = NS_STATUS_TEMPORARY_OUT;
+  nsg_cavity_order(nroots, desc.data(), label_of.data());
+  const int32_t id = NS_STATUS_TEMPORARY_OUT + nroots;
   const double cube = g.side * g.side * g.side;
-  for (int32_t t = 0; t < nroots; t++) {
-    int32_t pick;
-    if ((t & 1) == 0) {
-      while (taken[pa]) pa++;
-      pick = pa;
-    } else {
-      while (taken[by_desc[pd]]) pd++;
-      pick = by_desc[pd];
-    }
-    taken[pick] = 1;
-    id++;
-    label_of[pick] = id;
-  }
   c->ncav = id - NS_STATUS_OUT;
   c->cav_size.assign(c->ncav, 0.0);
   c->cav_filled.assign(c->ncav, 0);

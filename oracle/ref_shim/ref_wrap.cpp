@@ -3,6 +3,10 @@
 // infrastructure only.
 #include "tools.h"
 
+// Globals the reference's tools.cpp refers to but that its main program defines.
+fstream* errorStream = nullptr;
+fstream* internals = nullptr;
+
 extern "C" {
 int ref_ray_sphere(const double* o, const double* d, const double* c, double r, double* t) {
   return raySphere(o, d, c, r, &t[0], &t[1]) ? 1 : 0;

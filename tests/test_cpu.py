@@ -1,0 +1,225 @@
+"""CPU tests: the oracle against the reference's own math (golden vectors), known answers,
+an independent brute-force SES sampler, host logic of the library and its C-ABI surface."""
+import ctypes
+import re
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import nanoshaper_b200 as nb
+from nanoshaper_b200 import generator
+
+ROOT = Path(__file__).resolve().parent.parent
+GOLD = ROOT / "tests" / "golden" / "ref_math.npz"
+
+
+@pytest.fixture(scope="module")
+def gold():
+    return np.load(GOLD)
+
+
+def test_oracle_ray_sphere_matches_reference(gold, oracle_mod):
+    L = oracle_mod.lib()
+    inp, out = gold["sphere_in"], gold["sphere_out"]
+    t = np.zeros(2)
+    for row, exp in zip(inp, out):
+        pa, d, c, r = (np.ascontiguousarray(row[0:3]), np.ascontiguousarray(row[3:6]),
+                       np.ascontiguousarray(row[6:9]), row[9])
+        ok = L.nso_ray_sphere(pa.ctypes.data, d.ctypes.data, c.ctypes.data, r, t.ctypes.data)
+        assert ok == int(exp[0])
+        if ok:
+            assert t[0] == exp[1] and t[1] == exp[2]
+
+
+def test_oracle_ray_torus_matches_reference(gold, oracle_mod):
+    L = oracle_mod.lib()
+    inp, out = gold["torus_in"], gold["torus_out"]
+    assert len(inp) > 500
+    for row, exp in zip(inp, out):
+        inv = np.ascontiguousarray(row[0:9])
+        tc = np.ascontiguousarray(row[9:12])
+        sc = np.ascontiguousarray(row[12:15])
+        probe, major, radius, panel = row[15], row[16], row[17], int(row[18])
+        pa = np.ascontiguousarray(row[19:22])
+        d = np.ascontiguousarray(row[22:25])
+        t = np.zeros(4)
+        t[:2] = row[25:27]
+        n = L.nso_ray_torus(inv.ctypes.data, tc.ctypes.data, sc.ctypes.data, probe, major, radius, panel,
+                            pa.ctypes.data, d.ctypes.data, t.ctypes.data)
+        assert n == int(exp[0])
+        np.testing.assert_array_equal(t[:n], exp[1:1 + n])
+
+
+def test_jitter_generator_matches_reference(gold, native_lib):
+    seed = ctypes.c_int64(1234)
+    seq = [native_lib.nsg_randnum(ctypes.byref(seed)) for _ in range(64)]
+    np.testing.assert_array_equal(np.array(seq), gold["randnum"])
+
+
+def test_rintp_matches_reference(gold):
+    np.testing.assert_array_equal(np.floor(gold["rint_in"] + 0.5), gold["rint_out"])
+
+
+def test_quartic_known_roots(oracle_mod):
+    L = oracle_mod.lib()
+    roots = np.zeros(4)
+    # (x-1)(x-2)(x-3)(x-4)
+    n = L.nso_quartic(-10.0, 35.0, -50.0, 24.0, roots.ctypes.data)
+    assert n == 4
+    np.testing.assert_allclose(np.sort(roots), [1, 2, 3, 4], atol=1e-9)
+    # (x^2+1)(x-1)(x-3): two real roots
+    n = L.nso_quartic(-4.0, 4.0, -4.0, 3.0, roots.ctypes.data)
+    assert n == 2
+    np.testing.assert_allclose(np.sort(roots[:2]), [1, 3], atol=1e-9)
+    # x^4 + 1: none
+    assert L.nso_quartic(0.0, 0.0, 0.0, 1.0, roots.ctypes.data) == 0
+
+
+def _surface(n, seed, scale, perfil, probe=1.4):
+    atoms = generator.rsa_globule(n, seed)
+    nb.reset_seed()
+    ds = nb.DelPhiShared(atoms, scale, perfil)
+    surf = nb.ConnollySurface(nb.ConfigFile(text=f"Probe_Radius = {probe}\n"), ds)
+    surf.build()
+    return atoms, ds, surf
+
+
+def test_patch_builder_agrees_with_brute_force_ses(oracle_mod):
+    """Status map of the oracle (fed by the host patch builder) against an independent SES
+    sampler: a node is inside when a probe sphere centred there would not reach the
+    solvent-accessible surface (sampled densely on the non-buried parts of the expanded spheres)."""
+    from scipy.spatial import cKDTree
+    atoms, ds, surf = _surface(80, 5, 2.5, 70.0)
+    ref = oracle_mod.run(ds.grid, surf.patches, flags=oracle_mod.STATUS)
+    g = ds.grid
+    c = surf.delphi.atoms[:, :3]
+    R = surf.delphi.atoms[:, 3] + 1.4
+    k = np.arange(60000) + 0.5
+    phi = np.arccos(1 - 2 * k / len(k))
+    th = np.pi * (1 + 5 ** 0.5) * k
+    u = np.stack([np.cos(th) * np.sin(phi), np.sin(th) * np.sin(phi), np.cos(phi)], 1)
+    tree = cKDTree(c)
+    sas = []
+    for i in range(len(c)):
+        p = c[i] + R[i] * u
+        ok = np.ones(len(p), bool)
+        for j in tree.query_ball_point(c[i], R[i] + R.max()):
+            if j != i:
+                ok &= ((p - c[j]) ** 2).sum(1) >= R[j] ** 2
+        sas.append(p[ok])
+    sas = np.concatenate(sas)
+    z, y, x = np.meshgrid(g.zmin + np.arange(g.nz) * g.side, g.ymin + np.arange(g.ny) * g.side,
+                          g.xmin + np.arange(g.nx) * g.side, indexing="ij")
+    q = np.stack([x.ravel(), y.ravel(), z.ravel()], 1)
+    d_sas, _ = cKDTree(sas).query(q)
+    nbrs = tree.query_ball_point(q, R.max())
+    in_union = np.array([any(((qq - c[j]) ** 2).sum() < R[j] ** 2 for j in nb_) for qq, nb_ in zip(q, nbrs)])
+    brute = in_union & (d_sas >= 1.4)
+    ora = (ref.status == -1).ravel()
+    amb = np.abs(d_sas - 1.4) < 0.05
+    assert ((ora != brute) & ~amb).sum() == 0
+    assert (ora != brute).sum() < 1e-3 * len(ora)
+
+
+def test_rays_are_watertight(oracle_mod):
+    """Every ray of every ray set crosses the patch partition an even number of times."""
+    atoms, ds, surf = _surface(327, 1, 2.0, 70.0)
+    ref = oracle_mod.run(ds.grid, surf.patches)
+    for s in range(4):
+        cnt, _ = oracle_mod.ray_hits(ref, s)
+        assert (cnt % 2).sum() == 0
+
+
+def test_single_sphere_oracle_volume(oracle_mod):
+    ds = nb.DelPhiShared(np.array([[0.0, 0.0, 0.0, 1.7]]), 4.0, 50.0)
+    ps = nb.build_ses_patches(ds.atoms, 1.4)
+    assert ps.counts == (1, 0, 0, 0, 0)
+    ref = oracle_mod.run(ds.grid, ps)
+    assert abs(ref.volume - 4 / 3 * np.pi * 1.7 ** 3) / (4 / 3 * np.pi * 1.7 ** 3) < 0.02
+    assert abs(ref.area - 4 * np.pi * 1.7 ** 2) / (4 * np.pi * 1.7 ** 2) < 0.05
+
+
+def test_two_sphere_torus_patch(oracle_mod):
+    """Two atoms closer than two probe diameters: one torus, two point cells, no probe patch."""
+    atoms = np.array([[0.0, 0.0, 0.0, 1.7], [3.0, 0.0, 0.0, 1.7]])
+    ps = nb.build_ses_patches(atoms, 1.4)
+    assert ps.counts == (2, 0, 1, 0, 0)
+    # the torus: centre midway, major radius sqrt((r+p)^2 - (d/2)^2)
+    tor = ps.f64[ps.i32[:, 0] == 2][0]
+    np.testing.assert_allclose(tor[4:7], [1.5, 0, 0], atol=1e-12)
+    np.testing.assert_allclose(tor[7], np.sqrt(3.1 ** 2 - 1.5 ** 2), rtol=1e-12)
+
+
+def test_library_exports_header_symbols(native_lib):
+    header = (ROOT / "include" / "nsgpu.h").read_text()
+    decl = set(re.findall(r"\b(nsg_\w+)\s*\(", header))
+    out = subprocess.run(["nm", "-D", "--defined-only", str(ROOT / "nanoshaper_b200" / "lib" / "libnsgpu.so")],
+                         capture_output=True, text=True, check=True).stdout
+    exported = set(re.findall(r" T (nsg_\w+)", out))
+    assert decl, "no declarations parsed"
+    assert decl <= exported, f"missing: {sorted(decl - exported)}"
+    for name in decl:
+        getattr(native_lib, name)
+
+
+def test_config_file_semantics():
+    cf = nb.ConfigFile(text="# comment\nGrid_scale = 2.5 # trailing\nBuild_status_map = false\n"
+                            "Surface = ses\nName = a\n  b\n\nEndConfigFile\nAfter = 1\n")
+    assert cf.read("Grid_scale", 1.0) == 2.5
+    assert cf.read("Build_status_map", True) is False
+    assert cf.read("Surface", "x") == "ses"
+    assert cf.read("Name", "") == "a\n  b"
+    assert not cf.keyExists("After")
+    assert cf.read("Missing", 7) == 7
+    for v in ("false", "F", "no", "N", "0", "none"):
+        assert nb.ConfigFile(text=f"k = {v}\n").read("k", True) is False
+    assert nb.ConfigFile(text="k = yes\n").read("k", False) is True
+
+
+def test_grid_build_matches_reference_formula(native_lib):
+    atoms = generator.rsa_globule(50, 9)
+    ds = nb.DelPhiShared(atoms, 2.0, 70.0)
+    lo = (atoms[:, :3] - atoms[:, 3:]).min(0)
+    hi = (atoms[:, :3] + atoms[:, 3:]).max(0)
+    mid = (hi + lo) / 2
+    rmax = 2 * np.max(np.abs(np.concatenate([hi - mid, lo - mid])))
+    ig = int(np.floor(2.0 * 100.0 / 70.0 * rmax))
+    ig += 1 - ig % 2
+    assert ds.nx == ig and ds.grid.xmin == mid[0] - (ig - 1) / (2 * 2.0)
+
+
+def test_generator_is_seeded():
+    a = generator.rsa_globule(200, 3)
+    b = generator.rsa_globule(200, 3)
+    np.testing.assert_array_equal(a, b)
+    from scipy.spatial import cKDTree
+    d, _ = cKDTree(a[:, :3]).query(a[:, :3], k=2)
+    assert d[:, 1].min() >= generator.DMIN
+    assert set(np.unique(a[:, 3])) <= set(generator.RADII)
+
+
+def test_cavity_label_replay_matches_oracle(native_lib, oracle_mod):
+    """Host replay of the alternating seed scan over union-find regions reproduces the oracle's
+    sequential flood-fill labels."""
+    from scipy import ndimage
+    atoms, ds, surf = _surface(327, 1, 2.0, 70.0)
+    pre = oracle_mod.run(ds.grid, surf.patches, flags=oracle_mod.STATUS).status
+    post = oracle_mod.run(ds.grid, surf.patches, flags=oracle_mod.STATUS | oracle_mod.CAVITIES).status
+    lab, n = ndimage.label(pre == 2)
+    assert n > 3
+    flat = lab.ravel()
+    idx = np.arange(flat.size)
+    roots = np.array([idx[flat == c].min() for c in range(1, n + 1)])
+    g = ds.grid
+    plane = g.nx * g.ny
+    desc = np.array([((g.nz - 1 - idx[flat == c] // plane) * plane + idx[flat == c] % plane).min()
+                     for c in range(1, n + 1)], np.uint32)
+    order = np.argsort(roots)
+    labels = np.zeros(n, np.int32)
+    rc = native_lib.nsg_cavity_order(n, desc[order].ctypes.data, labels.ctypes.data)
+    assert rc == 0
+    for pos, c in enumerate(order):
+        node = roots[c]
+        assert post.ravel()[node] == labels[pos]
