@@ -91,6 +91,11 @@ struct nsg_ctx {
   int precision = 0;
   double volume = 0;
   bool have_status = false, have_bits = false;
+  // status map in run form (inside runs per row) and its free runs; the dense map is written
+  // on demand (download, cavity labelling)
+  DevBuf sruns, srun_off, srun_cnt, fr_cnt, fr_off, fruns, frow;
+  int64_t srun_cap = 0, n_fruns = 0;
+  bool status_dense = false;
   // cavities
   DevBuf labels, is_root, roots, cc_count, cc_desc, cc_label_of, cc_fill_of, nroots_d;
   int ncav = 0;
@@ -211,6 +216,51 @@ int bin_panel(nsg_ctx* c, int panel) {
   return NSG_OK;
 }
 
+nsg::RunArgs run_args(nsg_ctx* c) {
+  nsg::RunArgs A{};
+  const NsGrid& g = c->grid;
+  A.nx = g.nx; A.ny = g.ny; A.nz = g.nz;
+  A.nrows = g.ny * g.nz;
+  A.sruns = c->sruns.as<int2>();
+  A.srun_off = c->srun_off.as<int64_t>();
+  A.srun_cnt = c->srun_cnt.as<int32_t>();
+  A.fr_cnt = c->fr_cnt.as<int32_t>();
+  A.fr_off = c->fr_off.as<int64_t>();
+  A.fruns = c->fruns.as<int2>();
+  A.frow = c->frow.as<int32_t>();
+  A.nruns = c->n_fruns;
+  A.L = c->labels.as<int32_t>();
+  return A;
+}
+
+// Free runs of every status row (complement of the inside runs).
+int build_free_runs(nsg_ctx* c) {
+  const int64_t nrows = c->grid.ny * c->grid.nz;
+  CK(c->fr_cnt.ensure(nrows * sizeof(int32_t)));
+  CK(c->fr_off.ensure((nrows + 1) * sizeof(int64_t)));
+  nsg::RunArgs A = run_args(c);
+  LAUNCH(nsg::launch_free_runs(A, 0, c->stream));
+  int64_t n = 0;
+  int rc = scan_counts(c, c->fr_cnt.as<int32_t>(), nrows, c->fr_off.as<int64_t>(), &n);
+  if (rc) return rc;
+  CK(c->fruns.ensure(std::max<int64_t>(n, 1) * sizeof(int2)));
+  CK(c->frow.ensure(std::max<int64_t>(n, 1) * sizeof(int32_t)));
+  c->n_fruns = n;
+  A = run_args(c);
+  LAUNCH(nsg::launch_free_runs(A, 1, c->stream));
+  return NSG_OK;
+}
+
+// Dense status map from the runs (labels when cavity detection ran).
+int materialize_status(nsg_ctx* c, const int32_t* label_of_dev) {
+  const NsGrid& g = c->grid;
+  CK(c->status.ensure(g.nx * g.ny * g.nz * sizeof(int32_t)));
+  nsg::RunArgs A = run_args(c);
+  LAUNCH(nsg::status_write(A, label_of_dev, c->status.as<int32_t>(), c->stream));
+  c->status_dense = true;
+  return NSG_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -243,7 +293,8 @@ int nsg_ctx_destroy(nsg_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   DevBuf* bufs[] = {&c->f64, &c->i32, &c->pool, &c->flag, &c->win, &c->status, &c->bits, &c->pairs,
                     &c->ray_pair_off, &c->ray_pair_cnt, &c->cursors, &c->ovf_scratch, &c->err, &c->hits,
-                    &c->labels, &c->is_root, &c->roots, &c->cc_count, &c->cc_desc, &c->cc_label_of,
+                    &c->labels, &c->is_root, &c->sruns, &c->srun_off, &c->srun_cnt, &c->fr_cnt, &c->fr_off,
+                    &c->fruns, &c->frow, &c->roots, &c->cc_count, &c->cc_desc, &c->cc_label_of,
                     &c->cc_fill_of, &c->nroots_d, &c->surv_cnt, &c->surv_off, &c->vpos, &c->vkey,
                     &c->row_act_cnt, &c->row_mid_cnt, &c->row_act_off, &c->row_mid_off, &c->act_rec,
                     &c->act_mid, &c->tri_cnt, &c->tri_off, &c->tris, &c->cube_area, &c->red_out, &c->temp};
@@ -349,7 +400,12 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
   stage_end(c, kStageBin);
   const int64_t nwords = nwords_of(g);
   const int64_t nrays_mc = g.nz * g.ny + g.ny * g.nx + g.nz * g.nx;
-  if (do_status) CK(c->status.ensure(tot * sizeof(int32_t)));
+  const int64_t nrows = g.ny * g.nz;
+  if (do_status) {
+    CK(c->srun_off.ensure(nrows * sizeof(int64_t)));
+    CK(c->srun_cnt.ensure(nrows * sizeof(int32_t)));
+    if (c->srun_cap == 0) c->srun_cap = std::max<int64_t>(4 * nrows, 1 << 16);
+  }
   if (do_mc) {
     CK(c->bits.ensure(nwords * sizeof(uint32_t)));
     CK(cudaMemsetAsync(c->bits.p, 0xff, nwords * sizeof(uint32_t), c->stream));
@@ -363,6 +419,10 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
   const int ovf_cap = 1 << 16;
   for (int attempt = 0; attempt < 4; attempt++) {
     if (do_mc) CK(c->pairs.ensure(c->pair_cap * 2 * sizeof(double)));
+    if (do_status) {
+      CK(c->sruns.ensure(c->srun_cap * sizeof(int2)));
+      CK(cudaMemsetAsync(c->srun_cnt.p, 0, nrows * sizeof(int32_t), c->stream));
+    }
     if (keep_hits) {
       if (c->hit_cap == 0) c->hit_cap = std::max<int64_t>(8 * (nrays_mc + g.nz * g.ny), 1 << 16);
       CK(c->hits.ensure(c->hit_cap * sizeof(double)));
@@ -385,7 +445,11 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
       CK(c->vol_ray[s].ensure(nr * sizeof(double)));
       CK(c->ovf_rays[s].ensure(ovf_cap * sizeof(int32_t)));
       nsg::TraceOut o{};
-      o.status = c->status.as<int32_t>();
+      o.sruns = c->sruns.as<int2>();
+      o.srun_cap = c->srun_cap;
+      o.srun_cursor = cur + 2;
+      o.srun_off = c->srun_off.as<int64_t>();
+      o.srun_cnt = c->srun_cnt.as<int32_t>();
       o.bits = c->bits.as<uint32_t>();
       o.vol_ray = c->vol_ray[s].as<double>();
       o.pairs = c->pairs.as<double>();
@@ -432,13 +496,14 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
     stage_end(c, kStageOverflow);
     c->last_overflow_rays = tot_ovf;
     int32_t errflag = 0;
-    unsigned long long used[2] = {0, 0};
+    unsigned long long used[3] = {0, 0, 0};
     CK(cudaMemcpyAsync(&errflag, c->err.p, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaMemcpyAsync(used, cur, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(used, cur, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     if (errflag == 0) break;
     if (errflag == 3) { c->pair_cap = std::max<int64_t>(2 * c->pair_cap, (int64_t)used[0] + 1024); continue; }
     if (errflag == 2) { c->hit_cap = std::max<int64_t>(2 * c->hit_cap, (int64_t)used[1] + 1024); continue; }
+    if (errflag == 5) { c->srun_cap = std::max<int64_t>(2 * c->srun_cap, (int64_t)used[2] + 1024); continue; }
     return fail(NSG_ERR_CAPACITY, errflag == 1 ? "too many overflow rays" : "ray hit capacity exceeded");
   }
   // volume: A * sum of interval lengths over the ray sets / number of ray sets
@@ -455,6 +520,11 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
   }
   c->volume = flag_sum ? g.A * vsum / flag_sum : 0.0;
   if (volume) *volume = c->volume;
+  if (do_status) {
+    int rc = build_free_runs(c);
+    if (rc) return rc;
+  }
+  c->status_dense = false;
   c->have_status = do_status;
   c->have_bits = do_mc;
   c->n_vert = c->n_tri = 0;
@@ -493,31 +563,33 @@ int nsg_cavities(nsg_ctx* c, double cav_vol, int* ncav_out) {
   if (!c || !c->have_status) return fail(NSG_ERR_STATE, "cavity detection needs the status map");
   CK(cudaSetDevice(c->device));
   const NsGrid& g = c->grid;
-  const int64_t tot = g.nx * g.ny * g.nz;
-  CK(c->labels.ensure(tot * sizeof(int32_t)));
-  CK(c->is_root.ensure(tot));
-  stage_begin(c, kStageCavity);
-  c->launches += 3;
-  CK(nsg::cc_label(c->status.as<int32_t>(), c->labels.as<int32_t>(), c->is_root.as<uint8_t>(), g.nx, g.ny, g.nz,
-                   c->stream));
-  CK(c->nroots_d.ensure(sizeof(int32_t)));
-  size_t tb = 0;
-  CK(nsg::cc_select_roots(c->is_root.as<uint8_t>(), tot, nullptr, nullptr, nullptr, &tb, c->stream));
-  CK(c->temp.ensure(tb));
-  tb = c->temp.cap;
-  // the root list is at most the number of free nodes; size it lazily from the flag count
-  CK(c->roots.ensure(tot * sizeof(int32_t)));
-  int64_t max_roots = (int64_t)(c->roots.cap / sizeof(int32_t));
-  CK(nsg::cc_select_roots(c->is_root.as<uint8_t>(), tot, c->roots.as<int32_t>(), c->nroots_d.as<int32_t>(),
-                          c->temp.p, &tb, c->stream));
-  int32_t nroots = 0;
-  CK(cudaMemcpyAsync(&nroots, c->nroots_d.p, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
-  if (nroots > max_roots) return fail(NSG_ERR_CAPACITY, "too many free regions");
+  const int64_t nr = c->n_fruns;
   c->cav_size.clear();
   c->cav_filled.clear();
+  stage_begin(c, kStageCavity);
+  CK(c->labels.ensure(std::max<int64_t>(nr, 1) * sizeof(int32_t)));
+  CK(c->is_root.ensure(std::max<int64_t>(nr, 1)));
+  CK(c->roots.ensure(std::max<int64_t>(nr, 1) * sizeof(int32_t)));
+  CK(c->nroots_d.ensure(sizeof(int32_t)));
+  nsg::RunArgs A = run_args(c);
+  c->launches += 3;
+  CK(nsg::run_label(A, c->is_root.as<uint8_t>(), c->stream));
+  int32_t nroots = 0;
+  if (nr > 0) {
+    size_t tb = 0;
+    CK(nsg::run_select_roots(c->is_root.as<uint8_t>(), nr, nullptr, nullptr, nullptr, &tb, c->stream));
+    CK(c->temp.ensure(tb));
+    tb = c->temp.cap;
+    CK(nsg::run_select_roots(c->is_root.as<uint8_t>(), nr, c->roots.as<int32_t>(), c->nroots_d.as<int32_t>(),
+                             c->temp.p, &tb, c->stream));
+    CK(cudaMemcpyAsync(&nroots, c->nroots_d.p, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  }
   if (nroots == 0) {
     c->ncav = 0;
+    int rc = materialize_status(c, nullptr);
+    if (rc) return rc;
+    stage_end(c, kStageCavity);
     if (ncav_out) *ncav_out = 0;
     return NSG_OK;
   }
@@ -525,8 +597,8 @@ int nsg_cavities(nsg_ctx* c, double cav_vol, int* ncav_out) {
   CK(c->cc_desc.ensure(nroots * sizeof(unsigned int)));
   CK(cudaMemsetAsync(c->cc_count.p, 0, nroots * sizeof(unsigned long long), c->stream));
   CK(cudaMemsetAsync(c->cc_desc.p, 0xff, nroots * sizeof(unsigned int), c->stream));
-  LAUNCH(nsg::cc_stats(c->labels.as<int32_t>(), c->roots.as<int32_t>(), nroots, c->cc_count.as<unsigned long long>(),
-                   c->cc_desc.as<unsigned int>(), g.nx, g.ny, g.nz, c->stream));
+  LAUNCH(nsg::run_stats(A, c->roots.as<int32_t>(), nroots, c->cc_count.as<unsigned long long>(),
+                        c->cc_desc.as<unsigned int>(), c->stream));
   std::vector<unsigned long long> cnt(nroots);
   std::vector<unsigned int> desc(nroots);
   CK(cudaMemcpyAsync(cnt.data(), c->cc_count.p, nroots * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
@@ -554,9 +626,10 @@ int nsg_cavities(nsg_ctx* c, double cav_vol, int* ncav_out) {
   CK(c->cc_fill_of.ensure(nroots));
   CK(cudaMemcpyAsync(c->cc_label_of.p, label_of.data(), nroots * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->cc_fill_of.p, fill_of.data(), nroots, cudaMemcpyHostToDevice, c->stream));
-  LAUNCH(nsg::cc_label_fill(c->status.as<int32_t>(), c->labels.as<int32_t>(), c->cc_label_of.as<int32_t>(),
-                        c->cc_fill_of.as<uint8_t>(), c->have_bits ? c->bits.as<uint32_t>() : nullptr, nwords_of(g),
-                        g.nx, g.ny, g.nz, c->stream));
+  if (c->have_bits)
+    LAUNCH(nsg::run_fill(A, c->cc_fill_of.as<uint8_t>(), c->bits.as<uint32_t>(), nwords_of(g), c->stream));
+  int rc = materialize_status(c, c->cc_label_of.as<int32_t>());
+  if (rc) return rc;
   stage_end(c, kStageCavity);
   CK(cudaStreamSynchronize(c->stream));
   if (ncav_out) *ncav_out = c->ncav;
@@ -683,6 +756,11 @@ int nsg_triangulate(nsg_ctx* c, double* area_out, int64_t* nverts, int64_t* ntri
 
 int nsg_download_status(nsg_ctx* c, int32_t* dst) {
   if (!c || !dst || !c->have_status) return NSG_ERR_STATE;
+  CK(cudaSetDevice(c->device));
+  if (!c->status_dense) {
+    int rc = materialize_status(c, nullptr);
+    if (rc) return rc;
+  }
   const NsGrid& g = c->grid;
   CK(cudaMemcpyAsync(dst, c->status.p, g.nx * g.ny * g.nz * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));

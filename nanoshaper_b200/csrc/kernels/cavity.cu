@@ -1,4 +1,4 @@
-// Cavity detection and conditional filling on the status map.
+// Status map materialisation, cavity detection and conditional cavity filling.
 //
 // The reference labels the 6-connected regions of STATUS_POINT_TEMPORARY_OUT nodes one at a time
 // with a scanline flood fill seeded at the first remaining node of a scan whose z direction
@@ -8,10 +8,13 @@
 // times side^3 does not exceed the threshold get the insideness bits of the 8 corners of each of
 // their nodes cleared (fillCavities :2355-2484).
 //
-// On the GPU all regions are found at once with a lock-free union-find whose roots are the
-// smallest node index of each region (= the region's first node in ascending scan order).  The
-// region's first node in descending scan order is reduced with atomicMin.  The host then replays
-// the alternating seed selection over these two keys, which reproduces the reference labels.
+// Here the status map is kept as runs: the status rays give, per x-row (j, k), the runs of
+// inside nodes; their complement are the runs of free nodes.  Regions are found with a lock-free
+// union-find over free runs (two runs are joined when they overlap in x in rows (j+1, k) or
+// (j, k+1)), with each region's root being its smallest run index = its first node in ascending
+// scan order.  Its first node in descending-z scan order is reduced per region.  The host
+// replays the alternating seed selection over these two keys (nsg_cavity_order), which
+// reproduces the reference labels; the dense status map is then written once, row by row.
 #include <cub/cub.cuh>
 
 #include "cavity.h"
@@ -24,7 +27,7 @@ __device__ __forceinline__ int32_t find_root(int32_t* L, int32_t v) {
   int32_t p = L[v];
   while (p != v) {
     int32_t gp = L[p];
-    if (gp != p) L[v] = gp;  // path halving; benign race
+    if (gp != p) L[v] = gp;  // path halving; only ever points a node to an ancestor
     v = p;
     p = gp;
   }
@@ -43,52 +46,76 @@ __device__ __forceinline__ void unite(int32_t* L, int32_t a, int32_t b) {
   }
 }
 
-__global__ void k_cc_init(const int32_t* __restrict__ status, int32_t* L, int64_t tot) {
-  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < tot; v += (int64_t)gridDim.x * blockDim.x)
-    L[v] = (status[v] == NS_STATUS_TEMPORARY_OUT) ? (int32_t)v : -1;
-}
-
-// Hooks each free node to its +x, +y, +z free neighbours.
-__global__ void k_cc_hook(const int32_t* __restrict__ status, int32_t* L, int64_t nx, int64_t ny, int64_t nz) {
-  int64_t tot = nx * ny * nz;
-  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < tot; v += (int64_t)gridDim.x * blockDim.x) {
-    if (status[v] != NS_STATUS_TEMPORARY_OUT) continue;
-    int64_t i = v % nx;
-    int64_t r = v / nx;
-    int64_t j = r % ny;
-    int64_t k = r / ny;
-    if (i + 1 < nx && status[v + 1] == NS_STATUS_TEMPORARY_OUT) unite(L, (int32_t)v, (int32_t)(v + 1));
-    if (j + 1 < ny && status[v + nx] == NS_STATUS_TEMPORARY_OUT) unite(L, (int32_t)v, (int32_t)(v + nx));
-    if (k + 1 < nz && status[v + nx * ny] == NS_STATUS_TEMPORARY_OUT) unite(L, (int32_t)v, (int32_t)(v + nx * ny));
+// Free runs of a status row: the gaps between its (sorted) inside runs.
+__global__ void k_free_runs(RunArgs A, int emit) {
+  const int64_t NX = A.nx;
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < A.nrows; r += (int64_t)gridDim.x * blockDim.x) {
+    int cnt = A.srun_cnt[r];
+    const int2* in = A.sruns + (cnt ? A.srun_off[r] : 0);
+    int64_t prev = -1;
+    int nf = 0;
+    int64_t o = emit ? A.fr_off[r] : 0;
+    for (int q = 0; q <= cnt; q++) {
+      int64_t a = (q < cnt) ? in[q].x : NX;
+      if (a > prev + 1) {
+        if (emit) {
+          A.fruns[o + nf] = make_int2((int)(prev + 1), (int)(a - 1));
+          A.frow[o + nf] = (int32_t)r;
+        }
+        nf++;
+      }
+      if (q < cnt && in[q].y > prev) prev = in[q].y;
+    }
+    if (!emit) A.fr_cnt[r] = nf;
   }
 }
 
-// Final root of every node.  The walk does not shorten paths: a halving write issued by one
+__global__ void k_run_init(int32_t* L, int64_t n) {
+  for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < n; u += (int64_t)gridDim.x * blockDim.x)
+    L[u] = (int32_t)u;
+}
+
+__device__ __forceinline__ void hook_row(const RunArgs& A, int32_t u, int2 ru, int64_t s) {
+  int64_t lo = A.fr_off[s], hi = A.fr_off[s + 1];
+  // first run of row s ending at or after ru.x
+  while (lo < hi) {
+    int64_t mid = (lo + hi) >> 1;
+    if (A.fruns[mid].y < ru.x) lo = mid + 1;
+    else hi = mid;
+  }
+  for (int64_t v = lo; v < A.fr_off[s + 1] && A.fruns[v].x <= ru.y; v++) unite(A.L, u, (int32_t)v);
+}
+
+__global__ void k_run_hook(RunArgs A) {
+  for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < A.nruns; u += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = A.frow[u];
+    int64_t j = r % A.ny, k = r / A.ny;
+    int2 ru = A.fruns[u];
+    if (j + 1 < A.ny) hook_row(A, (int32_t)u, ru, r + 1);
+    if (k + 1 < A.nz) hook_row(A, (int32_t)u, ru, r + A.ny);
+  }
+}
+
+// Final root of every run.  The walk does not shorten paths: a halving write issued by one
 // thread could otherwise overwrite a label another thread has already set to its root.
-__global__ void k_cc_compress(int32_t* L, int64_t tot, uint8_t* is_root) {
-  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < tot; v += (int64_t)gridDim.x * blockDim.x) {
-    int32_t l = L[v];
-    if (l < 0) { is_root[v] = 0; continue; }
-    int32_t r = l;
+__global__ void k_run_compress(int32_t* L, int64_t n, uint8_t* is_root) {
+  for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < n; u += (int64_t)gridDim.x * blockDim.x) {
+    int32_t r = L[u];
     for (int32_t q = L[r]; q != r; q = L[r]) r = q;
-    L[v] = r;
-    is_root[v] = (r == v) ? 1 : 0;
+    L[u] = r;
+    is_root[u] = (r == u) ? 1 : 0;
   }
 }
 
-// Per node: component index by binary search in the sorted root list; size and descending-scan
-// key reductions.  L[v] is replaced by the component index.  Lanes of a warp that fall into the
-// same component (the common case: the outer region covers most of the grid) are combined
-// before the atomics, so the hot counters see one update per warp instead of one per node.
-__global__ void k_cc_stats(int32_t* L, const int32_t* __restrict__ roots, int32_t nroots, unsigned long long* count,
-                           unsigned int* desc_key, int64_t nx, int64_t ny, int64_t nz) {
-  int64_t tot = nx * ny * nz;
-  int64_t plane = nx * ny;
-  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < tot; v += (int64_t)gridDim.x * blockDim.x) {
+// Region index of every run (binary search in the sorted roots), region node counts and first
+// node in descending-z scan order.  Lanes of a warp in the same region are combined before the
+// atomics.
+__global__ void k_run_stats(RunArgs A, const int32_t* __restrict__ roots, int32_t nroots, unsigned long long* count,
+                            unsigned int* desc_key) {
+  const int64_t plane = A.nx * A.ny;
+  for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < A.nruns; u += (int64_t)gridDim.x * blockDim.x) {
     unsigned act = __activemask();
-    int32_t l = L[v];
-    unsigned has = __ballot_sync(act, l >= 0);
-    if (l < 0) continue;
+    int32_t l = A.L[u];
     int32_t lo = 0, hi = nroots - 1;
     if (roots[0] != l) {
       while (lo < hi) {
@@ -97,74 +124,108 @@ __global__ void k_cc_stats(int32_t* L, const int32_t* __restrict__ roots, int32_
         else hi = mid;
       }
     }
-    L[v] = lo;
-    int64_t k = v / plane;
-    unsigned key = (unsigned)((nz - 1 - k) * plane + (v - k * plane));
-    unsigned grp = __match_any_sync(has, lo);
+    A.L[u] = lo;
+    int64_t r = A.frow[u];
+    int64_t j = r % A.ny, k = r / A.ny;
+    int2 ru = A.fruns[u];
+    unsigned key = (unsigned)((A.nz - 1 - k) * plane + j * A.nx + ru.x);
+    unsigned len = (unsigned)(ru.y - ru.x + 1);
+    unsigned grp = __match_any_sync(act, lo);
     unsigned kmin = __reduce_min_sync(grp, key);
+    unsigned sum = __reduce_add_sync(grp, len);
     if ((int)(threadIdx.x & 31) == __ffs(grp) - 1) {
-      atomicAdd(count + lo, (unsigned long long)__popc(grp));
+      atomicAdd(count + lo, (unsigned long long)sum);
       atomicMin(desc_key + lo, kmin);
     }
   }
 }
 
-// Writes region labels into the status map and clears the 8 cube-corner insideness bits of the
-// nodes of filled cavities.
-__global__ void k_cc_label_fill(int32_t* status, const int32_t* __restrict__ L, const int32_t* __restrict__ label_of,
-                                const uint8_t* __restrict__ fill_of, uint32_t* bits, int64_t nwords, int64_t nx,
-                                int64_t ny, int64_t nz) {
-  int64_t tot = nx * ny * nz;
-  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < tot; v += (int64_t)gridDim.x * blockDim.x) {
-    int32_t c = L[v];
-    if (c < 0) continue;
-    int32_t lab = label_of[c];
-    status[v] = lab;
-    if (bits && fill_of[c]) {
-      for (int dk = 0; dk < 2; dk++)
-        for (int dj = 0; dj < 2; dj++)
-          for (int di = 0; di < 2; di++) {
-            int64_t f = v + di + dj * nx + dk * nx * ny;
-            if ((f >> 5) < nwords) atomicAnd(bits + (f >> 5), ~(1u << (f & 31)));
-          }
+// Clears the 8 cube-corner insideness bits of every node of the filled cavities: for a run
+// x0..x1 of row (j, k), bits x0..x1+1 of the rows (j, k), (j+1, k), (j, k+1), (j+1, k+1).
+__global__ void k_run_fill(RunArgs A, const uint8_t* __restrict__ fill_of, uint32_t* bits, int64_t nwords) {
+  for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < A.nruns; u += (int64_t)gridDim.x * blockDim.x) {
+    int32_t c = A.L[u];
+    if (!fill_of[c]) continue;
+    int64_t r = A.frow[u];
+    int2 ru = A.fruns[u];
+    for (int dk = 0; dk < 2; dk++)
+      for (int dj = 0; dj < 2; dj++) {
+        int64_t base = (r + dj + dk * A.ny) * A.nx;
+        int64_t f0 = base + ru.x, f1 = base + ru.y + 1;
+        if (f0 < 0) f0 = 0;
+        if (f1 > nwords * 32 - 1) f1 = nwords * 32 - 1;
+        for (int64_t w = f0 >> 5; w <= (f1 >> 5); w++) {
+          int64_t wl = w << 5;
+          int s = (int)(f0 > wl ? f0 - wl : 0);
+          int e = (int)(f1 < wl + 31 ? f1 - wl : 31);
+          uint32_t mask = (e - s == 31) ? 0xffffffffu : (((1u << (e - s + 1)) - 1u) << s);
+          atomicAnd(bits + w, ~mask);
+        }
+      }
+  }
+}
+
+// Dense status map, one warp per x-row: free runs get their region label (or TEMPORARY_OUT
+// before cavity detection), all other nodes STATUS_POINT_INSIDE.
+__global__ void k_status_write(RunArgs A, const int32_t* __restrict__ label_of, int32_t* status) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t r = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); r < A.nrows; r += warps) {
+    int64_t b = A.fr_off[r], e = A.fr_off[r + 1];
+    int32_t* row = status + r * A.nx;
+    int64_t p = b;
+    for (int64_t i = lane; i < A.nx; i += 32) {
+      while (p < e && A.fruns[p].y < i) p++;
+      int32_t v = NS_STATUS_INSIDE;
+      if (p < e && A.fruns[p].x <= i) v = label_of ? label_of[A.L[p]] : NS_STATUS_TEMPORARY_OUT;
+      row[i] = v;
     }
   }
 }
 
-int grid_for(int64_t tot) {
-  int64_t b = (tot + 255) / 256;
-  return (int)(b < 148 * 64 ? (b < 1 ? 1 : b) : 148 * 64);
+int grid_for(int64_t n, int threads = 256) {
+  int64_t b = (n + threads - 1) / threads;
+  return (int)(b < 148 * 32 ? (b < 1 ? 1 : b) : 148 * 32);
 }
 
 }  // namespace
 
-cudaError_t cc_label(const int32_t* status, int32_t* L, uint8_t* is_root, int64_t nx, int64_t ny, int64_t nz,
-                     cudaStream_t s) {
-  int64_t tot = nx * ny * nz;
-  k_cc_init<<<grid_for(tot), 256, 0, s>>>(status, L, tot);
-  k_cc_hook<<<grid_for(tot), 256, 0, s>>>(status, L, nx, ny, nz);
-  k_cc_compress<<<grid_for(tot), 256, 0, s>>>(L, tot, is_root);
+cudaError_t launch_free_runs(const RunArgs& A, int emit, cudaStream_t s) {
+  if (A.nrows <= 0) return cudaSuccess;
+  k_free_runs<<<grid_for(A.nrows), 256, 0, s>>>(A, emit);
   return cudaGetLastError();
 }
 
-cudaError_t cc_select_roots(const uint8_t* is_root, int64_t tot, int32_t* roots, int32_t* nroots, void* temp,
-                            size_t* temp_bytes, cudaStream_t s) {
+cudaError_t run_label(const RunArgs& A, uint8_t* is_root, cudaStream_t s) {
+  if (A.nruns <= 0) return cudaSuccess;
+  k_run_init<<<grid_for(A.nruns), 256, 0, s>>>(A.L, A.nruns);
+  k_run_hook<<<grid_for(A.nruns), 256, 0, s>>>(A);
+  k_run_compress<<<grid_for(A.nruns), 256, 0, s>>>(A.L, A.nruns, is_root);
+  return cudaGetLastError();
+}
+
+cudaError_t run_select_roots(const uint8_t* is_root, int64_t n, int32_t* roots, int32_t* nroots, void* temp,
+                             size_t* temp_bytes, cudaStream_t s) {
   cub::CountingInputIterator<int32_t> it(0);
-  return cub::DeviceSelect::Flagged(temp, *temp_bytes, it, is_root, roots, nroots, tot, s);
+  return cub::DeviceSelect::Flagged(temp, *temp_bytes, it, is_root, roots, nroots, n, s);
 }
 
-cudaError_t cc_stats(int32_t* L, const int32_t* roots, int32_t nroots, unsigned long long* count, unsigned int* desc_key,
-                     int64_t nx, int64_t ny, int64_t nz, cudaStream_t s) {
-  int64_t tot = nx * ny * nz;
-  if (nroots <= 0) return cudaSuccess;
-  k_cc_stats<<<grid_for(tot), 256, 0, s>>>(L, roots, nroots, count, desc_key, nx, ny, nz);
+cudaError_t run_stats(const RunArgs& A, const int32_t* roots, int32_t nroots, unsigned long long* count,
+                      unsigned int* desc_key, cudaStream_t s) {
+  if (A.nruns <= 0 || nroots <= 0) return cudaSuccess;
+  k_run_stats<<<grid_for(A.nruns), 256, 0, s>>>(A, roots, nroots, count, desc_key);
   return cudaGetLastError();
 }
 
-cudaError_t cc_label_fill(int32_t* status, const int32_t* L, const int32_t* label_of, const uint8_t* fill_of,
-                          uint32_t* bits, int64_t nwords, int64_t nx, int64_t ny, int64_t nz, cudaStream_t s) {
-  int64_t tot = nx * ny * nz;
-  k_cc_label_fill<<<grid_for(tot), 256, 0, s>>>(status, L, label_of, fill_of, bits, nwords, nx, ny, nz);
+cudaError_t run_fill(const RunArgs& A, const uint8_t* fill_of, uint32_t* bits, int64_t nwords, cudaStream_t s) {
+  if (A.nruns <= 0 || !bits) return cudaSuccess;
+  k_run_fill<<<grid_for(A.nruns), 256, 0, s>>>(A, fill_of, bits, nwords);
+  return cudaGetLastError();
+}
+
+cudaError_t status_write(const RunArgs& A, const int32_t* label_of, int32_t* status, cudaStream_t s) {
+  if (A.nrows <= 0) return cudaSuccess;
+  k_status_write<<<grid_for(A.nrows * 32), 256, 0, s>>>(A, label_of, status);
   return cudaGetLastError();
 }
 

@@ -1,4 +1,4 @@
-// Cavity kernels (cavity.cu).
+// Status map, cavity detection and cavity filling kernels (cavity.cu).
 #pragma once
 #include <cuda_runtime.h>
 #include <stddef.h>
@@ -8,18 +8,33 @@
 
 namespace nsg {
 
-// Union-find labelling of the TEMPORARY_OUT nodes; L[v] = smallest node index of v's region
-// (-1 for other nodes), is_root[v] = 1 for region roots.
-cudaError_t cc_label(const int32_t* status, int32_t* L, uint8_t* is_root, int64_t nx, int64_t ny, int64_t nz,
-                     cudaStream_t s);
-// Sorted list of region roots; pass roots == nullptr-free temp == nullptr to query temp_bytes.
-cudaError_t cc_select_roots(const uint8_t* is_root, int64_t tot, int32_t* roots, int32_t* nroots, void* temp,
-                            size_t* temp_bytes, cudaStream_t s);
-// Region sizes and descending-scan keys; replaces L[v] by the region index.
-cudaError_t cc_stats(int32_t* L, const int32_t* roots, int32_t nroots, unsigned long long* count, unsigned int* desc_key,
-                     int64_t nx, int64_t ny, int64_t nz, cudaStream_t s);
-// Final labels into the status map and cavity filling on the insideness bits.
-cudaError_t cc_label_fill(int32_t* status, const int32_t* L, const int32_t* label_of, const uint8_t* fill_of,
-                          uint32_t* bits, int64_t nwords, int64_t nx, int64_t ny, int64_t nz, cudaStream_t s);
+// Status map in run form and the free-run union-find state.
+struct RunArgs {
+  int64_t nx, ny, nz;
+  int64_t nrows;              // ny * nz status rows, row = k*ny + j
+  const int2* sruns;          // inside runs (first, last node) per row
+  const int64_t* srun_off;
+  const int32_t* srun_cnt;
+  int32_t* fr_cnt;            // free runs per row
+  const int64_t* fr_off;      // nrows + 1 offsets
+  int2* fruns;                // free runs (first, last node), row-major
+  int32_t* frow;              // row of every free run
+  int64_t nruns;
+  int32_t* L;                 // union-find parents, then region index per run
+};
+
+cudaError_t launch_free_runs(const RunArgs& A, int emit, cudaStream_t s);
+// Union-find over free runs; is_root[u] = 1 for region roots (smallest run of each region).
+cudaError_t run_label(const RunArgs& A, uint8_t* is_root, cudaStream_t s);
+// Sorted list of region roots; pass temp == nullptr to query temp_bytes.
+cudaError_t run_select_roots(const uint8_t* is_root, int64_t n, int32_t* roots, int32_t* nroots, void* temp,
+                             size_t* temp_bytes, cudaStream_t s);
+// Region sizes (nodes) and first nodes in descending-z scan order; L becomes the region index.
+cudaError_t run_stats(const RunArgs& A, const int32_t* roots, int32_t nroots, unsigned long long* count,
+                      unsigned int* desc_key, cudaStream_t s);
+// Cavity filling on the insideness bits.
+cudaError_t run_fill(const RunArgs& A, const uint8_t* fill_of, uint32_t* bits, int64_t nwords, cudaStream_t s);
+// Dense status map from the runs; label_of == nullptr writes TEMPORARY_OUT for free nodes.
+cudaError_t status_write(const RunArgs& A, const int32_t* label_of, int32_t* status, cudaStream_t s);
 
 }  // namespace nsg

@@ -150,7 +150,20 @@ __device__ __forceinline__ int own_midpoints(const MCArgs& A, int64_t i, int64_t
   return mm;
 }
 
-// One warp per cube row (j, k); pass 0 counts, pass 1 emits active cubes and midpoint vertices.
+// 32 consecutive bits of the flat bit grid starting at bit f (missing words read as outside).
+__device__ __forceinline__ uint32_t bits32(const uint32_t* __restrict__ bits, int64_t nwords, int64_t f) {
+  int64_t w = f >> 5;
+  int s = (int)(f & 31);
+  uint32_t lo = w < nwords ? bits[w] : 0xffffffffu;
+  if (s == 0) return lo;
+  uint32_t hi = (w + 1) < nwords ? bits[w + 1] : 0xffffffffu;
+  return __funnelshift_r(lo, hi, s);
+}
+
+// One warp per cube row (j, k); every lane classifies 32 consecutive cubes at once from the four
+// bit rows the cubes touch (corner inside = bit 0): a cube is active unless its 8 corners agree.
+// Only active cubes look up vertices.  Pass 0 counts, pass 1 emits active cubes (in i order) and
+// their midpoint vertices.
 __global__ void k_mc_rows(MCArgs A, int emit) {
   const GridDev& g = A.g;
   const int64_t NX = g.n[0], NY = g.n[1];
@@ -159,50 +172,77 @@ __global__ void k_mc_rows(MCArgs A, int emit) {
   for (int64_t row = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); row < A.nrows; row += warps) {
     int64_t j = 1 + row % (NY - 2);
     int64_t k = 1 + row / (NY - 2);
+    const int64_t b00 = (k * NY + j) * NX, b10 = b00 + NX, b01 = b00 + NX * NY, b11 = b01 + NX;
     int64_t act_run = 0, mid_run = 0;
     int64_t act_base = emit ? A.row_act_off[row] : 0;
     int64_t mid_base = emit ? A.row_mid_off[row] : 0;
-    for (int64_t i0 = 1; i0 < NX - 1; i0 += 32) {
-      int64_t i = i0 + lane;
-      int act = 0, mm = 0, c = 0;
-      if (i < NX - 1) {
-        c = cube_case(A, i, j, k);
-        int em = c_emask[c];
-        if (em) {
-          act = 1;
-          mm = own_midpoints(A, i, j, k, em);
-        }
+    for (int64_t i0 = 1; i0 < NX - 1; i0 += 32 * 32) {
+      int64_t ic = i0 + 32 * lane;
+      uint32_t act = 0;
+      uint32_t c[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      if (ic < NX - 1) {
+        int64_t nvalid = NX - 1 - ic;
+        uint32_t vm = nvalid >= 32 ? 0xffffffffu : ((1u << nvalid) - 1u);
+        c[0] = ~bits32(A.bits, A.nwords, b00 + ic);
+        c[1] = ~bits32(A.bits, A.nwords, b00 + ic + 1);
+        c[2] = ~bits32(A.bits, A.nwords, b10 + ic + 1);
+        c[3] = ~bits32(A.bits, A.nwords, b10 + ic);
+        c[4] = ~bits32(A.bits, A.nwords, b01 + ic);
+        c[5] = ~bits32(A.bits, A.nwords, b01 + ic + 1);
+        c[6] = ~bits32(A.bits, A.nwords, b11 + ic + 1);
+        c[7] = ~bits32(A.bits, A.nwords, b11 + ic);
+        uint32_t d = 0;
+#pragma unroll
+        for (int q = 1; q < 8; q++) d |= c[0] ^ c[q];
+        act = d & vm;
       }
-      int nm = __popc(mm);
-      int ia = act, im = nm;
+      int na = __popc(act);
+      int nm = 0;
+      for (uint32_t m = act; m; m &= m - 1) {
+        int b = __ffs(m) - 1;
+        int cs = 0;
+#pragma unroll
+        for (int q = 0; q < 8; q++) cs |= ((c[q] >> b) & 1u) << q;
+        nm += __popc(own_midpoints(A, ic + b, j, k, c_emask[cs]));
+      }
+      int ia = na, im = nm;
       for (int o = 1; o < 32; o <<= 1) {
         int va = __shfl_up_sync(0xffffffffu, ia, o);
-        int vm = __shfl_up_sync(0xffffffffu, im, o);
-        if (lane >= o) { ia += va; im += vm; }
+        int vm2 = __shfl_up_sync(0xffffffffu, im, o);
+        if (lane >= o) { ia += va; im += vm2; }
       }
       int ta = __shfl_sync(0xffffffffu, ia, 31), tm = __shfl_sync(0xffffffffu, im, 31);
-      if (emit && act) {
-        int64_t slot = act_base + act_run + ia - act;
-        int64_t mbase = mid_base + mid_run + im - nm;
-        A.act_rec[slot] = make_int4((int)i, (int)j, (int)k, c | (mm << 8));
-        A.act_mid[slot] = (int32_t)(A.n_analytic + mbase);
-        int64_t v = A.n_analytic + mbase;
-        if (mm & 1) {
-          A.vpos[3 * v] = gcoord(g, 0, i + 1) - g.hside; A.vpos[3 * v + 1] = gcoord(g, 1, j);
-          A.vpos[3 * v + 2] = gcoord(g, 2, k + 1) - g.hside;
-          A.vkey[v] = make_int4((int)(i + 1), (int)j, (int)(k + 1), NS_Y_DIR);
-          v++;
-        }
-        if (mm & 2) {
-          A.vpos[3 * v] = gcoord(g, 0, i); A.vpos[3 * v + 1] = gcoord(g, 1, j + 1) - g.hside;
-          A.vpos[3 * v + 2] = gcoord(g, 2, k + 1) - g.hside;
-          A.vkey[v] = make_int4((int)i, (int)(j + 1), (int)(k + 1), NS_X_DIR);
-          v++;
-        }
-        if (mm & 4) {
-          A.vpos[3 * v] = gcoord(g, 0, i + 1) - g.hside; A.vpos[3 * v + 1] = gcoord(g, 1, j + 1) - g.hside;
-          A.vpos[3 * v + 2] = gcoord(g, 2, k);
-          A.vkey[v] = make_int4((int)(i + 1), (int)(j + 1), (int)k, NS_Z_DIR);
+      if (emit && na) {
+        int64_t slot = act_base + act_run + ia - na;
+        int64_t v = A.n_analytic + mid_base + mid_run + im - nm;
+        for (uint32_t m = act; m; m &= m - 1) {
+          int b = __ffs(m) - 1;
+          int64_t i = ic + b;
+          int cs = 0;
+#pragma unroll
+          for (int q = 0; q < 8; q++) cs |= ((c[q] >> b) & 1u) << q;
+          int mm = own_midpoints(A, i, j, k, c_emask[cs]);
+          A.act_rec[slot] = make_int4((int)i, (int)j, (int)k, cs | (mm << 8));
+          A.act_mid[slot] = (int32_t)v;
+          slot++;
+          if (mm & 1) {
+            A.vpos[3 * v] = gcoord(g, 0, i + 1) - g.hside; A.vpos[3 * v + 1] = gcoord(g, 1, j);
+            A.vpos[3 * v + 2] = gcoord(g, 2, k + 1) - g.hside;
+            A.vkey[v] = make_int4((int)(i + 1), (int)j, (int)(k + 1), NS_Y_DIR);
+            v++;
+          }
+          if (mm & 2) {
+            A.vpos[3 * v] = gcoord(g, 0, i); A.vpos[3 * v + 1] = gcoord(g, 1, j + 1) - g.hside;
+            A.vpos[3 * v + 2] = gcoord(g, 2, k + 1) - g.hside;
+            A.vkey[v] = make_int4((int)i, (int)(j + 1), (int)(k + 1), NS_X_DIR);
+            v++;
+          }
+          if (mm & 4) {
+            A.vpos[3 * v] = gcoord(g, 0, i + 1) - g.hside; A.vpos[3 * v + 1] = gcoord(g, 1, j + 1) - g.hside;
+            A.vpos[3 * v + 2] = gcoord(g, 2, k);
+            A.vkey[v] = make_int4((int)(i + 1), (int)(j + 1), (int)k, NS_Z_DIR);
+            v++;
+          }
         }
       }
       act_run += ta;

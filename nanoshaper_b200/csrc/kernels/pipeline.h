@@ -59,7 +59,12 @@ __host__ __device__ inline RaySet make_ray_set(int set, const GridDev& g) {
 
 // Outputs of one trace launch.
 struct TraceOut {
-  int32_t* status;         // set 0: full status map rows
+  // set 0: runs of inside nodes per status row (row = k*ny + j), the status map in run form
+  int2* sruns;
+  int64_t srun_cap;
+  unsigned long long* srun_cursor;
+  int64_t* srun_off;
+  int32_t* srun_cnt;
   uint32_t* bits;          // sets 1..3: insideness bits (1 = outside), cleared with atomicAnd
   double* vol_ray;         // per ray interval length sum, indexed by n*nb+m
   // pair store (sets 1..3): lim1/lim2 of vertex-producing pairs

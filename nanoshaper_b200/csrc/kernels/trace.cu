@@ -138,6 +138,43 @@ __device__ __forceinline__ int make_pairs(double* col, int stride, int nh, doubl
   return np;
 }
 
+// Nodes of a status row inside one interval: the reference loops over the clamped rintp range
+// [i1, i2] and marks the nodes with lim1 <= x <= lim2 (src/Surface.cpp:5427-5552); that set is
+// the contiguous range returned here (ia > ib when empty).
+__device__ __forceinline__ void status_node_range(const GridDev& g, double lim1, double lim2, int64_t* ia, int64_t* ib) {
+  const int64_t NX = g.n[0];
+  int64_t i1 = (int64_t)rintp((lim1 - g.mn[0]) * g.scale);
+  int64_t i2 = (int64_t)rintp((lim2 - g.mn[0]) * g.scale);
+  i1 = i1 < 0 ? 0 : (i1 >= NX ? NX - 1 : i1);
+  i2 = i2 < 0 ? 0 : (i2 >= NX ? NX - 1 : i2);
+  int64_t a = i1, b = i2;
+  while (a <= b && gcoord(g, 0, a) < lim1) a++;
+  while (b >= a && gcoord(g, 0, b) > lim2) b--;
+  *ia = a;
+  *ib = b;
+}
+
+// Warp-aggregated append of this lane's `cnt` records to a shared store; returns the lane's first
+// slot, or -1 when the store is full (the error flag is then set to `code`).
+__device__ __forceinline__ int64_t warp_append(unsigned long long* cursor, int64_t cap, int cnt, int32_t* error_flag,
+                                               int code) {
+  const int lane = threadIdx.x & 31;
+  int incl = cnt;
+  for (int o = 1; o < 32; o <<= 1) {
+    int v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  int total = __shfl_sync(0xffffffffu, incl, 31);
+  unsigned long long base = 0;
+  if (lane == 31 && total > 0) base = atomicAdd(cursor, (unsigned long long)total);
+  base = __shfl_sync(0xffffffffu, base, 31);
+  if ((int64_t)base + total > cap) {
+    if (lane == 0 && total > 0) atomicExch(error_flag, code);
+    return -1;
+  }
+  return (int64_t)base + incl - cnt;
+}
+
 __device__ __forceinline__ void clear_bits_range(uint32_t* bits, int64_t nwords, int64_t f0, int64_t f1) {
   // clears bits f0..f1 inclusive of the flat bit grid (bit = 0 means inside)
   if (f1 < f0) return;
@@ -255,41 +292,36 @@ __global__ void __launch_bounds__(kTraceThreads) k_trace(TraceCtx C, const int64
   __syncwarp();
   const int64_t NX = g.n[0], NY = g.n[1];
   if (!mc) {
-    // status rows: ray (m = j, n = k) owns row (., j, k); write the whole row
-    for (int r = 0; r < 32; r++) {
-      int np_r = __shfl_sync(0xffffffffu, np, r);
-      int skip = __shfl_sync(0xffffffffu, (int)(!valid || ovf), r);
-      if (skip) continue;
-      const double* cr = s_hit + warp * 32 + r;
-      int64_t j = tm * kTileM + r;
-      int32_t* row = C.out.status + (n * NY + j) * NX;
-      int p = 0;
-      for (int64_t i = lane; i < NX; i += 32) {
-        double x = gcoord(g, 0, i);
-        while (p < np_r && cr[(2 * p + 1) * kThreads] < x) p++;
-        bool inside = p < np_r && cr[(2 * p) * kThreads] <= x;
-        row[i] = inside ? NS_STATUS_INSIDE : NS_STATUS_TEMPORARY_OUT;
+    // status row (., j = m, k = n): runs of inside nodes
+    int nr = 0;
+    if (valid && !ovf)
+      for (int q = 0; q < np; q++) {
+        int64_t ia, ib;
+        status_node_range(g, col[(2 * q) * kThreads], col[(2 * q + 1) * kThreads], &ia, &ib);
+        if (ia > ib) continue;
+        col[(2 * nr) * kThreads] = (double)ia;
+        col[(2 * nr + 1) * kThreads] = (double)ib;
+        nr++;
+      }
+    int64_t off = warp_append(C.out.srun_cursor, C.out.srun_cap, nr, C.out.error_flag, 5);
+    if (valid && !ovf) {
+      if (off >= 0) {
+        for (int q = 0; q < nr; q++)
+          C.out.sruns[off + q] = make_int2((int)col[(2 * q) * kThreads], (int)col[(2 * q + 1) * kThreads]);
+        C.out.srun_off[rid] = off;
+        C.out.srun_cnt[rid] = nr;
+      } else {
+        C.out.srun_cnt[rid] = 0;
       }
     }
     return;
   }
   // accurate-triangulation rays: pair store for the vertex assembly
   {
-    int incl = np;
-    for (int o = 1; o < 32; o <<= 1) {
-      int v = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += v;
-    }
-    int total = __shfl_sync(0xffffffffu, incl, 31);
-    unsigned long long base = 0;
-    if (lane == 31 && total > 0) base = atomicAdd(C.out.pair_cursor, (unsigned long long)total);
-    base = __shfl_sync(0xffffffffu, base, 31);
-    int64_t off = (int64_t)base + incl - np;
-    bool fits = (int64_t)base + total <= C.out.pair_cap;
-    if (!fits && lane == 0 && total > 0) atomicExch(C.out.error_flag, 3);
+    int64_t off = warp_append(C.out.pair_cursor, C.out.pair_cap, np, C.out.error_flag, 3);
     if (valid && !ovf) {
       int64_t ord = rs.ordinal_base + rid;
-      if (fits) {
+      if (off >= 0) {
         for (int q = 0; q < np; q++) {
           C.out.pairs[2 * (off + q)] = col[(2 * q) * kThreads];
           C.out.pairs[2 * (off + q) + 1] = col[(2 * q + 1) * kThreads];
@@ -430,12 +462,23 @@ __global__ void k_trace_overflow(TraceCtx C, const int64_t* __restrict__ tile_of
   C.out.vol_ray[rid] = vol;
   const int64_t NX = g.n[0], NY = g.n[1];
   if (!mc) {
-    int32_t* row = C.out.status + (n * NY + m) * NX;
-    int p = 0;
-    for (int64_t i = 0; i < NX; i++) {
-      double x = gcoord(g, 0, i);
-      while (p < np && col[2 * p + 1] < x) p++;
-      row[i] = (p < np && col[2 * p] <= x) ? NS_STATUS_INSIDE : NS_STATUS_TEMPORARY_OUT;
+    int nr = 0;
+    for (int q = 0; q < np; q++) {
+      int64_t ia, ib;
+      status_node_range(g, col[2 * q], col[2 * q + 1], &ia, &ib);
+      if (ia > ib) continue;
+      col[2 * nr] = (double)ia;
+      col[2 * nr + 1] = (double)ib;
+      nr++;
+    }
+    unsigned long long off = nr ? atomicAdd(C.out.srun_cursor, (unsigned long long)nr) : 0;
+    if ((int64_t)off + nr <= C.out.srun_cap) {
+      for (int q = 0; q < nr; q++) C.out.sruns[off + q] = make_int2((int)col[2 * q], (int)col[2 * q + 1]);
+      C.out.srun_off[rid] = (int64_t)off;
+      C.out.srun_cnt[rid] = nr;
+    } else {
+      C.out.srun_cnt[rid] = 0;
+      atomicExch(C.out.error_flag, 5);
     }
     return;
   }
