@@ -215,6 +215,7 @@ def main():
     p = surf.patches
     ctx = surf._context().handle
     prec = 0 if args.precision == "fp64" else 1
+    surf.precision = args.precision
     flags = N.STATUS | N.ACCURATE_TRIANGULATION
 
     def barrier():
@@ -236,12 +237,16 @@ def main():
         N.check(L.nsg_triangulate(ctx, ctypes.byref(a), ctypes.byref(nv), ctypes.byref(nt)), "triangulate")
         return v.value, a.value, nc.value, nv.value, nt.value
 
-    # per-stage kernel times from one profiled (untimed) pass
+    # per-stage kernel times from one profiled (untimed) pass, after a first pass that sizes the
+    # context's buffers
+    step()
     N.check(L.nsg_profile(ctx, 1), "profile")
     step()
     stage_ms = np.zeros(8)
     stage_calls = np.zeros(8, np.int64)
     L.nsg_stage_times(ctx, stage_ms.ctypes.data, stage_calls.ctypes.data, 8)
+    counters = np.zeros(8, np.int64)
+    L.nsg_trace_counters(ctx, counters.ctypes.data, 8)
     N.check(L.nsg_profile(ctx, 0), "profile")
     stats = surf.stats()
 
@@ -363,6 +368,8 @@ def main():
             "e2e": {"value": world * 1000.0 / e2e_ms, "unit": "structures/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms},
             "gpu_launches": int(launches),
+            "trace_counters": dict(zip(("candidates", "torus_candidates", "fallback_sphere", "fallback_quartic",
+                                        "fallback_root"), counters[:5].tolist())),
             "roofline": roofline,
             "cpu_baseline": cpu,
         }

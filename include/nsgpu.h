@@ -129,6 +129,9 @@ int nsg_event_elapsed(nsg_ctx* ctx, int slot_a, int slot_b, double* ms);
 int nsg_profile(nsg_ctx* ctx, int enable);
 int nsg_stage_times(nsg_ctx* ctx, double* ms, int64_t* calls, int n);
 int64_t nsg_launch_count(nsg_ctx* ctx);
+/* Counters of the last profiled ray cast: candidates, torus candidates, mixed-precision fallbacks
+ * (near-tangent sphere, quartic isolation, root polish), feasibility re-evaluations. */
+int nsg_trace_counters(nsg_ctx* ctx, int64_t* out, int n);
 
 #ifdef __cplusplus
 }

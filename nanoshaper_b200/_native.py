@@ -75,6 +75,7 @@ _SIGNATURES = {
     "nsg_profile": ([_P, _INT], _INT),
     "nsg_stage_times": ([_P, _P, _P, _INT], _INT),
     "nsg_launch_count": ([_P], _I64),
+    "nsg_trace_counters": ([_P, _P, _INT], _INT),
     "nsg_get_stream": ([_P], _P),
     "nsg_volume": ([_P], _D),
     "nsg_area": ([_P], _D),

@@ -74,14 +74,19 @@ struct nsg_ctx {
   // patches
   int64_t np = 0, npool = 0;
   double probe = 1.4;
-  DevBuf f64, i32, pool, flag, win;
+  DevBuf f64, i32, pool, flag, win, pool32;
+  bool pool32_valid = false;
   const double* ext_f64 = nullptr;  // device-resident patch arrays bound by the caller
   const int32_t* ext_i32 = nullptr;
   const double* ext_pool = nullptr;
   const int8_t* ext_flag = nullptr;
   bool has_patches = false;
   // binning per panel
-  DevBuf tile_cnt[3], tile_off[3], tile_list[3];
+  DevBuf tile_cnt[3], tile_off[3], tile_list[3], bin_area;
+  int64_t win_area[3] = {0, 0, 0};
+  // wavefront tracing: candidate lists and the slot-major hit store
+  DevBuf cand_sph, cand_tor, hit_t, hit_cnt;
+  int64_t cand_cap = 0;
   // trace outputs
   DevBuf status, bits, vol_ray[4];
   DevBuf pairs, ray_pair_off, ray_pair_cnt, cursors, ovf_rays[4], ovf_scratch, err;
@@ -115,6 +120,8 @@ struct nsg_ctx {
   double stage_ms[8] = {};
   int64_t stage_calls[8] = {};
   int64_t launches = 0;
+  DevBuf counters;
+  unsigned long long counter_host[8] = {};
 };
 
 namespace {
@@ -126,6 +133,7 @@ nsg::PatchDev patch_dev(nsg_ctx* c) {
   P.i32 = c->ext_i32 ? c->ext_i32 : c->i32.as<int32_t>();
   P.pool = (const double4*)(c->ext_pool ? c->ext_pool : c->pool.as<double>());
   P.flag = c->ext_flag ? c->ext_flag : c->flag.as<int8_t>();
+  P.pool32 = c->pool32.as<float4>();
   P.probe = c->probe;
   P.win = c->win.as<int32_t>();
   return P;
@@ -205,10 +213,17 @@ int bin_panel(nsg_ctx* c, int panel) {
   CK(c->tile_off[panel].ensure((ntiles + 1) * sizeof(int64_t)));
   CK(cudaMemsetAsync(c->tile_cnt[panel].p, 0, (ntiles + 1) * sizeof(int32_t), c->stream));
   nsg::PatchDev P = patch_dev(c);
-  LAUNCH(nsg::launch_bin_count(P, c->gd, rs, c->tile_cnt[panel].as<int32_t>(), c->stream));
+  CK(c->bin_area.ensure(3 * sizeof(unsigned long long)));
+  unsigned long long* area = c->bin_area.as<unsigned long long>() + panel;
+  CK(cudaMemsetAsync(area, 0, sizeof(unsigned long long), c->stream));
+  LAUNCH(nsg::launch_bin_count(P, c->gd, rs, c->tile_cnt[panel].as<int32_t>(), area, c->stream));
   int64_t total = 0;
   int rc = scan_counts(c, c->tile_cnt[panel].as<int32_t>(), ntiles, c->tile_off[panel].as<int64_t>(), &total);
   if (rc) return rc;
+  unsigned long long a_host = 0;
+  CK(cudaMemcpyAsync(&a_host, area, sizeof(a_host), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->win_area[panel] = (int64_t)a_host;
   CK(c->tile_list[panel].ensure(std::max<int64_t>(total, 1) * sizeof(int32_t)));
   CK(cudaMemsetAsync(c->tile_cnt[panel].p, 0, (ntiles + 1) * sizeof(int32_t), c->stream));
   LAUNCH(nsg::launch_bin_fill(P, c->gd, rs, c->tile_off[panel].as<int64_t>(), c->tile_cnt[panel].as<int32_t>(),
@@ -291,7 +306,8 @@ int nsg_ctx_destroy(nsg_ctx* c) {
   if (!c) return NSG_ERR_ARG;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
-  DevBuf* bufs[] = {&c->f64, &c->i32, &c->pool, &c->flag, &c->win, &c->status, &c->bits, &c->pairs,
+  DevBuf* bufs[] = {&c->f64, &c->i32, &c->pool, &c->flag, &c->win, &c->pool32, &c->counters, &c->bin_area,
+                    &c->cand_sph, &c->cand_tor, &c->hit_t, &c->hit_cnt, &c->status, &c->bits, &c->pairs,
                     &c->ray_pair_off, &c->ray_pair_cnt, &c->cursors, &c->ovf_scratch, &c->err, &c->hits,
                     &c->labels, &c->is_root, &c->sruns, &c->srun_off, &c->srun_cnt, &c->fr_cnt, &c->fr_off,
                     &c->fruns, &c->frow, &c->roots, &c->cc_count, &c->cc_desc, &c->cc_label_of,
@@ -343,6 +359,7 @@ static int upload_common(nsg_ctx* c, int64_t n, int64_t npool, double probe) {
   c->probe = probe;
   CK(c->win.ensure(std::max<int64_t>(n, 1) * 6 * sizeof(int32_t)));
   c->has_patches = true;
+  c->pool32_valid = false;
   return NSG_OK;
 }
 
@@ -379,7 +396,8 @@ int nsg_bind_patches_device(nsg_ctx* c, int64_t n, const double* f64, const int3
 
 int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
   if (!c || !c->has_grid || !c->has_patches) return fail(NSG_ERR_STATE, "grid and patches must be set first");
-  if (precision != 0) return fail(NSG_ERR_ARG, "unsupported precision");
+  if (precision != NSG_PRECISION_FP64 && precision != NSG_PRECISION_MIXED)
+    return fail(NSG_ERR_ARG, "unsupported precision");
   CK(cudaSetDevice(c->device));
   const NsGrid& g = c->grid;
   const int64_t tot = g.nx * g.ny * g.nz;
@@ -388,6 +406,12 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
   const bool keep_hits = flags & 16;
   c->flags = flags;
   c->precision = precision;
+  if (precision == NSG_PRECISION_MIXED && !c->pool32_valid) {
+    CK(c->pool32.ensure(std::max<int64_t>(c->npool, 1) * sizeof(float4)));
+    nsg::PatchDev P0 = patch_dev(c);
+    LAUNCH(nsg::launch_pool32(P0, c->pool32.as<float4>(), c->stream));
+    c->pool32_valid = true;
+  }
   nsg::PatchDev P = patch_dev(c);
   stage_begin(c, kStageBin);
   LAUNCH(nsg::launch_windows(P, c->win.as<int32_t>(), c->gd, c->stream));
@@ -414,11 +438,20 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
     CK(cudaMemsetAsync(c->ray_pair_cnt.p, 0, nrays_mc * sizeof(int32_t), c->stream));
     if (c->pair_cap == 0) c->pair_cap = std::max<int64_t>(4 * nrays_mc, 1 << 16);
   }
-  CK(c->cursors.ensure(8 * sizeof(unsigned long long)));
+  CK(c->cursors.ensure(16 * sizeof(unsigned long long)));
+  {
+    int64_t amax = std::max(c->win_area[0], std::max(c->win_area[1], c->win_area[2]));
+    c->cand_cap = std::max<int64_t>(c->cand_cap, amax + 1024);
+    int64_t nr_max = std::max(g.ny * g.nz, std::max(g.nx * g.ny, g.nx * g.nz));
+    CK(c->hit_t.ensure((size_t)nr_max * nsg::kHitCap * sizeof(double)));
+    CK(c->hit_cnt.ensure(nr_max * sizeof(int32_t)));
+  }
   CK(c->err.ensure(sizeof(int32_t)));
   const int ovf_cap = 1 << 16;
   for (int attempt = 0; attempt < 4; attempt++) {
     if (do_mc) CK(c->pairs.ensure(c->pair_cap * 2 * sizeof(double)));
+    CK(c->cand_sph.ensure(c->cand_cap * sizeof(int2)));
+    CK(c->cand_tor.ensure(c->cand_cap * sizeof(int2)));
     if (do_status) {
       CK(c->sruns.ensure(c->srun_cap * sizeof(int2)));
       CK(cudaMemsetAsync(c->srun_cnt.p, 0, nrows * sizeof(int32_t), c->stream));
@@ -427,7 +460,7 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
       if (c->hit_cap == 0) c->hit_cap = std::max<int64_t>(8 * (nrays_mc + g.nz * g.ny), 1 << 16);
       CK(c->hits.ensure(c->hit_cap * sizeof(double)));
     }
-    CK(cudaMemsetAsync(c->cursors.p, 0, 8 * sizeof(unsigned long long), c->stream));
+    CK(cudaMemsetAsync(c->cursors.p, 0, 16 * sizeof(unsigned long long), c->stream));
     CK(cudaMemsetAsync(c->err.p, 0, sizeof(int32_t), c->stream));
     if (do_mc) CK(cudaMemsetAsync(c->bits.p, 0xff, nwords * sizeof(uint32_t), c->stream));
     unsigned long long* cur = c->cursors.as<unsigned long long>();
@@ -436,6 +469,10 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
     if (do_status) sets[nsets++] = 0;
     if (do_mc) { sets[nsets++] = 1; sets[nsets++] = 2; sets[nsets++] = 3; }
     nsg::TraceOut outs[4];
+    if (c->profile) {
+      CK(c->counters.ensure(8 * sizeof(unsigned long long)));
+      CK(cudaMemsetAsync(c->counters.p, 0, 8 * sizeof(unsigned long long), c->stream));
+    }
     stage_begin(c, kStageTrace);
     for (int si = 0; si < nsets; si++) {
       int s = sets[si];
@@ -461,6 +498,7 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
       o.ovf_cap = ovf_cap;
       o.ovf_count = ovf_count + s;
       o.error_flag = c->err.as<int32_t>();
+      o.counters = c->profile ? c->counters.as<unsigned long long>() : nullptr;
       if (keep_hits) {
         CK(c->ray_hit_off[s].ensure(nr * sizeof(int64_t)));
         CK(c->ray_hit_cnt[s].ensure(nr * sizeof(int32_t)));
@@ -472,7 +510,11 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
         o.ray_hit_cnt = c->ray_hit_cnt[s].as<int32_t>();
       }
       outs[s] = o;
-      LAUNCH(nsg::launch_trace(P, c->gd, rs, c->tile_off[panel].as<int64_t>(), c->tile_list[panel].as<int32_t>(), o,
+      nsg::CandOut co{c->cand_sph.as<int2>(), c->cand_tor.as<int2>(), c->cand_cap, cur + 8 + 2 * s};
+      nsg::HitStore hs{c->hit_t.as<double>(), c->hit_cnt.as<int32_t>(), nr};
+      CK(cudaMemsetAsync(c->hit_cnt.p, 0, nr * sizeof(int32_t), c->stream));
+      c->launches += 4;
+      CK(nsg::launch_trace(P, c->gd, rs, c->tile_off[panel].as<int64_t>(), c->tile_list[panel].as<int32_t>(), o, co, hs,
                            precision, c->stream));
     }
     stage_end(c, kStageTrace);
@@ -495,6 +537,11 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
     }
     stage_end(c, kStageOverflow);
     c->last_overflow_rays = tot_ovf;
+    if (c->profile) {
+      CK(cudaMemcpyAsync(c->counter_host, c->counters.p, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                         c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+    }
     int32_t errflag = 0;
     unsigned long long used[3] = {0, 0, 0};
     CK(cudaMemcpyAsync(&errflag, c->err.p, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
@@ -504,6 +551,7 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
     if (errflag == 3) { c->pair_cap = std::max<int64_t>(2 * c->pair_cap, (int64_t)used[0] + 1024); continue; }
     if (errflag == 2) { c->hit_cap = std::max<int64_t>(2 * c->hit_cap, (int64_t)used[1] + 1024); continue; }
     if (errflag == 5) { c->srun_cap = std::max<int64_t>(2 * c->srun_cap, (int64_t)used[2] + 1024); continue; }
+    if (errflag == 6) { c->cand_cap *= 2; continue; }
     return fail(NSG_ERR_CAPACITY, errflag == 1 ? "too many overflow rays" : "ray hit capacity exceeded");
   }
   // volume: A * sum of interval lengths over the ray sets / number of ray sets
@@ -663,10 +711,7 @@ int nsg_triangulate(nsg_ctx* c, double* area_out, int64_t* nverts, int64_t* ntri
   // rows of cubes
   const int64_t nrows = (g.ny - 2) * (g.nz - 2);
   CK(c->row_act_cnt.ensure((nrows + 1) * sizeof(int64_t)));
-  CK(c->row_mid_cnt.ensure((nrows + 1) * sizeof(int64_t)));
   CK(c->row_act_off.ensure((nrows + 1) * sizeof(int64_t)));
-  CK(c->row_mid_off.ensure((nrows + 1) * sizeof(int64_t)));
-  // vertex buffers: analytic now, midpoints appended later (reallocation keeps analytic data)
   nsg::MCArgs M{};
   M.g = c->gd;
   M.bits = c->bits.as<uint32_t>();
@@ -676,8 +721,7 @@ int nsg_triangulate(nsg_ctx* c, double* area_out, int64_t* nverts, int64_t* ntri
   M.n_analytic = n_an;
   M.nrows = nrows;
   M.row_act_cnt = c->row_act_cnt.as<int64_t>();
-  M.row_mid_cnt = c->row_mid_cnt.as<int64_t>();
-  // analytic vertices first (the midpoint count pass needs their edge keys)
+  // analytic vertices first (the midpoint pass needs their edge keys)
   CK(c->vkey.ensure(std::max<int64_t>(n_an, 1) * sizeof(int4)));
   CK(c->vpos.ensure(std::max<int64_t>(n_an, 1) * 3 * sizeof(double)));
   V.vpos = c->vpos.as<double>();
@@ -687,14 +731,28 @@ int nsg_triangulate(nsg_ctx* c, double* area_out, int64_t* nverts, int64_t* ntri
   stage_begin(c, kStageMC);
   M.vpos = c->vpos.as<double>();
   M.vkey = c->vkey.as<int4>();
+  // active cubes
   LAUNCH(nsg::launch_mc_rows(M, 0, c->stream));
   int64_t n_act = 0, n_mid = 0;
   rc = scan_counts(c, c->row_act_cnt.as<int64_t>(), nrows, c->row_act_off.as<int64_t>(), &n_act);
   if (rc) return rc;
-  rc = scan_counts(c, c->row_mid_cnt.as<int64_t>(), nrows, c->row_mid_off.as<int64_t>(), &n_mid);
+  M.row_act_off = c->row_act_off.as<int64_t>();
+  CK(c->act_rec.ensure(std::max<int64_t>(n_act, 1) * sizeof(int4)));
+  CK(c->act_mid.ensure(std::max<int64_t>(n_act, 1) * sizeof(int32_t)));
+  CK(c->row_mid_cnt.ensure(std::max<int64_t>(n_act, 1) * sizeof(int32_t)));
+  CK(c->row_mid_off.ensure((n_act + 1) * sizeof(int64_t)));
+  M.act_rec = c->act_rec.as<int4>();
+  M.act_mid = c->act_mid.as<int32_t>();
+  M.mid_cnt = c->row_mid_cnt.as<int32_t>();
+  M.mid_off = c->row_mid_off.as<int64_t>();
+  M.n_active = n_act;
+  LAUNCH(nsg::launch_mc_rows(M, 1, c->stream));
+  // midpoint vertices of cut edges without an analytic vertex
+  LAUNCH(nsg::launch_mc_mid(M, 0, c->stream));
+  rc = scan_counts(c, c->row_mid_cnt.as<int32_t>(), n_act, c->row_mid_off.as<int64_t>(), &n_mid);
   if (rc) return rc;
   const int64_t n_v = n_an + n_mid;
-  if ((size_t)n_v * sizeof(int4) > c->vkey.cap) {
+  if ((size_t)n_v * sizeof(int4) > c->vkey.cap || (size_t)n_v * 3 * sizeof(double) > c->vpos.cap) {
     DevBuf nk, np_;
     CK(nk.ensure(n_v * sizeof(int4)));
     CK(np_.ensure(n_v * 3 * sizeof(double)));
@@ -708,23 +766,9 @@ int nsg_triangulate(nsg_ctx* c, double* area_out, int64_t* nverts, int64_t* ntri
     c->vkey = nk;
     c->vpos = np_;
   }
-  if ((size_t)n_v * 3 * sizeof(double) > c->vpos.cap) {
-    DevBuf np_;
-    CK(np_.ensure(n_v * 3 * sizeof(double)));
-    if (n_an) CK(cudaMemcpyAsync(np_.p, c->vpos.p, n_an * 3 * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    c->vpos.release();
-    c->vpos = np_;
-  }
   M.vpos = c->vpos.as<double>();
   M.vkey = c->vkey.as<int4>();
-  M.row_act_off = c->row_act_off.as<int64_t>();
-  M.row_mid_off = c->row_mid_off.as<int64_t>();
-  CK(c->act_rec.ensure(std::max<int64_t>(n_act, 1) * sizeof(int4)));
-  CK(c->act_mid.ensure(std::max<int64_t>(n_act, 1) * sizeof(int32_t)));
-  M.act_rec = c->act_rec.as<int4>();
-  M.act_mid = c->act_mid.as<int32_t>();
-  LAUNCH(nsg::launch_mc_rows(M, 1, c->stream));
+  LAUNCH(nsg::launch_mc_mid(M, 1, c->stream));
   M.n_active = n_act;
   CK(c->tri_cnt.ensure(std::max<int64_t>(n_act, 1) * sizeof(int32_t)));
   CK(c->tri_off.ensure((n_act + 1) * sizeof(int64_t)));
@@ -854,6 +898,14 @@ int nsg_stage_times(nsg_ctx* c, double* ms, int64_t* calls, int n) {
     if (ms) ms[i] = c->stage_ms[i];
     if (calls) calls[i] = c->stage_calls[i];
   }
+  return NSG_OK;
+}
+
+// Event counters of the last profiled ray cast: candidates, torus candidates, mixed-precision
+// fallbacks (near-tangent sphere, quartic isolation, root polish), feasibility re-evaluations.
+int nsg_trace_counters(nsg_ctx* c, int64_t* out, int n) {
+  if (!c || !out) return NSG_ERR_ARG;
+  for (int i = 0; i < n && i < 8; i++) out[i] = (int64_t)c->counter_host[i];
   return NSG_OK;
 }
 

@@ -16,6 +16,9 @@
 #define NSG_ERR_GEOMETRY (-8)
 #define NSG_ERR_TIMEOUT (-9)
 
+#define NSG_PRECISION_FP64 0
+#define NSG_PRECISION_MIXED 1
+
 #ifdef __cplusplus
 extern "C" {
 #endif

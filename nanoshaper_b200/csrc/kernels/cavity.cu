@@ -165,20 +165,28 @@ __global__ void k_run_fill(RunArgs A, const uint8_t* __restrict__ fill_of, uint3
   }
 }
 
-// Dense status map, one warp per x-row: free runs get their region label (or TEMPORARY_OUT
-// before cavity detection), all other nodes STATUS_POINT_INSIDE.
+// Dense status map, one warp per x-row: the row is the sequence of its free runs (region label,
+// or TEMPORARY_OUT before cavity detection) and the inside segments between them
+// (STATUS_POINT_INSIDE); every segment is written by the whole warp with coalesced stores.
 __global__ void k_status_write(RunArgs A, const int32_t* __restrict__ label_of, int32_t* status) {
   const int lane = threadIdx.x & 31;
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t r = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); r < A.nrows; r += warps) {
-    int64_t b = A.fr_off[r], e = A.fr_off[r + 1];
+    const int64_t b = A.fr_off[r], e = A.fr_off[r + 1];
     int32_t* row = status + r * A.nx;
-    int64_t p = b;
-    for (int64_t i = lane; i < A.nx; i += 32) {
-      while (p < e && A.fruns[p].y < i) p++;
-      int32_t v = NS_STATUS_INSIDE;
-      if (p < e && A.fruns[p].x <= i) v = label_of ? label_of[A.L[p]] : NS_STATUS_TEMPORARY_OUT;
-      row[i] = v;
+    int64_t next = 0;  // first node not yet written
+    for (int64_t u = b; u <= e; u++) {
+      int64_t x0 = A.nx, x1 = A.nx - 1;
+      int32_t lab = NS_STATUS_TEMPORARY_OUT;
+      if (u < e) {
+        int2 ru = A.fruns[u];
+        x0 = ru.x;
+        x1 = ru.y;
+        if (label_of) lab = label_of[A.L[u]];
+      }
+      for (int64_t i = next + lane; i < x0; i += 32) row[i] = NS_STATUS_INSIDE;
+      for (int64_t i = x0 + lane; i <= x1; i += 32) row[i] = lab;
+      next = x1 + 1;
     }
   }
 }

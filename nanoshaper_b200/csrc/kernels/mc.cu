@@ -162,8 +162,7 @@ __device__ __forceinline__ uint32_t bits32(const uint32_t* __restrict__ bits, in
 
 // One warp per cube row (j, k); every lane classifies 32 consecutive cubes at once from the four
 // bit rows the cubes touch (corner inside = bit 0): a cube is active unless its 8 corners agree.
-// Only active cubes look up vertices.  Pass 0 counts, pass 1 emits active cubes (in i order) and
-// their midpoint vertices.
+// Pass 0 counts the active cubes of the row, pass 1 writes them in i order.
 __global__ void k_mc_rows(MCArgs A, int emit) {
   const GridDev& g = A.g;
   const int64_t NX = g.n[0], NY = g.n[1];
@@ -173,9 +172,8 @@ __global__ void k_mc_rows(MCArgs A, int emit) {
     int64_t j = 1 + row % (NY - 2);
     int64_t k = 1 + row / (NY - 2);
     const int64_t b00 = (k * NY + j) * NX, b10 = b00 + NX, b01 = b00 + NX * NY, b11 = b01 + NX;
-    int64_t act_run = 0, mid_run = 0;
+    int64_t act_run = 0;
     int64_t act_base = emit ? A.row_act_off[row] : 0;
-    int64_t mid_base = emit ? A.row_mid_off[row] : 0;
     for (int64_t i0 = 1; i0 < NX - 1; i0 += 32 * 32) {
       int64_t ic = i0 + 32 * lane;
       uint32_t act = 0;
@@ -197,60 +195,61 @@ __global__ void k_mc_rows(MCArgs A, int emit) {
         act = d & vm;
       }
       int na = __popc(act);
-      int nm = 0;
-      for (uint32_t m = act; m; m &= m - 1) {
-        int b = __ffs(m) - 1;
-        int cs = 0;
-#pragma unroll
-        for (int q = 0; q < 8; q++) cs |= ((c[q] >> b) & 1u) << q;
-        nm += __popc(own_midpoints(A, ic + b, j, k, c_emask[cs]));
-      }
-      int ia = na, im = nm;
+      int ia = na;
       for (int o = 1; o < 32; o <<= 1) {
         int va = __shfl_up_sync(0xffffffffu, ia, o);
-        int vm2 = __shfl_up_sync(0xffffffffu, im, o);
-        if (lane >= o) { ia += va; im += vm2; }
+        if (lane >= o) ia += va;
       }
-      int ta = __shfl_sync(0xffffffffu, ia, 31), tm = __shfl_sync(0xffffffffu, im, 31);
+      int ta = __shfl_sync(0xffffffffu, ia, 31);
       if (emit && na) {
         int64_t slot = act_base + act_run + ia - na;
-        int64_t v = A.n_analytic + mid_base + mid_run + im - nm;
         for (uint32_t m = act; m; m &= m - 1) {
           int b = __ffs(m) - 1;
-          int64_t i = ic + b;
           int cs = 0;
 #pragma unroll
           for (int q = 0; q < 8; q++) cs |= ((c[q] >> b) & 1u) << q;
-          int mm = own_midpoints(A, i, j, k, c_emask[cs]);
-          A.act_rec[slot] = make_int4((int)i, (int)j, (int)k, cs | (mm << 8));
-          A.act_mid[slot] = (int32_t)v;
-          slot++;
-          if (mm & 1) {
-            A.vpos[3 * v] = gcoord(g, 0, i + 1) - g.hside; A.vpos[3 * v + 1] = gcoord(g, 1, j);
-            A.vpos[3 * v + 2] = gcoord(g, 2, k + 1) - g.hside;
-            A.vkey[v] = make_int4((int)(i + 1), (int)j, (int)(k + 1), NS_Y_DIR);
-            v++;
-          }
-          if (mm & 2) {
-            A.vpos[3 * v] = gcoord(g, 0, i); A.vpos[3 * v + 1] = gcoord(g, 1, j + 1) - g.hside;
-            A.vpos[3 * v + 2] = gcoord(g, 2, k + 1) - g.hside;
-            A.vkey[v] = make_int4((int)i, (int)(j + 1), (int)(k + 1), NS_X_DIR);
-            v++;
-          }
-          if (mm & 4) {
-            A.vpos[3 * v] = gcoord(g, 0, i + 1) - g.hside; A.vpos[3 * v + 1] = gcoord(g, 1, j + 1) - g.hside;
-            A.vpos[3 * v + 2] = gcoord(g, 2, k);
-            A.vkey[v] = make_int4((int)(i + 1), (int)(j + 1), (int)k, NS_Z_DIR);
-            v++;
-          }
+          A.act_rec[slot++] = make_int4((int)(ic + b), (int)j, (int)k, cs);
         }
       }
       act_run += ta;
-      mid_run += tm;
     }
-    if (!emit && lane == 0) {
-      A.row_act_cnt[row] = act_run;
-      A.row_mid_cnt[row] = mid_run;
+    if (!emit && lane == 0) A.row_act_cnt[row] = act_run;
+  }
+}
+
+// One thread per active cube.  Pass 0: which of the cube's own edges 5, 6, 10 need a midpoint
+// vertex (cut edge without an analytic vertex); the mask goes to bits 8..10 of the record and the
+// count to mid_cnt.  Pass 1: writes those vertices at their final indices (act_mid).
+__global__ void k_mc_mid(MCArgs A, int emit) {
+  const GridDev& g = A.g;
+  for (int64_t a = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; a < A.n_active; a += (int64_t)gridDim.x * blockDim.x) {
+    int4 rec = A.act_rec[a];
+    const int64_t i = rec.x, j = rec.y, k = rec.z;
+    if (!emit) {
+      int mm = own_midpoints(A, i, j, k, c_emask[rec.w & 255]);
+      A.act_rec[a].w = (rec.w & 255) | (mm << 8);
+      A.mid_cnt[a] = __popc(mm);
+      continue;
+    }
+    int mm = (rec.w >> 8) & 7;
+    int64_t v = A.n_analytic + A.mid_off[a];
+    A.act_mid[a] = (int32_t)v;
+    if (mm & 1) {
+      A.vpos[3 * v] = gcoord(g, 0, i + 1) - g.hside; A.vpos[3 * v + 1] = gcoord(g, 1, j);
+      A.vpos[3 * v + 2] = gcoord(g, 2, k + 1) - g.hside;
+      A.vkey[v] = make_int4((int)(i + 1), (int)j, (int)(k + 1), NS_Y_DIR);
+      v++;
+    }
+    if (mm & 2) {
+      A.vpos[3 * v] = gcoord(g, 0, i); A.vpos[3 * v + 1] = gcoord(g, 1, j + 1) - g.hside;
+      A.vpos[3 * v + 2] = gcoord(g, 2, k + 1) - g.hside;
+      A.vkey[v] = make_int4((int)i, (int)(j + 1), (int)(k + 1), NS_X_DIR);
+      v++;
+    }
+    if (mm & 4) {
+      A.vpos[3 * v] = gcoord(g, 0, i + 1) - g.hside; A.vpos[3 * v + 1] = gcoord(g, 1, j + 1) - g.hside;
+      A.vpos[3 * v + 2] = gcoord(g, 2, k);
+      A.vkey[v] = make_int4((int)(i + 1), (int)(j + 1), (int)k, NS_Z_DIR);
     }
   }
 }
@@ -373,6 +372,12 @@ cudaError_t launch_mc_rows(const MCArgs& A, int emit, cudaStream_t s) {
   if (A.nrows <= 0) return cudaSuccess;
   int64_t warps = A.nrows;
   k_mc_rows<<<grid_for(warps * 32, 256), 256, 0, s>>>(A, emit);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mc_mid(const MCArgs& A, int emit, cudaStream_t s) {
+  if (A.n_active <= 0) return cudaSuccess;
+  k_mc_mid<<<grid_for(A.n_active, 256), 256, 0, s>>>(A, emit);
   return cudaGetLastError();
 }
 

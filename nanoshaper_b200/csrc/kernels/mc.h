@@ -32,10 +32,10 @@ struct MCArgs {
   int4* vkey;
   int64_t nrows;                 // (NY-2)*(NZ-2) cube rows
   int64_t* row_act_cnt;
-  int64_t* row_mid_cnt;
   const int64_t* row_act_off;    // nrows+1 entries
-  const int64_t* row_mid_off;
   int4* act_rec;                 // i, j, k, case | midpoint mask << 8
+  int32_t* mid_cnt;              // midpoint vertices per active cube
+  const int64_t* mid_off;        // exclusive scan of mid_cnt
   int32_t* act_mid;              // index of the first midpoint vertex of the cube
   int64_t n_active;
   int32_t* tri_cnt;
@@ -47,6 +47,7 @@ struct MCArgs {
 cudaError_t mc_init_tables();
 cudaError_t launch_vert(const VertArgs& A, int emit, cudaStream_t s);
 cudaError_t launch_mc_rows(const MCArgs& A, int emit, cudaStream_t s);
+cudaError_t launch_mc_mid(const MCArgs& A, int emit, cudaStream_t s);
 cudaError_t launch_mc_tris(const MCArgs& A, int emit, cudaStream_t s);
 
 }  // namespace nsg

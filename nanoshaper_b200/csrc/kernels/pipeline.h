@@ -84,6 +84,29 @@ struct TraceOut {
   int64_t* ray_hit_off;    // indexed by n*nb+m
   int32_t* ray_hit_cnt;
   int32_t* error_flag;     // set when a device-side capacity is exceeded
+  // optional event counters (profiling): candidates, torus candidates, mixed-precision fallbacks
+  // (near-tangent sphere, quartic isolation, root polish / root boundary), FP64 re-evaluations of
+  // feasibility tests
+  unsigned long long* counters;
+};
+
+enum { kCntCandidates = 0, kCntTorus = 1, kCntFbSphere = 2, kCntFbQuartic = 3, kCntFbRoot = 4, kCntRecheck = 5,
+       kCntN = 8 };
+
+// Candidate (ray, patch) pairs of one ray set, by patch type (0 spheres, 1 tori).
+struct CandOut {
+  int2* sph;
+  int2* tor;
+  int64_t cap;
+  unsigned long long* count;  // 2 counters
+};
+
+// Slot-major hit store of one ray set: hit i of ray r at t[i * nrays + r]; cnt[r] counts the
+// hits filed (more than kHitCap sends the ray to the overflow path).
+struct HitStore {
+  double* t;
+  int32_t* cnt;
+  int64_t nrays;
 };
 
 struct PatchDev {
@@ -91,6 +114,7 @@ struct PatchDev {
   const double* f64;
   const int32_t* i32;
   const double4* pool;
+  const float4* pool32;  // pool in patch-local FP32 form (mixed precision)
   const int8_t* flag;
   double probe;
   const int32_t* win;  // 6 per patch: start x,y,z, end x,y,z; start = -1 when culled
@@ -98,12 +122,15 @@ struct PatchDev {
 
 // trace.cu
 cudaError_t launch_windows(const PatchDev& P, int32_t* win, const GridDev& g, cudaStream_t s);
+// Patch-local FP32 copy of the pool: planes (n, d + n.c), clipping spheres (s - c, r^2).
+cudaError_t launch_pool32(const PatchDev& P, float4* pool32, cudaStream_t s);
 cudaError_t launch_bin_count(const PatchDev& P, const GridDev& g, const RaySet& rs, int32_t* tile_cnt,
-                             cudaStream_t s);
+                             unsigned long long* area, cudaStream_t s);
 cudaError_t launch_bin_fill(const PatchDev& P, const GridDev& g, const RaySet& rs, const int64_t* tile_off,
                             int32_t* tile_cursor, int32_t* tile_list, cudaStream_t s);
 cudaError_t launch_trace(const PatchDev& P, const GridDev& g, const RaySet& rs, const int64_t* tile_off,
-                         const int32_t* tile_list, const TraceOut& out, int precision, cudaStream_t s);
+                         const int32_t* tile_list, const TraceOut& out, const CandOut& co, const HitStore& hs,
+                         int precision, cudaStream_t s);
 cudaError_t launch_trace_overflow(const PatchDev& P, const GridDev& g, const RaySet& rs, const int64_t* tile_off,
                                   const int32_t* tile_list, const TraceOut& out, int n_ovf, double* scratch,
                                   int precision, cudaStream_t s);

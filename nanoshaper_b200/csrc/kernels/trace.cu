@@ -15,6 +15,7 @@
 
 #include "pipeline.h"
 #include "ray_math.cuh"
+#include "ray_math_mixed.cuh"
 
 namespace nsg {
 
@@ -52,12 +53,33 @@ __global__ void k_windows(PatchDev P, int32_t* win, GridDev g) {
   }
 }
 
-__global__ void k_bin(PatchDev P, GridDev g, RaySet rs, int32_t* tile_cnt, const int64_t* tile_off,
-                      int32_t* tile_cursor, int32_t* tile_list) {
+__global__ void k_pool32(PatchDev P, float4* out) {
   int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (p >= P.n) return;
-  const int32_t* w = P.win + 6 * p;
-  if (w[0] < 0) return;
+  const double* f = P.f64 + (int64_t)NS_PATCH_F64 * p;
+  const int32_t* ir = P.i32 + NS_PATCH_I32 * p;
+  const int kind = ir[0];
+  for (int q = ir[1]; q < ir[1] + ir[2]; q++) {
+    double4 w = P.pool[q];
+    if (kind == NS_POINT)
+      out[q] = make_float4((float)(w.x - f[0]), (float)(w.y - f[1]), (float)(w.z - f[2]), (float)w.w);
+    else
+      out[q] = make_float4((float)w.x, (float)w.y, (float)w.z, (float)(w.w + (w.x * f[0] + w.y * f[1] + w.z * f[2])));
+  }
+}
+
+__global__ void k_bin(PatchDev P, GridDev g, RaySet rs, int32_t* tile_cnt, const int64_t* tile_off,
+                      int32_t* tile_cursor, int32_t* tile_list, unsigned long long* area) {
+  int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int32_t* w = P.win + 6 * (p < P.n ? p : 0);
+  bool live = p < P.n && w[0] >= 0;
+  if (area) {
+    // pixel-window area: an upper bound of the patch's candidate rays in this panel
+    unsigned a = live ? (unsigned)((w[3 + rs.fd] - w[rs.fd] + 1) * (w[3 + rs.ld] - w[rs.ld] + 1)) : 0u;
+    unsigned sum = __reduce_add_sync(0xffffffffu, a);
+    if ((threadIdx.x & 31) == 0 && sum) atomicAdd(area, (unsigned long long)sum);
+  }
+  if (!live) return;
   int64_t ntm = (rs.nb + kTileM - 1) / kTileM;
   int m0 = w[rs.fd] / kTileM, m1 = w[3 + rs.fd] / kTileM;
   int n0 = w[rs.ld] / kTileN, n1 = w[3 + rs.ld] / kTileN;
@@ -73,18 +95,25 @@ __global__ void k_bin(PatchDev P, GridDev g, RaySet rs, int32_t* tile_cnt, const
     }
 }
 
-// Tests one (ray, patch) candidate and reports the feasible hits in t[0..n-1].
-__device__ __forceinline__ int ray_patch_f64(const double* f, int kind, int first, int cnt, const PatchDev& P,
-                                             const RaySet& rs, const double* pa, const double* dir, double ray_dir,
-                                             double* t) {
-  int fd = rs.fd, ld = rs.ld, vc = rs.vc;
+// Candidate test of the reference's pixel loop: the ray origin lies inside the patch's bounding
+// box and equatorial disc (src/ConnollySurface.cpp:4469-4502); the pixel window test is done by
+// the caller.
+__device__ __forceinline__ bool candidate(const double* f, const RaySet& rs, const double* pa) {
+  int fd = rs.fd, ld = rs.ld;
   double r = f[kR];
-  if (pa[fd] < f[fd] - r || pa[fd] > f[fd] + r) return 0;
-  if (pa[ld] < f[ld] - r || pa[ld] > f[ld] + r) return 0;
+  if (pa[fd] < f[fd] - r || pa[fd] > f[fd] + r) return false;
+  if (pa[ld] < f[ld] - r || pa[ld] > f[ld] + r) return false;
   double dx = f[fd] - pa[fd];
   double dy = f[ld] - pa[ld];
-  if (dx * dx + dy * dy > r * r) return 0;
-  if (!ray_sphere_f64(pa, dir, f, r, &t[0], &t[1])) return 0;
+  return !(dx * dx + dy * dy > r * r);
+}
+
+// Double-precision intersection of a candidate: hits in t[0..n-1] (ray parameter units).
+__device__ __forceinline__ int intersect_f64(const double* f, int kind, int first, int cnt, const PatchDev& P,
+                                             const RaySet& rs, const double* pa, const double* dir, double ray_dir,
+                                             double* t) {
+  int vc = rs.vc;
+  if (!ray_sphere_f64(pa, dir, f, f[kR], &t[0], &t[1])) return 0;
   int numInt = 2;
   if (kind == NS_EDGE_REG || kind == NS_EDGE_SING) numInt = ray_torus_f64(f, P.probe, vc, pa, ray_dir, t);
   int out = 0;
@@ -92,6 +121,174 @@ __device__ __forceinline__ int ray_patch_f64(const double* f, int kind, int firs
     double ip[3] = {pa[0], pa[1], pa[2]};
     ip[vc] += t[i] * ray_dir;
     if (feasible_f64(f, kind, first, cnt, P.pool, P.flag, ip)) t[out++] = t[i];
+  }
+  return out;
+}
+
+// Tests one (ray, patch) candidate and reports the feasible hits in t[0..n-1].
+__device__ __forceinline__ int ray_patch_f64(const double* f, int kind, int first, int cnt, const PatchDev& P,
+                                             const RaySet& rs, const double* pa, const double* dir, double ray_dir,
+                                             double* t) {
+  if (!candidate(f, rs, pa)) return 0;
+  return intersect_f64(f, kind, first, cnt, P, rs, pa, dir, ray_dir, t);
+}
+
+// Axes of a panel as compile-time constants: pixel axes (fd, ld) and ray axis vc.
+template <int P>
+struct Ax {
+  static constexpr int fd = P == 0 ? 1 : 0;
+  static constexpr int ld = P == 1 ? 1 : 2;
+  static constexpr int vc = P == 0 ? 0 : (P == 1 ? 2 : 1);
+};
+
+template <int P>
+__device__ __forceinline__ bool candidate_p(const double* f, const double* pa) {
+  constexpr int fd = Ax<P>::fd, ld = Ax<P>::ld;
+  double r = f[kR];
+  if (pa[fd] < f[fd] - r || pa[fd] > f[fd] + r) return false;
+  if (pa[ld] < f[ld] - r || pa[ld] > f[ld] + r) return false;
+  double dx = f[fd] - pa[fd];
+  double dy = f[ld] - pa[ld];
+  return !(dx * dx + dy * dy > r * r);
+}
+
+// raySphere for a ray along axis VC with direction length d: the dot products of the generic
+// routine reduce to single products (the other terms are zero), the rest keeps its operation order.
+template <int VC>
+__device__ __forceinline__ bool ray_sphere_axis(const double* orig, double d, const double* c, double r, double* t1,
+                                                double* t2) {
+  double temp0 = orig[0] - c[0], temp1 = orig[1] - c[1], temp2 = orig[2] - c[2];
+  double tv = VC == 0 ? temp0 : (VC == 1 ? temp1 : temp2);
+  double A = d * d;
+  double B = tv * d;
+  double C = temp0 * temp0 + temp1 * temp1 + temp2 * temp2 - r * r;
+  double det = B * B - A * C;
+  if (det < 0.) return false;
+  det = sqrt(det);
+  double a = (-B - det) / A;
+  double b = (-B + det) / A;
+  if (b < a) { double tt = a; a = b; b = tt; }
+  *t1 = a;
+  *t2 = b;
+  return true;
+}
+
+template <int P, bool kTorus>
+__device__ __forceinline__ int intersect_f64_p(const double* f, int kind, int first, int cnt, const PatchDev& Pd,
+                                               const double* pa, double ray_dir, double* t) {
+  constexpr int vc = Ax<P>::vc;
+  if (!ray_sphere_axis<vc>(pa, ray_dir, f, f[kR], &t[0], &t[1])) return 0;
+  int numInt = 2;
+  if (kTorus) numInt = ray_torus_f64(f, Pd.probe, vc, pa, ray_dir, t);
+  int out = 0;
+  for (int i = 0; i < numInt; i++) {
+    double ip[3] = {pa[0], pa[1], pa[2]};
+    ip[vc] += t[i] * ray_dir;
+    if (feasible_f64(f, kind, first, cnt, Pd.pool, Pd.flag, ip)) t[out++] = t[i];
+  }
+  return out;
+}
+
+template <int P>
+__device__ __noinline__ int intersect_f64_fallback_p(const double* f, int kind, int first, int cnt,
+                                                     const PatchDev& Pd, const double* pa, double ray_dir,
+                                                     double* t) {
+  if (kind == NS_EDGE_REG || kind == NS_EDGE_SING) return intersect_f64_p<P, true>(f, kind, first, cnt, Pd, pa, ray_dir, t);
+  return intersect_f64_p<P, false>(f, kind, first, cnt, Pd, pa, ray_dir, t);
+}
+
+// Out-of-line double-precision intersection: the fallback of the mixed path, kept out of the
+// caller so that the rare fallback does not inflate the mixed kernel's register allocation.
+__device__ __noinline__ int intersect_f64_fallback(const double* f, int kind, int first, int cnt, const PatchDev& P,
+                                                   const RaySet& rs, const double* pa, const double* dir,
+                                                   double ray_dir, double* t) {
+  return intersect_f64(f, kind, first, cnt, P, rs, pa, dir, ray_dir, t);
+}
+
+// Mixed-precision intersection of a candidate (see ray_math_mixed.cuh); falls back to the
+// double-precision path for undecided candidates.
+template <int PN, bool kTorus>
+__device__ __forceinline__ int intersect_mixed(const double* f, int kind, int first, int cnt, const PatchDev& P,
+                                               const double* pa, double ray_dir, double inv_dir, double* t,
+                                               unsigned long long* ctr) {
+  constexpr int fd = Ax<PN>::fd, ld = Ax<PN>::ld, vc = Ax<PN>::vc;
+  const double r = f[kR];
+  const double dx64 = pa[fd] - f[fd], dy64 = pa[ld] - f[ld];
+  const float dxf = (float)dx64, dyf = (float)dy64, rf = (float)r;
+  float disc = rf * rf - dxf * dxf - dyf * dyf;
+  if (disc < kDiscTol) {
+    if (ctr) atomicAdd(ctr + kCntFbSphere, 1ull);
+    return intersect_f64_fallback_p<PN>(f, kind, first, cnt, P, pa, ray_dir, t);
+  }
+  float s32 = sqrtf(disc);
+  double disc64 = r * r - dx64 * dx64 - dy64 * dy64;
+  double sd = (double)s32;
+  sd = sd + (disc64 - sd * sd) * (double)(0.5f / s32);
+  double xs[4];
+  int nx = 0;
+  const double cv = f[vc];
+  if (kTorus) {
+    const double x_in = cv - sd;
+    double orig1[3];
+    orig1[fd] = pa[fd];
+    orig1[ld] = pa[ld];
+    orig1[vc] = x_in;
+    double B, C, D, E;
+    torus_coeffs_f64(f, P.probe, vc, orig1, &B, &C, &D, &E);
+    float rt[4];
+    int nr = quartic_f32(rt, (float)B, (float)C, (float)D, (float)E);
+    if (ctr) atomicAdd(ctr + kCntTorus, 1ull);
+    if (nr < 0) {
+      if (ctr) atomicAdd(ctr + kCntFbQuartic, 1ull);
+      return intersect_f64_fallback_p<PN>(f, kind, first, cnt, P, pa, ray_dir, t);
+    }
+    double roots[4];
+    for (int i = 0; i < nr; i++) {
+      roots[i] = (double)rt[i];
+      if (!polish_root(B, C, D, E, roots[i])) {
+        if (ctr) atomicAdd(ctr + kCntFbRoot, 1ull);
+        return intersect_f64_fallback_p<PN>(f, kind, first, cnt, P, pa, ray_dir, t);
+      }
+    }
+    for (int i = 0; i < nr; i++)
+      for (int j = i + 1; j < nr; j++)
+        if (fabs(roots[i] - roots[j]) < 1e-6) {
+          if (ctr) atomicAdd(ctr + kCntFbRoot, 1ull);
+          return intersect_f64_fallback_p<PN>(f, kind, first, cnt, P, pa, ray_dir, t);
+        }
+    const double r2 = r * r;
+    for (int i = 0; i < nr; i++) {
+      double root = roots[i];
+      if (fabs(root) < 1e-9) {
+        if (ctr) atomicAdd(ctr + kCntFbRoot, 1ull);
+        return intersect_f64_fallback_p<PN>(f, kind, first, cnt, P, pa, ray_dir, t);
+      }
+      if (root < 0) continue;
+      double px = x_in + root;
+      double e0 = f[fd] - pa[fd], e1 = f[ld] - pa[ld], e2 = cv - px;
+      double dd = e0 * e0 + e1 * e1 + e2 * e2;
+      if (fabs(dd - r2) < 1e-9) {
+        if (ctr) atomicAdd(ctr + kCntFbRoot, 1ull);
+        return intersect_f64_fallback_p<PN>(f, kind, first, cnt, P, pa, ray_dir, t);
+      }
+      if (dd < r2) xs[nx++] = px;
+    }
+  } else {
+    xs[0] = cv - sd;
+    xs[1] = cv + sd;
+    nx = 2;
+  }
+  int out = 0;
+  for (int i = 0; i < nx; i++) {
+    float pl[3];
+    pl[fd] = dxf;
+    pl[ld] = dyf;
+    pl[vc] = (float)(xs[i] - cv);
+    double p64[3];
+    p64[fd] = pa[fd];
+    p64[ld] = pa[ld];
+    p64[vc] = xs[i];
+    if (feasible_mixed(f, kind, first, cnt, P.pool, P.pool32, P.flag, pl, p64)) t[out++] = (xs[i] - pa[vc]) * inv_dir;
   }
   return out;
 }
@@ -198,16 +395,151 @@ struct TraceCtx {
   int64_t nwords;
 };
 
-template <int kThreads>
-__global__ void __launch_bounds__(kTraceThreads) k_trace(TraceCtx C, const int64_t* __restrict__ tile_off,
-                                                          const int32_t* __restrict__ tile_list) {
+// Wavefront ray tracing of one ray set, three kernel kinds:
+//  * k_cand: one CTA per 32x4 ray tile stages the tile's patch list in shared memory; for each
+//    patch a warp tests its 32 rays against the reference's candidate conditions (pixel window,
+//    bounding box, equatorial disc) and appends the surviving (ray, patch) pairs to a warp buffer
+//    split by patch type (spheres: atoms and probes; tori), flushed to global candidate lists
+//    with one atomic per flush;
+//  * k_isect<torus, mixed>: one thread per candidate pair, sphere and torus pairs in separate
+//    launches so that both run converged with their own register budget; hits are filed into
+//    the ray's slots of a slot-major hit store through a per-ray atomic counter;
+//  * k_fill: one CTA per tile loads each ray's hits, sorts them and performs the interval fill.
+constexpr int kWarpBuf = 256;
+
+__global__ void __launch_bounds__(kTraceThreads) k_cand(TraceCtx C, const int64_t* __restrict__ tile_off,
+                                                         const int32_t* __restrict__ tile_list, CandOut co) {
+  constexpr int kThreads = kTraceThreads;
   const GridDev& g = C.g;
   const RaySet& rs = C.rs;
   __shared__ double s_f[kChunk * NS_PATCH_F64];
-  __shared__ int s_i[kChunk * 3];
+  __shared__ int s_i[kChunk];
+  __shared__ int s_pid[kChunk];
   __shared__ int s_w[kChunk * 4];
-  __shared__ double s_hit[kHitCap * kThreads];
+  __shared__ int2 s_buf[kTileN][2][kWarpBuf];
+  const int64_t ntm = (rs.nb + kTileM - 1) / kTileM;
+  const int64_t tile = blockIdx.x;
+  const int64_t tm = tile % ntm, tn = tile / ntm;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t m = tm * kTileM + lane;
+  const int64_t n = tn * kTileN + warp;
+  const bool valid = (m < rs.nb) && (n < rs.na);
+  const int tid = threadIdx.x;
+  const int32_t rid = (int32_t)(n * rs.nb + m);
+  double pa[3];
+  pa[rs.fd] = gcoord(g, rs.fd, valid ? m : 0) + rs.delta;
+  pa[rs.ld] = gcoord(g, rs.ld, n < rs.na ? n : 0) + rs.delta;
+  pa[rs.vc] = gcoord(g, rs.vc, 0) + rs.delta;
+  int fill[2] = {0, 0};
+  auto flush = [&](int ty) {
+    int cnt = fill[ty];
+    unsigned long long base = 0;
+    if (lane == 0 && cnt) base = atomicAdd(co.count + ty, (unsigned long long)cnt);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    int2* dst = ty ? co.tor : co.sph;
+    for (int i = lane; i < cnt; i += 32) {
+      if ((int64_t)(base + i) < co.cap) dst[base + i] = s_buf[warp][ty][i];
+    }
+    if (lane == 0 && cnt && (int64_t)(base + cnt) > co.cap) atomicExch(C.out.error_flag, 6);
+    __syncwarp();
+    fill[ty] = 0;
+  };
+  const int64_t beg = tile_off[tile], end = tile_off[tile + 1];
+  for (int64_t base = beg; base < end; base += kChunk) {
+    int cnt = (int)((end - base) < kChunk ? (end - base) : kChunk);
+    __syncthreads();
+    for (int e = tid; e < cnt * 4; e += kThreads) {
+      int q = e >> 2, k = e & 3;
+      int64_t pid = tile_list[base + q];
+      s_f[q * NS_PATCH_F64 + k] = __ldg(C.P.f64 + (int64_t)NS_PATCH_F64 * pid + k);
+    }
+    for (int q = tid; q < cnt; q += kThreads) {
+      int64_t pid = tile_list[base + q];
+      s_pid[q] = (int)pid;
+      int kind = C.P.i32[NS_PATCH_I32 * pid];
+      s_i[q] = (kind == NS_EDGE_REG || kind == NS_EDGE_SING) ? 1 : 0;
+      const int32_t* w = C.P.win + 6 * pid;
+      s_w[4 * q + 0] = w[rs.fd];
+      s_w[4 * q + 1] = w[3 + rs.fd];
+      s_w[4 * q + 2] = w[rs.ld];
+      s_w[4 * q + 3] = w[3 + rs.ld];
+    }
+    __syncthreads();
+    for (int q = 0; q < cnt; q++) {
+      bool pass = valid && m >= s_w[4 * q] && m <= s_w[4 * q + 1] && n >= s_w[4 * q + 2] && n <= s_w[4 * q + 3] &&
+                  candidate(s_f + q * NS_PATCH_F64, rs, pa);
+      unsigned mask = __ballot_sync(0xffffffffu, pass);
+      if (!mask) continue;
+      const int ty = s_i[q];
+      if (pass) s_buf[warp][ty][fill[ty] + __popc(mask & ((1u << lane) - 1u))] = make_int2(rid, s_pid[q]);
+      fill[ty] += __popc(mask);
+      __syncwarp();
+      if (fill[ty] > kWarpBuf - 32) flush(ty);
+    }
+  }
+  __syncwarp();
+  flush(0);
+  flush(1);
+}
 
+// One thread per candidate pair of one type: intersection, feasibility, hit filing.
+template <int PN, bool kTorus, bool kMixed>
+__global__ void __launch_bounds__(256) k_isect(TraceCtx C, CandOut co, HitStore hs) {
+  constexpr int fd = Ax<PN>::fd, ld = Ax<PN>::ld, vc = Ax<PN>::vc;
+  const GridDev& g = C.g;
+  const RaySet& rs = C.rs;
+  const int64_t ncand = *(co.count + (kTorus ? 1 : 0));
+  const int2* list = kTorus ? co.tor : co.sph;
+  const int64_t nlim = ncand < co.cap ? ncand : co.cap;
+  const double ray_dir = gcoord(g, vc, g.n[vc] - 1) - gcoord(g, vc, 0);
+  const double inv_dir = 1.0 / ray_dir;
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < nlim; c += (int64_t)gridDim.x * blockDim.x) {
+    int2 e = list[c];
+    const int64_t rid = e.x, pid = e.y;
+    const int64_t m = rid % rs.nb, n = rid / rs.nb;
+    double pa[3];
+    pa[fd] = gcoord(g, fd, m) + rs.delta;
+    pa[ld] = gcoord(g, ld, n) + rs.delta;
+    pa[vc] = gcoord(g, vc, 0) + rs.delta;
+    double f[NS_PATCH_F64];
+    const double* src = C.P.f64 + (int64_t)NS_PATCH_F64 * pid;
+    constexpr int nf = kTorus ? 18 : 4;
+#pragma unroll
+    for (int k = 0; k < nf; k++) f[k] = __ldg(src + k);
+    const int32_t* ir = C.P.i32 + NS_PATCH_I32 * pid;
+    const int kind = ir[0], first = ir[1], cnt = ir[2];
+    double t[4];
+    int k;
+    if (kMixed)
+      k = intersect_mixed<PN, kTorus>(f, kind, first, cnt, C.P, pa, ray_dir, inv_dir, t, C.out.counters);
+    else
+      k = intersect_f64_p<PN, kTorus>(f, kind, first, cnt, C.P, pa, ray_dir, t);
+    if (k == 0) continue;
+    int pos = atomicAdd(hs.cnt + rid, k);
+    for (int i = 0; i < k; i++)
+      if (pos + i < kHitCap) hs.t[(int64_t)(pos + i) * hs.nrays + rid] = t[i];
+  }
+}
+
+template <int PN>
+void launch_isect(const TraceCtx& C, const CandOut& co, const HitStore& hs, int precision, cudaStream_t s) {
+  const int ig = 148 * 16;
+  if (precision == 1) {
+    k_isect<PN, false, true><<<ig, 256, 0, s>>>(C, co, hs);
+    k_isect<PN, true, true><<<ig, 256, 0, s>>>(C, co, hs);
+  } else {
+    k_isect<PN, false, false><<<ig, 256, 0, s>>>(C, co, hs);
+    k_isect<PN, true, false><<<ig, 256, 0, s>>>(C, co, hs);
+  }
+}
+
+// One CTA per 32x4 ray tile: loads, sorts and pairs the hits of its rays and performs the
+// interval fill (status runs, insideness bits, pair store, volume).
+__global__ void __launch_bounds__(kTraceThreads) k_fill(TraceCtx C, HitStore hs) {
+  constexpr int kThreads = kTraceThreads;
+  const GridDev& g = C.g;
+  const RaySet& rs = C.rs;
+  __shared__ double s_hit[kHitCap * kThreads];
   const int64_t ntm = (rs.nb + kTileM - 1) / kTileM;
   const int64_t tile = blockIdx.x;
   const int64_t tm = tile % ntm, tn = tile / ntm;
@@ -217,46 +549,18 @@ __global__ void __launch_bounds__(kTraceThreads) k_trace(TraceCtx C, const int64
   const bool valid = (m < rs.nb) && (n < rs.na);
   const int tid = threadIdx.x;
   double* col = s_hit + tid;
-
-  double pa[3], dir[3] = {0., 0., 0.};
-  pa[rs.fd] = gcoord(g, rs.fd, valid ? m : 0) + rs.delta;
-  pa[rs.ld] = gcoord(g, rs.ld, valid ? n : 0) + rs.delta;
-  pa[rs.vc] = gcoord(g, rs.vc, 0) + rs.delta;
-  const double ray_dir = gcoord(g, rs.vc, g.n[rs.vc] - 1) - gcoord(g, rs.vc, 0);
-  dir[rs.vc] = ray_dir;
-
-  int nh = 0;
-  bool ovf = false;
-  const int64_t beg = tile_off[tile], end = tile_off[tile + 1];
-  for (int64_t base = beg; base < end; base += kChunk) {
-    int cnt = (int)((end - base) < kChunk ? (end - base) : kChunk);
-    __syncthreads();
-    for (int e = tid; e < cnt * NS_PATCH_F64; e += kThreads) {
-      int q = e / NS_PATCH_F64, k = e - q * NS_PATCH_F64;
-      int64_t pid = tile_list[base + q];
-      s_f[e] = __ldg(C.P.f64 + (int64_t)NS_PATCH_F64 * pid + k);
+  int hc = valid ? hs.cnt[n * rs.nb + m] : 0;
+  bool ovf = hc > kHitCap;
+  int nh = ovf ? 0 : hc;
+  for (int i = 0; i < nh; i++) col[i * kThreads] = hs.t[(int64_t)i * hs.nrays + n * rs.nb + m];
+  for (int i = 1; i < nh; i++) {
+    double v = col[i * kThreads];
+    int j = i;
+    while (j > 0 && col[(j - 1) * kThreads] > v) {
+      col[j * kThreads] = col[(j - 1) * kThreads];
+      j--;
     }
-    for (int q = tid; q < cnt; q += kThreads) {
-      int64_t pid = tile_list[base + q];
-      s_i[3 * q + 0] = C.P.i32[NS_PATCH_I32 * pid + 0];
-      s_i[3 * q + 1] = C.P.i32[NS_PATCH_I32 * pid + 1];
-      s_i[3 * q + 2] = C.P.i32[NS_PATCH_I32 * pid + 2];
-      const int32_t* w = C.P.win + 6 * pid;
-      s_w[4 * q + 0] = w[rs.fd];
-      s_w[4 * q + 1] = w[3 + rs.fd];
-      s_w[4 * q + 2] = w[rs.ld];
-      s_w[4 * q + 3] = w[3 + rs.ld];
-    }
-    __syncthreads();
-    if (!valid || ovf) continue;
-    for (int q = 0; q < cnt; q++) {
-      if (m < s_w[4 * q] || m > s_w[4 * q + 1] || n < s_w[4 * q + 2] || n > s_w[4 * q + 3]) continue;
-      double t[4];
-      int k = ray_patch_f64(s_f + q * NS_PATCH_F64, s_i[3 * q], s_i[3 * q + 1], s_i[3 * q + 2], C.P, rs, pa, dir,
-                            ray_dir, t);
-      for (int i = 0; i < k; i++)
-        if (!insert_hit(col, kThreads, nh, kHitCap, t[i])) ovf = true;
-    }
+    col[j * kThreads] = v;
   }
   const int64_t rid = n * rs.nb + m;
   if (valid && ovf) {
@@ -521,26 +825,36 @@ cudaError_t launch_windows(const PatchDev& P, int32_t* win, const GridDev& g, cu
   return cudaGetLastError();
 }
 
-cudaError_t launch_bin_count(const PatchDev& P, const GridDev& g, const RaySet& rs, int32_t* tile_cnt,
-                             cudaStream_t s) {
+cudaError_t launch_pool32(const PatchDev& P, float4* pool32, cudaStream_t s) {
   if (P.n == 0) return cudaSuccess;
-  k_bin<<<(unsigned)((P.n + 255) / 256), 256, 0, s>>>(P, g, rs, tile_cnt, nullptr, nullptr, nullptr);
+  k_pool32<<<(unsigned)((P.n + 255) / 256), 256, 0, s>>>(P, pool32);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_bin_count(const PatchDev& P, const GridDev& g, const RaySet& rs, int32_t* tile_cnt,
+                             unsigned long long* area, cudaStream_t s) {
+  if (P.n == 0) return cudaSuccess;
+  k_bin<<<(unsigned)((P.n + 255) / 256), 256, 0, s>>>(P, g, rs, tile_cnt, nullptr, nullptr, nullptr, area);
   return cudaGetLastError();
 }
 
 cudaError_t launch_bin_fill(const PatchDev& P, const GridDev& g, const RaySet& rs, const int64_t* tile_off,
                             int32_t* tile_cursor, int32_t* tile_list, cudaStream_t s) {
   if (P.n == 0) return cudaSuccess;
-  k_bin<<<(unsigned)((P.n + 255) / 256), 256, 0, s>>>(P, g, rs, nullptr, tile_off, tile_cursor, tile_list);
+  k_bin<<<(unsigned)((P.n + 255) / 256), 256, 0, s>>>(P, g, rs, nullptr, tile_off, tile_cursor, tile_list, nullptr);
   return cudaGetLastError();
 }
 
 cudaError_t launch_trace(const PatchDev& P, const GridDev& g, const RaySet& rs, const int64_t* tile_off,
-                         const int32_t* tile_list, const TraceOut& out, int precision, cudaStream_t s) {
-  (void)precision;
+                         const int32_t* tile_list, const TraceOut& out, const CandOut& co, const HitStore& hs,
+                         int precision, cudaStream_t s) {
   TraceCtx C{P, g, rs, out, words_of(g)};
   int64_t ntiles = ((rs.nb + kTileM - 1) / kTileM) * ((rs.na + kTileN - 1) / kTileN);
-  k_trace<kTraceThreads><<<(unsigned)ntiles, kTraceThreads, 0, s>>>(C, tile_off, tile_list);
+  k_cand<<<(unsigned)ntiles, kTraceThreads, 0, s>>>(C, tile_off, tile_list, co);
+  if (rs.panel == 0) launch_isect<0>(C, co, hs, precision, s);
+  else if (rs.panel == 1) launch_isect<1>(C, co, hs, precision, s);
+  else launch_isect<2>(C, co, hs, precision, s);
+  k_fill<<<(unsigned)ntiles, kTraceThreads, 0, s>>>(C, hs);
   return cudaGetLastError();
 }
 

@@ -72,3 +72,27 @@ def test_single_sphere_volume(native_lib):
     exact_a = 4.0 * np.pi * 1.7 ** 2
     assert abs(vol - exact_v) / exact_v < 0.02
     assert abs(area - exact_a) / exact_a < 0.05
+
+
+@pytest.mark.parametrize("n_atoms,seed,scale,perfil", [(327, 1, 2.0, 70.0), (1000, 3, 3.0, 70.0)])
+def test_mixed_precision_matches_oracle(n_atoms, seed, scale, perfil, native_lib, oracle_mod):
+    """Mixed precision (FP32 bulk, FP64 polish): same hit counts as the FP64 oracle, hit positions
+    within 1e-5 A, status map and insideness bits equal except at near-node hits."""
+    import compare
+    ds, surf = _setup(n_atoms, seed, scale, perfil)
+    surf.precision = "mixed"
+    vol = surf.getSurf(True, True, 10.0, keep_hits=True)
+    area = surf.triangulateSurface()
+    ref = oracle_mod.run(ds.grid, surf.patches, cav_vol=10.0)
+    g = ds.grid
+    ray_len = ((g.nx - 1) * g.side, (g.nx - 1) * g.side, (g.nz - 1) * g.side, (g.ny - 1) * g.side)
+    worst = 0.0
+    for s in range(4):
+        cnt_g, val_g = surf.hits(s)
+        cnt_o, val_o = oracle_mod.ray_hits(ref, s)
+        assert np.array_equal(cnt_g, cnt_o), f"ray set {s}: {(cnt_g != cnt_o).sum()} rays with other hit counts"
+        if len(val_o):
+            worst = max(worst, float(np.abs(val_g - val_o).max()) * ray_len[s])
+    assert worst <= 1e-5, f"max hit error {worst} A"
+    figs = compare.compare_surface(surf, ds, ref, rel_tol=1e-9, vert_tol=1e-5)
+    print(f"mixed n={n_atoms}: max hit error {worst:.3e} A, {figs}")
