@@ -120,6 +120,21 @@ int nsg_download_cavities(nsg_ctx* ctx, double* sizes, int32_t* filled);
 /* Sorted hit parameters per ray of one ray set (tests). */
 int nsg_download_hits(nsg_ctx* ctx, int ray_set, int32_t* counts, double* dst, int64_t dst_capacity);
 
+/* ---- allocation-free status ray cast ----
+ * No counterpart in the reference: an addition for callers that may not allocate device memory
+ * (a host framework that owns every device allocation through its own pool, or a process whose
+ * memory is fixed after start-up).  Status map (flat int32, k*ny*nx + j*nx + i; INSIDE /
+ * TEMPORARY_OUT as nsg_raycast with NSG_RAYCAST_STATUS writes it) and status-ray volume of a grid
+ * from a patch set, all in device memory the caller owns.  Scratch is one fixed file-scope device
+ * array (16.5 MiB): at most 65536 status rays (ny * nz) and 32 hits per ray; larger grids return
+ * NSG_ERR_CAPACITY before any launch, a ray with more hits returns NSG_ERR_CAPACITY after the
+ * call.  Allocates nothing.  The first call on each device (with that device current) looks up
+ * the scratch address and must come before any stream capture.  Calls that overlap on the GPU
+ * share the scratch and race: serialise them.  Synchronises `stream` before returning. */
+int nsg_status_noalloc(const NsGrid* grid, int64_t n_patches, const double* d_f64, const int32_t* d_i32,
+                       const double* d_pool, const int8_t* d_pool_flag, double probe_radius, int32_t* d_status,
+                       double* volume, void* stream);
+
 /* ---- instrumentation ---- */
 int nsg_stats(nsg_ctx* ctx, int64_t* out, int n);
 double nsg_volume(nsg_ctx* ctx);
