@@ -94,6 +94,23 @@ int nsg_upload_patches(nsg_ctx* ctx, int64_t n, const double* f64, const int32_t
 int nsg_bind_patches_device(nsg_ctx* ctx, int64_t n, const double* f64, const int32_t* i32, int64_t n_pool,
                             const double* pool, const int8_t* pool_flag, double probe_radius);
 
+/* ---- batches (many structures, each on its own grid, in the same launches) ----
+ * No single counterpart in the reference, which builds one Surface per structure; a batch of n
+ * runs the same per-structure pipeline (one getSurf + triangulateSurface each) with every kernel
+ * launch covering all n structures.  nsg_set_batch replaces the grid set by nsg_set_grid (which
+ * is a batch of one).  Cavity detection and the dense status map stay single-structure calls;
+ * insideness bits download concatenated (structure b's words follow those of b-1), and the mesh
+ * arrays hold all structures' vertices (analytic ones of every structure, then the midpoint
+ * ones) with batch-wide indices. */
+int nsg_set_batch(nsg_ctx* ctx, int32_t n, const NsGrid* grids);
+/* Concatenated patch sets: structure b owns patches [patch_off[b], patch_off[b+1]) and pool
+ * entries [pool_off[b], pool_off[b+1]); pool indices inside each record are local to its
+ * structure (as nsg_patchset_export writes them). */
+int nsg_upload_batch(nsg_ctx* ctx, const int64_t* patch_off, const double* f64, const int32_t* i32,
+                     const int64_t* pool_off, const double* pool, const int8_t* pool_flag, double probe_radius);
+/* Per-structure volume (last nsg_raycast) and area (last nsg_triangulate); either may be NULL. */
+int nsg_batch_results(nsg_ctx* ctx, double* volumes, double* areas);
+
 /* ---- the hot path ---- */
 /* Ray casting of Surface::getSurf: getPatchIntersectionData (src/ConnollySurface.cpp:4319-4590),
  * pixel binning and sort (src/Surface.cpp:4766-5095), setVerticesAndGridsWithIntersectionData

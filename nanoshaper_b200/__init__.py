@@ -7,6 +7,7 @@ from .surface import (  # noqa: F401
     NanoShaper,
     PatchSet,
     Surface,
+    SurfaceBatch,
     SurfaceFactory,
     build_ses_patches,
     read_xyzr,

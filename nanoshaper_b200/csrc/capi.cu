@@ -68,9 +68,18 @@ struct nsg_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
-  NsGrid grid{};
-  nsg::GridDev gd{};
+  NsGrid grid{};  // first structure's grid
   bool has_grid = false;
+  // batch layout: one StructDev per structure (a single structure is a batch of one)
+  int32_t nstruct = 0;
+  std::vector<NsGrid> grids;
+  std::vector<nsg::StructDev> sd;
+  DevBuf d_sd, d_patch_struct, d_tile_struct[3], d_ray_base[4], d_mc_base, d_row_base;
+  int64_t tiles_tot[3] = {0, 0, 0}, rays_tot[4] = {0, 0, 0, 0}, mc_tot = 0, rows_tot = 0, words_tot = 0;
+  int32_t patch_nstruct = 0;  // structures the uploaded patches belong to
+  bool patch_struct_valid = false;
+  std::vector<double> volumes, areas;
+  DevBuf vol_struct, area_struct;
   // patches
   int64_t np = 0, npool = 0;
   double probe = 1.4;
@@ -85,8 +94,8 @@ struct nsg_ctx {
   DevBuf tile_cnt[3], tile_off[3], tile_list[3], bin_area;
   int64_t win_area[3] = {0, 0, 0};
   // wavefront tracing: candidate lists and the slot-major hit store
-  DevBuf cand_sph, cand_tor, hit_t, hit_cnt;
-  int64_t cand_cap = 0;
+  DevBuf cand_sph, cand_tor, hit_t, hit_cnt, def_sph, def_tor;
+  int64_t cand_cap = 0, def_cap = 0;
   // trace outputs
   DevBuf status, bits, vol_ray[4];
   DevBuf pairs, ray_pair_off, ray_pair_cnt, cursors, ovf_rays[4], ovf_scratch, err;
@@ -140,6 +149,109 @@ nsg::PatchDev patch_dev(nsg_ctx* c) {
 }
 
 int64_t nwords_of(const NsGrid& g) { return ((g.nx + 31) >> 5) * g.ny * g.nz; }
+
+nsg::GridDev grid_dev(const NsGrid& g) {
+  nsg::GridDev d{};
+  d.n[0] = g.nx; d.n[1] = g.ny; d.n[2] = g.nz;
+  d.mn[0] = g.xmin; d.mn[1] = g.ymin; d.mn[2] = g.zmin;
+  d.mx[0] = g.xmax; d.mx[1] = g.ymax; d.mx[2] = g.zmax;
+  d.scale = g.scale; d.side = g.side; d.hside = g.hside;
+  return d;
+}
+
+nsg::BatchDev batch_dev(nsg_ctx* c) {
+  nsg::BatchDev B{};
+  B.n = c->nstruct;
+  B.s = c->d_sd.as<nsg::StructDev>();
+  B.patch_struct = c->d_patch_struct.as<int32_t>();
+  for (int i = 0; i < 3; i++) B.tile_struct[i] = c->d_tile_struct[i].as<int32_t>();
+  for (int i = 0; i < 4; i++) B.ray_base[i] = c->d_ray_base[i].as<int64_t>();
+  B.mc_base = c->d_mc_base.as<int64_t>();
+  B.row_base = c->d_row_base.as<int64_t>();
+  return B;
+}
+
+template <class T>
+cudaError_t upload_vec(DevBuf& d, const std::vector<T>& h, cudaStream_t s) {
+  cudaError_t e = d.ensure(std::max<size_t>(h.size(), 1) * sizeof(T));
+  if (e != cudaSuccess || h.empty()) return e;
+  return cudaMemcpyAsync(d.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, s);
+}
+
+// Host and device layout of the batch: per-structure bases of tiles, rays, MC ray ordinals, cube
+// rows and bit words, and the reverse maps tile -> structure.
+int batch_layout(nsg_ctx* c, const NsGrid* grids, int32_t n) {
+  std::vector<nsg::StructDev> sd(n);
+  std::vector<int64_t> rb[4], mcb(n + 1), rowb(n + 1);
+  std::vector<int32_t> ts[3];
+  for (int i = 0; i < 4; i++) rb[i].resize(n + 1);
+  int64_t tiles[3] = {0, 0, 0}, rays[4] = {0, 0, 0, 0}, mc = 0, rows = 0, words = 0;
+  for (int32_t b = 0; b < n; b++) {
+    const NsGrid& G = grids[b];
+    if (G.nx < 3 || G.ny < 3 || G.nz < 3) return fail(NSG_ERR_ARG, "grid must have at least 3 nodes per axis");
+    if (G.nx * G.ny * G.nz >= (int64_t)1 << 31) return fail(NSG_ERR_ARG, "grid larger than 2^31 nodes");
+    nsg::StructDev& S = sd[b];
+    S.g = grid_dev(G);
+    S.nwords = nwords_of(G);
+    S.word_base = words;
+    words += S.nwords;
+    for (int panel = 0; panel < 3; panel++) {
+      nsg::RaySet rs = nsg::make_ray_set(panel == 0 ? 0 : panel + 1, S.g);
+      int64_t nt = ((rs.nb + nsg::kTileM - 1) / nsg::kTileM) * ((rs.na + nsg::kTileN - 1) / nsg::kTileN);
+      S.tile_base[panel] = tiles[panel];
+      ts[panel].insert(ts[panel].end(), nt, b);
+      tiles[panel] += nt;
+    }
+    for (int set = 0; set < 4; set++) {
+      nsg::RaySet rs = nsg::make_ray_set(set, S.g);
+      S.ray_base[set] = rb[set][b] = rays[set];
+      rays[set] += rs.nb * rs.na;
+    }
+    S.mc_base = mcb[b] = mc;
+    mc += G.nz * G.ny + G.ny * G.nx + G.nz * G.nx;
+    S.row_base = rowb[b] = rows;
+    rows += (G.ny - 2) * (G.nz - 2);
+    for (int d = 0; d < 3; d++) {
+      S.ray_dir[d] = (S.g.mn[d] + (double)(S.g.n[d] - 1) * S.g.side) - (S.g.mn[d] + 0.0 * S.g.side);
+      S.inv_dir[d] = 1.0 / S.ray_dir[d];
+    }
+  }
+  for (int i = 0; i < 4; i++) {
+    rb[i][n] = rays[i];
+    if (rays[i] >= (int64_t)1 << 31) return fail(NSG_ERR_CAPACITY, "more than 2^31 rays in one ray set of a batch");
+  }
+  mcb[n] = mc;
+  rowb[n] = rows;
+  CK(upload_vec(c->d_sd, sd, c->stream));
+  for (int i = 0; i < 3; i++) CK(upload_vec(c->d_tile_struct[i], ts[i], c->stream));
+  for (int i = 0; i < 4; i++) CK(upload_vec(c->d_ray_base[i], rb[i], c->stream));
+  CK(upload_vec(c->d_mc_base, mcb, c->stream));
+  CK(upload_vec(c->d_row_base, rowb, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->nstruct = n;
+  c->grids.assign(grids, grids + n);
+  c->sd = sd;
+  c->grid = grids[0];
+  for (int i = 0; i < 3; i++) c->tiles_tot[i] = tiles[i];
+  for (int i = 0; i < 4; i++) c->rays_tot[i] = rays[i];
+  c->mc_tot = mc;
+  c->rows_tot = rows;
+  c->words_tot = words;
+  c->has_grid = true;
+  c->have_status = c->have_bits = false;
+  c->volumes.assign(n, 0.0);
+  c->areas.assign(n, 0.0);
+  return NSG_OK;
+}
+
+// Structure index of every patch: all 0 for a single structure.
+int ensure_patch_struct(nsg_ctx* c) {
+  if (c->patch_struct_valid) return NSG_OK;
+  CK(c->d_patch_struct.ensure(std::max<int64_t>(c->np, 1) * sizeof(int32_t)));
+  CK(cudaMemsetAsync(c->d_patch_struct.p, 0, std::max<int64_t>(c->np, 1) * sizeof(int32_t), c->stream));
+  c->patch_struct_valid = true;
+  return NSG_OK;
+}
 
 // Stage ids of the per-stage kernel timers.
 enum { kStageBin = 0, kStageTrace = 1, kStageOverflow = 2, kStageCavity = 3, kStageVertex = 4, kStageMC = 5,
@@ -207,8 +319,9 @@ int reduce_sum(nsg_ctx* c, const double* in, int64_t n, double* host_out) {
 }
 
 int bin_panel(nsg_ctx* c, int panel) {
-  nsg::RaySet rs = nsg::make_ray_set(panel == 0 ? 0 : panel + 1, c->gd);
-  int64_t ntiles = ((rs.nb + nsg::kTileM - 1) / nsg::kTileM) * ((rs.na + nsg::kTileN - 1) / nsg::kTileN);
+  const int set = panel == 0 ? 0 : panel + 1;
+  const int64_t ntiles = c->tiles_tot[panel];
+  const nsg::BatchDev B = batch_dev(c);
   CK(c->tile_cnt[panel].ensure((ntiles + 1) * sizeof(int32_t)));
   CK(c->tile_off[panel].ensure((ntiles + 1) * sizeof(int64_t)));
   CK(cudaMemsetAsync(c->tile_cnt[panel].p, 0, (ntiles + 1) * sizeof(int32_t), c->stream));
@@ -216,7 +329,7 @@ int bin_panel(nsg_ctx* c, int panel) {
   CK(c->bin_area.ensure(3 * sizeof(unsigned long long)));
   unsigned long long* area = c->bin_area.as<unsigned long long>() + panel;
   CK(cudaMemsetAsync(area, 0, sizeof(unsigned long long), c->stream));
-  LAUNCH(nsg::launch_bin_count(P, c->gd, rs, c->tile_cnt[panel].as<int32_t>(), area, c->stream));
+  LAUNCH(nsg::launch_bin_count(P, B, set, c->tile_cnt[panel].as<int32_t>(), area, c->stream));
   int64_t total = 0;
   int rc = scan_counts(c, c->tile_cnt[panel].as<int32_t>(), ntiles, c->tile_off[panel].as<int64_t>(), &total);
   if (rc) return rc;
@@ -226,7 +339,7 @@ int bin_panel(nsg_ctx* c, int panel) {
   c->win_area[panel] = (int64_t)a_host;
   CK(c->tile_list[panel].ensure(std::max<int64_t>(total, 1) * sizeof(int32_t)));
   CK(cudaMemsetAsync(c->tile_cnt[panel].p, 0, (ntiles + 1) * sizeof(int32_t), c->stream));
-  LAUNCH(nsg::launch_bin_fill(P, c->gd, rs, c->tile_off[panel].as<int64_t>(), c->tile_cnt[panel].as<int32_t>(),
+  LAUNCH(nsg::launch_bin_fill(P, B, set, c->tile_off[panel].as<int64_t>(), c->tile_cnt[panel].as<int32_t>(),
                           c->tile_list[panel].as<int32_t>(), c->stream));
   return NSG_OK;
 }
@@ -307,7 +420,7 @@ int nsg_ctx_destroy(nsg_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   DevBuf* bufs[] = {&c->f64, &c->i32, &c->pool, &c->flag, &c->win, &c->pool32, &c->counters, &c->bin_area,
-                    &c->cand_sph, &c->cand_tor, &c->hit_t, &c->hit_cnt, &c->status, &c->bits, &c->pairs,
+                    &c->cand_sph, &c->cand_tor, &c->def_sph, &c->def_tor, &c->hit_t, &c->hit_cnt, &c->status, &c->bits, &c->pairs,
                     &c->ray_pair_off, &c->ray_pair_cnt, &c->cursors, &c->ovf_scratch, &c->err, &c->hits,
                     &c->labels, &c->is_root, &c->sruns, &c->srun_off, &c->srun_cnt, &c->fr_cnt, &c->fr_off,
                     &c->fruns, &c->frow, &c->roots, &c->cc_count, &c->cc_desc, &c->cc_label_of,
@@ -316,6 +429,10 @@ int nsg_ctx_destroy(nsg_ctx* c) {
                     &c->act_mid, &c->tri_cnt, &c->tri_off, &c->tris, &c->cube_area, &c->red_out, &c->temp};
   for (DevBuf* b : bufs) b->release();
   for (int i = 0; i < 3; i++) { c->tile_cnt[i].release(); c->tile_off[i].release(); c->tile_list[i].release(); }
+  c->d_sd.release(); c->d_patch_struct.release(); c->d_mc_base.release(); c->d_row_base.release();
+  c->vol_struct.release(); c->area_struct.release();
+  for (int i = 0; i < 3; i++) c->d_tile_struct[i].release();
+  for (int i = 0; i < 4; i++) c->d_ray_base[i].release();
   for (int i = 0; i < 4; i++) {
     c->vol_ray[i].release(); c->ovf_rays[i].release(); c->ray_hit_off[i].release(); c->ray_hit_cnt[i].release();
   }
@@ -341,16 +458,15 @@ int nsg_set_stream(nsg_ctx* c, void* stream) {
 
 int nsg_set_grid(nsg_ctx* c, const NsGrid* g) {
   if (!c || !g) return NSG_ERR_ARG;
-  if (g->nx < 3 || g->ny < 3 || g->nz < 3) return fail(NSG_ERR_ARG, "grid must have at least 3 nodes per axis");
-  if (g->nx * g->ny * g->nz >= (int64_t)1 << 31) return fail(NSG_ERR_ARG, "grid larger than 2^31 nodes");
-  c->grid = *g;
-  c->gd.n[0] = g->nx; c->gd.n[1] = g->ny; c->gd.n[2] = g->nz;
-  c->gd.mn[0] = g->xmin; c->gd.mn[1] = g->ymin; c->gd.mn[2] = g->zmin;
-  c->gd.mx[0] = g->xmax; c->gd.mx[1] = g->ymax; c->gd.mx[2] = g->zmax;
-  c->gd.scale = g->scale; c->gd.side = g->side; c->gd.hside = g->hside;
-  c->has_grid = true;
-  c->have_status = c->have_bits = false;
-  return NSG_OK;
+  CK(cudaSetDevice(c->device));
+  return batch_layout(c, g, 1);
+}
+
+// A batch of structures, each on its own grid; patches follow with nsg_upload_batch.
+int nsg_set_batch(nsg_ctx* c, int32_t n, const NsGrid* grids) {
+  if (!c || n < 1 || !grids) return NSG_ERR_ARG;
+  CK(cudaSetDevice(c->device));
+  return batch_layout(c, grids, n);
 }
 
 static int upload_common(nsg_ctx* c, int64_t n, int64_t npool, double probe) {
@@ -360,6 +476,8 @@ static int upload_common(nsg_ctx* c, int64_t n, int64_t npool, double probe) {
   CK(c->win.ensure(std::max<int64_t>(n, 1) * 6 * sizeof(int32_t)));
   c->has_patches = true;
   c->pool32_valid = false;
+  c->patch_nstruct = 1;
+  c->patch_struct_valid = false;
   return NSG_OK;
 }
 
@@ -384,6 +502,65 @@ int nsg_upload_patches(nsg_ctx* c, int64_t n, const double* f64, const int32_t* 
   return upload_common(c, n, npool, probe);
 }
 
+// Patch sets of the structures of a batch, concatenated: structure b owns patches
+// [patch_off[b], patch_off[b+1]) and pool entries [pool_off[b], pool_off[b+1]); the pool indices in
+// each patch record are local to its structure's pool.
+int nsg_upload_batch(nsg_ctx* c, const int64_t* patch_off, const double* f64, const int32_t* i32,
+                     const int64_t* pool_off, const double* pool, const int8_t* pool_flag, double probe) {
+  if (!c || !patch_off || !pool_off) return NSG_ERR_ARG;
+  if (c->nstruct < 1) return fail(NSG_ERR_STATE, "nsg_set_batch must come first");
+  const int32_t nb = c->nstruct;
+  if (patch_off[0] != 0 || pool_off[0] != 0) return fail(NSG_ERR_ARG, "offsets must start at 0");
+  for (int32_t b = 0; b < nb; b++)
+    if (patch_off[b + 1] < patch_off[b] || pool_off[b + 1] < pool_off[b])
+      return fail(NSG_ERR_ARG, "offsets must be non-decreasing");
+  const int64_t n = patch_off[nb], npool = pool_off[nb];
+  if ((n > 0 && (!f64 || !i32)) || (npool > 0 && (!pool || !pool_flag))) return NSG_ERR_ARG;
+  if (n >= (int64_t)1 << 31 || npool >= (int64_t)1 << 31) return fail(NSG_ERR_CAPACITY, "more than 2^31 patches");
+  std::vector<int32_t> gi32(i32, i32 + n * NS_PATCH_I32);
+  std::vector<int32_t> ps(std::max<int64_t>(n, 1), 0);
+  for (int32_t b = 0; b < nb; b++)
+    for (int64_t p = patch_off[b]; p < patch_off[b + 1]; p++) {
+      int32_t* r = gi32.data() + NS_PATCH_I32 * p;
+      if (r[1] < 0 || r[2] < 0 || r[1] + (int64_t)r[2] > pool_off[b + 1] - pool_off[b])
+        return fail(NSG_ERR_ARG, "patch pool range outside its structure's pool");
+      r[1] += (int32_t)pool_off[b];
+      ps[p] = b;
+    }
+  CK(cudaSetDevice(c->device));
+  CK(c->f64.ensure(std::max<int64_t>(n, 1) * NS_PATCH_F64 * sizeof(double)));
+  CK(c->i32.ensure(std::max<int64_t>(n, 1) * NS_PATCH_I32 * sizeof(int32_t)));
+  CK(c->pool.ensure(std::max<int64_t>(npool, 1) * 4 * sizeof(double)));
+  CK(c->flag.ensure(std::max<int64_t>(npool, 1)));
+  if (n) {
+    CK(cudaMemcpyAsync(c->f64.p, f64, n * NS_PATCH_F64 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->i32.p, gi32.data(), n * NS_PATCH_I32 * sizeof(int32_t), cudaMemcpyHostToDevice,
+                       c->stream));
+  }
+  if (npool) {
+    CK(cudaMemcpyAsync(c->pool.p, pool, npool * 4 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->flag.p, pool_flag, npool, cudaMemcpyHostToDevice, c->stream));
+  }
+  CK(upload_vec(c->d_patch_struct, ps, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->ext_f64 = nullptr; c->ext_i32 = nullptr; c->ext_pool = nullptr; c->ext_flag = nullptr;
+  int rc = upload_common(c, n, npool, probe);
+  if (rc) return rc;
+  c->patch_nstruct = nb;
+  c->patch_struct_valid = true;
+  return NSG_OK;
+}
+
+// Per-structure volume and area of the last ray cast / triangulation of the batch.
+int nsg_batch_results(nsg_ctx* c, double* volumes, double* areas) {
+  if (!c || c->nstruct < 1) return NSG_ERR_ARG;
+  for (int32_t b = 0; b < c->nstruct; b++) {
+    if (volumes) volumes[b] = c->volumes[b];
+    if (areas) areas[b] = c->areas[b];
+  }
+  return NSG_OK;
+}
+
 // Binds patch arrays that already live in device memory (no copy); they must stay valid until
 // the next bind/upload or the context's destruction.
 int nsg_bind_patches_device(nsg_ctx* c, int64_t n, const double* f64, const int32_t* i32, int64_t npool,
@@ -396,11 +573,15 @@ int nsg_bind_patches_device(nsg_ctx* c, int64_t n, const double* f64, const int3
 
 int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
   if (!c || !c->has_grid || !c->has_patches) return fail(NSG_ERR_STATE, "grid and patches must be set first");
+  if (c->patch_nstruct != c->nstruct) return fail(NSG_ERR_STATE, "patches were uploaded for another batch layout");
   if (precision != NSG_PRECISION_FP64 && precision != NSG_PRECISION_MIXED)
     return fail(NSG_ERR_ARG, "unsupported precision");
   CK(cudaSetDevice(c->device));
-  const NsGrid& g = c->grid;
-  const int64_t tot = g.nx * g.ny * g.nz;
+  {
+    int rc = ensure_patch_struct(c);
+    if (rc) return rc;
+  }
+  const nsg::BatchDev B = batch_dev(c);
   const bool do_status = flags & 1;
   const bool do_mc = flags & 2;
   const bool keep_hits = flags & 16;
@@ -414,7 +595,7 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
   }
   nsg::PatchDev P = patch_dev(c);
   stage_begin(c, kStageBin);
-  LAUNCH(nsg::launch_windows(P, c->win.as<int32_t>(), c->gd, c->stream));
+  LAUNCH(nsg::launch_windows(P, c->win.as<int32_t>(), B, c->stream));
   for (int panel = 0; panel < 3; panel++) {
     if (panel == 0 && !(do_status || do_mc)) continue;
     if (panel > 0 && !do_mc) continue;
@@ -422,9 +603,9 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
     if (rc) return rc;
   }
   stage_end(c, kStageBin);
-  const int64_t nwords = nwords_of(g);
-  const int64_t nrays_mc = g.nz * g.ny + g.ny * g.nx + g.nz * g.nx;
-  const int64_t nrows = g.ny * g.nz;
+  const int64_t nwords = c->words_tot;
+  const int64_t nrays_mc = c->mc_tot;
+  const int64_t nrows = c->rays_tot[0];
   if (do_status) {
     CK(c->srun_off.ensure(nrows * sizeof(int64_t)));
     CK(c->srun_cnt.ensure(nrows * sizeof(int32_t)));
@@ -438,11 +619,11 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
     CK(cudaMemsetAsync(c->ray_pair_cnt.p, 0, nrays_mc * sizeof(int32_t), c->stream));
     if (c->pair_cap == 0) c->pair_cap = std::max<int64_t>(4 * nrays_mc, 1 << 16);
   }
-  CK(c->cursors.ensure(16 * sizeof(unsigned long long)));
+  CK(c->cursors.ensure(32 * sizeof(unsigned long long)));
   {
     int64_t amax = std::max(c->win_area[0], std::max(c->win_area[1], c->win_area[2]));
     c->cand_cap = std::max<int64_t>(c->cand_cap, amax + 1024);
-    int64_t nr_max = std::max(g.ny * g.nz, std::max(g.nx * g.ny, g.nx * g.nz));
+    int64_t nr_max = std::max(std::max(c->rays_tot[0], c->rays_tot[1]), std::max(c->rays_tot[2], c->rays_tot[3]));
     CK(c->hit_t.ensure((size_t)nr_max * nsg::kHitCap * sizeof(double)));
     CK(c->hit_cnt.ensure(nr_max * sizeof(int32_t)));
   }
@@ -452,15 +633,20 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
     if (do_mc) CK(c->pairs.ensure(c->pair_cap * 2 * sizeof(double)));
     CK(c->cand_sph.ensure(c->cand_cap * sizeof(int2)));
     CK(c->cand_tor.ensure(c->cand_cap * sizeof(int2)));
+    if (precision == NSG_PRECISION_MIXED) {
+      c->def_cap = std::max<int64_t>(c->def_cap, c->cand_cap / 16 + (1 << 16));
+      CK(c->def_sph.ensure(c->def_cap * sizeof(int2)));
+      CK(c->def_tor.ensure(c->def_cap * sizeof(int2)));
+    }
     if (do_status) {
       CK(c->sruns.ensure(c->srun_cap * sizeof(int2)));
       CK(cudaMemsetAsync(c->srun_cnt.p, 0, nrows * sizeof(int32_t), c->stream));
     }
     if (keep_hits) {
-      if (c->hit_cap == 0) c->hit_cap = std::max<int64_t>(8 * (nrays_mc + g.nz * g.ny), 1 << 16);
+      if (c->hit_cap == 0) c->hit_cap = std::max<int64_t>(8 * (nrays_mc + c->rays_tot[0]), 1 << 16);
       CK(c->hits.ensure(c->hit_cap * sizeof(double)));
     }
-    CK(cudaMemsetAsync(c->cursors.p, 0, 16 * sizeof(unsigned long long), c->stream));
+    CK(cudaMemsetAsync(c->cursors.p, 0, 32 * sizeof(unsigned long long), c->stream));
     CK(cudaMemsetAsync(c->err.p, 0, sizeof(int32_t), c->stream));
     if (do_mc) CK(cudaMemsetAsync(c->bits.p, 0xff, nwords * sizeof(uint32_t), c->stream));
     unsigned long long* cur = c->cursors.as<unsigned long long>();
@@ -476,9 +662,8 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
     stage_begin(c, kStageTrace);
     for (int si = 0; si < nsets; si++) {
       int s = sets[si];
-      nsg::RaySet rs = nsg::make_ray_set(s, c->gd);
-      int panel = rs.panel;
-      int64_t nr = rs.nb * rs.na;
+      int panel = s == 0 ? 0 : s - 1;
+      int64_t nr = c->rays_tot[s];
       CK(c->vol_ray[s].ensure(nr * sizeof(double)));
       CK(c->ovf_rays[s].ensure(ovf_cap * sizeof(int32_t)));
       nsg::TraceOut o{};
@@ -510,12 +695,13 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
         o.ray_hit_cnt = c->ray_hit_cnt[s].as<int32_t>();
       }
       outs[s] = o;
-      nsg::CandOut co{c->cand_sph.as<int2>(), c->cand_tor.as<int2>(), c->cand_cap, cur + 8 + 2 * s};
+      nsg::CandOut co{c->cand_sph.as<int2>(), c->cand_tor.as<int2>(), c->cand_cap, cur + 8 + 2 * s,
+                      c->def_sph.as<int2>(), c->def_tor.as<int2>(), c->def_cap, cur + 16 + 2 * s};
       nsg::HitStore hs{c->hit_t.as<double>(), c->hit_cnt.as<int32_t>(), nr};
       CK(cudaMemsetAsync(c->hit_cnt.p, 0, nr * sizeof(int32_t), c->stream));
-      c->launches += 4;
-      CK(nsg::launch_trace(P, c->gd, rs, c->tile_off[panel].as<int64_t>(), c->tile_list[panel].as<int32_t>(), o, co, hs,
-                           precision, c->stream));
+      c->launches += precision == NSG_PRECISION_MIXED ? 6 : 4;
+      CK(nsg::launch_trace(P, B, s, c->tiles_tot[panel], c->tile_off[panel].as<int64_t>(),
+                           c->tile_list[panel].as<int32_t>(), o, co, hs, precision, c->stream));
     }
     stage_end(c, kStageTrace);
     int32_t novf[4] = {0, 0, 0, 0};
@@ -528,11 +714,10 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
       int n = std::min(novf[s], ovf_cap);
       tot_ovf += n;
       if (n == 0) continue;
-      nsg::RaySet rs = nsg::make_ray_set(s, c->gd);
+      const int panel = s == 0 ? 0 : s - 1;
       CK(c->ovf_scratch.ensure((size_t)n * nsg::kOverflowCap * sizeof(double)));
-      LAUNCH(nsg::launch_trace_overflow(P, c->gd, rs, c->tile_off[rs.panel].as<int64_t>(),
-                                    c->tile_list[rs.panel].as<int32_t>(), outs[s], n, c->ovf_scratch.as<double>(),
-                                    precision, c->stream));
+      LAUNCH(nsg::launch_trace_overflow(P, B, s, c->tile_off[panel].as<int64_t>(), c->tile_list[panel].as<int32_t>(),
+                                        outs[s], n, c->ovf_scratch.as<double>(), precision, c->stream));
       CK(cudaStreamSynchronize(c->stream));
     }
     stage_end(c, kStageOverflow);
@@ -552,23 +737,35 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
     if (errflag == 2) { c->hit_cap = std::max<int64_t>(2 * c->hit_cap, (int64_t)used[1] + 1024); continue; }
     if (errflag == 5) { c->srun_cap = std::max<int64_t>(2 * c->srun_cap, (int64_t)used[2] + 1024); continue; }
     if (errflag == 6) { c->cand_cap *= 2; continue; }
+    if (errflag == 7) { c->def_cap *= 2; continue; }
     return fail(NSG_ERR_CAPACITY, errflag == 1 ? "too many overflow rays" : "ray hit capacity exceeded");
   }
-  // volume: A * sum of interval lengths over the ray sets / number of ray sets
-  double vsum = 0;
+  // volume: A * sum of interval lengths over the ray sets / number of ray sets, per structure
+  const int32_t nb = c->nstruct;
+  std::vector<double> vsum(nb, 0.0);
   int flag_sum = 0;
+  if (nb > 1) CK(c->vol_struct.ensure(nb * sizeof(double)));
   for (int s = 0; s < 4; s++) {
     if ((s == 0 && !do_status) || (s > 0 && !do_mc)) continue;
-    nsg::RaySet rs = nsg::make_ray_set(s, c->gd);
-    double v = 0;
-    int rc = reduce_sum(c, c->vol_ray[s].as<double>(), rs.nb * rs.na, &v);
-    if (rc) return rc;
-    vsum += v;
+    if (nb == 1) {
+      double v = 0;
+      int rc = reduce_sum(c, c->vol_ray[s].as<double>(), c->rays_tot[s], &v);
+      if (rc) return rc;
+      vsum[0] += v;
+    } else {
+      LAUNCH(nsg::launch_segment_sums(c->vol_ray[s].as<double>(), B.ray_base[s], nullptr, nb,
+                                      c->vol_struct.as<double>(), flag_sum > 0, c->stream));
+    }
     flag_sum++;
   }
-  c->volume = flag_sum ? g.A * vsum / flag_sum : 0.0;
+  if (nb > 1 && flag_sum) {
+    CK(cudaMemcpyAsync(vsum.data(), c->vol_struct.p, nb * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  }
+  for (int32_t b = 0; b < nb; b++) c->volumes[b] = flag_sum ? c->grids[b].A * vsum[b] / flag_sum : 0.0;
+  c->volume = c->volumes[0];
   if (volume) *volume = c->volume;
-  if (do_status) {
+  if (do_status && nb == 1) {
     int rc = build_free_runs(c);
     if (rc) return rc;
   }
@@ -609,6 +806,7 @@ int nsg_cavity_order(int32_t n, const uint32_t* desc_key, int32_t* label_out) {
 
 int nsg_cavities(nsg_ctx* c, double cav_vol, int* ncav_out) {
   if (!c || !c->have_status) return fail(NSG_ERR_STATE, "cavity detection needs the status map");
+  if (c->nstruct != 1) return fail(NSG_ERR_STATE, "cavity detection runs on a single structure");
   CK(cudaSetDevice(c->device));
   const NsGrid& g = c->grid;
   const int64_t nr = c->n_fruns;
@@ -688,19 +886,17 @@ int nsg_cavities(nsg_ctx* c, double cav_vol, int* ncav_out) {
 int nsg_triangulate(nsg_ctx* c, double* area_out, int64_t* nverts, int64_t* ntris) {
   if (!c || !c->have_bits) return fail(NSG_ERR_STATE, "triangulation needs the accurate-triangulation rays");
   CK(cudaSetDevice(c->device));
-  const NsGrid& g = c->grid;
-  const int64_t nwords = nwords_of(g);
-  const int64_t nrays = g.nz * g.ny + g.ny * g.nx + g.nz * g.nx;
+  const nsg::BatchDev B = batch_dev(c);
+  const int64_t nrays = c->mc_tot;
   CK(c->surv_cnt.ensure(nrays * sizeof(int32_t)));
   CK(c->surv_off.ensure((nrays + 1) * sizeof(int64_t)));
   nsg::VertArgs V{};
-  V.g = c->gd;
+  V.B = B;
   V.nrays = nrays;
   V.ray_pair_off = c->ray_pair_off.as<int64_t>();
   V.ray_pair_cnt = c->ray_pair_cnt.as<int32_t>();
   V.pairs = c->pairs.as<double>();
   V.bits = c->bits.as<uint32_t>();
-  V.nwords = nwords;
   V.surv_cnt = c->surv_cnt.as<int32_t>();
   V.surv_off = c->surv_off.as<int64_t>();
   stage_begin(c, kStageVertex);
@@ -709,13 +905,12 @@ int nsg_triangulate(nsg_ctx* c, double* area_out, int64_t* nverts, int64_t* ntri
   int rc = scan_counts(c, c->surv_cnt.as<int32_t>(), nrays, c->surv_off.as<int64_t>(), &n_an);
   if (rc) return rc;
   // rows of cubes
-  const int64_t nrows = (g.ny - 2) * (g.nz - 2);
+  const int64_t nrows = c->rows_tot;
   CK(c->row_act_cnt.ensure((nrows + 1) * sizeof(int64_t)));
   CK(c->row_act_off.ensure((nrows + 1) * sizeof(int64_t)));
   nsg::MCArgs M{};
-  M.g = c->gd;
+  M.B = B;
   M.bits = c->bits.as<uint32_t>();
-  M.nwords = nwords;
   M.surv_cnt = c->surv_cnt.as<int32_t>();
   M.surv_off = c->surv_off.as<int64_t>();
   M.n_analytic = n_an;
@@ -784,8 +979,19 @@ int nsg_triangulate(nsg_ctx* c, double* area_out, int64_t* nverts, int64_t* ntri
   M.cube_area = c->cube_area.as<double>();
   LAUNCH(nsg::launch_mc_tris(M, 1, c->stream));
   double area = 0;
-  rc = reduce_sum(c, c->cube_area.as<double>(), n_act, &area);
-  if (rc) return rc;
+  if (c->nstruct == 1) {
+    rc = reduce_sum(c, c->cube_area.as<double>(), n_act, &area);
+    if (rc) return rc;
+    c->areas[0] = area;
+  } else {
+    CK(c->area_struct.ensure(c->nstruct * sizeof(double)));
+    LAUNCH(nsg::launch_segment_sums(c->cube_area.as<double>(), c->row_act_off.as<int64_t>(), B.row_base, c->nstruct,
+                                    c->area_struct.as<double>(), false, c->stream));
+    CK(cudaMemcpyAsync(c->areas.data(), c->area_struct.p, c->nstruct * sizeof(double), cudaMemcpyDeviceToHost,
+                       c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    area = c->areas[0];
+  }
   stage_end(c, kStageMC);
   c->n_analytic = n_an;
   c->n_vert = n_v;
@@ -800,6 +1006,7 @@ int nsg_triangulate(nsg_ctx* c, double* area_out, int64_t* nverts, int64_t* ntri
 
 int nsg_download_status(nsg_ctx* c, int32_t* dst) {
   if (!c || !dst || !c->have_status) return NSG_ERR_STATE;
+  if (c->nstruct != 1) return fail(NSG_ERR_STATE, "the dense status map is kept for a single structure");
   CK(cudaSetDevice(c->device));
   if (!c->status_dense) {
     int rc = materialize_status(c, nullptr);
@@ -813,7 +1020,7 @@ int nsg_download_status(nsg_ctx* c, int32_t* dst) {
 
 int nsg_download_insideness(nsg_ctx* c, uint32_t* dst) {
   if (!c || !dst || !c->have_bits) return NSG_ERR_STATE;
-  CK(cudaMemcpyAsync(dst, c->bits.p, nwords_of(c->grid) * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(dst, c->bits.p, c->words_tot * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return NSG_OK;
 }
@@ -841,8 +1048,7 @@ int nsg_download_cavities(nsg_ctx* c, double* sizes, int32_t* filled) {
 // n*nb + m of the set; hits are gathered in that order into dst.
 int nsg_download_hits(nsg_ctx* c, int set, int32_t* counts, double* dst, int64_t dst_cap) {
   if (!c || set < 0 || set > 3 || !(c->flags & 16)) return NSG_ERR_STATE;
-  nsg::RaySet rs = nsg::make_ray_set(set, c->gd);
-  int64_t nr = rs.nb * rs.na;
+  int64_t nr = c->rays_tot[set];
   std::vector<int64_t> off(nr);
   std::vector<int32_t> cnt(nr);
   CK(cudaMemcpyAsync(off.data(), c->ray_hit_off[set].p, nr * sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));

@@ -63,25 +63,30 @@ __device__ __forceinline__ bool keeps(const GridDev& g, const uint32_t* bits, in
 }
 
 __global__ void k_vert(VertArgs A, int emit) {
-  const GridDev& g = A.g;
   for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < A.nrays; r += (int64_t)gridDim.x * blockDim.x) {
     int np = A.ray_pair_cnt[r];
     if (!emit) {
       int cnt = 0;
       if (np > 0) {
-        RayId id = ray_of(g, r);
+        const StructDev& S = A.B.s[find_struct(A.B.mc_base, A.B.n, r)];
+        const GridDev& g = S.g;
+        const uint32_t* bits = A.bits + S.word_base;
+        RayId id = ray_of(g, r - S.mc_base);
         int vc = id.panel == 0 ? 0 : (id.panel == 1 ? 2 : 1);
         const double* pr = A.pairs + 2 * A.ray_pair_off[r];
         for (int q = 0; q < 2 * np; q++) {
           int64_t a = (int64_t)floor((pr[q] - g.mn[vc]) * g.scale + 0.5);
-          if (keeps(g, A.bits, A.nwords, edge_key(id, a))) cnt++;
+          if (keeps(g, bits, S.nwords, edge_key(id, a))) cnt++;
         }
       }
       A.surv_cnt[r] = cnt;
       continue;
     }
     if (np == 0 || A.surv_cnt[r] == 0) continue;
-    RayId id = ray_of(g, r);
+    const StructDev& S = A.B.s[find_struct(A.B.mc_base, A.B.n, r)];
+    const GridDev& g = S.g;
+    const uint32_t* bits = A.bits + S.word_base;
+    RayId id = ray_of(g, r - S.mc_base);
     int vc = id.panel == 0 ? 0 : (id.panel == 1 ? 2 : 1);
     const double* pr = A.pairs + 2 * A.ray_pair_off[r];
     const double delta = NS_DELTA - g.hside;
@@ -93,7 +98,7 @@ __global__ void k_vert(VertArgs A, int emit) {
     for (int q = 0; q < 2 * np; q++) {
       int64_t a = (int64_t)floor((pr[q] - g.mn[vc]) * g.scale + 0.5);
       int4 e = edge_key(id, a);
-      if (!keeps(g, A.bits, A.nwords, e)) continue;
+      if (!keeps(g, bits, S.nwords, e)) continue;
       double p[3] = {base[0], base[1], base[2]};
       p[vc] = pr[q];
       A.vpos[3 * o + 0] = p[0];
@@ -106,13 +111,15 @@ __global__ void k_vert(VertArgs A, int emit) {
 }
 
 // Index of the analytic vertex on edge (dir, i, j, k), -1 if none.
-__device__ __forceinline__ int64_t analytic_vertex(const MCArgs& A, int dir, int64_t i, int64_t j, int64_t k) {
-  const GridDev& g = A.g;
+__device__ __forceinline__ int64_t analytic_vertex(const MCArgs& A, const StructDev& S, int dir, int64_t i, int64_t j,
+                                                   int64_t k) {
+  const GridDev& g = S.g;
   const int64_t NX = g.n[0], NY = g.n[1], NZ = g.n[2];
   int64_t r, e;
   if (dir == NS_X_DIR) { r = k * NY + j; e = i; }
   else if (dir == NS_Z_DIR) { r = NZ * NY + j * NX + i; e = k; }
   else { r = NZ * NY + NY * NX + k * NX + i; e = j; }
+  r += S.mc_base;
   int cnt = A.surv_cnt[r];
   if (cnt == 0) return -1;
   int64_t off = A.surv_off[r];
@@ -125,30 +132,17 @@ __device__ __forceinline__ int64_t analytic_vertex(const MCArgs& A, int dir, int
   return -1;
 }
 
-__device__ __forceinline__ int cube_case(const MCArgs& A, int64_t i, int64_t j, int64_t k) {
-  const int64_t NX = A.g.n[0], NY = A.g.n[1];
-  int64_t f = (k * NY + j) * NX + i;
-  int64_t sy = NX, sz = NX * NY;
-  int c = 0;
-  if (!rbit(A.bits, A.nwords, f)) c |= 1;
-  if (!rbit(A.bits, A.nwords, f + 1)) c |= 2;
-  if (!rbit(A.bits, A.nwords, f + 1 + sy)) c |= 4;
-  if (!rbit(A.bits, A.nwords, f + sy)) c |= 8;
-  if (!rbit(A.bits, A.nwords, f + sz)) c |= 16;
-  if (!rbit(A.bits, A.nwords, f + 1 + sz)) c |= 32;
-  if (!rbit(A.bits, A.nwords, f + 1 + sy + sz)) c |= 64;
-  if (!rbit(A.bits, A.nwords, f + sy + sz)) c |= 128;
-  return c;
-}
-
 // Midpoint vertices a cube creates on its own edges 5 (y), 6 (x), 10 (z): bit 0, 1, 2.
-__device__ __forceinline__ int own_midpoints(const MCArgs& A, int64_t i, int64_t j, int64_t k, int em) {
+__device__ __forceinline__ int own_midpoints(const MCArgs& A, const StructDev& S, int64_t i, int64_t j, int64_t k,
+                                             int em) {
   int mm = 0;
-  if ((em & 32) && analytic_vertex(A, NS_Y_DIR, i + 1, j, k + 1) < 0) mm |= 1;
-  if ((em & 64) && analytic_vertex(A, NS_X_DIR, i, j + 1, k + 1) < 0) mm |= 2;
-  if ((em & 1024) && analytic_vertex(A, NS_Z_DIR, i + 1, j + 1, k) < 0) mm |= 4;
+  if ((em & 32) && analytic_vertex(A, S, NS_Y_DIR, i + 1, j, k + 1) < 0) mm |= 1;
+  if ((em & 64) && analytic_vertex(A, S, NS_X_DIR, i, j + 1, k + 1) < 0) mm |= 2;
+  if ((em & 1024) && analytic_vertex(A, S, NS_Z_DIR, i + 1, j + 1, k) < 0) mm |= 4;
   return mm;
 }
+
+__device__ __forceinline__ int rec_struct(int w) { return (int)((unsigned)w >> 11); }
 
 // 32 consecutive bits of the flat bit grid starting at bit f (missing words read as outside).
 __device__ __forceinline__ uint32_t bits32(const uint32_t* __restrict__ bits, int64_t nwords, int64_t f) {
@@ -164,13 +158,17 @@ __device__ __forceinline__ uint32_t bits32(const uint32_t* __restrict__ bits, in
 // bit rows the cubes touch (corner inside = bit 0): a cube is active unless its 8 corners agree.
 // Pass 0 counts the active cubes of the row, pass 1 writes them in i order.
 __global__ void k_mc_rows(MCArgs A, int emit) {
-  const GridDev& g = A.g;
-  const int64_t NX = g.n[0], NY = g.n[1];
   const int lane = threadIdx.x & 31;
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t row = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); row < A.nrows; row += warps) {
-    int64_t j = 1 + row % (NY - 2);
-    int64_t k = 1 + row / (NY - 2);
+    const int b = find_struct(A.B.row_base, A.B.n, row);
+    const StructDev& S = A.B.s[b];
+    const int64_t NX = S.g.n[0], NY = S.g.n[1];
+    const uint32_t* bits = A.bits + S.word_base;
+    const int64_t nwords = S.nwords;
+    const int64_t lrow = row - S.row_base;
+    int64_t j = 1 + lrow % (NY - 2);
+    int64_t k = 1 + lrow / (NY - 2);
     const int64_t b00 = (k * NY + j) * NX, b10 = b00 + NX, b01 = b00 + NX * NY, b11 = b01 + NX;
     int64_t act_run = 0;
     int64_t act_base = emit ? A.row_act_off[row] : 0;
@@ -181,14 +179,14 @@ __global__ void k_mc_rows(MCArgs A, int emit) {
       if (ic < NX - 1) {
         int64_t nvalid = NX - 1 - ic;
         uint32_t vm = nvalid >= 32 ? 0xffffffffu : ((1u << nvalid) - 1u);
-        c[0] = ~bits32(A.bits, A.nwords, b00 + ic);
-        c[1] = ~bits32(A.bits, A.nwords, b00 + ic + 1);
-        c[2] = ~bits32(A.bits, A.nwords, b10 + ic + 1);
-        c[3] = ~bits32(A.bits, A.nwords, b10 + ic);
-        c[4] = ~bits32(A.bits, A.nwords, b01 + ic);
-        c[5] = ~bits32(A.bits, A.nwords, b01 + ic + 1);
-        c[6] = ~bits32(A.bits, A.nwords, b11 + ic + 1);
-        c[7] = ~bits32(A.bits, A.nwords, b11 + ic);
+        c[0] = ~bits32(bits, nwords, b00 + ic);
+        c[1] = ~bits32(bits, nwords, b00 + ic + 1);
+        c[2] = ~bits32(bits, nwords, b10 + ic + 1);
+        c[3] = ~bits32(bits, nwords, b10 + ic);
+        c[4] = ~bits32(bits, nwords, b01 + ic);
+        c[5] = ~bits32(bits, nwords, b01 + ic + 1);
+        c[6] = ~bits32(bits, nwords, b11 + ic + 1);
+        c[7] = ~bits32(bits, nwords, b11 + ic);
         uint32_t d = 0;
 #pragma unroll
         for (int q = 1; q < 8; q++) d |= c[0] ^ c[q];
@@ -204,11 +202,11 @@ __global__ void k_mc_rows(MCArgs A, int emit) {
       if (emit && na) {
         int64_t slot = act_base + act_run + ia - na;
         for (uint32_t m = act; m; m &= m - 1) {
-          int b = __ffs(m) - 1;
+          int bit = __ffs(m) - 1;
           int cs = 0;
 #pragma unroll
-          for (int q = 0; q < 8; q++) cs |= ((c[q] >> b) & 1u) << q;
-          A.act_rec[slot++] = make_int4((int)(ic + b), (int)j, (int)k, cs);
+          for (int q = 0; q < 8; q++) cs |= ((c[q] >> bit) & 1u) << q;
+          A.act_rec[slot++] = make_int4((int)(ic + bit), (int)j, (int)k, cs | (b << 11));
         }
       }
       act_run += ta;
@@ -221,13 +219,14 @@ __global__ void k_mc_rows(MCArgs A, int emit) {
 // vertex (cut edge without an analytic vertex); the mask goes to bits 8..10 of the record and the
 // count to mid_cnt.  Pass 1: writes those vertices at their final indices (act_mid).
 __global__ void k_mc_mid(MCArgs A, int emit) {
-  const GridDev& g = A.g;
   for (int64_t a = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; a < A.n_active; a += (int64_t)gridDim.x * blockDim.x) {
     int4 rec = A.act_rec[a];
     const int64_t i = rec.x, j = rec.y, k = rec.z;
+    const StructDev& S = A.B.s[rec_struct(rec.w)];
+    const GridDev& g = S.g;
     if (!emit) {
-      int mm = own_midpoints(A, i, j, k, c_emask[rec.w & 255]);
-      A.act_rec[a].w = (rec.w & 255) | (mm << 8);
+      int mm = own_midpoints(A, S, i, j, k, c_emask[rec.w & 255]);
+      A.act_rec[a].w = (rec.w & ~(7 << 8)) | (mm << 8);
       A.mid_cnt[a] = __popc(mm);
       continue;
     }
@@ -255,15 +254,16 @@ __global__ void k_mc_mid(MCArgs A, int emit) {
 }
 
 // Midpoint vertex created by the cube that owns edge (dir, ex, ey, ez), -1 if none.
-__device__ __forceinline__ int64_t midpoint_vertex(const MCArgs& A, int dir, int64_t ex, int64_t ey, int64_t ez) {
-  const int64_t NX = A.g.n[0], NY = A.g.n[1], NZ = A.g.n[2];
+__device__ __forceinline__ int64_t midpoint_vertex(const MCArgs& A, const StructDev& S, int dir, int64_t ex, int64_t ey,
+                                                   int64_t ez) {
+  const int64_t NX = S.g.n[0], NY = S.g.n[1], NZ = S.g.n[2];
   int64_t oi = ex, oj = ey, ok = ez;
   int bit;
   if (dir == NS_Y_DIR) { oi = ex - 1; ok = ez - 1; bit = 0; }
   else if (dir == NS_X_DIR) { oj = ey - 1; ok = ez - 1; bit = 1; }
   else { oi = ex - 1; oj = ey - 1; bit = 2; }
   if (oi < 1 || oj < 1 || ok < 1 || oi > NX - 2 || oj > NY - 2 || ok > NZ - 2) return -1;
-  int64_t row = (ok - 1) * (NY - 2) + (oj - 1);
+  int64_t row = S.row_base + (ok - 1) * (NY - 2) + (oj - 1);
   int64_t lo = A.row_act_off[row], hi = A.row_act_off[row + 1];
   while (lo < hi) {
     int64_t mid = (lo + hi) >> 1;
@@ -276,7 +276,8 @@ __device__ __forceinline__ int64_t midpoint_vertex(const MCArgs& A, int dir, int
   return A.act_mid[lo] + __popc(mm & ((1 << bit) - 1));
 }
 
-__device__ __forceinline__ int64_t edge_vertex(const MCArgs& A, int e, int64_t i, int64_t j, int64_t k) {
+__device__ __forceinline__ int64_t edge_vertex(const MCArgs& A, const StructDev& S, int e, int64_t i, int64_t j,
+                                               int64_t k) {
   // cube edge -> grid edge (dir, ex, ey, ez)
   int dir;
   int64_t x = i, y = j, z = k;
@@ -294,9 +295,9 @@ __device__ __forceinline__ int64_t edge_vertex(const MCArgs& A, int e, int64_t i
     case 10: dir = NS_Z_DIR; x = i + 1; y = j + 1; break;
     default: dir = NS_Z_DIR; y = j + 1; break;
   }
-  int64_t v = analytic_vertex(A, dir, x, y, z);
+  int64_t v = analytic_vertex(A, S, dir, x, y, z);
   if (v >= 0) return v;
-  return midpoint_vertex(A, dir, x, y, z);
+  return midpoint_vertex(A, S, dir, x, y, z);
 }
 
 __device__ __forceinline__ double vdist(const double* a, const double* b) {
@@ -309,9 +310,10 @@ __global__ void k_mc_tris(MCArgs A, int emit) {
     int4 rec = A.act_rec[a];
     int c = rec.w & 255;
     int64_t i = rec.x, j = rec.y, k = rec.z;
+    const StructDev& S = A.B.s[rec_struct(rec.w)];
     int64_t vl[12];
     int em = c_emask[c];
-    for (int e = 0; e < 12; e++) vl[e] = (em >> e) & 1 ? edge_vertex(A, e, i, j, k) : -1;
+    for (int e = 0; e < 12; e++) vl[e] = (em >> e) & 1 ? edge_vertex(A, S, e, i, j, k) : -1;
     int cnt = 0;
     int64_t o = emit ? A.tri_off[a] : 0;
     double area = 0.0;

@@ -7,14 +7,15 @@
 
 namespace nsg {
 
+// Both argument blocks cover a whole batch: ray ordinals, cube rows, active cubes and vertices
+// are batch-wide; every structure's bit grid starts at its word_base in `bits`.
 struct VertArgs {
-  GridDev g;
-  int64_t nrays;                 // accurate-triangulation rays of the three panels
+  BatchDev B;
+  int64_t nrays;                 // accurate-triangulation rays of the three panels, all structures
   const int64_t* ray_pair_off;
   const int32_t* ray_pair_cnt;
   const double* pairs;
   const uint32_t* bits;
-  int64_t nwords;
   int32_t* surv_cnt;             // surviving vertices per ray
   const int64_t* surv_off;       // exclusive scan of surv_cnt
   double* vpos;                  // 3 per vertex
@@ -22,18 +23,17 @@ struct VertArgs {
 };
 
 struct MCArgs {
-  GridDev g;
+  BatchDev B;
   const uint32_t* bits;
-  int64_t nwords;
   const int32_t* surv_cnt;
   const int64_t* surv_off;
   int64_t n_analytic;
   double* vpos;
   int4* vkey;
-  int64_t nrows;                 // (NY-2)*(NZ-2) cube rows
+  int64_t nrows;                 // cube rows, (NY-2)*(NZ-2) per structure
   int64_t* row_act_cnt;
   const int64_t* row_act_off;    // nrows+1 entries
-  int4* act_rec;                 // i, j, k, case | midpoint mask << 8
+  int4* act_rec;                 // i, j, k, case | midpoint mask << 8 | structure << 11
   int32_t* mid_cnt;              // midpoint vertices per active cube
   const int64_t* mid_off;        // exclusive scan of mid_cnt
   int32_t* act_mid;              // index of the first midpoint vertex of the cube

@@ -38,6 +38,43 @@ struct GridDev {
   double scale, side, hside;
 };
 
+// One structure of a batch: its grid and where its tiles, rays, bits and cube rows start in the
+// batch-wide arrays.  A single structure is a batch of one with every base 0.
+struct StructDev {
+  GridDev g;
+  int64_t nwords;        // words of its 32x-packed insideness bit grid
+  int64_t word_base;     // first word in the batch's bit array
+  int64_t tile_base[3];  // first tile of each panel in the panel's tile arrays
+  int64_t ray_base[4];   // first ray of each ray set in the set's ray arrays
+  int64_t mc_base;       // first accurate-triangulation ray ordinal (its 3 panels are contiguous)
+  int64_t row_base;      // first marching-cubes row ((NY-2)*(NZ-2) rows per structure)
+  double ray_dir[3];     // ray length along each axis: coordinate of the last node minus the first
+  double inv_dir[3];     // 1 / ray_dir
+};
+
+// Batch-wide lookup tables.  The *_base arrays hold n+1 entries (the last is the total), for a
+// binary search from a batch-wide index to its structure.
+struct BatchDev {
+  int32_t n;
+  const StructDev* s;
+  const int32_t* patch_struct;    // structure of every patch
+  const int32_t* tile_struct[3];  // structure of every tile of each panel
+  const int64_t* ray_base[4];     // n+1 per ray set
+  const int64_t* mc_base;         // n+1
+  const int64_t* row_base;        // n+1
+};
+
+// Largest b with base[b] <= x (base ascending, base[0] = 0).
+__device__ __forceinline__ int find_struct(const int64_t* __restrict__ base, int n, int64_t x) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (base[mid] <= x) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
 __host__ __device__ inline RaySet make_ray_set(int set, const GridDev& g) {
   RaySet r;
   r.set = set;
@@ -93,12 +130,17 @@ struct TraceOut {
 enum { kCntCandidates = 0, kCntTorus = 1, kCntFbSphere = 2, kCntFbQuartic = 3, kCntFbRoot = 4, kCntRecheck = 5,
        kCntN = 8 };
 
-// Candidate (ray, patch) pairs of one ray set, by patch type (0 spheres, 1 tori).
+// Candidate (ray, patch) pairs of one ray set, by patch type (0 spheres, 1 tori), and the
+// candidates the mixed-precision pass defers to the double-precision pass (same split).
 struct CandOut {
   int2* sph;
   int2* tor;
   int64_t cap;
-  unsigned long long* count;  // 2 counters
+  unsigned long long* count;   // 2 counters
+  int2* dsph;
+  int2* dtor;
+  int64_t dcap;
+  unsigned long long* dcount;  // 2 counters
 };
 
 // Slot-major hit store of one ray set: hit i of ray r at t[i * nrays + r]; cnt[r] counts the
@@ -120,19 +162,25 @@ struct PatchDev {
   const int32_t* win;  // 6 per patch: start x,y,z, end x,y,z; start = -1 when culled
 };
 
-// trace.cu
-cudaError_t launch_windows(const PatchDev& P, int32_t* win, const GridDev& g, cudaStream_t s);
+// trace.cu: every launch covers all structures of the batch; `set` is the ray set (0..3) and
+// tile and ray indices are batch-wide.
+cudaError_t launch_windows(const PatchDev& P, int32_t* win, const BatchDev& B, cudaStream_t s);
 // Patch-local FP32 copy of the pool: planes (n, d + n.c), clipping spheres (s - c, r^2).
 cudaError_t launch_pool32(const PatchDev& P, float4* pool32, cudaStream_t s);
-cudaError_t launch_bin_count(const PatchDev& P, const GridDev& g, const RaySet& rs, int32_t* tile_cnt,
+cudaError_t launch_bin_count(const PatchDev& P, const BatchDev& B, int set, int32_t* tile_cnt,
                              unsigned long long* area, cudaStream_t s);
-cudaError_t launch_bin_fill(const PatchDev& P, const GridDev& g, const RaySet& rs, const int64_t* tile_off,
+cudaError_t launch_bin_fill(const PatchDev& P, const BatchDev& B, int set, const int64_t* tile_off,
                             int32_t* tile_cursor, int32_t* tile_list, cudaStream_t s);
-cudaError_t launch_trace(const PatchDev& P, const GridDev& g, const RaySet& rs, const int64_t* tile_off,
+cudaError_t launch_trace(const PatchDev& P, const BatchDev& B, int set, int64_t ntiles, const int64_t* tile_off,
                          const int32_t* tile_list, const TraceOut& out, const CandOut& co, const HitStore& hs,
                          int precision, cudaStream_t s);
-cudaError_t launch_trace_overflow(const PatchDev& P, const GridDev& g, const RaySet& rs, const int64_t* tile_off,
+cudaError_t launch_trace_overflow(const PatchDev& P, const BatchDev& B, int set, const int64_t* tile_off,
                                   const int32_t* tile_list, const TraceOut& out, int n_ovf, double* scratch,
                                   int precision, cudaStream_t s);
+
+// reduce.cu: out[b] (+)= sum of v over structure b's segment [base[i(b)], base[i(b+1)]) with
+// i(b) = idx[b] (idx given) or b; one CTA per structure, fixed summation order.
+cudaError_t launch_segment_sums(const double* v, const int64_t* base, const int64_t* idx, int n, double* out,
+                                bool accumulate, cudaStream_t s);
 
 }  // namespace nsg

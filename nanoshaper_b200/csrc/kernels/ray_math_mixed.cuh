@@ -4,11 +4,13 @@
 //   * sphere hits: the discriminant and square root in FP32 on local offsets, then one FP64
 //     Newton correction of the square root against the FP64 discriminant; near-tangent rays
 //     (|disc| below a threshold) fall back to the double-precision test;
-//   * torus hits: quartic coefficients in FP64, real roots isolated in FP32 with the same
-//     Ferrari-type resolvent as the double-precision solver, each root polished by two FP64
-//     Newton steps on the FP64 polynomial; whenever the FP32 isolation is near a decision boundary
-//     (discriminant, resolvent root, merging roots, small derivative) the candidate falls back to
-//     the double-precision solver;
+//   * torus hits: every decision of the Ferrari-type solver (discriminant and root count,
+//     resolvent branch and sign, which root pairs are real) in FP64 with the double-precision
+//     solver's expressions; its transcendental steps (cube roots, arccos, cos) and the root
+//     estimates in FP32, the resolvent root refined by FP64 Newton steps and each quartic root
+//     polished by two FP64 Newton steps on the FP64 polynomial; a decision within rounding of its
+//     threshold, merging roots or a small derivative defer the candidate to the double-precision
+//     solver;
 //   * feasibility: plane and sphere tests in FP32 on local coordinates; a test whose FP32 value is
 //     within a tolerance of zero is re-evaluated in FP64 from the double-precision pool.
 // Hit points therefore carry FP64 accuracy and the accept/reject decisions equal the
@@ -24,81 +26,96 @@ namespace nsg {
 constexpr float kDiscTol = 1e-3f;     // sphere discriminant r^2 - dx^2 - dy^2 [A^2]
 constexpr float kPlaneTol = 1e-3f;    // plane test value [A] (planes are unit normals)
 constexpr float kSphereTol = 1e-2f;   // clipping-sphere test |p-s|^2 - r^2 [A^2]
-constexpr float kRelTol = 1e-4f;      // relative closeness of quartic decision quantities
 
-// Cubic resolvent root in FP32 (same branch structure as the double-precision restatement).
-__device__ __forceinline__ float real_cubic_f32(float b, float c, float d) {
-  float p = -(1.0f / 3.0f) * b * b + c;
-  float q = (2.f / 27.f) * b * b * b - (1.f / 3.f) * b * c + d;
-  float D3p = (1.f / 27.f) * p * p * p;
-  float D3 = D3p + 0.25f * q * q;
-  if (fabsf(c) < b * b * 1.E-6f && fabsf(d) < fabsf(b) * 1.E-6f) {
-    return c / b - b - d / (b * b);
-  } else if (fabsf(d / c) < 4.E-4f) {
-    float ratio = d / c;
-    if (D3 <= 0.f) {
-      return 0.5f * (ratio - b + sqrtf((b - ratio) * (b - ratio) - 4.f * (c - ratio * (b - ratio))));
-    } else {
-      float eps = -ratio * ratio * (b - ratio) / (3.f * ratio * ratio - 2.f * b * ratio + c);
-      return eps - ratio;
-    }
+// Estimate of the resolvent root chosen by the double-precision solver (real_cubic_f64): the
+// branch decisions are taken in FP64 with the same expressions, so the same root is approximated;
+// the chosen closed form (Cardano cube roots, or the trigonometric form) is evaluated in FP32.
+__device__ __forceinline__ float real_cubic_mixed(double b, double c, double d) {
+  const double p = -(1.0 / 3.0) * b * b + c;
+  const double q = (2. / 27.) * b * b * b - (1. / 3.) * b * c + d;
+  const double D3p = (1. / 27.) * p * p * p;
+  const double D3 = D3p + 0.25 * q * q;
+  const float bf = (float)b;
+  if (fabs(c) < b * b * 1.E-6 && fabs(d) < fabs(b) * 1.E-6) {
+    return (float)(c / b - b - d / (b * b));
+  } else if (fabs(d / c) < 4.E-4) {
+    const double ratio = d / c;
+    if (D3 <= 0.) return (float)(0.5 * (ratio - b + sqrt((b - ratio) * (b - ratio) - 4. * (c - ratio * (b - ratio)))));
+    return (float)(-ratio * ratio * (b - ratio) / (3. * ratio * ratio - 2. * b * ratio + c) - ratio);
+  } else if (D3 >= 0.) {
+    const float radD3 = sqrtf((float)D3);
+    const float hq = (float)(0.5 * q);
+    return cbrtf(radD3 - hq) - cbrtf(radD3 + hq) - (1.f / 3.f) * bf;
   } else {
-    if (D3 >= 0.f) {
-      float radD3 = sqrtf(D3);
-      float A = cbrtf(radD3 - 0.5f * q);
-      float psu3A = cbrtf(radD3 + 0.5f * q);
-      return A - psu3A - (1.f / 3.f) * b;
-    } else {
-      float Aarg = acosf(-0.5f * q / sqrtf(-D3p));
-      return 2.f * sqrtf(-(1.f / 3.f) * p) * cosf((1.f / 3.f) * Aarg) - (1.f / 3.f) * b;
-    }
+    const float Aarg = acosf((float)(-0.5 * q / sqrt(-D3p)));
+    return 2.f * sqrtf((float)(-(1. / 3.) * p)) * cosf((1.f / 3.f) * Aarg) - (1.f / 3.f) * bf;
   }
 }
 
-// FP32 root isolation of the monic quartic; returns the number of roots, or -1 when a decision
-// is too close to call in FP32.
-__device__ __forceinline__ int quartic_f32(float roots[4], float b, float c, float d, float e) {
-  float b_2 = 0.5f * b;
-  float b_4 = 0.25f * b;
-  float p = c - 1.5f * (b_2 * b_2);
-  float q = d + b_2 * (b_2 * b_2 - c);
-  float r = e + b_4 * (b_4 * (c - 3.0f * b_4 * b_4) - d);
-  if (fabsf(p) > 3.E+3f || fabsf(r) > 3.E+3f || fabsf(q) > 3.E+3f) return -1;  // reciprocal variant: FP64
-  float f = p * p - 4.f * r;
-  float t1 = 4.f * r * (p * p), t2 = p * (q * q), t3 = 16.f * (r * r);
-  float t4 = 128.f * p * r, t5 = 27.f * (q * q);
-  float delta = 4.f * f * (t1 - t2 - t3) + (q * q) * (t4 - t5);
-  float dscale = fabsf(4.f * f) * (fabsf(t1) + fabsf(t2) + fabsf(t3)) + (q * q) * (fabsf(t4) + fabsf(t5));
-  if (!(fabsf(delta) > kRelTol * dscale)) return -1;
-  if (fabsf(delta) > 1.E+14f) return -1;
+// Root isolation of the monic quartic x^4 + b x^3 + c x^2 + d x + e, following the
+// double-precision solver (quartic_f64): the depressed coefficients, the discriminant and the
+// root-count decision in FP64 with the same operation sequence; the resolvent root estimated in
+// FP32 on the same branch and refined by FP64 Newton steps on the resolvent cubic; the
+// square-root arguments that decide which root pairs are real in FP64; the root estimates in
+// FP32 (each is polished on the FP64 quartic afterwards).  Returns the number of roots, or -1
+// when a decision is within rounding of its threshold (the resolvent refinement did not converge,
+// the resolvent root or a square-root argument is near zero) or the coefficients need the
+// reciprocal variant.
+__device__ __forceinline__ int quartic_mixed(float roots[4], double b, double c, double d, double e) {
+  const double b_2 = 0.5 * b;
+  const double b_4 = 0.25 * b;
+  const double p = c - 1.5 * (b_2 * b_2);
+  const double q = d + b_2 * (b_2 * b_2 - c);
+  const double r = e + b_4 * (b_4 * (c - 3.0 * b_4 * b_4) - d);
+  const double f = p * p - 4. * r;
+  const double delta =
+      4. * f * (4. * r * (p * p) - p * (q * q) - 16. * (r * r)) + (q * q) * (128. * p * r - 27. * (q * q));
+  if (e != 0. && (fabs(p) > 3.E+3 || fabs(r) > 3.E+3 || fabs(q) > 3.E+3 || fabs(delta) > 1.E+14)) return -1;
   int num_sol;
-  if (delta < 0.f) {
+  if (delta < 0. || (delta == 0. && (p >= 0. || f < 0.)))
     num_sol = 2;
-  } else {
-    if (fabsf(p) < kRelTol * (fabsf(c) + 1.f) || fabsf(f) < kRelTol * (p * p + fabsf(4.f * r))) return -1;
-    if (p < 0.f && f > 0.f) num_sol = 4;
-    else return 0;
+  else if ((p < 0. && f > 0.) || (delta == 0. && p == 0. && r == 0.))
+    num_sol = 4;
+  else
+    return 0;
+  // resolvent m^3 + p m^2 + (p^2/4 - r) m - q^2/8
+  const double cb = p, cc = 0.25 * (p * p) - r, cd = (-0.125) * (q * q);
+  double m = (double)real_cubic_mixed(cb, cc, cd);
+  const double mscale = fabs(p) + sqrt(fabs(r)) + 1e-30;
+  for (int it = 0; it < 3; it++) {
+    const double g = ((m + cb) * m + cc) * m + cd;
+    const double gp = (3.0 * m + 2.0 * cb) * m + cc;
+    if (!(fabs(gp) > 1e-8 * (mscale * mscale + 1e-30))) return -1;
+    const double step = g / gp;
+    m -= step;
+    if (it == 2 && !(fabs(step) <= 1e-12 * (fabs(m) + 1e-6 * mscale))) return -1;
   }
-  float m = real_cubic_f32(p, 0.25f * (p * p) - r, (-0.125f) * (q * q));
-  float mscale = fabsf(p) + sqrtf(fabsf(r)) + 1e-30f;
-  if (!(fabsf(m) > kRelTol * mscale)) return -1;
-  if (m <= 0.f) return 0;
-  float p1 = -2.f * (p + m);
-  float p2 = sqrtf(2.f * (q * q) / m);
-  float coeff = sqrtf(2.f * m);
-  float sdmax = p1 + p2;
-  float sscale = fabsf(p1) + fabsf(p2);
-  if (!(fabsf(sdmax) > kRelTol * sscale) || sdmax < 0.f) return -1;
-  float sq = (q >= 0.f) ? -coeff : coeff;
-  roots[0] = 0.5f * (sq - sqrtf(sdmax)) - 0.25f * b;
-  roots[1] = 0.5f * (sq + sqrtf(sdmax)) - 0.25f * b;
+  if (!(fabs(m) > 1e-9 * mscale) || fabs(m) < 1.E-13) return -1;
+  if (m <= 0.) return 0;
+  const double p1 = -2. * (p + m);
+  const double p2 = sqrt(2. * (q * q) / m);
+  const double sscale = fabs(p1) + fabs(p2);
+  const double sdmax = p1 + p2;
+  if (!(fabs(sdmax) > 1e-9 * sscale)) return -1;
+  const float coeff = sqrtf((float)(2. * m));
+  const float b4f = (float)b_4;
+  const float sq = (q >= 0.) ? -coeff : coeff;
+  int n = 0;
+  if (sdmax > 0.) {
+    const float s = sqrtf((float)sdmax);
+    roots[n++] = 0.5f * (sq - s) - b4f;
+    roots[n++] = 0.5f * (sq + s) - b4f;
+  }
   if (num_sol == 4) {
-    float sdmin = p1 - p2;
-    if (!(fabsf(sdmin) > kRelTol * sscale) || sdmin < 0.f) return -1;
-    roots[2] = 0.5f * (-sq - sqrtf(sdmin)) - 0.25f * b;
-    roots[3] = 0.5f * (-sq + sqrtf(sdmin)) - 0.25f * b;
+    const double sdmin = p1 - p2;
+    if (!(fabs(sdmin) > 1e-9 * sscale)) return -1;
+    if (sdmin > 0.) {
+      const float s = sqrtf((float)sdmin);
+      roots[n++] = 0.5f * (-sq - s) - b4f;
+      roots[n++] = 0.5f * (-sq + s) - b4f;
+    }
   }
-  return num_sol;
+  return n;
 }
 
 // Two Newton steps on the FP64 monic quartic; returns false when the derivative is too small

@@ -25,9 +25,10 @@ constexpr int kChunk = 32;  // patches staged per shared-memory chunk
 
 __device__ __forceinline__ double gcoord(const GridDev& g, int d, int64_t i) { return g.mn[d] + (double)i * g.side; }
 
-__global__ void k_windows(PatchDev P, int32_t* win, GridDev g) {
+__global__ void k_windows(PatchDev P, int32_t* win, BatchDev B) {
   int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (p >= P.n) return;
+  const GridDev& g = B.s[B.patch_struct[p]].g;
   const double* f = P.f64 + (int64_t)NS_PATCH_F64 * p;
   double r = f[3];
   double down[3], up[3];
@@ -68,11 +69,13 @@ __global__ void k_pool32(PatchDev P, float4* out) {
   }
 }
 
-__global__ void k_bin(PatchDev P, GridDev g, RaySet rs, int32_t* tile_cnt, const int64_t* tile_off,
+__global__ void k_bin(PatchDev P, BatchDev B, int set, int32_t* tile_cnt, const int64_t* tile_off,
                       int32_t* tile_cursor, int32_t* tile_list, unsigned long long* area) {
   int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const int32_t* w = P.win + 6 * (p < P.n ? p : 0);
   bool live = p < P.n && w[0] >= 0;
+  const StructDev& S = B.s[p < P.n ? B.patch_struct[p] : 0];
+  const RaySet rs = make_ray_set(set, S.g);
   if (area) {
     // pixel-window area: an upper bound of the patch's candidate rays in this panel
     unsigned a = live ? (unsigned)((w[3 + rs.fd] - w[rs.fd] + 1) * (w[3 + rs.ld] - w[rs.ld] + 1)) : 0u;
@@ -85,7 +88,7 @@ __global__ void k_bin(PatchDev P, GridDev g, RaySet rs, int32_t* tile_cnt, const
   int n0 = w[rs.ld] / kTileN, n1 = w[3 + rs.ld] / kTileN;
   for (int tn = n0; tn <= n1; tn++)
     for (int tm = m0; tm <= m1; tm++) {
-      int64_t t = (int64_t)tn * ntm + tm;
+      int64_t t = S.tile_base[rs.panel] + (int64_t)tn * ntm + tm;
       if (tile_list == nullptr) {
         atomicAdd(tile_cnt + t, 1);
       } else {
@@ -189,24 +192,13 @@ __device__ __forceinline__ int intersect_f64_p(const double* f, int kind, int fi
   return out;
 }
 
-template <int P>
-__device__ __noinline__ int intersect_f64_fallback_p(const double* f, int kind, int first, int cnt,
-                                                     const PatchDev& Pd, const double* pa, double ray_dir,
-                                                     double* t) {
-  if (kind == NS_EDGE_REG || kind == NS_EDGE_SING) return intersect_f64_p<P, true>(f, kind, first, cnt, Pd, pa, ray_dir, t);
-  return intersect_f64_p<P, false>(f, kind, first, cnt, Pd, pa, ray_dir, t);
-}
+// Result of the mixed-precision test for a candidate it cannot decide: the candidate goes to a
+// deferred list that a double-precision pass takes afterwards, so that the mixed kernel's warps
+// never wait on a double-precision path taken by one lane.
+constexpr int kDefer = -1;
 
-// Out-of-line double-precision intersection: the fallback of the mixed path, kept out of the
-// caller so that the rare fallback does not inflate the mixed kernel's register allocation.
-__device__ __noinline__ int intersect_f64_fallback(const double* f, int kind, int first, int cnt, const PatchDev& P,
-                                                   const RaySet& rs, const double* pa, const double* dir,
-                                                   double ray_dir, double* t) {
-  return intersect_f64(f, kind, first, cnt, P, rs, pa, dir, ray_dir, t);
-}
-
-// Mixed-precision intersection of a candidate (see ray_math_mixed.cuh); falls back to the
-// double-precision path for undecided candidates.
+// Mixed-precision intersection of a candidate (see ray_math_mixed.cuh): the number of feasible
+// hits, or kDefer when the single-precision bracket cannot decide the candidate.
 template <int PN, bool kTorus>
 __device__ __forceinline__ int intersect_mixed(const double* f, int kind, int first, int cnt, const PatchDev& P,
                                                const double* pa, double ray_dir, double inv_dir, double* t,
@@ -218,7 +210,7 @@ __device__ __forceinline__ int intersect_mixed(const double* f, int kind, int fi
   float disc = rf * rf - dxf * dxf - dyf * dyf;
   if (disc < kDiscTol) {
     if (ctr) atomicAdd(ctr + kCntFbSphere, 1ull);
-    return intersect_f64_fallback_p<PN>(f, kind, first, cnt, P, pa, ray_dir, t);
+    return kDefer;
   }
   float s32 = sqrtf(disc);
   double disc64 = r * r - dx64 * dx64 - dy64 * dy64;
@@ -236,32 +228,32 @@ __device__ __forceinline__ int intersect_mixed(const double* f, int kind, int fi
     double B, C, D, E;
     torus_coeffs_f64(f, P.probe, vc, orig1, &B, &C, &D, &E);
     float rt[4];
-    int nr = quartic_f32(rt, (float)B, (float)C, (float)D, (float)E);
+    int nr = quartic_mixed(rt, B, C, D, E);
     if (ctr) atomicAdd(ctr + kCntTorus, 1ull);
     if (nr < 0) {
       if (ctr) atomicAdd(ctr + kCntFbQuartic, 1ull);
-      return intersect_f64_fallback_p<PN>(f, kind, first, cnt, P, pa, ray_dir, t);
+      return kDefer;
     }
     double roots[4];
     for (int i = 0; i < nr; i++) {
       roots[i] = (double)rt[i];
       if (!polish_root(B, C, D, E, roots[i])) {
         if (ctr) atomicAdd(ctr + kCntFbRoot, 1ull);
-        return intersect_f64_fallback_p<PN>(f, kind, first, cnt, P, pa, ray_dir, t);
+        return kDefer;
       }
     }
     for (int i = 0; i < nr; i++)
       for (int j = i + 1; j < nr; j++)
         if (fabs(roots[i] - roots[j]) < 1e-6) {
           if (ctr) atomicAdd(ctr + kCntFbRoot, 1ull);
-          return intersect_f64_fallback_p<PN>(f, kind, first, cnt, P, pa, ray_dir, t);
+          return kDefer;
         }
     const double r2 = r * r;
     for (int i = 0; i < nr; i++) {
       double root = roots[i];
       if (fabs(root) < 1e-9) {
         if (ctr) atomicAdd(ctr + kCntFbRoot, 1ull);
-        return intersect_f64_fallback_p<PN>(f, kind, first, cnt, P, pa, ray_dir, t);
+        return kDefer;
       }
       if (root < 0) continue;
       double px = x_in + root;
@@ -269,7 +261,7 @@ __device__ __forceinline__ int intersect_mixed(const double* f, int kind, int fi
       double dd = e0 * e0 + e1 * e1 + e2 * e2;
       if (fabs(dd - r2) < 1e-9) {
         if (ctr) atomicAdd(ctr + kCntFbRoot, 1ull);
-        return intersect_f64_fallback_p<PN>(f, kind, first, cnt, P, pa, ray_dir, t);
+        return kDefer;
       }
       if (dd < r2) xs[nx++] = px;
     }
@@ -389,10 +381,9 @@ __device__ __forceinline__ void clear_bits_range(uint32_t* bits, int64_t nwords,
 
 struct TraceCtx {
   PatchDev P;
-  GridDev g;
-  RaySet rs;
+  BatchDev B;
+  int set;
   TraceOut out;
-  int64_t nwords;
 };
 
 // Wavefront ray tracing of one ray set, three kernel kinds:
@@ -410,22 +401,25 @@ constexpr int kWarpBuf = 256;
 __global__ void __launch_bounds__(kTraceThreads) k_cand(TraceCtx C, const int64_t* __restrict__ tile_off,
                                                          const int32_t* __restrict__ tile_list, CandOut co) {
   constexpr int kThreads = kTraceThreads;
-  const GridDev& g = C.g;
-  const RaySet& rs = C.rs;
+  const int panel = C.set == 0 ? 0 : C.set - 1;
+  const int64_t tile = blockIdx.x;
+  const StructDev& S = C.B.s[C.B.tile_struct[panel][tile]];
+  const GridDev& g = S.g;
+  const RaySet rs = make_ray_set(C.set, g);
   __shared__ double s_f[kChunk * NS_PATCH_F64];
   __shared__ int s_i[kChunk];
   __shared__ int s_pid[kChunk];
   __shared__ int s_w[kChunk * 4];
   __shared__ int2 s_buf[kTileN][2][kWarpBuf];
   const int64_t ntm = (rs.nb + kTileM - 1) / kTileM;
-  const int64_t tile = blockIdx.x;
-  const int64_t tm = tile % ntm, tn = tile / ntm;
+  const int64_t lt = tile - S.tile_base[panel];
+  const int64_t tm = lt % ntm, tn = lt / ntm;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t m = tm * kTileM + lane;
   const int64_t n = tn * kTileN + warp;
   const bool valid = (m < rs.nb) && (n < rs.na);
   const int tid = threadIdx.x;
-  const int32_t rid = (int32_t)(n * rs.nb + m);
+  const int32_t rid = (int32_t)(S.ray_base[C.set] + n * rs.nb + m);
   double pa[3];
   pa[rs.fd] = gcoord(g, rs.fd, valid ? m : 0) + rs.delta;
   pa[rs.ld] = gcoord(g, rs.ld, n < rs.na ? n : 0) + rs.delta;
@@ -486,21 +480,24 @@ __global__ void __launch_bounds__(kTraceThreads) k_cand(TraceCtx C, const int64_
 template <int PN, bool kTorus, bool kMixed>
 __global__ void __launch_bounds__(256) k_isect(TraceCtx C, CandOut co, HitStore hs) {
   constexpr int fd = Ax<PN>::fd, ld = Ax<PN>::ld, vc = Ax<PN>::vc;
-  const GridDev& g = C.g;
-  const RaySet& rs = C.rs;
   const int64_t ncand = *(co.count + (kTorus ? 1 : 0));
   const int2* list = kTorus ? co.tor : co.sph;
   const int64_t nlim = ncand < co.cap ? ncand : co.cap;
-  const double ray_dir = gcoord(g, vc, g.n[vc] - 1) - gcoord(g, vc, 0);
-  const double inv_dir = 1.0 / ray_dir;
   for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < nlim; c += (int64_t)gridDim.x * blockDim.x) {
     int2 e = list[c];
     const int64_t rid = e.x, pid = e.y;
-    const int64_t m = rid % rs.nb, n = rid / rs.nb;
+    const StructDev& S = C.B.s[C.B.patch_struct[pid]];
+    const GridDev& g = S.g;
+    const double delta = C.set == 0 ? 0.0 : NS_DELTA - g.hside;
+    const double ray_dir = S.ray_dir[vc];
+    const double inv_dir = S.inv_dir[vc];
+    const int64_t nb = g.n[fd];
+    const int64_t lr = rid - S.ray_base[C.set];
+    const int64_t m = lr % nb, n = lr / nb;
     double pa[3];
-    pa[fd] = gcoord(g, fd, m) + rs.delta;
-    pa[ld] = gcoord(g, ld, n) + rs.delta;
-    pa[vc] = gcoord(g, vc, 0) + rs.delta;
+    pa[fd] = gcoord(g, fd, m) + delta;
+    pa[ld] = gcoord(g, ld, n) + delta;
+    pa[vc] = gcoord(g, vc, 0) + delta;
     double f[NS_PATCH_F64];
     const double* src = C.P.f64 + (int64_t)NS_PATCH_F64 * pid;
     constexpr int nf = kTorus ? 18 : 4;
@@ -510,11 +507,28 @@ __global__ void __launch_bounds__(256) k_isect(TraceCtx C, CandOut co, HitStore 
     const int kind = ir[0], first = ir[1], cnt = ir[2];
     double t[4];
     int k;
-    if (kMixed)
+    if (kMixed) {
       k = intersect_mixed<PN, kTorus>(f, kind, first, cnt, C.P, pa, ray_dir, inv_dir, t, C.out.counters);
-    else
+      // warp-aggregated append of the deferred candidates
+      const bool defer = k == kDefer;
+      const unsigned am = __activemask();
+      const unsigned dm = __ballot_sync(am, defer);
+      if (dm) {
+        const int lane = threadIdx.x & 31;
+        const int leader = __ffs(dm) - 1;
+        unsigned long long base = 0;
+        if (lane == leader) base = atomicAdd(co.dcount + (kTorus ? 1 : 0), (unsigned long long)__popc(dm));
+        base = __shfl_sync(am, base, leader);
+        if (defer) {
+          unsigned long long slot = base + __popc(dm & ((1u << lane) - 1u));
+          if ((int64_t)slot < co.dcap) (kTorus ? co.dtor : co.dsph)[slot] = e;
+          else atomicExch(C.out.error_flag, 7);
+        }
+      }
+    } else {
       k = intersect_f64_p<PN, kTorus>(f, kind, first, cnt, C.P, pa, ray_dir, t);
-    if (k == 0) continue;
+    }
+    if (k <= 0) continue;
     int pos = atomicAdd(hs.cnt + rid, k);
     for (int i = 0; i < k; i++)
       if (pos + i < kHitCap) hs.t[(int64_t)(pos + i) * hs.nrays + rid] = t[i];
@@ -527,6 +541,10 @@ void launch_isect(const TraceCtx& C, const CandOut& co, const HitStore& hs, int 
   if (precision == 1) {
     k_isect<PN, false, true><<<ig, 256, 0, s>>>(C, co, hs);
     k_isect<PN, true, true><<<ig, 256, 0, s>>>(C, co, hs);
+    // the deferred candidates, in double precision
+    const CandOut dco{co.dsph, co.dtor, co.dcap, co.dcount, nullptr, nullptr, 0, nullptr};
+    k_isect<PN, false, false><<<ig, 256, 0, s>>>(C, dco, hs);
+    k_isect<PN, true, false><<<ig, 256, 0, s>>>(C, dco, hs);
   } else {
     k_isect<PN, false, false><<<ig, 256, 0, s>>>(C, co, hs);
     k_isect<PN, true, false><<<ig, 256, 0, s>>>(C, co, hs);
@@ -537,22 +555,29 @@ void launch_isect(const TraceCtx& C, const CandOut& co, const HitStore& hs, int 
 // interval fill (status runs, insideness bits, pair store, volume).
 __global__ void __launch_bounds__(kTraceThreads) k_fill(TraceCtx C, HitStore hs) {
   constexpr int kThreads = kTraceThreads;
-  const GridDev& g = C.g;
-  const RaySet& rs = C.rs;
+  const int panel = C.set == 0 ? 0 : C.set - 1;
+  const int64_t tile = blockIdx.x;
+  const StructDev& S = C.B.s[C.B.tile_struct[panel][tile]];
+  const GridDev g = S.g;
+  const RaySet rs = make_ray_set(C.set, g);
+  uint32_t* const bits = C.out.bits + S.word_base;
+  const int64_t nwords = S.nwords;
   __shared__ double s_hit[kHitCap * kThreads];
   const int64_t ntm = (rs.nb + kTileM - 1) / kTileM;
-  const int64_t tile = blockIdx.x;
-  const int64_t tm = tile % ntm, tn = tile / ntm;
+  const int64_t lt = tile - S.tile_base[panel];
+  const int64_t tm = lt % ntm, tn = lt / ntm;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t m = tm * kTileM + lane;
   const int64_t n = tn * kTileN + warp;
   const bool valid = (m < rs.nb) && (n < rs.na);
   const int tid = threadIdx.x;
   double* col = s_hit + tid;
-  int hc = valid ? hs.cnt[n * rs.nb + m] : 0;
+  const int64_t lrid = n * rs.nb + m;
+  const int64_t rid = S.ray_base[C.set] + lrid;
+  int hc = valid ? hs.cnt[rid] : 0;
   bool ovf = hc > kHitCap;
   int nh = ovf ? 0 : hc;
-  for (int i = 0; i < nh; i++) col[i * kThreads] = hs.t[(int64_t)i * hs.nrays + n * rs.nb + m];
+  for (int i = 0; i < nh; i++) col[i * kThreads] = hs.t[(int64_t)i * hs.nrays + rid];
   for (int i = 1; i < nh; i++) {
     double v = col[i * kThreads];
     int j = i;
@@ -562,7 +587,6 @@ __global__ void __launch_bounds__(kTraceThreads) k_fill(TraceCtx C, HitStore hs)
     }
     col[j * kThreads] = v;
   }
-  const int64_t rid = n * rs.nb + m;
   if (valid && ovf) {
     int slot = atomicAdd(C.out.ovf_count, 1);
     if (slot < C.out.ovf_cap) C.out.ovf_rays[slot] = (int32_t)rid;
@@ -624,7 +648,7 @@ __global__ void __launch_bounds__(kTraceThreads) k_fill(TraceCtx C, HitStore hs)
   {
     int64_t off = warp_append(C.out.pair_cursor, C.out.pair_cap, np, C.out.error_flag, 3);
     if (valid && !ovf) {
-      int64_t ord = rs.ordinal_base + rid;
+      int64_t ord = S.mc_base + rs.ordinal_base + lrid;
       if (off >= 0) {
         for (int q = 0; q < np; q++) {
           C.out.pairs[2 * (off + q)] = col[(2 * q) * kThreads];
@@ -651,7 +675,7 @@ __global__ void __launch_bounds__(kTraceThreads) k_fill(TraceCtx C, HitStore hs)
         int64_t b = (int64_t)rintp((cr[(2 * q + 1) * kThreads] - vmin) * g.scale);
         int64_t lo = f0 + a + 1, hi = f0 + b;
         if (lo < 0) lo = 0;
-        int64_t maxb = C.nwords * 32 - 1;
+        int64_t maxb = nwords * 32 - 1;
         if (hi > maxb) hi = maxb;
         if (hi < lo) continue;
         for (int64_t w = (lo >> 5) + lane; w <= (hi >> 5); w += 32) {
@@ -659,7 +683,7 @@ __global__ void __launch_bounds__(kTraceThreads) k_fill(TraceCtx C, HitStore hs)
           int s = (int)(lo > wl ? lo - wl : 0);
           int e = (int)(hi < wl + 31 ? hi - wl : 31);
           uint32_t mask = (e - s == 31) ? 0xffffffffu : (((1u << (e - s + 1)) - 1u) << s);
-          atomicAnd(C.out.bits + w, ~mask);
+          atomicAnd(bits + w, ~mask);
         }
       }
     }
@@ -701,8 +725,8 @@ __global__ void __launch_bounds__(kTraceThreads) k_fill(TraceCtx C, HitStore hs)
       if (f0 >= 0) {
         int64_t w = f0 >> 5;
         int s = (int)(f0 & 31);
-        if (w < C.nwords) atomicAnd(C.out.bits + w, ~(mask << s));
-        if (s && w + 1 < C.nwords) atomicAnd(C.out.bits + w + 1, ~(mask >> (32 - s)));
+        if (w < nwords) atomicAnd(bits + w, ~(mask << s));
+        if (s && w + 1 < nwords) atomicAnd(bits + w + 1, ~(mask >> (32 - s)));
       }
     }
   }
@@ -713,12 +737,16 @@ __global__ void k_trace_overflow(TraceCtx C, const int64_t* __restrict__ tile_of
                                  int n_ovf, double* scratch) {
   int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= n_ovf) return;
-  const GridDev& g = C.g;
-  const RaySet& rs = C.rs;
   int64_t rid = C.out.ovf_rays[idx];
-  int64_t m = rid % rs.nb, n = rid / rs.nb;
+  const StructDev& S = C.B.s[find_struct(C.B.ray_base[C.set], C.B.n, rid)];
+  const GridDev g = S.g;
+  const RaySet rs = make_ray_set(C.set, g);
+  uint32_t* const bits = C.out.bits + S.word_base;
+  const int64_t nwords = S.nwords;
+  const int64_t lrid = rid - S.ray_base[C.set];
+  int64_t m = lrid % rs.nb, n = lrid / rs.nb;
   int64_t ntm = (rs.nb + kTileM - 1) / kTileM;
-  int64_t tile = (n / kTileN) * ntm + m / kTileM;
+  int64_t tile = S.tile_base[rs.panel] + (n / kTileN) * ntm + m / kTileM;
   double* col = scratch + (int64_t)idx * kOverflowCap;
   double pa[3], dir[3] = {0., 0., 0.};
   pa[rs.fd] = gcoord(g, rs.fd, m) + rs.delta;
@@ -786,7 +814,7 @@ __global__ void k_trace_overflow(TraceCtx C, const int64_t* __restrict__ tile_of
     }
     return;
   }
-  int64_t ord = rs.ordinal_base + rid;
+  int64_t ord = S.mc_base + rs.ordinal_base + lrid;
   unsigned long long off = np ? atomicAdd(C.out.pair_cursor, (unsigned long long)np) : 0;
   if ((int64_t)off + np <= C.out.pair_cap) {
     for (int q = 0; q < np; q++) {
@@ -805,23 +833,21 @@ __global__ void k_trace_overflow(TraceCtx C, const int64_t* __restrict__ tile_of
     int64_t b = (int64_t)rintp((col[2 * q + 1] - vmin) * g.scale);
     if (rs.panel == 0) {
       int64_t f0 = (n * NY + m) * NX;
-      clear_bits_range(C.out.bits, C.nwords, f0 + a + 1, f0 + b);
+      clear_bits_range(bits, nwords, f0 + a + 1, f0 + b);
     } else {
       for (int64_t v = a + 1; v <= b; v++) {
         int64_t f = (rs.panel == 1) ? ((v * NY + n) * NX + m) : ((n * NY + v) * NX + m);
-        clear_bits_range(C.out.bits, C.nwords, f, f);
+        clear_bits_range(bits, nwords, f, f);
       }
     }
   }
 }
 
-int64_t words_of(const GridDev& g) { return ((g.n[0] + 31) >> 5) * g.n[1] * g.n[2]; }
-
 }  // namespace
 
-cudaError_t launch_windows(const PatchDev& P, int32_t* win, const GridDev& g, cudaStream_t s) {
+cudaError_t launch_windows(const PatchDev& P, int32_t* win, const BatchDev& B, cudaStream_t s) {
   if (P.n == 0) return cudaSuccess;
-  k_windows<<<(unsigned)((P.n + 255) / 256), 256, 0, s>>>(P, win, g);
+  k_windows<<<(unsigned)((P.n + 255) / 256), 256, 0, s>>>(P, win, B);
   return cudaGetLastError();
 }
 
@@ -831,39 +857,40 @@ cudaError_t launch_pool32(const PatchDev& P, float4* pool32, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_bin_count(const PatchDev& P, const GridDev& g, const RaySet& rs, int32_t* tile_cnt,
+cudaError_t launch_bin_count(const PatchDev& P, const BatchDev& B, int set, int32_t* tile_cnt,
                              unsigned long long* area, cudaStream_t s) {
   if (P.n == 0) return cudaSuccess;
-  k_bin<<<(unsigned)((P.n + 255) / 256), 256, 0, s>>>(P, g, rs, tile_cnt, nullptr, nullptr, nullptr, area);
+  k_bin<<<(unsigned)((P.n + 255) / 256), 256, 0, s>>>(P, B, set, tile_cnt, nullptr, nullptr, nullptr, area);
   return cudaGetLastError();
 }
 
-cudaError_t launch_bin_fill(const PatchDev& P, const GridDev& g, const RaySet& rs, const int64_t* tile_off,
+cudaError_t launch_bin_fill(const PatchDev& P, const BatchDev& B, int set, const int64_t* tile_off,
                             int32_t* tile_cursor, int32_t* tile_list, cudaStream_t s) {
   if (P.n == 0) return cudaSuccess;
-  k_bin<<<(unsigned)((P.n + 255) / 256), 256, 0, s>>>(P, g, rs, nullptr, tile_off, tile_cursor, tile_list, nullptr);
+  k_bin<<<(unsigned)((P.n + 255) / 256), 256, 0, s>>>(P, B, set, nullptr, tile_off, tile_cursor, tile_list, nullptr);
   return cudaGetLastError();
 }
 
-cudaError_t launch_trace(const PatchDev& P, const GridDev& g, const RaySet& rs, const int64_t* tile_off,
+cudaError_t launch_trace(const PatchDev& P, const BatchDev& B, int set, int64_t ntiles, const int64_t* tile_off,
                          const int32_t* tile_list, const TraceOut& out, const CandOut& co, const HitStore& hs,
                          int precision, cudaStream_t s) {
-  TraceCtx C{P, g, rs, out, words_of(g)};
-  int64_t ntiles = ((rs.nb + kTileM - 1) / kTileM) * ((rs.na + kTileN - 1) / kTileN);
+  if (ntiles <= 0) return cudaSuccess;
+  TraceCtx C{P, B, set, out};
+  const int panel = set == 0 ? 0 : set - 1;
   k_cand<<<(unsigned)ntiles, kTraceThreads, 0, s>>>(C, tile_off, tile_list, co);
-  if (rs.panel == 0) launch_isect<0>(C, co, hs, precision, s);
-  else if (rs.panel == 1) launch_isect<1>(C, co, hs, precision, s);
+  if (panel == 0) launch_isect<0>(C, co, hs, precision, s);
+  else if (panel == 1) launch_isect<1>(C, co, hs, precision, s);
   else launch_isect<2>(C, co, hs, precision, s);
   k_fill<<<(unsigned)ntiles, kTraceThreads, 0, s>>>(C, hs);
   return cudaGetLastError();
 }
 
-cudaError_t launch_trace_overflow(const PatchDev& P, const GridDev& g, const RaySet& rs, const int64_t* tile_off,
+cudaError_t launch_trace_overflow(const PatchDev& P, const BatchDev& B, int set, const int64_t* tile_off,
                                   const int32_t* tile_list, const TraceOut& out, int n_ovf, double* scratch,
                                   int precision, cudaStream_t s) {
   (void)precision;
   if (n_ovf <= 0) return cudaSuccess;
-  TraceCtx C{P, g, rs, out, words_of(g)};
+  TraceCtx C{P, B, set, out};
   k_trace_overflow<<<(n_ovf + 63) / 64, 64, 0, s>>>(C, tile_off, tile_list, n_ovf, scratch);
   return cudaGetLastError();
 }

@@ -387,6 +387,103 @@ class ConnollySurface(Surface):
         return True
 
 
+class SurfaceBatch:
+    """Many built surfaces, each with its own grid and patch set, ray cast and triangulated in the
+    same kernel launches: one ``getSurf`` + ``triangulateSurface`` per structure, batched.
+
+    Per-structure results are the volumes and areas; the insideness bits come back concatenated.
+    Cavity detection and the dense status map stay with the single-structure ``Surface``.
+    """
+
+    def __init__(self, surfaces: list[Surface], device: int = 0, precision: str | None = None):
+        if not surfaces:
+            raise ValueError("empty batch")
+        for s in surfaces:
+            if s.patches is None or s.delphi is None:
+                raise RuntimeError("every surface of a batch must be built first")
+        self.surfaces = surfaces
+        self.device = device
+        self.precision = (precision or surfaces[0].precision).strip().lower()
+        self.ctx: Context | None = None
+        self.volumes: np.ndarray | None = None
+        self.areas: np.ndarray | None = None
+        self.n_vertices = 0
+        self.n_triangles = 0
+        self.insideness: list[np.ndarray] | None = None
+
+    def __len__(self) -> int:
+        return len(self.surfaces)
+
+    def _context(self) -> Context:
+        if self.ctx is None:
+            self.ctx = Context(self.device)
+        return self.ctx
+
+    def packed(self) -> tuple:
+        """Concatenated patch arrays and their per-structure offsets (host)."""
+        ps = [s.patches for s in self.surfaces]
+        patch_off = np.zeros(len(ps) + 1, np.int64)
+        pool_off = np.zeros(len(ps) + 1, np.int64)
+        patch_off[1:] = np.cumsum([p.n for p in ps])
+        pool_off[1:] = np.cumsum([len(p.pool) for p in ps])
+        f64 = np.ascontiguousarray(np.concatenate([p.f64 for p in ps]))
+        i32 = np.ascontiguousarray(np.concatenate([p.i32 for p in ps]))
+        pool = np.ascontiguousarray(np.concatenate([p.pool for p in ps])) if pool_off[-1] else np.zeros((1, 4))
+        flag = np.ascontiguousarray(np.concatenate([p.pool_flag for p in ps])) if pool_off[-1] else np.zeros(1, np.int8)
+        return patch_off, pool_off, f64, i32, pool, flag
+
+    def upload(self) -> None:
+        c = self._context().handle
+        n = len(self.surfaces)
+        grids = (N.NsGrid * n)(*[s.delphi.grid for s in self.surfaces])
+        N.check(N.lib().nsg_set_batch(c, n, grids), "set_batch")
+        patch_off, pool_off, f64, i32, pool, flag = self.packed()
+        probe = self.surfaces[0].patches.probe
+        N.check(N.lib().nsg_upload_batch(c, N.ptr(patch_off), N.ptr(f64), N.ptr(i32), N.ptr(pool_off), N.ptr(pool),
+                                         N.ptr(flag), probe), "upload_batch")
+
+    def getSurf(self, download: bool = False) -> np.ndarray:
+        """Ray casts every structure's grid; returns the per-structure volumes."""
+        self.upload()
+        c = self._context().handle
+        s0 = self.surfaces[0]
+        flags = 0
+        if s0.delphi.buildStatus:
+            flags |= N.STATUS
+        if s0.accurateTriangulation:
+            flags |= N.ACCURATE_TRIANGULATION
+        prec = PRECISIONS.get(self.precision)
+        if prec is None:
+            raise ValueError(f"unknown Gpu_Precision {self.precision}")
+        vol = ctypes.c_double()
+        N.check(N.lib().nsg_raycast(c, flags, prec, ctypes.byref(vol)), "ray casting")
+        self.volumes = np.zeros(len(self))
+        N.check(N.lib().nsg_batch_results(c, N.ptr(self.volumes), None), "batch results")
+        if download and s0.accurateTriangulation:
+            words = [((s.delphi.grid.nx + 31) >> 5) * s.delphi.grid.ny * s.delphi.grid.nz for s in self.surfaces]
+            bits = np.empty(sum(words), np.uint32)
+            N.check(N.lib().nsg_download_insideness(c, N.ptr(bits)), "download insideness")
+            self.insideness = np.split(bits, np.cumsum(words)[:-1])
+        return self.volumes
+
+    def triangulateSurface(self) -> np.ndarray:
+        """Marching cubes on every structure; returns the per-structure areas."""
+        c = self._context().handle
+        area = ctypes.c_double()
+        nv = ctypes.c_int64()
+        nt = ctypes.c_int64()
+        N.check(N.lib().nsg_triangulate(c, ctypes.byref(area), ctypes.byref(nv), ctypes.byref(nt)), "triangulation")
+        self.n_vertices, self.n_triangles = nv.value, nt.value
+        self.areas = np.zeros(len(self))
+        N.check(N.lib().nsg_batch_results(c, None, N.ptr(self.areas)), "batch results")
+        return self.areas
+
+    def close(self) -> None:
+        if self.ctx is not None:
+            self.ctx.close()
+            self.ctx = None
+
+
 class SurfaceFactory:
     """Surface registry keyed by the .prm ``Surface`` value."""
 

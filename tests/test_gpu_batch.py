@@ -1,0 +1,64 @@
+"""Batched pipeline (nsg_set_batch / nsg_upload_batch): every structure of a batch must give the
+same result as the same structure run alone.  Insideness bits, vertex and triangle counts equal;
+volumes and areas within 1e-12 relative (the per-structure sums are taken in another order).
+The single-structure path is itself checked against the oracle in test_gpu_parity.py.
+"""
+import numpy as np
+import pytest
+
+import nanoshaper_b200 as nb
+from nanoshaper_b200 import generator
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-12
+
+
+def _structures(specs):
+    out = []
+    nb.reset_seed()
+    for n_atoms, seed, scale, perfil in specs:
+        atoms = generator.rsa_globule(n_atoms, seed)
+        cf = nb.ConfigFile()
+        cf.add("Surface", "ses")
+        cf.add("Probe_Radius", 1.4)
+        cf.add("Accurate_Triangulation", True)
+        cf.add("Triangulation", True)
+        ds = nb.DelPhiShared(atoms, scale, perfil)
+        s = nb.surfaceFactory().create(cf, ds)
+        s.build()
+        out.append(s)
+    return out
+
+
+SPECS = [(60, 11, 2.0, 80.0), (327, 1, 2.0, 80.0), (150, 5, 2.5, 70.0), (800, 7, 2.0, 80.0), (40, 2, 3.0, 60.0),
+         (500, 9, 2.0, 80.0)]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batch_matches_single(precision, native_lib):
+    surfs = _structures(SPECS)
+    vols, areas, bits, nv, nt = [], [], [], 0, 0
+    for s in surfs:
+        s.precision = precision
+        vols.append(s.getSurf(True, False, 0.0))
+        areas.append(s.triangulateSurface())
+        bits.append(s.insideness.copy())
+        nv += len(s.vertices)
+        nt += len(s.triangles)
+        s.ctx.close()
+        s.ctx = None
+    batch = nb.SurfaceBatch(surfs, precision=precision)
+    bvol = batch.getSurf(download=True)
+    barea = batch.triangulateSurface()
+    for b in range(len(surfs)):
+        assert np.array_equal(batch.insideness[b], bits[b]), f"structure {b}: insideness bits differ"
+        assert abs(bvol[b] - vols[b]) <= RTOL * abs(vols[b]), f"structure {b}: volume {bvol[b]} vs {vols[b]}"
+        assert abs(barea[b] - areas[b]) <= RTOL * abs(areas[b]), f"structure {b}: area {barea[b]} vs {areas[b]}"
+    assert batch.n_vertices == nv
+    assert batch.n_triangles == nt
+    # a second pass over the same batch gives the same numbers
+    bvol2 = batch.getSurf()
+    barea2 = batch.triangulateSurface()
+    assert np.array_equal(bvol, bvol2) and np.array_equal(barea, barea2)
+    batch.close()
