@@ -38,7 +38,14 @@ sys.path.insert(0, str(ROOT))
 METRIC = "structures/s and rays/s, mixed-prec vs FP64 GPU kernel at ≤1e-5 Å hit error"
 
 WORKLOADS = {
-    # name: atoms, generator seed, probe, scale, perfil, cavity fill threshold
+    # conformer ensemble: 32 globules of 500..8000 atoms, 16 perturbations (0.3 A) each, every
+    # structure on its own grid, one batch
+    "ensemble_512": dict(n_base=32, n_perturb=16, n_min=500, n_max=8000, sigma=0.3, seed=5, probe=1.4, scale=2.0,
+                         perfil=80.0),
+    # the same generator with 4 globules (profiling-size case)
+    "ensemble_64": dict(n_base=4, n_perturb=16, n_min=500, n_max=8000, sigma=0.3, seed=5, probe=1.4, scale=2.0,
+                        perfil=80.0),
+    # single structures: atoms, generator seed, probe, scale, perfil, cavity fill threshold
     "ses_100k": dict(n=100000, seed=3, probe=1.4, scale=4.0, perfil=70.0, cav_vol=10.0),
     "ses_10k": dict(n=10000, seed=2, probe=1.4, scale=3.0, perfil=80.0, cav_vol=10.0),
     "ses_327": dict(n=327, seed=1, probe=1.4, scale=2.0, perfil=70.0, cav_vol=10.0),
@@ -160,18 +167,333 @@ def run_reference(args, w, ds, surf) -> dict:
             "unit": "structures/s"}
 
 
+def make_ensemble(w: dict):
+    """Seeded conformer ensemble and its SES patch sets (host)."""
+    from nanoshaper_b200 import generator
+    import nanoshaper_b200 as nb
+    t0 = time.perf_counter()
+    atoms = generator.ensemble(w["n_base"], w["n_perturb"], w["n_min"], w["n_max"], w["sigma"], w["seed"])
+    t_gen = time.perf_counter() - t0
+    nb.reset_seed()
+    surfs = []
+    t0 = time.perf_counter()
+    for a in atoms:
+        ds = nb.DelPhiShared(a, w["scale"], w["perfil"])
+        cf = nb.ConfigFile()
+        cf.add("Surface", "ses")
+        cf.add("Probe_Radius", w["probe"])
+        cf.add("Accurate_Triangulation", True)
+        cf.add("Triangulation", True)
+        sf = nb.surfaceFactory().create(cf, ds)
+        sf.build()
+        surfs.append(sf)
+    t_build = time.perf_counter() - t0
+    return atoms, surfs, t_gen, t_build
+
+
+def rays_of(g) -> int:
+    """Rays of one structure: the status ray set and the three accurate-triangulation ray sets."""
+    return g.nz * g.ny + (g.nz * g.ny + g.ny * g.nx + g.nz * g.nx)
+
+
+def ensemble_cpu_baseline(surfs, threads: int, target_s: float = 10.0, steps: int = 1) -> dict:
+    """Oracle ray casting on a central slab of the first structure, all host threads; structures/s
+    scaled by the ensemble's mean rays per structure."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+    O.build()
+    s0 = surfs[0]
+    g = s0.delphi.grid
+    t_probe, r_probe = O.time_slab(g, s0.patches, threads, 0.45, 0.55)
+    per_ray = t_probe / max(r_probe, 1)
+    frac = min(1.0, max(0.05, target_s / max(per_ray * rays_of(g), 1e-9)))
+    lo, hi = 0.5 - frac / 2, 0.5 + frac / 2
+    times, rays = [], 0
+    for _ in range(steps):
+        dt, rays = O.time_slab(g, s0.patches, threads, lo, hi)
+        times.append(dt)
+    t = max(statistics.median(times), 1e-9)
+    rays_per_s = rays / t
+    mean_rays = statistics.mean(rays_of(sf.delphi.grid) for sf in surfs)
+    sample = (f"ray casting (status + 3 triangulation ray sets) of the slab [{lo:.3f}, {hi:.3f}) of structure 0 "
+              f"({len(s0.delphi.atoms)} atoms, grid {g.nx}x{g.ny}x{g.nz}): {rays} rays; structures/s = rays/s / "
+              f"mean rays per structure ({mean_rays:.0f}); marching cubes not included")
+    return {"value": rays_per_s / mean_rays, "rays_per_s": rays_per_s, "cores": threads, "kind": "port",
+            "sample": sample, "unit": "structures/s"}
+
+
+def run_ensemble(args, world: int, rank: int, local: int) -> None:
+    """Batched conformer ensemble: one step = ray casting (4 ray sets) + marching cubes of every
+    structure of the ensemble in one batch; value = structures/s over all ranks (replicas)."""
+    w = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        atoms, surfs, t_gen, t_build = make_ensemble(w)
+        threads = os.cpu_count() or 1
+        cb = ensemble_cpu_baseline(surfs, threads, steps=max(args.steps, 1))
+        line = {
+            "impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "structures/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "rays_per_s": cb["rays_per_s"],
+            "config": {"workload": args.workload, "structures": len(surfs),
+                       "atoms_total": int(sum(len(a) for a in atoms)), "probe": w["probe"], "scale": w["scale"],
+                       "perfil": w["perfil"]},
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": cb["value"], "unit": "structures/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line))
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        pg = dist
+
+    import nanoshaper_b200 as nb
+    from nanoshaper_b200 import _native as N
+    from nanoshaper_b200 import build as nbuild
+    nbuild.build()
+    L = N.lib()
+
+    def barrier():
+        if pg is not None:
+            pg.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x: float) -> float:
+        if pg is None:
+            return x
+        t = torch.tensor([x], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    atoms, surfs, t_gen, t_build = make_ensemble(w)
+    nstruct = len(surfs)
+    prec = 0 if args.precision == "fp64" else 1
+    batch = nb.SurfaceBatch(surfs, device=local, precision=args.precision)
+    batch.upload()
+    ctx = batch._context().handle
+    flags = N.STATUS | N.ACCURATE_TRIANGULATION
+
+    def step(precision: int):
+        v = ctypes.c_double()
+        N.check(L.nsg_raycast(ctx, flags, precision, ctypes.byref(v)), "raycast")
+        a = ctypes.c_double()
+        nv = ctypes.c_int64()
+        nt = ctypes.c_int64()
+        N.check(L.nsg_triangulate(ctx, ctypes.byref(a), ctypes.byref(nv), ctypes.byref(nt)), "triangulate")
+        return nv.value, nt.value
+
+    def timed(precision: int, steps: int) -> float:
+        N.check(L.nsg_event_record(ctx, 0), "event")
+        for _ in range(steps):
+            step(precision)
+        N.check(L.nsg_event_record(ctx, 1), "event")
+        ms = ctypes.c_double()
+        N.check(L.nsg_event_elapsed(ctx, 0, 1, ctypes.byref(ms)), "elapsed")
+        return ms.value / steps
+
+    def results():
+        vol = np.zeros(nstruct)
+        area = np.zeros(nstruct)
+        N.check(L.nsg_batch_results(ctx, N.ptr(vol), N.ptr(area)), "batch results")
+        return vol, area
+
+    # double-precision batch: reference numbers for the accuracy comparison
+    step(0)
+    vol64, area64 = results()
+    # per-stage kernel times of the measured precision from one profiled pass
+    step(prec)
+    N.check(L.nsg_profile(ctx, 1), "profile")
+    step(prec)
+    stage_ms = np.zeros(8)
+    stage_calls = np.zeros(8, np.int64)
+    L.nsg_stage_times(ctx, stage_ms.ctypes.data, stage_calls.ctypes.data, 8)
+    counters = np.zeros(8, np.int64)
+    L.nsg_trace_counters(ctx, counters.ctypes.data, 8)
+    N.check(L.nsg_profile(ctx, 0), "profile")
+
+    for _ in range(args.warmup):
+        nv, nt = step(prec)
+    barrier()
+    clk = ClockSampler(local)
+    clk.start()
+    launches0 = L.nsg_launch_count(ctx)
+    ms_per_step = timed(prec, args.steps)
+    launches = L.nsg_launch_count(ctx) - launches0
+    barrier()
+    clocks = clk.stop()
+    ms_per_step = max_over_ranks(ms_per_step)
+    vol, area = results()
+
+    # the same batch in double precision, and the plain per-structure double-precision path
+    ms_fp64_batch = max_over_ranks(timed(0, max(1, min(args.steps, 3))))
+    plain = nb.Context(local)
+    dev = torch.device("cuda", local)
+    dpatch = []
+    for sf in surfs:
+        p = sf.patches
+        dpatch.append([torch.from_numpy(x).to(dev) for x in (p.f64, p.i32, p.pool, p.pool_flag)])
+    torch.cuda.synchronize()
+
+    def plain_pass(count: int) -> None:
+        for b in range(count):
+            sf, (f64, i32, pool, flag) = surfs[b], dpatch[b]
+            p = sf.patches
+            N.check(L.nsg_set_grid(plain.handle, ctypes.byref(sf.delphi.grid)), "set_grid")
+            N.check(L.nsg_bind_patches_device(plain.handle, p.n, f64.data_ptr(), i32.data_ptr(), len(p.pool),
+                                              pool.data_ptr(), flag.data_ptr(), p.probe), "bind")
+            v = ctypes.c_double()
+            N.check(L.nsg_raycast(plain.handle, flags, 0, ctypes.byref(v)), "raycast")
+            a = ctypes.c_double()
+            nv_, nt_ = ctypes.c_int64(), ctypes.c_int64()
+            N.check(L.nsg_triangulate(plain.handle, ctypes.byref(a), ctypes.byref(nv_), ctypes.byref(nt_)), "tri")
+
+    plain_pass(min(8, nstruct))
+    torch.cuda.synchronize()
+    N.check(L.nsg_event_record(plain.handle, 0), "event")
+    plain_pass(nstruct)
+    N.check(L.nsg_event_record(plain.handle, 1), "event")
+    pms = ctypes.c_double()
+    N.check(L.nsg_event_elapsed(plain.handle, 0, 1, ctypes.byref(pms)), "elapsed")
+    ms_plain = max_over_ranks(pms.value)
+    plain.close()
+    del dpatch
+
+    # e2e: patch sets from pinned host memory, the batch, per-structure results back to the host
+    patch_off, pool_off, f64, i32, pool, flag = batch.packed()
+    pin = {}
+    for name, a in (("f64", f64), ("i32", i32), ("pool", pool), ("flag", flag)):
+        t = torch.empty(a.nbytes, dtype=torch.uint8, pin_memory=True)
+        t.numpy()[:] = a.view(np.uint8).ravel()
+        pin[name] = t
+    grids = (N.NsGrid * nstruct)(*[sf.delphi.grid for sf in surfs])
+    h2d = sum(t.numel() for t in pin.values())
+    vol_h = np.zeros(nstruct)
+    area_h = np.zeros(nstruct)
+
+    def e2e_step():
+        N.check(L.nsg_set_batch(ctx, nstruct, grids), "set_batch")
+        N.check(L.nsg_upload_batch(ctx, N.ptr(patch_off), pin["f64"].data_ptr(), pin["i32"].data_ptr(),
+                                   N.ptr(pool_off), pin["pool"].data_ptr(), pin["flag"].data_ptr(),
+                                   surfs[0].patches.probe), "upload_batch")
+        step(prec)
+        N.check(L.nsg_batch_results(ctx, N.ptr(vol_h), N.ptr(area_h)), "batch results")
+
+    e2e_step()
+    barrier()
+    e2e_steps = max(2, min(args.steps, 5))
+    N.check(L.nsg_event_record(ctx, 2), "event")
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    N.check(L.nsg_event_record(ctx, 3), "event")
+    e2e_wall = (time.perf_counter() - t0) / e2e_steps
+    e_ms = ctypes.c_double()
+    N.check(L.nsg_event_elapsed(ctx, 2, 3, ctypes.byref(e_ms)), "elapsed")
+    e2e_ms = max_over_ranks(max(e_ms.value / e2e_steps, e2e_wall * 1000.0))
+    d2h = 2 * 8 * nstruct
+
+    grids_l = [sf.delphi.grid for sf in surfs]
+    rays = sum(rays_of(g) for g in grids_l)
+    nodes = sum(g.nx * g.ny * g.nz for g in grids_l)
+    nwords = sum(((g.nx + 31) // 32) * g.ny * g.nz for g in grids_l)
+    structs_per_s = world * nstruct * 1000.0 / ms_per_step
+    hit_store_gb = max(sum(g.ny * g.nz for g in grids_l), sum(g.nx * g.ny for g in grids_l),
+                       sum(g.nx * g.nz for g in grids_l)) * 32 * 8 / 1e9
+
+    peaks = load_peaks()
+    stage_times = {STAGES[i]: float(stage_ms[i]) for i in range(len(STAGES))}
+    dominant = max(stage_times, key=stage_times.get)
+    alg_bytes = {
+        # bit grids cleared by three ray sets (read + write), per-ray interval sums, pair records
+        "trace": 3 * 2 * 4 * nwords + 8 * rays + 16 * nv,
+        "overflow": 8 * rays,
+        "bin": 6 * 4 * sum(sf.patches.n for sf in surfs),
+        "cavity": 0,
+        "vertex": 8 * 2 * nv + 40 * nv,
+        # bit rows read by both passes of the row classification, vertices, triangles
+        "mc": nwords * 4 * 8 + 40 * nv + 12 * nt,
+    }
+    dom_ms = stage_times[dominant] / max(int(stage_calls[STAGES.index(dominant)]), 1)
+    achieved = alg_bytes[dominant] / (dom_ms / 1000.0) / 1e9
+    roofline = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / peaks["hbm_gbs"], "traffic": None, "peak_source": peaks["source"],
+                "stage_ms": stage_times, "algorithmic_bytes": alg_bytes[dominant]}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cb = ensemble_cpu_baseline(surfs, os.cpu_count() or 1)
+            cpu = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+            cpu["rays_per_s"] = cb["rays_per_s"]
+        except Exception as e:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": "structures/s", "cores": 0, "kind": "port", "sample": f"failed: {e}"}
+
+    def rel(a, b):
+        return float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-300)))
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": structs_per_s, "unit": "structures/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+            "precision": args.precision, "data": "synthetic",
+            "rays_per_s": structs_per_s * rays / nstruct, "nodes_per_s": structs_per_s * nodes / nstruct,
+            "config": {"workload": args.workload, "structures": nstruct,
+                       "atoms_total": int(sum(len(a) for a in atoms)), "probe": w["probe"], "scale": w["scale"],
+                       "perfil": w["perfil"], "rays_per_step": rays, "nodes_per_step": nodes,
+                       "l2": "inputs larger than L2 (hit store %.1f GB, bit grids %.2f GB)" % (
+                           hit_store_gb, nwords * 4 / 1e9),
+                       "parallelism": f"replicas x{world}"},
+            "comparison": {
+                "fp64_batched_structures_per_s": world * nstruct * 1000.0 / ms_fp64_batch,
+                "fp64_plain_per_structure_structures_per_s": world * nstruct * 1000.0 / ms_plain,
+                "speedup_vs_fp64_plain": ms_plain / ms_per_step,
+                "speedup_vs_fp64_batched": ms_fp64_batch / ms_per_step,
+                "max_rel_volume_diff_vs_fp64": rel(vol, vol64), "max_rel_area_diff_vs_fp64": rel(area, area64),
+            },
+            "result": {"volume_sum": float(vol.sum()), "area_sum": float(area.sum()), "vertices": nv,
+                       "triangles": nt},
+            "host": {"patch_build_s": t_build, "generator_s": t_gen},
+            "clocks": clocks,
+            "e2e": {"value": world * nstruct * 1000.0 / e2e_ms, "unit": "structures/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms},
+            "gpu_launches": int(launches),
+            "trace_counters": dict(zip(("candidates", "torus_candidates", "deferred_sphere", "deferred_quartic",
+                                        "deferred_root"), counters[:5].tolist())),
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    batch.close()
+    if pg is not None:
+        pg.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
-    ap.add_argument("--workload", default="ses_100k", choices=sorted(WORKLOADS))
-    ap.add_argument("--precision", default="fp64", choices=("fp64", "mixed"))
+    ap.add_argument("--workload", default="ensemble_512", choices=sorted(WORKLOADS))
+    ap.add_argument("--precision", default=None, choices=("fp64", "mixed"),
+                    help="default: mixed for the ensembles, fp64 for single structures")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+    if args.precision is None:
+        args.precision = "mixed" if args.workload.startswith("ensemble") else "fp64"
     world, rank, local = dist_setup()
+    if args.workload.startswith("ensemble"):
+        return run_ensemble(args, world, rank, local)
 
     if args.impl == "reference":
         if rank != 0:

@@ -74,7 +74,8 @@ struct nsg_ctx {
   int32_t nstruct = 0;
   std::vector<NsGrid> grids;
   std::vector<nsg::StructDev> sd;
-  DevBuf d_sd, d_patch_struct, d_tile_struct[3], d_ray_base[4], d_mc_base, d_row_base;
+  DevBuf d_sd, d_patch_struct, d_tile_struct[3], d_ray_base[4], d_mc_base, d_row_base, d_row_chunks;
+  int64_t nchunks = 0;
   int64_t tiles_tot[3] = {0, 0, 0}, rays_tot[4] = {0, 0, 0, 0}, mc_tot = 0, rows_tot = 0, words_tot = 0;
   int32_t patch_nstruct = 0;  // structures the uploaded patches belong to
   bool patch_struct_valid = false;
@@ -184,6 +185,8 @@ int batch_layout(nsg_ctx* c, const NsGrid* grids, int32_t n) {
   std::vector<nsg::StructDev> sd(n);
   std::vector<int64_t> rb[4], mcb(n + 1), rowb(n + 1);
   std::vector<int32_t> ts[3];
+  std::vector<int4> chunks;  // marching-cubes row chunks: structure, first row, row count
+  constexpr int32_t kRowChunk = 64;
   for (int i = 0; i < 4; i++) rb[i].resize(n + 1);
   int64_t tiles[3] = {0, 0, 0}, rays[4] = {0, 0, 0, 0}, mc = 0, rows = 0, words = 0;
   for (int32_t b = 0; b < n; b++) {
@@ -210,7 +213,10 @@ int batch_layout(nsg_ctx* c, const NsGrid* grids, int32_t n) {
     S.mc_base = mcb[b] = mc;
     mc += G.nz * G.ny + G.ny * G.nx + G.nz * G.nx;
     S.row_base = rowb[b] = rows;
-    rows += (G.ny - 2) * (G.nz - 2);
+    const int64_t srows = (G.ny - 2) * (G.nz - 2);
+    for (int64_t r = 0; r < srows; r += kRowChunk)
+      chunks.push_back(make_int4(b, (int32_t)r, (int32_t)std::min<int64_t>(kRowChunk, srows - r), 0));
+    rows += srows;
     for (int d = 0; d < 3; d++) {
       S.ray_dir[d] = (S.g.mn[d] + (double)(S.g.n[d] - 1) * S.g.side) - (S.g.mn[d] + 0.0 * S.g.side);
       S.inv_dir[d] = 1.0 / S.ray_dir[d];
@@ -227,7 +233,9 @@ int batch_layout(nsg_ctx* c, const NsGrid* grids, int32_t n) {
   for (int i = 0; i < 4; i++) CK(upload_vec(c->d_ray_base[i], rb[i], c->stream));
   CK(upload_vec(c->d_mc_base, mcb, c->stream));
   CK(upload_vec(c->d_row_base, rowb, c->stream));
+  CK(upload_vec(c->d_row_chunks, chunks, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  c->nchunks = (int64_t)chunks.size();
   c->nstruct = n;
   c->grids.assign(grids, grids + n);
   c->sd = sd;
@@ -430,6 +438,7 @@ int nsg_ctx_destroy(nsg_ctx* c) {
   for (DevBuf* b : bufs) b->release();
   for (int i = 0; i < 3; i++) { c->tile_cnt[i].release(); c->tile_off[i].release(); c->tile_list[i].release(); }
   c->d_sd.release(); c->d_patch_struct.release(); c->d_mc_base.release(); c->d_row_base.release();
+  c->d_row_chunks.release();
   c->vol_struct.release(); c->area_struct.release();
   for (int i = 0; i < 3; i++) c->d_tile_struct[i].release();
   for (int i = 0; i < 4; i++) c->d_ray_base[i].release();
@@ -725,7 +734,16 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
     if (c->profile) {
       CK(cudaMemcpyAsync(c->counter_host, c->counters.p, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                          c->stream));
+      unsigned long long cand[8];
+      CK(cudaMemcpyAsync(cand, cur + 8, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
       CK(cudaStreamSynchronize(c->stream));
+      // candidate pairs (spheres + tori) and torus pairs of all ray sets
+      c->counter_host[nsg::kCntCandidates] = 0;
+      c->counter_host[nsg::kCntTorus] = 0;
+      for (int si = 0; si < nsets; si++) {
+        c->counter_host[nsg::kCntCandidates] += cand[2 * sets[si]] + cand[2 * sets[si] + 1];
+        c->counter_host[nsg::kCntTorus] += cand[2 * sets[si] + 1];
+      }
     }
     int32_t errflag = 0;
     unsigned long long used[3] = {0, 0, 0};
@@ -910,6 +928,8 @@ int nsg_triangulate(nsg_ctx* c, double* area_out, int64_t* nverts, int64_t* ntri
   CK(c->row_act_off.ensure((nrows + 1) * sizeof(int64_t)));
   nsg::MCArgs M{};
   M.B = B;
+  M.row_chunks = c->d_row_chunks.as<int4>();
+  M.nchunks = c->nchunks;
   M.bits = c->bits.as<uint32_t>();
   M.surv_cnt = c->surv_cnt.as<int32_t>();
   M.surv_off = c->surv_off.as<int64_t>();

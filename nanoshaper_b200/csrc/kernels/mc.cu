@@ -6,7 +6,7 @@
 // (assembleVerticesList src/Surface.cpp:7415-7667).  Vertices keep the reference order: panel 0
 // rays (z-major), panel 1 rays (y-major), panel 2 rays (z-major), pairs in ray order.  Because a
 // ray's surviving vertices are sorted along the ray, the vertex of a grid edge is found by a
-// short scan of that one ray's survivors, so no dense edge-index grids are needed.
+// binary search over that one ray's survivors, so no dense edge-index grids are needed.
 //
 // Marching cubes: cubes (i,j,k) in [1, N-2]^3 are classified from the 8 insideness bits; active
 // cubes add an edge-midpoint vertex to their own edges 5, 6, 10 that carry no analytic vertex,
@@ -122,14 +122,16 @@ __device__ __forceinline__ int64_t analytic_vertex(const MCArgs& A, const Struct
   r += S.mc_base;
   int cnt = A.surv_cnt[r];
   if (cnt == 0) return -1;
-  int64_t off = A.surv_off[r];
-  for (int s = 0; s < cnt; s++) {
-    int4 key = A.vkey[off + s];
-    int along = dir == NS_X_DIR ? key.x : (dir == NS_Y_DIR ? key.y : key.z);
-    if (along == e) return off + s;
-    if (along > e) break;
+  // the ray's survivors are sorted along the ray: first one at position >= e
+  const int64_t off = A.surv_off[r];
+  const int* kv = (const int*)(A.vkey + off) + (dir == NS_X_DIR ? 0 : (dir == NS_Y_DIR ? 1 : 2));
+  int lo = 0, hi = cnt;
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (kv[4 * mid] < e) lo = mid + 1;
+    else hi = mid;
   }
-  return -1;
+  return (lo < cnt && kv[4 * lo] == e) ? off + lo : -1;
 }
 
 // Midpoint vertices a cube creates on its own edges 5 (y), 6 (x), 10 (z): bit 0, 1, 2.
@@ -154,64 +156,79 @@ __device__ __forceinline__ uint32_t bits32(const uint32_t* __restrict__ bits, in
   return __funnelshift_r(lo, hi, s);
 }
 
-// One warp per cube row (j, k); every lane classifies 32 consecutive cubes at once from the four
-// bit rows the cubes touch (corner inside = bit 0): a cube is active unless its 8 corners agree.
-// Pass 0 counts the active cubes of the row, pass 1 writes them in i order.
+// Cube rows (j, k) in chunks of consecutive rows of one structure, one warp per chunk.  Every
+// lane classifies 32 consecutive cubes of a row at once from the four bit rows the cubes touch
+// (corner inside = bit 0): a cube is active unless its 8 corners agree.  A row needs
+// W = ceil((NX-2)/32) lanes; when W <= 32 the warp packs 32/W rows side by side, otherwise it walks
+// the row in blocks of 32 words.  Pass 0 counts the active cubes of each row, pass 1 writes them
+// in i order at the row's offset.
 __global__ void k_mc_rows(MCArgs A, int emit) {
   const int lane = threadIdx.x & 31;
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-  for (int64_t row = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); row < A.nrows; row += warps) {
-    const int b = find_struct(A.B.row_base, A.B.n, row);
-    const StructDev& S = A.B.s[b];
-    const int64_t NX = S.g.n[0], NY = S.g.n[1];
+  for (int64_t ch = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); ch < A.nchunks; ch += warps) {
+    const int4 C = A.row_chunks[ch];  // structure, first local row, row count
+    const StructDev& S = A.B.s[C.x];
+    const int NX = (int)S.g.n[0], NY = (int)S.g.n[1];
     const uint32_t* bits = A.bits + S.word_base;
     const int64_t nwords = S.nwords;
-    const int64_t lrow = row - S.row_base;
-    int64_t j = 1 + lrow % (NY - 2);
-    int64_t k = 1 + lrow / (NY - 2);
-    const int64_t b00 = (k * NY + j) * NX, b10 = b00 + NX, b01 = b00 + NX * NY, b11 = b01 + NX;
-    int64_t act_run = 0;
-    int64_t act_base = emit ? A.row_act_off[row] : 0;
-    for (int64_t i0 = 1; i0 < NX - 1; i0 += 32 * 32) {
-      int64_t ic = i0 + 32 * lane;
-      uint32_t act = 0;
-      uint32_t c[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-      if (ic < NX - 1) {
-        int64_t nvalid = NX - 1 - ic;
-        uint32_t vm = nvalid >= 32 ? 0xffffffffu : ((1u << nvalid) - 1u);
-        c[0] = ~bits32(bits, nwords, b00 + ic);
-        c[1] = ~bits32(bits, nwords, b00 + ic + 1);
-        c[2] = ~bits32(bits, nwords, b10 + ic + 1);
-        c[3] = ~bits32(bits, nwords, b10 + ic);
-        c[4] = ~bits32(bits, nwords, b01 + ic);
-        c[5] = ~bits32(bits, nwords, b01 + ic + 1);
-        c[6] = ~bits32(bits, nwords, b11 + ic + 1);
-        c[7] = ~bits32(bits, nwords, b11 + ic);
-        uint32_t d = 0;
+    const int W = (NX - 2 + 31) >> 5;
+    const int WB = W < 32 ? W : 32;
+    const int R = 32 / WB;
+    const int NB = (W + 31) >> 5;
+    const int sub = lane / WB, wl = lane - sub * WB;
+    const int head = sub * WB;
+    const int tail = head + WB - 1 < 31 ? head + WB - 1 : 31;
+    for (int r0 = 0; r0 < C.z; r0 += R) {
+      const bool row_ok = sub < R && r0 + sub < C.z;
+      const int lr = C.y + r0 + (row_ok ? sub : 0);
+      const int j = 1 + lr % (NY - 2), k = 1 + lr / (NY - 2);
+      const int64_t grow = S.row_base + lr;
+      const int64_t b00 = ((int64_t)k * NY + j) * NX, b10 = b00 + NX, b01 = b00 + (int64_t)NX * NY, b11 = b01 + NX;
+      const int64_t act_base = (emit && row_ok) ? A.row_act_off[grow] : 0;
+      int64_t run = 0;
+      for (int wb = 0; wb < NB; wb++) {
+        const int word = wb * 32 + wl;
+        const int64_t ic = 1 + 32 * (int64_t)word;
+        uint32_t act = 0;
+        uint32_t c[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        if (row_ok && word < W) {
+          int64_t nvalid = NX - 1 - ic;
+          uint32_t vm = nvalid >= 32 ? 0xffffffffu : ((1u << nvalid) - 1u);
+          c[0] = ~bits32(bits, nwords, b00 + ic);
+          c[1] = ~bits32(bits, nwords, b00 + ic + 1);
+          c[2] = ~bits32(bits, nwords, b10 + ic + 1);
+          c[3] = ~bits32(bits, nwords, b10 + ic);
+          c[4] = ~bits32(bits, nwords, b01 + ic);
+          c[5] = ~bits32(bits, nwords, b01 + ic + 1);
+          c[6] = ~bits32(bits, nwords, b11 + ic + 1);
+          c[7] = ~bits32(bits, nwords, b11 + ic);
+          uint32_t d = 0;
 #pragma unroll
-        for (int q = 1; q < 8; q++) d |= c[0] ^ c[q];
-        act = d & vm;
-      }
-      int na = __popc(act);
-      int ia = na;
-      for (int o = 1; o < 32; o <<= 1) {
-        int va = __shfl_up_sync(0xffffffffu, ia, o);
-        if (lane >= o) ia += va;
-      }
-      int ta = __shfl_sync(0xffffffffu, ia, 31);
-      if (emit && na) {
-        int64_t slot = act_base + act_run + ia - na;
-        for (uint32_t m = act; m; m &= m - 1) {
-          int bit = __ffs(m) - 1;
-          int cs = 0;
-#pragma unroll
-          for (int q = 0; q < 8; q++) cs |= ((c[q] >> bit) & 1u) << q;
-          A.act_rec[slot++] = make_int4((int)(ic + bit), (int)j, (int)k, cs | (b << 11));
+          for (int q = 1; q < 8; q++) d |= c[0] ^ c[q];
+          act = d & vm;
         }
+        const int na = __popc(act);
+        int incl = na;
+        for (int o = 1; o < 32; o <<= 1) {
+          int v = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += v;
+        }
+        const int head_excl = __shfl_sync(0xffffffffu, incl - na, head);
+        const int row_total = __shfl_sync(0xffffffffu, incl, tail) - head_excl;
+        if (emit && na) {
+          int64_t slot = act_base + run + (incl - na - head_excl);
+          for (uint32_t m = act; m; m &= m - 1) {
+            int bit = __ffs(m) - 1;
+            int cs = 0;
+#pragma unroll
+            for (int q = 0; q < 8; q++) cs |= ((c[q] >> bit) & 1u) << q;
+            A.act_rec[slot++] = make_int4((int)(ic + bit), j, k, cs | (C.x << 11));
+          }
+        }
+        run += row_total;
       }
-      act_run += ta;
+      if (!emit && row_ok && wl == 0) A.row_act_cnt[grow] = run;
     }
-    if (!emit && lane == 0) A.row_act_cnt[row] = act_run;
   }
 }
 
@@ -311,19 +328,19 @@ __global__ void k_mc_tris(MCArgs A, int emit) {
     int c = rec.w & 255;
     int64_t i = rec.x, j = rec.y, k = rec.z;
     const StructDev& S = A.B.s[rec_struct(rec.w)];
-    int64_t vl[12];
+    int32_t vl[12];
     int em = c_emask[c];
-    for (int e = 0; e < 12; e++) vl[e] = (em >> e) & 1 ? edge_vertex(A, S, e, i, j, k) : -1;
+    for (int e = 0; e < 12; e++) vl[e] = (em >> e) & 1 ? (int32_t)edge_vertex(A, S, e, i, j, k) : -1;
     int cnt = 0;
     int64_t o = emit ? A.tri_off[a] : 0;
     double area = 0.0;
     for (int q = 0; q < 16 && c_tri[c][q] >= 0; q += 3) {
-      int64_t v0 = vl[c_tri[c][q]], v1 = vl[c_tri[c][q + 1]], v2 = vl[c_tri[c][q + 2]];
+      int32_t v0 = vl[c_tri[c][q]], v1 = vl[c_tri[c][q + 1]], v2 = vl[c_tri[c][q + 2]];
       if (v0 < 0 || v1 < 0 || v2 < 0) continue;
       if (emit) {
-        const double* P0 = A.vpos + 3 * v0;
-        const double* P1 = A.vpos + 3 * v1;
-        const double* P2 = A.vpos + 3 * v2;
+        const double* P0 = A.vpos + 3 * (int64_t)v0;
+        const double* P1 = A.vpos + 3 * (int64_t)v1;
+        const double* P2 = A.vpos + 3 * (int64_t)v2;
         double da = vdist(P0, P1), db = vdist(P0, P2), dc = vdist(P1, P2);
         double ttt = (da + db + dc) * (db + dc - da) * (dc + da - db) * (da + db - dc);
         if (ttt > 0) area += 0.25 * sqrt(ttt);
@@ -371,9 +388,8 @@ cudaError_t launch_vert(const VertArgs& A, int emit, cudaStream_t s) {
 }
 
 cudaError_t launch_mc_rows(const MCArgs& A, int emit, cudaStream_t s) {
-  if (A.nrows <= 0) return cudaSuccess;
-  int64_t warps = A.nrows;
-  k_mc_rows<<<grid_for(warps * 32, 256), 256, 0, s>>>(A, emit);
+  if (A.nchunks <= 0) return cudaSuccess;
+  k_mc_rows<<<grid_for(A.nchunks * 32, 256), 256, 0, s>>>(A, emit);
   return cudaGetLastError();
 }
 

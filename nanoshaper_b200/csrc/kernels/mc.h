@@ -31,6 +31,8 @@ struct MCArgs {
   double* vpos;
   int4* vkey;
   int64_t nrows;                 // cube rows, (NY-2)*(NZ-2) per structure
+  const int4* row_chunks;        // structure, first local row, row count (consecutive rows)
+  int64_t nchunks;
   int64_t* row_act_cnt;
   const int64_t* row_act_off;    // nrows+1 entries
   int4* act_rec;                 // i, j, k, case | midpoint mask << 8 | structure << 11

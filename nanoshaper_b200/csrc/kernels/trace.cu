@@ -229,7 +229,6 @@ __device__ __forceinline__ int intersect_mixed(const double* f, int kind, int fi
     torus_coeffs_f64(f, P.probe, vc, orig1, &B, &C, &D, &E);
     float rt[4];
     int nr = quartic_mixed(rt, B, C, D, E);
-    if (ctr) atomicAdd(ctr + kCntTorus, 1ull);
     if (nr < 0) {
       if (ctr) atomicAdd(ctr + kCntFbQuartic, 1ull);
       return kDefer;
