@@ -1,16 +1,20 @@
 #!/usr/bin/env python
 """Benchmark of the B200 grid ray-casting surface builder.
 
-One step = one full surface pass of one structure: ray casting of the status ray set and the
-three accurate-triangulation ray sets (hits, status map, insideness bits, volume), cavity
-detection and filling, vertex assembly and marching cubes.  ``value`` is measured with the patch
-set resident in HBM; ``e2e`` is the same pass through the C-ABI with host buffers: patch upload
-from pinned memory, the GPU pass, and the download of the status map, the mesh and the cavity
-table.  The status map (4 bytes per node) is larger than L2, so no extra flush is needed.
+Default workload: the conformer ensemble (512 structures of 500-8000 atoms, 32 globules x 16
+perturbations, each on its own grid), ray cast and triangulated as one batch in mixed precision.
+One step = ray casting of the status ray set and the three accurate-triangulation ray sets
+(hits, status runs, insideness bits, volume), vertex assembly and marching cubes of all 512
+structures.  ``value`` is structures/s with the patch sets resident in HBM; ``e2e`` is the same
+step through the C-ABI with host buffers (batch layout and patch upload from pinned memory, the
+per-structure volumes and areas back).  The same batch in double precision and the plain
+per-structure double-precision path are timed beside it (``comparison``).  The hit store and the
+bit grids are larger than L2, so no extra flush is needed.
 
-The default workload is the large SES globule: 100,000 atoms, probe 1.4 A, grid scale 4.0,
-perfil 70 (about 1050^3 nodes).  Multiple GPUs run independent replicas (the path has no
-cross-GPU exchange).
+``--workload ses_100k`` runs one large structure instead: 100,000 atoms, probe 1.4 A, grid scale
+4.0, perfil 70 (1049^3 nodes); its step adds cavity detection and filling and its e2e downloads
+the status map and the mesh.  Multiple GPUs run independent replicas (the path has no cross-GPU
+exchange).
 
 ``--impl reference`` times the CPU restatement of the reference path on a bounded slab sample of
 the same workload with all host threads, and prints the same JSON line with ``impl: reference``.
