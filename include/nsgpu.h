@@ -31,6 +31,11 @@ extern "C" {
 #define NSG_RAYCAST_STATUS 1            /* status map: Build_status_map = true */
 #define NSG_RAYCAST_TRIANGULATION 2     /* accurate-triangulation rays: Accurate_Triangulation = true */
 #define NSG_RAYCAST_KEEP_HITS 16        /* keep per-ray sorted hits for nsg_download_hits */
+#define NSG_RAYCAST_GRAD 32             /* adjoint: d volume (and d area of the next nsg_triangulate) / d patch */
+
+/* Gradient slots per patch (nsg_patch_grads): point (cx, cy, cz, r), facet (px, py, pz),
+ * edge (tcx, tcy, tcz, ux, uy, uz, R); unused slots are 0. */
+#define NSG_GRAD_PER_PATCH 8
 
 /* precision of nsg_raycast */
 #define NSG_PRECISION_FP64 0
@@ -76,7 +81,15 @@ int64_t nsg_read_xyzr(const char* path, double* out, int64_t capacity);
 int nsg_ses_build(const double* atoms_xyzr, int64_t n_atoms, double probe_radius, int n_threads, NsPatchSet** out);
 int nsg_patchset_info(const NsPatchSet* ps, int64_t* n_patches, int64_t* n_pool, int64_t counts[5]);
 int nsg_patchset_export(const NsPatchSet* ps, double* f64, int32_t* i32, double* pool, int8_t* pool_flag);
+/* The atoms every patch depends on, 3 per patch (-1 unused): point (i), facet (i, j, k), edge (i, j). */
+int nsg_patchset_atoms(const NsPatchSet* ps, int32_t* out);
 void nsg_patchset_free(NsPatchSet* ps);
+/* Chain rule of the adjoint, no counterpart in the reference (which has no derivatives):
+ * grad_atoms (n_atoms x 4: x, y, z, r) += d out / d atoms from per-patch parameter derivatives
+ * gpatch (n_patches x NSG_GRAD_PER_PATCH), for patches built from atoms_xyzr (after jitter). */
+int nsg_ses_chain_grad(const double* atoms_xyzr, int64_t n_atoms, double probe_radius, int64_t n_patches,
+                       const int32_t* i32, const double* f64, const int32_t* patch_atoms, const double* gpatch,
+                       double* grad_atoms);
 
 /* ---- device context ---- */
 int nsg_version(void);
@@ -110,6 +123,14 @@ int nsg_upload_batch(nsg_ctx* ctx, const int64_t* patch_off, const double* f64, 
                      const int64_t* pool_off, const double* pool, const int8_t* pool_flag, double probe_radius);
 /* Per-structure volume (last nsg_raycast) and area (last nsg_triangulate); either may be NULL. */
 int nsg_batch_results(nsg_ctx* ctx, double* volumes, double* areas);
+
+/* ---- adjoint (no counterpart in the reference) ----
+ * After nsg_raycast with NSG_RAYCAST_GRAD (and the nsg_triangulate that follows it): the
+ * derivatives of the volume and of the area with respect to every patch's surface parameters,
+ * NSG_GRAD_PER_PATCH doubles per patch in upload order (batch: all structures, concatenated).
+ * Each hit x on its ray axis e moves by ds = -(dF/dtheta . dtheta) / (dF/dx . e) on the patch
+ * surface F = 0; the volume sums them over interval ends, the area over analytic vertices. */
+int nsg_patch_grads(nsg_ctx* ctx, double* d_volume, double* d_area);
 
 /* ---- the hot path ---- */
 /* Ray casting of Surface::getSurf: getPatchIntersectionData (src/ConnollySurface.cpp:4319-4590),

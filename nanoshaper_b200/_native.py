@@ -30,6 +30,7 @@ ERRORS = {
 STATUS = 1
 ACCURATE_TRIANGULATION = 2
 KEEP_HITS = 16
+GRAD = 32
 
 
 class NsGrid(ctypes.Structure):
@@ -90,6 +91,9 @@ _SIGNATURES = {
     "nsg_patchset_info": ([_P, ctypes.POINTER(_I64), ctypes.POINTER(_I64), _P], _INT),
     "nsg_patchset_export": ([_P, _P, _P, _P, _P], _INT),
     "nsg_patchset_free": ([_P], None),
+    "nsg_patchset_atoms": ([_P, _P], _INT),
+    "nsg_patch_grads": ([_P, _P, _P], _INT),
+    "nsg_ses_chain_grad": ([_P, _I64, _D, _I64, _P, _P, _P, _P, _P], _INT),
 }
 
 _lib = None

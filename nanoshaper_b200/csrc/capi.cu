@@ -96,6 +96,9 @@ struct nsg_ctx {
   int64_t win_area[3] = {0, 0, 0};
   // wavefront tracing: candidate lists and the slot-major hit store
   DevBuf cand_sph, cand_tor, hit_t, hit_cnt, def_sph, def_tor;
+  // gradient mode: hit / pair / vertex patches and the per-patch derivatives of volume and area
+  DevBuf hit_pid, pair_pid, ovf_pscratch, gvol, garea, vpid, vgrad;
+  bool grad_mode = false, have_gvol = false, have_garea = false;
   int64_t cand_cap = 0, def_cap = 0;
   // trace outputs
   DevBuf status, bits, vol_ray[4];
@@ -195,6 +198,7 @@ int batch_layout(nsg_ctx* c, const NsGrid* grids, int32_t n) {
     if (G.nx * G.ny * G.nz >= (int64_t)1 << 31) return fail(NSG_ERR_ARG, "grid larger than 2^31 nodes");
     nsg::StructDev& S = sd[b];
     S.g = grid_dev(G);
+    S.A = G.A;
     S.nwords = nwords_of(G);
     S.word_base = words;
     words += S.nwords;
@@ -430,6 +434,7 @@ int nsg_ctx_destroy(nsg_ctx* c) {
   DevBuf* bufs[] = {&c->f64, &c->i32, &c->pool, &c->flag, &c->win, &c->pool32, &c->counters, &c->bin_area,
                     &c->cand_sph, &c->cand_tor, &c->def_sph, &c->def_tor, &c->hit_t, &c->hit_cnt, &c->status, &c->bits, &c->pairs,
                     &c->ray_pair_off, &c->ray_pair_cnt, &c->cursors, &c->ovf_scratch, &c->err, &c->hits,
+                    &c->hit_pid, &c->pair_pid, &c->ovf_pscratch, &c->gvol, &c->garea, &c->vpid, &c->vgrad,
                     &c->labels, &c->is_root, &c->sruns, &c->srun_off, &c->srun_cnt, &c->fr_cnt, &c->fr_off,
                     &c->fruns, &c->frow, &c->roots, &c->cc_count, &c->cc_desc, &c->cc_label_of,
                     &c->cc_fill_of, &c->nroots_d, &c->surv_cnt, &c->surv_off, &c->vpos, &c->vkey,
@@ -560,6 +565,21 @@ int nsg_upload_batch(nsg_ctx* c, const int64_t* patch_off, const double* f64, co
   return NSG_OK;
 }
 
+// Derivatives of the volume (last nsg_raycast with NSG_RAYCAST_GRAD) and of the area (the
+// nsg_triangulate that followed it) with respect to the patch surface parameters,
+// NS_GRAD_PER_PATCH doubles per patch in upload order; either pointer may be NULL.
+int nsg_patch_grads(nsg_ctx* c, double* gvol, double* garea) {
+  if (!c) return NSG_ERR_ARG;
+  if ((gvol && !c->have_gvol) || (garea && !c->have_garea))
+    return fail(NSG_ERR_STATE, "no gradient-mode ray cast / triangulation to read");
+  CK(cudaSetDevice(c->device));
+  const size_t bytes = (size_t)c->np * NS_GRAD_PER_PATCH * sizeof(double);
+  if (gvol && c->np) CK(cudaMemcpyAsync(gvol, c->gvol.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+  if (garea && c->np) CK(cudaMemcpyAsync(garea, c->garea.p, bytes, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return NSG_OK;
+}
+
 // Per-structure volume and area of the last ray cast / triangulation of the batch.
 int nsg_batch_results(nsg_ctx* c, double* volumes, double* areas) {
   if (!c || c->nstruct < 1) return NSG_ERR_ARG;
@@ -594,6 +614,9 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
   const bool do_status = flags & 1;
   const bool do_mc = flags & 2;
   const bool keep_hits = flags & 16;
+  const bool grad = flags & 32;
+  c->grad_mode = grad;
+  c->have_gvol = c->have_garea = false;
   c->flags = flags;
   c->precision = precision;
   if (precision == NSG_PRECISION_MIXED && !c->pool32_valid) {
@@ -635,11 +658,18 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
     int64_t nr_max = std::max(std::max(c->rays_tot[0], c->rays_tot[1]), std::max(c->rays_tot[2], c->rays_tot[3]));
     CK(c->hit_t.ensure((size_t)nr_max * nsg::kHitCap * sizeof(double)));
     CK(c->hit_cnt.ensure(nr_max * sizeof(int32_t)));
+    if (grad) {
+      CK(c->hit_pid.ensure((size_t)nr_max * nsg::kHitCap * sizeof(int32_t)));
+      CK(c->gvol.ensure(std::max<int64_t>(c->np, 1) * NS_GRAD_PER_PATCH * sizeof(double)));
+    }
   }
   CK(c->err.ensure(sizeof(int32_t)));
   const int ovf_cap = 1 << 16;
   for (int attempt = 0; attempt < 4; attempt++) {
     if (do_mc) CK(c->pairs.ensure(c->pair_cap * 2 * sizeof(double)));
+    if (do_mc && grad) CK(c->pair_pid.ensure(c->pair_cap * sizeof(int2)));
+    if (grad)
+      CK(cudaMemsetAsync(c->gvol.p, 0, std::max<int64_t>(c->np, 1) * NS_GRAD_PER_PATCH * sizeof(double), c->stream));
     CK(c->cand_sph.ensure(c->cand_cap * sizeof(int2)));
     CK(c->cand_tor.ensure(c->cand_cap * sizeof(int2)));
     if (precision == NSG_PRECISION_MIXED) {
@@ -693,6 +723,11 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
       o.ovf_count = ovf_count + s;
       o.error_flag = c->err.as<int32_t>();
       o.counters = c->profile ? c->counters.as<unsigned long long>() : nullptr;
+      if (grad) {
+        o.gvol = c->gvol.as<double>();
+        o.pair_pid = c->pair_pid.as<int2>();
+        o.grad_scale = 1.0 / (double)((do_status ? 1 : 0) + (do_mc ? 3 : 0));
+      }
       if (keep_hits) {
         CK(c->ray_hit_off[s].ensure(nr * sizeof(int64_t)));
         CK(c->ray_hit_cnt[s].ensure(nr * sizeof(int32_t)));
@@ -706,7 +741,7 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
       outs[s] = o;
       nsg::CandOut co{c->cand_sph.as<int2>(), c->cand_tor.as<int2>(), c->cand_cap, cur + 8 + 2 * s,
                       c->def_sph.as<int2>(), c->def_tor.as<int2>(), c->def_cap, cur + 16 + 2 * s};
-      nsg::HitStore hs{c->hit_t.as<double>(), c->hit_cnt.as<int32_t>(), nr};
+      nsg::HitStore hs{c->hit_t.as<double>(), c->hit_cnt.as<int32_t>(), nr, grad ? c->hit_pid.as<int32_t>() : nullptr};
       CK(cudaMemsetAsync(c->hit_cnt.p, 0, nr * sizeof(int32_t), c->stream));
       c->launches += precision == NSG_PRECISION_MIXED ? 6 : 4;
       CK(nsg::launch_trace(P, B, s, c->tiles_tot[panel], c->tile_off[panel].as<int64_t>(),
@@ -725,8 +760,10 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
       if (n == 0) continue;
       const int panel = s == 0 ? 0 : s - 1;
       CK(c->ovf_scratch.ensure((size_t)n * nsg::kOverflowCap * sizeof(double)));
+      if (grad) CK(c->ovf_pscratch.ensure((size_t)n * nsg::kOverflowCap * sizeof(int32_t)));
       LAUNCH(nsg::launch_trace_overflow(P, B, s, c->tile_off[panel].as<int64_t>(), c->tile_list[panel].as<int32_t>(),
-                                        outs[s], n, c->ovf_scratch.as<double>(), precision, c->stream));
+                                        outs[s], n, c->ovf_scratch.as<double>(),
+                                        grad ? c->ovf_pscratch.as<int32_t>() : nullptr, precision, c->stream));
       CK(cudaStreamSynchronize(c->stream));
     }
     stage_end(c, kStageOverflow);
@@ -788,6 +825,7 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
     if (rc) return rc;
   }
   c->status_dense = false;
+  c->have_gvol = grad;
   c->have_status = do_status;
   c->have_bits = do_mc;
   c->n_vert = c->n_tri = 0;
@@ -941,6 +979,12 @@ int nsg_triangulate(nsg_ctx* c, double* area_out, int64_t* nverts, int64_t* ntri
   CK(c->vpos.ensure(std::max<int64_t>(n_an, 1) * 3 * sizeof(double)));
   V.vpos = c->vpos.as<double>();
   V.vkey = c->vkey.as<int4>();
+  const bool grad = c->grad_mode && c->have_gvol;
+  if (grad) {
+    CK(c->vpid.ensure(std::max<int64_t>(n_an, 1) * sizeof(int32_t)));
+    V.pair_pid = c->pair_pid.as<int2>();
+    V.vpid = c->vpid.as<int32_t>();
+  }
   LAUNCH(nsg::launch_vert(V, 1, c->stream));
   stage_end(c, kStageVertex);
   stage_begin(c, kStageMC);
@@ -997,7 +1041,22 @@ int nsg_triangulate(nsg_ctx* c, double* area_out, int64_t* nverts, int64_t* ntri
   M.tri_off = c->tri_off.as<int64_t>();
   M.tris = c->tris.as<int32_t>();
   M.cube_area = c->cube_area.as<double>();
+  if (grad) {
+    const nsg::PatchDev P = patch_dev(c);
+    CK(c->vgrad.ensure(std::max<int64_t>(n_an, 1) * sizeof(double)));
+    CK(c->garea.ensure(std::max<int64_t>(c->np, 1) * NS_GRAD_PER_PATCH * sizeof(double)));
+    CK(cudaMemsetAsync(c->vgrad.p, 0, std::max<int64_t>(n_an, 1) * sizeof(double), c->stream));
+    CK(cudaMemsetAsync(c->garea.p, 0, std::max<int64_t>(c->np, 1) * NS_GRAD_PER_PATCH * sizeof(double), c->stream));
+    M.vpid = c->vpid.as<int32_t>();
+    M.vgrad = c->vgrad.as<double>();
+    M.garea = c->garea.as<double>();
+    M.f64 = P.f64;
+    M.i32 = P.i32;
+    M.probe = P.probe;
+  }
   LAUNCH(nsg::launch_mc_tris(M, 1, c->stream));
+  if (grad) LAUNCH(nsg::launch_grad_vert(M, c->stream));
+  c->have_garea = grad;
   double area = 0;
   if (c->nstruct == 1) {
     rc = reduce_sum(c, c->cube_area.as<double>(), n_act, &area);

@@ -35,7 +35,12 @@ int nsg_ses_build(const double* atoms_xyzr, int64_t n_atoms, double probe_radius
                   NsPatchSet** out);
 int nsg_patchset_info(const NsPatchSet* ps, int64_t* n_patches, int64_t* n_pool, int64_t counts[5]);
 int nsg_patchset_export(const NsPatchSet* ps, double* f64, int32_t* i32, double* pool, int8_t* pool_flag);
+int nsg_patchset_atoms(const NsPatchSet* ps, int32_t* out);
 void nsg_patchset_free(NsPatchSet* ps);
+
+int nsg_ses_chain_grad(const double* atoms_xyzr, int64_t n_atoms, double probe, int64_t n_patches,
+                       const int32_t* i32, const double* f64, const int32_t* patch_atoms, const double* gpatch,
+                       double* grad_atoms);
 
 #ifdef __cplusplus
 }

@@ -192,8 +192,13 @@ struct NsPatchSet {
   std::vector<int32_t> i32;
   std::vector<double> pool;
   std::vector<int8_t> pool_flag;
+  std::vector<int32_t> atoms;  // 3 per patch: the atoms the patch's surface depends on, -1 unused
   int64_t counts[5] = {0, 0, 0, 0, 0};
-  void add_patch(int kind, const double* rec, const double* pool4, const int8_t* flags, int64_t npool) {
+  void add_patch(int kind, const double* rec, const double* pool4, const int8_t* flags, int64_t npool, int32_t a0,
+                 int32_t a1, int32_t a2) {
+    atoms.push_back(a0);
+    atoms.push_back(a1);
+    atoms.push_back(a2);
     int64_t first = (int64_t)pool_flag.size();
     f64.insert(f64.end(), rec, rec + NS_PATCH_F64);
     i32.push_back(kind);
@@ -713,7 +718,7 @@ struct SesBuilder {
       rec[8] = -1.0;
       std::vector<double> all = clip[i];
       all.insert(all.end(), bclip[i].begin(), bclip[i].end());
-      ps->add_patch(NS_POINT, rec, all.data(), nullptr, (int64_t)all.size() / 4);
+      ps->add_patch(NS_POINT, rec, all.data(), nullptr, (int64_t)all.size() / 4, (int32_t)i, -1, -1);
     }
     for (auto& f : facets) {
       memset(rec, 0, sizeof rec);
@@ -722,14 +727,15 @@ struct SesBuilder {
       std::vector<double> pl;
       for (int q = f.singular ? 0 : 1; q < 4; q++) pl.insert(pl.end(), f.planes[q], f.planes[q] + 4);
       pl.insert(pl.end(), f.si_planes.begin(), f.si_planes.end());
-      ps->add_patch(f.singular ? NS_FACE_SING : NS_FACE_REG, rec, pl.data(), nullptr, (int64_t)pl.size() / 4);
+      ps->add_patch(f.singular ? NS_FACE_SING : NS_FACE_REG, rec, pl.data(), nullptr, (int64_t)pl.size() / 4, f.id[0],
+                    f.id[1], f.id[2]);
     }
     for (auto& e : edges) {
       memset(rec, 0, sizeof rec);
       rec[0] = e.clip_c[0]; rec[1] = e.clip_c[1]; rec[2] = e.clip_c[2]; rec[3] = e.clip_r;
       rec[4] = e.tc[0]; rec[5] = e.tc[1]; rec[6] = e.tc[2]; rec[7] = e.bigR; rec[8] = e.sir;
       for (int q = 0; q < 9; q++) rec[9 + q] = e.invrot[q];
-      ps->add_patch(e.kind, rec, e.planes.data(), e.flags.data(), (int64_t)e.planes.size() / 4);
+      ps->add_patch(e.kind, rec, e.planes.data(), e.flags.data(), (int64_t)e.planes.size() / 4, e.i, e.j, -1);
     }
   }
 };
@@ -773,6 +779,12 @@ int nsg_patchset_export(const NsPatchSet* ps, double* f64, int32_t* i32, double*
   if (i32) memcpy(i32, ps->i32.data(), ps->i32.size() * sizeof(int32_t));
   if (pool) memcpy(pool, ps->pool.data(), ps->pool.size() * sizeof(double));
   if (pool_flag) memcpy(pool_flag, ps->pool_flag.data(), ps->pool_flag.size());
+  return NSG_OK;
+}
+
+int nsg_patchset_atoms(const NsPatchSet* ps, int32_t* out) {
+  if (!ps || !out) return NSG_ERR_ARG;
+  memcpy(out, ps->atoms.data(), ps->atoms.size() * sizeof(int32_t));
   return NSG_OK;
 }
 

@@ -17,6 +17,7 @@
 #include <cub/cub.cuh>
 
 #include "../mc_cases.h"
+#include "grad.cuh"
 #include "mc.h"
 
 namespace nsg {
@@ -105,6 +106,10 @@ __global__ void k_vert(VertArgs A, int emit) {
       A.vpos[3 * o + 1] = p[1];
       A.vpos[3 * o + 2] = p[2];
       A.vkey[o] = e;
+      if (A.vpid) {
+        const int2 pp = A.pair_pid[A.ray_pair_off[r] + (q >> 1)];
+        A.vpid[o] = (q & 1) ? pp.y : pp.x;
+      }
       o++;
     }
   }
@@ -343,7 +348,31 @@ __global__ void k_mc_tris(MCArgs A, int emit) {
         const double* P2 = A.vpos + 3 * (int64_t)v2;
         double da = vdist(P0, P1), db = vdist(P0, P2), dc = vdist(P1, P2);
         double ttt = (da + db + dc) * (db + dc - da) * (dc + da - db) * (da + db - dc);
-        if (ttt > 0) area += 0.25 * sqrt(ttt);
+        if (ttt > 0) {
+          area += 0.25 * sqrt(ttt);
+          if (A.vgrad) {
+            // area = |n| / 2, n = (P1 - P0) x (P2 - P0): d area / d P0 = (P1 - P2) x n / (2 |n|), cyclic
+            const double e1[3] = {P1[0] - P0[0], P1[1] - P0[1], P1[2] - P0[2]};
+            const double e2[3] = {P2[0] - P0[0], P2[1] - P0[1], P2[2] - P0[2]};
+            double nn[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+            const double nl = sqrt(nn[0] * nn[0] + nn[1] * nn[1] + nn[2] * nn[2]);
+            if (nl > 0) {
+              for (int d = 0; d < 3; d++) nn[d] /= 2.0 * nl;
+              const int32_t vv[3] = {v0, v1, v2};
+              const double* PP[3] = {P0, P1, P2};
+              for (int t3 = 0; t3 < 3; t3++) {
+                if (vv[t3] >= A.n_analytic) continue;
+                const double* Pa = PP[(t3 + 1) % 3];
+                const double* Pb = PP[(t3 + 2) % 3];
+                const double dd[3] = {Pa[0] - Pb[0], Pa[1] - Pb[1], Pa[2] - Pb[2]};
+                const int ax = A.vkey[vv[t3]].w;  // ray axis of an analytic vertex = its edge direction
+                const int a1 = (ax + 1) % 3, a2 = (ax + 2) % 3;
+                const double comp = dd[a1] * nn[a2] - dd[a2] * nn[a1];
+                if (comp != 0.0) atomicAdd(A.vgrad + vv[t3], comp);
+              }
+            }
+          }
+        }
         A.tris[3 * (o + cnt) + 0] = (int32_t)v2;
         A.tris[3 * (o + cnt) + 1] = (int32_t)v1;
         A.tris[3 * (o + cnt) + 2] = (int32_t)v0;
@@ -352,6 +381,16 @@ __global__ void k_mc_tris(MCArgs A, int emit) {
     }
     if (!emit) A.tri_cnt[a] = cnt;
     else A.cube_area[a] = area;
+  }
+}
+
+// One thread per analytic vertex: d area / d patch parameters += (d area / d s) * ds / d theta.
+__global__ void k_grad_vert(MCArgs A) {
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < A.n_analytic; v += (int64_t)gridDim.x * blockDim.x) {
+    const double gv = A.vgrad[v];
+    if (gv == 0.0) continue;
+    const double x[3] = {A.vpos[3 * v], A.vpos[3 * v + 1], A.vpos[3 * v + 2]};
+    add_hit_grad(A.f64, A.i32, A.probe, A.vpid[v], x, A.vkey[v].w, gv, A.garea);
   }
 }
 
@@ -402,6 +441,12 @@ cudaError_t launch_mc_mid(const MCArgs& A, int emit, cudaStream_t s) {
 cudaError_t launch_mc_tris(const MCArgs& A, int emit, cudaStream_t s) {
   if (A.n_active <= 0) return cudaSuccess;
   k_mc_tris<<<grid_for(A.n_active, 128), 128, 0, s>>>(A, emit);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_grad_vert(const MCArgs& A, cudaStream_t s) {
+  if (A.n_analytic <= 0 || !A.vgrad) return cudaSuccess;
+  k_grad_vert<<<grid_for(A.n_analytic, 256), 256, 0, s>>>(A);
   return cudaGetLastError();
 }
 

@@ -20,6 +20,8 @@ struct VertArgs {
   const int64_t* surv_off;       // exclusive scan of surv_cnt
   double* vpos;                  // 3 per vertex
   int4* vkey;                    // ix, iy, iz, dir per vertex
+  const int2* pair_pid;          // gradient mode: patches of the pair ends, else null
+  int32_t* vpid;                 // gradient mode: patch of every analytic vertex
 };
 
 struct MCArgs {
@@ -44,6 +46,14 @@ struct MCArgs {
   const int64_t* tri_off;
   int32_t* tris;
   double* cube_area;
+  // gradient mode (vgrad null otherwise): d area / d (analytic vertex position along its ray),
+  // then d area / d patch parameters
+  const int32_t* vpid;
+  double* vgrad;
+  double* garea;
+  const double* f64;
+  const int32_t* i32;
+  double probe;
 };
 
 cudaError_t mc_init_tables();
@@ -51,5 +61,7 @@ cudaError_t launch_vert(const VertArgs& A, int emit, cudaStream_t s);
 cudaError_t launch_mc_rows(const MCArgs& A, int emit, cudaStream_t s);
 cudaError_t launch_mc_mid(const MCArgs& A, int emit, cudaStream_t s);
 cudaError_t launch_mc_tris(const MCArgs& A, int emit, cudaStream_t s);
+// d area / d patch parameters from the per-vertex derivatives (gradient mode).
+cudaError_t launch_grad_vert(const MCArgs& A, cudaStream_t s);
 
 }  // namespace nsg

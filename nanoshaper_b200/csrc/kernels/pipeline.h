@@ -48,6 +48,7 @@ struct StructDev {
   int64_t ray_base[4];   // first ray of each ray set in the set's ray arrays
   int64_t mc_base;       // first accurate-triangulation ray ordinal (its 3 panels are contiguous)
   int64_t row_base;      // first marching-cubes row ((NY-2)*(NZ-2) rows per structure)
+  double A;              // side^2: the area of one pixel, volume weight of an interval length
   double ray_dir[3];     // ray length along each axis: coordinate of the last node minus the first
   double inv_dir[3];     // 1 / ray_dir
 };
@@ -121,6 +122,11 @@ struct TraceOut {
   int64_t* ray_hit_off;    // indexed by n*nb+m
   int32_t* ray_hit_cnt;
   int32_t* error_flag;     // set when a device-side capacity is exceeded
+  // gradient mode (null otherwise): d volume / d patch parameters (NS_GRAD_PER_PATCH per patch),
+  // the patches of the stored pair ends, and 1 / (number of ray sets cast) of the volume formula
+  double* gvol;
+  int2* pair_pid;
+  double grad_scale;
   // optional event counters (profiling): candidates, torus candidates, mixed-precision fallbacks
   // (near-tangent sphere, quartic isolation, root polish / root boundary), FP64 re-evaluations of
   // feasibility tests
@@ -149,6 +155,7 @@ struct HitStore {
   double* t;
   int32_t* cnt;
   int64_t nrays;
+  int32_t* pid;  // patch of every hit, same layout as t (gradient mode only, else null)
 };
 
 struct PatchDev {
@@ -174,9 +181,10 @@ cudaError_t launch_bin_fill(const PatchDev& P, const BatchDev& B, int set, const
 cudaError_t launch_trace(const PatchDev& P, const BatchDev& B, int set, int64_t ntiles, const int64_t* tile_off,
                          const int32_t* tile_list, const TraceOut& out, const CandOut& co, const HitStore& hs,
                          int precision, cudaStream_t s);
+// pscratch: patch column of the overflow hits (gradient mode), else null.
 cudaError_t launch_trace_overflow(const PatchDev& P, const BatchDev& B, int set, const int64_t* tile_off,
                                   const int32_t* tile_list, const TraceOut& out, int n_ovf, double* scratch,
-                                  int precision, cudaStream_t s);
+                                  int32_t* pscratch, int precision, cudaStream_t s);
 
 // reduce.cu: out[b] (+)= sum of v over structure b's segment [base[i(b)], base[i(b+1)]) with
 // i(b) = idx[b] (idx given) or b; one CTA per structure, fixed summation order.

@@ -16,6 +16,7 @@
 #include "pipeline.h"
 #include "ray_math.cuh"
 #include "ray_math_mixed.cuh"
+#include "grad.cuh"
 
 namespace nsg {
 
@@ -284,24 +285,24 @@ __device__ __forceinline__ int intersect_mixed(const double* f, int kind, int fi
   return out;
 }
 
-// Sorted insertion into a strided hit column; returns false when the column is full.
-__device__ __forceinline__ bool insert_hit(double* col, int stride, int& nh, int cap, double t) {
-  if (nh >= cap) return false;
-  int pos = nh;
-  while (pos > 0 && col[(pos - 1) * stride] > t) {
-    col[pos * stride] = col[(pos - 1) * stride];
-    pos--;
-  }
-  col[pos * stride] = t;
-  nh++;
-  return true;
-}
-
 // Pairs the sorted hits of one ray in place (NEW_INTERSECTION_FILTERING) and turns them into
 // interval ends along the ray axis; returns the number of pairs and the interval length sum.
 // When vertex_pairs is set, only pairs that clear at least one insideness node are kept.
+// With pcol (the hits' patches, gradient mode) the patch column is compacted alongside, and every
+// interval end adds its term of d volume / d patch parameters (GradCtx).
+struct GradCtx {
+  const double* f64;
+  const int32_t* i32;
+  double probe;
+  double w;          // volume weight of an interval length: A / number of ray sets
+  double x[3];       // ray origin; x[vc] is replaced by the interval end
+  int vc;
+  double* gvol;
+};
+
 __device__ __forceinline__ int make_pairs(double* col, int stride, int nh, double pa_vc, double dir, double vmin,
-                                          double scale, bool vertex_pairs, double* vol) {
+                                          double scale, bool vertex_pairs, double* vol, int32_t* pcol = nullptr,
+                                          GradCtx* gc = nullptr) {
   double v = 0.0;
   int np = 0;
   if (nh > 0 && (nh & 1) == 0) {
@@ -311,6 +312,16 @@ __device__ __forceinline__ int make_pairs(double* col, int stride, int nh, doubl
         double lim1 = pa_vc + dir * t1;
         double lim2 = pa_vc + dir * t2;
         v += lim2 - lim1;
+        int32_t p1 = 0, p2 = 0;
+        if (pcol) {
+          p1 = pcol[q * stride];
+          p2 = pcol[(q + 1) * stride];
+          double x[3] = {gc->x[0], gc->x[1], gc->x[2]};
+          x[gc->vc] = lim1;
+          add_hit_grad(gc->f64, gc->i32, gc->probe, p1, x, gc->vc, -gc->w, gc->gvol);
+          x[gc->vc] = lim2;
+          add_hit_grad(gc->f64, gc->i32, gc->probe, p2, x, gc->vc, gc->w, gc->gvol);
+        }
         if (vertex_pairs) {
           int64_t a = (int64_t)rintp((lim1 - vmin) * scale);
           int64_t b = (int64_t)rintp((lim2 - vmin) * scale);
@@ -318,6 +329,10 @@ __device__ __forceinline__ int make_pairs(double* col, int stride, int nh, doubl
         }
         col[(2 * np) * stride] = lim1;
         col[(2 * np + 1) * stride] = lim2;
+        if (pcol) {
+          pcol[(2 * np) * stride] = p1;
+          pcol[(2 * np + 1) * stride] = p2;
+        }
         np++;
       }
     }
@@ -530,7 +545,10 @@ __global__ void __launch_bounds__(256) k_isect(TraceCtx C, CandOut co, HitStore 
     if (k <= 0) continue;
     int pos = atomicAdd(hs.cnt + rid, k);
     for (int i = 0; i < k; i++)
-      if (pos + i < kHitCap) hs.t[(int64_t)(pos + i) * hs.nrays + rid] = t[i];
+      if (pos + i < kHitCap) {
+        hs.t[(int64_t)(pos + i) * hs.nrays + rid] = t[i];
+        if (hs.pid) hs.pid[(int64_t)(pos + i) * hs.nrays + rid] = (int32_t)pid;
+      }
   }
 }
 
@@ -552,6 +570,9 @@ void launch_isect(const TraceCtx& C, const CandOut& co, const HitStore& hs, int 
 
 // One CTA per 32x4 ray tile: loads, sorts and pairs the hits of its rays and performs the
 // interval fill (status runs, insideness bits, pair store, volume).
+// kGrad: the hits carry their patches (sorted along), and every interval end adds its term of
+// d volume / d patch parameters; the stored pairs keep their patches for the area adjoint.
+template <bool kGrad>
 __global__ void __launch_bounds__(kTraceThreads) k_fill(TraceCtx C, HitStore hs) {
   constexpr int kThreads = kTraceThreads;
   const int panel = C.set == 0 ? 0 : C.set - 1;
@@ -562,6 +583,7 @@ __global__ void __launch_bounds__(kTraceThreads) k_fill(TraceCtx C, HitStore hs)
   uint32_t* const bits = C.out.bits + S.word_base;
   const int64_t nwords = S.nwords;
   __shared__ double s_hit[kHitCap * kThreads];
+  __shared__ int32_t s_pid[kGrad ? kHitCap * kThreads : 1];
   const int64_t ntm = (rs.nb + kTileM - 1) / kTileM;
   const int64_t lt = tile - S.tile_base[panel];
   const int64_t tm = lt % ntm, tn = lt / ntm;
@@ -576,15 +598,21 @@ __global__ void __launch_bounds__(kTraceThreads) k_fill(TraceCtx C, HitStore hs)
   int hc = valid ? hs.cnt[rid] : 0;
   bool ovf = hc > kHitCap;
   int nh = ovf ? 0 : hc;
+  int32_t* pcol = kGrad ? s_pid + tid : nullptr;
   for (int i = 0; i < nh; i++) col[i * kThreads] = hs.t[(int64_t)i * hs.nrays + rid];
+  if (kGrad)
+    for (int i = 0; i < nh; i++) pcol[i * kThreads] = hs.pid[(int64_t)i * hs.nrays + rid];
   for (int i = 1; i < nh; i++) {
     double v = col[i * kThreads];
+    int32_t pv = kGrad ? pcol[i * kThreads] : 0;
     int j = i;
     while (j > 0 && col[(j - 1) * kThreads] > v) {
       col[j * kThreads] = col[(j - 1) * kThreads];
+      if (kGrad) pcol[j * kThreads] = pcol[(j - 1) * kThreads];
       j--;
     }
     col[j * kThreads] = v;
+    if (kGrad) pcol[j * kThreads] = pv;
   }
   if (valid && ovf) {
     int slot = atomicAdd(C.out.ovf_count, 1);
@@ -614,7 +642,21 @@ __global__ void __launch_bounds__(kTraceThreads) k_fill(TraceCtx C, HitStore hs)
   }
   double vol = 0.0;
   int np = 0;
-  if (valid && !ovf) np = make_pairs(col, kThreads, nh, pa_vc, dirl, g.mn[rs.vc], g.scale, mc, &vol);
+  if (kGrad) {
+    GradCtx gc;
+    gc.f64 = C.P.f64;
+    gc.i32 = C.P.i32;
+    gc.probe = C.P.probe;
+    gc.w = S.A * C.out.grad_scale;
+    gc.x[rs.fd] = gcoord(g, rs.fd, valid ? m : 0) + rs.delta;
+    gc.x[rs.ld] = gcoord(g, rs.ld, valid ? n : 0) + rs.delta;
+    gc.x[rs.vc] = 0.0;
+    gc.vc = rs.vc;
+    gc.gvol = C.out.gvol;
+    if (valid && !ovf) np = make_pairs(col, kThreads, nh, pa_vc, dirl, g.mn[rs.vc], g.scale, mc, &vol, pcol, &gc);
+  } else {
+    if (valid && !ovf) np = make_pairs(col, kThreads, nh, pa_vc, dirl, g.mn[rs.vc], g.scale, mc, &vol);
+  }
   if (valid && !ovf) C.out.vol_ray[rid] = vol;
   __syncwarp();
   const int64_t NX = g.n[0], NY = g.n[1];
@@ -652,6 +694,7 @@ __global__ void __launch_bounds__(kTraceThreads) k_fill(TraceCtx C, HitStore hs)
         for (int q = 0; q < np; q++) {
           C.out.pairs[2 * (off + q)] = col[(2 * q) * kThreads];
           C.out.pairs[2 * (off + q) + 1] = col[(2 * q + 1) * kThreads];
+          if (kGrad) C.out.pair_pid[off + q] = make_int2(pcol[(2 * q) * kThreads], pcol[(2 * q + 1) * kThreads]);
         }
         C.out.ray_pair_off[ord] = off;
         C.out.ray_pair_cnt[ord] = np;
@@ -733,7 +776,7 @@ __global__ void __launch_bounds__(kTraceThreads) k_fill(TraceCtx C, HitStore hs)
 
 // One thread per overflow ray: the same candidate tests with the hits kept in a global column.
 __global__ void k_trace_overflow(TraceCtx C, const int64_t* __restrict__ tile_off, const int32_t* __restrict__ tile_list,
-                                 int n_ovf, double* scratch) {
+                                 int n_ovf, double* scratch, int32_t* pscratch) {
   int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= n_ovf) return;
   int64_t rid = C.out.ovf_rays[idx];
@@ -747,6 +790,7 @@ __global__ void k_trace_overflow(TraceCtx C, const int64_t* __restrict__ tile_of
   int64_t ntm = (rs.nb + kTileM - 1) / kTileM;
   int64_t tile = S.tile_base[rs.panel] + (n / kTileN) * ntm + m / kTileM;
   double* col = scratch + (int64_t)idx * kOverflowCap;
+  int32_t* pcol = pscratch ? pscratch + (int64_t)idx * kOverflowCap : nullptr;
   double pa[3], dir[3] = {0., 0., 0.};
   pa[rs.fd] = gcoord(g, rs.fd, m) + rs.delta;
   pa[rs.ld] = gcoord(g, rs.ld, n) + rs.delta;
@@ -763,11 +807,20 @@ __global__ void k_trace_overflow(TraceCtx C, const int64_t* __restrict__ tile_of
     const int32_t* ir = C.P.i32 + NS_PATCH_I32 * pid;
     double t[4];
     int k = ray_patch_f64(f, ir[0], ir[1], ir[2], C.P, rs, pa, dir, ray_dir, t);
-    for (int i = 0; i < k; i++)
-      if (!insert_hit(col, 1, nh, kOverflowCap, t[i])) {
+    for (int i = 0; i < k; i++) {
+      if (nh >= kOverflowCap) {
         atomicExch(C.out.error_flag, 4);
         return;
       }
+      int pos = nh++;
+      while (pos > 0 && col[pos - 1] > t[i]) {
+        col[pos] = col[pos - 1];
+        if (pcol) pcol[pos] = pcol[pos - 1];
+        pos--;
+      }
+      col[pos] = t[i];
+      if (pcol) pcol[pos] = (int32_t)pid;
+    }
   }
   if (C.out.hits) {
     unsigned long long off = atomicAdd(C.out.hit_cursor, (unsigned long long)nh);
@@ -789,7 +842,17 @@ __global__ void k_trace_overflow(TraceCtx C, const int64_t* __restrict__ tile_of
     dirl = (gcoord(g, rs.vc, g.n[rs.vc] - 1) + rs.delta) - pa_vc;
   }
   double vol = 0.0;
-  int np = make_pairs(col, 1, nh, pa_vc, dirl, g.mn[rs.vc], g.scale, mc, &vol);
+  GradCtx gc;
+  gc.f64 = C.P.f64;
+  gc.i32 = C.P.i32;
+  gc.probe = C.P.probe;
+  gc.w = S.A * C.out.grad_scale;
+  gc.x[rs.fd] = pa[rs.fd];
+  gc.x[rs.ld] = pa[rs.ld];
+  gc.x[rs.vc] = 0.0;
+  gc.vc = rs.vc;
+  gc.gvol = C.out.gvol;
+  int np = make_pairs(col, 1, nh, pa_vc, dirl, g.mn[rs.vc], g.scale, mc, &vol, pcol, pcol ? &gc : nullptr);
   C.out.vol_ray[rid] = vol;
   const int64_t NX = g.n[0], NY = g.n[1];
   if (!mc) {
@@ -819,6 +882,7 @@ __global__ void k_trace_overflow(TraceCtx C, const int64_t* __restrict__ tile_of
     for (int q = 0; q < np; q++) {
       C.out.pairs[2 * (off + q)] = col[2 * q];
       C.out.pairs[2 * (off + q) + 1] = col[2 * q + 1];
+      if (pcol) C.out.pair_pid[off + q] = make_int2(pcol[2 * q], pcol[2 * q + 1]);
     }
     C.out.ray_pair_off[ord] = (int64_t)off;
     C.out.ray_pair_cnt[ord] = np;
@@ -880,17 +944,18 @@ cudaError_t launch_trace(const PatchDev& P, const BatchDev& B, int set, int64_t 
   if (panel == 0) launch_isect<0>(C, co, hs, precision, s);
   else if (panel == 1) launch_isect<1>(C, co, hs, precision, s);
   else launch_isect<2>(C, co, hs, precision, s);
-  k_fill<<<(unsigned)ntiles, kTraceThreads, 0, s>>>(C, hs);
+  if (out.gvol) k_fill<true><<<(unsigned)ntiles, kTraceThreads, 0, s>>>(C, hs);
+  else k_fill<false><<<(unsigned)ntiles, kTraceThreads, 0, s>>>(C, hs);
   return cudaGetLastError();
 }
 
 cudaError_t launch_trace_overflow(const PatchDev& P, const BatchDev& B, int set, const int64_t* tile_off,
                                   const int32_t* tile_list, const TraceOut& out, int n_ovf, double* scratch,
-                                  int precision, cudaStream_t s) {
+                                  int32_t* pscratch, int precision, cudaStream_t s) {
   (void)precision;
   if (n_ovf <= 0) return cudaSuccess;
   TraceCtx C{P, B, set, out};
-  k_trace_overflow<<<(n_ovf + 63) / 64, 64, 0, s>>>(C, tile_off, tile_list, n_ovf, scratch);
+  k_trace_overflow<<<(n_ovf + 63) / 64, 64, 0, s>>>(C, tile_off, tile_list, n_ovf, scratch, pscratch);
   return cudaGetLastError();
 }
 

@@ -36,6 +36,9 @@ enum NsPatchKind {
 #define NS_PATCH_F64 20
 // Per-patch int record (NS_PATCH_I32 ints per patch): kind, first pool entry, pool entry count, unused.
 #define NS_PATCH_I32 4
+// Per-patch surface-parameter gradient slots: point (cx, cy, cz, r), facet (px, py, pz),
+// edge (tcx, tcy, tcz, ux, uy, uz, R).
+#define NS_GRAD_PER_PATCH 8
 
 // Pool entries are 4 doubles.
 //   POINT: clipping sphere (cx, cy, cz, r^2); a point strictly inside any of them is infeasible.

@@ -121,7 +121,7 @@ class DelPhiShared:
     """Grid environment: the atoms, the cubic grid and the maps produced on it."""
 
     def __init__(self, atoms: np.ndarray, scale: float = DEFAULT_SCALE, perfil: float = DEFAULT_PERFIL,
-                 build_status: bool = True, build_eps_map: bool = False):
+                 build_status: bool = True, build_eps_map: bool = False, grid: "N.NsGrid | None" = None):
         self.atoms = np.ascontiguousarray(np.asarray(atoms, np.float64).reshape(-1, 4)).copy()
         if len(self.atoms) == 0:
             raise ValueError("Cannot build grid with no atoms!")
@@ -130,7 +130,12 @@ class DelPhiShared:
         if build_eps_map:
             raise NotImplementedError("epsilon maps are not built by this implementation")
         self.grid = N.NsGrid()
-        self.buildGrid(scale, perfil)
+        if grid is None:
+            self.buildGrid(scale, perfil)
+        else:
+            # a given grid (e.g. kept fixed while the atoms move by finite differences)
+            ctypes.pointer(self.grid)[0] = grid
+            self._grid_fields()
         self.status: np.ndarray | None = None
         self.cavitiesSize: list[float] = []
         self.cavitiesFlag: list[bool] = []
@@ -138,6 +143,10 @@ class DelPhiShared:
     def buildGrid(self, scale: float, perfil: float) -> bool:
         N.check(N.lib().nsg_grid_build(N.ptr(self.atoms), len(self.atoms), scale, perfil, ctypes.byref(self.grid)),
                 "buildGrid")
+        self._grid_fields()
+        return True
+
+    def _grid_fields(self) -> None:
         g = self.grid
         self.nx, self.ny, self.nz = g.nx, g.ny, g.nz
         self.scale, self.side, self.hside, self.A = g.scale, g.side, g.hside, g.A
@@ -147,7 +156,6 @@ class DelPhiShared:
         self.x = g.xmin + np.arange(g.nx) * g.side
         self.y = g.ymin + np.arange(g.ny) * g.side
         self.z = g.zmin + np.arange(g.nz) * g.side
-        return True
 
 
 class PatchSet:
@@ -156,13 +164,18 @@ class PatchSet:
     KINDS = ("point", "regular_edge", "singular_edge", "regular_facet", "singular_facet")
 
     def __init__(self, f64: np.ndarray, i32: np.ndarray, pool: np.ndarray, pool_flag: np.ndarray, probe: float,
-                 counts: tuple[int, ...] = ()):
+                 counts: tuple[int, ...] = (), atoms_of: np.ndarray | None = None,
+                 built_from: np.ndarray | None = None):
         self.f64 = np.ascontiguousarray(f64, np.float64).reshape(-1, 20)
         self.i32 = np.ascontiguousarray(i32, np.int32).reshape(-1, 4)
         self.pool = np.ascontiguousarray(pool, np.float64).reshape(-1, 4)
         self.pool_flag = np.ascontiguousarray(pool_flag, np.int8).reshape(-1)
         self.probe = float(probe)
         self.counts = tuple(counts) or tuple(int((self.i32[:, 0] == k).sum()) for k in range(5))
+        # atoms each patch depends on (3 per patch, -1 unused) and the atoms the set was built
+        # from (after jitter): the chain rule from patch parameters to atoms needs both
+        self.atoms_of = None if atoms_of is None else np.ascontiguousarray(atoms_of, np.int32).reshape(-1, 3)
+        self.built_from = built_from
 
     @property
     def n(self) -> int:
@@ -180,7 +193,25 @@ class PatchSet:
         pool = np.zeros((npool.value, 4))
         flag = np.zeros(npool.value, np.int8)
         N.check(L.nsg_patchset_export(handle, N.ptr(f64), N.ptr(i32), N.ptr(pool), N.ptr(flag)), "patchset_export")
-        return cls(f64, i32, pool, flag, probe, tuple(counts))
+        atoms_of = np.zeros((n.value, 3), np.int32)
+        if n.value:
+            N.check(L.nsg_patchset_atoms(handle, N.ptr(atoms_of)), "patchset_atoms")
+        return cls(f64, i32, pool, flag, probe, tuple(counts), atoms_of)
+
+    def chain_to_atoms(self, gpatch: np.ndarray, atoms: np.ndarray | None = None) -> np.ndarray:
+        """(n_atoms, 4) derivative with respect to atom x, y, z, r from per-patch parameter
+        derivatives (n_patches x 8)."""
+        atoms = self.built_from if atoms is None else atoms
+        if atoms is None or self.atoms_of is None:
+            raise RuntimeError("patch set has no atom map")
+        atoms = np.ascontiguousarray(atoms, np.float64)
+        gpatch = np.ascontiguousarray(gpatch, np.float64)
+        out = np.zeros((len(atoms), 4))
+        rc = N.lib().nsg_ses_chain_grad(N.ptr(atoms), len(atoms), self.probe, self.n, N.ptr(self.i32), N.ptr(self.f64),
+                                        N.ptr(self.atoms_of), N.ptr(gpatch), N.ptr(out))
+        if rc not in (N.NSG_OK, -8):
+            N.check(rc, "gradient chain rule")
+        return out
 
 
 def build_ses_patches(atoms: np.ndarray, probe: float, threads: int = 0) -> PatchSet:
@@ -193,6 +224,7 @@ def build_ses_patches(atoms: np.ndarray, probe: float, threads: int = 0) -> Patc
     try:
         ps = PatchSet.from_native(h, probe)
         ps.degenerate = rc == -8
+        ps.built_from = atoms.copy()
         return ps
     finally:
         N.lib().nsg_patchset_free(h)
@@ -272,8 +304,10 @@ class Surface:
                                            N.ptr(p.pool_flag), p.probe), "upload_patches")
 
     def getSurf(self, optimize_grids: bool = True, fill: bool = False, cav_vol: float = 0.0,
-                keep_hits: bool = False, download: bool = True) -> float:
-        """Ray casts the grid: status map, insideness bits, volume; optional cavity filling."""
+                keep_hits: bool = False, download: bool = True, grad: bool = False) -> float:
+        """Ray casts the grid: status map, insideness bits, volume; optional cavity filling.
+        With ``grad`` the derivatives of the volume (and of the area of the following
+        ``triangulateSurface``) with respect to the atoms become available from ``gradients``."""
         if self.delphi is None:
             raise RuntimeError("Cannot get surface without DelPhi environment!")
         self.upload()
@@ -285,6 +319,8 @@ class Surface:
             flags |= N.ACCURATE_TRIANGULATION
         if keep_hits:
             flags |= N.KEEP_HITS
+        if grad:
+            flags |= N.GRAD
         prec = PRECISIONS.get(self.precision)
         if prec is None:
             raise ValueError(f"unknown Gpu_Precision {self.precision}")
@@ -358,6 +394,23 @@ class Surface:
         vals = np.zeros(int(counts.sum()))
         N.check(N.lib().nsg_download_hits(c, ray_set, N.ptr(counts), N.ptr(vals), len(vals)), "download hits")
         return counts.reshape(na, nb), vals
+
+    def patch_gradients(self, area: bool = True) -> tuple[np.ndarray, np.ndarray | None]:
+        """Per-patch derivatives (n_patches x 8) of the volume and, when the triangulation ran in
+        gradient mode, of the area."""
+        c = self._context().handle
+        gv = np.zeros((self.patches.n, 8))
+        ga = np.zeros((self.patches.n, 8)) if area else None
+        N.check(N.lib().nsg_patch_grads(c, N.ptr(gv), N.ptr(ga)), "patch gradients")
+        return gv, ga
+
+    def gradients(self, dvol: float = 1.0, darea: float = 0.0) -> np.ndarray:
+        """(n_atoms, 4) derivative of dvol * volume + darea * area with respect to the atoms'
+        x, y, z and radius, on the fixed grid of the last gradient-mode getSurf (and
+        triangulateSurface when darea is nonzero)."""
+        gv, ga = self.patch_gradients(area=darea != 0.0)
+        g = dvol * gv if ga is None else dvol * gv + darea * ga
+        return self.patches.chain_to_atoms(g)
 
     def stats(self) -> dict:
         out = np.zeros(8, np.int64)

@@ -223,3 +223,42 @@ def test_cavity_label_replay_matches_oracle(native_lib, oracle_mod):
     for pos, c in enumerate(order):
         node = roots[c]
         assert post.ravel()[node] == labels[pos]
+
+
+def test_patch_gradient_chain_rule(native_lib):
+    """Host chain rule from patch surface parameters to atoms (nsg_ses_chain_grad) against central
+    differences of the patch parameters themselves: for a random per-patch weight vector w,
+    d(sum_p w_p . theta_p(atoms)) / d(atoms) where theta is the sphere centre and radius of atom
+    patches, the probe centre of facets and (tc, u, R) of tori."""
+    atoms = generator.rsa_globule(60, 3)
+
+    def theta(a):
+        ps = nb.build_ses_patches(a, 1.4, 1)
+        f, k = ps.f64, ps.i32[:, 0]
+        th = np.zeros((ps.n, 8))
+        pt = k == 0
+        th[pt, :4] = f[pt, :4]
+        fc = (k == 3) | (k == 4)
+        th[fc, :3] = f[fc, :3]
+        ed = (k == 1) | (k == 2)
+        th[ed, :3] = f[ed, 4:7]
+        th[ed, 3:6] = f[ed, 15:18]
+        th[ed, 6] = f[ed, 7]
+        return ps, th
+
+    ps0, th0 = theta(atoms)
+    w = np.random.default_rng(1).normal(size=th0.shape)
+    g = ps0.chain_to_atoms(w)
+    h = 1e-6
+    rng = np.random.default_rng(2)
+    for i in rng.choice(len(atoms), size=12, replace=False):
+        for d in range(4):
+            a1 = atoms.copy()
+            a1[i, d] += h
+            a2 = atoms.copy()
+            a2[i, d] -= h
+            p1, t1 = theta(a1)
+            p2, t2 = theta(a2)
+            assert p1.n == p2.n == ps0.n
+            fd = float(((t1 - t2) * w).sum() / (2 * h))
+            assert abs(fd - g[i, d]) <= 1e-6 * (abs(fd) + 1.0), (i, d, fd, g[i, d])
