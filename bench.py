@@ -5,9 +5,11 @@ Default workload: the conformer ensemble (512 structures of 500-8000 atoms, 32 g
 perturbations, each on its own grid), ray cast and triangulated as one batch in mixed precision.
 One step = ray casting of the status ray set and the three accurate-triangulation ray sets
 (hits, status runs, insideness bits, volume), vertex assembly and marching cubes of all 512
-structures.  ``value`` is structures/s with the patch sets resident in HBM; ``e2e`` is the same
-step through the C-ABI with host buffers (batch layout and patch upload from pinned memory, the
-per-structure volumes and areas back).  The same batch in double precision and the plain
+structures, in gradient mode: the derivatives of every structure's volume and area with respect
+to its atoms (x, y, z, r) are part of the step.  ``value`` is structures/s with the patch sets
+resident in HBM; ``e2e`` is the same step through the C-ABI with host buffers (batch layout,
+patch and atom upload from pinned memory; the per-structure volumes, areas and atom derivatives
+back).  The same batch in double precision and the plain
 per-structure double-precision path are timed beside it (``comparison``).  The hit store and the
 bit grids are larger than L2, so no extra flush is needed.
 
@@ -283,15 +285,22 @@ def run_ensemble(args, world: int, rank: int, local: int) -> None:
     batch = nb.SurfaceBatch(surfs, device=local, precision=args.precision)
     batch.upload()
     ctx = batch._context().handle
-    flags = N.STATUS | N.ACCURATE_TRIANGULATION
+    atom_off, atoms_cat, patch_atoms = batch.packed_atoms()
+    N.check(L.nsg_upload_atoms(ctx, N.ptr(atom_off), N.ptr(atoms_cat), N.ptr(patch_atoms)), "upload atoms")
+    flags = N.STATUS | N.ACCURATE_TRIANGULATION | N.GRAD
 
-    def step(precision: int):
+    def step(precision: int, gv_host=None, ga_host=None):
+        """Volume, area and their atom derivatives of every structure (results stay on the device
+        unless host buffers are given)."""
         v = ctypes.c_double()
         N.check(L.nsg_raycast(ctx, flags, precision, ctypes.byref(v)), "raycast")
         a = ctypes.c_double()
         nv = ctypes.c_int64()
         nt = ctypes.c_int64()
         N.check(L.nsg_triangulate(ctx, ctypes.byref(a), ctypes.byref(nv), ctypes.byref(nt)), "triangulate")
+        rc = L.nsg_atom_grads(ctx, gv_host, ga_host)
+        if rc not in (N.NSG_OK, -8):
+            N.check(rc, "atom gradients")
         return nv.value, nt.value
 
     def timed(precision: int, steps: int) -> float:
@@ -341,6 +350,7 @@ def run_ensemble(args, world: int, rank: int, local: int) -> None:
     plain = nb.Context(local)
     dev = torch.device("cuda", local)
     dpatch = []
+    plain_off = [np.array([0, len(sf.patches.built_from)], np.int64) for sf in surfs]
     for sf in surfs:
         p = sf.patches
         dpatch.append([torch.from_numpy(x).to(dev) for x in (p.f64, p.i32, p.pool, p.pool_flag)])
@@ -353,11 +363,16 @@ def run_ensemble(args, world: int, rank: int, local: int) -> None:
             N.check(L.nsg_set_grid(plain.handle, ctypes.byref(sf.delphi.grid)), "set_grid")
             N.check(L.nsg_bind_patches_device(plain.handle, p.n, f64.data_ptr(), i32.data_ptr(), len(p.pool),
                                               pool.data_ptr(), flag.data_ptr(), p.probe), "bind")
+            N.check(L.nsg_upload_atoms(plain.handle, N.ptr(plain_off[b]), N.ptr(p.built_from), N.ptr(p.atoms_of)),
+                    "atoms")
             v = ctypes.c_double()
             N.check(L.nsg_raycast(plain.handle, flags, 0, ctypes.byref(v)), "raycast")
             a = ctypes.c_double()
             nv_, nt_ = ctypes.c_int64(), ctypes.c_int64()
             N.check(L.nsg_triangulate(plain.handle, ctypes.byref(a), ctypes.byref(nv_), ctypes.byref(nt_)), "tri")
+            rc = L.nsg_atom_grads(plain.handle, None, None)
+            if rc not in (N.NSG_OK, -8):
+                N.check(rc, "atom gradients")
 
     plain_pass(min(8, nstruct))
     torch.cuda.synchronize()
@@ -381,13 +396,22 @@ def run_ensemble(args, world: int, rank: int, local: int) -> None:
     h2d = sum(t.numel() for t in pin.values())
     vol_h = np.zeros(nstruct)
     area_h = np.zeros(nstruct)
+    for name, a in (("atoms", atoms_cat), ("patch_atoms", patch_atoms)):
+        t = torch.empty(a.nbytes, dtype=torch.uint8, pin_memory=True)
+        t.numpy()[:] = a.view(np.uint8).ravel()
+        pin[name] = t
+    h2d = sum(t.numel() for t in pin.values())
+    gv_h = torch.empty(len(atoms_cat) * 4, dtype=torch.float64, pin_memory=True)
+    ga_h = torch.empty(len(atoms_cat) * 4, dtype=torch.float64, pin_memory=True)
 
     def e2e_step():
         N.check(L.nsg_set_batch(ctx, nstruct, grids), "set_batch")
         N.check(L.nsg_upload_batch(ctx, N.ptr(patch_off), pin["f64"].data_ptr(), pin["i32"].data_ptr(),
                                    N.ptr(pool_off), pin["pool"].data_ptr(), pin["flag"].data_ptr(),
                                    surfs[0].patches.probe), "upload_batch")
-        step(prec)
+        N.check(L.nsg_upload_atoms(ctx, N.ptr(atom_off), pin["atoms"].data_ptr(), pin["patch_atoms"].data_ptr()),
+                "upload atoms")
+        step(prec, gv_h.data_ptr(), ga_h.data_ptr())
         N.check(L.nsg_batch_results(ctx, N.ptr(vol_h), N.ptr(area_h)), "batch results")
 
     e2e_step()
@@ -402,7 +426,7 @@ def run_ensemble(args, world: int, rank: int, local: int) -> None:
     e_ms = ctypes.c_double()
     N.check(L.nsg_event_elapsed(ctx, 2, 3, ctypes.byref(e_ms)), "elapsed")
     e2e_ms = max_over_ranks(max(e_ms.value / e2e_steps, e2e_wall * 1000.0))
-    d2h = 2 * 8 * nstruct
+    d2h = 2 * 8 * nstruct + 2 * gv_h.numel() * 8
 
     grids_l = [sf.delphi.grid for sf in surfs]
     rays = sum(rays_of(g) for g in grids_l)
@@ -453,6 +477,7 @@ def run_ensemble(args, world: int, rank: int, local: int) -> None:
             "config": {"workload": args.workload, "structures": nstruct,
                        "atoms_total": int(sum(len(a) for a in atoms)), "probe": w["probe"], "scale": w["scale"],
                        "perfil": w["perfil"], "rays_per_step": rays, "nodes_per_step": nodes,
+                       "outputs": "volume, area, d volume / d atoms, d area / d atoms per structure",
                        "l2": "inputs larger than L2 (hit store %.1f GB, bit grids %.2f GB)" % (
                            hit_store_gb, nwords * 4 / 1e9),
                        "parallelism": f"replicas x{world}"},

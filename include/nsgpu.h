@@ -131,6 +131,12 @@ int nsg_batch_results(nsg_ctx* ctx, double* volumes, double* areas);
  * Each hit x on its ray axis e moves by ds = -(dF/dtheta . dtheta) / (dF/dx . e) on the patch
  * surface F = 0; the volume sums them over interval ends, the area over analytic vertices. */
 int nsg_patch_grads(nsg_ctx* ctx, double* d_volume, double* d_area);
+/* The atoms behind the uploaded patches (after jitter; structure b owns [atom_off[b],
+ * atom_off[b+1])) and the 3 structure-local atoms of every patch (nsg_patchset_atoms). */
+int nsg_upload_atoms(nsg_ctx* ctx, const int64_t* atom_off, const double* atoms_xyzr, const int32_t* patch_atoms);
+/* d volume and d area of every structure with respect to its atoms' x, y, z, r (n_atoms x 4 each),
+ * chained from the patch derivatives on the device; either pointer may be NULL. */
+int nsg_atom_grads(nsg_ctx* ctx, double* d_volume, double* d_area);
 
 /* ---- the hot path ---- */
 /* Ray casting of Surface::getSurf: getPatchIntersectionData (src/ConnollySurface.cpp:4319-4590),

@@ -93,6 +93,8 @@ _SIGNATURES = {
     "nsg_patchset_free": ([_P], None),
     "nsg_patchset_atoms": ([_P, _P], _INT),
     "nsg_patch_grads": ([_P, _P, _P], _INT),
+    "nsg_upload_atoms": ([_P, _P, _P, _P], _INT),
+    "nsg_atom_grads": ([_P, _P, _P], _INT),
     "nsg_ses_chain_grad": ([_P, _I64, _D, _I64, _P, _P, _P, _P, _P], _INT),
 }
 

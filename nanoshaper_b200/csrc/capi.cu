@@ -98,6 +98,11 @@ struct nsg_ctx {
   DevBuf cand_sph, cand_tor, hit_t, hit_cnt, def_sph, def_tor;
   // gradient mode: hit / pair / vertex patches and the per-patch derivatives of volume and area
   DevBuf hit_pid, pair_pid, ovf_pscratch, gvol, garea, vpid, vgrad;
+  // atoms behind the patches (for the device chain rule) and the atom derivatives
+  std::vector<int64_t> patch_off{0, 0};
+  DevBuf d_atoms, d_patch_atoms, d_gatoms_vol, d_gatoms_area, d_bad;
+  int64_t n_atoms = 0;
+  bool have_atoms = false;
   bool grad_mode = false, have_gvol = false, have_garea = false;
   int64_t cand_cap = 0, def_cap = 0;
   // trace outputs
@@ -435,6 +440,7 @@ int nsg_ctx_destroy(nsg_ctx* c) {
                     &c->cand_sph, &c->cand_tor, &c->def_sph, &c->def_tor, &c->hit_t, &c->hit_cnt, &c->status, &c->bits, &c->pairs,
                     &c->ray_pair_off, &c->ray_pair_cnt, &c->cursors, &c->ovf_scratch, &c->err, &c->hits,
                     &c->hit_pid, &c->pair_pid, &c->ovf_pscratch, &c->gvol, &c->garea, &c->vpid, &c->vgrad,
+                    &c->d_atoms, &c->d_patch_atoms, &c->d_gatoms_vol, &c->d_gatoms_area, &c->d_bad,
                     &c->labels, &c->is_root, &c->sruns, &c->srun_off, &c->srun_cnt, &c->fr_cnt, &c->fr_off,
                     &c->fruns, &c->frow, &c->roots, &c->cc_count, &c->cc_desc, &c->cc_label_of,
                     &c->cc_fill_of, &c->nroots_d, &c->surv_cnt, &c->surv_off, &c->vpos, &c->vkey,
@@ -492,6 +498,8 @@ static int upload_common(nsg_ctx* c, int64_t n, int64_t npool, double probe) {
   c->pool32_valid = false;
   c->patch_nstruct = 1;
   c->patch_struct_valid = false;
+  c->patch_off.assign({0, n});
+  c->have_atoms = false;
   return NSG_OK;
 }
 
@@ -562,6 +570,69 @@ int nsg_upload_batch(nsg_ctx* c, const int64_t* patch_off, const double* f64, co
   if (rc) return rc;
   c->patch_nstruct = nb;
   c->patch_struct_valid = true;
+  c->patch_off.assign(patch_off, patch_off + nb + 1);
+  return NSG_OK;
+}
+
+// The atoms the uploaded patches were built from (after jitter), concatenated over the batch
+// (structure b owns atoms [atom_off[b], atom_off[b+1])), and the 3 atoms of every patch with
+// indices local to its structure (nsg_patchset_atoms); needed by nsg_atom_grads.
+int nsg_upload_atoms(nsg_ctx* c, const int64_t* atom_off, const double* atoms_xyzr, const int32_t* patch_atoms) {
+  if (!c || !atom_off || !atoms_xyzr || !patch_atoms) return NSG_ERR_ARG;
+  if (!c->has_patches || c->patch_nstruct != c->nstruct || (int32_t)c->patch_off.size() != c->nstruct + 1)
+    return fail(NSG_ERR_STATE, "patches of the current batch must be uploaded first");
+  const int32_t nb = c->nstruct;
+  if (atom_off[0] != 0) return fail(NSG_ERR_ARG, "atom offsets must start at 0");
+  std::vector<int32_t> g(std::max<int64_t>(3 * c->np, 1));
+  for (int32_t b = 0; b < nb; b++) {
+    const int64_t na = atom_off[b + 1] - atom_off[b];
+    if (na < 0) return fail(NSG_ERR_ARG, "atom offsets must be non-decreasing");
+    for (int64_t p = c->patch_off[b]; p < c->patch_off[b + 1]; p++)
+      for (int q = 0; q < 3; q++) {
+        const int32_t a = patch_atoms[3 * p + q];
+        if (a >= na) return fail(NSG_ERR_ARG, "patch atom index outside its structure");
+        g[3 * p + q] = a < 0 ? -1 : (int32_t)(a + atom_off[b]);
+      }
+  }
+  const int64_t n = atom_off[nb];
+  if (n >= ((int64_t)1 << 31)) return fail(NSG_ERR_CAPACITY, "more than 2^31 atoms");
+  CK(cudaSetDevice(c->device));
+  CK(c->d_atoms.ensure(std::max<int64_t>(n, 1) * 4 * sizeof(double)));
+  if (n) CK(cudaMemcpyAsync(c->d_atoms.p, atoms_xyzr, n * 4 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(upload_vec(c->d_patch_atoms, g, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->n_atoms = n;
+  c->have_atoms = true;
+  return NSG_OK;
+}
+
+// Derivatives of every structure's volume and area (last gradient-mode nsg_raycast /
+// nsg_triangulate) with respect to its atoms' x, y, z, r (n_atoms x 4 each, batch atom order),
+// chained on the device; either host pointer may be NULL.
+int nsg_atom_grads(nsg_ctx* c, double* d_volume, double* d_area) {
+  if (!c) return NSG_ERR_ARG;
+  if (!c->have_gvol || !c->have_atoms) return fail(NSG_ERR_STATE, "needs a gradient-mode ray cast and the atoms");
+  CK(cudaSetDevice(c->device));
+  const int64_t n = std::max<int64_t>(c->n_atoms, 1) * 4;
+  CK(c->d_gatoms_vol.ensure(n * sizeof(double)));
+  CK(c->d_gatoms_area.ensure(n * sizeof(double)));
+  CK(c->d_bad.ensure(sizeof(int32_t)));
+  CK(cudaMemsetAsync(c->d_gatoms_vol.p, 0, n * sizeof(double), c->stream));
+  CK(cudaMemsetAsync(c->d_gatoms_area.p, 0, n * sizeof(double), c->stream));
+  CK(cudaMemsetAsync(c->d_bad.p, 0, sizeof(int32_t), c->stream));
+  const nsg::PatchDev P = patch_dev(c);
+  LAUNCH(nsg::launch_chain(c->np, P.i32, P.f64, c->d_patch_atoms.as<int32_t>(), c->d_atoms.as<double>(), c->probe,
+                           c->gvol.as<double>(), c->have_garea ? c->garea.as<double>() : nullptr,
+                           c->d_gatoms_vol.as<double>(), c->d_gatoms_area.as<double>(), c->d_bad.as<int32_t>(),
+                           c->stream));
+  int32_t bad = 0;
+  CK(cudaMemcpyAsync(&bad, c->d_bad.p, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+  if (d_volume && c->n_atoms)
+    CK(cudaMemcpyAsync(d_volume, c->d_gatoms_vol.p, c->n_atoms * 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (d_area && c->n_atoms)
+    CK(cudaMemcpyAsync(d_area, c->d_gatoms_area.p, c->n_atoms * 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (bad) return fail(NSG_ERR_GEOMETRY, "a probe patch with a singular placement system was skipped");
   return NSG_OK;
 }
 

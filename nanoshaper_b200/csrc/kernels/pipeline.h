@@ -191,4 +191,10 @@ cudaError_t launch_trace_overflow(const PatchDev& P, const BatchDev& B, int set,
 cudaError_t launch_segment_sums(const double* v, const int64_t* base, const int64_t* idx, int n, double* out,
                                 bool accumulate, cudaStream_t s);
 
+// chain.cu: atom derivatives (x, y, z, r per atom; atomics) of volume and area from the per-patch
+// parameter derivatives; patch_atoms are batch-wide atom indices; n_bad counts singular facets.
+cudaError_t launch_chain(int64_t np, const int32_t* i32, const double* f64, const int32_t* patch_atoms,
+                         const double* atoms, double probe, const double* gpatch_vol, const double* gpatch_area,
+                         double* gvol_atoms, double* garea_atoms, int32_t* n_bad, cudaStream_t s);
+
 }  // namespace nsg

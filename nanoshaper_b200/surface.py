@@ -495,8 +495,10 @@ class SurfaceBatch:
         N.check(N.lib().nsg_upload_batch(c, N.ptr(patch_off), N.ptr(f64), N.ptr(i32), N.ptr(pool_off), N.ptr(pool),
                                          N.ptr(flag), probe), "upload_batch")
 
-    def getSurf(self, download: bool = False) -> np.ndarray:
-        """Ray casts every structure's grid; returns the per-structure volumes."""
+    def getSurf(self, download: bool = False, grad: bool = False) -> np.ndarray:
+        """Ray casts every structure's grid; returns the per-structure volumes.  With ``grad`` the
+        atom derivatives of the volumes (and of the areas of the following triangulateSurface)
+        become available from ``atom_gradients``."""
         self.upload()
         c = self._context().handle
         s0 = self.surfaces[0]
@@ -505,6 +507,8 @@ class SurfaceBatch:
             flags |= N.STATUS
         if s0.accurateTriangulation:
             flags |= N.ACCURATE_TRIANGULATION
+        if grad:
+            flags |= N.GRAD
         prec = PRECISIONS.get(self.precision)
         if prec is None:
             raise ValueError(f"unknown Gpu_Precision {self.precision}")
@@ -530,6 +534,28 @@ class SurfaceBatch:
         self.areas = np.zeros(len(self))
         N.check(N.lib().nsg_batch_results(c, None, N.ptr(self.areas)), "batch results")
         return self.areas
+
+    def packed_atoms(self) -> tuple:
+        """Concatenated atoms the patch sets were built from, their offsets and the patch atom map."""
+        ps = [s.patches for s in self.surfaces]
+        atom_off = np.zeros(len(ps) + 1, np.int64)
+        atom_off[1:] = np.cumsum([len(p.built_from) for p in ps])
+        atoms = np.ascontiguousarray(np.concatenate([p.built_from for p in ps]))
+        patch_atoms = np.ascontiguousarray(np.concatenate([p.atoms_of for p in ps]))
+        return atom_off, atoms, patch_atoms
+
+    def atom_gradients(self) -> list[tuple[np.ndarray, np.ndarray]]:
+        """Per structure: (d volume / d atoms, d area / d atoms), each (n_atoms, 4) for x, y, z, r,
+        after a gradient-mode getSurf and triangulateSurface (chained on the device)."""
+        c = self._context().handle
+        atom_off, atoms, patch_atoms = self.packed_atoms()
+        N.check(N.lib().nsg_upload_atoms(c, N.ptr(atom_off), N.ptr(atoms), N.ptr(patch_atoms)), "upload atoms")
+        gv = np.zeros((len(atoms), 4))
+        ga = np.zeros((len(atoms), 4))
+        rc = N.lib().nsg_atom_grads(c, N.ptr(gv), N.ptr(ga))
+        if rc not in (N.NSG_OK, -8):
+            N.check(rc, "atom gradients")
+        return [(gv[atom_off[b]:atom_off[b + 1]], ga[atom_off[b]:atom_off[b + 1]]) for b in range(len(self))]
 
     def close(self) -> None:
         if self.ctx is not None:

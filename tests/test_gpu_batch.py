@@ -62,3 +62,24 @@ def test_batch_matches_single(precision, native_lib):
     barea2 = batch.triangulateSurface()
     assert np.array_equal(bvol, bvol2) and np.array_equal(barea, barea2)
     batch.close()
+
+
+def test_batch_gradients_match_single(native_lib):
+    """Atom derivatives of volume and area from the batched device chain rule equal those of each
+    structure run alone through the host chain rule (1e-10 relative: atomics sum in any order)."""
+    surfs = _structures(SPECS[:4])
+    single = []
+    for s in surfs:
+        s.getSurf(True, False, 0.0, download=False, grad=True)
+        s.triangulateSurface(download=False)
+        single.append((s.gradients(1.0, 0.0), s.gradients(0.0, 1.0)))
+        s.ctx.close()
+        s.ctx = None
+    batch = nb.SurfaceBatch(surfs)
+    batch.getSurf(grad=True)
+    batch.triangulateSurface()
+    for b, (gv, ga) in enumerate(batch.atom_gradients()):
+        sv, sa = single[b]
+        assert np.abs(gv - sv).max() <= 1e-10 * np.abs(sv).max(), f"structure {b}: volume gradient"
+        assert np.abs(ga - sa).max() <= 1e-10 * np.abs(sa).max(), f"structure {b}: area gradient"
+    batch.close()
