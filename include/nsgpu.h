@@ -91,6 +91,17 @@ int nsg_ses_chain_grad(const double* atoms_xyzr, int64_t n_atoms, double probe_r
                        const int32_t* i32, const double* f64, const int32_t* patch_atoms, const double* gpatch,
                        double* grad_atoms);
 
+/* ---- files in the reference's layouts (host) ---- */
+/* DelPhiShared::saveStatus (src/DelphiShared.cpp:1458-1502): "%d " per node, i outer, k inner. */
+int nsg_write_status(const char* path, const int32_t* status, int64_t nx, int64_t ny, int64_t nz);
+/* DelPhiShared::saveCavities (src/DelphiShared.cpp:1889-1946): cavities.txt and cavitiesSize.txt. */
+int nsg_write_cavities(const char* cavities_path, const char* sizes_path, const int32_t* status, const NsGrid* grid,
+                       int32_t n_cavities, const double* sizes, const int32_t* filled);
+/* Surface::saveMesh (src/Surface.cpp:10857-11052): format 0 = root.off + roottriangleAreas.txt,
+ * 1 = root.ply (binary); revert writes every triangle in the opposite winding. */
+int nsg_write_mesh(const char* root, int format, const double* vertices, int64_t n_vertices, const int32_t* triangles,
+                   int64_t n_triangles, int revert);
+
 /* ---- device context ---- */
 int nsg_version(void);
 const char* nsg_last_error(void);

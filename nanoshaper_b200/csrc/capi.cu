@@ -125,6 +125,7 @@ struct nsg_ctx {
   std::vector<double> cav_size;
   std::vector<int32_t> cav_filled;
   // mesh
+  DevBuf cube_vl;
   DevBuf surv_cnt, surv_off, vpos, vkey, row_act_cnt, row_mid_cnt, row_act_off, row_mid_off, act_rec, act_mid,
       tri_cnt, tri_off, tris, cube_area, red_out;
   int64_t n_vert = 0, n_analytic = 0, n_tri = 0, n_active = 0;
@@ -440,7 +441,7 @@ int nsg_ctx_destroy(nsg_ctx* c) {
                     &c->cand_sph, &c->cand_tor, &c->def_sph, &c->def_tor, &c->hit_t, &c->hit_cnt, &c->status, &c->bits, &c->pairs,
                     &c->ray_pair_off, &c->ray_pair_cnt, &c->cursors, &c->ovf_scratch, &c->err, &c->hits,
                     &c->hit_pid, &c->pair_pid, &c->ovf_pscratch, &c->gvol, &c->garea, &c->vpid, &c->vgrad,
-                    &c->d_atoms, &c->d_patch_atoms, &c->d_gatoms_vol, &c->d_gatoms_area, &c->d_bad,
+                    &c->d_atoms, &c->d_patch_atoms, &c->d_gatoms_vol, &c->d_gatoms_area, &c->d_bad, &c->cube_vl,
                     &c->labels, &c->is_root, &c->sruns, &c->srun_off, &c->srun_cnt, &c->fr_cnt, &c->fr_off,
                     &c->fruns, &c->frow, &c->roots, &c->cc_count, &c->cc_desc, &c->cc_label_of,
                     &c->cc_fill_of, &c->nroots_d, &c->surv_cnt, &c->surv_off, &c->vpos, &c->vkey,
@@ -1104,6 +1105,8 @@ int nsg_triangulate(nsg_ctx* c, double* area_out, int64_t* nverts, int64_t* ntri
   CK(c->tri_off.ensure((n_act + 1) * sizeof(int64_t)));
   CK(c->cube_area.ensure(std::max<int64_t>(n_act, 1) * sizeof(double)));
   M.tri_cnt = c->tri_cnt.as<int32_t>();
+  CK(c->cube_vl.ensure(std::max<int64_t>(n_act, 1) * 12 * sizeof(int32_t)));
+  M.cube_vl = c->cube_vl.as<int32_t>();
   LAUNCH(nsg::launch_mc_tris(M, 0, c->stream));
   int64_t n_tri = 0;
   rc = scan_counts(c, c->tri_cnt.as<int32_t>(), n_act, c->tri_off.as<int64_t>(), &n_tri);

@@ -1,0 +1,140 @@
+// On-disk outputs in the reference's text layouts, written from caller-owned host arrays:
+//   status map      DelPhiShared::saveStatus (src/DelphiShared.cpp:1458-1502): "%d " per node,
+//                   i outer, j, k inner; a newline after every k row and a blank line per i
+//   cavities        DelPhiShared::saveCavities (src/DelphiShared.cpp:1889-1946): cavities.txt
+//                   lists the nodes of every cavity ("\n %f %f %f", k, j, i scan); cavitiesSize.txt
+//                   the count ("%f\n") then per cavity its node barycentre, volume and fill flag
+//                   ("%lf %lf %lf %lf %d\n")
+//   meshes          Surface::saveMesh (src/Surface.cpp:10857-11052): OFF ("%.3f" vertices,
+//                   "3 %d %d %d" faces, winding reversed on request) with triangleAreas.txt
+//                   (Heron area "%f" per triangle, "0." when degenerate); PLY as binary little
+//                   endian (double x, y, z; int32 faces with a uchar count)
+#include <cmath>
+#include <cstdio>
+#include <ctime>
+#include <string>
+#include <vector>
+
+#include "../ns_types.h"
+#include "host_api.h"
+
+namespace {
+
+const char* kProg = "nanoshaper_b200";
+const char* kVersion = "0.1.0";
+
+double coord(double vmin, double side, int64_t i) { return vmin + (double)i * side; }
+
+}  // namespace
+
+extern "C" {
+
+int nsg_write_status(const char* path, const int32_t* status, int64_t nx, int64_t ny, int64_t nz) {
+  if (!path || !status || nx <= 0 || ny <= 0 || nz <= 0) return NSG_ERR_ARG;
+  FILE* fp = fopen(path, "w");
+  if (!fp) return NSG_ERR_IO;
+  for (int64_t i = 0; i < nx; i++) {
+    for (int64_t j = 0; j < ny; j++) {
+      for (int64_t k = 0; k < nz; k++) fprintf(fp, "%d ", status[(k * ny + j) * nx + i]);
+      fprintf(fp, "\n");
+    }
+    fprintf(fp, "\n");
+  }
+  return fclose(fp) == 0 ? NSG_OK : NSG_ERR_IO;
+}
+
+int nsg_write_cavities(const char* cavities_path, const char* sizes_path, const int32_t* status, const NsGrid* g,
+                       int32_t n_cav, const double* sizes, const int32_t* filled) {
+  if (!cavities_path || !sizes_path || !status || !g || n_cav < 0 || (n_cav > 0 && (!sizes || !filled)))
+    return NSG_ERR_ARG;
+  FILE* fp = fopen(cavities_path, "w");
+  if (!fp) return NSG_ERR_IO;
+  std::vector<double> bx(n_cav, 0.0), by(n_cav, 0.0), bz(n_cav, 0.0);
+  std::vector<int64_t> cnt(n_cav, 0);
+  for (int64_t k = 0; k < g->nz; k++)
+    for (int64_t j = 0; j < g->ny; j++)
+      for (int64_t i = 0; i < g->nx; i++) {
+        const int32_t s = status[(k * g->ny + j) * g->nx + i];
+        if (s <= NS_STATUS_OUT) continue;
+        const double x = coord(g->xmin, g->side, i), y = coord(g->ymin, g->side, j), z = coord(g->zmin, g->side, k);
+        fprintf(fp, "\n %f %f %f", x, y, z);
+        const int c = s - NS_STATUS_FIRST_CAV;
+        if (c >= 0 && c < n_cav) {
+          bx[c] += x;
+          by[c] += y;
+          bz[c] += z;
+          cnt[c]++;
+        }
+      }
+  if (fclose(fp) != 0) return NSG_ERR_IO;
+  fp = fopen(sizes_path, "w");
+  if (!fp) return NSG_ERR_IO;
+  fprintf(fp, "%f\n", (float)n_cav);
+  for (int32_t c = 0; c < n_cav; c++) {
+    const double n = cnt[c] ? (double)cnt[c] : 1.0;
+    fprintf(fp, "%lf %lf %lf %lf %d\n", bx[c] / n, by[c] / n, bz[c] / n, sizes[c], filled[c] ? 1 : 0);
+  }
+  return fclose(fp) == 0 ? NSG_OK : NSG_ERR_IO;
+}
+
+// format: 0 OFF (+ triangleAreas.txt), 1 PLY (binary little endian).  root is the path without
+// extension; the reference's file names are root + ".off" / ".ply" and root + "triangleAreas.txt".
+int nsg_write_mesh(const char* root, int format, const double* vertices, int64_t n_vertices, const int32_t* triangles,
+                   int64_t n_triangles, int revert) {
+  if (!root || n_vertices < 0 || n_triangles < 0 || (n_vertices && !vertices) || (n_triangles && !triangles))
+    return NSG_ERR_ARG;
+  std::string base(root);
+  for (int64_t t = 0; t < 3 * n_triangles; t++)
+    if (triangles[t] < 0 || triangles[t] >= n_vertices) return NSG_ERR_ARG;
+  auto tri = [&](int64_t t, int q) { return triangles[3 * t + (revert ? 2 - q : q)]; };
+  if (format == 0) {
+    FILE* fp = fopen((base + ".off").c_str(), "w");
+    if (!fp) return NSG_ERR_IO;
+    time_t pt;
+    time(&pt);
+    fprintf(fp, "OFF\n");
+    fprintf(fp, "# File created by %s version %s date %s\n", kProg, kVersion, ctime(&pt));
+    fprintf(fp, "%d %d 0\n", (int)n_vertices, (int)n_triangles);
+    for (int64_t v = 0; v < n_vertices; v++)
+      fprintf(fp, "%.3f %.3f %.3f\n", vertices[3 * v], vertices[3 * v + 1], vertices[3 * v + 2]);
+    for (int64_t t = 0; t < n_triangles; t++) fprintf(fp, "3 %d %d %d\n", tri(t, 0), tri(t, 1), tri(t, 2));
+    if (fclose(fp) != 0) return NSG_ERR_IO;
+  } else if (format == 1) {
+    FILE* fp = fopen((base + ".ply").c_str(), "wb");
+    if (!fp) return NSG_ERR_IO;
+    fprintf(fp,
+            "ply\nformat binary_little_endian 1.0\nelement vertex %lld\nproperty double x\nproperty double y\n"
+            "property double z\nelement face %lld\nproperty list uchar int vertex_indices\nend_header\n",
+            (long long)n_vertices, (long long)n_triangles);
+    if (n_vertices) fwrite(vertices, sizeof(double), 3 * n_vertices, fp);
+    for (int64_t t = 0; t < n_triangles; t++) {
+      const unsigned char three = 3;
+      const int32_t f[3] = {tri(t, 0), tri(t, 1), tri(t, 2)};
+      fwrite(&three, 1, 1, fp);
+      fwrite(f, sizeof(int32_t), 3, fp);
+    }
+    if (fclose(fp) != 0) return NSG_ERR_IO;
+    return NSG_OK;
+  } else {
+    return NSG_ERR_ARG;
+  }
+  FILE* fp = fopen((base + "triangleAreas.txt").c_str(), "w");
+  if (!fp) return NSG_ERR_IO;
+  for (int64_t t = 0; t < n_triangles; t++) {
+    const double* p0 = vertices + 3 * (int64_t)triangles[3 * t];
+    const double* p1 = vertices + 3 * (int64_t)triangles[3 * t + 1];
+    const double* p2 = vertices + 3 * (int64_t)triangles[3 * t + 2];
+    auto dist = [](const double* a, const double* b) {
+      return sqrt((a[0] - b[0]) * (a[0] - b[0]) + (a[1] - b[1]) * (a[1] - b[1]) + (a[2] - b[2]) * (a[2] - b[2]));
+    };
+    const double a = dist(p0, p1), b = dist(p0, p2), c = dist(p1, p2);
+    const double ttt = (a + b + c) * (b + c - a) * (c + a - b) * (a + b - c);
+    if (ttt > 0)
+      fprintf(fp, "%f\n", 0.25 * sqrt(ttt));
+    else
+      fprintf(fp, "0.\n");
+  }
+  return fclose(fp) == 0 ? NSG_OK : NSG_ERR_IO;
+}
+
+}  // extern "C"

@@ -38,6 +38,12 @@ int nsg_patchset_export(const NsPatchSet* ps, double* f64, int32_t* i32, double*
 int nsg_patchset_atoms(const NsPatchSet* ps, int32_t* out);
 void nsg_patchset_free(NsPatchSet* ps);
 
+int nsg_write_status(const char* path, const int32_t* status, int64_t nx, int64_t ny, int64_t nz);
+int nsg_write_cavities(const char* cavities_path, const char* sizes_path, const int32_t* status, const NsGrid* g,
+                       int32_t n_cav, const double* sizes, const int32_t* filled);
+int nsg_write_mesh(const char* root, int format, const double* vertices, int64_t n_vertices, const int32_t* triangles,
+                   int64_t n_triangles, int revert);
+
 int nsg_ses_chain_grad(const double* atoms_xyzr, int64_t n_atoms, double probe, int64_t n_patches,
                        const int32_t* i32, const double* f64, const int32_t* patch_atoms, const double* gpatch,
                        double* grad_atoms);

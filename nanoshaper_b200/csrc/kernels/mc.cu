@@ -335,7 +335,16 @@ __global__ void k_mc_tris(MCArgs A, int emit) {
     const StructDev& S = A.B.s[rec_struct(rec.w)];
     int32_t vl[12];
     int em = c_emask[c];
-    for (int e = 0; e < 12; e++) vl[e] = (em >> e) & 1 ? (int32_t)edge_vertex(A, S, e, i, j, k) : -1;
+    int32_t* cv = A.cube_vl + 12 * a;
+    if (!emit) {
+      // the edge -> vertex searches run once; the emit pass reads their results
+      for (int e = 0; e < 12; e++) {
+        vl[e] = (em >> e) & 1 ? (int32_t)edge_vertex(A, S, e, i, j, k) : -1;
+        cv[e] = vl[e];
+      }
+    } else {
+      for (int e = 0; e < 12; e++) vl[e] = cv[e];
+    }
     int cnt = 0;
     int64_t o = emit ? A.tri_off[a] : 0;
     double area = 0.0;

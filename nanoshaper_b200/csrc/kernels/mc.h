@@ -43,6 +43,7 @@ struct MCArgs {
   int32_t* act_mid;              // index of the first midpoint vertex of the cube
   int64_t n_active;
   int32_t* tri_cnt;
+  int32_t* cube_vl;              // 12 per active cube: vertex of each cut edge (-1 none), pass 0 -> 1
   const int64_t* tri_off;
   int32_t* tris;
   double* cube_area;

@@ -140,6 +140,28 @@ class DelPhiShared:
         self.cavitiesSize: list[float] = []
         self.cavitiesFlag: list[bool] = []
 
+    def saveStatus(self, fname: str | Path = "") -> None:
+        """``fname.status.txt`` and the cavity files (DelPhiShared::saveStatus / saveCavities)."""
+        if self.status is None:
+            raise RuntimeError("Cannot save null status!")
+        st = np.ascontiguousarray(self.status, np.int32).reshape(-1)
+        N.check(N.lib().nsg_write_status(f"{fname}.status.txt".encode(), N.ptr(st), self.nx, self.ny, self.nz),
+                "saveStatus")
+        self.saveCavities(Path(str(fname)).parent if str(fname) else Path("."))
+
+    def saveCavities(self, directory: str | Path = ".") -> None:
+        """``cavities.txt`` (cavity nodes) and ``cavitiesSize.txt`` (barycentre, volume, filled)."""
+        if self.status is None:
+            raise RuntimeError("Cannot save cavities with null status!")
+        st = np.ascontiguousarray(self.status, np.int32).reshape(-1)
+        sizes = np.ascontiguousarray(self.cavitiesSize, np.float64)
+        flags = np.ascontiguousarray([1 if f else 0 for f in self.cavitiesFlag], np.int32)
+        d = Path(directory)
+        N.check(N.lib().nsg_write_cavities(str(d / "cavities.txt").encode(), str(d / "cavitiesSize.txt").encode(),
+                                           N.ptr(st), ctypes.byref(self.grid), len(sizes),
+                                           N.ptr(sizes) if len(sizes) else None, N.ptr(flags) if len(flags) else None),
+                "saveCavities")
+
     def buildGrid(self, scale: float, perfil: float) -> bool:
         N.check(N.lib().nsg_grid_build(N.ptr(self.atoms), len(self.atoms), scale, perfil, ctypes.byref(self.grid)),
                 "buildGrid")
@@ -368,19 +390,23 @@ class Surface:
             N.check(N.lib().nsg_download_mesh(c, N.ptr(self.vertices), N.ptr(self.vertex_edges),
                                               N.ptr(self.triangles)), "download mesh")
         if outputMesh:
-            self.saveMesh(fileName + ".off")
+            self.saveMesh("off", False, fileName)
         return self.area
 
-    def saveMesh(self, path: str | Path) -> None:
-        """OFF mesh file (vertices then triangles), as the reference's default output."""
-        v, t = self.vertices, self.triangles
-        with open(path, "w") as f:
-            f.write("OFF\n")
-            f.write(f"{len(v)} {len(t)} 0\n")
-            for p in v:
-                f.write(f"{p[0]:.6f} {p[1]:.6f} {p[2]:.6f}\n")
-            for q in t:
-                f.write(f"3 {q[0]} {q[1]} {q[2]}\n")
+    MESH_FORMATS = {"off": 0, "ply": 1}
+
+    def saveMesh(self, format: str = "off", revert: bool = False, fileName: str | Path = "triangulatedSurf") -> None:
+        """Mesh file in the reference's layout: ``fileName.off`` (+ ``fileNametriangleAreas.txt``)
+        or ``fileName.ply`` (Surface::saveMesh, src/Surface.cpp:10857-11052)."""
+        if self.vertices is None or self.triangles is None:
+            raise RuntimeError("no mesh: call triangulateSurface() first")
+        fmt = self.MESH_FORMATS.get(str(format).lower())
+        if fmt is None:
+            raise ValueError(f"unsupported mesh format {format}; available: {sorted(self.MESH_FORMATS)}")
+        v = np.ascontiguousarray(self.vertices, np.float64)
+        t = np.ascontiguousarray(self.triangles, np.int32)
+        N.check(N.lib().nsg_write_mesh(str(fileName).encode(), fmt, N.ptr(v), len(v), N.ptr(t), len(t), int(revert)),
+                "saveMesh")
 
     def hits(self, ray_set: int) -> tuple[np.ndarray, np.ndarray]:
         """Per-ray sorted hit parameters of one ray set from the last keep_hits ray cast."""

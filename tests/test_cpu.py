@@ -262,3 +262,44 @@ def test_patch_gradient_chain_rule(native_lib):
             assert p1.n == p2.n == ps0.n
             fd = float(((t1 - t2) * w).sum() / (2 * h))
             assert abs(fd - g[i, d]) <= 1e-6 * (abs(fd) + 1.0), (i, d, fd, g[i, d])
+
+
+def test_file_writers_layouts(native_lib, tmp_path):
+    """Status, cavity and mesh files follow the reference's layouts (DelPhiShared::saveStatus /
+    saveCavities, Surface::saveMesh)."""
+    ds = nb.DelPhiShared(np.array([[0.0, 0.0, 0.0, 1.5]]), 2.0, 50.0)
+    g = ds.grid
+    st = np.full((g.nz, g.ny, g.nx), 2, np.int32)
+    st[1, 2, 3] = -1
+    st[2, 1, 1] = 4
+    st[2, 1, 2] = 4
+    ds.status = st
+    ds.cavitiesSize = [0.25]
+    ds.cavitiesFlag = [True]
+    ds.saveStatus(str(tmp_path / "run"))
+    text = (tmp_path / "run.status.txt").read_text()
+    blocks = text.split("\n\n")
+    assert len(blocks) == g.nx + 1 and blocks[-1] == ""
+    rows = blocks[3].split("\n")
+    vals = [int(x) for x in rows[2].split()]
+    assert len(rows) == g.ny and len(vals) == g.nz and vals[1] == -1  # i=3, j=2, k=1
+    cav = (tmp_path / "cavities.txt").read_text().split("\n")
+    assert cav[0] == "" and len(cav) == 3
+    x1, y1, z1 = (float(v) for v in cav[1].split())
+    assert abs(x1 - ds.x[1]) < 1e-6 and abs(y1 - ds.y[1]) < 1e-6 and abs(z1 - ds.z[2]) < 1e-6
+    sz = (tmp_path / "cavitiesSize.txt").read_text().splitlines()
+    assert sz[0] == "1.000000"
+    bx, by, bz, vol, flag = sz[1].split()
+    assert abs(float(bx) - 0.5 * (ds.x[1] + ds.x[2])) < 1e-6 and flag == "1" and float(vol) == 0.25
+    s = nb.ConnollySurface(nb.ConfigFile(), ds)
+    s.vertices = np.array([[0.0, 0.0, 0.0], [1.0, 0.0, 0.0], [0.0, 1.0, 0.0]])
+    s.triangles = np.array([[0, 1, 2]], np.int32)
+    s.saveMesh("off", True, str(tmp_path / "mesh"))
+    off = (tmp_path / "mesh.off").read_text().splitlines()
+    assert off[0] == "OFF" and off[1].startswith("# File created by") and off[3] == "3 1 0"
+    assert off[4] == "0.000 0.000 0.000" and off[-1] == "3 2 1 0"
+    assert (tmp_path / "meshtriangleAreas.txt").read_text() == "0.500000\n"
+    s.saveMesh("ply", False, str(tmp_path / "mesh"))
+    raw = (tmp_path / "mesh.ply").read_bytes()
+    head, body = raw.split(b"end_header\n")
+    assert b"element vertex 3" in head and b"element face 1" in head and len(body) == 3 * 24 + 13
