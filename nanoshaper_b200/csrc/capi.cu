@@ -336,6 +336,23 @@ int reduce_sum(nsg_ctx* c, const double* in, int64_t n, double* host_out) {
   return NSG_OK;
 }
 
+// Window-area sum of a panel (the bound of its candidate count).
+int panel_area(nsg_ctx* c, int panel) {
+  const int set = panel == 0 ? 0 : panel + 1;
+  const nsg::BatchDev B = batch_dev(c);
+  nsg::PatchDev P = patch_dev(c);
+  CK(c->bin_area.ensure(3 * sizeof(unsigned long long)));
+  unsigned long long* area = c->bin_area.as<unsigned long long>() + panel;
+  CK(cudaMemsetAsync(area, 0, sizeof(unsigned long long), c->stream));
+  LAUNCH(nsg::launch_bin_count(P, B, set, nullptr, area, c->stream));
+  unsigned long long a_host = 0;
+  CK(cudaMemcpyAsync(&a_host, area, sizeof(a_host), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->win_area[panel] = (int64_t)a_host;
+  return NSG_OK;
+}
+
+// Patch lists of every 32x4 ray tile of a panel (CSR), for the per-ray overflow path.
 int bin_panel(nsg_ctx* c, int panel) {
   const int set = panel == 0 ? 0 : panel + 1;
   const int64_t ntiles = c->tiles_tot[panel];
@@ -344,17 +361,10 @@ int bin_panel(nsg_ctx* c, int panel) {
   CK(c->tile_off[panel].ensure((ntiles + 1) * sizeof(int64_t)));
   CK(cudaMemsetAsync(c->tile_cnt[panel].p, 0, (ntiles + 1) * sizeof(int32_t), c->stream));
   nsg::PatchDev P = patch_dev(c);
-  CK(c->bin_area.ensure(3 * sizeof(unsigned long long)));
-  unsigned long long* area = c->bin_area.as<unsigned long long>() + panel;
-  CK(cudaMemsetAsync(area, 0, sizeof(unsigned long long), c->stream));
-  LAUNCH(nsg::launch_bin_count(P, B, set, c->tile_cnt[panel].as<int32_t>(), area, c->stream));
+  LAUNCH(nsg::launch_bin_count(P, B, set, c->tile_cnt[panel].as<int32_t>(), nullptr, c->stream));
   int64_t total = 0;
   int rc = scan_counts(c, c->tile_cnt[panel].as<int32_t>(), ntiles, c->tile_off[panel].as<int64_t>(), &total);
   if (rc) return rc;
-  unsigned long long a_host = 0;
-  CK(cudaMemcpyAsync(&a_host, area, sizeof(a_host), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
-  c->win_area[panel] = (int64_t)a_host;
   CK(c->tile_list[panel].ensure(std::max<int64_t>(total, 1) * sizeof(int32_t)));
   CK(cudaMemsetAsync(c->tile_cnt[panel].p, 0, (ntiles + 1) * sizeof(int32_t), c->stream));
   LAUNCH(nsg::launch_bin_fill(P, B, set, c->tile_off[panel].as<int64_t>(), c->tile_cnt[panel].as<int32_t>(),
@@ -703,7 +713,7 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
   for (int panel = 0; panel < 3; panel++) {
     if (panel == 0 && !(do_status || do_mc)) continue;
     if (panel > 0 && !do_mc) continue;
-    int rc = bin_panel(c, panel);
+    int rc = panel_area(c, panel);
     if (rc) return rc;
   }
   stage_end(c, kStageBin);
@@ -816,14 +826,14 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
       nsg::HitStore hs{c->hit_t.as<double>(), c->hit_cnt.as<int32_t>(), nr, grad ? c->hit_pid.as<int32_t>() : nullptr};
       CK(cudaMemsetAsync(c->hit_cnt.p, 0, nr * sizeof(int32_t), c->stream));
       c->launches += precision == NSG_PRECISION_MIXED ? 6 : 4;
-      CK(nsg::launch_trace(P, B, s, c->tiles_tot[panel], c->tile_off[panel].as<int64_t>(),
-                           c->tile_list[panel].as<int32_t>(), o, co, hs, precision, c->stream));
+      CK(nsg::launch_trace(P, B, s, c->tiles_tot[panel], o, co, hs, precision, c->stream));
     }
     stage_end(c, kStageTrace);
     int32_t novf[4] = {0, 0, 0, 0};
     CK(cudaMemcpyAsync(novf, ovf_count, 4 * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     int64_t tot_ovf = 0;
+    bool tiles_built[3] = {false, false, false};
     stage_begin(c, kStageOverflow);
     for (int si = 0; si < nsets; si++) {
       int s = sets[si];
@@ -831,6 +841,11 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
       tot_ovf += n;
       if (n == 0) continue;
       const int panel = s == 0 ? 0 : s - 1;
+      if (!tiles_built[panel]) {
+        int rc = bin_panel(c, panel);
+        if (rc) return rc;
+        tiles_built[panel] = true;
+      }
       CK(c->ovf_scratch.ensure((size_t)n * nsg::kOverflowCap * sizeof(double)));
       if (grad) CK(c->ovf_pscratch.ensure((size_t)n * nsg::kOverflowCap * sizeof(int32_t)));
       LAUNCH(nsg::launch_trace_overflow(P, B, s, c->tile_off[panel].as<int64_t>(), c->tile_list[panel].as<int32_t>(),

@@ -174,13 +174,13 @@ struct PatchDev {
 cudaError_t launch_windows(const PatchDev& P, int32_t* win, const BatchDev& B, cudaStream_t s);
 // Patch-local FP32 copy of the pool: planes (n, d + n.c), clipping spheres (s - c, r^2).
 cudaError_t launch_pool32(const PatchDev& P, float4* pool32, cudaStream_t s);
+// tile_cnt null: only the window-area sum (the candidate bound of the panel).
 cudaError_t launch_bin_count(const PatchDev& P, const BatchDev& B, int set, int32_t* tile_cnt,
                              unsigned long long* area, cudaStream_t s);
 cudaError_t launch_bin_fill(const PatchDev& P, const BatchDev& B, int set, const int64_t* tile_off,
                             int32_t* tile_cursor, int32_t* tile_list, cudaStream_t s);
-cudaError_t launch_trace(const PatchDev& P, const BatchDev& B, int set, int64_t ntiles, const int64_t* tile_off,
-                         const int32_t* tile_list, const TraceOut& out, const CandOut& co, const HitStore& hs,
-                         int precision, cudaStream_t s);
+cudaError_t launch_trace(const PatchDev& P, const BatchDev& B, int set, int64_t ntiles, const TraceOut& out,
+                         const CandOut& co, const HitStore& hs, int precision, cudaStream_t s);
 // pscratch: patch column of the overflow hits (gradient mode), else null.
 cudaError_t launch_trace_overflow(const PatchDev& P, const BatchDev& B, int set, const int64_t* tile_off,
                                   const int32_t* tile_list, const TraceOut& out, int n_ovf, double* scratch,

@@ -22,7 +22,6 @@ namespace nsg {
 
 namespace {
 
-constexpr int kChunk = 32;  // patches staged per shared-memory chunk
 
 __device__ __forceinline__ double gcoord(const GridDev& g, int d, int64_t i) { return g.mn[d] + (double)i * g.side; }
 
@@ -79,11 +78,12 @@ __global__ void k_bin(PatchDev P, BatchDev B, int set, int32_t* tile_cnt, const 
   const RaySet rs = make_ray_set(set, S.g);
   if (area) {
     // pixel-window area: an upper bound of the patch's candidate rays in this panel
-    unsigned a = live ? (unsigned)((w[3 + rs.fd] - w[rs.fd] + 1) * (w[3 + rs.ld] - w[rs.ld] + 1)) : 0u;
+    const int ww = w[3 + rs.fd] - w[rs.fd] + 1, wh = w[3 + rs.ld] - w[rs.ld] + 1;
+    unsigned a = (live && ww > 0 && wh > 0) ? (unsigned)(ww * wh) : 0u;
     unsigned sum = __reduce_add_sync(0xffffffffu, a);
     if ((threadIdx.x & 31) == 0 && sum) atomicAdd(area, (unsigned long long)sum);
   }
-  if (!live) return;
+  if (!live || (tile_cnt == nullptr && tile_list == nullptr)) return;
   int64_t ntm = (rs.nb + kTileM - 1) / kTileM;
   int m0 = w[rs.fd] / kTileM, m1 = w[3 + rs.fd] / kTileM;
   int n0 = w[rs.ld] / kTileN, n1 = w[3 + rs.ld] / kTileN;
@@ -401,93 +401,63 @@ struct TraceCtx {
 };
 
 // Wavefront ray tracing of one ray set, three kernel kinds:
-//  * k_cand: one CTA per 32x4 ray tile stages the tile's patch list in shared memory; for each
-//    patch a warp tests its 32 rays against the reference's candidate conditions (pixel window,
-//    bounding box, equatorial disc) and appends the surviving (ray, patch) pairs to a warp buffer
-//    split by patch type (spheres: atoms and probes; tori), flushed to global candidate lists
-//    with one atomic per flush;
+//  * k_cand: one warp per patch walks the patch's pixel window (the reference's CELL_CULLING
+//    window, k_windows), 32 rays at a time, tests each against the bounding box and equatorial
+//    disc and appends the surviving (ray, patch) pairs with one atomic per warp step, to the
+//    sphere list (atoms and probes) or the torus list; a patch's candidates stay contiguous, so
+//    the intersection kernels read its record once per warp;
 //  * k_isect<torus, mixed>: one thread per candidate pair, sphere and torus pairs in separate
 //    launches so that both run converged with their own register budget; hits are filed into
 //    the ray's slots of a slot-major hit store through a per-ray atomic counter;
-//  * k_fill: one CTA per tile loads each ray's hits, sorts them and performs the interval fill.
-constexpr int kWarpBuf = 256;
-
-__global__ void __launch_bounds__(kTraceThreads) k_cand(TraceCtx C, const int64_t* __restrict__ tile_off,
-                                                         const int32_t* __restrict__ tile_list, CandOut co) {
-  constexpr int kThreads = kTraceThreads;
-  const int panel = C.set == 0 ? 0 : C.set - 1;
-  const int64_t tile = blockIdx.x;
-  const StructDev& S = C.B.s[C.B.tile_struct[panel][tile]];
-  const GridDev& g = S.g;
-  const RaySet rs = make_ray_set(C.set, g);
-  __shared__ double s_f[kChunk * NS_PATCH_F64];
-  __shared__ int s_i[kChunk];
-  __shared__ int s_pid[kChunk];
-  __shared__ int s_w[kChunk * 4];
-  __shared__ int2 s_buf[kTileN][2][kWarpBuf];
-  const int64_t ntm = (rs.nb + kTileM - 1) / kTileM;
-  const int64_t lt = tile - S.tile_base[panel];
-  const int64_t tm = lt % ntm, tn = lt / ntm;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int64_t m = tm * kTileM + lane;
-  const int64_t n = tn * kTileN + warp;
-  const bool valid = (m < rs.nb) && (n < rs.na);
-  const int tid = threadIdx.x;
-  const int32_t rid = (int32_t)(S.ray_base[C.set] + n * rs.nb + m);
-  double pa[3];
-  pa[rs.fd] = gcoord(g, rs.fd, valid ? m : 0) + rs.delta;
-  pa[rs.ld] = gcoord(g, rs.ld, n < rs.na ? n : 0) + rs.delta;
-  pa[rs.vc] = gcoord(g, rs.vc, 0) + rs.delta;
-  int fill[2] = {0, 0};
-  auto flush = [&](int ty) {
-    int cnt = fill[ty];
-    unsigned long long base = 0;
-    if (lane == 0 && cnt) base = atomicAdd(co.count + ty, (unsigned long long)cnt);
-    base = __shfl_sync(0xffffffffu, base, 0);
+//  * k_fill: one CTA per 32x4 ray tile loads each ray's hits, sorts them and performs the
+//    interval fill.
+__global__ void __launch_bounds__(256) k_cand(TraceCtx C, CandOut co) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t pid = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); pid < C.P.n; pid += warps) {
+    const int32_t* w = C.P.win + 6 * pid;
+    if (w[0] < 0) continue;
+    const StructDev& S = C.B.s[C.B.patch_struct[pid]];
+    const GridDev& g = S.g;
+    const RaySet rs = make_ray_set(C.set, g);
+    const int m0 = w[rs.fd], n0 = w[rs.ld];
+    const int W = w[3 + rs.fd] - m0 + 1, H = w[3 + rs.ld] - n0 + 1;
+    if (W <= 0 || H <= 0) continue;
+    const int total = W * H;
+    const double* src = C.P.f64 + (int64_t)NS_PATCH_F64 * pid;
+    double f[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) f[k] = __ldg(src + k);
+    const int kind = C.P.i32[NS_PATCH_I32 * pid];
+    const int ty = (kind == NS_EDGE_REG || kind == NS_EDGE_SING) ? 1 : 0;
     int2* dst = ty ? co.tor : co.sph;
-    for (int i = lane; i < cnt; i += 32) {
-      if ((int64_t)(base + i) < co.cap) dst[base + i] = s_buf[warp][ty][i];
-    }
-    if (lane == 0 && cnt && (int64_t)(base + cnt) > co.cap) atomicExch(C.out.error_flag, 6);
-    __syncwarp();
-    fill[ty] = 0;
-  };
-  const int64_t beg = tile_off[tile], end = tile_off[tile + 1];
-  for (int64_t base = beg; base < end; base += kChunk) {
-    int cnt = (int)((end - base) < kChunk ? (end - base) : kChunk);
-    __syncthreads();
-    for (int e = tid; e < cnt * 4; e += kThreads) {
-      int q = e >> 2, k = e & 3;
-      int64_t pid = tile_list[base + q];
-      s_f[q * NS_PATCH_F64 + k] = __ldg(C.P.f64 + (int64_t)NS_PATCH_F64 * pid + k);
-    }
-    for (int q = tid; q < cnt; q += kThreads) {
-      int64_t pid = tile_list[base + q];
-      s_pid[q] = (int)pid;
-      int kind = C.P.i32[NS_PATCH_I32 * pid];
-      s_i[q] = (kind == NS_EDGE_REG || kind == NS_EDGE_SING) ? 1 : 0;
-      const int32_t* w = C.P.win + 6 * pid;
-      s_w[4 * q + 0] = w[rs.fd];
-      s_w[4 * q + 1] = w[3 + rs.fd];
-      s_w[4 * q + 2] = w[rs.ld];
-      s_w[4 * q + 3] = w[3 + rs.ld];
-    }
-    __syncthreads();
-    for (int q = 0; q < cnt; q++) {
-      bool pass = valid && m >= s_w[4 * q] && m <= s_w[4 * q + 1] && n >= s_w[4 * q + 2] && n <= s_w[4 * q + 3] &&
-                  candidate(s_f + q * NS_PATCH_F64, rs, pa);
-      unsigned mask = __ballot_sync(0xffffffffu, pass);
+    const int64_t rbase = S.ray_base[C.set];
+    for (int base = 0; base < total; base += 32) {
+      const int idx = base + lane;
+      bool pass = false;
+      int64_t rid = 0;
+      if (idx < total) {
+        const int dn = idx / W;
+        const int m = m0 + (idx - dn * W), n = n0 + dn;
+        double pa[3];
+        pa[rs.fd] = gcoord(g, rs.fd, m) + rs.delta;
+        pa[rs.ld] = gcoord(g, rs.ld, n) + rs.delta;
+        pa[rs.vc] = gcoord(g, rs.vc, 0) + rs.delta;
+        pass = candidate(f, rs, pa);
+        rid = rbase + (int64_t)n * rs.nb + m;
+      }
+      const unsigned mask = __ballot_sync(0xffffffffu, pass);
       if (!mask) continue;
-      const int ty = s_i[q];
-      if (pass) s_buf[warp][ty][fill[ty] + __popc(mask & ((1u << lane) - 1u))] = make_int2(rid, s_pid[q]);
-      fill[ty] += __popc(mask);
-      __syncwarp();
-      if (fill[ty] > kWarpBuf - 32) flush(ty);
+      unsigned long long slot = 0;
+      if (lane == 0) slot = atomicAdd(co.count + ty, (unsigned long long)__popc(mask));
+      slot = __shfl_sync(0xffffffffu, slot, 0);
+      if (pass) {
+        const unsigned long long q = slot + __popc(mask & ((1u << lane) - 1u));
+        if ((int64_t)q < co.cap) dst[q] = make_int2((int)rid, (int)pid);
+      }
+      if (lane == 0 && (int64_t)(slot + __popc(mask)) > co.cap) atomicExch(C.out.error_flag, 6);
     }
   }
-  __syncwarp();
-  flush(0);
-  flush(1);
 }
 
 // One thread per candidate pair of one type: intersection, feasibility, hit filing.
@@ -934,13 +904,16 @@ cudaError_t launch_bin_fill(const PatchDev& P, const BatchDev& B, int set, const
   return cudaGetLastError();
 }
 
-cudaError_t launch_trace(const PatchDev& P, const BatchDev& B, int set, int64_t ntiles, const int64_t* tile_off,
-                         const int32_t* tile_list, const TraceOut& out, const CandOut& co, const HitStore& hs,
-                         int precision, cudaStream_t s) {
+cudaError_t launch_trace(const PatchDev& P, const BatchDev& B, int set, int64_t ntiles, const TraceOut& out,
+                         const CandOut& co, const HitStore& hs, int precision, cudaStream_t s) {
   if (ntiles <= 0) return cudaSuccess;
   TraceCtx C{P, B, set, out};
   const int panel = set == 0 ? 0 : set - 1;
-  k_cand<<<(unsigned)ntiles, kTraceThreads, 0, s>>>(C, tile_off, tile_list, co);
+  if (P.n > 0) {
+    int64_t blocks = (P.n + 7) / 8;
+    if (blocks > 148 * 64) blocks = 148 * 64;
+    k_cand<<<(unsigned)blocks, 256, 0, s>>>(C, co);
+  }
   if (panel == 0) launch_isect<0>(C, co, hs, precision, s);
   else if (panel == 1) launch_isect<1>(C, co, hs, precision, s);
   else launch_isect<2>(C, co, hs, precision, s);
