@@ -115,10 +115,8 @@ class ClockSampler:
 
 
 def dist_setup():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return world, rank, local
+    from nanoshaper_b200 import dist as D
+    return D.env()
 
 
 def make_workload(name: str):
@@ -253,13 +251,9 @@ def run_ensemble(args, world: int, rank: int, local: int) -> None:
         return
 
     import torch
+    from nanoshaper_b200 import dist as D
     torch.cuda.set_device(local)
-    pg = None
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
-        pg = dist
+    pg = D.init("nccl")
 
     import nanoshaper_b200 as nb
     from nanoshaper_b200 import _native as N
@@ -268,16 +262,11 @@ def run_ensemble(args, world: int, rank: int, local: int) -> None:
     L = N.lib()
 
     def barrier():
-        if pg is not None:
-            pg.barrier()
+        D.barrier(pg)
         torch.cuda.synchronize()
 
     def max_over_ranks(x: float) -> float:
-        if pg is None:
-            return x
-        t = torch.tensor([x], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        return float(t.item())
+        return D.max_over_ranks(pg, x)
 
     atoms, surfs, t_gen, t_build = make_ensemble(w)
     nstruct = len(surfs)
@@ -432,7 +421,7 @@ def run_ensemble(args, world: int, rank: int, local: int) -> None:
     rays = sum(rays_of(g) for g in grids_l)
     nodes = sum(g.nx * g.ny * g.nz for g in grids_l)
     nwords = sum(((g.nx + 31) // 32) * g.ny * g.nz for g in grids_l)
-    structs_per_s = world * nstruct * 1000.0 / ms_per_step
+    structs_per_s = D.throughput(nstruct, world, ms_per_step)
     hit_store_gb = max(sum(g.ny * g.nz for g in grids_l), sum(g.nx * g.ny for g in grids_l),
                        sum(g.nx * g.nz for g in grids_l)) * 32 * 8 / 1e9
 
@@ -502,8 +491,7 @@ def run_ensemble(args, world: int, rank: int, local: int) -> None:
         }
         print(json.dumps(line))
     batch.close()
-    if pg is not None:
-        pg.destroy_process_group()
+    D.close(pg)
 
 
 def main():
@@ -545,13 +533,9 @@ def main():
         return
 
     import torch
+    from nanoshaper_b200 import dist as D
     torch.cuda.set_device(local)
-    pg = None
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
-        pg = dist
+    pg = D.init("nccl")
 
     import nanoshaper_b200 as nb
     from nanoshaper_b200 import _native as N
@@ -570,8 +554,7 @@ def main():
     flags = N.STATUS | N.ACCURATE_TRIANGULATION
 
     def barrier():
-        if pg is not None:
-            pg.barrier()
+        D.barrier(pg)
         torch.cuda.synchronize()
 
     # device-resident inputs
@@ -616,15 +599,11 @@ def main():
     launches = L.nsg_launch_count(ctx) - launches0
     barrier()
     clocks = clk.stop()
-    ms_per_step = ms.value / args.steps
-    if pg is not None:
-        t = torch.tensor([ms_per_step], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms_per_step = float(t.item())
+    ms_per_step = D.max_over_ranks(pg, ms.value / args.steps)
 
     rays_per_struct = g.nz * g.ny + (g.nz * g.ny + g.ny * g.nx + g.nz * g.nx)
     nodes = g.nx * g.ny * g.nz
-    structs_per_s = world * 1000.0 / ms_per_step
+    structs_per_s = D.throughput(1, world, ms_per_step)
     rays_per_s = structs_per_s * rays_per_struct
     nodes_per_s = structs_per_s * nodes
 
@@ -660,11 +639,7 @@ def main():
     e2e_wall = (time.perf_counter() - t0) / e2e_steps
     e_ms = ctypes.c_double()
     N.check(L.nsg_event_elapsed(ctx, 2, 3, ctypes.byref(e_ms)), "elapsed")
-    e2e_ms = max(e_ms.value / e2e_steps, e2e_wall * 1000.0)
-    if pg is not None:
-        t = torch.tensor([e2e_ms], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = D.max_over_ranks(pg, max(e_ms.value / e2e_steps, e2e_wall * 1000.0))
     d2h = nodes * 4 + r[3] * (24 + 16) + r[4] * 12
 
     # roofline of the dominant stage (HBM: algorithmic bytes per launch / measured launch time)
@@ -726,8 +701,7 @@ def main():
         }
         print(json.dumps(line))
     surf.ctx.close()
-    if pg is not None:
-        pg.destroy_process_group()
+    D.close(pg)
 
 
 if __name__ == "__main__":

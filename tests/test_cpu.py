@@ -303,3 +303,40 @@ def test_file_writers_layouts(native_lib, tmp_path):
     raw = (tmp_path / "mesh.ply").read_bytes()
     head, body = raw.split(b"end_header\n")
     assert b"element vertex 3" in head and b"element face 1" in head and len(body) == 3 * 24 + 13
+
+
+def _replica_rank(rank, world, port, out):
+    import os
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world),
+                      LOCAL_RANK=str(rank))
+    from nanoshaper_b200 import dist as D
+    pg = D.init("gloo", timeout_s=60)
+    try:
+        step_ms = 10.0 + 5.0 * rank  # the second replica is slower
+        worst = D.max_over_ranks(pg, step_ms)
+        D.barrier(pg)
+        out.put((rank, worst, D.throughput(512, world, worst)))
+    finally:
+        D.close(pg)
+
+
+def test_replica_timing_gloo_world2():
+    """Two replicas over gloo: every rank sees the slowest rank's time and the whole-job
+    throughput counts both ranks' structures (the bench's multi-GPU aggregation)."""
+    import multiprocessing as mp
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_replica_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, worst, thr in res:
+        assert worst == 15.0
+        assert abs(thr - 2 * 512 * 1000.0 / 15.0) < 1e-9
