@@ -4,13 +4,11 @@
 //   * sphere hits: the discriminant and square root in FP32 on local offsets, then one FP64
 //     Newton correction of the square root against the FP64 discriminant; near-tangent rays
 //     (|disc| below a threshold) fall back to the double-precision test;
-//   * torus hits: every decision of the Ferrari-type solver (discriminant and root count,
-//     resolvent branch and sign, which root pairs are real) in FP64 with the double-precision
-//     solver's expressions; its transcendental steps (cube roots, arccos, cos) and the root
-//     estimates in FP32, the resolvent root refined by FP64 Newton steps and each quartic root
-//     polished by two FP64 Newton steps on the FP64 polynomial; a decision within rounding of its
-//     threshold, merging roots or a small derivative defer the candidate to the double-precision
-//     solver;
+//   * torus hits: the clipping-sphere entry as for spheres; the quartic root isolation stays in
+//     FP64 (the double-precision solver, its decisions guarded: a discriminant, resolvent root or
+//     square-root argument within rounding of its threshold defers the candidate); measured on
+//     B200, an FP32 isolation followed by FP64 Newton polishing costs more FP64 issue than the
+//     FP64 solver itself;
 //   * feasibility: plane and sphere tests in FP32 on local coordinates; a test whose FP32 value is
 //     within a tolerance of zero is re-evaluated in FP64 from the double-precision pool.
 // Hit points therefore carry FP64 accuracy and the accept/reject decisions equal the
@@ -27,111 +25,57 @@ constexpr float kDiscTol = 1e-3f;     // sphere discriminant r^2 - dx^2 - dy^2 [
 constexpr float kPlaneTol = 1e-3f;    // plane test value [A] (planes are unit normals)
 constexpr float kSphereTol = 1e-2f;   // clipping-sphere test |p-s|^2 - r^2 [A^2]
 
-// Estimate of the resolvent root chosen by the double-precision solver (real_cubic_f64): the
-// branch decisions are taken in FP64 with the same expressions, so the same root is approximated;
-// the chosen closed form (Cardano cube roots, or the trigonometric form) is evaluated in FP32.
-__device__ __forceinline__ float real_cubic_mixed(double b, double c, double d) {
-  const double p = -(1.0 / 3.0) * b * b + c;
-  const double q = (2. / 27.) * b * b * b - (1. / 3.) * b * c + d;
-  const double D3p = (1. / 27.) * p * p * p;
-  const double D3 = D3p + 0.25 * q * q;
-  const float bf = (float)b;
-  if (fabs(c) < b * b * 1.E-6 && fabs(d) < fabs(b) * 1.E-6) {
-    return (float)(c / b - b - d / (b * b));
-  } else if (fabs(d / c) < 4.E-4) {
-    const double ratio = d / c;
-    if (D3 <= 0.) return (float)(0.5 * (ratio - b + sqrt((b - ratio) * (b - ratio) - 4. * (c - ratio * (b - ratio)))));
-    return (float)(-ratio * ratio * (b - ratio) / (3. * ratio * ratio - 2. * b * ratio + c) - ratio);
-  } else if (D3 >= 0.) {
-    const float radD3 = sqrtf((float)D3);
-    const float hq = (float)(0.5 * q);
-    return cbrtf(radD3 - hq) - cbrtf(radD3 + hq) - (1.f / 3.f) * bf;
-  } else {
-    const float Aarg = acosf((float)(-0.5 * q / sqrt(-D3p)));
-    return 2.f * sqrtf((float)(-(1. / 3.) * p)) * cosf((1.f / 3.f) * Aarg) - (1.f / 3.f) * bf;
-  }
-}
-
-// Root isolation of the monic quartic x^4 + b x^3 + c x^2 + d x + e, following the
-// double-precision solver (quartic_f64): the depressed coefficients, the discriminant and the
-// root-count decision in FP64 with the same operation sequence; the resolvent root estimated in
-// FP32 on the same branch and refined by FP64 Newton steps on the resolvent cubic; the
-// square-root arguments that decide which root pairs are real in FP64; the root estimates in
-// FP32 (each is polished on the FP64 quartic afterwards).  Returns the number of roots, or -1
-// when a decision is within rounding of its threshold (the resolvent refinement did not converge,
-// the resolvent root or a square-root argument is near zero) or the coefficients need the
-// reciprocal variant.
-__device__ __forceinline__ int quartic_mixed(float roots[4], double b, double c, double d, double e) {
+// The double-precision quartic solver (quartic_f64: the reference's Ferrari-type
+// quarticEqSolutions, src/tools.cpp:525-639) with every decision guarded: it returns -1 when the
+// discriminant, the resolvent root or a square-root argument lies within relative rounding of its
+// threshold, or when the coefficients need the reciprocal variant.  Otherwise the roots equal
+// those of quartic_f64 on the same coefficients (the same operation sequence), with complex pairs
+// (negative square-root arguments) left out instead of returned as NaN.
+__device__ __forceinline__ int quartic_guarded(double roots[4], double b, double c, double d, double e) {
+  constexpr double kRel = 1e-10;
   const double b_2 = 0.5 * b;
   const double b_4 = 0.25 * b;
   const double p = c - 1.5 * (b_2 * b_2);
   const double q = d + b_2 * (b_2 * b_2 - c);
   const double r = e + b_4 * (b_4 * (c - 3.0 * b_4 * b_4) - d);
   const double f = p * p - 4. * r;
-  const double delta =
-      4. * f * (4. * r * (p * p) - p * (q * q) - 16. * (r * r)) + (q * q) * (128. * p * r - 27. * (q * q));
+  const double t1 = 4. * r * (p * p), t2 = p * (q * q), t3 = 16. * (r * r), t4 = 128. * p * r, t5 = 27. * (q * q);
+  const double delta = 4. * f * (t1 - t2 - t3) + (q * q) * (t4 - t5);
   if (e != 0. && (fabs(p) > 3.E+3 || fabs(r) > 3.E+3 || fabs(q) > 3.E+3 || fabs(delta) > 1.E+14)) return -1;
+  const double dscale = fabs(4. * f) * (fabs(t1) + fabs(t2) + fabs(t3)) + (q * q) * (fabs(t4) + fabs(t5));
+  if (!(fabs(delta) > kRel * dscale)) return -1;
   int num_sol;
-  if (delta < 0. || (delta == 0. && (p >= 0. || f < 0.)))
+  if (delta < 0.) {
     num_sol = 2;
-  else if ((p < 0. && f > 0.) || (delta == 0. && p == 0. && r == 0.))
-    num_sol = 4;
-  else
-    return 0;
-  // resolvent m^3 + p m^2 + (p^2/4 - r) m - q^2/8
-  const double cb = p, cc = 0.25 * (p * p) - r, cd = (-0.125) * (q * q);
-  double m = (double)real_cubic_mixed(cb, cc, cd);
-  const double mscale = fabs(p) + sqrt(fabs(r)) + 1e-30;
-  for (int it = 0; it < 3; it++) {
-    const double g = ((m + cb) * m + cc) * m + cd;
-    const double gp = (3.0 * m + 2.0 * cb) * m + cc;
-    if (!(fabs(gp) > 1e-8 * (mscale * mscale + 1e-30))) return -1;
-    const double step = g / gp;
-    m -= step;
-    if (it == 2 && !(fabs(step) <= 1e-12 * (fabs(m) + 1e-6 * mscale))) return -1;
+  } else {
+    if (!(fabs(p) > kRel * (fabs(c) + 1.5 * b_2 * b_2)) || !(fabs(f) > kRel * (p * p + fabs(4. * r)))) return -1;
+    if (p < 0. && f > 0.) num_sol = 4;
+    else return 0;
   }
-  if (!(fabs(m) > 1e-9 * mscale) || fabs(m) < 1.E-13) return -1;
-  if (m <= 0.) return 0;
+  const double m = real_cubic_f64(p, 0.25 * (p * p) - r, (-0.125) * (q * q));
+  const double mscale = fabs(p) + sqrt(fabs(r)) + 1e-300;
+  if (!(fabs(m) > kRel * mscale) || fabs(m) < 1.E-13) return -1;
+  if (m <= 0) return 0;
   const double p1 = -2. * (p + m);
   const double p2 = sqrt(2. * (q * q) / m);
+  const double coeff = sqrt(2. * m);
   const double sscale = fabs(p1) + fabs(p2);
   const double sdmax = p1 + p2;
-  if (!(fabs(sdmax) > 1e-9 * sscale)) return -1;
-  const float coeff = sqrtf((float)(2. * m));
-  const float b4f = (float)b_4;
-  const float sq = (q >= 0.) ? -coeff : coeff;
+  if (!(fabs(sdmax) > kRel * sscale)) return -1;
   int n = 0;
   if (sdmax > 0.) {
-    const float s = sqrtf((float)sdmax);
-    roots[n++] = 0.5f * (sq - s) - b4f;
-    roots[n++] = 0.5f * (sq + s) - b4f;
+    roots[n++] = 0.5 * (((q >= 0.) ? -coeff : coeff) - sqrt(sdmax)) - 0.25 * b;
+    roots[n++] = 0.5 * (((q >= 0.) ? -coeff : coeff) + sqrt(sdmax)) - 0.25 * b;
   }
   if (num_sol == 4) {
     const double sdmin = p1 - p2;
-    if (!(fabs(sdmin) > 1e-9 * sscale)) return -1;
+    if (!(fabs(sdmin) > kRel * sscale)) return -1;
     if (sdmin > 0.) {
-      const float s = sqrtf((float)sdmin);
-      roots[n++] = 0.5f * (-sq - s) - b4f;
-      roots[n++] = 0.5f * (-sq + s) - b4f;
+      roots[n++] = 0.5 * (((q >= 0.) ? coeff : -coeff) - sqrt(sdmin)) - 0.25 * b;
+      roots[n++] = 0.5 * (((q >= 0.) ? coeff : -coeff) + sqrt(sdmin)) - 0.25 * b;
     }
   }
   return n;
-}
-
-// Two Newton steps on the FP64 monic quartic; returns false when the derivative is too small
-// for the polish to be trusted (a root of multiplicity > 1 is close) or when the FP32 estimate
-// was not already close to a root.
-__device__ __forceinline__ bool polish_root(double B, double C, double D, double E, double& x) {
-  for (int it = 0; it < 2; it++) {
-    double f = (((x + B) * x + C) * x + D) * x + E;
-    double fp = ((4.0 * x + 3.0 * B) * x + 2.0 * C) * x + D;
-    double scale = fabs(D) + fabs(C) + fabs(B) + 1.0;
-    if (!(fabs(fp) > 1e-3 * scale)) return false;
-    double step = f / fp;
-    if (it == 0 && !(fabs(step) < 1e-3 * (fabs(x) + 1.0))) return false;
-    x -= step;
-  }
-  return true;
 }
 
 // Plane test value in FP64 (from the double-precision pool) when the FP32 one is undecided.

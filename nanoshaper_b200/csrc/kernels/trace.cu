@@ -228,26 +228,12 @@ __device__ __forceinline__ int intersect_mixed(const double* f, int kind, int fi
     orig1[vc] = x_in;
     double B, C, D, E;
     torus_coeffs_f64(f, P.probe, vc, orig1, &B, &C, &D, &E);
-    float rt[4];
-    int nr = quartic_mixed(rt, B, C, D, E);
+    double roots[4];
+    int nr = quartic_guarded(roots, B, C, D, E);
     if (nr < 0) {
       if (ctr) atomicAdd(ctr + kCntFbQuartic, 1ull);
       return kDefer;
     }
-    double roots[4];
-    for (int i = 0; i < nr; i++) {
-      roots[i] = (double)rt[i];
-      if (!polish_root(B, C, D, E, roots[i])) {
-        if (ctr) atomicAdd(ctr + kCntFbRoot, 1ull);
-        return kDefer;
-      }
-    }
-    for (int i = 0; i < nr; i++)
-      for (int j = i + 1; j < nr; j++)
-        if (fabs(roots[i] - roots[j]) < 1e-6) {
-          if (ctr) atomicAdd(ctr + kCntFbRoot, 1ull);
-          return kDefer;
-        }
     const double r2 = r * r;
     for (int i = 0; i < nr; i++) {
       double root = roots[i];
@@ -417,8 +403,11 @@ __global__ void __launch_bounds__(256) k_cand(TraceCtx C, CandOut co) {
   for (int64_t pid = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); pid < C.P.n; pid += warps) {
     const int32_t* w = C.P.win + 6 * pid;
     if (w[0] < 0) continue;
-    const StructDev& S = C.B.s[C.B.patch_struct[pid]];
-    const GridDev& g = S.g;
+    const int b = C.B.patch_struct[pid];
+    // grid values in registers: the loop below stores to global memory, which would otherwise
+    // force re-reads of the structure record
+    const GridDev g = C.B.s[b].g;
+    const int64_t rbase = C.B.s[b].ray_base[C.set];
     const RaySet rs = make_ray_set(C.set, g);
     const int m0 = w[rs.fd], n0 = w[rs.ld];
     const int W = w[3 + rs.fd] - m0 + 1, H = w[3 + rs.ld] - n0 + 1;
@@ -431,31 +420,40 @@ __global__ void __launch_bounds__(256) k_cand(TraceCtx C, CandOut co) {
     const int kind = C.P.i32[NS_PATCH_I32 * pid];
     const int ty = (kind == NS_EDGE_REG || kind == NS_EDGE_SING) ? 1 : 0;
     int2* dst = ty ? co.tor : co.sph;
-    const int64_t rbase = S.ray_base[C.set];
+    auto test = [&](int idx, int64_t* rid) {
+      const int dn = idx / W;
+      const int m = m0 + (idx - dn * W), n = n0 + dn;
+      double pa[3];
+      // gcoord(g, d, i) + delta, with the same operation order
+      pa[rs.fd] = (g.mn[rs.fd] + (double)m * g.side) + rs.delta;
+      pa[rs.ld] = (g.mn[rs.ld] + (double)n * g.side) + rs.delta;
+      pa[rs.vc] = (g.mn[rs.vc] + 0.0 * g.side) + rs.delta;
+      *rid = rbase + (int64_t)n * rs.nb + m;
+      return candidate(f, rs, pa);
+    };
+    // pass 1 counts the window's candidates, one atomic reserves their slots, pass 2 writes them
+    int cnt = 0;
     for (int base = 0; base < total; base += 32) {
       const int idx = base + lane;
-      bool pass = false;
+      int64_t rid;
+      const bool pass = idx < total && test(idx, &rid);
+      cnt += __popc(__ballot_sync(0xffffffffu, pass));
+    }
+    if (cnt == 0) continue;
+    unsigned long long slot = 0;
+    if (lane == 0) slot = atomicAdd(co.count + ty, (unsigned long long)cnt);
+    slot = __shfl_sync(0xffffffffu, slot, 0);
+    if ((int64_t)(slot + cnt) > co.cap) {
+      if (lane == 0) atomicExch(C.out.error_flag, 6);
+      continue;
+    }
+    for (int base = 0; base < total; base += 32) {
+      const int idx = base + lane;
       int64_t rid = 0;
-      if (idx < total) {
-        const int dn = idx / W;
-        const int m = m0 + (idx - dn * W), n = n0 + dn;
-        double pa[3];
-        pa[rs.fd] = gcoord(g, rs.fd, m) + rs.delta;
-        pa[rs.ld] = gcoord(g, rs.ld, n) + rs.delta;
-        pa[rs.vc] = gcoord(g, rs.vc, 0) + rs.delta;
-        pass = candidate(f, rs, pa);
-        rid = rbase + (int64_t)n * rs.nb + m;
-      }
+      const bool pass = idx < total && test(idx, &rid);
       const unsigned mask = __ballot_sync(0xffffffffu, pass);
-      if (!mask) continue;
-      unsigned long long slot = 0;
-      if (lane == 0) slot = atomicAdd(co.count + ty, (unsigned long long)__popc(mask));
-      slot = __shfl_sync(0xffffffffu, slot, 0);
-      if (pass) {
-        const unsigned long long q = slot + __popc(mask & ((1u << lane) - 1u));
-        if ((int64_t)q < co.cap) dst[q] = make_int2((int)rid, (int)pid);
-      }
-      if (lane == 0 && (int64_t)(slot + __popc(mask)) > co.cap) atomicExch(C.out.error_flag, 6);
+      if (pass) dst[slot + __popc(mask & ((1u << lane) - 1u))] = make_int2((int)rid, (int)pid);
+      slot += __popc(mask);
     }
   }
 }
