@@ -241,13 +241,18 @@ __global__ void k_mc_rows(MCArgs A, int emit) {
 // vertex (cut edge without an analytic vertex); the mask goes to bits 8..10 of the record and the
 // count to mid_cnt.  Pass 1: writes those vertices at their final indices (act_mid).
 __global__ void k_mc_mid(MCArgs A, int emit) {
+  // case tables in shared memory: a constant-bank read with a different index per lane is
+  // serialised across the warp
+  __shared__ uint16_t s_emask[256];
+  for (int t = threadIdx.x; t < 256; t += blockDim.x) s_emask[t] = c_emask[t];
+  __syncthreads();
   for (int64_t a = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; a < A.n_active; a += (int64_t)gridDim.x * blockDim.x) {
     int4 rec = A.act_rec[a];
     const int64_t i = rec.x, j = rec.y, k = rec.z;
     const StructDev& S = A.B.s[rec_struct(rec.w)];
     const GridDev& g = S.g;
     if (!emit) {
-      int mm = own_midpoints(A, S, i, j, k, c_emask[rec.w & 255]);
+      int mm = own_midpoints(A, S, i, j, k, s_emask[rec.w & 255]);
       A.act_rec[a].w = (rec.w & ~(7 << 8)) | (mm << 8);
       A.mid_cnt[a] = __popc(mm);
       continue;
@@ -328,13 +333,18 @@ __device__ __forceinline__ double vdist(const double* a, const double* b) {
 
 // One thread per active cube; pass 0 counts triangles, pass 1 writes them and their areas.
 __global__ void k_mc_tris(MCArgs A, int emit) {
+  __shared__ int8_t s_tri[256][16];
+  __shared__ uint16_t s_emask[256];
+  for (int t = threadIdx.x; t < 256 * 16; t += blockDim.x) (&s_tri[0][0])[t] = (&c_tri[0][0])[t];
+  for (int t = threadIdx.x; t < 256; t += blockDim.x) s_emask[t] = c_emask[t];
+  __syncthreads();
   for (int64_t a = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; a < A.n_active; a += (int64_t)gridDim.x * blockDim.x) {
     int4 rec = A.act_rec[a];
     int c = rec.w & 255;
     int64_t i = rec.x, j = rec.y, k = rec.z;
     const StructDev& S = A.B.s[rec_struct(rec.w)];
     int32_t vl[12];
-    int em = c_emask[c];
+    int em = s_emask[c];
     int32_t* cv = A.cube_vl + 12 * a;
     if (!emit) {
       // the edge -> vertex searches run once; the emit pass reads their results
@@ -348,8 +358,8 @@ __global__ void k_mc_tris(MCArgs A, int emit) {
     int cnt = 0;
     int64_t o = emit ? A.tri_off[a] : 0;
     double area = 0.0;
-    for (int q = 0; q < 16 && c_tri[c][q] >= 0; q += 3) {
-      int32_t v0 = vl[c_tri[c][q]], v1 = vl[c_tri[c][q + 1]], v2 = vl[c_tri[c][q + 2]];
+    for (int q = 0; q < 16 && s_tri[c][q] >= 0; q += 3) {
+      int32_t v0 = vl[s_tri[c][q]], v1 = vl[s_tri[c][q + 1]], v2 = vl[s_tri[c][q + 2]];
       if (v0 < 0 || v1 < 0 || v2 < 0) continue;
       if (emit) {
         const double* P0 = A.vpos + 3 * (int64_t)v0;

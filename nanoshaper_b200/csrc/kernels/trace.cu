@@ -286,9 +286,16 @@ struct GradCtx {
   double* gvol;
 };
 
+struct SamePid {
+  __device__ __forceinline__ int32_t operator()(int32_t p) const { return p; }
+};
+
+// pcol holds, per hit, an id that pid_of turns into the hit's patch (the patch itself, or the
+// hit's slot in the hit store).
+template <class IdT = int32_t, class PidOf = SamePid>
 __device__ __forceinline__ int make_pairs(double* col, int stride, int nh, double pa_vc, double dir, double vmin,
-                                          double scale, bool vertex_pairs, double* vol, int32_t* pcol = nullptr,
-                                          GradCtx* gc = nullptr) {
+                                          double scale, bool vertex_pairs, double* vol, IdT* pcol = nullptr,
+                                          GradCtx* gc = nullptr, PidOf pid_of = PidOf()) {
   double v = 0.0;
   int np = 0;
   if (nh > 0 && (nh & 1) == 0) {
@@ -298,15 +305,15 @@ __device__ __forceinline__ int make_pairs(double* col, int stride, int nh, doubl
         double lim1 = pa_vc + dir * t1;
         double lim2 = pa_vc + dir * t2;
         v += lim2 - lim1;
-        int32_t p1 = 0, p2 = 0;
+        IdT p1 = 0, p2 = 0;
         if (pcol) {
           p1 = pcol[q * stride];
           p2 = pcol[(q + 1) * stride];
           double x[3] = {gc->x[0], gc->x[1], gc->x[2]};
           x[gc->vc] = lim1;
-          add_hit_grad(gc->f64, gc->i32, gc->probe, p1, x, gc->vc, -gc->w, gc->gvol);
+          add_hit_grad(gc->f64, gc->i32, gc->probe, pid_of(p1), x, gc->vc, -gc->w, gc->gvol);
           x[gc->vc] = lim2;
-          add_hit_grad(gc->f64, gc->i32, gc->probe, p2, x, gc->vc, gc->w, gc->gvol);
+          add_hit_grad(gc->f64, gc->i32, gc->probe, pid_of(p2), x, gc->vc, gc->w, gc->gvol);
         }
         if (vertex_pairs) {
           int64_t a = (int64_t)rintp((lim1 - vmin) * scale);
@@ -551,7 +558,9 @@ __global__ void __launch_bounds__(kTraceThreads) k_fill(TraceCtx C, HitStore hs)
   uint32_t* const bits = C.out.bits + S.word_base;
   const int64_t nwords = S.nwords;
   __shared__ double s_hit[kHitCap * kThreads];
-  __shared__ int32_t s_pid[kGrad ? kHitCap * kThreads : 1];
+  // gradient mode: each hit's slot in the hit store (its patch is read from there when needed),
+  // one byte per hit to keep the shared-memory footprint and so the occupancy up
+  __shared__ uint8_t s_slot[kGrad ? kHitCap * kThreads : 1];
   const int64_t ntm = (rs.nb + kTileM - 1) / kTileM;
   const int64_t lt = tile - S.tile_base[panel];
   const int64_t tm = lt % ntm, tn = lt / ntm;
@@ -566,13 +575,13 @@ __global__ void __launch_bounds__(kTraceThreads) k_fill(TraceCtx C, HitStore hs)
   int hc = valid ? hs.cnt[rid] : 0;
   bool ovf = hc > kHitCap;
   int nh = ovf ? 0 : hc;
-  int32_t* pcol = kGrad ? s_pid + tid : nullptr;
+  uint8_t* pcol = kGrad ? s_slot + tid : nullptr;
   for (int i = 0; i < nh; i++) col[i * kThreads] = hs.t[(int64_t)i * hs.nrays + rid];
   if (kGrad)
-    for (int i = 0; i < nh; i++) pcol[i * kThreads] = hs.pid[(int64_t)i * hs.nrays + rid];
+    for (int i = 0; i < nh; i++) pcol[i * kThreads] = (uint8_t)i;
   for (int i = 1; i < nh; i++) {
     double v = col[i * kThreads];
-    int32_t pv = kGrad ? pcol[i * kThreads] : 0;
+    uint8_t pv = kGrad ? pcol[i * kThreads] : 0;
     int j = i;
     while (j > 0 && col[(j - 1) * kThreads] > v) {
       col[j * kThreads] = col[(j - 1) * kThreads];
@@ -610,6 +619,7 @@ __global__ void __launch_bounds__(kTraceThreads) k_fill(TraceCtx C, HitStore hs)
   }
   double vol = 0.0;
   int np = 0;
+  const auto slot_pid = [&](uint8_t sl) { return hs.pid[(int64_t)sl * hs.nrays + rid]; };
   if (kGrad) {
     GradCtx gc;
     gc.f64 = C.P.f64;
@@ -621,7 +631,8 @@ __global__ void __launch_bounds__(kTraceThreads) k_fill(TraceCtx C, HitStore hs)
     gc.x[rs.vc] = 0.0;
     gc.vc = rs.vc;
     gc.gvol = C.out.gvol;
-    if (valid && !ovf) np = make_pairs(col, kThreads, nh, pa_vc, dirl, g.mn[rs.vc], g.scale, mc, &vol, pcol, &gc);
+    if (valid && !ovf)
+      np = make_pairs(col, kThreads, nh, pa_vc, dirl, g.mn[rs.vc], g.scale, mc, &vol, pcol, &gc, slot_pid);
   } else {
     if (valid && !ovf) np = make_pairs(col, kThreads, nh, pa_vc, dirl, g.mn[rs.vc], g.scale, mc, &vol);
   }
@@ -662,7 +673,8 @@ __global__ void __launch_bounds__(kTraceThreads) k_fill(TraceCtx C, HitStore hs)
         for (int q = 0; q < np; q++) {
           C.out.pairs[2 * (off + q)] = col[(2 * q) * kThreads];
           C.out.pairs[2 * (off + q) + 1] = col[(2 * q + 1) * kThreads];
-          if (kGrad) C.out.pair_pid[off + q] = make_int2(pcol[(2 * q) * kThreads], pcol[(2 * q + 1) * kThreads]);
+          if (kGrad)
+            C.out.pair_pid[off + q] = make_int2(slot_pid(pcol[(2 * q) * kThreads]), slot_pid(pcol[(2 * q + 1) * kThreads]));
         }
         C.out.ray_pair_off[ord] = off;
         C.out.ray_pair_cnt[ord] = np;
