@@ -69,4 +69,33 @@ __device__ __forceinline__ void add_hit_grad(const double* __restrict__ f64, con
     if (g[k] != 0.0) atomicAdd(o + k, w * g[k]);
 }
 
+// Warp-collective: lanes holding terms g (already weighted) for patch pid (-1: none) add them to
+// gsum[8 * pid + k].  Consecutive lanes with the same patch (neighbouring rays or vertices usually
+// hit the same patch) are summed with a segmented shuffle scan first, so each run of equal pids
+// issues one atomic per component instead of one per lane.  All 32 lanes must call it.
+__device__ __forceinline__ void warp_add_grad(int32_t pid, double* g, double* gsum) {
+  const int lane = threadIdx.x & 31;
+  const int32_t prev = __shfl_up_sync(0xffffffffu, pid, 1);
+  const bool head = lane == 0 || prev != pid;
+  const unsigned heads = __ballot_sync(0xffffffffu, head);
+  const int start = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));
+  const bool tail = lane == 31 || ((heads >> (lane + 1)) & 1u);
+#pragma unroll
+  for (int k = 0; k < NS_GRAD_PER_PATCH; k++) {
+    double v = g[k];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const double u = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane - o >= start) v += u;
+    }
+    g[k] = v;
+  }
+  if (tail && pid >= 0) {
+    double* o = gsum + (int64_t)NS_GRAD_PER_PATCH * pid;
+#pragma unroll
+    for (int k = 0; k < NS_GRAD_PER_PATCH; k++)
+      if (g[k] != 0.0) atomicAdd(o + k, g[k]);
+  }
+}
+
 }  // namespace nsg

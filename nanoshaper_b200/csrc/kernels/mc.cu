@@ -404,12 +404,29 @@ __global__ void k_mc_tris(MCArgs A, int emit) {
 }
 
 // One thread per analytic vertex: d area / d patch parameters += (d area / d s) * ds / d theta.
+// Consecutive vertices (along a ray, and of neighbouring rays) mostly lie on the same patch, so the
+// per-patch sums go through warp_add_grad.
 __global__ void k_grad_vert(MCArgs A) {
-  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < A.n_analytic; v += (int64_t)gridDim.x * blockDim.x) {
-    const double gv = A.vgrad[v];
-    if (gv == 0.0) continue;
-    const double x[3] = {A.vpos[3 * v], A.vpos[3 * v + 1], A.vpos[3 * v + 2]};
-    add_hit_grad(A.f64, A.i32, A.probe, A.vpid[v], x, A.vkey[v].w, gv, A.garea);
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < A.n_analytic; base += stride) {
+    const int64_t v = base + (threadIdx.x & 31);
+    double g[NS_GRAD_PER_PATCH];
+    int32_t pid = -1;
+    const double gv = v < A.n_analytic ? A.vgrad[v] : 0.0;
+    if (gv != 0.0) {
+      const double x[3] = {A.vpos[3 * v], A.vpos[3 * v + 1], A.vpos[3 * v + 2]};
+      pid = A.vpid[v];
+      if (hit_grad(A.f64 + (int64_t)NS_PATCH_F64 * pid, A.i32[NS_PATCH_I32 * pid], A.probe, x, A.vkey[v].w, g)) {
+#pragma unroll
+        for (int k = 0; k < NS_GRAD_PER_PATCH; k++) g[k] *= gv;
+      } else {
+        pid = -1;
+      }
+    }
+    if (pid < 0)
+#pragma unroll
+      for (int k = 0; k < NS_GRAD_PER_PATCH; k++) g[k] = 0.0;
+    warp_add_grad(pid, g, A.garea);
   }
 }
 

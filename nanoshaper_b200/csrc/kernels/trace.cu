@@ -309,11 +309,13 @@ __device__ __forceinline__ int make_pairs(double* col, int stride, int nh, doubl
         if (pcol) {
           p1 = pcol[q * stride];
           p2 = pcol[(q + 1) * stride];
-          double x[3] = {gc->x[0], gc->x[1], gc->x[2]};
-          x[gc->vc] = lim1;
-          add_hit_grad(gc->f64, gc->i32, gc->probe, pid_of(p1), x, gc->vc, -gc->w, gc->gvol);
-          x[gc->vc] = lim2;
-          add_hit_grad(gc->f64, gc->i32, gc->probe, pid_of(p2), x, gc->vc, gc->w, gc->gvol);
+          if (gc) {
+            double x[3] = {gc->x[0], gc->x[1], gc->x[2]};
+            x[gc->vc] = lim1;
+            add_hit_grad(gc->f64, gc->i32, gc->probe, pid_of(p1), x, gc->vc, -gc->w, gc->gvol);
+            x[gc->vc] = lim2;
+            add_hit_grad(gc->f64, gc->i32, gc->probe, pid_of(p2), x, gc->vc, gc->w, gc->gvol);
+          }
         }
         if (vertex_pairs) {
           int64_t a = (int64_t)rintp((lim1 - vmin) * scale);
@@ -621,18 +623,47 @@ __global__ void __launch_bounds__(kTraceThreads) k_fill(TraceCtx C, HitStore hs)
   int np = 0;
   const auto slot_pid = [&](uint8_t sl) { return hs.pid[(int64_t)sl * hs.nrays + rid]; };
   if (kGrad) {
-    GradCtx gc;
-    gc.f64 = C.P.f64;
-    gc.i32 = C.P.i32;
-    gc.probe = C.P.probe;
-    gc.w = S.A * C.out.grad_scale;
-    gc.x[rs.fd] = gcoord(g, rs.fd, valid ? m : 0) + rs.delta;
-    gc.x[rs.ld] = gcoord(g, rs.ld, valid ? n : 0) + rs.delta;
-    gc.x[rs.vc] = 0.0;
-    gc.vc = rs.vc;
-    gc.gvol = C.out.gvol;
+    // d volume / d patch parameters, interval end by interval end (the pairing rule of
+    // make_pairs), summed over runs of lanes on the same patch before the atomics
+    const double W = S.A * C.out.grad_scale;
+    double xb[3];
+    xb[rs.fd] = gcoord(g, rs.fd, valid ? m : 0) + rs.delta;
+    xb[rs.ld] = gcoord(g, rs.ld, valid ? n : 0) + rs.delta;
+    xb[rs.vc] = 0.0;
+    const int nhw = (valid && !ovf && nh > 0 && (nh & 1) == 0) ? nh : 0;
+    const int maxn = (int)__reduce_max_sync(0xffffffffu, (unsigned)nhw);
+    for (int q = 0; q < maxn; q += 2) {
+      bool ok = q + 1 < nhw;
+      double t1 = 0.0, t2 = 0.0;
+      if (ok) {
+        t1 = col[q * kThreads];
+        t2 = col[(q + 1) * kThreads];
+        ok = fabs(t2 - t1) >= NS_EPS_INT;
+      }
+      for (int e = 0; e < 2; e++) {
+        double gk[NS_GRAD_PER_PATCH];
+        int32_t pid = -1;
+        if (ok) {
+          pid = slot_pid(pcol[(q + e) * kThreads]);
+          double x[3] = {xb[0], xb[1], xb[2]};
+          x[rs.vc] = pa_vc + dirl * (e ? t2 : t1);
+          if (hit_grad(C.P.f64 + (int64_t)NS_PATCH_F64 * pid, C.P.i32[NS_PATCH_I32 * pid], C.P.probe, x, rs.vc, gk)) {
+            const double w = e ? W : -W;
+#pragma unroll
+            for (int k = 0; k < NS_GRAD_PER_PATCH; k++) gk[k] *= w;
+          } else {
+            pid = -1;
+          }
+        }
+        if (pid < 0)
+#pragma unroll
+          for (int k = 0; k < NS_GRAD_PER_PATCH; k++) gk[k] = 0.0;
+        warp_add_grad(pid, gk, C.out.gvol);
+      }
+    }
     if (valid && !ovf)
-      np = make_pairs(col, kThreads, nh, pa_vc, dirl, g.mn[rs.vc], g.scale, mc, &vol, pcol, &gc, slot_pid);
+      np = make_pairs(col, kThreads, nh, pa_vc, dirl, g.mn[rs.vc], g.scale, mc, &vol, pcol, (GradCtx*)nullptr,
+                      slot_pid);
   } else {
     if (valid && !ovf) np = make_pairs(col, kThreads, nh, pa_vc, dirl, g.mn[rs.vc], g.scale, mc, &vol);
   }
