@@ -1122,13 +1122,6 @@ int nsg_triangulate(nsg_ctx* c, double* area_out, int64_t* nverts, int64_t* ntri
   M.tri_cnt = c->tri_cnt.as<int32_t>();
   CK(c->cube_vl.ensure(std::max<int64_t>(n_act, 1) * 12 * sizeof(int32_t)));
   M.cube_vl = c->cube_vl.as<int32_t>();
-  LAUNCH(nsg::launch_mc_tris(M, 0, c->stream));
-  int64_t n_tri = 0;
-  rc = scan_counts(c, c->tri_cnt.as<int32_t>(), n_act, c->tri_off.as<int64_t>(), &n_tri);
-  if (rc) return rc;
-  CK(c->tris.ensure(std::max<int64_t>(n_tri, 1) * 3 * sizeof(int32_t)));
-  M.tri_off = c->tri_off.as<int64_t>();
-  M.tris = c->tris.as<int32_t>();
   M.cube_area = c->cube_area.as<double>();
   if (grad) {
     const nsg::PatchDev P = patch_dev(c);
@@ -1143,6 +1136,13 @@ int nsg_triangulate(nsg_ctx* c, double* area_out, int64_t* nverts, int64_t* ntri
     M.i32 = P.i32;
     M.probe = P.probe;
   }
+  LAUNCH(nsg::launch_mc_tris(M, 0, c->stream));
+  int64_t n_tri = 0;
+  rc = scan_counts(c, c->tri_cnt.as<int32_t>(), n_act, c->tri_off.as<int64_t>(), &n_tri);
+  if (rc) return rc;
+  CK(c->tris.ensure(std::max<int64_t>(n_tri, 1) * 3 * sizeof(int32_t)));
+  M.tri_off = c->tri_off.as<int64_t>();
+  M.tris = c->tris.as<int32_t>();
   LAUNCH(nsg::launch_mc_tris(M, 1, c->stream));
   if (grad) LAUNCH(nsg::launch_grad_vert(M, c->stream));
   c->have_garea = grad;

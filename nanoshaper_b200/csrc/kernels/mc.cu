@@ -331,7 +331,9 @@ __device__ __forceinline__ double vdist(const double* a, const double* b) {
   return sqrt((a[0] - b[0]) * (a[0] - b[0]) + (a[1] - b[1]) * (a[1] - b[1]) + (a[2] - b[2]) * (a[2] - b[2]));
 }
 
-// One thread per active cube; pass 0 counts triangles, pass 1 writes them and their areas.
+// One thread per active cube.  Pass 0 finds the vertex of every cut edge, counts the triangles
+// and sums their areas (and, in gradient mode, their derivatives with respect to the analytic
+// vertices); pass 1 writes the triangles at their offsets from the stored vertex ids.
 __global__ void k_mc_tris(MCArgs A, int emit) {
   __shared__ int8_t s_tri[256][16];
   __shared__ uint16_t s_emask[256];
@@ -362,6 +364,10 @@ __global__ void k_mc_tris(MCArgs A, int emit) {
       int32_t v0 = vl[s_tri[c][q]], v1 = vl[s_tri[c][q + 1]], v2 = vl[s_tri[c][q + 2]];
       if (v0 < 0 || v1 < 0 || v2 < 0) continue;
       if (emit) {
+        A.tris[3 * (o + cnt) + 0] = (int32_t)v2;
+        A.tris[3 * (o + cnt) + 1] = (int32_t)v1;
+        A.tris[3 * (o + cnt) + 2] = (int32_t)v0;
+      } else {
         const double* P0 = A.vpos + 3 * (int64_t)v0;
         const double* P1 = A.vpos + 3 * (int64_t)v1;
         const double* P2 = A.vpos + 3 * (int64_t)v2;
@@ -392,14 +398,13 @@ __global__ void k_mc_tris(MCArgs A, int emit) {
             }
           }
         }
-        A.tris[3 * (o + cnt) + 0] = (int32_t)v2;
-        A.tris[3 * (o + cnt) + 1] = (int32_t)v1;
-        A.tris[3 * (o + cnt) + 2] = (int32_t)v0;
       }
       cnt++;
     }
-    if (!emit) A.tri_cnt[a] = cnt;
-    else A.cube_area[a] = area;
+    if (!emit) {
+      A.tri_cnt[a] = cnt;
+      A.cube_area[a] = area;
+    }
   }
 }
 
