@@ -272,7 +272,8 @@ def run_ensemble(args, world: int, rank: int, local: int) -> None:
     nstruct = len(surfs)
     prec = 0 if args.precision == "fp64" else 1
     batch = nb.SurfaceBatch(surfs, device=local, precision=args.precision)
-    batch.upload()
+    # launch shapes of the tracer for this batch and precision (untimed; uploads the batch)
+    tuning, tune_ms = batch.autotune(grad=True, reps=1)
     ctx = batch._context().handle
     atom_off, atoms_cat, patch_atoms = batch.packed_atoms()
     N.check(L.nsg_upload_atoms(ctx, N.ptr(atom_off), N.ptr(atoms_cat), N.ptr(patch_atoms)), "upload atoms")
@@ -467,6 +468,8 @@ def run_ensemble(args, world: int, rank: int, local: int) -> None:
                        "atoms_total": int(sum(len(a) for a in atoms)), "probe": w["probe"], "scale": w["scale"],
                        "perfil": w["perfil"], "rays_per_step": rays, "nodes_per_step": nodes,
                        "outputs": "volume, area, d volume / d atoms, d area / d atoms per structure",
+                       "tuning": {"isect_threads": tuning[0], "isect_blocks_per_sm": tuning[1],
+                                  "cand_threads": tuning[2], "raycast_ms": tune_ms},
                        "l2": "inputs larger than L2 (hit store %.1f GB, bit grids %.2f GB)" % (
                            hit_store_gb, nwords * 4 / 1e9),
                        "parallelism": f"replicas x{world}"},

@@ -135,6 +135,14 @@ int nsg_upload_batch(nsg_ctx* ctx, const int64_t* patch_off, const double* f64, 
 /* Per-structure volume (last nsg_raycast) and area (last nsg_triangulate); either may be NULL. */
 int nsg_batch_results(nsg_ctx* ctx, double* volumes, double* areas);
 
+/* ---- launch-shape tuning (no counterpart in the reference) ----
+ * params: [intersection threads per block (64..256), intersection blocks per SM (1..64),
+ * candidate-kernel threads per block (32..1024)].  nsg_autotune times `reps` ray casts of the
+ * current batch per candidate shape and keeps the fastest in the context. */
+int nsg_set_tuning(nsg_ctx* ctx, const int32_t* params, int n);
+int nsg_get_tuning(nsg_ctx* ctx, int32_t* params, int n);
+int nsg_autotune(nsg_ctx* ctx, int flags, int precision, int reps, double* best_ms);
+
 /* ---- adjoint (no counterpart in the reference) ----
  * After nsg_raycast with NSG_RAYCAST_GRAD (and the nsg_triangulate that follows it): the
  * derivatives of the volume and of the area with respect to every patch's surface parameters,

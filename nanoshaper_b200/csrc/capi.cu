@@ -126,6 +126,7 @@ struct nsg_ctx {
   std::vector<int32_t> cav_filled;
   // mesh
   DevBuf cube_vl;
+  nsg::TuneParams tune;
   DevBuf surv_cnt, surv_off, vpos, vkey, row_act_cnt, row_mid_cnt, row_act_off, row_mid_off, act_rec, act_mid,
       tri_cnt, tri_off, tris, cube_area, red_out;
   int64_t n_vert = 0, n_analytic = 0, n_tri = 0, n_active = 0;
@@ -662,6 +663,72 @@ int nsg_patch_grads(nsg_ctx* c, double* gvol, double* garea) {
   return NSG_OK;
 }
 
+int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume);
+
+// Launch shapes of the tracer: [isect threads per block, isect blocks per SM, candidate threads
+// per block].
+int nsg_set_tuning(nsg_ctx* c, const int32_t* params, int n) {
+  if (!c || !params || n < 3) return NSG_ERR_ARG;
+  const int it = params[0], bpsm = params[1], ct = params[2];
+  if (it < 64 || it > 256 || it % 32 || bpsm < 1 || bpsm > 64 || ct < 32 || ct > 1024 || ct % 32)
+    return fail(NSG_ERR_ARG, "tuning parameters out of range");
+  c->tune.isect_threads = it;
+  c->tune.isect_bpsm = bpsm;
+  c->tune.cand_threads = ct;
+  return NSG_OK;
+}
+
+int nsg_get_tuning(nsg_ctx* c, int32_t* params, int n) {
+  if (!c || !params || n < 3) return NSG_ERR_ARG;
+  params[0] = c->tune.isect_threads;
+  params[1] = c->tune.isect_bpsm;
+  params[2] = c->tune.cand_threads;
+  return NSG_OK;
+}
+
+// Picks the tracer's launch shapes for the current batch and precision: every candidate shape
+// runs `reps` timed ray casts (after one untimed) and the fastest is kept in the context.
+// best_ms (optional) receives its time per ray cast.
+int nsg_autotune(nsg_ctx* c, int flags, int precision, int reps, double* best_ms) {
+  if (!c || reps < 1) return NSG_ERR_ARG;
+  static const int kThreads[] = {128, 256};
+  static const int kBpsm[] = {4, 8, 16, 32};
+  static const int kCand[] = {128, 256};
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  nsg::TuneParams best = c->tune;
+  double best_t = 1e300;
+  int rc = NSG_OK;
+  for (int it : kThreads)
+    for (int bp : kBpsm)
+      for (int ct : kCand) {
+        c->tune.isect_threads = it;
+        c->tune.isect_bpsm = bp;
+        c->tune.cand_threads = ct;
+        double v = 0;
+        rc = nsg_raycast(c, flags, precision, &v);
+        if (rc) break;
+        cudaEventRecord(e0, c->stream);
+        for (int r = 0; r < reps && !rc; r++) rc = nsg_raycast(c, flags, precision, &v);
+        cudaEventRecord(e1, c->stream);
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (rc) break;
+        if (ms / reps < best_t) {
+          best_t = ms / reps;
+          best = c->tune;
+        }
+      }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c->tune = best;
+  if (rc) return rc;
+  if (best_ms) *best_ms = best_t;
+  return NSG_OK;
+}
+
 // Per-structure volume and area of the last ray cast / triangulation of the batch.
 int nsg_batch_results(nsg_ctx* c, double* volumes, double* areas) {
   if (!c || c->nstruct < 1) return NSG_ERR_ARG;
@@ -826,7 +893,7 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
       nsg::HitStore hs{c->hit_t.as<double>(), c->hit_cnt.as<int32_t>(), nr, grad ? c->hit_pid.as<int32_t>() : nullptr};
       CK(cudaMemsetAsync(c->hit_cnt.p, 0, nr * sizeof(int32_t), c->stream));
       c->launches += precision == NSG_PRECISION_MIXED ? 6 : 4;
-      CK(nsg::launch_trace(P, B, s, c->tiles_tot[panel], o, co, hs, precision, c->stream));
+      CK(nsg::launch_trace(P, B, s, c->tiles_tot[panel], o, co, hs, precision, c->tune, c->stream));
     }
     stage_end(c, kStageTrace);
     int32_t novf[4] = {0, 0, 0, 0};

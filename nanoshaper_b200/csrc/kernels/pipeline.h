@@ -169,6 +169,13 @@ struct PatchDev {
   const int32_t* win;  // 6 per patch: start x,y,z, end x,y,z; start = -1 when culled
 };
 
+// Launch shapes of the tracer, picked per context by nsg_autotune (defaults below).
+struct TuneParams {
+  int isect_threads = 256;  // threads per block of the intersection kernels (64..256)
+  int isect_bpsm = 16;      // their blocks per SM (grid = 148 * isect_bpsm, grid-stride)
+  int cand_threads = 256;   // threads per block of the candidate kernel (one warp per patch)
+};
+
 // trace.cu: every launch covers all structures of the batch; `set` is the ray set (0..3) and
 // tile and ray indices are batch-wide.
 cudaError_t launch_windows(const PatchDev& P, int32_t* win, const BatchDev& B, cudaStream_t s);
@@ -180,7 +187,7 @@ cudaError_t launch_bin_count(const PatchDev& P, const BatchDev& B, int set, int3
 cudaError_t launch_bin_fill(const PatchDev& P, const BatchDev& B, int set, const int64_t* tile_off,
                             int32_t* tile_cursor, int32_t* tile_list, cudaStream_t s);
 cudaError_t launch_trace(const PatchDev& P, const BatchDev& B, int set, int64_t ntiles, const TraceOut& out,
-                         const CandOut& co, const HitStore& hs, int precision, cudaStream_t s);
+                         const CandOut& co, const HitStore& hs, int precision, const TuneParams& tp, cudaStream_t s);
 // pscratch: patch column of the overflow hits (gradient mode), else null.
 cudaError_t launch_trace_overflow(const PatchDev& P, const BatchDev& B, int set, const int64_t* tile_off,
                                   const int32_t* tile_list, const TraceOut& out, int n_ovf, double* scratch,

@@ -530,18 +530,19 @@ __global__ void __launch_bounds__(256) k_isect(TraceCtx C, CandOut co, HitStore 
 }
 
 template <int PN>
-void launch_isect(const TraceCtx& C, const CandOut& co, const HitStore& hs, int precision, cudaStream_t s) {
-  const int ig = 148 * 16;
+void launch_isect(const TraceCtx& C, const CandOut& co, const HitStore& hs, int precision, const TuneParams& tp,
+                  cudaStream_t s) {
+  const int ig = 148 * tp.isect_bpsm, it = tp.isect_threads;
   if (precision == 1) {
-    k_isect<PN, false, true><<<ig, 256, 0, s>>>(C, co, hs);
-    k_isect<PN, true, true><<<ig, 256, 0, s>>>(C, co, hs);
-    // the deferred candidates, in double precision
+    k_isect<PN, false, true><<<ig, it, 0, s>>>(C, co, hs);
+    k_isect<PN, true, true><<<ig, it, 0, s>>>(C, co, hs);
+    // the deferred candidates, in double precision (few: a small grid)
     const CandOut dco{co.dsph, co.dtor, co.dcap, co.dcount, nullptr, nullptr, 0, nullptr};
-    k_isect<PN, false, false><<<ig, 256, 0, s>>>(C, dco, hs);
-    k_isect<PN, true, false><<<ig, 256, 0, s>>>(C, dco, hs);
+    k_isect<PN, false, false><<<148, 256, 0, s>>>(C, dco, hs);
+    k_isect<PN, true, false><<<148, 256, 0, s>>>(C, dco, hs);
   } else {
-    k_isect<PN, false, false><<<ig, 256, 0, s>>>(C, co, hs);
-    k_isect<PN, true, false><<<ig, 256, 0, s>>>(C, co, hs);
+    k_isect<PN, false, false><<<ig, it, 0, s>>>(C, co, hs);
+    k_isect<PN, true, false><<<ig, it, 0, s>>>(C, co, hs);
   }
 }
 
@@ -946,18 +947,19 @@ cudaError_t launch_bin_fill(const PatchDev& P, const BatchDev& B, int set, const
 }
 
 cudaError_t launch_trace(const PatchDev& P, const BatchDev& B, int set, int64_t ntiles, const TraceOut& out,
-                         const CandOut& co, const HitStore& hs, int precision, cudaStream_t s) {
+                         const CandOut& co, const HitStore& hs, int precision, const TuneParams& tp, cudaStream_t s) {
   if (ntiles <= 0) return cudaSuccess;
   TraceCtx C{P, B, set, out};
   const int panel = set == 0 ? 0 : set - 1;
   if (P.n > 0) {
-    int64_t blocks = (P.n + 7) / 8;
+    const int wpb = tp.cand_threads / 32;
+    int64_t blocks = (P.n + wpb - 1) / wpb;
     if (blocks > 148 * 64) blocks = 148 * 64;
-    k_cand<<<(unsigned)blocks, 256, 0, s>>>(C, co);
+    k_cand<<<(unsigned)blocks, tp.cand_threads, 0, s>>>(C, co);
   }
-  if (panel == 0) launch_isect<0>(C, co, hs, precision, s);
-  else if (panel == 1) launch_isect<1>(C, co, hs, precision, s);
-  else launch_isect<2>(C, co, hs, precision, s);
+  if (panel == 0) launch_isect<0>(C, co, hs, precision, tp, s);
+  else if (panel == 1) launch_isect<1>(C, co, hs, precision, tp, s);
+  else launch_isect<2>(C, co, hs, precision, tp, s);
   if (out.gvol) k_fill<true><<<(unsigned)ntiles, kTraceThreads, 0, s>>>(C, hs);
   else k_fill<false><<<(unsigned)ntiles, kTraceThreads, 0, s>>>(C, hs);
   return cudaGetLastError();

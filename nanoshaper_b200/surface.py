@@ -561,6 +561,21 @@ class SurfaceBatch:
         N.check(N.lib().nsg_batch_results(c, None, N.ptr(self.areas)), "batch results")
         return self.areas
 
+    def autotune(self, grad: bool = False, reps: int = 2) -> tuple[list[int], float]:
+        """Picks the tracer's launch shapes (intersection block size and blocks per SM, candidate
+        block size) for this batch by timing ray casts; returns the shape and its ms per cast."""
+        self.upload()
+        c = self._context().handle
+        s0 = self.surfaces[0]
+        flags = (N.STATUS if s0.delphi.buildStatus else 0) | (N.ACCURATE_TRIANGULATION if s0.accurateTriangulation else 0)
+        if grad:
+            flags |= N.GRAD
+        ms = ctypes.c_double()
+        N.check(N.lib().nsg_autotune(c, flags, PRECISIONS[self.precision], reps, ctypes.byref(ms)), "autotune")
+        p = np.zeros(3, np.int32)
+        N.check(N.lib().nsg_get_tuning(c, N.ptr(p), 3), "get tuning")
+        return p.tolist(), ms.value
+
     def packed_atoms(self) -> tuple:
         """Concatenated atoms the patch sets were built from, their offsets and the patch atom map."""
         ps = [s.patches for s in self.surfaces]

@@ -83,3 +83,17 @@ def test_batch_gradients_match_single(native_lib):
         assert np.abs(gv - sv).max() <= 1e-10 * np.abs(sv).max(), f"structure {b}: volume gradient"
         assert np.abs(ga - sa).max() <= 1e-10 * np.abs(sa).max(), f"structure {b}: area gradient"
     batch.close()
+
+
+def test_autotune_keeps_results(native_lib):
+    """The autotuner only changes launch shapes: volumes and areas are unchanged."""
+    surfs = _structures(SPECS[:3])
+    batch = nb.SurfaceBatch(surfs, precision="mixed")
+    v0 = batch.getSurf().copy()
+    a0 = batch.triangulateSurface().copy()
+    shape, ms = batch.autotune(reps=1)
+    assert 64 <= shape[0] <= 256 and 1 <= shape[1] <= 64 and 32 <= shape[2] <= 1024 and ms > 0
+    v1 = batch.getSurf()
+    a1 = batch.triangulateSurface()
+    assert np.array_equal(v0, v1) and np.array_equal(a0, a1)
+    batch.close()
