@@ -100,7 +100,7 @@ struct nsg_ctx {
   DevBuf hit_pid, pair_pid, ovf_pscratch, gvol, garea, vpid, vgrad;
   // atoms behind the patches (for the device chain rule) and the atom derivatives
   std::vector<int64_t> patch_off{0, 0};
-  DevBuf d_atoms, d_patch_atoms, d_gatoms_vol, d_gatoms_area, d_bad;
+  DevBuf d_atoms, d_patch_atoms, d_gatoms_vol, d_gatoms_area, d_bad, d_patch_off, d_pool_off, d_atom_off;
   int64_t n_atoms = 0;
   bool have_atoms = false;
   bool grad_mode = false, have_gvol = false, have_garea = false;
@@ -453,6 +453,7 @@ int nsg_ctx_destroy(nsg_ctx* c) {
                     &c->ray_pair_off, &c->ray_pair_cnt, &c->cursors, &c->ovf_scratch, &c->err, &c->hits,
                     &c->hit_pid, &c->pair_pid, &c->ovf_pscratch, &c->gvol, &c->garea, &c->vpid, &c->vgrad,
                     &c->d_atoms, &c->d_patch_atoms, &c->d_gatoms_vol, &c->d_gatoms_area, &c->d_bad, &c->cube_vl,
+                    &c->d_patch_off, &c->d_pool_off, &c->d_atom_off,
                     &c->labels, &c->is_root, &c->sruns, &c->srun_off, &c->srun_cnt, &c->fr_cnt, &c->fr_off,
                     &c->fruns, &c->frow, &c->roots, &c->cc_count, &c->cc_desc, &c->cc_label_of,
                     &c->cc_fill_of, &c->nroots_d, &c->surv_cnt, &c->surv_off, &c->vpos, &c->vkey,
@@ -551,32 +552,37 @@ int nsg_upload_batch(nsg_ctx* c, const int64_t* patch_off, const double* f64, co
   const int64_t n = patch_off[nb], npool = pool_off[nb];
   if ((n > 0 && (!f64 || !i32)) || (npool > 0 && (!pool || !pool_flag))) return NSG_ERR_ARG;
   if (n >= (int64_t)1 << 31 || npool >= (int64_t)1 << 31) return fail(NSG_ERR_CAPACITY, "more than 2^31 patches");
-  std::vector<int32_t> gi32(i32, i32 + n * NS_PATCH_I32);
-  std::vector<int32_t> ps(std::max<int64_t>(n, 1), 0);
-  for (int32_t b = 0; b < nb; b++)
-    for (int64_t p = patch_off[b]; p < patch_off[b + 1]; p++) {
-      int32_t* r = gi32.data() + NS_PATCH_I32 * p;
-      if (r[1] < 0 || r[2] < 0 || r[1] + (int64_t)r[2] > pool_off[b + 1] - pool_off[b])
-        return fail(NSG_ERR_ARG, "patch pool range outside its structure's pool");
-      r[1] += (int32_t)pool_off[b];
-      ps[p] = b;
-    }
   CK(cudaSetDevice(c->device));
   CK(c->f64.ensure(std::max<int64_t>(n, 1) * NS_PATCH_F64 * sizeof(double)));
   CK(c->i32.ensure(std::max<int64_t>(n, 1) * NS_PATCH_I32 * sizeof(int32_t)));
   CK(c->pool.ensure(std::max<int64_t>(npool, 1) * 4 * sizeof(double)));
   CK(c->flag.ensure(std::max<int64_t>(npool, 1)));
+  CK(c->d_patch_struct.ensure(std::max<int64_t>(n, 1) * sizeof(int32_t)));
+  // straight copies of the caller's arrays (pinned buffers copy at full link speed); the pool
+  // indices are made batch-wide and the patch -> structure map is built on the device
   if (n) {
     CK(cudaMemcpyAsync(c->f64.p, f64, n * NS_PATCH_F64 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMemcpyAsync(c->i32.p, gi32.data(), n * NS_PATCH_I32 * sizeof(int32_t), cudaMemcpyHostToDevice,
-                       c->stream));
+    CK(cudaMemcpyAsync(c->i32.p, i32, n * NS_PATCH_I32 * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
   }
   if (npool) {
     CK(cudaMemcpyAsync(c->pool.p, pool, npool * 4 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(c->flag.p, pool_flag, npool, cudaMemcpyHostToDevice, c->stream));
   }
-  CK(upload_vec(c->d_patch_struct, ps, c->stream));
+  std::vector<int64_t> po(patch_off, patch_off + nb + 1), qo(pool_off, pool_off + nb + 1);
+  CK(upload_vec(c->d_patch_off, po, c->stream));
+  CK(upload_vec(c->d_pool_off, qo, c->stream));
+  CK(c->d_bad.ensure(sizeof(int32_t)));
+  CK(cudaMemsetAsync(c->d_bad.p, 0, sizeof(int32_t), c->stream));
+  LAUNCH(nsg::launch_batch_patches(n, c->d_patch_off.as<int64_t>(), nb, c->d_pool_off.as<int64_t>(),
+                                   c->i32.as<int32_t>(), c->d_patch_struct.as<int32_t>(), c->d_bad.as<int32_t>(),
+                                   c->stream));
+  int32_t bad = 0;
+  CK(cudaMemcpyAsync(&bad, c->d_bad.p, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  if (bad) {
+    c->has_patches = false;
+    return fail(NSG_ERR_ARG, "patch pool range outside its structure's pool");
+  }
   c->ext_f64 = nullptr; c->ext_i32 = nullptr; c->ext_pool = nullptr; c->ext_flag = nullptr;
   int rc = upload_common(c, n, npool, probe);
   if (rc) return rc;
@@ -595,24 +601,29 @@ int nsg_upload_atoms(nsg_ctx* c, const int64_t* atom_off, const double* atoms_xy
     return fail(NSG_ERR_STATE, "patches of the current batch must be uploaded first");
   const int32_t nb = c->nstruct;
   if (atom_off[0] != 0) return fail(NSG_ERR_ARG, "atom offsets must start at 0");
-  std::vector<int32_t> g(std::max<int64_t>(3 * c->np, 1));
-  for (int32_t b = 0; b < nb; b++) {
-    const int64_t na = atom_off[b + 1] - atom_off[b];
-    if (na < 0) return fail(NSG_ERR_ARG, "atom offsets must be non-decreasing");
-    for (int64_t p = c->patch_off[b]; p < c->patch_off[b + 1]; p++)
-      for (int q = 0; q < 3; q++) {
-        const int32_t a = patch_atoms[3 * p + q];
-        if (a >= na) return fail(NSG_ERR_ARG, "patch atom index outside its structure");
-        g[3 * p + q] = a < 0 ? -1 : (int32_t)(a + atom_off[b]);
-      }
-  }
+  for (int32_t b = 0; b < nb; b++)
+    if (atom_off[b + 1] < atom_off[b]) return fail(NSG_ERR_ARG, "atom offsets must be non-decreasing");
   const int64_t n = atom_off[nb];
   if (n >= ((int64_t)1 << 31)) return fail(NSG_ERR_CAPACITY, "more than 2^31 atoms");
   CK(cudaSetDevice(c->device));
+  int rc = ensure_patch_struct(c);
+  if (rc) return rc;
   CK(c->d_atoms.ensure(std::max<int64_t>(n, 1) * 4 * sizeof(double)));
+  CK(c->d_patch_atoms.ensure(std::max<int64_t>(3 * c->np, 1) * sizeof(int32_t)));
   if (n) CK(cudaMemcpyAsync(c->d_atoms.p, atoms_xyzr, n * 4 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  CK(upload_vec(c->d_patch_atoms, g, c->stream));
+  if (c->np)
+    CK(cudaMemcpyAsync(c->d_patch_atoms.p, patch_atoms, 3 * c->np * sizeof(int32_t), cudaMemcpyHostToDevice,
+                       c->stream));
+  std::vector<int64_t> ao(atom_off, atom_off + nb + 1);
+  CK(upload_vec(c->d_atom_off, ao, c->stream));
+  CK(c->d_bad.ensure(sizeof(int32_t)));
+  CK(cudaMemsetAsync(c->d_bad.p, 0, sizeof(int32_t), c->stream));
+  LAUNCH(nsg::launch_batch_atoms(c->np, c->d_patch_struct.as<int32_t>(), c->d_atom_off.as<int64_t>(),
+                                 c->d_patch_atoms.as<int32_t>(), c->d_bad.as<int32_t>(), c->stream));
+  int32_t bad = 0;
+  CK(cudaMemcpyAsync(&bad, c->d_bad.p, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  if (bad) return fail(NSG_ERR_ARG, "patch atom index outside its structure");
   c->n_atoms = n;
   c->have_atoms = true;
   return NSG_OK;

@@ -198,6 +198,14 @@ cudaError_t launch_trace_overflow(const PatchDev& P, const BatchDev& B, int set,
 cudaError_t launch_segment_sums(const double* v, const int64_t* base, const int64_t* idx, int n, double* out,
                                 bool accumulate, cudaStream_t s);
 
+// reduce.cu, batch uploads: per-patch structure and batch-wide pool index (err set on a pool
+// range outside the structure's pool); batch-wide patch atom indices (err on an index outside
+// the structure's atoms).
+cudaError_t launch_batch_patches(int64_t np, const int64_t* patch_off, int n, const int64_t* pool_off, int32_t* i32,
+                                 int32_t* patch_struct, int32_t* err, cudaStream_t s);
+cudaError_t launch_batch_atoms(int64_t np, const int32_t* patch_struct, const int64_t* atom_off, int32_t* patch_atoms,
+                               int32_t* err, cudaStream_t s);
+
 // chain.cu: atom derivatives (x, y, z, r per atom; atomics) of volume and area from the per-patch
 // parameter derivatives; patch_atoms are batch-wide atom indices; n_bad counts singular facets.
 cudaError_t launch_chain(int64_t np, const int32_t* i32, const double* f64, const int32_t* patch_atoms,

@@ -38,3 +38,59 @@ cudaError_t launch_segment_sums(const double* v, const int64_t* base, const int6
 }
 
 }  // namespace nsg
+
+namespace nsg {
+
+namespace {
+
+// Batch upload fix-ups, one thread per patch: the structure of the patch (binary search in the
+// patch offsets), its pool index made batch-wide, and the range checked against its structure's
+// pool; its three atom indices made batch-wide and checked against its structure's atoms.
+__global__ void k_batch_patches(int64_t np, const int64_t* __restrict__ patch_off, int n,
+                                const int64_t* __restrict__ pool_off, int32_t* i32, int32_t* patch_struct,
+                                int32_t* err) {
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < np; p += (int64_t)gridDim.x * blockDim.x) {
+    const int b = find_struct(patch_off, n, p);
+    int32_t* r = i32 + NS_PATCH_I32 * p;
+    const int64_t first = r[1], cnt = r[2];
+    if (first < 0 || cnt < 0 || first + cnt > pool_off[b + 1] - pool_off[b]) atomicExch(err, 1);
+    r[1] = (int32_t)(first + pool_off[b]);
+    patch_struct[p] = b;
+  }
+}
+
+__global__ void k_batch_atoms(int64_t np, const int32_t* __restrict__ patch_struct,
+                              const int64_t* __restrict__ atom_off, int32_t* patch_atoms, int32_t* err) {
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < np; p += (int64_t)gridDim.x * blockDim.x) {
+    const int b = patch_struct[p];
+    const int64_t base = atom_off[b], na = atom_off[b + 1] - base;
+    for (int q = 0; q < 3; q++) {
+      const int64_t a = patch_atoms[3 * p + q];
+      if (a >= na) atomicExch(err, 1);
+      patch_atoms[3 * p + q] = a < 0 ? -1 : (int32_t)(a + base);
+    }
+  }
+}
+
+int grid_of(int64_t n) {
+  int64_t b = (n + 255) / 256;
+  return (int)(b < 1 ? 1 : (b > 148 * 32 ? 148 * 32 : b));
+}
+
+}  // namespace
+
+cudaError_t launch_batch_patches(int64_t np, const int64_t* patch_off, int n, const int64_t* pool_off, int32_t* i32,
+                                 int32_t* patch_struct, int32_t* err, cudaStream_t s) {
+  if (np <= 0) return cudaSuccess;
+  k_batch_patches<<<grid_of(np), 256, 0, s>>>(np, patch_off, n, pool_off, i32, patch_struct, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_atoms(int64_t np, const int32_t* patch_struct, const int64_t* atom_off, int32_t* patch_atoms,
+                               int32_t* err, cudaStream_t s) {
+  if (np <= 0) return cudaSuccess;
+  k_batch_atoms<<<grid_of(np), 256, 0, s>>>(np, patch_struct, atom_off, patch_atoms, err);
+  return cudaGetLastError();
+}
+
+}  // namespace nsg
