@@ -201,27 +201,34 @@ def rays_of(g) -> int:
 
 
 def ensemble_cpu_baseline(surfs, threads: int, target_s: float = 10.0, steps: int = 1) -> dict:
-    """Oracle ray casting on a central slab of the first structure, all host threads; structures/s
-    scaled by the ensemble's mean rays per structure."""
+    """Oracle ray casting (all four ray sets, whole structures, all host threads) of a sample of the
+    ensemble: structures in a seeded random order until about target_s seconds; structures/s =
+    sample rays/s / the ensemble's mean rays per structure."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as O
     O.build()
-    s0 = surfs[0]
-    g = s0.delphi.grid
-    t_probe, r_probe = O.time_slab(g, s0.patches, threads, 0.45, 0.55)
-    per_ray = t_probe / max(r_probe, 1)
-    frac = min(1.0, max(0.05, target_s / max(per_ray * rays_of(g), 1e-9)))
-    lo, hi = 0.5 - frac / 2, 0.5 + frac / 2
-    times, rays = [], 0
-    for _ in range(steps):
-        dt, rays = O.time_slab(g, s0.patches, threads, lo, hi)
-        times.append(dt)
-    t = max(statistics.median(times), 1e-9)
-    rays_per_s = rays / t
+    order = list(range(len(surfs)))
+    np.random.default_rng(0).shuffle(order)
+    rates, sample_idx, sample_rays = [], [], 0
+    for _ in range(max(steps, 1)):
+        t_tot, r_tot, idx = 0.0, 0, []
+        for b in order:
+            sf = surfs[b]
+            dt, r = O.time_slab(sf.delphi.grid, sf.patches, threads, 0.0, 1.0)
+            t_tot += dt
+            r_tot += r
+            idx.append(b)
+            if t_tot >= target_s:
+                break
+        rates.append(r_tot / max(t_tot, 1e-9))
+        sample_idx, sample_rays = idx, r_tot
+    rays_per_s = statistics.median(rates)
     mean_rays = statistics.mean(rays_of(sf.delphi.grid) for sf in surfs)
-    sample = (f"ray casting (status + 3 triangulation ray sets) of the slab [{lo:.3f}, {hi:.3f}) of structure 0 "
-              f"({len(s0.delphi.atoms)} atoms, grid {g.nx}x{g.ny}x{g.nz}): {rays} rays; structures/s = rays/s / "
-              f"mean rays per structure ({mean_rays:.0f}); marching cubes not included")
+    sizes = [len(surfs[b].delphi.atoms) for b in sample_idx]
+    sample = (f"ray casting (status + 3 triangulation ray sets) of {len(sample_idx)} whole structures drawn at random "
+              f"({min(sizes)}-{max(sizes)} atoms, {sample_rays} rays, about {target_s:.0f} s); "
+              f"structures/s = rays/s / mean rays per structure of the ensemble ({mean_rays:.0f}); marching cubes "
+              f"and gradients not included")
     return {"value": rays_per_s / mean_rays, "rays_per_s": rays_per_s, "cores": threads, "kind": "port",
             "sample": sample, "unit": "structures/s"}
 
