@@ -57,7 +57,13 @@ WORKLOADS = {
     "ses_327": dict(n=327, seed=1, probe=1.4, scale=2.0, perfil=70.0, cav_vol=10.0),
 }
 
-STAGES = ("bin", "trace", "overflow", "cavity", "vertex", "mc")
+STAGES = ("bin", "trace", "overflow", "cavity", "vertex", "mc", "cand", "isect", "fill")
+
+# Floating-point operations per candidate of the mixed-precision intersection kernels (adds, muls
+# and 2 per fused multiply-add, predicated-on thread instructions), measured with ncu
+# (smsp__sass_thread_inst_executed_op_{dadd,dmul,dfma,fadd,fmul,ffma}_pred_on.sum) on the
+# 64-structure conformer ensemble and divided by its candidate counts.
+FLOPS_PER_CANDIDATE = {"torus": {"fp64": 312.0, "fp32": 35.0}, "sphere": {"fp64": 26.0, "fp32": 74.0}}
 
 
 def load_peaks() -> dict:
@@ -322,9 +328,9 @@ def run_ensemble(args, world: int, rank: int, local: int) -> None:
     step(prec)
     N.check(L.nsg_profile(ctx, 1), "profile")
     step(prec)
-    stage_ms = np.zeros(8)
-    stage_calls = np.zeros(8, np.int64)
-    L.nsg_stage_times(ctx, stage_ms.ctypes.data, stage_calls.ctypes.data, 8)
+    stage_ms = np.zeros(12)
+    stage_calls = np.zeros(12, np.int64)
+    L.nsg_stage_times(ctx, stage_ms.ctypes.data, stage_calls.ctypes.data, 12)
     counters = np.zeros(8, np.int64)
     L.nsg_trace_counters(ctx, counters.ctypes.data, 8)
     N.check(L.nsg_profile(ctx, 0), "profile")
@@ -409,22 +415,32 @@ def run_ensemble(args, world: int, rank: int, local: int) -> None:
 
     peaks = load_peaks()
     stage_times = {STAGES[i]: float(stage_ms[i]) for i in range(len(STAGES))}
-    dominant = max(stage_times, key=stage_times.get)
-    alg_bytes = {
-        # bit grids cleared by three ray sets (read + write), per-ray interval sums, pair records
-        "trace": 3 * 2 * 4 * nwords + 8 * rays + 16 * nv,
-        "overflow": 8 * rays,
-        "bin": 6 * 4 * sum(sf.patches.n for sf in surfs),
-        "cavity": 0,
-        "vertex": 8 * 2 * nv + 40 * nv,
-        # bit rows read by both passes of the row classification, vertices, triangles
-        "mc": nwords * 4 * 8 + 40 * nv + 12 * nt,
-    }
-    dom_ms = stage_times[dominant] / max(int(stage_calls[STAGES.index(dominant)]), 1)
-    achieved = alg_bytes[dominant] / (dom_ms / 1000.0) / 1e9
-    roofline = {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                "frac": achieved / peaks["hbm_gbs"], "traffic": None, "peak_source": peaks["source"],
-                "stage_ms": stage_times, "algorithmic_bytes": alg_bytes[dominant]}
+    # The dominant kernels are the intersection kernels (the largest share of the trace stage),
+    # bound by FP64 arithmetic: achieved = operation model x candidates / their event-timed time,
+    # against the FP64 rate of this GPU measured live with FMA chains.
+    n_tor = int(counters[1])
+    n_sph = int(counters[0]) - n_tor
+    flops64 = n_tor * FLOPS_PER_CANDIDATE["torus"]["fp64"] + n_sph * FLOPS_PER_CANDIDATE["sphere"]["fp64"]
+    flops32 = n_tor * FLOPS_PER_CANDIDATE["torus"]["fp32"] + n_sph * FLOPS_PER_CANDIDATE["sphere"]["fp32"]
+    isect_s = stage_times["isect"] / 1000.0
+    pk64, pk32 = ctypes.c_double(), ctypes.c_double()
+    pctx = nb.Context(local)
+    N.check(L.nsg_fp_peak(pctx.handle, 0, ctypes.byref(pk64)), "fp64 peak")
+    N.check(L.nsg_fp_peak(pctx.handle, 1, ctypes.byref(pk32)), "fp32 peak")
+    pctx.close()
+    ach64 = flops64 / isect_s / 1e12 if isect_s > 0 else 0.0
+    ach32 = flops32 / isect_s / 1e12 if isect_s > 0 else 0.0
+    # the memory-side figure of the trace stage's fill kernel (bit grids, interval sums, pairs)
+    fill_bytes = 3 * 2 * 4 * nwords + 8 * rays + 16 * nv
+    roofline = {"bound": "fp64", "kernel": "k_isect (ray-patch intersection, 4 ray sets)", "achieved": ach64,
+                "peak": pk64.value / 1e12, "unit": "TFLOP/s", "frac": ach64 / (pk64.value / 1e12),
+                "traffic": None, "peak_source": "measured live: FMA chains on this GPU (nsg_fp_peak)",
+                "flops_per_step": {"fp64": flops64, "fp32": flops32},
+                "fp32": {"achieved": ach32, "peak": pk32.value / 1e12, "frac": ach32 / (pk32.value / 1e12)},
+                "hbm_fill": {"kernel": "k_fill", "achieved_gbs": fill_bytes / (stage_times["fill"] / 1000.0) / 1e9
+                             if stage_times["fill"] > 0 else 0.0, "peak_gbs": peaks["hbm_gbs"],
+                             "peak_source": peaks["source"]},
+                "stage_ms": stage_times}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -561,9 +577,9 @@ def main():
     step()
     N.check(L.nsg_profile(ctx, 1), "profile")
     step()
-    stage_ms = np.zeros(8)
-    stage_calls = np.zeros(8, np.int64)
-    L.nsg_stage_times(ctx, stage_ms.ctypes.data, stage_calls.ctypes.data, 8)
+    stage_ms = np.zeros(12)
+    stage_calls = np.zeros(12, np.int64)
+    L.nsg_stage_times(ctx, stage_ms.ctypes.data, stage_calls.ctypes.data, 12)
     counters = np.zeros(8, np.int64)
     L.nsg_trace_counters(ctx, counters.ctypes.data, 8)
     N.check(L.nsg_profile(ctx, 0), "profile")

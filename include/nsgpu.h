@@ -210,6 +210,8 @@ int64_t nsg_launch_count(nsg_ctx* ctx);
 /* Counters of the last profiled ray cast: candidates, torus candidates, mixed-precision fallbacks
  * (near-tangent sphere, quartic isolation, root polish), feasibility re-evaluations. */
 int nsg_trace_counters(nsg_ctx* ctx, int64_t* out, int n);
+/* Peak FP64 (precision 0) or FP32 (1) rate of the GPU, measured with FMA chains (flop/s). */
+int nsg_fp_peak(nsg_ctx* ctx, int precision, double* flops_per_s);
 
 #ifdef __cplusplus
 }

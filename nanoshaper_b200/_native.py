@@ -68,6 +68,7 @@ _SIGNATURES = {
     "nsg_set_tuning": ([_P, _P, _INT], _INT),
     "nsg_get_tuning": ([_P, _P, _INT], _INT),
     "nsg_autotune": ([_P, _INT, _INT, _INT, ctypes.POINTER(_D)], _INT),
+    "nsg_fp_peak": ([_P, _INT, ctypes.POINTER(_D)], _INT),
     "nsg_cavities": ([_P, _D, ctypes.POINTER(_INT)], _INT),
     "nsg_cavity_order": ([ctypes.c_int32, _P, _P], _INT),
     "nsg_triangulate": ([_P, ctypes.POINTER(_D), ctypes.POINTER(_I64), ctypes.POINTER(_I64)], _INT),

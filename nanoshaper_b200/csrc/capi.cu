@@ -136,9 +136,10 @@ struct nsg_ctx {
   // timing: user events and per-stage kernel times (milliseconds, summed over calls)
   cudaEvent_t user_ev[8] = {};
   bool profile = false;
-  cudaEvent_t st_ev[2 * 8] = {};
-  double stage_ms[8] = {};
-  int64_t stage_calls[8] = {};
+  cudaEvent_t st_ev[2 * 12] = {};
+  double stage_ms[12] = {};
+  int64_t stage_calls[12] = {};
+  cudaEvent_t sub_ev[4][4] = {};  // per ray set: before candidates, after candidates / intersections / fill
   int64_t launches = 0;
   DevBuf counters;
   unsigned long long counter_host[8] = {};
@@ -274,7 +275,7 @@ int ensure_patch_struct(nsg_ctx* c) {
 
 // Stage ids of the per-stage kernel timers.
 enum { kStageBin = 0, kStageTrace = 1, kStageOverflow = 2, kStageCavity = 3, kStageVertex = 4, kStageMC = 5,
-       kStageCount = 6 };
+       kStageCand = 6, kStageIsect = 7, kStageFill = 8, kStageCount = 9 };
 
 void stage_begin(nsg_ctx* c, int id) {
   if (!c->profile) return;
@@ -471,8 +472,11 @@ int nsg_ctx_destroy(nsg_ctx* c) {
   }
   for (int i = 0; i < 8; i++)
     if (c->user_ev[i]) cudaEventDestroy(c->user_ev[i]);
-  for (int i = 0; i < 16; i++)
+  for (int i = 0; i < 24; i++)
     if (c->st_ev[i]) cudaEventDestroy(c->st_ev[i]);
+  for (int i = 0; i < 4; i++)
+    for (int q = 0; q < 4; q++)
+      if (c->sub_ev[i][q]) cudaEventDestroy(c->sub_ev[i][q]);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return NSG_OK;
@@ -675,6 +679,37 @@ int nsg_patch_grads(nsg_ctx* c, double* gvol, double* garea) {
 }
 
 int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume);
+
+// Peak floating-point rate of this GPU measured live: independent fused multiply-add chains
+// (8 per thread, 148 x 8 blocks of 256 threads), 2 flops per FMA; precision 0 = FP64, 1 = FP32.
+int nsg_fp_peak(nsg_ctx* c, int precision, double* flops_per_s) {
+  if (!c || !flops_per_s || (precision != 0 && precision != 1)) return NSG_ERR_ARG;
+  CK(cudaSetDevice(c->device));
+  const int blocks = 148 * 8, threads = 256, iters = 4096;
+  CK(c->red_out.ensure(blocks * threads * sizeof(double)));
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  float best = 1e30f;
+  for (int rep = 0; rep < 4; rep++) {
+    cudaEventRecord(e0, c->stream);
+    cudaError_t e = nsg::launch_fma_peak(precision, blocks, threads, iters, c->red_out.p, c->stream);
+    cudaEventRecord(e1, c->stream);
+    if (e != cudaSuccess) {
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      return fail(NSG_ERR_CUDA, "fma peak", e);
+    }
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (rep > 0 && ms < best) best = ms;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *flops_per_s = 2.0 * 8.0 * (double)blocks * threads * iters / (best * 1e-3);
+  return NSG_OK;
+}
 
 // Launch shapes of the tracer: [isect threads per block, isect blocks per SM, candidate threads
 // per block].
@@ -904,9 +939,27 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
       nsg::HitStore hs{c->hit_t.as<double>(), c->hit_cnt.as<int32_t>(), nr, grad ? c->hit_pid.as<int32_t>() : nullptr};
       CK(cudaMemsetAsync(c->hit_cnt.p, 0, nr * sizeof(int32_t), c->stream));
       c->launches += precision == NSG_PRECISION_MIXED ? 6 : 4;
-      CK(nsg::launch_trace(P, B, s, c->tiles_tot[panel], o, co, hs, precision, c->tune, c->stream));
+      cudaEvent_t* ev = nullptr;
+      if (c->profile) {
+        for (int q = 0; q < 4; q++)
+          if (!c->sub_ev[s][q]) CK(cudaEventCreate(&c->sub_ev[s][q]));
+        ev = c->sub_ev[s];
+      }
+      CK(nsg::launch_trace(P, B, s, c->tiles_tot[panel], o, co, hs, precision, c->tune, c->stream, ev));
     }
     stage_end(c, kStageTrace);
+    if (c->profile) {
+      // candidate, intersection and fill kernels of every ray set (stage_end synchronised the stream)
+      for (int si = 0; si < nsets; si++) {
+        const int s = sets[si];
+        for (int q = 0; q < 3; q++) {
+          float ms = 0;
+          CK(cudaEventElapsedTime(&ms, c->sub_ev[s][q], c->sub_ev[s][q + 1]));
+          c->stage_ms[kStageCand + q] += ms;
+          c->stage_calls[kStageCand + q]++;
+        }
+      }
+    }
     int32_t novf[4] = {0, 0, 0, 0};
     CK(cudaMemcpyAsync(novf, ovf_count, 4 * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
@@ -1339,14 +1392,15 @@ int nsg_profile(nsg_ctx* c, int enable) {
   if (!c) return NSG_ERR_ARG;
   c->profile = enable != 0;
   if (c->profile)
-    for (int i = 0; i < 8; i++) { c->stage_ms[i] = 0; c->stage_calls[i] = 0; }
+    for (int i = 0; i < 12; i++) { c->stage_ms[i] = 0; c->stage_calls[i] = 0; }
   return NSG_OK;
 }
 
-// Accumulated per-stage milliseconds and call counts: bin, trace, overflow, cavity, vertex, mc.
+// Accumulated per-stage milliseconds and call counts: bin, trace, overflow, cavity, vertex, mc, and
+// within the trace the candidate, intersection and fill kernels.
 int nsg_stage_times(nsg_ctx* c, double* ms, int64_t* calls, int n) {
   if (!c) return NSG_ERR_ARG;
-  for (int i = 0; i < n && i < 8; i++) {
+  for (int i = 0; i < n && i < 12; i++) {
     if (ms) ms[i] = c->stage_ms[i];
     if (calls) calls[i] = c->stage_calls[i];
   }

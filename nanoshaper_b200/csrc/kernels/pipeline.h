@@ -186,8 +186,11 @@ cudaError_t launch_bin_count(const PatchDev& P, const BatchDev& B, int set, int3
                              unsigned long long* area, cudaStream_t s);
 cudaError_t launch_bin_fill(const PatchDev& P, const BatchDev& B, int set, const int64_t* tile_off,
                             int32_t* tile_cursor, int32_t* tile_list, cudaStream_t s);
+// ev (optional, profiling): 4 events recorded before the candidate kernel and after the candidate,
+// intersection and fill kernels.
 cudaError_t launch_trace(const PatchDev& P, const BatchDev& B, int set, int64_t ntiles, const TraceOut& out,
-                         const CandOut& co, const HitStore& hs, int precision, const TuneParams& tp, cudaStream_t s);
+                         const CandOut& co, const HitStore& hs, int precision, const TuneParams& tp, cudaStream_t s,
+                         cudaEvent_t* ev = nullptr);
 // pscratch: patch column of the overflow hits (gradient mode), else null.
 cudaError_t launch_trace_overflow(const PatchDev& P, const BatchDev& B, int set, const int64_t* tile_off,
                                   const int32_t* tile_list, const TraceOut& out, int n_ovf, double* scratch,
@@ -205,6 +208,10 @@ cudaError_t launch_batch_patches(int64_t np, const int64_t* patch_off, int n, co
                                  int32_t* patch_struct, int32_t* err, cudaStream_t s);
 cudaError_t launch_batch_atoms(int64_t np, const int32_t* patch_struct, const int64_t* atom_off, int32_t* patch_atoms,
                                int32_t* err, cudaStream_t s);
+
+// reduce.cu: FMA-chain kernel timing the FP64 (precision 0) or FP32 (1) peak; out holds
+// blocks * threads elements.
+cudaError_t launch_fma_peak(int precision, int blocks, int threads, int iters, void* out, cudaStream_t s);
 
 // chain.cu: atom derivatives (x, y, z, r per atom; atomics) of volume and area from the per-patch
 // parameter derivatives; patch_atoms are batch-wide atom indices; n_bad counts singular facets.

@@ -93,4 +93,31 @@ cudaError_t launch_batch_atoms(int64_t np, const int32_t* patch_struct, const in
   return cudaGetLastError();
 }
 
+namespace {
+
+// 8 independent FMA chains per thread; the result is stored so that nothing is optimised away.
+template <class T>
+__global__ void k_fma_peak(int iters, T* out) {
+  T a[8];
+  const T m = (T)0.999999, c = (T)1e-7;
+#pragma unroll
+  for (int q = 0; q < 8; q++) a[q] = (T)(threadIdx.x + q);
+  for (int i = 0; i < iters; i++) {
+#pragma unroll
+    for (int q = 0; q < 8; q++) a[q] = fma(a[q], m, c);
+  }
+  T s = 0;
+#pragma unroll
+  for (int q = 0; q < 8; q++) s += a[q];
+  out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+}  // namespace
+
+cudaError_t launch_fma_peak(int precision, int blocks, int threads, int iters, void* out, cudaStream_t s) {
+  if (precision == 0) k_fma_peak<double><<<blocks, threads, 0, s>>>(iters, (double*)out);
+  else k_fma_peak<float><<<blocks, threads, 0, s>>>(iters, (float*)out);
+  return cudaGetLastError();
+}
+
 }  // namespace nsg

@@ -947,21 +947,26 @@ cudaError_t launch_bin_fill(const PatchDev& P, const BatchDev& B, int set, const
 }
 
 cudaError_t launch_trace(const PatchDev& P, const BatchDev& B, int set, int64_t ntiles, const TraceOut& out,
-                         const CandOut& co, const HitStore& hs, int precision, const TuneParams& tp, cudaStream_t s) {
+                         const CandOut& co, const HitStore& hs, int precision, const TuneParams& tp, cudaStream_t s,
+                         cudaEvent_t* ev) {
   if (ntiles <= 0) return cudaSuccess;
   TraceCtx C{P, B, set, out};
   const int panel = set == 0 ? 0 : set - 1;
+  if (ev) cudaEventRecord(ev[0], s);
   if (P.n > 0) {
     const int wpb = tp.cand_threads / 32;
     int64_t blocks = (P.n + wpb - 1) / wpb;
     if (blocks > 148 * 64) blocks = 148 * 64;
     k_cand<<<(unsigned)blocks, tp.cand_threads, 0, s>>>(C, co);
   }
+  if (ev) cudaEventRecord(ev[1], s);
   if (panel == 0) launch_isect<0>(C, co, hs, precision, tp, s);
   else if (panel == 1) launch_isect<1>(C, co, hs, precision, tp, s);
   else launch_isect<2>(C, co, hs, precision, tp, s);
+  if (ev) cudaEventRecord(ev[2], s);
   if (out.gvol) k_fill<true><<<(unsigned)ntiles, kTraceThreads, 0, s>>>(C, hs);
   else k_fill<false><<<(unsigned)ntiles, kTraceThreads, 0, s>>>(C, hs);
+  if (ev) cudaEventRecord(ev[3], s);
   return cudaGetLastError();
 }
 
