@@ -286,7 +286,12 @@ def run_ensemble(args, world: int, rank: int, local: int) -> None:
     prec = 0 if args.precision == "fp64" else 1
     batch = nb.SurfaceBatch(surfs, device=local, precision=args.precision)
     # launch shapes of the tracer for this batch and precision (untimed; uploads the batch)
-    tuning, tune_ms = batch.autotune(grad=True, reps=1)
+    if args.tuning:
+        tuning, tune_ms = [int(x) for x in args.tuning.split(",")], None
+        batch.upload()
+        batch.set_tuning(tuning)
+    else:
+        tuning, tune_ms = batch.autotune(grad=True, reps=1)
     ctx = batch._context().handle
     atom_off, atoms_cat, patch_atoms = batch.packed_atoms()
     N.check(L.nsg_upload_atoms(ctx, N.ptr(atom_off), N.ptr(atoms_cat), N.ptr(patch_atoms)), "upload atoms")
@@ -505,6 +510,9 @@ def main():
     ap.add_argument("--precision", default=None, choices=("fp64", "mixed"),
                     help="default: mixed for the ensembles, fp64 for single structures")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tuning", default=None,
+                    help="fixed tracer launch shapes 'isect_threads,isect_blocks_per_sm,cand_threads' "
+                         "instead of the autotuner (ensembles)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     if args.precision is None:

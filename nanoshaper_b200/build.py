@@ -2,7 +2,9 @@
 
 Device code is compiled with ``--fmad=false`` so that grid coordinates and the double-precision
 ray tests round exactly as the host restatement does; kernels that want fused multiply-adds
-request them explicitly.  Host code is compiled with ``-ffp-contract=off`` for the same reason.
+request them explicitly.  The one exception is ``kernels/trace_mixed.cu`` (the mixed-precision
+intersection kernels, held to a tolerance rather than to bit equality), compiled with
+``--fmad=true``.  Host code is compiled with ``-ffp-contract=off``.
 """
 from __future__ import annotations
 
@@ -18,7 +20,7 @@ LIB_DIR = PKG / "lib"
 BUILD_DIR = PKG / "_build"
 LIB = LIB_DIR / "libnsgpu.so"
 
-CU_SOURCES = ["capi.cu", "kernels/trace.cu", "kernels/cavity.cu", "kernels/mc.cu", "kernels/reduce.cu", "kernels/chain.cu", "noalloc.cu"]
+CU_SOURCES = ["capi.cu", "kernels/trace.cu", "kernels/trace_mixed.cu", "kernels/cavity.cu", "kernels/mc.cu", "kernels/reduce.cu", "kernels/chain.cu", "noalloc.cu"]
 CPP_SOURCES = ["host/grid.cpp", "host/ses_builder.cpp", "host/grad.cpp", "host/formats.cpp"]
 
 NVCC_FLAGS = [
@@ -26,6 +28,8 @@ NVCC_FLAGS = [
     "-O3", "-std=c++17", "-lineinfo", "--fmad=false",
     "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
 ]
+# Files whose device code may contract products and sums into fused multiply-adds (flag replaced).
+FMAD_FILES = {"kernels/trace_mixed.cu": {"--fmad=false": "--fmad=true"}}
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-Wall"]
 
 
@@ -62,7 +66,8 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         o = BUILD_DIR / (src.replace("/", "_") + ".o")
         objs.append(o)
         if force or _stale(o, [s] + headers):
-            cmd = [nvcc, *NVCC_FLAGS, "-I", str(CSRC), "-c", str(s), "-o", str(o)]
+            flags = [f for f in NVCC_FLAGS if f not in FMAD_FILES.get(src, {})] + list(FMAD_FILES.get(src, {}).values())
+            cmd = [nvcc, *flags, "-I", str(CSRC), "-c", str(s), "-o", str(o)]
             if verbose:
                 print(" ".join(cmd))
             _run(cmd)

@@ -17,13 +17,13 @@
 #include "ray_math.cuh"
 #include "ray_math_mixed.cuh"
 #include "grad.cuh"
+#include "isect.cuh"
 
 namespace nsg {
 
 namespace {
 
 
-__device__ __forceinline__ double gcoord(const GridDev& g, int d, int64_t i) { return g.mn[d] + (double)i * g.side; }
 
 __global__ void k_windows(PatchDev P, int32_t* win, BatchDev B) {
   int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -135,140 +135,6 @@ __device__ __forceinline__ int ray_patch_f64(const double* f, int kind, int firs
                                              double* t) {
   if (!candidate(f, rs, pa)) return 0;
   return intersect_f64(f, kind, first, cnt, P, rs, pa, dir, ray_dir, t);
-}
-
-// Axes of a panel as compile-time constants: pixel axes (fd, ld) and ray axis vc.
-template <int P>
-struct Ax {
-  static constexpr int fd = P == 0 ? 1 : 0;
-  static constexpr int ld = P == 1 ? 1 : 2;
-  static constexpr int vc = P == 0 ? 0 : (P == 1 ? 2 : 1);
-};
-
-template <int P>
-__device__ __forceinline__ bool candidate_p(const double* f, const double* pa) {
-  constexpr int fd = Ax<P>::fd, ld = Ax<P>::ld;
-  double r = f[kR];
-  if (pa[fd] < f[fd] - r || pa[fd] > f[fd] + r) return false;
-  if (pa[ld] < f[ld] - r || pa[ld] > f[ld] + r) return false;
-  double dx = f[fd] - pa[fd];
-  double dy = f[ld] - pa[ld];
-  return !(dx * dx + dy * dy > r * r);
-}
-
-// raySphere for a ray along axis VC with direction length d: the dot products of the generic
-// routine reduce to single products (the other terms are zero), the rest keeps its operation order.
-template <int VC>
-__device__ __forceinline__ bool ray_sphere_axis(const double* orig, double d, const double* c, double r, double* t1,
-                                                double* t2) {
-  double temp0 = orig[0] - c[0], temp1 = orig[1] - c[1], temp2 = orig[2] - c[2];
-  double tv = VC == 0 ? temp0 : (VC == 1 ? temp1 : temp2);
-  double A = d * d;
-  double B = tv * d;
-  double C = temp0 * temp0 + temp1 * temp1 + temp2 * temp2 - r * r;
-  double det = B * B - A * C;
-  if (det < 0.) return false;
-  det = sqrt(det);
-  double a = (-B - det) / A;
-  double b = (-B + det) / A;
-  if (b < a) { double tt = a; a = b; b = tt; }
-  *t1 = a;
-  *t2 = b;
-  return true;
-}
-
-template <int P, bool kTorus>
-__device__ __forceinline__ int intersect_f64_p(const double* f, int kind, int first, int cnt, const PatchDev& Pd,
-                                               const double* pa, double ray_dir, double* t) {
-  constexpr int vc = Ax<P>::vc;
-  if (!ray_sphere_axis<vc>(pa, ray_dir, f, f[kR], &t[0], &t[1])) return 0;
-  int numInt = 2;
-  if (kTorus) numInt = ray_torus_f64(f, Pd.probe, vc, pa, ray_dir, t);
-  int out = 0;
-  for (int i = 0; i < numInt; i++) {
-    double ip[3] = {pa[0], pa[1], pa[2]};
-    ip[vc] += t[i] * ray_dir;
-    if (feasible_f64(f, kind, first, cnt, Pd.pool, Pd.flag, ip)) t[out++] = t[i];
-  }
-  return out;
-}
-
-// Result of the mixed-precision test for a candidate it cannot decide: the candidate goes to a
-// deferred list that a double-precision pass takes afterwards, so that the mixed kernel's warps
-// never wait on a double-precision path taken by one lane.
-constexpr int kDefer = -1;
-
-// Mixed-precision intersection of a candidate (see ray_math_mixed.cuh): the number of feasible
-// hits, or kDefer when the single-precision bracket cannot decide the candidate.
-template <int PN, bool kTorus>
-__device__ __forceinline__ int intersect_mixed(const double* f, int kind, int first, int cnt, const PatchDev& P,
-                                               const double* pa, double ray_dir, double inv_dir, double* t,
-                                               unsigned long long* ctr) {
-  constexpr int fd = Ax<PN>::fd, ld = Ax<PN>::ld, vc = Ax<PN>::vc;
-  const double r = f[kR];
-  const double dx64 = pa[fd] - f[fd], dy64 = pa[ld] - f[ld];
-  const float dxf = (float)dx64, dyf = (float)dy64, rf = (float)r;
-  float disc = rf * rf - dxf * dxf - dyf * dyf;
-  if (disc < kDiscTol) {
-    if (ctr) atomicAdd(ctr + kCntFbSphere, 1ull);
-    return kDefer;
-  }
-  float s32 = sqrtf(disc);
-  double disc64 = r * r - dx64 * dx64 - dy64 * dy64;
-  double sd = (double)s32;
-  sd = sd + (disc64 - sd * sd) * (double)(0.5f / s32);
-  double xs[4];
-  int nx = 0;
-  const double cv = f[vc];
-  if (kTorus) {
-    const double x_in = cv - sd;
-    double orig1[3];
-    orig1[fd] = pa[fd];
-    orig1[ld] = pa[ld];
-    orig1[vc] = x_in;
-    double B, C, D, E;
-    torus_coeffs_f64(f, P.probe, vc, orig1, &B, &C, &D, &E);
-    double roots[4];
-    int nr = quartic_guarded(roots, B, C, D, E);
-    if (nr < 0) {
-      if (ctr) atomicAdd(ctr + kCntFbQuartic, 1ull);
-      return kDefer;
-    }
-    const double r2 = r * r;
-    for (int i = 0; i < nr; i++) {
-      double root = roots[i];
-      if (fabs(root) < 1e-9) {
-        if (ctr) atomicAdd(ctr + kCntFbRoot, 1ull);
-        return kDefer;
-      }
-      if (root < 0) continue;
-      double px = x_in + root;
-      double e0 = f[fd] - pa[fd], e1 = f[ld] - pa[ld], e2 = cv - px;
-      double dd = e0 * e0 + e1 * e1 + e2 * e2;
-      if (fabs(dd - r2) < 1e-9) {
-        if (ctr) atomicAdd(ctr + kCntFbRoot, 1ull);
-        return kDefer;
-      }
-      if (dd < r2) xs[nx++] = px;
-    }
-  } else {
-    xs[0] = cv - sd;
-    xs[1] = cv + sd;
-    nx = 2;
-  }
-  int out = 0;
-  for (int i = 0; i < nx; i++) {
-    float pl[3];
-    pl[fd] = dxf;
-    pl[ld] = dyf;
-    pl[vc] = (float)(xs[i] - cv);
-    double p64[3];
-    p64[fd] = pa[fd];
-    p64[ld] = pa[ld];
-    p64[vc] = xs[i];
-    if (feasible_mixed(f, kind, first, cnt, P.pool, P.pool32, P.flag, pl, p64)) t[out++] = (xs[i] - pa[vc]) * inv_dir;
-  }
-  return out;
 }
 
 // Pairs the sorted hits of one ray in place (NEW_INTERSECTION_FILTERING) and turns them into
@@ -388,19 +254,14 @@ __device__ __forceinline__ void clear_bits_range(uint32_t* bits, int64_t nwords,
   }
 }
 
-struct TraceCtx {
-  PatchDev P;
-  BatchDev B;
-  int set;
-  TraceOut out;
-};
 
 // Wavefront ray tracing of one ray set, three kernel kinds:
-//  * k_cand: one warp per patch walks the patch's pixel window (the reference's CELL_CULLING
-//    window, k_windows), 32 rays at a time, tests each against the bounding box and equatorial
-//    disc and appends the surviving (ray, patch) pairs with one atomic per warp step, to the
-//    sphere list (atoms and probes) or the torus list; a patch's candidates stay contiguous, so
-//    the intersection kernels read its record once per warp;
+//  * k_cand: one warp per patch, one lane per pixel row of the patch's pixel window (the
+//    reference's CELL_CULLING window, k_windows): each row's rays that pass the bounding-box and
+//    equatorial-disc test form an interval, found by binary search with the exact test; the
+//    surviving (ray, patch) pairs are appended with one atomic per patch, in row-major order, to
+//    the sphere list (atoms and probes) or the torus list; a patch's candidates stay contiguous,
+//    so the intersection kernels read its record once per warp;
 //  * k_isect<torus, mixed>: one thread per candidate pair, sphere and torus pairs in separate
 //    launches so that both run converged with their own register budget; hits are filed into
 //    the ray's slots of a slot-major hit store through a per-ray atomic counter;
@@ -421,111 +282,86 @@ __global__ void __launch_bounds__(256) k_cand(TraceCtx C, CandOut co) {
     const int m0 = w[rs.fd], n0 = w[rs.ld];
     const int W = w[3 + rs.fd] - m0 + 1, H = w[3 + rs.ld] - n0 + 1;
     if (W <= 0 || H <= 0) continue;
-    const int total = W * H;
+    const int m1 = m0 + W - 1;
     const double* src = C.P.f64 + (int64_t)NS_PATCH_F64 * pid;
-    double f[4];
-#pragma unroll
-    for (int k = 0; k < 4; k++) f[k] = __ldg(src + k);
+    const double cf = __ldg(src + rs.fd), cl = __ldg(src + rs.ld), r = __ldg(src + kR);
+    // the operands of candidate(), rounded as there
+    const double lo_fd = cf - r, hi_fd = cf + r, lo_ld = cl - r, hi_ld = cl + r, r2 = r * r;
     const int kind = C.P.i32[NS_PATCH_I32 * pid];
     const int ty = (kind == NS_EDGE_REG || kind == NS_EDGE_SING) ? 1 : 0;
     int2* dst = ty ? co.tor : co.sph;
-    auto test = [&](int idx, int64_t* rid) {
-      const int dn = idx / W;
-      const int m = m0 + (idx - dn * W), n = n0 + dn;
-      double pa[3];
-      // gcoord(g, d, i) + delta, with the same operation order
-      pa[rs.fd] = (g.mn[rs.fd] + (double)m * g.side) + rs.delta;
-      pa[rs.ld] = (g.mn[rs.ld] + (double)n * g.side) + rs.delta;
-      pa[rs.vc] = (g.mn[rs.vc] + 0.0 * g.side) + rs.delta;
-      *rid = rbase + (int64_t)n * rs.nb + m;
-      return candidate(f, rs, pa);
-    };
-    // pass 1 counts the window's candidates, one atomic reserves their slots, pass 2 writes them
-    int cnt = 0;
-    for (int base = 0; base < total; base += 32) {
-      const int idx = base + lane;
-      int64_t rid;
-      const bool pass = idx < total && test(idx, &rid);
-      cnt += __popc(__ballot_sync(0xffffffffu, pass));
-    }
-    if (cnt == 0) continue;
-    unsigned long long slot = 0;
-    if (lane == 0) slot = atomicAdd(co.count + ty, (unsigned long long)cnt);
-    slot = __shfl_sync(0xffffffffu, slot, 0);
-    if ((int64_t)(slot + cnt) > co.cap) {
-      if (lane == 0) atomicExch(C.out.error_flag, 6);
-      continue;
-    }
-    for (int base = 0; base < total; base += 32) {
-      const int idx = base + lane;
-      int64_t rid = 0;
-      const bool pass = idx < total && test(idx, &rid);
-      const unsigned mask = __ballot_sync(0xffffffffu, pass);
-      if (pass) dst[slot + __popc(mask & ((1u << lane) - 1u))] = make_int2((int)rid, (int)pid);
-      slot += __popc(mask);
-    }
-  }
-}
-
-// One thread per candidate pair of one type: intersection, feasibility, hit filing.
-template <int PN, bool kTorus, bool kMixed>
-__global__ void __launch_bounds__(256) k_isect(TraceCtx C, CandOut co, HitStore hs) {
-  constexpr int fd = Ax<PN>::fd, ld = Ax<PN>::ld, vc = Ax<PN>::vc;
-  const int64_t ncand = *(co.count + (kTorus ? 1 : 0));
-  const int2* list = kTorus ? co.tor : co.sph;
-  const int64_t nlim = ncand < co.cap ? ncand : co.cap;
-  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < nlim; c += (int64_t)gridDim.x * blockDim.x) {
-    int2 e = list[c];
-    const int64_t rid = e.x, pid = e.y;
-    const StructDev& S = C.B.s[C.B.patch_struct[pid]];
-    const GridDev& g = S.g;
-    const double delta = C.set == 0 ? 0.0 : NS_DELTA - g.hside;
-    const double ray_dir = S.ray_dir[vc];
-    const double inv_dir = S.inv_dir[vc];
-    const int64_t nb = g.n[fd];
-    const int64_t lr = rid - S.ray_base[C.set];
-    const int64_t m = lr % nb, n = lr / nb;
-    double pa[3];
-    pa[fd] = gcoord(g, fd, m) + delta;
-    pa[ld] = gcoord(g, ld, n) + delta;
-    pa[vc] = gcoord(g, vc, 0) + delta;
-    double f[NS_PATCH_F64];
-    const double* src = C.P.f64 + (int64_t)NS_PATCH_F64 * pid;
-    constexpr int nf = kTorus ? 18 : 4;
-#pragma unroll
-    for (int k = 0; k < nf; k++) f[k] = __ldg(src + k);
-    const int32_t* ir = C.P.i32 + NS_PATCH_I32 * pid;
-    const int kind = ir[0], first = ir[1], cnt = ir[2];
-    double t[4];
-    int k;
-    if (kMixed) {
-      k = intersect_mixed<PN, kTorus>(f, kind, first, cnt, C.P, pa, ray_dir, inv_dir, t, C.out.counters);
-      // warp-aggregated append of the deferred candidates
-      const bool defer = k == kDefer;
-      const unsigned am = __activemask();
-      const unsigned dm = __ballot_sync(am, defer);
-      if (dm) {
-        const int lane = threadIdx.x & 31;
-        const int leader = __ffs(dm) - 1;
-        unsigned long long base = 0;
-        if (lane == leader) base = atomicAdd(co.dcount + (kTorus ? 1 : 0), (unsigned long long)__popc(dm));
-        base = __shfl_sync(am, base, leader);
-        if (defer) {
-          unsigned long long slot = base + __popc(dm & ((1u << lane) - 1u));
-          if ((int64_t)slot < co.dcap) (kTorus ? co.dtor : co.dsph)[slot] = e;
-          else atomicExch(C.out.error_flag, 7);
+    // One lane per pixel row.  Along a row the pixel coordinate pa(m) is non-decreasing in m and
+    // dx = cf - pa(m) non-increasing; fl(fl(dx*dx) + fl(dy*dy)) is non-decreasing in |dx|.  So
+    //   Low(m)  = pa(m) >= lo_fd && (dx < 0 || disc(dx))   holds on an upper set of m,
+    //   High(m) = pa(m) <= hi_fd && (dx > 0 || disc(dx))   holds on a lower set of m,
+    // and candidate() (box in both axes, then disc) passes exactly when the row's box test holds and
+    // Low(m) && High(m).  The row's candidates are the interval [first Low, last High] of the
+    // window, found by two binary searches with the exact double-precision tests.
+    for (int row0 = 0; row0 < H; row0 += 32) {
+      int a = 0, cnt = 0;
+      if (row0 + lane < H) {
+        const int n = n0 + row0 + lane;
+        const double pld = (g.mn[rs.ld] + (double)n * g.side) + rs.delta;
+        if (!(pld < lo_ld || pld > hi_ld)) {
+          const double dy = cl - pld;
+          const double dy2 = dy * dy;
+          int lo = m0, hi = m1 + 1;
+          while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            const double pa = (g.mn[rs.fd] + (double)mid * g.side) + rs.delta;
+            const double dx = cf - pa;
+            const bool low = !(pa < lo_fd) && (dx < 0. || !(dx * dx + dy2 > r2));
+            if (low) hi = mid;
+            else lo = mid + 1;
+          }
+          a = lo;
+          lo = a;
+          hi = m1 + 1;
+          while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            const double pa = (g.mn[rs.fd] + (double)mid * g.side) + rs.delta;
+            const double dx = cf - pa;
+            const bool high = !(pa > hi_fd) && (dx > 0. || !(dx * dx + dy2 > r2));
+            if (!high) hi = mid;
+            else lo = mid + 1;
+          }
+          cnt = lo - a;  // [a, lo - 1]
         }
       }
-    } else {
-      k = intersect_f64_p<PN, kTorus>(f, kind, first, cnt, C.P, pa, ray_dir, t);
-    }
-    if (k <= 0) continue;
-    int pos = atomicAdd(hs.cnt + rid, k);
-    for (int i = 0; i < k; i++)
-      if (pos + i < kHitCap) {
-        hs.t[(int64_t)(pos + i) * hs.nrays + rid] = t[i];
-        if (hs.pid) hs.pid[(int64_t)(pos + i) * hs.nrays + rid] = (int32_t)pid;
+      int incl = cnt;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
       }
+      const int total = __shfl_sync(0xffffffffu, incl, 31);
+      if (total == 0) continue;
+      unsigned long long slot = 0;
+      if (lane == 0) slot = atomicAdd(co.count + ty, (unsigned long long)total);
+      slot = __shfl_sync(0xffffffffu, slot, 0);
+      if ((int64_t)(slot + total) > co.cap) {
+        if (lane == 0) atomicExch(C.out.error_flag, 6);
+        continue;
+      }
+      const int excl = incl - cnt;
+      // coalesced stores: output k belongs to the row whose inclusive prefix first exceeds k
+      for (int base = 0; base < total; base += 32) {
+        const int k = base + lane;
+        const int kk = k < total ? k : total - 1;
+        int rr = 0;
+#pragma unroll
+        for (int step = 16; step; step >>= 1) {
+          const int v = __shfl_sync(0xffffffffu, incl, rr + step - 1);
+          if (v <= kk) rr += step;
+        }
+        const int ar = __shfl_sync(0xffffffffu, a, rr), er = __shfl_sync(0xffffffffu, excl, rr);
+        if (k < total) {
+          const int m = ar + (k - er);
+          const int64_t n = n0 + row0 + rr;
+          dst[slot + k] = make_int2((int)(rbase + n * rs.nb + m), (int)pid);
+        }
+      }
+    }
   }
 }
 
@@ -534,8 +370,7 @@ void launch_isect(const TraceCtx& C, const CandOut& co, const HitStore& hs, int 
                   cudaStream_t s) {
   const int ig = 148 * tp.isect_bpsm, it = tp.isect_threads;
   if (precision == 1) {
-    k_isect<PN, false, true><<<ig, it, 0, s>>>(C, co, hs);
-    k_isect<PN, true, true><<<ig, it, 0, s>>>(C, co, hs);
+    launch_isect_mixed<PN>(C, co, hs, tp, s);
     // the deferred candidates, in double precision (few: a small grid)
     const CandOut dco{co.dsph, co.dtor, co.dcap, co.dcount, nullptr, nullptr, 0, nullptr};
     k_isect<PN, false, false><<<148, 256, 0, s>>>(C, dco, hs);

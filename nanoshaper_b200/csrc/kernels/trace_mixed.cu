@@ -1,0 +1,19 @@
+// Mixed-precision ray-patch intersection kernels, compiled with fused multiply-adds (the build
+// gives this file --fmad=true; every other device file is compiled with --fmad=false).
+#include "isect.cuh"
+
+namespace nsg {
+
+template <int PN>
+void launch_isect_mixed(const TraceCtx& C, const CandOut& co, const HitStore& hs, const TuneParams& tp,
+                        cudaStream_t s) {
+  const int ig = 148 * tp.isect_bpsm, it = tp.isect_threads;
+  k_isect<PN, false, true><<<ig, it, 0, s>>>(C, co, hs);
+  k_isect<PN, true, true><<<ig, it, 0, s>>>(C, co, hs);
+}
+
+template void launch_isect_mixed<0>(const TraceCtx&, const CandOut&, const HitStore&, const TuneParams&, cudaStream_t);
+template void launch_isect_mixed<1>(const TraceCtx&, const CandOut&, const HitStore&, const TuneParams&, cudaStream_t);
+template void launch_isect_mixed<2>(const TraceCtx&, const CandOut&, const HitStore&, const TuneParams&, cudaStream_t);
+
+}  // namespace nsg

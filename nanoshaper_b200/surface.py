@@ -561,6 +561,12 @@ class SurfaceBatch:
         N.check(N.lib().nsg_batch_results(c, None, N.ptr(self.areas)), "batch results")
         return self.areas
 
+    def set_tuning(self, params) -> None:
+        """Sets the tracer's launch shapes: [intersection threads per block, intersection blocks
+        per SM, candidate threads per block] (the ranges of ``nsg_set_tuning``)."""
+        p = np.ascontiguousarray(params, np.int32)
+        N.check(N.lib().nsg_set_tuning(self._context().handle, N.ptr(p), len(p)), "set tuning")
+
     def autotune(self, grad: bool = False, reps: int = 2) -> tuple[list[int], float]:
         """Picks the tracer's launch shapes (intersection block size and blocks per SM, candidate
         block size) for this batch by timing ray casts; returns the shape and its ms per cast."""
