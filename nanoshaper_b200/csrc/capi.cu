@@ -716,7 +716,7 @@ int nsg_fp_peak(nsg_ctx* c, int precision, double* flops_per_s) {
 int nsg_set_tuning(nsg_ctx* c, const int32_t* params, int n) {
   if (!c || !params || n < 3) return NSG_ERR_ARG;
   const int it = params[0], bpsm = params[1], ct = params[2];
-  if (it < 64 || it > 256 || it % 32 || bpsm < 1 || bpsm > 64 || ct < 32 || ct > 1024 || ct % 32)
+  if (it < 64 || it > 256 || it % 32 || bpsm < 1 || bpsm > 64 || ct < 32 || ct > 256 || ct % 32)
     return fail(NSG_ERR_ARG, "tuning parameters out of range");
   c->tune.isect_threads = it;
   c->tune.isect_bpsm = bpsm;

@@ -256,40 +256,71 @@ __device__ __forceinline__ void clear_bits_range(uint32_t* bits, int64_t nwords,
 
 
 // Wavefront ray tracing of one ray set, three kernel kinds:
-//  * k_cand: one warp per patch, one lane per pixel row of the patch's pixel window (the
-//    reference's CELL_CULLING window, k_windows): each row's rays that pass the bounding-box and
-//    equatorial-disc test form an interval, found by binary search with the exact test; the
-//    surviving (ray, patch) pairs are appended with one atomic per patch, in row-major order, to
-//    the sphere list (atoms and probes) or the torus list; a patch's candidates stay contiguous,
-//    so the intersection kernels read its record once per warp;
+//  * k_cand: one warp per batch of 32 patches, whose records the lanes load together; then, patch
+//    by patch, one lane per pixel row of the patch's pixel window (the reference's CELL_CULLING
+//    window, k_windows): each row's rays that pass the bounding-box and equatorial-disc test form
+//    an interval, found by binary search with the exact test.  One atomic per list and batch
+//    reserves the slots; the (ray, patch) pairs follow in row-major order, in the sphere list
+//    (atoms and probes) or the torus list; a patch's candidates stay contiguous, so the
+//    intersection kernels read its record once per warp;
 //  * k_isect<torus, mixed>: one thread per candidate pair, sphere and torus pairs in separate
 //    launches so that both run converged with their own register budget; hits are filed into
 //    the ray's slots of a slot-major hit store through a per-ray atomic counter;
 //  * k_fill: one CTA per 32x4 ray tile loads each ray's hits, sorts them and performs the
 //    interval fill.
+// One patch of a k_cand batch, staged in shared memory: the operands of candidate() rounded as
+// there, the pixel window and where the patch's rays start.
+struct CandPatch {
+  double cf, cl, lo_fd, hi_fd, lo_ld, hi_ld, r2, mn_fd, mn_ld, side, delta;
+  int64_t nb, rbase;
+  int m0, m1, n0, H, ty, pid;
+};
+
 __global__ void __launch_bounds__(256) k_cand(TraceCtx C, CandOut co) {
-  const int lane = threadIdx.x & 31;
+  __shared__ CandPatch s_rec[8][32];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  CandPatch* rec = s_rec[wib];
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
-  for (int64_t pid = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); pid < C.P.n; pid += warps) {
-    const int32_t* w = C.P.win + 6 * pid;
-    if (w[0] < 0) continue;
-    const int b = C.B.patch_struct[pid];
-    // grid values in registers: the loop below stores to global memory, which would otherwise
-    // force re-reads of the structure record
-    const GridDev g = C.B.s[b].g;
-    const int64_t rbase = C.B.s[b].ray_base[C.set];
-    const RaySet rs = make_ray_set(C.set, g);
-    const int m0 = w[rs.fd], n0 = w[rs.ld];
-    const int W = w[3 + rs.fd] - m0 + 1, H = w[3 + rs.ld] - n0 + 1;
-    if (W <= 0 || H <= 0) continue;
-    const int m1 = m0 + W - 1;
-    const double* src = C.P.f64 + (int64_t)NS_PATCH_F64 * pid;
-    const double cf = __ldg(src + rs.fd), cl = __ldg(src + rs.ld), r = __ldg(src + kR);
-    // the operands of candidate(), rounded as there
-    const double lo_fd = cf - r, hi_fd = cf + r, lo_ld = cl - r, hi_ld = cl + r, r2 = r * r;
-    const int kind = C.P.i32[NS_PATCH_I32 * pid];
-    const int ty = (kind == NS_EDGE_REG || kind == NS_EDGE_SING) ? 1 : 0;
-    int2* dst = ty ? co.tor : co.sph;
+  for (int64_t base = (blockIdx.x * (int64_t)(blockDim.x >> 5) + wib) * 32; base < C.P.n; base += warps * 32) {
+    // 1. the batch's 32 patches, one per lane
+    {
+      const int64_t pid = base + lane;
+      CandPatch q;
+      q.H = 0;
+      q.ty = 0;
+      q.pid = (int)pid;
+      const int32_t* w = C.P.win + 6 * pid;
+      if (pid < C.P.n && w[0] >= 0) {
+        const StructDev& S = C.B.s[C.B.patch_struct[pid]];
+        const GridDev& g = S.g;
+        const RaySet rs = make_ray_set(C.set, g);
+        const double* src = C.P.f64 + (int64_t)NS_PATCH_F64 * pid;
+        const double cf = __ldg(src + rs.fd), cl = __ldg(src + rs.ld), r = __ldg(src + kR);
+        q.cf = cf;
+        q.cl = cl;
+        q.lo_fd = cf - r;
+        q.hi_fd = cf + r;
+        q.lo_ld = cl - r;
+        q.hi_ld = cl + r;
+        q.r2 = r * r;
+        q.mn_fd = g.mn[rs.fd];
+        q.mn_ld = g.mn[rs.ld];
+        q.side = g.side;
+        q.delta = rs.delta;
+        q.nb = rs.nb;
+        q.rbase = S.ray_base[C.set];
+        q.m0 = w[rs.fd];
+        q.m1 = w[3 + rs.fd];
+        q.n0 = w[rs.ld];
+        const int H = w[3 + rs.ld] - q.n0 + 1;
+        q.H = (q.m1 >= q.m0 && H > 0) ? H : 0;
+        const int kind = C.P.i32[NS_PATCH_I32 * pid];
+        q.ty = (kind == NS_EDGE_REG || kind == NS_EDGE_SING) ? 1 : 0;
+      }
+      rec[lane] = q;
+    }
+    __syncwarp();
+    unsigned live = __ballot_sync(0xffffffffu, rec[lane].H > 0);
     // One lane per pixel row.  Along a row the pixel coordinate pa(m) is non-decreasing in m and
     // dx = cf - pa(m) non-increasing; fl(fl(dx*dx) + fl(dy*dy)) is non-decreasing in |dx|.  So
     //   Low(m)  = pa(m) >= lo_fd && (dx < 0 || disc(dx))   holds on an upper set of m,
@@ -297,71 +328,108 @@ __global__ void __launch_bounds__(256) k_cand(TraceCtx C, CandOut co) {
     // and candidate() (box in both axes, then disc) passes exactly when the row's box test holds and
     // Low(m) && High(m).  The row's candidates are the interval [first Low, last High] of the
     // window, found by two binary searches with the exact double-precision tests.
-    for (int row0 = 0; row0 < H; row0 += 32) {
-      int a = 0, cnt = 0;
-      if (row0 + lane < H) {
-        const int n = n0 + row0 + lane;
-        const double pld = (g.mn[rs.ld] + (double)n * g.side) + rs.delta;
-        if (!(pld < lo_ld || pld > hi_ld)) {
-          const double dy = cl - pld;
-          const double dy2 = dy * dy;
-          int lo = m0, hi = m1 + 1;
-          while (lo < hi) {
-            const int mid = (lo + hi) >> 1;
-            const double pa = (g.mn[rs.fd] + (double)mid * g.side) + rs.delta;
-            const double dx = cf - pa;
-            const bool low = !(pa < lo_fd) && (dx < 0. || !(dx * dx + dy2 > r2));
-            if (low) hi = mid;
-            else lo = mid + 1;
-          }
-          a = lo;
-          lo = a;
-          hi = m1 + 1;
-          while (lo < hi) {
-            const int mid = (lo + hi) >> 1;
-            const double pa = (g.mn[rs.fd] + (double)mid * g.side) + rs.delta;
-            const double dx = cf - pa;
-            const bool high = !(pa > hi_fd) && (dx > 0. || !(dx * dx + dy2 > r2));
-            if (!high) hi = mid;
-            else lo = mid + 1;
-          }
-          cnt = lo - a;  // [a, lo - 1]
-        }
+    auto row_span = [&](const CandPatch& q, int row, int& a) -> int {
+      a = 0;
+      if (row >= q.H) return 0;
+      const double pld = (q.mn_ld + (double)(q.n0 + row) * q.side) + q.delta;
+      if (pld < q.lo_ld || pld > q.hi_ld) return 0;
+      const double dy = q.cl - pld;
+      const double dy2 = dy * dy;
+      int lo = q.m0, hi = q.m1 + 1;
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        const double pa = (q.mn_fd + (double)mid * q.side) + q.delta;
+        const double dx = q.cf - pa;
+        const bool low = !(pa < q.lo_fd) && (dx < 0. || !(dx * dx + dy2 > q.r2));
+        if (low) hi = mid;
+        else lo = mid + 1;
       }
-      int incl = cnt;
+      a = lo;
+      hi = q.m1 + 1;
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        const double pa = (q.mn_fd + (double)mid * q.side) + q.delta;
+        const double dx = q.cf - pa;
+        const bool high = !(pa > q.hi_fd) && (dx > 0. || !(dx * dx + dy2 > q.r2));
+        if (!high) hi = mid;
+        else lo = mid + 1;
+      }
+      return lo - a;
+    };
+    // 2. candidate count of every patch of the batch (lane p keeps patch p's)
+    int my_total = 0;
+    for (unsigned m = live; m; m &= m - 1) {
+      const int p = __ffs(m) - 1;
+      const CandPatch q = rec[p];
+      int t = 0;
+      for (int row0 = 0; row0 < q.H; row0 += 32) {
+        int a;
+        t += __reduce_add_sync(0xffffffffu, row_span(q, row0 + lane, a));
+      }
+      if (lane == p) my_total = t;
+    }
+    // 3. one atomic per candidate list for the whole batch
+    const int my_ty = rec[lane].ty;
+    int inc0 = my_ty == 0 ? my_total : 0, inc1 = my_ty == 1 ? my_total : 0;
 #pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int v = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += v;
-      }
-      const int total = __shfl_sync(0xffffffffu, incl, 31);
-      if (total == 0) continue;
-      unsigned long long slot = 0;
-      if (lane == 0) slot = atomicAdd(co.count + ty, (unsigned long long)total);
-      slot = __shfl_sync(0xffffffffu, slot, 0);
-      if ((int64_t)(slot + total) > co.cap) {
-        if (lane == 0) atomicExch(C.out.error_flag, 6);
-        continue;
-      }
-      const int excl = incl - cnt;
-      // coalesced stores: output k belongs to the row whose inclusive prefix first exceeds k
-      for (int base = 0; base < total; base += 32) {
-        const int k = base + lane;
-        const int kk = k < total ? k : total - 1;
-        int rr = 0;
-#pragma unroll
-        for (int step = 16; step; step >>= 1) {
-          const int v = __shfl_sync(0xffffffffu, incl, rr + step - 1);
-          if (v <= kk) rr += step;
-        }
-        const int ar = __shfl_sync(0xffffffffu, a, rr), er = __shfl_sync(0xffffffffu, excl, rr);
-        if (k < total) {
-          const int m = ar + (k - er);
-          const int64_t n = n0 + row0 + rr;
-          dst[slot + k] = make_int2((int)(rbase + n * rs.nb + m), (int)pid);
-        }
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v0 = __shfl_up_sync(0xffffffffu, inc0, o), v1 = __shfl_up_sync(0xffffffffu, inc1, o);
+      if (lane >= o) {
+        inc0 += v0;
+        inc1 += v1;
       }
     }
+    const int sum0 = __shfl_sync(0xffffffffu, inc0, 31), sum1 = __shfl_sync(0xffffffffu, inc1, 31);
+    unsigned long long b0 = 0, b1 = 0;
+    if (lane == 0 && sum0) b0 = atomicAdd(co.count + 0, (unsigned long long)sum0);
+    if (lane == 0 && sum1) b1 = atomicAdd(co.count + 1, (unsigned long long)sum1);
+    b0 = __shfl_sync(0xffffffffu, b0, 0);
+    b1 = __shfl_sync(0xffffffffu, b1, 0);
+    if ((int64_t)(b0 + sum0) > co.cap || (int64_t)(b1 + sum1) > co.cap) {
+      if (lane == 0) atomicExch(C.out.error_flag, 6);
+      __syncwarp();
+      continue;
+    }
+    const unsigned long long my_slot = my_ty == 0 ? b0 + (inc0 - my_total) : b1 + (inc1 - my_total);
+    // 4. the candidates, patch by patch, rows in order, coalesced
+    for (unsigned m = __ballot_sync(0xffffffffu, my_total > 0); m; m &= m - 1) {
+      const int p = __ffs(m) - 1;
+      const CandPatch q = rec[p];
+      unsigned long long slot = __shfl_sync(0xffffffffu, my_slot, p);
+      int2* dst = q.ty ? co.tor : co.sph;
+      for (int row0 = 0; row0 < q.H; row0 += 32) {
+        int a;
+        const int cnt = row_span(q, row0 + lane, a);
+        int incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int v = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += v;
+        }
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        if (total == 0) continue;
+        const int excl = incl - cnt;
+        // output k belongs to the row whose inclusive prefix first exceeds k
+        for (int kb = 0; kb < total; kb += 32) {
+          const int k = kb + lane;
+          const int kk = k < total ? k : total - 1;
+          int rr = 0;
+#pragma unroll
+          for (int step = 16; step; step >>= 1) {
+            const int v = __shfl_sync(0xffffffffu, incl, rr + step - 1);
+            if (v <= kk) rr += step;
+          }
+          const int ar = __shfl_sync(0xffffffffu, a, rr), er = __shfl_sync(0xffffffffu, excl, rr);
+          if (k < total) {
+            const int mm = ar + (k - er);
+            const int64_t n = q.n0 + row0 + rr;
+            dst[slot + k] = make_int2((int)(q.rbase + n * q.nb + mm), q.pid);
+          }
+        }
+        slot += total;
+      }
+    }
+    __syncwarp();
   }
 }
 
@@ -790,7 +858,7 @@ cudaError_t launch_trace(const PatchDev& P, const BatchDev& B, int set, int64_t 
   if (ev) cudaEventRecord(ev[0], s);
   if (P.n > 0) {
     const int wpb = tp.cand_threads / 32;
-    int64_t blocks = (P.n + wpb - 1) / wpb;
+    int64_t blocks = (P.n + 32 * wpb - 1) / (32 * wpb);
     if (blocks > 148 * 64) blocks = 148 * 64;
     k_cand<<<(unsigned)blocks, tp.cand_threads, 0, s>>>(C, co);
   }
