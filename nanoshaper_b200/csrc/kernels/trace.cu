@@ -268,27 +268,78 @@ __device__ __forceinline__ void clear_bits_range(uint32_t* bits, int64_t nwords,
 //    the ray's slots of a slot-major hit store through a per-ray atomic counter;
 //  * k_fill: one CTA per 32x4 ray tile loads each ray's hits, sorts them and performs the
 //    interval fill.
-// One patch of a k_cand batch, staged in shared memory: the operands of candidate() rounded as
-// there, the pixel window and where the patch's rays start.
-struct CandPatch {
-  double cf, cl, lo_fd, hi_fd, lo_ld, hi_ld, r2, mn_fd, mn_ld, side, delta;
-  int64_t nb, rbase;
-  int m0, m1, n0, H, ty, pid;
+// A k_cand batch of 32 patches, staged in shared memory (structure of arrays, one entry per lane
+// of the warp that loaded it): the operands of candidate() rounded as there, the pixel window
+// and where the patch's rays start.
+struct CandBatch {
+  double cf[32], cl[32], lo_fd[32], hi_fd[32], lo_ld[32], hi_ld[32], r2[32], mn_fd[32], mn_ld[32], side[32],
+      delta[32];
+  int64_t nb[32], rbase[32], base[32];
+  int m0[32], m1[32], n0[32], ty[32], pid[32];
+  int64_t gfirst[32], gend[32];
 };
 
+// Candidate count of pixel row `row` of batch patch p (its first candidate pixel in *a).  Along a
+// row the pixel coordinate pa(m) is non-decreasing in m and dx = cf - pa(m) non-increasing;
+// fl(fl(dx*dx) + fl(dy*dy)) is non-decreasing in |dx|.  So
+//   Low(m)  = pa(m) >= lo_fd && (dx < 0 || disc(dx))   holds on an upper set of m,
+//   High(m) = pa(m) <= hi_fd && (dx > 0 || disc(dx))   holds on a lower set of m,
+// and candidate() (box in both axes, then disc) passes exactly when the row's box test holds and
+// Low(m) && High(m).  The row's candidates are the interval [first Low, last High] of the
+// window, found by two binary searches with the exact double-precision tests.
+__device__ __forceinline__ int cand_row(const CandBatch& q, int p, int row, int* a) {
+  *a = 0;
+  const double pld = (q.mn_ld[p] + (double)(q.n0[p] + row) * q.side[p]) + q.delta[p];
+  if (pld < q.lo_ld[p] || pld > q.hi_ld[p]) return 0;
+  const double cl = q.cl[p], cf = q.cf[p], r2 = q.r2[p], mn = q.mn_fd[p], side = q.side[p], delta = q.delta[p];
+  const double lo_fd = q.lo_fd[p], hi_fd = q.hi_fd[p];
+  const double dy = cl - pld;
+  const double dy2 = dy * dy;
+  int lo = q.m0[p], hi = q.m1[p] + 1;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    const double pa = (mn + (double)mid * side) + delta;
+    const double dx = cf - pa;
+    const bool low = !(pa < lo_fd) && (dx < 0. || !(dx * dx + dy2 > r2));
+    if (low) hi = mid;
+    else lo = mid + 1;
+  }
+  *a = lo;
+  hi = q.m1[p] + 1;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    const double pa = (mn + (double)mid * side) + delta;
+    const double dx = cf - pa;
+    const bool high = !(pa > hi_fd) && (dx > 0. || !(dx * dx + dy2 > r2));
+    if (!high) hi = mid;
+    else lo = mid + 1;
+  }
+  return lo - *a;
+}
+
+// Smallest lane whose inclusive prefix v exceeds k (k below the warp total).
+__device__ __forceinline__ int owner_lane(int v, int k) {
+  int rr = 0;
+#pragma unroll
+  for (int step = 16; step; step >>= 1) {
+    const int x = __shfl_sync(0xffffffffu, v, rr + step - 1);
+    if (x <= k) rr += step;
+  }
+  return rr;
+}
+
 __global__ void __launch_bounds__(256) k_cand(TraceCtx C, CandOut co) {
-  __shared__ CandPatch s_rec[8][32];
+  __shared__ CandBatch s_batch[8];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  CandPatch* rec = s_rec[wib];
+  CandBatch& q = s_batch[wib];
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t base = (blockIdx.x * (int64_t)(blockDim.x >> 5) + wib) * 32; base < C.P.n; base += warps * 32) {
     // 1. the batch's 32 patches, one per lane
+    int H = 0;
     {
       const int64_t pid = base + lane;
-      CandPatch q;
-      q.H = 0;
-      q.ty = 0;
-      q.pid = (int)pid;
+      q.ty[lane] = 0;
+      q.pid[lane] = (int)pid;
       const int32_t* w = C.P.win + 6 * pid;
       if (pid < C.P.n && w[0] >= 0) {
         const StructDev& S = C.B.s[C.B.patch_struct[pid]];
@@ -296,80 +347,66 @@ __global__ void __launch_bounds__(256) k_cand(TraceCtx C, CandOut co) {
         const RaySet rs = make_ray_set(C.set, g);
         const double* src = C.P.f64 + (int64_t)NS_PATCH_F64 * pid;
         const double cf = __ldg(src + rs.fd), cl = __ldg(src + rs.ld), r = __ldg(src + kR);
-        q.cf = cf;
-        q.cl = cl;
-        q.lo_fd = cf - r;
-        q.hi_fd = cf + r;
-        q.lo_ld = cl - r;
-        q.hi_ld = cl + r;
-        q.r2 = r * r;
-        q.mn_fd = g.mn[rs.fd];
-        q.mn_ld = g.mn[rs.ld];
-        q.side = g.side;
-        q.delta = rs.delta;
-        q.nb = rs.nb;
-        q.rbase = S.ray_base[C.set];
-        q.m0 = w[rs.fd];
-        q.m1 = w[3 + rs.fd];
-        q.n0 = w[rs.ld];
-        const int H = w[3 + rs.ld] - q.n0 + 1;
-        q.H = (q.m1 >= q.m0 && H > 0) ? H : 0;
+        q.cf[lane] = cf;
+        q.cl[lane] = cl;
+        q.lo_fd[lane] = cf - r;
+        q.hi_fd[lane] = cf + r;
+        q.lo_ld[lane] = cl - r;
+        q.hi_ld[lane] = cl + r;
+        q.r2[lane] = r * r;
+        q.mn_fd[lane] = g.mn[rs.fd];
+        q.mn_ld[lane] = g.mn[rs.ld];
+        q.side[lane] = g.side;
+        q.delta[lane] = rs.delta;
+        q.nb[lane] = rs.nb;
+        q.rbase[lane] = S.ray_base[C.set];
+        q.m0[lane] = w[rs.fd];
+        q.m1[lane] = w[3 + rs.fd];
+        q.n0[lane] = w[rs.ld];
+        const int h = w[3 + rs.ld] - w[rs.ld] + 1;
+        H = (w[3 + rs.fd] >= w[rs.fd] && h > 0) ? h : 0;
         const int kind = C.P.i32[NS_PATCH_I32 * pid];
-        q.ty = (kind == NS_EDGE_REG || kind == NS_EDGE_SING) ? 1 : 0;
+        q.ty[lane] = (kind == NS_EDGE_REG || kind == NS_EDGE_SING) ? 1 : 0;
       }
-      rec[lane] = q;
+      q.gfirst[lane] = 0;
+      q.gend[lane] = 0;
+    }
+    // the batch's pixel rows, patch after patch, are processed 32 at a time
+    int hincl = H;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, hincl, o);
+      if (lane >= o) hincl += v;
+    }
+    const int hexcl = hincl - H;
+    const int R = __shfl_sync(0xffffffffu, hincl, 31);
+    __syncwarp();
+    if (R == 0) continue;
+    // 2. candidate counts: G = running exclusive prefix of the row counts in batch order; the
+    //    lanes holding a patch's first and last rows record G there
+    int64_t running = 0;
+    for (int rb = 0; rb < R; rb += 32) {
+      const int k = rb + lane;
+      const int kk = k < R ? k : R - 1;
+      const int p = owner_lane(hincl, kk);
+      const int row = kk - __shfl_sync(0xffffffffu, hexcl, p);
+      const int hp = __shfl_sync(0xffffffffu, H, p);
+      int a, cnt = 0;
+      if (k < R) cnt = cand_row(q, p, row, &a);
+      int cincl = cnt;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, cincl, o);
+        if (lane >= o) cincl += v;
+      }
+      if (k < R && row == 0) q.gfirst[p] = running + (cincl - cnt);
+      if (k < R && row == hp - 1) q.gend[p] = running + cincl;
+      running += __shfl_sync(0xffffffffu, cincl, 31);
     }
     __syncwarp();
-    unsigned live = __ballot_sync(0xffffffffu, rec[lane].H > 0);
-    // One lane per pixel row.  Along a row the pixel coordinate pa(m) is non-decreasing in m and
-    // dx = cf - pa(m) non-increasing; fl(fl(dx*dx) + fl(dy*dy)) is non-decreasing in |dx|.  So
-    //   Low(m)  = pa(m) >= lo_fd && (dx < 0 || disc(dx))   holds on an upper set of m,
-    //   High(m) = pa(m) <= hi_fd && (dx > 0 || disc(dx))   holds on a lower set of m,
-    // and candidate() (box in both axes, then disc) passes exactly when the row's box test holds and
-    // Low(m) && High(m).  The row's candidates are the interval [first Low, last High] of the
-    // window, found by two binary searches with the exact double-precision tests.
-    auto row_span = [&](const CandPatch& q, int row, int& a) -> int {
-      a = 0;
-      if (row >= q.H) return 0;
-      const double pld = (q.mn_ld + (double)(q.n0 + row) * q.side) + q.delta;
-      if (pld < q.lo_ld || pld > q.hi_ld) return 0;
-      const double dy = q.cl - pld;
-      const double dy2 = dy * dy;
-      int lo = q.m0, hi = q.m1 + 1;
-      while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        const double pa = (q.mn_fd + (double)mid * q.side) + q.delta;
-        const double dx = q.cf - pa;
-        const bool low = !(pa < q.lo_fd) && (dx < 0. || !(dx * dx + dy2 > q.r2));
-        if (low) hi = mid;
-        else lo = mid + 1;
-      }
-      a = lo;
-      hi = q.m1 + 1;
-      while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        const double pa = (q.mn_fd + (double)mid * q.side) + q.delta;
-        const double dx = q.cf - pa;
-        const bool high = !(pa > q.hi_fd) && (dx > 0. || !(dx * dx + dy2 > q.r2));
-        if (!high) hi = mid;
-        else lo = mid + 1;
-      }
-      return lo - a;
-    };
-    // 2. candidate count of every patch of the batch (lane p keeps patch p's)
-    int my_total = 0;
-    for (unsigned m = live; m; m &= m - 1) {
-      const int p = __ffs(m) - 1;
-      const CandPatch q = rec[p];
-      int t = 0;
-      for (int row0 = 0; row0 < q.H; row0 += 32) {
-        int a;
-        t += __reduce_add_sync(0xffffffffu, row_span(q, row0 + lane, a));
-      }
-      if (lane == p) my_total = t;
-    }
+    const int my_total = H > 0 ? (int)(q.gend[lane] - q.gfirst[lane]) : 0;
     // 3. one atomic per candidate list for the whole batch
-    const int my_ty = rec[lane].ty;
+    const int my_ty = q.ty[lane];
     int inc0 = my_ty == 0 ? my_total : 0, inc1 = my_ty == 1 ? my_total : 0;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -390,44 +427,41 @@ __global__ void __launch_bounds__(256) k_cand(TraceCtx C, CandOut co) {
       __syncwarp();
       continue;
     }
-    const unsigned long long my_slot = my_ty == 0 ? b0 + (inc0 - my_total) : b1 + (inc1 - my_total);
-    // 4. the candidates, patch by patch, rows in order, coalesced
-    for (unsigned m = __ballot_sync(0xffffffffu, my_total > 0); m; m &= m - 1) {
-      const int p = __ffs(m) - 1;
-      const CandPatch q = rec[p];
-      unsigned long long slot = __shfl_sync(0xffffffffu, my_slot, p);
-      int2* dst = q.ty ? co.tor : co.sph;
-      for (int row0 = 0; row0 < q.H; row0 += 32) {
-        int a;
-        const int cnt = row_span(q, row0 + lane, a);
-        int incl = cnt;
+    // a row's candidate j sits at base[p] + G(row) + j in its patch's list
+    const int64_t my_slot = my_ty == 0 ? (int64_t)b0 + (inc0 - my_total) : (int64_t)b1 + (inc1 - my_total);
+    q.base[lane] = my_slot - q.gfirst[lane];
+    __syncwarp();
+    // 4. the candidates, rows in batch order, stores coalesced
+    running = 0;
+    for (int rb = 0; rb < R; rb += 32) {
+      const int k = rb + lane;
+      const int kk = k < R ? k : R - 1;
+      const int p = owner_lane(hincl, kk);
+      const int row = kk - __shfl_sync(0xffffffffu, hexcl, p);
+      int a = 0, cnt = 0;
+      if (k < R) cnt = cand_row(q, p, row, &a);
+      int cincl = cnt;
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const int v = __shfl_up_sync(0xffffffffu, incl, o);
-          if (lane >= o) incl += v;
-        }
-        const int total = __shfl_sync(0xffffffffu, incl, 31);
-        if (total == 0) continue;
-        const int excl = incl - cnt;
-        // output k belongs to the row whose inclusive prefix first exceeds k
-        for (int kb = 0; kb < total; kb += 32) {
-          const int k = kb + lane;
-          const int kk = k < total ? k : total - 1;
-          int rr = 0;
-#pragma unroll
-          for (int step = 16; step; step >>= 1) {
-            const int v = __shfl_sync(0xffffffffu, incl, rr + step - 1);
-            if (v <= kk) rr += step;
-          }
-          const int ar = __shfl_sync(0xffffffffu, a, rr), er = __shfl_sync(0xffffffffu, excl, rr);
-          if (k < total) {
-            const int mm = ar + (k - er);
-            const int64_t n = q.n0 + row0 + rr;
-            dst[slot + k] = make_int2((int)(q.rbase + n * q.nb + mm), q.pid);
-          }
-        }
-        slot += total;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, cincl, o);
+        if (lane >= o) cincl += v;
       }
+      const int T = __shfl_sync(0xffffffffu, cincl, 31);
+      const int cexcl = cincl - cnt;
+      for (int kb = 0; kb < T; kb += 32) {
+        const int j = kb + lane;
+        const int jj = j < T ? j : T - 1;
+        const int rr = owner_lane(cincl, jj);
+        const int pr = __shfl_sync(0xffffffffu, p, rr), rowr = __shfl_sync(0xffffffffu, row, rr);
+        const int ar = __shfl_sync(0xffffffffu, a, rr), er = __shfl_sync(0xffffffffu, cexcl, rr);
+        if (j < T) {
+          const int m = ar + (j - er);
+          const int64_t n = q.n0[pr] + rowr;
+          int2* dst = q.ty[pr] ? co.tor : co.sph;
+          dst[q.base[pr] + running + j] = make_int2((int)(q.rbase[pr] + n * q.nb[pr] + m), q.pid[pr]);
+        }
+      }
+      running += T;
     }
     __syncwarp();
   }
