@@ -334,34 +334,39 @@ __device__ __forceinline__ double vdist(const double* a, const double* b) {
 // One thread per active cube.  Pass 0 finds the vertex of every cut edge, counts the triangles
 // and sums their areas (and, in gradient mode, their derivatives with respect to the analytic
 // vertices); pass 1 writes the triangles at their offsets from the stored vertex ids.
-__global__ void k_mc_tris(MCArgs A, int emit) {
+__global__ void __launch_bounds__(128) k_mc_tris(MCArgs A, int emit) {
   __shared__ int8_t s_tri[256][16];
   __shared__ uint16_t s_emask[256];
+  // vertex of cut edge e of this thread's cube at [e][thread]: the case table indexes it at run
+  // time, which a register array cannot serve
+  __shared__ int32_t s_vl[12][128];
   for (int t = threadIdx.x; t < 256 * 16; t += blockDim.x) (&s_tri[0][0])[t] = (&c_tri[0][0])[t];
   for (int t = threadIdx.x; t < 256; t += blockDim.x) s_emask[t] = c_emask[t];
   __syncthreads();
+  int32_t* vl = &s_vl[0][threadIdx.x];
   for (int64_t a = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; a < A.n_active; a += (int64_t)gridDim.x * blockDim.x) {
     int4 rec = A.act_rec[a];
     int c = rec.w & 255;
     int64_t i = rec.x, j = rec.y, k = rec.z;
     const StructDev& S = A.B.s[rec_struct(rec.w)];
-    int32_t vl[12];
     int em = s_emask[c];
     int32_t* cv = A.cube_vl + 12 * a;
     if (!emit) {
       // the edge -> vertex searches run once; the emit pass reads their results
       for (int e = 0; e < 12; e++) {
-        vl[e] = (em >> e) & 1 ? (int32_t)edge_vertex(A, S, e, i, j, k) : -1;
-        cv[e] = vl[e];
+        const int32_t v = (em >> e) & 1 ? (int32_t)edge_vertex(A, S, e, i, j, k) : -1;
+        vl[e * 128] = v;
+        cv[e] = v;
       }
     } else {
-      for (int e = 0; e < 12; e++) vl[e] = cv[e];
+      for (int e = 0; e < 12; e++) vl[e * 128] = cv[e];
     }
     int cnt = 0;
     int64_t o = emit ? A.tri_off[a] : 0;
     double area = 0.0;
     for (int q = 0; q < 16 && s_tri[c][q] >= 0; q += 3) {
-      int32_t v0 = vl[s_tri[c][q]], v1 = vl[s_tri[c][q + 1]], v2 = vl[s_tri[c][q + 2]];
+      const int e0 = s_tri[c][q], e1 = s_tri[c][q + 1], e2 = s_tri[c][q + 2];
+      const int32_t v0 = vl[e0 * 128], v1 = vl[e1 * 128], v2 = vl[e2 * 128];
       if (v0 < 0 || v1 < 0 || v2 < 0) continue;
       if (emit) {
         A.tris[3 * (o + cnt) + 0] = (int32_t)v2;
@@ -371,30 +376,35 @@ __global__ void k_mc_tris(MCArgs A, int emit) {
         const double* P0 = A.vpos + 3 * (int64_t)v0;
         const double* P1 = A.vpos + 3 * (int64_t)v1;
         const double* P2 = A.vpos + 3 * (int64_t)v2;
-        double da = vdist(P0, P1), db = vdist(P0, P2), dc = vdist(P1, P2);
+        const double p0[3] = {P0[0], P0[1], P0[2]}, p1[3] = {P1[0], P1[1], P1[2]}, p2[3] = {P2[0], P2[1], P2[2]};
+        double da = vdist(p0, p1), db = vdist(p0, p2), dc = vdist(p1, p2);
         double ttt = (da + db + dc) * (db + dc - da) * (dc + da - db) * (da + db - dc);
         if (ttt > 0) {
           area += 0.25 * sqrt(ttt);
           if (A.vgrad) {
             // area = |n| / 2, n = (P1 - P0) x (P2 - P0): d area / d P0 = (P1 - P2) x n / (2 |n|), cyclic
-            const double e1[3] = {P1[0] - P0[0], P1[1] - P0[1], P1[2] - P0[2]};
-            const double e2[3] = {P2[0] - P0[0], P2[1] - P0[1], P2[2] - P0[2]};
-            double nn[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+            const double f1[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
+            const double f2[3] = {p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2]};
+            double nn[3] = {f1[1] * f2[2] - f1[2] * f2[1], f1[2] * f2[0] - f1[0] * f2[2], f1[0] * f2[1] - f1[1] * f2[0]};
             const double nl = sqrt(nn[0] * nn[0] + nn[1] * nn[1] + nn[2] * nn[2]);
             if (nl > 0) {
-              for (int d = 0; d < 3; d++) nn[d] /= 2.0 * nl;
-              const int32_t vv[3] = {v0, v1, v2};
-              const double* PP[3] = {P0, P1, P2};
-              for (int t3 = 0; t3 < 3; t3++) {
-                if (vv[t3] >= A.n_analytic) continue;
-                const double* Pa = PP[(t3 + 1) % 3];
-                const double* Pb = PP[(t3 + 2) % 3];
-                const double dd[3] = {Pa[0] - Pb[0], Pa[1] - Pb[1], Pa[2] - Pb[2]};
-                const int ax = A.vkey[vv[t3]].w;  // ray axis of an analytic vertex = its edge direction
-                const int a1 = (ax + 1) % 3, a2 = (ax + 2) % 3;
-                const double comp = dd[a1] * nn[a2] - dd[a2] * nn[a1];
-                if (comp != 0.0) atomicAdd(A.vgrad + vv[t3], comp);
-              }
+              const double h = 0.5 / nl;
+              nn[0] *= h;
+              nn[1] *= h;
+              nn[2] *= h;
+              // d area / d (position of vertex vv along the axis of its cube edge ev, which is
+              // the ray an analytic vertex moves on): ((Pa - Pb) x n / (2 |n|)) along that axis
+              const auto add = [&](int32_t vv, int ev, double dx, double dy, double dz) {
+                if (vv >= A.n_analytic) return;
+                double comp;
+                if (ev >= 8) comp = dx * nn[1] - dy * nn[0];        // z
+                else if (ev & 1) comp = dz * nn[0] - dx * nn[2];    // y
+                else comp = dy * nn[2] - dz * nn[1];                // x
+                if (comp != 0.0) atomicAdd(A.vgrad + vv, comp);
+              };
+              add(v0, e0, p1[0] - p2[0], p1[1] - p2[1], p1[2] - p2[2]);
+              add(v1, e1, p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2]);
+              add(v2, e2, p0[0] - p1[0], p0[1] - p1[1], p0[2] - p1[2]);
             }
           }
         }
