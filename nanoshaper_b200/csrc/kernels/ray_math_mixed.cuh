@@ -100,19 +100,24 @@ __device__ __forceinline__ bool feasible_mixed(const double* P, int kind, int fi
     return true;
   }
   if (kind == NS_POINT) {
-    for (int q = 0; q < cnt; q++) {
-      float4 s = lp[q];
+    // the hit is feasible unless it lies inside one of the clip spheres; four entries are loaded
+    // ahead of their tests so that the loads of a group overlap
+    const auto inside = [&](float4 s, int q) {
       float ex = pl32[0] - s.x, ey = pl32[1] - s.y, ez = pl32[2] - s.z;
       float dd = (ex * ex + ey * ey) + (ez * ez - s.w);
-      if (fabsf(dd) > kSphereTol) {
-        if (dd < 0.f) return false;
-        continue;
-      }
+      if (fabsf(dd) > kSphereTol) return dd < 0.f;
       double4 sd = pl[q];
       double d64 = (sd.x - p64[0]) * (sd.x - p64[0]) + (sd.y - p64[1]) * (sd.y - p64[1]) + (sd.z - p64[2]) * (sd.z - p64[2]);
       d64 -= sd.w;
-      if (d64 < 0) return false;
+      return d64 < 0;
+    };
+    int q = 0;
+    for (; q + 4 <= cnt; q += 4) {
+      const float4 s0 = lp[q], s1 = lp[q + 1], s2 = lp[q + 2], s3 = lp[q + 3];
+      if (inside(s0, q) || inside(s1, q + 1) || inside(s2, q + 2) || inside(s3, q + 3)) return false;
     }
+    for (; q < cnt; q++)
+      if (inside(lp[q], q)) return false;
     return true;
   }
   double sir = P[kSir];

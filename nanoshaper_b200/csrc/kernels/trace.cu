@@ -564,40 +564,64 @@ __global__ void __launch_bounds__(kTraceThreads) k_fill(TraceCtx C, HitStore hs)
     // d volume / d patch parameters, interval end by interval end (the pairing rule of
     // make_pairs), summed over runs of lanes on the same patch before the atomics
     const double W = S.A * C.out.grad_scale;
-    double xb[3];
-    xb[rs.fd] = gcoord(g, rs.fd, valid ? m : 0) + rs.delta;
-    xb[rs.ld] = gcoord(g, rs.ld, valid ? n : 0) + rs.delta;
-    xb[rs.vc] = 0.0;
+    __syncwarp();  // the lanes read each other's sorted hit columns below
     const int nhw = (valid && !ovf && nh > 0 && (nh & 1) == 0) ? nh : 0;
     const int maxn = (int)__reduce_max_sync(0xffffffffu, (unsigned)nhw);
-    for (int q = 0; q < maxn; q += 2) {
-      bool ok = q + 1 < nhw;
-      double t1 = 0.0, t2 = 0.0;
-      if (ok) {
-        t1 = col[q * kThreads];
-        t2 = col[(q + 1) * kThreads];
-        ok = fabs(t2 - t1) >= NS_EPS_INT;
-      }
-      for (int e = 0; e < 2; e++) {
-        double gk[NS_GRAD_PER_PATCH];
-        int32_t pid = -1;
-        if (ok) {
-          pid = slot_pid(pcol[(q + e) * kThreads]);
-          double x[3] = {xb[0], xb[1], xb[2]};
-          x[rs.vc] = pa_vc + dirl * (e ? t2 : t1);
-          if (hit_grad(C.P.f64 + (int64_t)NS_PATCH_F64 * pid, C.P.i32[NS_PATCH_I32 * pid], C.P.probe, x, rs.vc, gk)) {
-            const double w = e ? W : -W;
+    // The warp's interval ends, 32 at a time: end q of every ray that has one (level q), levels in
+    // order, so that neighbouring lanes hold neighbouring rays (which mostly hit the same patch).
+    // Lane q keeps the ray mask of level q.
+    unsigned lvl_mask = 0;
+    for (int q = 0; q < maxn; q++) {
+      const unsigned mq = __ballot_sync(0xffffffffu, nhw > q);
+      if (lane == q) lvl_mask = mq;
+    }
+    const int lvl_size = __popc(lvl_mask);
+    int lincl = lvl_size;
 #pragma unroll
-            for (int k = 0; k < NS_GRAD_PER_PATCH; k++) gk[k] *= w;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, lincl, o);
+      if (lane >= o) lincl += v;
+    }
+    const int nends = __shfl_sync(0xffffffffu, lincl, 31);
+    for (int kb = 0; kb < nends; kb += 32) {
+      const int k = kb + lane;
+      const int kk = k < nends ? k : nends - 1;
+      int q = 0;
+#pragma unroll
+      for (int step = 16; step; step >>= 1) {
+        const int x = __shfl_sync(0xffffffffu, lincl, q + step - 1);
+        if (x <= kk) q += step;
+      }
+      const int idx = kk - __shfl_sync(0xffffffffu, lincl - lvl_size, q);
+      unsigned mq = __shfl_sync(0xffffffffu, lvl_mask, q);
+      for (int c2 = 0; c2 < idx; c2++) mq &= mq - 1;
+      const int r = __ffs(mq) - 1;  // the ray (lane) of this end
+      const int64_t rid_r = __shfl_sync(0xffffffffu, rid, r);
+      double gk[NS_GRAD_PER_PATCH];
+      int32_t pid = -1;
+      if (k < nends) {
+        const double* cr = s_hit + warp * 32 + r;
+        const double t1 = cr[(q & ~1) * kThreads], t2 = cr[(q | 1) * kThreads];
+        if (fabs(t2 - t1) >= NS_EPS_INT) {
+          const uint8_t sl = s_slot[(q * kThreads) + warp * 32 + r];
+          pid = hs.pid[(int64_t)sl * hs.nrays + rid_r];
+          double x[3];
+          x[rs.fd] = gcoord(g, rs.fd, tm * kTileM + r) + rs.delta;
+          x[rs.ld] = gcoord(g, rs.ld, n) + rs.delta;
+          x[rs.vc] = pa_vc + dirl * ((q & 1) ? t2 : t1);
+          if (hit_grad(C.P.f64 + (int64_t)NS_PATCH_F64 * pid, C.P.i32[NS_PATCH_I32 * pid], C.P.probe, x, rs.vc, gk)) {
+            const double w = (q & 1) ? W : -W;
+#pragma unroll
+            for (int c3 = 0; c3 < NS_GRAD_PER_PATCH; c3++) gk[c3] *= w;
           } else {
             pid = -1;
           }
         }
-        if (pid < 0)
-#pragma unroll
-          for (int k = 0; k < NS_GRAD_PER_PATCH; k++) gk[k] = 0.0;
-        warp_add_grad(pid, gk, C.out.gvol);
       }
+      if (pid < 0)
+#pragma unroll
+        for (int c3 = 0; c3 < NS_GRAD_PER_PATCH; c3++) gk[c3] = 0.0;
+      warp_add_grad(pid, gk, C.out.gvol);
     }
     if (valid && !ovf)
       np = make_pairs(col, kThreads, nh, pa_vc, dirl, g.mn[rs.vc], g.scale, mc, &vol, pcol, (GradCtx*)nullptr,
