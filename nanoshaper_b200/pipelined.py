@@ -8,6 +8,10 @@ the other copies the next, so the copy engines and the SMs work at the same time
 one batch (``nsg_set_batch`` / ``nsg_upload_batch`` / ``nsg_upload_atoms``, then the ray cast,
 the triangulation and the atom derivatives).  The results are the same as one batch of the whole
 ensemble.
+
+Two details shorten the start of the pipeline, when no kernel has work yet: the first chunk is half
+the size of the others, and one upload is in flight at a time (a lock), so that each copy has the
+whole host link and the first chunk's kernels start as early as possible.
 """
 from __future__ import annotations
 
@@ -55,13 +59,20 @@ class PipelinedBatches:
         if not surfaces:
             raise ValueError("empty ensemble")
         n_chunks = max(1, min(n_chunks, len(surfaces)))
-        bounds = np.linspace(0, len(surfaces), n_chunks + 1).astype(int)
+        # chunk weights 1/2, 1, 1, ...: a short first chunk starts the kernels early
+        weights = np.array([0.5] + [1.0] * (n_chunks - 1))
+        bounds = np.round(np.concatenate([[0.0], np.cumsum(weights)]) / weights.sum() * len(surfaces)).astype(int)
+        bounds = np.maximum.accumulate(bounds)
+        keep = [0] + [i for i in range(1, len(bounds)) if bounds[i] > bounds[i - 1]]
+        bounds = bounds[keep]
+        n_chunks = len(bounds) - 1
         self.chunks = [_Chunk(surfaces, int(bounds[i]), int(bounds[i + 1])) for i in range(n_chunks)]
         self.n = len(surfaces)
         self.prec = S.PRECISIONS[precision]
         s0 = surfaces[0]
         self.flags = (N.STATUS if s0.delphi.buildStatus else 0) | N.ACCURATE_TRIANGULATION | N.GRAD
         self.ctxs = [S.Context(device), S.Context(device)]
+        self._upload_lock = threading.Lock()
         if tuning is not None:
             p = np.ascontiguousarray(tuning, np.int32)
             for c in self.ctxs:
@@ -77,12 +88,13 @@ class PipelinedBatches:
 
     def _run_chunk(self, c, ch: _Chunk) -> None:
         L = N.lib()
-        N.check(L.nsg_set_batch(c, ch.hi - ch.lo, ch.grids), "set_batch")
-        N.check(L.nsg_upload_batch(c, N.ptr(ch.patch_off), ch.pin["f64"].data_ptr(), ch.pin["i32"].data_ptr(),
-                                   N.ptr(ch.pool_off), ch.pin["pool"].data_ptr(), ch.pin["flag"].data_ptr(), ch.probe),
-                "upload_batch")
-        N.check(L.nsg_upload_atoms(c, N.ptr(ch.atom_off), ch.pin["atoms"].data_ptr(),
-                                   ch.pin["patch_atoms"].data_ptr()), "upload atoms")
+        with self._upload_lock:
+            N.check(L.nsg_set_batch(c, ch.hi - ch.lo, ch.grids), "set_batch")
+            N.check(L.nsg_upload_batch(c, N.ptr(ch.patch_off), ch.pin["f64"].data_ptr(), ch.pin["i32"].data_ptr(),
+                                       N.ptr(ch.pool_off), ch.pin["pool"].data_ptr(), ch.pin["flag"].data_ptr(),
+                                       ch.probe), "upload_batch")
+            N.check(L.nsg_upload_atoms(c, N.ptr(ch.atom_off), ch.pin["atoms"].data_ptr(),
+                                       ch.pin["patch_atoms"].data_ptr()), "upload atoms")
         v = ctypes.c_double()
         N.check(L.nsg_raycast(c, self.flags, self.prec, ctypes.byref(v)), "raycast")
         a = ctypes.c_double()
