@@ -325,18 +325,6 @@ int scan_counts(nsg_ctx* c, const In* in, int64_t n, int64_t* out, int64_t* tota
   return NSG_OK;
 }
 
-int reduce_sum(nsg_ctx* c, const double* in, int64_t n, double* host_out) {
-  if (n == 0) { *host_out = 0; return NSG_OK; }
-  CK(c->red_out.ensure(sizeof(double)));
-  size_t tb = 0;
-  CK(cub::DeviceReduce::Sum(nullptr, tb, in, c->red_out.as<double>(), n, c->stream));
-  CK(c->temp.ensure(tb));
-  tb = c->temp.cap;
-  CK(cub::DeviceReduce::Sum(c->temp.p, tb, in, c->red_out.as<double>(), n, c->stream));
-  CK(cudaMemcpyAsync(host_out, c->red_out.p, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
-  return NSG_OK;
-}
 
 // Window-area sum of a panel (the bound of its candidate count).
 int panel_area(nsg_ctx* c, int panel) {
@@ -1013,25 +1001,20 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
     if (errflag == 7) { c->def_cap *= 2; continue; }
     return fail(NSG_ERR_CAPACITY, errflag == 1 ? "too many overflow rays" : "ray hit capacity exceeded");
   }
-  // volume: A * sum of interval lengths over the ray sets / number of ray sets, per structure
+  // volume: A * sum of interval lengths over the ray sets / number of ray sets, per structure; the
+  // per-structure sums run in an order fixed by the structure alone, so a structure's volume does
+  // not depend on the batch it is part of
   const int32_t nb = c->nstruct;
   std::vector<double> vsum(nb, 0.0);
   int flag_sum = 0;
-  if (nb > 1) CK(c->vol_struct.ensure(nb * sizeof(double)));
+  CK(c->vol_struct.ensure(nb * sizeof(double)));
   for (int s = 0; s < 4; s++) {
     if ((s == 0 && !do_status) || (s > 0 && !do_mc)) continue;
-    if (nb == 1) {
-      double v = 0;
-      int rc = reduce_sum(c, c->vol_ray[s].as<double>(), c->rays_tot[s], &v);
-      if (rc) return rc;
-      vsum[0] += v;
-    } else {
-      LAUNCH(nsg::launch_segment_sums(c->vol_ray[s].as<double>(), B.ray_base[s], nullptr, nb,
-                                      c->vol_struct.as<double>(), flag_sum > 0, c->stream));
-    }
+    LAUNCH(nsg::launch_segment_sums(c->vol_ray[s].as<double>(), B.ray_base[s], nullptr, nb,
+                                    c->vol_struct.as<double>(), flag_sum > 0, c->stream));
     flag_sum++;
   }
-  if (nb > 1 && flag_sum) {
+  if (flag_sum) {
     CK(cudaMemcpyAsync(vsum.data(), c->vol_struct.p, nb * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
   }
@@ -1277,20 +1260,14 @@ int nsg_triangulate(nsg_ctx* c, double* area_out, int64_t* nverts, int64_t* ntri
   LAUNCH(nsg::launch_mc_tris(M, 1, c->stream));
   if (grad) LAUNCH(nsg::launch_grad_vert(M, c->stream));
   c->have_garea = grad;
-  double area = 0;
-  if (c->nstruct == 1) {
-    rc = reduce_sum(c, c->cube_area.as<double>(), n_act, &area);
-    if (rc) return rc;
-    c->areas[0] = area;
-  } else {
-    CK(c->area_struct.ensure(c->nstruct * sizeof(double)));
-    LAUNCH(nsg::launch_segment_sums(c->cube_area.as<double>(), c->row_act_off.as<int64_t>(), B.row_base, c->nstruct,
-                                    c->area_struct.as<double>(), false, c->stream));
-    CK(cudaMemcpyAsync(c->areas.data(), c->area_struct.p, c->nstruct * sizeof(double), cudaMemcpyDeviceToHost,
-                       c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    area = c->areas[0];
-  }
+  // per-structure areas in an order fixed by the structure alone (independent of the batch)
+  CK(c->area_struct.ensure(c->nstruct * sizeof(double)));
+  LAUNCH(nsg::launch_segment_sums(c->cube_area.as<double>(), c->row_act_off.as<int64_t>(), B.row_base, c->nstruct,
+                                  c->area_struct.as<double>(), false, c->stream));
+  CK(cudaMemcpyAsync(c->areas.data(), c->area_struct.p, c->nstruct * sizeof(double), cudaMemcpyDeviceToHost,
+                     c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  const double area = c->areas[0];
   stage_end(c, kStageMC);
   c->n_analytic = n_an;
   c->n_vert = n_v;

@@ -718,6 +718,9 @@ __global__ void __launch_bounds__(kTraceThreads) k_fill(TraceCtx C, HitStore hs)
     vhi = oh > vhi ? oh : vhi;
   }
   if (vlo > vhi) return;
+  // 32 positions at a time: every lane builds the 32-bit membership word of its ray over
+  // [v0, v0 + 31] from its intervals, 32 ballots transpose the words so that lane l holds the mask
+  // of the 32 rays at position v0 + l, and the lanes clear their rows' bits in parallel
   int q = 0;
   int64_t qa = 0, qb = -1;
   if (np > 0) {
@@ -725,23 +728,37 @@ __global__ void __launch_bounds__(kTraceThreads) k_fill(TraceCtx C, HitStore hs)
     qb = (int64_t)rintp((col[kThreads] - vmin) * g.scale);
   }
   const int64_t m0 = tm * kTileM;
-  for (int64_t v = vlo; v <= vhi; v++) {
-    while (q < np && qb < v) {
+  for (int64_t v0 = vlo; v0 <= vhi; v0 += 32) {
+    const int64_t v1 = v0 + 31;
+    unsigned mem = 0;
+    while (q < np && qa < v1) {
+      // positions qa < v <= qb of the current interval that fall in [v0, v1]
+      const int64_t lo = qa + 1 > v0 ? qa + 1 : v0, hi = qb < v1 ? qb : v1;
+      if (lo <= hi) {
+        const int s0 = (int)(lo - v0), s1 = (int)(hi - v0);
+        mem |= (s1 - s0 == 31) ? 0xffffffffu : (((1u << (s1 - s0 + 1)) - 1u) << s0);
+      }
+      if (qb > v1) break;  // the interval continues in the next window
       q++;
       if (q < np) {
         qa = (int64_t)rintp((col[(2 * q) * kThreads] - vmin) * g.scale);
         qb = (int64_t)rintp((col[(2 * q + 1) * kThreads] - vmin) * g.scale);
       }
     }
-    bool inside = q < np && qa < v && v <= qb;
-    unsigned mask = __ballot_sync(0xffffffffu, inside);
-    if (lane == 0 && mask) {
-      int64_t f0 = (rs.panel == 1) ? ((v * NY + n) * NX + m0) : ((n * NY + v) * NX + m0);
+    unsigned mask = 0;
+#pragma unroll
+    for (int b = 0; b < 32; b++) {
+      const unsigned mb = __ballot_sync(0xffffffffu, (mem >> b) & 1u);
+      if (lane == b) mask = mb;
+    }
+    const int64_t v = v0 + lane;
+    if (mask && v <= vhi) {
+      const int64_t f0 = (rs.panel == 1) ? ((v * NY + n) * NX + m0) : ((n * NY + v) * NX + m0);
       if (f0 >= 0) {
-        int64_t w = f0 >> 5;
-        int s = (int)(f0 & 31);
-        if (w < nwords) atomicAnd(bits + w, ~(mask << s));
-        if (s && w + 1 < nwords) atomicAnd(bits + w + 1, ~(mask >> (32 - s)));
+        const int64_t w = f0 >> 5;
+        const int sh = (int)(f0 & 31);
+        if (w < nwords) atomicAnd(bits + w, ~(mask << sh));
+        if (sh && w + 1 < nwords) atomicAnd(bits + w + 1, ~(mask >> (32 - sh)));
       }
     }
   }
