@@ -153,14 +153,15 @@ __device__ __forceinline__ int intersect_mixed(const double* f, int kind, int fi
     p64[fd] = pa[fd];
     p64[ld] = pa[ld];
     p64[vc] = xs[i];
-    if (feasible_mixed(f, kind, first, cnt, P.pool, P.pool32, P.flag, pl, p64)) t[out++] = (xs[i] - pa[vc]) * inv_dir;
+    if (feasible_mixed<kTorus>(f, kind, first, cnt, P.pool, P.pool32, P.flag, pl, p64))
+      t[out++] = (xs[i] - pa[vc]) * inv_dir;
   }
   return out;
 }
 
 // One thread per candidate pair of one type: intersection, feasibility, hit filing.
 template <int PN, bool kTorus, bool kMixed>
-__global__ void __launch_bounds__(256) k_isect(TraceCtx C, CandOut co, HitStore hs) {
+__device__ __forceinline__ void isect_body(const TraceCtx& C, const CandOut& co, const HitStore& hs) {
   constexpr int fd = Ax<PN>::fd, ld = Ax<PN>::ld, vc = Ax<PN>::vc;
   const int64_t ncand = *(co.count + (kTorus ? 1 : 0));
   const int2* list = kTorus ? co.tor : co.sph;
@@ -218,6 +219,19 @@ __global__ void __launch_bounds__(256) k_isect(TraceCtx C, CandOut co, HitStore 
         if (hs.pid) hs.pid[(int64_t)(pos + i) * hs.nrays + rid] = (int32_t)pid;
       }
   }
+}
+
+// The double-precision kernels (the FP64 path and the deferred lists of the mixed path) and the
+// mixed-precision ones; the latter ask for enough blocks per SM to keep the sphere kernel, which
+// waits on its loads, and the torus kernel at full residency.
+template <int PN, bool kTorus>
+__global__ void __launch_bounds__(256) k_isect(TraceCtx C, CandOut co, HitStore hs) {
+  isect_body<PN, kTorus, false>(C, co, hs);
+}
+
+template <int PN, bool kTorus>
+__global__ void __launch_bounds__(256, kTorus ? 3 : 6) k_isect_mixed(TraceCtx C, CandOut co, HitStore hs) {
+  isect_body<PN, kTorus, true>(C, co, hs);
 }
 
 }  // namespace

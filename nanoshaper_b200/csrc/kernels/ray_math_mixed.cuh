@@ -88,19 +88,21 @@ __device__ __forceinline__ double plane_value(float4 lw, const double4* pl, int 
 
 // Feasibility with FP32 tests on patch-local coordinates (pl32 = hit - patch centre) and FP64
 // re-evaluation of undecided tests (p64 = absolute hit point).
+// kTorus: the patch is an edge (torus) patch; otherwise a point (atom) or face (probe) patch.
+template <bool kTorus>
 __device__ __forceinline__ bool feasible_mixed(const double* P, int kind, int first, int cnt,
                                                const double4* __restrict__ pool, const float4* __restrict__ pool32,
                                                const int8_t* __restrict__ pflag, const float* pl32,
                                                const double* p64) {
   const double4* pl = pool + first;
   const float4* lp = pool32 + first;
-  if (kind == NS_FACE_REG || kind == NS_FACE_SING) {
+  if (!kTorus && (kind == NS_FACE_REG || kind == NS_FACE_SING)) {
     for (int q = 0; q < cnt; q++)
       if (plane_value(lp[q], pl, q, pl32, p64) > 0) return false;
     return true;
   }
-  if (kind == NS_POINT) {
-    // the hit is feasible unless it lies inside one of the clip spheres; four entries are loaded
+  if (!kTorus) {
+    // a point patch: the hit is feasible unless it lies inside one of the clip spheres; four entries are loaded
     // ahead of their tests so that the loads of a group overlap
     const auto inside = [&](float4 s, int q) {
       float ex = pl32[0] - s.x, ey = pl32[1] - s.y, ez = pl32[2] - s.z;

@@ -263,9 +263,10 @@ __device__ __forceinline__ void clear_bits_range(uint32_t* bits, int64_t nwords,
 //    reserves the slots; the (ray, patch) pairs follow in row-major order, in the sphere list
 //    (atoms and probes) or the torus list; a patch's candidates stay contiguous, so the
 //    intersection kernels read its record once per warp;
-//  * k_isect<torus, mixed>: one thread per candidate pair, sphere and torus pairs in separate
-//    launches so that both run converged with their own register budget; hits are filed into
-//    the ray's slots of a slot-major hit store through a per-ray atomic counter;
+//  * k_isect<torus> (double precision) and k_isect_mixed<torus> (trace_mixed.cu): one thread per
+//    candidate pair, sphere and torus pairs in separate launches so that both run converged with
+//    their own register budget; hits are filed into the ray's slots of a slot-major hit store
+//    through a per-ray atomic counter;
 //  * k_fill: one CTA per 32x4 ray tile loads each ray's hits, sorts them and performs the
 //    interval fill.
 // A k_cand batch of 32 patches, staged in shared memory (structure of arrays, one entry per lane
@@ -475,11 +476,11 @@ void launch_isect(const TraceCtx& C, const CandOut& co, const HitStore& hs, int 
     launch_isect_mixed<PN>(C, co, hs, tp, s);
     // the deferred candidates, in double precision (few: a small grid)
     const CandOut dco{co.dsph, co.dtor, co.dcap, co.dcount, nullptr, nullptr, 0, nullptr};
-    k_isect<PN, false, false><<<148, 256, 0, s>>>(C, dco, hs);
-    k_isect<PN, true, false><<<148, 256, 0, s>>>(C, dco, hs);
+    k_isect<PN, false><<<148, 256, 0, s>>>(C, dco, hs);
+    k_isect<PN, true><<<148, 256, 0, s>>>(C, dco, hs);
   } else {
-    k_isect<PN, false, false><<<ig, it, 0, s>>>(C, co, hs);
-    k_isect<PN, true, false><<<ig, it, 0, s>>>(C, co, hs);
+    k_isect<PN, false><<<ig, it, 0, s>>>(C, co, hs);
+    k_isect<PN, true><<<ig, it, 0, s>>>(C, co, hs);
   }
 }
 
@@ -678,26 +679,21 @@ __global__ void __launch_bounds__(kTraceThreads) k_fill(TraceCtx C, HitStore hs)
   }
   const double vmin = g.mn[rs.vc];
   if (rs.panel == 0) {
-    // row bits (i, j = m, k = n), i in (a, b]
-    for (int r = 0; r < 32; r++) {
-      int np_r = __shfl_sync(0xffffffffu, np, r);
-      if (np_r == 0) continue;
-      const double* cr = s_hit + warp * 32 + r;
-      int64_t j = tm * kTileM + r;
-      int64_t f0 = (n * NY + j) * NX;
-      for (int q = 0; q < np_r; q++) {
-        int64_t a = (int64_t)rintp((cr[(2 * q) * kThreads] - vmin) * g.scale);
-        int64_t b = (int64_t)rintp((cr[(2 * q + 1) * kThreads] - vmin) * g.scale);
+    // row bits (i, j = m, k = n), i in (a, b]: every lane clears the runs of its own row
+    if (valid && !ovf) {
+      const int64_t f0 = (n * NY + m) * NX;
+      const int64_t maxb = nwords * 32 - 1;
+      for (int q = 0; q < np; q++) {
+        const int64_t a = (int64_t)rintp((col[(2 * q) * kThreads] - vmin) * g.scale);
+        const int64_t b = (int64_t)rintp((col[(2 * q + 1) * kThreads] - vmin) * g.scale);
         int64_t lo = f0 + a + 1, hi = f0 + b;
         if (lo < 0) lo = 0;
-        int64_t maxb = nwords * 32 - 1;
         if (hi > maxb) hi = maxb;
-        if (hi < lo) continue;
-        for (int64_t w = (lo >> 5) + lane; w <= (hi >> 5); w += 32) {
-          int64_t wl = w << 5;
-          int s = (int)(lo > wl ? lo - wl : 0);
-          int e = (int)(hi < wl + 31 ? hi - wl : 31);
-          uint32_t mask = (e - s == 31) ? 0xffffffffu : (((1u << (e - s + 1)) - 1u) << s);
+        for (int64_t w = lo >> 5; w <= (hi >> 5) && hi >= lo; w++) {
+          const int64_t wl = w << 5;
+          const int s0 = (int)(lo > wl ? lo - wl : 0);
+          const int s1 = (int)(hi < wl + 31 ? hi - wl : 31);
+          const uint32_t mask = (s1 - s0 == 31) ? 0xffffffffu : (((1u << (s1 - s0 + 1)) - 1u) << s0);
           atomicAnd(bits + w, ~mask);
         }
       }

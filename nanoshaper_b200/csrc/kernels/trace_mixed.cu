@@ -8,8 +8,8 @@ template <int PN>
 void launch_isect_mixed(const TraceCtx& C, const CandOut& co, const HitStore& hs, const TuneParams& tp,
                         cudaStream_t s) {
   const int ig = 148 * tp.isect_bpsm, it = tp.isect_threads;
-  k_isect<PN, false, true><<<ig, it, 0, s>>>(C, co, hs);
-  k_isect<PN, true, true><<<ig, it, 0, s>>>(C, co, hs);
+  k_isect_mixed<PN, false><<<ig, it, 0, s>>>(C, co, hs);
+  k_isect_mixed<PN, true><<<ig, it, 0, s>>>(C, co, hs);
 }
 
 template void launch_isect_mixed<0>(const TraceCtx&, const CandOut&, const HitStore&, const TuneParams&, cudaStream_t);
