@@ -80,7 +80,7 @@ struct nsg_ctx {
   int32_t patch_nstruct = 0;  // structures the uploaded patches belong to
   bool patch_struct_valid = false;
   std::vector<double> volumes, areas;
-  DevBuf vol_struct, area_struct;
+  DevBuf vol_struct, area_struct, seg_part;
   // patches
   int64_t np = 0, npool = 0;
   double probe = 1.4;
@@ -452,7 +452,7 @@ int nsg_ctx_destroy(nsg_ctx* c) {
   for (int i = 0; i < 3; i++) { c->tile_cnt[i].release(); c->tile_off[i].release(); c->tile_list[i].release(); }
   c->d_sd.release(); c->d_patch_struct.release(); c->d_mc_base.release(); c->d_row_base.release();
   c->d_row_chunks.release();
-  c->vol_struct.release(); c->area_struct.release();
+  c->vol_struct.release(); c->area_struct.release(); c->seg_part.release();
   for (int i = 0; i < 3; i++) c->d_tile_struct[i].release();
   for (int i = 0; i < 4; i++) c->d_ray_base[i].release();
   for (int i = 0; i < 4; i++) {
@@ -1008,10 +1008,11 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
   std::vector<double> vsum(nb, 0.0);
   int flag_sum = 0;
   CK(c->vol_struct.ensure(nb * sizeof(double)));
+  CK(c->seg_part.ensure((size_t)nb * nsg::kSegParts * sizeof(double)));
   for (int s = 0; s < 4; s++) {
     if ((s == 0 && !do_status) || (s > 0 && !do_mc)) continue;
     LAUNCH(nsg::launch_segment_sums(c->vol_ray[s].as<double>(), B.ray_base[s], nullptr, nb,
-                                    c->vol_struct.as<double>(), flag_sum > 0, c->stream));
+                                    c->vol_struct.as<double>(), c->seg_part.as<double>(), flag_sum > 0, c->stream));
     flag_sum++;
   }
   if (flag_sum) {
@@ -1262,8 +1263,9 @@ int nsg_triangulate(nsg_ctx* c, double* area_out, int64_t* nverts, int64_t* ntri
   c->have_garea = grad;
   // per-structure areas in an order fixed by the structure alone (independent of the batch)
   CK(c->area_struct.ensure(c->nstruct * sizeof(double)));
+  CK(c->seg_part.ensure((size_t)c->nstruct * nsg::kSegParts * sizeof(double)));
   LAUNCH(nsg::launch_segment_sums(c->cube_area.as<double>(), c->row_act_off.as<int64_t>(), B.row_base, c->nstruct,
-                                  c->area_struct.as<double>(), false, c->stream));
+                                  c->area_struct.as<double>(), c->seg_part.as<double>(), false, c->stream));
   CK(cudaMemcpyAsync(c->areas.data(), c->area_struct.p, c->nstruct * sizeof(double), cudaMemcpyDeviceToHost,
                      c->stream));
   CK(cudaStreamSynchronize(c->stream));

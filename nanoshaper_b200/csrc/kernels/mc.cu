@@ -11,7 +11,8 @@
 // Marching cubes: cubes (i,j,k) in [1, N-2]^3 are classified from the 8 insideness bits; active
 // cubes add an edge-midpoint vertex to their own edges 5, 6, 10 that carry no analytic vertex,
 // in (k, j, i, edge) order, appended after the analytic ones (getVertices :8002-8327); a second
-// pass emits the case-table triangles with reversed winding and sums their Heron areas
+// pass emits the case-table triangles with reversed winding and sums their areas (the reference
+// sums Heron areas; here |cross product| / 2, the same quantity)
 // (triangulationKernel :9075-9318, getTriangles :14559-14780).  Triangles with an edge without a
 // vertex are skipped, as the reference does.
 #include <cub/cub.cuh>
@@ -327,9 +328,6 @@ __device__ __forceinline__ int64_t edge_vertex(const MCArgs& A, const StructDev&
   return midpoint_vertex(A, S, dir, x, y, z);
 }
 
-__device__ __forceinline__ double vdist(const double* a, const double* b) {
-  return sqrt((a[0] - b[0]) * (a[0] - b[0]) + (a[1] - b[1]) * (a[1] - b[1]) + (a[2] - b[2]) * (a[2] - b[2]));
-}
 
 // One thread per active cube.  Pass 0 finds the vertex of every cut edge, counts the triangles
 // and sums their areas (and, in gradient mode, their derivatives with respect to the analytic
@@ -377,17 +375,17 @@ __global__ void __launch_bounds__(128) k_mc_tris(MCArgs A, int emit) {
         const double* P1 = A.vpos + 3 * (int64_t)v1;
         const double* P2 = A.vpos + 3 * (int64_t)v2;
         const double p0[3] = {P0[0], P0[1], P0[2]}, p1[3] = {P1[0], P1[1], P1[2]}, p2[3] = {P2[0], P2[1], P2[2]};
-        double da = vdist(p0, p1), db = vdist(p0, p2), dc = vdist(p1, p2);
-        double ttt = (da + db + dc) * (db + dc - da) * (dc + da - db) * (da + db - dc);
-        if (ttt > 0) {
-          area += 0.25 * sqrt(ttt);
+        // area = |n| / 2, n = (P1 - P0) x (P2 - P0): the area the reference computes with Heron's
+        // formula (getTriangles, src/Surface.cpp:14559-14780), with one square root instead of four
+        const double f1[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
+        const double f2[3] = {p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2]};
+        double nn[3] = {f1[1] * f2[2] - f1[2] * f2[1], f1[2] * f2[0] - f1[0] * f2[2], f1[0] * f2[1] - f1[1] * f2[0]};
+        const double nl = sqrt(nn[0] * nn[0] + nn[1] * nn[1] + nn[2] * nn[2]);
+        if (nl > 0) {
+          area += 0.5 * nl;
           if (A.vgrad) {
-            // area = |n| / 2, n = (P1 - P0) x (P2 - P0): d area / d P0 = (P1 - P2) x n / (2 |n|), cyclic
-            const double f1[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
-            const double f2[3] = {p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2]};
-            double nn[3] = {f1[1] * f2[2] - f1[2] * f2[1], f1[2] * f2[0] - f1[0] * f2[2], f1[0] * f2[1] - f1[1] * f2[0]};
-            const double nl = sqrt(nn[0] * nn[0] + nn[1] * nn[1] + nn[2] * nn[2]);
-            if (nl > 0) {
+            // d area / d P0 = (P1 - P2) x n / (2 |n|), cyclic
+            {
               const double h = 0.5 / nl;
               nn[0] *= h;
               nn[1] *= h;

@@ -197,9 +197,11 @@ cudaError_t launch_trace_overflow(const PatchDev& P, const BatchDev& B, int set,
                                   int32_t* pscratch, int precision, cudaStream_t s);
 
 // reduce.cu: out[b] (+)= sum of v over structure b's segment [base[i(b)], base[i(b+1)]) with
-// i(b) = idx[b] (idx given) or b; one CTA per structure, fixed summation order.
+// i(b) = idx[b] (idx given) or b, in a summation order fixed by the segment alone; part is scratch
+// for n * kSegParts doubles.
+constexpr int kSegParts = 64;
 cudaError_t launch_segment_sums(const double* v, const int64_t* base, const int64_t* idx, int n, double* out,
-                                bool accumulate, cudaStream_t s);
+                                double* part, bool accumulate, cudaStream_t s);
 
 // reduce.cu, batch uploads: per-patch structure and batch-wide pool index (err set on a pool
 // range outside the structure's pool); batch-wide patch atom indices (err on an index outside

@@ -1,6 +1,8 @@
-// Per-structure sums of a batch (interval lengths per ray, triangle areas per active cube): one
-// CTA per structure sums its contiguous segment in a fixed order, so that the result does not
-// depend on scheduling.
+// Per-structure sums of a batch (interval lengths per ray, triangle areas per active cube) in an
+// order fixed by the structure alone, so that the result depends neither on scheduling nor on the
+// batch the structure is part of: kSegParts CTAs per structure sum interleaved blocks of its
+// segment (by the element's index within the segment), and one thread per structure adds their
+// partial sums in CTA order.
 #include "pipeline.h"
 
 namespace nsg {
@@ -9,31 +11,42 @@ namespace {
 
 constexpr int kSumThreads = 256;
 
-// out[b] (+)= sum of v[lo .. hi), lo = base[idx ? idx[b] : b], hi = base[idx ? idx[b+1] : b+1].
-__global__ void __launch_bounds__(kSumThreads) k_segment_sums(const double* __restrict__ v,
-                                                               const int64_t* __restrict__ base,
-                                                               const int64_t* __restrict__ idx, double* out,
-                                                               int accumulate) {
-  __shared__ double part[kSumThreads];
-  const int b = blockIdx.x;
+// part[b * kSegParts + k] = sum over the elements of segment b whose index i within the segment
+// has (i / kSumThreads) % kSegParts == k; lo = base[idx ? idx[b] : b], hi = base[idx ? idx[b+1] : b+1].
+__global__ void __launch_bounds__(kSumThreads) k_segment_parts(const double* __restrict__ v,
+                                                                const int64_t* __restrict__ base,
+                                                                const int64_t* __restrict__ idx, double* part) {
+  __shared__ double red[kSumThreads];
+  const int b = blockIdx.x / kSegParts, k = blockIdx.x % kSegParts;
   const int64_t lo = base[idx ? idx[b] : b], hi = base[idx ? idx[b + 1] : b + 1];
   double s = 0.0;
-  for (int64_t i = lo + threadIdx.x; i < hi; i += kSumThreads) s += v[i];
-  part[threadIdx.x] = s;
+  for (int64_t i = lo + (int64_t)k * kSumThreads + threadIdx.x; i < hi; i += (int64_t)kSegParts * kSumThreads)
+    s += v[i];
+  red[threadIdx.x] = s;
   __syncthreads();
   for (int w = kSumThreads / 2; w > 0; w >>= 1) {
-    if ((int)threadIdx.x < w) part[threadIdx.x] += part[threadIdx.x + w];
+    if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
     __syncthreads();
   }
-  if (threadIdx.x == 0) out[b] = accumulate ? out[b] + part[0] : part[0];
+  if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+// out[b] (+)= the partial sums of segment b in CTA order.
+__global__ void k_segment_total(const double* __restrict__ part, int n, double* out, int accumulate) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  double s = 0.0;
+  for (int k = 0; k < kSegParts; k++) s += part[(int64_t)b * kSegParts + k];
+  out[b] = accumulate ? out[b] + s : s;
 }
 
 }  // namespace
 
 cudaError_t launch_segment_sums(const double* v, const int64_t* base, const int64_t* idx, int n, double* out,
-                                bool accumulate, cudaStream_t s) {
+                                double* part, bool accumulate, cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
-  k_segment_sums<<<n, kSumThreads, 0, s>>>(v, base, idx, out, accumulate ? 1 : 0);
+  k_segment_parts<<<(unsigned)(n * kSegParts), kSumThreads, 0, s>>>(v, base, idx, part);
+  k_segment_total<<<(n + 127) / 128, 128, 0, s>>>(part, n, out, accumulate ? 1 : 0);
   return cudaGetLastError();
 }
 
