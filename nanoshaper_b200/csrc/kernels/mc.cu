@@ -332,7 +332,7 @@ __device__ __forceinline__ int64_t edge_vertex(const MCArgs& A, const StructDev&
 // One thread per active cube.  Pass 0 finds the vertex of every cut edge, counts the triangles
 // and sums their areas (and, in gradient mode, their derivatives with respect to the analytic
 // vertices); pass 1 writes the triangles at their offsets from the stored vertex ids.
-__global__ void __launch_bounds__(128) k_mc_tris(MCArgs A, int emit) {
+__global__ void __launch_bounds__(128, 8) k_mc_tris(MCArgs A, int emit) {
   __shared__ int8_t s_tri[256][16];
   __shared__ uint16_t s_emask[256];
   // vertex of cut edge e of this thread's cube at [e][thread]: the case table indexes it at run

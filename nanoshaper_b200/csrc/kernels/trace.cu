@@ -489,7 +489,7 @@ void launch_isect(const TraceCtx& C, const CandOut& co, const HitStore& hs, int 
 // kGrad: the hits carry their patches (sorted along), and every interval end adds its term of
 // d volume / d patch parameters; the stored pairs keep their patches for the area adjoint.
 template <bool kGrad>
-__global__ void __launch_bounds__(kTraceThreads) k_fill(TraceCtx C, HitStore hs) {
+__global__ void __launch_bounds__(kTraceThreads, 6) k_fill(TraceCtx C, HitStore hs) {
   constexpr int kThreads = kTraceThreads;
   const int panel = C.set == 0 ? 0 : C.set - 1;
   const int64_t tile = blockIdx.x;
