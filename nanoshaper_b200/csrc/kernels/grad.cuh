@@ -74,6 +74,11 @@ __device__ __forceinline__ void add_hit_grad(const double* __restrict__ f64, con
 // hit the same patch) are summed with a segmented shuffle scan first, so each run of equal pids
 // issues one atomic per component instead of one per lane.  All 32 lanes must call it.
 __device__ __forceinline__ void warp_add_grad(int32_t pid, double* g, double* gsum) {
+  // hit_grad fills at most the first kGradUsed components (a torus: centre, axis terms, major
+  // radius); the last slot of a patch's record stays zero
+  constexpr int kGradUsed = 7;
+  static_assert(kGradUsed <= NS_GRAD_PER_PATCH, "gradient record too short");
+  if (!__any_sync(0xffffffffu, pid >= 0)) return;
   const int lane = threadIdx.x & 31;
   const int32_t prev = __shfl_up_sync(0xffffffffu, pid, 1);
   const bool head = lane == 0 || prev != pid;
@@ -81,7 +86,7 @@ __device__ __forceinline__ void warp_add_grad(int32_t pid, double* g, double* gs
   const int start = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));
   const bool tail = lane == 31 || ((heads >> (lane + 1)) & 1u);
 #pragma unroll
-  for (int k = 0; k < NS_GRAD_PER_PATCH; k++) {
+  for (int k = 0; k < kGradUsed; k++) {
     double v = g[k];
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -93,7 +98,7 @@ __device__ __forceinline__ void warp_add_grad(int32_t pid, double* g, double* gs
   if (tail && pid >= 0) {
     double* o = gsum + (int64_t)NS_GRAD_PER_PATCH * pid;
 #pragma unroll
-    for (int k = 0; k < NS_GRAD_PER_PATCH; k++)
+    for (int k = 0; k < kGradUsed; k++)
       if (g[k] != 0.0) atomicAdd(o + k, g[k]);
   }
 }
