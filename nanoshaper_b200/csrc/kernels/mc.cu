@@ -152,14 +152,18 @@ __device__ __forceinline__ int own_midpoints(const MCArgs& A, const StructDev& S
 
 __device__ __forceinline__ int rec_struct(int w) { return (int)((unsigned)w >> 11); }
 
-// 32 consecutive bits of the flat bit grid starting at bit f (missing words read as outside).
-__device__ __forceinline__ uint32_t bits32(const uint32_t* __restrict__ bits, int64_t nwords, int64_t f) {
-  int64_t w = f >> 5;
-  int s = (int)(f & 31);
-  uint32_t lo = w < nwords ? bits[w] : 0xffffffffu;
-  if (s == 0) return lo;
-  uint32_t hi = (w + 1) < nwords ? bits[w + 1] : 0xffffffffu;
-  return __funnelshift_r(lo, hi, s);
+
+// The 32 bits of the flat bit grid starting at bit f (missing words read as outside), and in *next
+// the 32 bits starting at f + 1, from the same two words.
+__device__ __forceinline__ uint32_t bits32_pair(const uint32_t* __restrict__ bits, int64_t nwords, int64_t f,
+                                                uint32_t* next) {
+  const int64_t w = f >> 5;
+  const int s = (int)(f & 31);
+  const uint32_t lo = w < nwords ? bits[w] : 0xffffffffu;
+  const uint32_t hi = (w + 1) < nwords ? bits[w + 1] : 0xffffffffu;
+  const uint32_t x = s ? __funnelshift_r(lo, hi, s) : lo;
+  *next = (x >> 1) | (((hi >> s) & 1u) << 31);  // bit f + 32 is bit s of the second word
+  return x;
 }
 
 // Cube rows (j, k) in chunks of consecutive rows of one structure, one warp per chunk.  Every
@@ -200,14 +204,16 @@ __global__ void k_mc_rows(MCArgs A, int emit) {
         if (row_ok && word < W) {
           int64_t nvalid = NX - 1 - ic;
           uint32_t vm = nvalid >= 32 ? 0xffffffffu : ((1u << nvalid) - 1u);
-          c[0] = ~bits32(bits, nwords, b00 + ic);
-          c[1] = ~bits32(bits, nwords, b00 + ic + 1);
-          c[2] = ~bits32(bits, nwords, b10 + ic + 1);
-          c[3] = ~bits32(bits, nwords, b10 + ic);
-          c[4] = ~bits32(bits, nwords, b01 + ic);
-          c[5] = ~bits32(bits, nwords, b01 + ic + 1);
-          c[6] = ~bits32(bits, nwords, b11 + ic + 1);
-          c[7] = ~bits32(bits, nwords, b11 + ic);
+          // corners i and i + 1 of each of the four bit rows from one pair of words per row
+          uint32_t n0, n1, n2, n3;
+          c[0] = ~bits32_pair(bits, nwords, b00 + ic, &n0);
+          c[1] = ~n0;
+          c[3] = ~bits32_pair(bits, nwords, b10 + ic, &n1);
+          c[2] = ~n1;
+          c[4] = ~bits32_pair(bits, nwords, b01 + ic, &n2);
+          c[5] = ~n2;
+          c[7] = ~bits32_pair(bits, nwords, b11 + ic, &n3);
+          c[6] = ~n3;
           uint32_t d = 0;
 #pragma unroll
           for (int q = 1; q < 8; q++) d |= c[0] ^ c[q];
