@@ -166,8 +166,13 @@ __device__ __forceinline__ void isect_body(const TraceCtx& C, const CandOut& co,
   const int64_t ncand = *(co.count + (kTorus ? 1 : 0));
   const int2* list = kTorus ? co.tor : co.sph;
   const int64_t nlim = ncand < co.cap ? ncand : co.cap;
-  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < nlim; c += (int64_t)gridDim.x * blockDim.x) {
-    int2 e = list[c];
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  // the next candidate of this thread is loaded one iteration ahead
+  int2 e_next = c < nlim ? list[c] : make_int2(0, 0);
+  for (; c < nlim; c += stride) {
+    const int2 e = e_next;
+    if (c + stride < nlim) e_next = list[c + stride];
     const int64_t rid = e.x, pid = e.y;
     const StructDev& S = C.B.s[C.B.patch_struct[pid]];
     const GridDev& g = S.g;
