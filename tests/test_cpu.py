@@ -340,3 +340,73 @@ def test_replica_timing_gloo_world2():
     for rank, worst, thr in res:
         assert worst == 15.0
         assert abs(thr - 2 * 512 * 1000.0 / 15.0) < 1e-9
+
+
+def _row_interval(cf, cl, r, mn_fd, mn_ld, side, delta, m0, m1, n):
+    """The candidate kernel's row search, restated: the first pixel of the row where
+    Low(m) = pa(m) >= cf - r and (dx < 0 or disc(dx)) holds and the first where
+    High(m) = pa(m) <= cf + r and (dx > 0 or disc(dx)) fails, by binary search over [m0, m1]."""
+    lo_fd, hi_fd, lo_ld, hi_ld, r2 = cf - r, cf + r, cl - r, cl + r, r * r
+    pld = (mn_ld + float(n) * side) + delta
+    if pld < lo_ld or pld > hi_ld:
+        return []
+    dy = cl - pld
+    dy2 = dy * dy
+    lo, hi = m0, m1 + 1
+    while lo < hi:
+        mid = (lo + hi) >> 1
+        pa = (mn_fd + float(mid) * side) + delta
+        dx = cf - pa
+        if (not pa < lo_fd) and (dx < 0 or not dx * dx + dy2 > r2):
+            hi = mid
+        else:
+            lo = mid + 1
+    a, hi = lo, m1 + 1
+    while lo < hi:
+        mid = (lo + hi) >> 1
+        pa = (mn_fd + float(mid) * side) + delta
+        dx = cf - pa
+        if (not pa > hi_fd) and (dx > 0 or not dx * dx + dy2 > r2):
+            lo = mid + 1
+        else:
+            hi = mid
+    return list(range(a, lo))
+
+
+def test_candidate_row_intervals_match_pixel_test():
+    """The candidate kernel replaces the reference's per-pixel bounding-box and equatorial-disc
+    test (src/ConnollySurface.cpp:4469-4502) by an interval per pixel row found with two binary
+    searches.  In double precision the row predicates are monotone, so the interval must hold
+    exactly the pixels the per-pixel test accepts, tangent rows and pixels included."""
+    import random
+
+    def pixel_test(cf, cl, r, pfd, pld):
+        if pfd < cf - r or pfd > cf + r or pld < cl - r or pld > cl + r:
+            return False
+        dx, dy = cf - pfd, cl - pld
+        return not (dx * dx + dy * dy > r * r)
+
+    rng = random.Random(11)
+    rows = 0
+    for _ in range(3000):
+        side = rng.choice([0.5, 1.0 / 3.0, 0.25, 1.0 / 2.2])
+        mn_fd, mn_ld = rng.uniform(-50, 50), rng.uniform(-50, 50)
+        delta = rng.choice([0.0, 1e-10 - side / 2])
+        mc, nc = rng.randint(0, 40), rng.randint(0, 40)
+        kind = rng.random()
+        if kind < 0.4:  # centre on a pixel, radius a multiple of the spacing: exact tangencies
+            cf, cl = (mn_fd + float(mc) * side) + delta, (mn_ld + float(nc) * side) + delta
+            r = side * rng.randint(1, 10)
+        else:
+            cf, cl = mn_fd + rng.uniform(0, 40) * side, mn_ld + rng.uniform(0, 40) * side
+            r = rng.uniform(0.1, 6.0)
+        m0 = max(0, int(round((cf - r - mn_fd) / side)) - rng.randint(0, 2))
+        m1 = int(round((cf + r - mn_fd) / side)) + rng.randint(-1, 2)
+        n0 = max(0, int(round((cl - r - mn_ld) / side)) - 1)
+        n1 = int(round((cl + r - mn_ld) / side)) + 1
+        for n in range(n0, n1 + 1):
+            want = [m for m in range(m0, m1 + 1)
+                    if pixel_test(cf, cl, r, (mn_fd + float(m) * side) + delta, (mn_ld + float(n) * side) + delta)]
+            assert _row_interval(cf, cl, r, mn_fd, mn_ld, side, delta, m0, m1, n) == want
+            rows += 1
+    assert rows > 10000
