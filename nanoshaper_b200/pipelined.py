@@ -25,6 +25,18 @@ from . import _native as N
 from . import surface as S
 
 
+def chunk_bounds(n: int, n_chunks: int) -> np.ndarray:
+    """Boundaries of the chunks of an ensemble of n structures: chunk weights 1/2, 1, 1, ... (a
+    short first chunk starts the kernels early), no empty chunk; returns n_chunks' + 1 increasing
+    offsets from 0 to n with n_chunks' <= n_chunks."""
+    n_chunks = max(1, min(n_chunks, n))
+    weights = np.array([0.5] + [1.0] * (n_chunks - 1))
+    bounds = np.round(np.concatenate([[0.0], np.cumsum(weights)]) / weights.sum() * n).astype(int)
+    bounds = np.maximum.accumulate(bounds)
+    keep = [0] + [i for i in range(1, len(bounds)) if bounds[i] > bounds[i - 1]]
+    return bounds[keep]
+
+
 class _Chunk:
     def __init__(self, surfs: list, lo: int, hi: int):
         self.lo, self.hi = lo, hi
@@ -58,13 +70,7 @@ class PipelinedBatches:
                  tuning: list[int] | None = None):
         if not surfaces:
             raise ValueError("empty ensemble")
-        n_chunks = max(1, min(n_chunks, len(surfaces)))
-        # chunk weights 1/2, 1, 1, ...: a short first chunk starts the kernels early
-        weights = np.array([0.5] + [1.0] * (n_chunks - 1))
-        bounds = np.round(np.concatenate([[0.0], np.cumsum(weights)]) / weights.sum() * len(surfaces)).astype(int)
-        bounds = np.maximum.accumulate(bounds)
-        keep = [0] + [i for i in range(1, len(bounds)) if bounds[i] > bounds[i - 1]]
-        bounds = bounds[keep]
+        bounds = chunk_bounds(len(surfaces), n_chunks)
         n_chunks = len(bounds) - 1
         self.chunks = [_Chunk(surfaces, int(bounds[i]), int(bounds[i + 1])) for i in range(n_chunks)]
         self.n = len(surfaces)

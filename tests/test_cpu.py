@@ -410,3 +410,35 @@ def test_candidate_row_intervals_match_pixel_test():
             assert _row_interval(cf, cl, r, mn_fd, mn_ld, side, delta, m0, m1, n) == want
             rows += 1
     assert rows > 10000
+
+
+def test_pipelined_chunk_bounds():
+    """Chunks of an ensemble cover every structure once, in order, with no empty chunk, and the
+    first is about half the size of the others."""
+    from nanoshaper_b200.pipelined import chunk_bounds
+    for n in range(1, 80):
+        for k in range(1, 10):
+            b = chunk_bounds(n, k)
+            assert b[0] == 0 and b[-1] == n and len(b) - 1 <= min(n, k)
+            assert np.all(np.diff(b) > 0)
+    b = chunk_bounds(512, 6)
+    sizes = np.diff(b)
+    assert len(sizes) == 6 and abs(sizes[0] - sizes[1] / 2) <= 1 and sizes[1:].max() - sizes[1:].min() <= 1
+
+
+def test_bench_reference_arm_contract():
+    """`bench.py --impl reference` (the oracle port on the host cores) prints one JSON line with
+    the driver's keys, on the small ensemble."""
+    import json
+    import sys
+    root = Path(__file__).resolve().parents[1]
+    res = subprocess.run([sys.executable, str(root / "bench.py"), "--impl", "reference", "--workload", "ensemble_64",
+                          "--steps", "1", "--warmup", "0"], capture_output=True, text=True, timeout=600, cwd=root)
+    assert res.returncode == 0, res.stderr[-2000:]
+    line = json.loads([ln for ln in res.stdout.splitlines() if ln.startswith("{")][-1])
+    for key in ("impl", "metric", "value", "unit", "n_gpus", "steps", "warmup", "higher_is_better", "config",
+                "cpu_baseline", "e2e"):
+        assert key in line, key
+    assert line["impl"] == "reference" and line["value"] > 0
+    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
