@@ -64,6 +64,10 @@ STAGES = ("bin", "trace", "overflow", "cavity", "vertex", "mc", "cand", "isect",
 # (smsp__sass_thread_inst_executed_op_{dadd,dmul,dfma,fadd,fmul,ffma}_pred_on.sum) on the
 # 64-structure conformer ensemble and divided by its candidate counts.
 FLOPS_PER_CANDIDATE = {"torus": {"fp64": 312.0, "fp32": 35.0}, "sphere": {"fp64": 26.0, "fp32": 74.0}}
+# DRAM bytes (read + written) of the mixed intersection launches per candidate, from an ncu capture
+# of the 64-structure ensemble (the ray set of panel 1: 283 MB for the sphere launch, 224 MB for the
+# torus launch, 5 MB for the deferred ones, over its 19.9 M candidates)
+ISECT_DRAM_BYTES_PER_CANDIDATE = 25.7
 
 
 def load_peaks() -> dict:
@@ -439,7 +443,10 @@ def run_ensemble(args, world: int, rank: int, local: int) -> None:
     fill_bytes = 3 * 2 * 4 * nwords + 8 * rays + 16 * nv
     roofline = {"bound": "fp64", "kernel": "k_isect (ray-patch intersection, 4 ray sets)", "achieved": ach64,
                 "peak": pk64.value / 1e12, "unit": "TFLOP/s", "frac": ach64 / (pk64.value / 1e12),
-                "traffic": None, "peak_source": "measured live: FMA chains on this GPU (nsg_fp_peak)",
+                "traffic": (n_tor + n_sph) * ISECT_DRAM_BYTES_PER_CANDIDATE,
+                "traffic_note": "DRAM bytes of the step's intersection launches: ncu-measured bytes per candidate "
+                                "on the 64-structure ensemble x this step's candidates",
+                "peak_source": "measured live: FMA chains on this GPU (nsg_fp_peak)",
                 "flops_per_step": {"fp64": flops64, "fp32": flops32},
                 "fp32": {"achieved": ach32, "peak": pk32.value / 1e12, "frac": ach32 / (pk32.value / 1e12)},
                 "hbm_fill": {"kernel": "k_fill", "achieved_gbs": fill_bytes / (stage_times["fill"] / 1000.0) / 1e9
