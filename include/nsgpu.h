@@ -101,6 +101,16 @@ int nsg_write_cavities(const char* cavities_path, const char* sizes_path, const 
  * 1 = root.ply (binary); revert writes every triangle in the opposite winding. */
 int nsg_write_mesh(const char* root, int format, const double* vertices, int64_t n_vertices, const int32_t* triangles,
                    int64_t n_triangles, int revert);
+/* Vertex normals of a mesh by triangle averaging: approximateNormals for a surface without analytic
+ * normals (src/Surface.cpp:10588-10660): the normalised sum of the unnormalised plane normals
+ * (plane3points, src/tools.cpp:258-274) of each vertex's triangles; 3 doubles per vertex. */
+int nsg_mesh_normals(const double* vertices, int64_t n_vertices, const int32_t* triangles, int64_t n_triangles,
+                     double* normals);
+/* Surface::saveMesh with normals (src/Surface.cpp:10857-11062): format 0 = root.off in OFF+N,
+ * 1 = MSMS without nearest-atom information (root.face, root.vert); both add
+ * roottriangleAreas.txt. */
+int nsg_write_mesh_normals(const char* root, int format, const double* vertices, const double* normals,
+                           int64_t n_vertices, const int32_t* triangles, int64_t n_triangles, int revert);
 
 /* ---- device context ---- */
 int nsg_version(void);

@@ -77,6 +77,29 @@ int nsg_write_cavities(const char* cavities_path, const char* sizes_path, const 
   return fclose(fp) == 0 ? NSG_OK : NSG_ERR_IO;
 }
 
+// root + "triangleAreas.txt": the Heron area of every triangle, "0." for degenerate ones
+// (Surface::saveMesh, src/Surface.cpp:11042-11062).
+static int write_triangle_areas(const std::string& base, const double* vertices, const int32_t* triangles,
+                                int64_t n_triangles) {
+  FILE* fp = fopen((base + "triangleAreas.txt").c_str(), "w");
+  if (!fp) return NSG_ERR_IO;
+  for (int64_t t = 0; t < n_triangles; t++) {
+    const double* p0 = vertices + 3 * (int64_t)triangles[3 * t];
+    const double* p1 = vertices + 3 * (int64_t)triangles[3 * t + 1];
+    const double* p2 = vertices + 3 * (int64_t)triangles[3 * t + 2];
+    auto dist = [](const double* a, const double* b) {
+      return sqrt((a[0] - b[0]) * (a[0] - b[0]) + (a[1] - b[1]) * (a[1] - b[1]) + (a[2] - b[2]) * (a[2] - b[2]));
+    };
+    const double a = dist(p0, p1), b = dist(p0, p2), c = dist(p1, p2);
+    const double ttt = (a + b + c) * (b + c - a) * (c + a - b) * (a + b - c);
+    if (ttt > 0)
+      fprintf(fp, "%f\n", 0.25 * sqrt(ttt));
+    else
+      fprintf(fp, "0.\n");
+  }
+  return fclose(fp) == 0 ? NSG_OK : NSG_ERR_IO;
+}
+
 // format: 0 OFF (+ triangleAreas.txt), 1 PLY (binary little endian).  root is the path without
 // extension; the reference's file names are root + ".off" / ".ply" and root + "triangleAreas.txt".
 int nsg_write_mesh(const char* root, int format, const double* vertices, int64_t n_vertices, const int32_t* triangles,
@@ -118,23 +141,89 @@ int nsg_write_mesh(const char* root, int format, const double* vertices, int64_t
   } else {
     return NSG_ERR_ARG;
   }
-  FILE* fp = fopen((base + "triangleAreas.txt").c_str(), "w");
-  if (!fp) return NSG_ERR_IO;
+  return write_triangle_areas(base, vertices, triangles, n_triangles);
+}
+
+// Vertex normals from the triangulation, as approximateNormals does for a surface without analytic
+// normals (src/Surface.cpp:10588-10660, updateVertexTrianglesLists :10526-10566): per vertex, the
+// sum over its triangles, in triangle order, of the unnormalised plane normal of plane3points
+// (src/tools.cpp:258-274), divided by its length.  A vertex without triangles gets 0/0, as there.
+int nsg_mesh_normals(const double* vertices, int64_t n_vertices, const int32_t* triangles, int64_t n_triangles,
+                     double* normals) {
+  if (n_vertices < 0 || n_triangles < 0 || (n_vertices && (!vertices || !normals)) || (n_triangles && !triangles))
+    return NSG_ERR_ARG;
+  for (int64_t t = 0; t < 3 * n_triangles; t++)
+    if (triangles[t] < 0 || triangles[t] >= n_vertices) return NSG_ERR_ARG;
+  for (int64_t k = 0; k < 3 * n_vertices; k++) normals[k] = 0.0;
   for (int64_t t = 0; t < n_triangles; t++) {
-    const double* p0 = vertices + 3 * (int64_t)triangles[3 * t];
-    const double* p1 = vertices + 3 * (int64_t)triangles[3 * t + 1];
-    const double* p2 = vertices + 3 * (int64_t)triangles[3 * t + 2];
-    auto dist = [](const double* a, const double* b) {
-      return sqrt((a[0] - b[0]) * (a[0] - b[0]) + (a[1] - b[1]) * (a[1] - b[1]) + (a[2] - b[2]) * (a[2] - b[2]));
-    };
-    const double a = dist(p0, p1), b = dist(p0, p2), c = dist(p1, p2);
-    const double ttt = (a + b + c) * (b + c - a) * (c + a - b) * (a + b - c);
-    if (ttt > 0)
-      fprintf(fp, "%f\n", 0.25 * sqrt(ttt));
-    else
-      fprintf(fp, "0.\n");
+    const double* p1 = vertices + 3 * (int64_t)triangles[3 * t];
+    const double* p2 = vertices + 3 * (int64_t)triangles[3 * t + 1];
+    const double* p3 = vertices + 3 * (int64_t)triangles[3 * t + 2];
+    const double w0 = p1[1] * (p2[2] - p3[2]) + p2[1] * (p3[2] - p1[2]) + p3[1] * (p1[2] - p2[2]);
+    const double w1 = p1[2] * (p2[0] - p3[0]) + p2[2] * (p3[0] - p1[0]) + p3[2] * (p1[0] - p2[0]);
+    const double w2 = p1[0] * (p2[1] - p3[1]) + p2[0] * (p3[1] - p1[1]) + p3[0] * (p1[1] - p2[1]);
+    for (int q = 0; q < 3; q++) {
+      double* nv = normals + 3 * (int64_t)triangles[3 * t + q];
+      nv[0] = nv[0] + w0;
+      nv[1] = nv[1] + w1;
+      nv[2] = nv[2] + w2;
+    }
   }
-  return fclose(fp) == 0 ? NSG_OK : NSG_ERR_IO;
+  for (int64_t v = 0; v < n_vertices; v++) {
+    double* nv = normals + 3 * v;
+    const double len = sqrt(nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2]);
+    nv[0] = nv[0] / len;
+    nv[1] = nv[1] / len;
+    nv[2] = nv[2] / len;
+  }
+  return NSG_OK;
+}
+
+// Mesh with vertex normals (Surface::saveMesh, src/Surface.cpp:10857-11062): format 0 = OFF+N
+// (root.off), 1 = MSMS without nearest-atom information (root.face, root.vert, 1-based indices);
+// both add roottriangleAreas.txt.  revert writes every triangle in the opposite winding.
+int nsg_write_mesh_normals(const char* root, int format, const double* vertices, const double* normals,
+                           int64_t n_vertices, const int32_t* triangles, int64_t n_triangles, int revert) {
+  if (!root || n_vertices < 0 || n_triangles < 0 || (n_vertices && (!vertices || !normals)) ||
+      (n_triangles && !triangles) || (format != 0 && format != 1))
+    return NSG_ERR_ARG;
+  for (int64_t t = 0; t < 3 * n_triangles; t++)
+    if (triangles[t] < 0 || triangles[t] >= n_vertices) return NSG_ERR_ARG;
+  const std::string base(root);
+  auto tri = [&](int64_t t, int q) { return triangles[3 * t + (revert ? 2 - q : q)]; };
+  time_t pt;
+  time(&pt);
+  if (format == 0) {
+    FILE* fp = fopen((base + ".off").c_str(), "w");
+    if (!fp) return NSG_ERR_IO;
+    fprintf(fp, "OFF+N\n");
+    fprintf(fp, "# File created by %s version %s date %s\n", kProg, kVersion, ctime(&pt));
+    fprintf(fp, "%d %d 0\n", (int)n_vertices, (int)n_triangles);
+    for (int64_t v = 0; v < n_vertices; v++)
+      fprintf(fp, "%.3f %.3f %.3f %.3f %.3f %.3f\n", vertices[3 * v], vertices[3 * v + 1], vertices[3 * v + 2],
+              normals[3 * v], normals[3 * v + 1], normals[3 * v + 2]);
+    for (int64_t t = 0; t < n_triangles; t++) fprintf(fp, "3 %d %d %d\n", tri(t, 0), tri(t, 1), tri(t, 2));
+    if (fclose(fp) != 0) return NSG_ERR_IO;
+  } else {
+    FILE* ff = fopen((base + ".face").c_str(), "w");
+    if (!ff) return NSG_ERR_IO;
+    fprintf(ff, "# File created by %s version %s date %s", kProg, kVersion, ctime(&pt));
+    fprintf(ff, "#faces\n");
+    fprintf(ff, "%d\n", (int)n_triangles);
+    for (int64_t t = 0; t < n_triangles; t++)
+      fprintf(ff, "%6d %6d %6d %2d %6d\n", tri(t, 0) + 1, tri(t, 1) + 1, tri(t, 2) + 1, 1, 1);
+    if (fclose(ff) != 0) return NSG_ERR_IO;
+    FILE* fv = fopen((base + ".vert").c_str(), "w");
+    if (!fv) return NSG_ERR_IO;
+    fprintf(fv, "# File created by %s version %s date %s", kProg, kVersion, ctime(&pt));
+    fprintf(fv, "#vertex\n");
+    fprintf(fv, "%d\n", (int)n_vertices);
+    for (int64_t v = 0; v < n_vertices; v++)
+      fprintf(fv, "%9.3f %9.3f %9.3f %9.3f %9.3f %9.3f %7d %7d %2d \n", vertices[3 * v], vertices[3 * v + 1],
+              vertices[3 * v + 2], normals[3 * v], normals[3 * v + 1], normals[3 * v + 2], 0, 1, 0);
+    if (fclose(fv) != 0) return NSG_ERR_IO;
+  }
+  return write_triangle_areas(base, vertices, triangles, n_triangles);
 }
 
 }  // extern "C"

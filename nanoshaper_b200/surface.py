@@ -394,17 +394,40 @@ class Surface:
         return self.area
 
     MESH_FORMATS = {"off": 0, "ply": 1}
+    # formats with vertex normals (nsg_write_mesh_normals)
+    NORMAL_MESH_FORMATS = {"off_n": 0, "msms_no_a": 1}
 
-    def saveMesh(self, format: str = "off", revert: bool = False, fileName: str | Path = "triangulatedSurf") -> None:
-        """Mesh file in the reference's layout: ``fileName.off`` (+ ``fileNametriangleAreas.txt``)
-        or ``fileName.ply`` (Surface::saveMesh, src/Surface.cpp:10857-11052)."""
+    def approximateNormals(self) -> np.ndarray:
+        """Vertex normals of the last triangulation by triangle averaging (the reference's
+        approximateNormals for surfaces without analytic normals, src/Surface.cpp:10588-10660);
+        (n_vertices, 3)."""
         if self.vertices is None or self.triangles is None:
             raise RuntimeError("no mesh: call triangulateSurface() first")
-        fmt = self.MESH_FORMATS.get(str(format).lower())
-        if fmt is None:
-            raise ValueError(f"unsupported mesh format {format}; available: {sorted(self.MESH_FORMATS)}")
         v = np.ascontiguousarray(self.vertices, np.float64)
         t = np.ascontiguousarray(self.triangles, np.int32)
+        out = np.zeros((len(v), 3))
+        N.check(N.lib().nsg_mesh_normals(N.ptr(v), len(v), N.ptr(t), len(t), N.ptr(out)), "mesh normals")
+        return out
+
+    def saveMesh(self, format: str = "off", revert: bool = False, fileName: str | Path = "triangulatedSurf") -> None:
+        """Mesh file in the reference's layout: ``fileName.off`` (+ ``fileNametriangleAreas.txt``),
+        ``fileName.ply``, or with vertex normals from approximateNormals() ``off_n`` (OFF+N) and
+        ``msms_no_a`` (``fileName.face`` / ``fileName.vert``) (Surface::saveMesh,
+        src/Surface.cpp:10857-11062)."""
+        if self.vertices is None or self.triangles is None:
+            raise RuntimeError("no mesh: call triangulateSurface() first")
+        name = str(format).lower()
+        v = np.ascontiguousarray(self.vertices, np.float64)
+        t = np.ascontiguousarray(self.triangles, np.int32)
+        if name in self.NORMAL_MESH_FORMATS:
+            nrm = np.ascontiguousarray(self.approximateNormals(), np.float64)
+            N.check(N.lib().nsg_write_mesh_normals(str(fileName).encode(), self.NORMAL_MESH_FORMATS[name], N.ptr(v),
+                                                   N.ptr(nrm), len(v), N.ptr(t), len(t), int(revert)), "saveMesh")
+            return
+        fmt = self.MESH_FORMATS.get(name)
+        if fmt is None:
+            raise ValueError(f"unsupported mesh format {format}; available: "
+                             f"{sorted(self.MESH_FORMATS) + sorted(self.NORMAL_MESH_FORMATS)}")
         N.check(N.lib().nsg_write_mesh(str(fileName).encode(), fmt, N.ptr(v), len(v), N.ptr(t), len(t), int(revert)),
                 "saveMesh")
 

@@ -442,3 +442,38 @@ def test_bench_reference_arm_contract():
     assert line["impl"] == "reference" and line["value"] > 0
     assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
+
+
+def test_mesh_normals_and_normal_formats(native_lib, tmp_path):
+    """Triangle-averaged vertex normals (approximateNormals without analytic normals) and the OFF+N
+    and MSMS writers (Surface::saveMesh)."""
+    v = np.array([[1.0, 0, 0], [-1.0, 0, 0], [0, 1.0, 0], [0, -1.0, 0], [0, 0, 1.0], [0, 0, -1.0]])
+    # octahedron, counter-clockwise seen from outside
+    t = np.array([[0, 2, 4], [2, 1, 4], [1, 3, 4], [3, 0, 4], [2, 0, 5], [1, 2, 5], [3, 1, 5], [0, 3, 5]], np.int32)
+    ds = nb.DelPhiShared(np.array([[0.0, 0.0, 0.0, 1.5]]), 2.0, 50.0)
+    s = nb.ConnollySurface(nb.ConfigFile(), ds)
+    s.vertices, s.triangles = v, t
+    n = s.approximateNormals()
+    # numpy restatement: sum of the unnormalised plane normals (p2 - p1) x (p3 - p1) per vertex
+    ref = np.zeros_like(v)
+    for a, b, c in t:
+        w = np.cross(v[b] - v[a], v[c] - v[a])
+        ref[a] += w
+        ref[b] += w
+        ref[c] += w
+    ref /= np.linalg.norm(ref, axis=1, keepdims=True)
+    assert np.allclose(n, ref, atol=1e-15) and np.allclose(n, v, atol=1e-15)
+    s.saveMesh("off_n", False, str(tmp_path / "m"))
+    off = (tmp_path / "m.off").read_text().splitlines()
+    assert off[0] == "OFF+N" and off[3] == "6 8 0"
+    assert off[4] == "1.000 0.000 0.000 1.000 0.000 0.000" and off[-1] == "3 0 3 5"
+    assert len((tmp_path / "mtriangleAreas.txt").read_text().splitlines()) == 8
+    s.saveMesh("msms_no_a", True, str(tmp_path / "m"))
+    face = (tmp_path / "m.face").read_text().splitlines()
+    assert face[0].startswith("# File created by") and face[1] == "#faces" and face[2] == "8"
+    assert face[3].split() == ["5", "3", "1", "1", "1"] and len(face) == 11  # reverted, 1-based
+    vert = (tmp_path / "m.vert").read_text().splitlines()
+    assert vert[1] == "#vertex" and vert[2] == "6" and len(vert) == 9
+    cols = vert[3].split()
+    assert len(cols) == 9 and cols[:6] == ["1.000", "0.000", "0.000", "1.000", "0.000", "0.000"] and cols[6:] == ["0", "1", "0"]
+    assert vert[3] == "%9.3f %9.3f %9.3f %9.3f %9.3f %9.3f %7d %7d %2d " % (1, 0, 0, 1, 0, 0, 0, 1, 0)
