@@ -106,11 +106,18 @@ int nsg_write_mesh(const char* root, int format, const double* vertices, int64_t
  * (plane3points, src/tools.cpp:258-274) of each vertex's triangles; 3 doubles per vertex. */
 int nsg_mesh_normals(const double* vertices, int64_t n_vertices, const int32_t* triangles, int64_t n_triangles,
                      double* normals);
-/* Surface::saveMesh with normals (src/Surface.cpp:10857-11062): format 0 = root.off in OFF+N,
- * 1 = MSMS without nearest-atom information (root.face, root.vert); both add
+/* Nearest atom of every vertex (vdwAccessible, src/Surface.cpp:16663-16715): least power distance
+ * |p - c|^2 - r^2 over all atoms (4 doubles each), ties to the lower index; 0-based, -1 without
+ * atoms. */
+int nsg_vertex_atoms(const double* vertices, int64_t n_vertices, const double* atoms_xyzr, int64_t n_atoms,
+                     int32_t* vertex_atoms);
+/* Surface::saveMesh with vertex attributes (src/Surface.cpp:10857-11062): format 0 = OFF+N,
+ * 1 = MSMS without nearest atoms (root.face, root.vert), 2 = OFF+A, 3 = OFF+N+A, 4 = MSMS; normals
+ * for 0, 1, 3, 4, vertex_atoms (0-based) for 2, 3, 4 (may be NULL otherwise); every format adds
  * roottriangleAreas.txt. */
-int nsg_write_mesh_normals(const char* root, int format, const double* vertices, const double* normals,
-                           int64_t n_vertices, const int32_t* triangles, int64_t n_triangles, int revert);
+int nsg_write_mesh_attrs(const char* root, int format, const double* vertices, const double* normals,
+                         const int32_t* vertex_atoms, int64_t n_vertices, const int32_t* triangles,
+                         int64_t n_triangles, int revert);
 
 /* ---- device context ---- */
 int nsg_version(void);

@@ -101,7 +101,8 @@ _SIGNATURES = {
                            _INT),
     "nsg_write_mesh": ([ctypes.c_char_p, _INT, _P, _I64, _P, _I64, _INT], _INT),
     "nsg_mesh_normals": ([_P, _I64, _P, _I64, _P], _INT),
-    "nsg_write_mesh_normals": ([ctypes.c_char_p, _INT, _P, _P, _I64, _P, _I64, _INT], _INT),
+    "nsg_vertex_atoms": ([_P, _I64, _P, _I64, _P], _INT),
+    "nsg_write_mesh_attrs": ([ctypes.c_char_p, _INT, _P, _P, _P, _I64, _P, _I64, _INT], _INT),
     "nsg_patch_grads": ([_P, _P, _P], _INT),
     "nsg_upload_atoms": ([_P, _P, _P, _P], _INT),
     "nsg_atom_grads": ([_P, _P, _P], _INT),

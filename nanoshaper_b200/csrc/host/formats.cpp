@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdio>
 #include <ctime>
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -179,13 +180,99 @@ int nsg_mesh_normals(const double* vertices, int64_t n_vertices, const int32_t* 
   return NSG_OK;
 }
 
-// Mesh with vertex normals (Surface::saveMesh, src/Surface.cpp:10857-11062): format 0 = OFF+N
-// (root.off), 1 = MSMS without nearest-atom information (root.face, root.vert, 1-based indices);
-// both add roottriangleAreas.txt.  revert writes every triangle in the opposite winding.
-int nsg_write_mesh_normals(const char* root, int format, const double* vertices, const double* normals,
-                           int64_t n_vertices, const int32_t* triangles, int64_t n_triangles, int revert) {
-  if (!root || n_vertices < 0 || n_triangles < 0 || (n_vertices && (!vertices || !normals)) ||
-      (n_triangles && !triangles) || (format != 0 && format != 1))
+// Nearest atom of every vertex, as vdwAccessible picks it (src/Surface.cpp:16663-16715): the atom of
+// least power distance |p - c|^2 - r^2 (ties: the lower index).  The reference searches the atoms
+// binned in the grid cells around the vertex; here a uniform grid of cells is searched in growing
+// shells until no atom outside the searched cells can win, so the winner is the global one.
+// atoms_xyzr: 4 doubles per atom; out: the 0-based atom index per vertex (-1 without atoms).
+int nsg_vertex_atoms(const double* vertices, int64_t n_vertices, const double* atoms_xyzr, int64_t n_atoms,
+                     int32_t* out) {
+  if (n_vertices < 0 || n_atoms < 0 || (n_vertices && (!vertices || !out)) || (n_atoms && !atoms_xyzr))
+    return NSG_ERR_ARG;
+  if (n_atoms == 0) {
+    for (int64_t v = 0; v < n_vertices; v++) out[v] = -1;
+    return NSG_OK;
+  }
+  double lo[3] = {atoms_xyzr[0], atoms_xyzr[1], atoms_xyzr[2]}, hi[3] = {lo[0], lo[1], lo[2]}, rmax = 0.0;
+  for (int64_t a = 0; a < n_atoms; a++) {
+    for (int d = 0; d < 3; d++) {
+      lo[d] = std::min(lo[d], atoms_xyzr[4 * a + d]);
+      hi[d] = std::max(hi[d], atoms_xyzr[4 * a + d]);
+    }
+    rmax = std::max(rmax, atoms_xyzr[4 * a + 3]);
+  }
+  const double cell = std::max(2.0, rmax);
+  int64_t dim[3];
+  for (int d = 0; d < 3; d++) dim[d] = std::max<int64_t>(1, (int64_t)((hi[d] - lo[d]) / cell) + 1);
+  const int64_t ncell = dim[0] * dim[1] * dim[2];
+  std::vector<int64_t> start(ncell + 1, 0);
+  std::vector<int32_t> items(n_atoms);
+  auto cell_of = [&](const double* p, int d) {
+    int64_t c = (int64_t)std::floor((p[d] - lo[d]) / cell);
+    return std::min<int64_t>(std::max<int64_t>(c, 0), dim[d] - 1);
+  };
+  auto cid = [&](int64_t x, int64_t y, int64_t z) { return (z * dim[1] + y) * dim[0] + x; };
+  for (int64_t a = 0; a < n_atoms; a++) {
+    const double* p = atoms_xyzr + 4 * a;
+    start[cid(cell_of(p, 0), cell_of(p, 1), cell_of(p, 2)) + 1]++;
+  }
+  for (int64_t c = 0; c < ncell; c++) start[c + 1] += start[c];
+  std::vector<int64_t> fill(start.begin(), start.end() - 1);
+  for (int64_t a = 0; a < n_atoms; a++) {
+    const double* p = atoms_xyzr + 4 * a;
+    items[fill[cid(cell_of(p, 0), cell_of(p, 1), cell_of(p, 2))]++] = (int32_t)a;
+  }
+  for (int64_t v = 0; v < n_vertices; v++) {
+    const double* p = vertices + 3 * v;
+    int64_t c0[3];
+    for (int d = 0; d < 3; d++) c0[d] = cell_of(p, d);
+    double best = INFINITY;
+    int32_t winner = -1;
+    // distance from p to the region outside the searched cube of cells [c0 - s, c0 + s]
+    for (int64_t s = 0;; s++) {
+      for (int64_t z = c0[2] - s; z <= c0[2] + s; z++)
+        for (int64_t y = c0[1] - s; y <= c0[1] + s; y++)
+          for (int64_t x = c0[0] - s; x <= c0[0] + s; x++) {
+            if (x < 0 || y < 0 || z < 0 || x >= dim[0] || y >= dim[1] || z >= dim[2]) continue;
+            if (std::max({std::llabs(x - c0[0]), std::llabs(y - c0[1]), std::llabs(z - c0[2])}) != s) continue;
+            const int64_t c = cid(x, y, z);
+            for (int64_t k = start[c]; k < start[c + 1]; k++) {
+              const int32_t a = items[k];
+              const double* q = atoms_xyzr + 4 * a;
+              const double pd = (q[0] - p[0]) * (q[0] - p[0]) + (q[1] - p[1]) * (q[1] - p[1]) +
+                                (q[2] - p[2]) * (q[2] - p[2]) - q[3] * q[3];
+              if (pd < best || (pd == best && a < winner)) {
+                best = pd;
+                winner = a;
+              }
+            }
+          }
+      // every atom outside the searched cells is at least `gap` from p
+      double gap = INFINITY;
+      for (int d = 0; d < 3; d++) {
+        if (c0[d] - s > 0) gap = std::min(gap, p[d] - (lo[d] + (double)(c0[d] - s) * cell));
+        if (c0[d] + s < dim[d] - 1) gap = std::min(gap, (lo[d] + (double)(c0[d] + s + 1) * cell) - p[d]);
+      }
+      if (gap == INFINITY) break;  // the whole grid searched
+      if (winner >= 0 && gap > 0 && gap * gap - rmax * rmax > best) break;
+    }
+    out[v] = winner;
+  }
+  return NSG_OK;
+}
+
+// Mesh with per-vertex normals and/or nearest atoms (Surface::saveMesh, src/Surface.cpp:10857-11062):
+// format 0 = OFF+N, 1 = MSMS without nearest atoms (root.face, root.vert), 2 = OFF+A, 3 = OFF+N+A,
+// 4 = MSMS (nearest atom + 1 in the .vert lines).  normals (3 doubles per vertex) are required by
+// formats 0, 1, 3, 4 and atoms (0-based atom index per vertex) by formats 2, 3, 4.  Every format adds
+// roottriangleAreas.txt.  revert writes every triangle in the opposite winding.
+int nsg_write_mesh_attrs(const char* root, int format, const double* vertices, const double* normals,
+                         const int32_t* atoms, int64_t n_vertices, const int32_t* triangles, int64_t n_triangles,
+                         int revert) {
+  const bool need_n = format == 0 || format == 1 || format == 3 || format == 4;
+  const bool need_a = format >= 2;
+  if (!root || n_vertices < 0 || n_triangles < 0 || format < 0 || format > 4 || (n_vertices && !vertices) ||
+      (n_vertices && need_n && !normals) || (n_vertices && need_a && !atoms) || (n_triangles && !triangles))
     return NSG_ERR_ARG;
   for (int64_t t = 0; t < 3 * n_triangles; t++)
     if (triangles[t] < 0 || triangles[t] >= n_vertices) return NSG_ERR_ARG;
@@ -193,15 +280,24 @@ int nsg_write_mesh_normals(const char* root, int format, const double* vertices,
   auto tri = [&](int64_t t, int q) { return triangles[3 * t + (revert ? 2 - q : q)]; };
   time_t pt;
   time(&pt);
-  if (format == 0) {
+  if (format == 0 || format == 2 || format == 3) {
     FILE* fp = fopen((base + ".off").c_str(), "w");
     if (!fp) return NSG_ERR_IO;
-    fprintf(fp, "OFF+N\n");
+    fprintf(fp, format == 0 ? "OFF+N\n" : (format == 2 ? "OFF+A\n" : "OFF+N+A\n"));
     fprintf(fp, "# File created by %s version %s date %s\n", kProg, kVersion, ctime(&pt));
     fprintf(fp, "%d %d 0\n", (int)n_vertices, (int)n_triangles);
-    for (int64_t v = 0; v < n_vertices; v++)
-      fprintf(fp, "%.3f %.3f %.3f %.3f %.3f %.3f\n", vertices[3 * v], vertices[3 * v + 1], vertices[3 * v + 2],
-              normals[3 * v], normals[3 * v + 1], normals[3 * v + 2]);
+    for (int64_t v = 0; v < n_vertices; v++) {
+      const double* x = vertices + 3 * v;
+      if (format == 2) {
+        fprintf(fp, "%.3f %.3f %.3f %d\n", x[0], x[1], x[2], atoms[v]);
+      } else {
+        const double* nn = normals + 3 * v;
+        if (format == 0)
+          fprintf(fp, "%.3f %.3f %.3f %.3f %.3f %.3f\n", x[0], x[1], x[2], nn[0], nn[1], nn[2]);
+        else
+          fprintf(fp, "%.3f %.3f %.3f %.3f %.3f %.3f %d\n", x[0], x[1], x[2], nn[0], nn[1], nn[2], atoms[v]);
+      }
+    }
     for (int64_t t = 0; t < n_triangles; t++) fprintf(fp, "3 %d %d %d\n", tri(t, 0), tri(t, 1), tri(t, 2));
     if (fclose(fp) != 0) return NSG_ERR_IO;
   } else {
@@ -220,7 +316,8 @@ int nsg_write_mesh_normals(const char* root, int format, const double* vertices,
     fprintf(fv, "%d\n", (int)n_vertices);
     for (int64_t v = 0; v < n_vertices; v++)
       fprintf(fv, "%9.3f %9.3f %9.3f %9.3f %9.3f %9.3f %7d %7d %2d \n", vertices[3 * v], vertices[3 * v + 1],
-              vertices[3 * v + 2], normals[3 * v], normals[3 * v + 1], normals[3 * v + 2], 0, 1, 0);
+              vertices[3 * v + 2], normals[3 * v], normals[3 * v + 1], normals[3 * v + 2], 0,
+              format == 4 ? atoms[v] + 1 : 1, 0);
     if (fclose(fv) != 0) return NSG_ERR_IO;
   }
   return write_triangle_areas(base, vertices, triangles, n_triangles);

@@ -394,8 +394,19 @@ class Surface:
         return self.area
 
     MESH_FORMATS = {"off": 0, "ply": 1}
-    # formats with vertex normals (nsg_write_mesh_normals)
-    NORMAL_MESH_FORMATS = {"off_n": 0, "msms_no_a": 1}
+    # formats with vertex normals and/or nearest atoms (nsg_write_mesh_attrs)
+    ATTR_MESH_FORMATS = {"off_n": 0, "msms_no_a": 1, "off_a": 2, "off_n_a": 3, "msms": 4}
+
+    def vertexAtoms(self) -> np.ndarray:
+        """Nearest atom (0-based, least power distance as vdwAccessible, src/Surface.cpp:16663-16715)
+        of every vertex of the last triangulation."""
+        if self.vertices is None:
+            raise RuntimeError("no mesh: call triangulateSurface() first")
+        v = np.ascontiguousarray(self.vertices, np.float64)
+        a = np.ascontiguousarray(self.delphi.atoms, np.float64)
+        out = np.zeros(len(v), np.int32)
+        N.check(N.lib().nsg_vertex_atoms(N.ptr(v), len(v), N.ptr(a), len(a), N.ptr(out)), "vertex atoms")
+        return out
 
     def approximateNormals(self) -> np.ndarray:
         """Vertex normals of the last triangulation by triangle averaging (the reference's
@@ -411,23 +422,27 @@ class Surface:
 
     def saveMesh(self, format: str = "off", revert: bool = False, fileName: str | Path = "triangulatedSurf") -> None:
         """Mesh file in the reference's layout: ``fileName.off`` (+ ``fileNametriangleAreas.txt``),
-        ``fileName.ply``, or with vertex normals from approximateNormals() ``off_n`` (OFF+N) and
-        ``msms_no_a`` (``fileName.face`` / ``fileName.vert``) (Surface::saveMesh,
-        src/Surface.cpp:10857-11062)."""
+        ``fileName.ply``, or with vertex normals from approximateNormals() and nearest atoms from
+        vertexAtoms(): ``off_n``, ``off_a``, ``off_n_a``, ``msms_no_a`` and ``msms``
+        (``fileName.face`` / ``fileName.vert``) (Surface::saveMesh, src/Surface.cpp:10857-11062)."""
         if self.vertices is None or self.triangles is None:
             raise RuntimeError("no mesh: call triangulateSurface() first")
         name = str(format).lower()
         v = np.ascontiguousarray(self.vertices, np.float64)
         t = np.ascontiguousarray(self.triangles, np.int32)
-        if name in self.NORMAL_MESH_FORMATS:
-            nrm = np.ascontiguousarray(self.approximateNormals(), np.float64)
-            N.check(N.lib().nsg_write_mesh_normals(str(fileName).encode(), self.NORMAL_MESH_FORMATS[name], N.ptr(v),
-                                                   N.ptr(nrm), len(v), N.ptr(t), len(t), int(revert)), "saveMesh")
+        if name in self.ATTR_MESH_FORMATS:
+            fmt = self.ATTR_MESH_FORMATS[name]
+            nrm = np.ascontiguousarray(self.approximateNormals(), np.float64) if fmt != 2 else None
+            ato = self.vertexAtoms() if fmt >= 2 else None
+            N.check(N.lib().nsg_write_mesh_attrs(str(fileName).encode(), fmt, N.ptr(v),
+                                                 None if nrm is None else N.ptr(nrm),
+                                                 None if ato is None else N.ptr(ato), len(v), N.ptr(t), len(t),
+                                                 int(revert)), "saveMesh")
             return
         fmt = self.MESH_FORMATS.get(name)
         if fmt is None:
             raise ValueError(f"unsupported mesh format {format}; available: "
-                             f"{sorted(self.MESH_FORMATS) + sorted(self.NORMAL_MESH_FORMATS)}")
+                             f"{sorted(self.MESH_FORMATS) + sorted(self.ATTR_MESH_FORMATS)}")
         N.check(N.lib().nsg_write_mesh(str(fileName).encode(), fmt, N.ptr(v), len(v), N.ptr(t), len(t), int(revert)),
                 "saveMesh")
 

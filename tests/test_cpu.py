@@ -445,8 +445,8 @@ def test_bench_reference_arm_contract():
 
 
 def test_mesh_normals_and_normal_formats(native_lib, tmp_path):
-    """Triangle-averaged vertex normals (approximateNormals without analytic normals) and the OFF+N
-    and MSMS writers (Surface::saveMesh)."""
+    """Triangle-averaged vertex normals (approximateNormals without analytic normals), nearest atoms
+    (vdwAccessible) and the OFF+N, OFF+A, OFF+N+A and MSMS writers (Surface::saveMesh)."""
     v = np.array([[1.0, 0, 0], [-1.0, 0, 0], [0, 1.0, 0], [0, -1.0, 0], [0, 0, 1.0], [0, 0, -1.0]])
     # octahedron, counter-clockwise seen from outside
     t = np.array([[0, 2, 4], [2, 1, 4], [1, 3, 4], [3, 0, 4], [2, 0, 5], [1, 2, 5], [3, 1, 5], [0, 3, 5]], np.int32)
@@ -468,6 +468,17 @@ def test_mesh_normals_and_normal_formats(native_lib, tmp_path):
     assert off[0] == "OFF+N" and off[3] == "6 8 0"
     assert off[4] == "1.000 0.000 0.000 1.000 0.000 0.000" and off[-1] == "3 0 3 5"
     assert len((tmp_path / "mtriangleAreas.txt").read_text().splitlines()) == 8
+    s.delphi.atoms = np.array([[2.0, 0, 0, 1.5], [0, 0, 2.5, 1.0], [-2.0, 0.1, 0, 1.7]])
+    va = s.vertexAtoms()
+    pd = ((v[:, None, :] - s.delphi.atoms[None, :, :3]) ** 2).sum(-1) - s.delphi.atoms[None, :, 3] ** 2
+    assert np.array_equal(va, np.argmin(pd, axis=1))
+    s.saveMesh("off_n_a", False, str(tmp_path / "a"))
+    offa = (tmp_path / "a.off").read_text().splitlines()
+    assert offa[0] == "OFF+N+A" and offa[4] == "1.000 0.000 0.000 1.000 0.000 0.000 %d" % va[0]
+    s.saveMesh("off_a", False, str(tmp_path / "b"))
+    assert (tmp_path / "b.off").read_text().splitlines()[4] == "1.000 0.000 0.000 %d" % va[0]
+    s.saveMesh("msms", False, str(tmp_path / "c"))
+    assert (tmp_path / "c.vert").read_text().splitlines()[3].split()[7] == str(va[0] + 1)
     s.saveMesh("msms_no_a", True, str(tmp_path / "m"))
     face = (tmp_path / "m.face").read_text().splitlines()
     assert face[0].startswith("# File created by") and face[1] == "#faces" and face[2] == "8"
@@ -477,3 +488,19 @@ def test_mesh_normals_and_normal_formats(native_lib, tmp_path):
     cols = vert[3].split()
     assert len(cols) == 9 and cols[:6] == ["1.000", "0.000", "0.000", "1.000", "0.000", "0.000"] and cols[6:] == ["0", "1", "0"]
     assert vert[3] == "%9.3f %9.3f %9.3f %9.3f %9.3f %9.3f %7d %7d %2d " % (1, 0, 0, 1, 0, 0, 0, 1, 0)
+
+
+def test_vertex_atoms_match_brute_force(native_lib):
+    """The nearest-atom search (shells of grid cells) equals the brute-force least power distance
+    on random globules, vertices inside, on and far outside the atoms' box."""
+    rng = np.random.default_rng(4)
+    L = nb._native.lib()
+    for trial in range(20):
+        n = int(rng.integers(1, 300))
+        atoms = np.concatenate([rng.uniform(-15, 15, (n, 3)), rng.uniform(1.0, 2.2, (n, 1))], axis=1)
+        verts = rng.uniform(-25, 25, (500, 3))
+        verts[:50] = atoms[rng.integers(0, n, 50), :3] + rng.normal(0, 0.5, (50, 3))
+        out = np.zeros(len(verts), np.int32)
+        assert L.nsg_vertex_atoms(verts.ctypes.data, len(verts), atoms.ctypes.data, n, out.ctypes.data) == 0
+        pd = ((verts[:, None, :] - atoms[None, :, :3]) ** 2).sum(-1) - atoms[None, :, 3] ** 2
+        assert np.array_equal(out, np.argmin(pd, axis=1))
