@@ -75,6 +75,10 @@ double nsg_randnum(int64_t* seed);
 int nsg_jitter_atoms(double* atoms_xyzr, int64_t n_atoms, double displacement, int64_t* seed);
 /* xyzr reading of DelPhiShared::loadAtoms (src/DelphiShared.cpp:309-704); out == NULL counts. */
 int64_t nsg_read_xyzr(const char* path, double* out, int64_t capacity);
+/* The ATOM / HETATM records of a pqr file (DelPhiShared::loadAtoms for ".pqr" names,
+ * src/DelphiShared.cpp:365-415, 520-545): x, y, z, radius per atom, atoms with a radius below
+ * 1e-20 skipped; NSG_ERR_ARG on a malformed record (where the reference exits). */
+int64_t nsg_read_pqr(const char* path, double* out, int64_t capacity);
 
 /* ---- patch construction (host) ---- */
 /* ConnollySurface::build / buildConnollyCGAL (src/ConnollySurface.cpp:256, 2326-3316). */

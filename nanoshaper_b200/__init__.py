@@ -10,6 +10,8 @@ from .surface import (  # noqa: F401
     SurfaceBatch,
     SurfaceFactory,
     build_ses_patches,
+    read_atoms,
+    read_pqr,
     read_xyzr,
     reset_seed,
     surfaceFactory,

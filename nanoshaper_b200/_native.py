@@ -91,6 +91,7 @@ _SIGNATURES = {
     "nsg_randnum": ([ctypes.POINTER(_I64)], _D),
     "nsg_jitter_atoms": ([_P, _I64, _D, ctypes.POINTER(_I64)], _INT),
     "nsg_read_xyzr": ([ctypes.c_char_p, _P, _I64], _I64),
+    "nsg_read_pqr": ([ctypes.c_char_p, _P, _I64], _I64),
     "nsg_ses_build": ([_P, _I64, _D, _INT, ctypes.POINTER(_P)], _INT),
     "nsg_patchset_info": ([_P, ctypes.POINTER(_I64), ctypes.POINTER(_I64), _P], _INT),
     "nsg_patchset_export": ([_P, _P, _P, _P, _P], _INT),

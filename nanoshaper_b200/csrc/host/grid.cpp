@@ -101,4 +101,64 @@ int64_t nsg_read_xyzr(const char* path, double* out, int64_t capacity) {
   return n;
 }
 
+// Reads the ATOM / HETATM records of a pqr file as DelPhiShared::loadAtoms does for a file name
+// containing ".pqr" (src/DelphiShared.cpp:365-415, 520-545): whitespace-separated fields, 11 of
+// them (serial, name, residue, chain, residue number, x, y, z, charge, radius) or 10 (no chain);
+// every numeric field must parse completely; other records and empty lines are skipped, and so
+// are atoms with a radius below 1e-20.  Returns the number of atoms (x, y, z, r into out unless
+// NULL), or a negative error code: NSG_ERR_IO (unreadable), NSG_ERR_ARG (a malformed ATOM or
+// HETATM record, where the reference exits), NSG_ERR_CAPACITY (more atoms than capacity).
+int64_t nsg_read_pqr(const char* path, double* out, int64_t capacity) {
+  FILE* f = fopen(path, "r");
+  if (!f) return NSG_ERR_IO;
+  char line[4096];
+  int64_t n = 0;
+  auto whole_int = [](const char* t) {
+    char* e = nullptr;
+    (void)strtol(t, &e, 10);
+    return e != t && *e == '\0';
+  };
+  auto whole_double = [](const char* t, double* v) {
+    char* e = nullptr;
+    *v = strtod(t, &e);
+    return e != t && *e == '\0';
+  };
+  while (fgets(line, sizeof line, f)) {
+    if (strlen(line) <= 1) continue;
+    char* fields[16];
+    int nf = 0;
+    for (char* tok = strtok(line, " \t\r\n"); tok; tok = strtok(nullptr, " \t\r\n")) {
+      if (nf < 16) fields[nf] = tok;
+      nf++;
+    }
+    if (nf == 0 || (strcmp(fields[0], "ATOM") != 0 && strcmp(fields[0], "HETATM") != 0)) continue;
+    if (nf != 10 && nf != 11) {
+      fclose(f);
+      return NSG_ERR_ARG;
+    }
+    const int off = nf == 11 ? 1 : 0;  // the chain field
+    double x, y, z, q, r;
+    if (!whole_int(fields[1]) || !whole_int(fields[4 + off]) || !whole_double(fields[5 + off], &x) ||
+        !whole_double(fields[6 + off], &y) || !whole_double(fields[7 + off], &z) ||
+        !whole_double(fields[8 + off], &q) || !whole_double(fields[9 + off], &r)) {
+      fclose(f);
+      return NSG_ERR_ARG;
+    }
+    if (r < 1e-20) continue;
+    if (out) {
+      if (n >= capacity) {
+        fclose(f);
+        return NSG_ERR_CAPACITY;
+      }
+      out[4 * n + 0] = x;
+      out[4 * n + 1] = y;
+      out[4 * n + 2] = z;
+      out[4 * n + 3] = r;
+    }
+    n++;
+  }
+  fclose(f);
+  return n;
+}
+
 }  // extern "C"

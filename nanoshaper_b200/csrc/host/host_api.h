@@ -27,6 +27,7 @@ int nsg_grid_build(const double* atoms_xyzr, int64_t n_atoms, double scale, doub
 double nsg_randnum(int64_t* seed);
 int nsg_jitter_atoms(double* atoms_xyzr, int64_t n_atoms, double displacement, int64_t* seed);
 int64_t nsg_read_xyzr(const char* path, double* out, int64_t capacity);
+int64_t nsg_read_pqr(const char* path, double* out, int64_t capacity);
 
 // Host-owned patch set produced by a patch builder.
 typedef struct NsPatchSet NsPatchSet;

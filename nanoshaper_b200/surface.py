@@ -117,6 +117,26 @@ def read_xyzr(path: str | Path) -> np.ndarray:
     return out
 
 
+def read_pqr(path: str | Path) -> np.ndarray:
+    """Atoms of the ATOM / HETATM records of a pqr file as an (N, 4) float64 array (x, y, z,
+    radius); atoms with a zero radius are skipped, as DelPhiShared::loadAtoms does."""
+    L = N.lib()
+    n = L.nsg_read_pqr(str(path).encode(), None, 0)
+    if n < 0:
+        raise N.NativeError(f"cannot read {path}: {N.ERRORS.get(n, n)}")
+    out = np.zeros((n, 4), np.float64)
+    n2 = L.nsg_read_pqr(str(path).encode(), N.ptr(out), n)
+    if n2 != n:
+        raise N.NativeError(f"cannot read {path}")
+    return out
+
+
+def read_atoms(path: str | Path) -> np.ndarray:
+    """Atoms of a molecule file, pqr when its name contains ".pqr" and xyzr otherwise (the choice
+    DelPhiShared::loadAtoms makes, src/DelphiShared.cpp:338-342)."""
+    return read_pqr(path) if ".pqr" in str(path) else read_xyzr(path)
+
+
 class DelPhiShared:
     """Grid environment: the atoms, the cubic grid and the maps produced on it."""
 
@@ -679,10 +699,18 @@ def surfaceFactory() -> SurfaceFactory:
 class NanoShaper:
     """Library facade: atoms + configuration in, surface volume / area / maps out."""
 
-    def __init__(self, atoms: np.ndarray, surface: str = "ses", probe: float = DEFAULT_PROBE,
-                 scale: float = DEFAULT_SCALE, perfil: float = DEFAULT_PERFIL, config: ConfigFile | None = None,
-                 device: int = 0, precision: str = "fp64"):
+    def __init__(self, atoms: "np.ndarray | str | Path | None" = None, surface: str = "ses",
+                 probe: float = DEFAULT_PROBE, scale: float = DEFAULT_SCALE, perfil: float = DEFAULT_PERFIL,
+                 config: ConfigFile | None = None, device: int = 0, precision: str = "fp64"):
         cf = config or ConfigFile()
+        # atoms: an (N, 4) array, a molecule file (xyzr, or pqr by name), or, when None, the
+        # configuration's XYZR_FileName as in a .prm file
+        if atoms is None:
+            if not cf.keyExists("XYZR_FileName"):
+                raise ValueError("no atoms: pass an array or a file, or set XYZR_FileName")
+            atoms = cf.read("XYZR_FileName", "", str).strip()
+        if isinstance(atoms, (str, Path)):
+            atoms = read_atoms(atoms)
         if not cf.keyExists("Surface"):
             cf.add("Surface", surface)
         if not cf.keyExists("Probe_Radius"):

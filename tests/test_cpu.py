@@ -504,3 +504,33 @@ def test_vertex_atoms_match_brute_force(native_lib):
         assert L.nsg_vertex_atoms(verts.ctypes.data, len(verts), atoms.ctypes.data, n, out.ctypes.data) == 0
         pd = ((verts[:, None, :] - atoms[None, :, :3]) ** 2).sum(-1) - atoms[None, :, 3] ** 2
         assert np.array_equal(out, np.argmin(pd, axis=1))
+
+
+def test_pqr_reader_and_facade_input(native_lib, tmp_path):
+    """pqr files are read as DelPhiShared::loadAtoms reads them: ATOM / HETATM records with 10 or
+    11 fields, other records skipped, zero-radius atoms dropped, a malformed record an error; the
+    facade takes an xyzr or pqr file, or XYZR_FileName from the configuration."""
+    pqr = tmp_path / "mol.pqr"
+    pqr.write_text("REMARK  generated\n"
+                   "ATOM      1  N   MET A   1      1.000   2.000   3.000  -0.30 1.8500\n"
+                   "ATOM      2  H   MET A   1      1.500   2.500   3.500   0.30 0.0000\n"
+                   "HETATM    3  O   HOH     2     -4.250   0.000  10.500  -0.80 1.5200\n"
+                   "\n"
+                   "TER\n"
+                   "END\n")
+    a = nb.read_pqr(pqr)
+    assert a.shape == (2, 4)
+    assert np.array_equal(a, [[1.0, 2.0, 3.0, 1.85], [-4.25, 0.0, 10.5, 1.52]])
+    assert np.array_equal(nb.read_atoms(pqr), a)
+    bad = tmp_path / "bad.pqr"
+    bad.write_text("ATOM      1  N   MET A   1      1.000   2.000   3.000  -0.30\n")
+    with pytest.raises(nb._native.NativeError):
+        nb.read_pqr(bad)
+    xyzr = tmp_path / "mol.xyzr"
+    xyzr.write_text("1.0 2.0 3.0 1.85\n-4.25 0.0 10.5 1.52\n")
+    assert np.array_equal(nb.read_atoms(xyzr), a)
+    ns = nb.NanoShaper(str(pqr))
+    assert np.array_equal(ns.ds.atoms, a)
+    cf = nb.ConfigFile()
+    cf.add("XYZR_FileName", str(xyzr))
+    assert np.array_equal(nb.NanoShaper(config=cf).ds.atoms, a)
