@@ -212,9 +212,12 @@ int nsg_download_hits(nsg_ctx* ctx, int ray_set, int32_t* counts, double* dst, i
  * from a patch set, all in device memory the caller owns.  Scratch is one fixed file-scope device
  * array (16.5 MiB): at most 65536 status rays (ny * nz) and 32 hits per ray; larger grids return
  * NSG_ERR_CAPACITY before any launch, a ray with more hits returns NSG_ERR_CAPACITY after the
- * call.  Allocates nothing.  The first call on each device (with that device current) looks up
- * the scratch address and must come before any stream capture.  Calls that overlap on the GPU
- * share the scratch and race: serialise them.  Synchronises `stream` before returning. */
+ * launches and leaves the status map unspecified.  d_pool and d_pool_flag may be NULL only when
+ * no patch has pool entries (else NSG_ERR_ARG).  Allocates nothing.  Every call looks up the
+ * scratch address on the current device; under lazy module loading the first call in a process
+ * reserves the array, so a process with fixed device memory makes one call at start-up.  A call
+ * synchronises `stream` and reads its result back, so it cannot be made while any stream is
+ * being captured.  Calls that overlap on the GPU share the scratch and race: serialise them. */
 int nsg_status_noalloc(const NsGrid* grid, int64_t n_patches, const double* d_f64, const int32_t* d_i32,
                        const double* d_pool, const int8_t* d_pool_flag, double probe_radius, int32_t* d_status,
                        double* volume, void* stream);

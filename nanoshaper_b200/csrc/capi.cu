@@ -669,11 +669,11 @@ int nsg_patch_grads(nsg_ctx* c, double* gvol, double* garea) {
 int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume);
 
 // Peak floating-point rate of this GPU measured live: independent fused multiply-add chains
-// (8 per thread, 148 x 8 blocks of 256 threads), 2 flops per FMA; precision 0 = FP64, 1 = FP32.
+// (8 per thread, 8 blocks of 256 threads per SM), 2 flops per FMA; precision 0 = FP64, 1 = FP32.
 int nsg_fp_peak(nsg_ctx* c, int precision, double* flops_per_s) {
   if (!c || !flops_per_s || (precision != 0 && precision != 1)) return NSG_ERR_ARG;
   CK(cudaSetDevice(c->device));
-  const int blocks = 148 * 8, threads = 256, iters = 4096;
+  const int blocks = nsg::sm_count() * 8, threads = 256, iters = 4096;
   CK(c->red_out.ensure(blocks * threads * sizeof(double)));
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));

@@ -18,6 +18,7 @@
 #include <cub/cub.cuh>
 
 #include "cavity.h"
+#include "pipeline.h"
 
 namespace nsg {
 
@@ -193,7 +194,8 @@ __global__ void k_status_write(RunArgs A, const int32_t* __restrict__ label_of, 
 
 int grid_for(int64_t n, int threads = 256) {
   int64_t b = (n + threads - 1) / threads;
-  return (int)(b < 148 * 32 ? (b < 1 ? 1 : b) : 148 * 32);
+  const int64_t cap = (int64_t)sm_count() * 32;
+  return (int)(b < cap ? (b < 1 ? 1 : b) : cap);
 }
 
 }  // namespace

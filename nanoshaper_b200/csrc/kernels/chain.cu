@@ -32,7 +32,7 @@ cudaError_t launch_chain(int64_t np, const int32_t* i32, const double* f64, cons
                          double* gvol_atoms, double* garea_atoms, int32_t* n_bad, cudaStream_t s) {
   if (np <= 0) return cudaSuccess;
   int64_t blocks = (np + 255) / 256;
-  if (blocks > 148 * 32) blocks = 148 * 32;
+  if (blocks > (int64_t)sm_count() * 32) blocks = (int64_t)sm_count() * 32;
   k_chain<<<(unsigned)blocks, 256, 0, s>>>(np, i32, f64, patch_atoms, atoms, probe, gpatch_vol, gpatch_area,
                                            gvol_atoms, garea_atoms, n_bad);
   return cudaGetLastError();

@@ -451,7 +451,8 @@ __global__ void k_grad_vert(MCArgs A) {
 
 int grid_for(int64_t n, int threads) {
   int64_t b = (n + threads - 1) / threads;
-  return (int)(b < 148 * 32 ? (b < 1 ? 1 : b) : 148 * 32);
+  const int64_t cap = (int64_t)sm_count() * 32;
+  return (int)(b < cap ? (b < 1 ? 1 : b) : cap);
 }
 
 }  // namespace

@@ -169,10 +169,14 @@ struct PatchDev {
   const int32_t* win;  // 6 per patch: start x,y,z, end x,y,z; start = -1 when culled
 };
 
+// Streaming multiprocessors of the current device (queried once per device and cached); grids of
+// the grid-stride kernels are sized as multiples of it.
+int sm_count();
+
 // Launch shapes of the tracer, picked per context by nsg_autotune (defaults below).
 struct TuneParams {
   int isect_threads = 256;  // threads per block of the intersection kernels (64..256)
-  int isect_bpsm = 16;      // their blocks per SM (grid = 148 * isect_bpsm, grid-stride)
+  int isect_bpsm = 16;      // their blocks per SM (grid = SMs * isect_bpsm, grid-stride)
   int cand_threads = 256;   // threads per block of the candidate kernel (one warp per patch)
 };
 

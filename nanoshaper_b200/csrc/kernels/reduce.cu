@@ -87,10 +87,23 @@ __global__ void k_batch_atoms(int64_t np, const int32_t* __restrict__ patch_stru
 
 int grid_of(int64_t n) {
   int64_t b = (n + 255) / 256;
-  return (int)(b < 1 ? 1 : (b > 148 * 32 ? 148 * 32 : b));
+  const int64_t cap = (int64_t)sm_count() * 32;
+  return (int)(b < 1 ? 1 : (b > cap ? cap : b));
 }
 
 }  // namespace
+
+int sm_count() {
+  static int cache[64] = {0};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  if (cache[dev] == 0) {
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+    cache[dev] = n;
+  }
+  return cache[dev];
+}
 
 cudaError_t launch_batch_patches(int64_t np, const int64_t* patch_off, int n, const int64_t* pool_off, int32_t* i32,
                                  int32_t* patch_struct, int32_t* err, cudaStream_t s) {

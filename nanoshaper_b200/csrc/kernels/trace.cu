@@ -471,13 +471,13 @@ __global__ void __launch_bounds__(256) k_cand(TraceCtx C, CandOut co) {
 template <int PN>
 void launch_isect(const TraceCtx& C, const CandOut& co, const HitStore& hs, int precision, const TuneParams& tp,
                   cudaStream_t s) {
-  const int ig = 148 * tp.isect_bpsm, it = tp.isect_threads;
+  const int ig = sm_count() * tp.isect_bpsm, it = tp.isect_threads;
   if (precision == 1) {
     launch_isect_mixed<PN>(C, co, hs, tp, s);
     // the deferred candidates, in double precision (few: a small grid)
     const CandOut dco{co.dsph, co.dtor, co.dcap, co.dcount, nullptr, nullptr, 0, nullptr};
-    k_isect<PN, false><<<148, 256, 0, s>>>(C, dco, hs);
-    k_isect<PN, true><<<148, 256, 0, s>>>(C, dco, hs);
+    k_isect<PN, false><<<sm_count(), 256, 0, s>>>(C, dco, hs);
+    k_isect<PN, true><<<sm_count(), 256, 0, s>>>(C, dco, hs);
   } else {
     k_isect<PN, false><<<ig, it, 0, s>>>(C, co, hs);
     k_isect<PN, true><<<ig, it, 0, s>>>(C, co, hs);
@@ -930,7 +930,7 @@ cudaError_t launch_trace(const PatchDev& P, const BatchDev& B, int set, int64_t 
   if (P.n > 0) {
     const int wpb = tp.cand_threads / 32;
     int64_t blocks = (P.n + 32 * wpb - 1) / (32 * wpb);
-    if (blocks > 148 * 64) blocks = 148 * 64;
+    if (blocks > (int64_t)sm_count() * 64) blocks = (int64_t)sm_count() * 64;
     k_cand<<<(unsigned)blocks, tp.cand_threads, 0, s>>>(C, co);
   }
   if (ev) cudaEventRecord(ev[1], s);

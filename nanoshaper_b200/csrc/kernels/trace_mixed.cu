@@ -7,7 +7,7 @@ namespace nsg {
 template <int PN>
 void launch_isect_mixed(const TraceCtx& C, const CandOut& co, const HitStore& hs, const TuneParams& tp,
                         cudaStream_t s) {
-  const int ig = 148 * tp.isect_bpsm, it = tp.isect_threads;
+  const int ig = sm_count() * tp.isect_bpsm, it = tp.isect_threads;
   k_isect_mixed<PN, false><<<ig, it, 0, s>>>(C, co, hs);
   k_isect_mixed<PN, true><<<ig, it, 0, s>>>(C, co, hs);
 }

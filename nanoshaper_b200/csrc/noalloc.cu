@@ -14,11 +14,16 @@
 // streams, or different host threads on the same device) race on the array and must be
 // serialised by the caller.
 //
-// The first call on each device looks up the array's device address with cudaGetSymbolAddress
-// while that device is current; make that first call before capturing a stream into a CUDA graph.
+// Every call looks up the array's device address with cudaGetSymbolAddress on the current
+// device, so the address stays valid across a cudaDeviceReset.  With lazy module loading (the
+// CUDA default) the first call in a process loads the module and reserves the array; a caller
+// whose device memory is fixed after start-up makes one call at start-up.  A call synchronises
+// its stream and reads the result back to the host, so it cannot be made while any stream is
+// being captured into a CUDA graph.
+//
+// A ray with more than kMaxHits hits makes the call return NSG_ERR_CAPACITY after its launches;
+// the status map is then unspecified.
 #include <cuda_runtime.h>
-
-#include <mutex>
 
 #include "host/host_api.h"
 #include "kernels/ray_math.cuh"
@@ -86,6 +91,11 @@ __global__ void k_status_noalloc(Geo g, int64_t np, const double* __restrict__ f
       double t[4];
       if (!nsg::ray_sphere_f64(pa, dir, f, rad, &t[0], &t[1])) continue;
       const int32_t* ir = i32 + NS_PATCH_I32 * p;
+      if (ir[2] > 0 && (pool == nullptr || flag == nullptr)) {
+        err[0] = 2.0;  // pool entries referenced but no pool given
+        ovf = true;
+        break;
+      }
       int numInt = 2;
       if (ir[0] == NS_EDGE_REG || ir[0] == NS_EDGE_SING) numInt = nsg::ray_torus_f64(f, probe, 0, pa, ray_dir, t);
       for (int i = 0; i < numInt; i++) {
@@ -147,21 +157,13 @@ __global__ void k_noalloc_sum(int64_t nrays, double* scratch) {
   if (threadIdx.x == 0) scratch[kScratch - 1] = part[0];
 }
 
-std::mutex g_setup_mutex;
-double* g_scratch_addr[64] = {};
-
-// Device address of the scratch array on the current device, looked up once per device.
+// Device address of the scratch array on the current device (host code cannot use the symbol
+// itself: on the host it names a stand-in, not device memory).
 int scratch_address(double** out) {
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return NSG_ERR_CUDA;
-  std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (!g_scratch_addr[dev]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p) return NSG_ERR_CUDA;
-    g_scratch_addr[dev] = (double*)p;
-  }
-  *out = g_scratch_addr[dev];
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p) return NSG_ERR_CUDA;
+  *out = (double*)p;
   return NSG_OK;
 }
 
@@ -198,6 +200,7 @@ int nsg_status_noalloc(const NsGrid* grid, int64_t n_patches, const double* d_f6
   double out[2] = {0.0, 0.0};
   if (cudaMemcpyAsync(out, err, 2 * sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess) return NSG_ERR_CUDA;
   if (cudaStreamSynchronize(s) != cudaSuccess) return NSG_ERR_CUDA;
+  if (out[0] == 2.0) return NSG_ERR_ARG;
   if (out[0] != 0.0) return NSG_ERR_CAPACITY;
   *volume = grid->A * out[1];
   return NSG_OK;

@@ -709,6 +709,9 @@ class NanoShaper:
             if not cf.keyExists("XYZR_FileName"):
                 raise ValueError("no atoms: pass an array or a file, or set XYZR_FileName")
             atoms = cf.read("XYZR_FileName", "", str).strip()
+            # the reference runs in the directory of its .prm file: a relative name is read there
+            if cf.path is not None and not Path(atoms).is_absolute() and not Path(atoms).exists():
+                atoms = str(cf.path.parent / atoms)
         if isinstance(atoms, (str, Path)):
             atoms = read_atoms(atoms)
         if not cf.keyExists("Surface"):

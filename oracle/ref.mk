@@ -1,7 +1,11 @@
 # Compiles the reference's self-contained math (src/tools.cpp, src/sturm, src/ConfigFile) from
-# its sources under /root/reference into oracle/_ref/libnsref.so, with the stand-in headers of
-# ref_shim/ for the two external headers that translation unit names.  Test infrastructure only.
-REF ?= /root/reference/src
+# its sources into oracle/_ref/libnsref.so, with the stand-in headers of ref_shim/ for the two
+# external headers that translation unit names.  Test infrastructure only.
+# NANOSHAPER_REFERENCE names the root of a NanoShaper source checkout (read only).
+ifeq ($(strip $(NANOSHAPER_REFERENCE)),)
+$(error set NANOSHAPER_REFERENCE to the root of a NanoShaper source checkout)
+endif
+REF ?= $(NANOSHAPER_REFERENCE)/src
 CXX ?= g++
 OUT = _ref
 CXXFLAGS = -O2 -std=c++14 -fPIC -ffp-contract=off -fno-fast-math -w \

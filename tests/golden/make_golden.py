@@ -1,11 +1,12 @@
 """Generates tests/golden/ref_math.npz: golden vectors of the reference's own ray/solver math.
 
-Needs the reference sources (compiled into oracle/_ref/libnsref.so by oracle/ref.mk).  Inputs are
+Needs the reference sources: NANOSHAPER_REFERENCE names the root of a NanoShaper source checkout,
+compiled into oracle/_ref/libnsref.so by oracle/ref.mk.  Inputs are
 seeded: rays of the status and triangulation panels of a synthetic globule against its sphere
 and torus patches (the patch set comes from this package's host builder), plus the jitter
 generator sequence, rintp and plane-through-three-points values.  Outputs are evaluated by the
 reference functions raySphere, rayTorus (analytical and Sturm), randnum, rintp and plane3points
-(src/tools.cpp).  Run:  python tests/golden/make_golden.py
+(src/tools.cpp).  Run:  NANOSHAPER_REFERENCE=<checkout> python tests/golden/make_golden.py
 """
 from __future__ import annotations
 

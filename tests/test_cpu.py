@@ -534,3 +534,34 @@ def test_pqr_reader_and_facade_input(native_lib, tmp_path):
     cf = nb.ConfigFile()
     cf.add("XYZR_FileName", str(xyzr))
     assert np.array_equal(nb.NanoShaper(config=cf).ds.atoms, a)
+
+
+def test_mc_case_table_matches_reference_tritable():
+    """The marching-cubes case table (csrc/mc_cases.h) equals the reference's triTable
+    (src/tools.h:181, extracted into tests/golden/fixtures/mc_tritable.npy) on all 256 cases."""
+    root = Path(__file__).resolve().parent.parent
+    text = (root / "nanoshaper_b200" / "csrc" / "mc_cases.h").read_text()
+    body = text[text.index("kNsMcCases[256]"):]
+    cases = re.findall(r'"([0-9a-b]*)"', body)
+    assert len(cases) == 256
+    ref = np.load(root / "tests" / "golden" / "fixtures" / "mc_tritable.npy")
+    for c, s in enumerate(cases):
+        ours = [int(ch, 16) for ch in s]
+        theirs = [int(v) for v in ref[c] if v >= 0]
+        assert ours == theirs, f"case {c}: {ours} vs {theirs}"
+
+
+def test_reference_fixture_config_parses(native_lib):
+    """The reference's own 1crn SES configuration, read through ConfigFile, drives the facade: the
+    atoms come from its XYZR_FileName (resolved beside the .prm), the grid from Grid_scale and
+    Grid_perfil."""
+    fx = Path(__file__).resolve().parent / "golden" / "fixtures"
+    cf = nb.ConfigFile(fx / "1crn_ses_conf.prm")
+    assert cf.read("Surface", "", str).strip() == "ses"
+    assert cf.read("Grid_perfil", 0.0, float) == 90.0
+    assert cf.read("Compute_Vertex_Normals", False, bool) is True
+    ns = nb.NanoShaper(config=cf)
+    assert len(ns.ds.atoms) == 327
+    assert ns.scale == 2.0 and ns.perfil == 90.0
+    ref_atoms = nb.read_xyzr(fx / "1crn.xyzr")
+    np.testing.assert_array_equal(ns.ds.atoms, ref_atoms)

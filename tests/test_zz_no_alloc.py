@@ -80,3 +80,33 @@ def test_noalloc_rejects_oversize_grid(native_lib):
     vol = ctypes.c_double()
     rc = fn(ctypes.byref(g), 0, None, None, None, None, 1.4, ctypes.c_void_p(16), ctypes.byref(vol), None)
     assert rc == ERR_CAPACITY
+
+
+def test_noalloc_reports_hit_overflow(native_lib):
+    """A status ray with more than 32 hits: 17 disjoint spheres strung along the x axis give 34
+    hits on the ray through their centres; the call returns NSG_ERR_CAPACITY after its launches."""
+    import torch
+
+    fn = _bind(native_lib)
+    n = 17
+    atoms = np.zeros((n, 4))
+    atoms[:, 0] = np.arange(n) * 3.0
+    atoms[:, 3] = 1.0
+    ds = nb.DelPhiShared(atoms, 2.0, 50.0)
+    g = ds.grid
+    f64 = np.zeros((n, 20))
+    f64[:, 0:4] = atoms
+    i32 = np.zeros((n, 4), np.int32)  # point patches without clipping spheres
+    # put the atom centres on the grid's middle status ray (j, k) so that it crosses all of them
+    jm, km = g.ny // 2, g.nz // 2
+    f64[:, 1] = g.ymin + jm * g.side
+    f64[:, 2] = g.zmin + km * g.side
+    dev = torch.device("cuda:0")
+    d_f64 = torch.from_numpy(f64).to(dev)
+    d_i32 = torch.from_numpy(i32).to(dev)
+    status = torch.zeros(g.nx * g.ny * g.nz, dtype=torch.int32, device=dev)
+    vol = ctypes.c_double()
+    stream = torch.cuda.current_stream(dev)
+    rc = fn(ctypes.byref(g), n, d_f64.data_ptr(), d_i32.data_ptr(), None, None, 1.4, status.data_ptr(),
+            ctypes.byref(vol), stream.cuda_stream)
+    assert rc == ERR_CAPACITY
