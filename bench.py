@@ -243,6 +243,115 @@ def ensemble_cpu_baseline(surfs, threads: int, target_s: float = 10.0, steps: in
             "sample": sample, "unit": "structures/s"}
 
 
+def mixed_vs_fp64_accuracy(L, N, ctx, surfs, flags: int) -> dict:
+    """Accuracy terms of the metric on a batch: the ray cast in double precision and in mixed
+    precision (untimed, hits kept), compared ray by ray.
+
+    * max_hit_error_A: largest |hit_mixed - hit_fp64| in Angstrom over every hit of every ray set
+      of every structure (rays with equal hit counts; count_mismatch_rays counts the others);
+    * status_mismatch_nodes: status-map nodes whose inside / outside decision differs, from the
+      status rays' interval ends (the node range [a, b] of each interval, as the fill computes it),
+      and how many of them lie within 1e-6 A of a double-precision interval end (near-node);
+    * insideness_mismatch_bits: differing bits of the insideness grids;
+    * near_node_hits: double-precision interval ends within 1e-6 A of a decision coordinate (a node
+      for status rays, a rintp half-integer for triangulation rays)."""
+    def run(prec):
+        v = ctypes.c_double()
+        N.check(L.nsg_raycast(ctx, flags | N.KEEP_HITS, prec, ctypes.byref(v)), "raycast")
+        sets = []
+        for s in range(4):
+            tot = sum(rays_in_set(sf.delphi.grid, s) for sf in surfs)
+            counts = np.zeros(tot, np.int32)
+            rc = L.nsg_download_hits(ctx, s, N.ptr(counts), None, 0)
+            if rc < 0:
+                N.check(rc, "download hits")
+            vals = np.zeros(int(counts.astype(np.int64).sum()))
+            N.check(L.nsg_download_hits(ctx, s, N.ptr(counts), N.ptr(vals), len(vals)), "download hits")
+            sets.append((counts, vals))
+        words = sum(((sf.delphi.grid.nx + 31) // 32) * sf.delphi.grid.ny * sf.delphi.grid.nz for sf in surfs)
+        bits = np.empty(words, np.uint32)
+        N.check(L.nsg_download_insideness(ctx, N.ptr(bits)), "download insideness")
+        return sets, bits
+
+    r64, b64 = run(0)
+    r32, b32 = run(1)
+    out = {"max_hit_error_A": 0.0, "count_mismatch_rays": 0, "status_mismatch_nodes": 0,
+           "status_mismatch_near_node": 0, "insideness_mismatch_bits": 0, "near_node_hits": 0, "hits_compared": 0}
+    out["insideness_mismatch_bits"] = int(np.unpackbits((b64 ^ b32).view(np.uint8)).sum())
+    near = 1e-6
+    for s in range(4):
+        c64, v64 = r64[s]
+        c32, v32 = r32[s]
+        ray0 = 0
+        h64 = np.concatenate([[0], np.cumsum(c64.astype(np.int64))])
+        h32 = np.concatenate([[0], np.cumsum(c32.astype(np.int64))])
+        for sf in surfs:
+            g = sf.delphi.grid
+            nr = rays_in_set(g, s)
+            a64, a32 = c64[ray0:ray0 + nr], c32[ray0:ray0 + nr]
+            t64 = v64[h64[ray0]:h64[ray0 + nr]]
+            t32 = v32[h32[ray0]:h32[ray0 + nr]]
+            ray0 += nr
+            eq = a64 == a32
+            out["count_mismatch_rays"] += int((~eq).sum())
+            vc = (0, 0, 2, 1)[s]
+            ncoord = (g.nx, g.ny, g.nz)[vc]
+            vmin = (g.xmin, g.ymin, g.zmin)[vc]
+            delta = 0.0 if s == 0 else 1e-10 - g.hside
+            pa = (vmin + 0.0 * g.side) + delta
+            dirl = ((vmin + (ncoord - 1) * g.side) + delta) - pa
+            m64 = np.repeat(eq, a64)
+            m32 = np.repeat(eq, a32)
+            if m64.any():
+                d = np.abs(t64[m64] - t32[m32]) * abs(dirl)
+                out["max_hit_error_A"] = max(out["max_hit_error_A"], float(d.max()))
+                out["hits_compared"] += int(m64.sum())
+            lim = pa + dirl * t64
+            u = (lim - vmin) * g.scale
+            if s == 0:
+                dist = np.abs(u - np.rint(u)) * g.side
+            else:
+                dist = np.abs(u - np.floor(u) - 0.5) * g.side
+            out["near_node_hits"] += int((dist < near).sum())
+            if s == 0:
+                # status decisions: node range [a, b] of every kept pair of rays with equal counts
+                even = eq & (a64 > 0) & (a64 % 2 == 0)
+                sel64 = np.repeat(even, a64)
+                sel32 = np.repeat(even, a32)
+                p64 = t64[sel64].reshape(-1, 2)
+                p32 = t32[sel32].reshape(-1, 2)
+                if len(p64):
+                    def ranges(p):
+                        keep = np.abs(p[:, 1] - p[:, 0]) >= 1e-8
+                        l1 = pa + dirl * p[:, 0]
+                        l2 = pa + dirl * p[:, 1]
+                        a = np.clip(np.floor((l1 - vmin) * g.scale + 0.5), 0, g.nx - 1)
+                        b = np.clip(np.floor((l2 - vmin) * g.scale + 0.5), 0, g.nx - 1)
+                        a = a + ((vmin + a * g.side) < l1)
+                        b = b - ((vmin + b * g.side) > l2)
+                        return keep, a, b, l1, l2
+                    k64, a_64, b_64, l1_64, l2_64 = ranges(p64)
+                    k32, a_32, b_32, _, _ = ranges(p32)
+                    e64 = np.where(k64 & (a_64 <= b_64), b_64 - a_64 + 1, 0)
+                    e32 = np.where(k32 & (a_32 <= b_32), b_32 - a_32 + 1, 0)
+                    diff = (k64 != k32) | (a_64 != a_32) | (b_64 != b_32)
+                    nodes = np.where(k64 == k32, np.abs(a_64 - a_32) + np.abs(b_64 - b_32), np.abs(e64 - e32))
+                    nodes = np.where(diff, np.maximum(nodes, 1), 0)
+                    out["status_mismatch_nodes"] += int(nodes.sum())
+                    if diff.any():
+                        ul1 = (l1_64 - vmin) * g.scale
+                        ul2 = (l2_64 - vmin) * g.scale
+                        nr1 = np.abs(ul1 - np.rint(ul1)) * g.side < near
+                        nr2 = np.abs(ul2 - np.rint(ul2)) * g.side < near
+                        out["status_mismatch_near_node"] += int(nodes[diff & (nr1 | nr2)].sum())
+    out["status_mismatch_not_near_node"] = out["status_mismatch_nodes"] - out["status_mismatch_near_node"]
+    return out
+
+
+def rays_in_set(g, s: int) -> int:
+    return (g.ny * g.nz, g.ny * g.nz, g.nx * g.ny, g.nx * g.nz)[s]
+
+
 def run_ensemble(args, world: int, rank: int, local: int) -> None:
     """Batched conformer ensemble: one step = ray casting (4 ray sets) + marching cubes of every
     structure of the ensemble in one batch; value = structures/s over all ranks (replicas)."""
@@ -330,7 +439,10 @@ def run_ensemble(args, world: int, rank: int, local: int) -> None:
         N.check(L.nsg_batch_results(ctx, N.ptr(vol), N.ptr(area)), "batch results")
         return vol, area
 
-    # double-precision batch: reference numbers for the accuracy comparison
+    # the metric's accuracy terms (untimed): every hit of the mixed-precision ray cast against the
+    # double-precision one, status and insideness decisions, near-node counts
+    accuracy = mixed_vs_fp64_accuracy(L, N, ctx, surfs, N.STATUS | N.ACCURATE_TRIANGULATION)
+    # double-precision batch: reference numbers for the volume / area comparison
     step(0)
     vol64, area64 = results()
     # per-stage kernel times of the measured precision from one profiled pass
@@ -346,6 +458,9 @@ def run_ensemble(args, world: int, rank: int, local: int) -> None:
 
     for _ in range(args.warmup):
         nv, nt = step(prec)
+    st = np.zeros(8, np.int64)
+    N.check(L.nsg_stats(ctx, N.ptr(st), 8), "stats")
+    active_cubes = int(st[4])
     barrier()
     clk = ClockSampler(local)
     clk.start()
@@ -488,9 +603,10 @@ def run_ensemble(args, world: int, rank: int, local: int) -> None:
                 "speedup_vs_fp64_plain": ms_plain / ms_per_step,
                 "speedup_vs_fp64_batched": ms_fp64_batch / ms_per_step,
                 "max_rel_volume_diff_vs_fp64": rel(vol, vol64), "max_rel_area_diff_vs_fp64": rel(area, area64),
+                "accuracy_vs_fp64": accuracy,
             },
             "result": {"volume_sum": float(vol.sum()), "area_sum": float(area.sum()), "vertices": nv,
-                       "triangles": nt},
+                       "triangles": nt, "active_cubes": active_cubes},
             "host": {"patch_build_s": t_build, "generator_s": t_gen},
             "clocks": clocks,
             "e2e": {"value": world * nstruct * 1000.0 / e2e_ms, "unit": "structures/s", "h2d_bytes_per_step": int(h2d),

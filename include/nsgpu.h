@@ -61,7 +61,16 @@ typedef struct NsGrid {
  *   pool: 4 doubles per entry: clipping sphere (x, y, z, r^2) for points, plane (a, b, c, d)
  *         for facets and edges (a point with a*x+b*y+c*z+d > 0 is cut away)
  *   pool_flag: 1 byte per entry; for edges, 1 on the first plane of an acute pair.
- * Mirrors the cell records of src/ConnollySurface.h:31-167. */
+ * Mirrors the cell records of src/ConnollySurface.h:31-167.
+ *
+ * Skin cells (kinds 5 Del0 / reduced Voronoi cell, 6 Del1 / edge prism, 7 Del2 / facet prism,
+ * 8 Del3 / reduced tetrahedron; the MixedCell records of src/SkinSurface.h:18-105):
+ *   f64 : [0..2] local origin (Del0: the atom centre, else the centre of the cell's box),
+ *         [3] Del0: atom radius (equatorial-disc culling), else half the box diagonal,
+ *         [4..13] quadric q11, q22, q33, q44, q12, q23, q34, q13, q24, q14 (the reference's coding,
+ *         src/SkinSurface.cpp:4461), [14..16] box low corner, [17..19] box high corner
+ *   pool: the cell's planes (a, b, c, d); a point with a*x+b*y+c*z+d > 0 is outside the cell
+ *         (Del0 planes are stored negated, which turns the reference's "< 0" test into this one). */
 
 typedef struct nsg_ctx nsg_ctx;
 typedef struct NsPatchSet NsPatchSet;
@@ -83,7 +92,18 @@ int64_t nsg_read_pqr(const char* path, double* out, int64_t capacity);
 /* ---- patch construction (host) ---- */
 /* ConnollySurface::build / buildConnollyCGAL (src/ConnollySurface.cpp:256, 2326-3316). */
 int nsg_ses_build(const double* atoms_xyzr, int64_t n_atoms, double probe_radius, int n_threads, NsPatchSet** out);
+/* SkinSurface::build / buildSkinCGAL (src/SkinSurface.cpp:329, 1271-1812): the mixed cells of
+ * atoms weighted r^2/s (jittered beforehand, nsg_jitter_atoms) plus the reference's six dummy
+ * points, with shrink factor s in (0, 1); the regular triangulation is this library's own (exact
+ * predicates), not CGAL's.  NSG_ERR_GEOMETRY flags a degenerate configuration (patches are still
+ * returned). */
+int nsg_skin_build(const double* atoms_xyzr, int64_t n_atoms, double shrink, int n_threads, NsPatchSet** out);
+/* Exact predicates of that triangulation on integer points (x, y, z, w; 5 points): orientation of
+ * points 0..3 (+1, 0, -1) and whether point 4 conflicts with their orthosphere (tests). */
+int nsg_skin_predicates(const int64_t* points, int* orient, int* conflict);
 int nsg_patchset_info(const NsPatchSet* ps, int64_t* n_patches, int64_t* n_pool, int64_t counts[5]);
+/* Patches per kind, counts[k] for k < n (kinds 0..8: the five SES kinds, then the four skin cells). */
+int nsg_patchset_kind_counts(const NsPatchSet* ps, int64_t* counts, int n);
 int nsg_patchset_export(const NsPatchSet* ps, double* f64, int32_t* i32, double* pool, int8_t* pool_flag);
 /* The atoms every patch depends on, 3 per patch (-1 unused): point (i), facet (i, j, k), edge (i, j). */
 int nsg_patchset_atoms(const NsPatchSet* ps, int32_t* out);
@@ -212,8 +232,9 @@ int nsg_download_hits(nsg_ctx* ctx, int ray_set, int32_t* counts, double* dst, i
  * from a patch set, all in device memory the caller owns.  Scratch is one fixed file-scope device
  * array (16.5 MiB): at most 65536 status rays (ny * nz) and 32 hits per ray; larger grids return
  * NSG_ERR_CAPACITY before any launch, a ray with more hits returns NSG_ERR_CAPACITY after the
- * launches and leaves the status map unspecified.  d_pool and d_pool_flag may be NULL only when
- * no patch has pool entries (else NSG_ERR_ARG).  Allocates nothing.  Every call looks up the
+ * launches and leaves the status map unspecified.  SES patch sets only (a skin cell returns
+ * NSG_ERR_ARG); d_pool and d_pool_flag may be NULL only when no patch has pool entries (else
+ * NSG_ERR_ARG).  Allocates nothing.  Every call looks up the
  * scratch address on the current device; under lazy module loading the first call in a process
  * reserves the array, so a process with fixed device memory makes one call at start-up.  A call
  * synchronises `stream` and reads its result back, so it cannot be made while any stream is

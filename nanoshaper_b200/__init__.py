@@ -8,8 +8,10 @@ from .surface import (  # noqa: F401
     PatchSet,
     Surface,
     SurfaceBatch,
+    SkinSurface,
     SurfaceFactory,
     build_ses_patches,
+    build_skin_patches,
     read_atoms,
     read_pqr,
     read_xyzr,

@@ -21,7 +21,7 @@ BUILD_DIR = PKG / "_build"
 LIB = LIB_DIR / "libnsgpu.so"
 
 CU_SOURCES = ["capi.cu", "kernels/trace.cu", "kernels/trace_mixed.cu", "kernels/cavity.cu", "kernels/mc.cu", "kernels/reduce.cu", "kernels/chain.cu", "noalloc.cu"]
-CPP_SOURCES = ["host/grid.cpp", "host/ses_builder.cpp", "host/grad.cpp", "host/formats.cpp"]
+CPP_SOURCES = ["host/grid.cpp", "host/ses_builder.cpp", "host/skin_builder.cpp", "host/grad.cpp", "host/formats.cpp"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

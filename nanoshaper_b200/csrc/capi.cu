@@ -84,8 +84,10 @@ struct nsg_ctx {
   // patches
   int64_t np = 0, npool = 0;
   double probe = 1.4;
-  DevBuf f64, i32, pool, flag, win, pool32;
+  DevBuf f64, i32, pool, flag, win, pool32, quad32, quadl, kind_mask_d;
   bool pool32_valid = false;
+  int kind_mask = 0;  // patch kinds present (bit per kind), valid when kind_mask_valid
+  bool kind_mask_valid = false;
   const double* ext_f64 = nullptr;  // device-resident patch arrays bound by the caller
   const int32_t* ext_i32 = nullptr;
   const double* ext_pool = nullptr;
@@ -155,8 +157,11 @@ nsg::PatchDev patch_dev(nsg_ctx* c) {
   P.pool = (const double4*)(c->ext_pool ? c->ext_pool : c->pool.as<double>());
   P.flag = c->ext_flag ? c->ext_flag : c->flag.as<int8_t>();
   P.pool32 = c->pool32.as<float4>();
+  P.quad32 = c->quad32.as<float4>();
+  P.quadl = c->quadl.as<double4>();
   P.probe = c->probe;
   P.win = c->win.as<int32_t>();
+  P.kind_mask = c->kind_mask;
   return P;
 }
 
@@ -232,6 +237,7 @@ int batch_layout(nsg_ctx* c, const NsGrid* grids, int32_t n) {
     for (int d = 0; d < 3; d++) {
       S.ray_dir[d] = (S.g.mn[d] + (double)(S.g.n[d] - 1) * S.g.side) - (S.g.mn[d] + 0.0 * S.g.side);
       S.inv_dir[d] = 1.0 / S.ray_dir[d];
+      S.box_dir[d] = S.g.mx[d] - S.g.mn[d];
     }
   }
   for (int i = 0; i < 4; i++) {
@@ -437,7 +443,7 @@ int nsg_ctx_destroy(nsg_ctx* c) {
   if (!c) return NSG_ERR_ARG;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
-  DevBuf* bufs[] = {&c->f64, &c->i32, &c->pool, &c->flag, &c->win, &c->pool32, &c->counters, &c->bin_area,
+  DevBuf* bufs[] = {&c->f64, &c->i32, &c->pool, &c->flag, &c->win, &c->pool32, &c->quad32, &c->quadl, &c->kind_mask_d, &c->counters, &c->bin_area,
                     &c->cand_sph, &c->cand_tor, &c->def_sph, &c->def_tor, &c->hit_t, &c->hit_cnt, &c->status, &c->bits, &c->pairs,
                     &c->ray_pair_off, &c->ray_pair_cnt, &c->cursors, &c->ovf_scratch, &c->err, &c->hits,
                     &c->hit_pid, &c->pair_pid, &c->ovf_pscratch, &c->gvol, &c->garea, &c->vpid, &c->vgrad,
@@ -501,6 +507,7 @@ static int upload_common(nsg_ctx* c, int64_t n, int64_t npool, double probe) {
   CK(c->win.ensure(std::max<int64_t>(n, 1) * 6 * sizeof(int32_t)));
   c->has_patches = true;
   c->pool32_valid = false;
+  c->kind_mask_valid = false;
   c->patch_nstruct = 1;
   c->patch_struct_valid = false;
   c->patch_off.assign({0, n});
@@ -798,14 +805,32 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
   const bool do_mc = flags & 2;
   const bool keep_hits = flags & 16;
   const bool grad = flags & 32;
+  if (!c->kind_mask_valid) {
+    // which patch kinds are present (SES and / or skin cells) selects the intersection kernels
+    CK(c->kind_mask_d.ensure(sizeof(int)));
+    CK(cudaMemsetAsync(c->kind_mask_d.p, 0, sizeof(int), c->stream));
+    nsg::PatchDev P0 = patch_dev(c);
+    LAUNCH(nsg::launch_kind_mask(P0, c->kind_mask_d.as<int>(), c->stream));
+    CK(cudaMemcpyAsync(&c->kind_mask, c->kind_mask_d.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->kind_mask_valid = true;
+  }
+  if (grad && (c->kind_mask & nsg::kSkinKinds))
+    return fail(NSG_ERR_STATE, "gradients are provided for SES patch sets, not for skin cells");
   c->grad_mode = grad;
   c->have_gvol = c->have_garea = false;
   c->flags = flags;
   c->precision = precision;
   if (precision == NSG_PRECISION_MIXED && !c->pool32_valid) {
     CK(c->pool32.ensure(std::max<int64_t>(c->npool, 1) * sizeof(float4)));
+    const bool skin = c->kind_mask & nsg::kSkinKinds;
+    if (skin) {
+      CK(c->quad32.ensure(std::max<int64_t>(c->np, 1) * 3 * sizeof(float4)));
+      CK(c->quadl.ensure(std::max<int64_t>(c->np, 1) * sizeof(double4)));
+    }
     nsg::PatchDev P0 = patch_dev(c);
-    LAUNCH(nsg::launch_pool32(P0, c->pool32.as<float4>(), c->stream));
+    LAUNCH(nsg::launch_pool32(P0, c->pool32.as<float4>(), skin ? c->quad32.as<float4>() : nullptr,
+                              skin ? c->quadl.as<double4>() : nullptr, c->stream));
     c->pool32_valid = true;
   }
   nsg::PatchDev P = patch_dev(c);

@@ -34,7 +34,10 @@ typedef struct NsPatchSet NsPatchSet;
 
 int nsg_ses_build(const double* atoms_xyzr, int64_t n_atoms, double probe_radius, int n_threads,
                   NsPatchSet** out);
+int nsg_skin_build(const double* atoms_xyzr, int64_t n_atoms, double shrink, int n_threads, NsPatchSet** out);
+int nsg_skin_predicates(const int64_t* points, int* orient, int* conflict);
 int nsg_patchset_info(const NsPatchSet* ps, int64_t* n_patches, int64_t* n_pool, int64_t counts[5]);
+int nsg_patchset_kind_counts(const NsPatchSet* ps, int64_t* counts, int n);
 int nsg_patchset_export(const NsPatchSet* ps, double* f64, int32_t* i32, double* pool, int8_t* pool_flag);
 int nsg_patchset_atoms(const NsPatchSet* ps, int32_t* out);
 void nsg_patchset_free(NsPatchSet* ps);

@@ -30,6 +30,7 @@
 
 #include "../ns_types.h"
 #include "host_api.h"
+#include "patchset.h"
 
 namespace {
 
@@ -186,33 +187,6 @@ void invert3(const double a[3][3], double* b) {
 }
 
 }  // namespace
-
-struct NsPatchSet {
-  std::vector<double> f64;
-  std::vector<int32_t> i32;
-  std::vector<double> pool;
-  std::vector<int8_t> pool_flag;
-  std::vector<int32_t> atoms;  // 3 per patch: the atoms the patch's surface depends on, -1 unused
-  int64_t counts[5] = {0, 0, 0, 0, 0};
-  void add_patch(int kind, const double* rec, const double* pool4, const int8_t* flags, int64_t npool, int32_t a0,
-                 int32_t a1, int32_t a2) {
-    atoms.push_back(a0);
-    atoms.push_back(a1);
-    atoms.push_back(a2);
-    int64_t first = (int64_t)pool_flag.size();
-    f64.insert(f64.end(), rec, rec + NS_PATCH_F64);
-    i32.push_back(kind);
-    i32.push_back((int32_t)first);
-    i32.push_back((int32_t)npool);
-    i32.push_back(0);
-    if (npool) {
-      pool.insert(pool.end(), pool4, pool4 + 4 * npool);
-      if (flags) pool_flag.insert(pool_flag.end(), flags, flags + npool);
-      else pool_flag.insert(pool_flag.end(), (size_t)npool, (int8_t)0);
-    }
-    counts[kind]++;
-  }
-};
 
 namespace {
 
@@ -770,6 +744,12 @@ int nsg_patchset_info(const NsPatchSet* ps, int64_t* n_patches, int64_t* n_pool,
   if (n_pool) *n_pool = (int64_t)ps->pool_flag.size();
   if (counts)
     for (int k = 0; k < 5; k++) counts[k] = ps->counts[k];
+  return NSG_OK;
+}
+
+int nsg_patchset_kind_counts(const NsPatchSet* ps, int64_t* counts, int n) {
+  if (!ps || !counts || n < 0) return NSG_ERR_ARG;
+  for (int k = 0; k < n; k++) counts[k] = k < NS_KIND_COUNT ? ps->counts[k] : 0;
   return NSG_OK;
 }
 

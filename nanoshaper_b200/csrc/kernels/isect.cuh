@@ -29,6 +29,10 @@ struct TraceCtx {
 template <int PN>
 void launch_isect_mixed(const TraceCtx& C, const CandOut& co, const HitStore& hs, const TuneParams& tp,
                         cudaStream_t s);
+// Mixed-precision skin cell launch of one panel (trace_mixed.cu).
+template <int PN>
+void launch_isect_quad_mixed(const TraceCtx& C, const CandOut& co, const HitStore& hs, const TuneParams& tp,
+                             cudaStream_t s);
 
 namespace {
 
@@ -193,6 +197,7 @@ __device__ __forceinline__ void isect_body(const TraceCtx& C, const CandOut& co,
     for (int k = 0; k < nf; k++) f[k] = __ldg(src + k);
     const int32_t* ir = C.P.i32 + NS_PATCH_I32 * pid;
     const int kind = ir[0], first = ir[1], cnt = ir[2];
+    if (!kTorus && ns_is_skin(kind)) continue;  // skin cells share the list; k_isect_quad takes them
     double t[4];
     int k;
     if (kMixed) {
@@ -224,6 +229,170 @@ __device__ __forceinline__ void isect_body(const TraceCtx& C, const CandOut& co,
         if (hs.pid) hs.pid[(int64_t)(pos + i) * hs.nrays + rid] = (int32_t)pid;
       }
   }
+}
+
+// ---- skin cells: ray-quadric tests inside the mixed cells ----
+
+// Double-precision skin cell test (getPatchIntersectionData of the skin, src/SkinSurface.cpp:
+// 3422-3760): the reference's rayQuadricIntersection along the panel's axis from the ray origin
+// pa (pa[vc] = min + delta), the cell's plane tests at pa + t e_vc, and the hit stored as
+// t / (max - min) of the axis.
+template <int PN>
+__device__ __forceinline__ int intersect_quadric_f64(const double* f, int first, int cnt, const PatchDev& Pd,
+                                                     const double* pa, double box_dir, double* t) {
+  constexpr int vc = Ax<PN>::vc;
+  double tt[2];
+  if (!ray_quadric_f64<vc>(f + NS_SKIN_Q, pa, tt)) return 0;
+  int out = 0;
+  for (int i = 0; i < 2; i++) {
+    double ip[3] = {pa[0], pa[1], pa[2]};
+    ip[vc] += tt[i];
+    if (feasible_skin_f64(Pd.pool, first, cnt, ip)) t[out++] = tt[i] / box_dir;
+  }
+  return out;
+}
+
+// FP32 tolerance of the mixed-precision quadric: a discriminant within kQuadRel of the size of its
+// terms leaves the candidate to the double-precision pass.
+constexpr float kQuadRel = 1e-4f;
+
+// Mixed-precision skin cell test: along the ray the quadric is a s^2 + 2 b s + c in s = x_vc -
+// c_vc (c the cell's local origin), with b and c from the transverse offsets of the ray to c, all
+// small numbers; the discriminant and roots are taken in FP32 (numerically stable form), each
+// root is polished by one Newton step against the FP64 local quadric, and the plane tests run in
+// FP32 on local coordinates with FP64 re-evaluation near zero.  Near-tangent rays (discriminant
+// within rounding of zero) are deferred to the double-precision kernel.
+template <int PN>
+__device__ __forceinline__ int intersect_quadric_mixed(const double* f, int first, int cnt, const PatchDev& P,
+                                                       int64_t pid, const double* pa, double box_dir, double* t,
+                                                       unsigned long long* ctr) {
+  constexpr int fd = Ax<PN>::fd, ld = Ax<PN>::ld, vc = Ax<PN>::vc;
+  // quadric coefficients about the local origin: A (symmetric), bl = A c + b, cl = f(c)
+  const float4 q0 = P.quad32[3 * pid], q1 = P.quad32[3 * pid + 1], q2 = P.quad32[3 * pid + 2];
+  const double4 ql = P.quadl[pid];
+  const float A00 = q0.x, A11 = q0.y, A22 = q0.z, A01 = q0.w, A12 = q1.x, A02 = q1.y;
+  const float Af[3][3] = {{A00, A01, A02}, {A01, A11, A12}, {A02, A12, A22}};
+  const float blf[3] = {q1.z, q1.w, q2.x};
+  const double* Q = f + NS_SKIN_Q;
+  const double A64[3][3] = {{Q[0], Q[4], Q[7]}, {Q[4], Q[1], Q[5]}, {Q[7], Q[5], Q[2]}};
+  const double bl64[3] = {ql.x, ql.y, ql.z};
+  const double a64 = A64[vc][vc];
+  if (a64 == 0) return 0;
+  const double u64f = pa[fd] - f[fd], u64l = pa[ld] - f[ld];
+  const float uf = (float)u64f, ul = (float)u64l;
+  const float a = Af[vc][vc];
+  const float b = (Af[vc][fd] * uf + Af[vc][ld] * ul) + blf[vc];
+  const float c = (Af[fd][fd] * uf * uf + Af[ld][ld] * ul * ul) + (2.f * Af[fd][ld] * uf * ul) +
+                  (2.f * (blf[fd] * uf + blf[ld] * ul) + q2.y);
+  const float bb = b * b, ac = a * c;
+  const float disc = bb - ac;
+  if (fabsf(disc) <= kQuadRel * (bb + fabsf(ac))) {
+    if (ctr) atomicAdd(ctr + kCntFbSphere, 1ull);
+    return kDefer;
+  }
+  if (disc < 0.f) return 0;
+  const float sq = sqrtf(disc);
+  const float qq = -(b + copysignf(sq, b));
+  float sr[2];
+  sr[0] = qq / a;
+  sr[1] = qq != 0.f ? c / qq : -b / a;
+  // the FP64 local quadratic along the ray: a s^2 + 2 b64 s + c64
+  const double b64 = (A64[vc][fd] * u64f + A64[vc][ld] * u64l) + bl64[vc];
+  const double c64 = (A64[fd][fd] * u64f * u64f + A64[ld][ld] * u64l * u64l) + (2.0 * A64[fd][ld] * u64f * u64l) +
+                     (2.0 * (bl64[fd] * u64f + bl64[ld] * u64l) + ql.w);
+  const double cv = f[vc];
+  int out = 0;
+  for (int i = 0; i < 2; i++) {
+    double sd = (double)sr[i];
+    const double res = (a64 * sd + 2.0 * b64) * sd + c64;
+    const float der = 2.f * (a * sr[i] + b);
+    sd -= res * (double)(1.f / der);
+    float pl[3];
+    pl[fd] = uf;
+    pl[ld] = ul;
+    pl[vc] = (float)sd;
+    double p64[3];
+    p64[fd] = pa[fd];
+    p64[ld] = pa[ld];
+    p64[vc] = cv + sd;
+    const float4* lp = P.pool32 + first;
+    const double4* dp = P.pool + first;
+    bool ok = true;
+    for (int q2i = 0; q2i < cnt && ok; q2i++)
+      if (plane_value(lp[q2i], dp, q2i, pl, p64) > 0) ok = false;
+    if (ok) t[out++] = (p64[vc] - pa[vc]) / box_dir;
+  }
+  return out;
+}
+
+// One thread per skin candidate (a cell in the sphere list): intersection, feasibility, hit filing.
+template <int PN, bool kMixed>
+__device__ __forceinline__ void isect_quadric_body(const TraceCtx& C, const CandOut& co, const HitStore& hs) {
+  constexpr int fd = Ax<PN>::fd, ld = Ax<PN>::ld, vc = Ax<PN>::vc;
+  const int64_t ncand = *co.count;
+  const int2* list = co.sph;
+  const int64_t nlim = ncand < co.cap ? ncand : co.cap;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < nlim; c += stride) {
+    const int2 e = list[c];
+    const int64_t rid = e.x, pid = e.y;
+    const int32_t* ir = C.P.i32 + NS_PATCH_I32 * pid;
+    const int kind = ir[0], first = ir[1], cnt = ir[2];
+    if (!ns_is_skin(kind)) continue;
+    const StructDev& S = C.B.s[C.B.patch_struct[pid]];
+    const GridDev& g = S.g;
+    const double delta = C.set == 0 ? 0.0 : NS_DELTA - g.hside;
+    const int64_t nb = g.n[fd];
+    const int64_t lr = rid - S.ray_base[C.set];
+    const int64_t m = lr % nb, n = lr / nb;
+    double pa[3];
+    pa[fd] = gcoord(g, fd, m) + delta;
+    pa[ld] = gcoord(g, ld, n) + delta;
+    pa[vc] = g.mn[vc] + delta;
+    double f[NS_SKIN_Q + 10];
+    const double* src = C.P.f64 + (int64_t)NS_PATCH_F64 * pid;
+#pragma unroll
+    for (int k = 0; k < NS_SKIN_Q + 10; k++) f[k] = __ldg(src + k);
+    double t[2];
+    int k;
+    if (kMixed) {
+      k = intersect_quadric_mixed<PN>(f, first, cnt, C.P, pid, pa, S.box_dir[vc], t, C.out.counters);
+      const bool defer = k == kDefer;
+      const unsigned am = __activemask();
+      const unsigned dm = __ballot_sync(am, defer);
+      if (dm) {
+        const int lane = threadIdx.x & 31;
+        const int leader = __ffs(dm) - 1;
+        unsigned long long base = 0;
+        if (lane == leader) base = atomicAdd(co.dcount, (unsigned long long)__popc(dm));
+        base = __shfl_sync(am, base, leader);
+        if (defer) {
+          unsigned long long slot = base + __popc(dm & ((1u << lane) - 1u));
+          if ((int64_t)slot < co.dcap) co.dsph[slot] = e;
+          else atomicExch(C.out.error_flag, 7);
+        }
+      }
+    } else {
+      k = intersect_quadric_f64<PN>(f, first, cnt, C.P, pa, S.box_dir[vc], t);
+    }
+    if (k <= 0) continue;
+    int pos = atomicAdd(hs.cnt + rid, k);
+    for (int i = 0; i < k; i++)
+      if (pos + i < kHitCap) {
+        hs.t[(int64_t)(pos + i) * hs.nrays + rid] = t[i];
+        if (hs.pid) hs.pid[(int64_t)(pos + i) * hs.nrays + rid] = (int32_t)pid;
+      }
+  }
+}
+
+template <int PN>
+__global__ void __launch_bounds__(256) k_isect_quad(TraceCtx C, CandOut co, HitStore hs) {
+  isect_quadric_body<PN, false>(C, co, hs);
+}
+
+template <int PN>
+__global__ void __launch_bounds__(256, 4) k_isect_quad_mixed(TraceCtx C, CandOut co, HitStore hs) {
+  isect_quadric_body<PN, true>(C, co, hs);
 }
 
 // The double-precision kernels (the FP64 path and the deferred lists of the mixed path) and the

@@ -51,6 +51,7 @@ struct StructDev {
   double A;              // side^2: the area of one pixel, volume weight of an interval length
   double ray_dir[3];     // ray length along each axis: coordinate of the last node minus the first
   double inv_dir[3];     // 1 / ray_dir
+  double box_dir[3];     // max - min of each axis: the skin tracer's ray-parameter unit
 };
 
 // Batch-wide lookup tables.  The *_base arrays hold n+1 entries (the last is the total), for a
@@ -167,7 +168,14 @@ struct PatchDev {
   const int8_t* flag;
   double probe;
   const int32_t* win;  // 6 per patch: start x,y,z, end x,y,z; start = -1 when culled
+  int kind_mask;       // bit k set when some patch has kind k (host copy)
+  const float4* quad32;  // skin cells in patch-local FP32 form, 3 per patch (mixed precision)
+  const double4* quadl;  // skin cells: (A c + b, f(c)) about the local origin c, FP64 (mixed precision)
 };
+
+constexpr int kSesKinds = (1 << NS_POINT) | (1 << NS_EDGE_REG) | (1 << NS_EDGE_SING) | (1 << NS_FACE_REG) |
+                          (1 << NS_FACE_SING);
+constexpr int kSkinKinds = (1 << NS_SKIN_POINT) | (1 << NS_SKIN_EDGE) | (1 << NS_SKIN_FACET) | (1 << NS_SKIN_TETRA);
 
 // Streaming multiprocessors of the current device (queried once per device and cached); grids of
 // the grid-stride kernels are sized as multiples of it.
@@ -183,8 +191,11 @@ struct TuneParams {
 // trace.cu: every launch covers all structures of the batch; `set` is the ray set (0..3) and
 // tile and ray indices are batch-wide.
 cudaError_t launch_windows(const PatchDev& P, int32_t* win, const BatchDev& B, cudaStream_t s);
-// Patch-local FP32 copy of the pool: planes (n, d + n.c), clipping spheres (s - c, r^2).
-cudaError_t launch_pool32(const PatchDev& P, float4* pool32, cudaStream_t s);
+// Patch-local FP32 copy of the pool: planes (n, d + n.c), clipping spheres (s - c, r^2); with
+// quad32, the skin cells' quadrics about their local origin (see k_pool32).
+cudaError_t launch_pool32(const PatchDev& P, float4* pool32, float4* quad32, double4* quadl, cudaStream_t s);
+// Bit mask of the patch kinds present (atomicOr into *mask, which the caller zeroes).
+cudaError_t launch_kind_mask(const PatchDev& P, int* mask, cudaStream_t s);
 // tile_cnt null: only the window-area sum (the candidate bound of the panel).
 cudaError_t launch_bin_count(const PatchDev& P, const BatchDev& B, int set, int32_t* tile_cnt,
                              unsigned long long* area, cudaStream_t s);

@@ -205,4 +205,46 @@ __device__ __forceinline__ bool feasible_f64(const double* P, int kind, int firs
   return false;
 }
 
+// rayQuadricIntersectionX/Y/Z of the skin surface (src/SkinSurface.cpp:4632-4709): a ray of unit
+// direction along axis VC from o against the quadric Q (coding q11, q22, q33, q44, q12, q23, q34,
+// q13, q24, q14); t[0..1] in Angstrom from o, operation for operation as the reference.
+template <int VC>
+__device__ __forceinline__ bool ray_quadric_f64(const double* Q, const double* o, double* t) {
+  const double q44 = Q[3], q33 = Q[2], q22 = Q[1], q11 = Q[0], q34 = Q[6], q24 = Q[8], q23 = Q[5], q14 = Q[9],
+               q13 = Q[7], q12 = Q[4];
+  double a, b;
+  if (VC == 0) {
+    a = q11;
+    if (a == 0) return false;
+    b = q14 + o[2] * q13 + o[1] * q12 + o[0] * q11;
+  } else if (VC == 1) {
+    a = q22;
+    if (a == 0) return false;
+    b = q24 + o[2] * q23 + o[1] * q22 + o[0] * q12;
+  } else {
+    a = q33;
+    if (a == 0) return false;
+    b = q34 + o[2] * q33 + o[1] * q23 + o[0] * q13;
+  }
+  const double c = q44 + (o[2] + o[2]) * q34 + (o[2] * o[2]) * q33 + (o[1] + o[1]) * q24 + (2 * o[1] * o[2]) * q23 +
+                   (o[1] * o[1]) * q22 + (o[0] + o[0]) * q14 + (2 * o[0] * o[2]) * q13 + (2 * o[0] * o[1]) * q12 +
+                   (o[0] * o[0]) * q11;
+  double delta = b * b - a * c;
+  if (delta < 0) return false;
+  delta = sqrt(delta);
+  t[0] = (-b - delta) / a;
+  t[1] = (-b + delta) / a;
+  return true;
+}
+
+// SkinSurface::isFeasible (src/SkinSurface.cpp:4374-4448) over the cell's planes: outside the cell
+// when a plane test is positive (Del0 planes are stored negated, see ns_types.h).
+__device__ __forceinline__ bool feasible_skin_f64(const double4* __restrict__ pool, int first, int cnt,
+                                                  const double* p) {
+  const double4* pl = pool + first;
+  for (int q = 0; q < cnt; q++)
+    if (plane_test_f64(pl[q], p) > 0) return false;
+  return true;
+}
+
 }  // namespace nsg

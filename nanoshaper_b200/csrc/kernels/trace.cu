@@ -33,9 +33,11 @@ __global__ void k_windows(PatchDev P, int32_t* win, BatchDev B) {
   double r = f[3];
   double down[3], up[3];
   bool cull = false;
+  const bool skin = ns_is_skin(P.i32[NS_PATCH_I32 * p]);
   for (int d = 0; d < 3; d++) {
-    down[d] = f[d] - r;
-    up[d] = f[d] + r;
+    // SES: the bounding sphere's box; skin: the cell's box (src/SkinSurface.cpp:3470-3500)
+    down[d] = skin ? f[NS_SKIN_LO + d] : f[d] - r;
+    up[d] = skin ? f[NS_SKIN_HI + d] : f[d] + r;
     if (down[d] > g.mx[d] + NS_EPS_INT) cull = true;
   }
   for (int d = 0; d < 3; d++)
@@ -54,19 +56,45 @@ __global__ void k_windows(PatchDev P, int32_t* win, BatchDev B) {
   }
 }
 
-__global__ void k_pool32(PatchDev P, float4* out) {
+__global__ void k_pool32(PatchDev P, float4* out, float4* quad32, double4* quadl) {
   int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (p >= P.n) return;
   const double* f = P.f64 + (int64_t)NS_PATCH_F64 * p;
   const int32_t* ir = P.i32 + NS_PATCH_I32 * p;
   const int kind = ir[0];
+  const bool skin = ns_is_skin(kind);
   for (int q = ir[1]; q < ir[1] + ir[2]; q++) {
     double4 w = P.pool[q];
-    if (kind == NS_POINT)
+    if (kind == NS_POINT) {
       out[q] = make_float4((float)(w.x - f[0]), (float)(w.y - f[1]), (float)(w.z - f[2]), (float)w.w);
-    else
-      out[q] = make_float4((float)w.x, (float)w.y, (float)w.z, (float)(w.w + (w.x * f[0] + w.y * f[1] + w.z * f[2])));
+    } else {
+      // planes about the local origin; the skin's (partly unnormalised) planes are scaled to unit
+      // normals so that the FP32 value is a distance (the scale does not change a sign)
+      const double inv = skin ? 1.0 / sqrt(w.x * w.x + w.y * w.y + w.z * w.z) : 1.0;
+      out[q] = make_float4((float)(w.x * inv), (float)(w.y * inv), (float)(w.z * inv),
+                           (float)((w.w + (w.x * f[0] + w.y * f[1] + w.z * f[2])) * inv));
+    }
   }
+  if (skin && quad32) {
+    // the quadric about the local origin c: A, bl = A c + b, cl = f(c)
+    const double* Q = f + NS_SKIN_Q;
+    const double A[3][3] = {{Q[0], Q[4], Q[7]}, {Q[4], Q[1], Q[5]}, {Q[7], Q[5], Q[2]}};
+    const double b[3] = {Q[9], Q[8], Q[6]};
+    double bl[3];
+    for (int i = 0; i < 3; i++) bl[i] = (A[i][0] * f[0] + A[i][1] * f[1] + A[i][2] * f[2]) + b[i];
+    const double cl = (f[0] * (bl[0] + b[0]) + f[1] * (bl[1] + b[1]) + f[2] * (bl[2] + b[2])) + Q[3];
+    quad32[3 * p] = make_float4((float)A[0][0], (float)A[1][1], (float)A[2][2], (float)A[0][1]);
+    quad32[3 * p + 1] = make_float4((float)A[1][2], (float)A[0][2], (float)bl[0], (float)bl[1]);
+    quad32[3 * p + 2] = make_float4((float)bl[2], (float)cl, 0.f, 0.f);
+    quadl[p] = make_double4(bl[0], bl[1], bl[2], cl);
+  }
+}
+
+__global__ void k_kind_mask(PatchDev P, int* mask) {
+  int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  int bit = p < P.n ? (1 << P.i32[NS_PATCH_I32 * p]) : 0;
+  bit = __reduce_or_sync(0xffffffffu, bit);
+  if ((threadIdx.x & 31) == 0 && bit) atomicOr(mask, bit);
 }
 
 __global__ void k_bin(PatchDev P, BatchDev B, int set, int32_t* tile_cnt, const int64_t* tile_off,
@@ -132,7 +160,29 @@ __device__ __forceinline__ int intersect_f64(const double* f, int kind, int firs
 // Tests one (ray, patch) candidate and reports the feasible hits in t[0..n-1].
 __device__ __forceinline__ int ray_patch_f64(const double* f, int kind, int first, int cnt, const PatchDev& P,
                                              const RaySet& rs, const double* pa, const double* dir, double ray_dir,
-                                             double* t) {
+                                             double box_dir, double* t) {
+  if (ns_is_skin(kind)) {
+    // the cell's box in the pixel axes, the atom disc for Del0 cells, then the ray-quadric test
+    for (int a = 0; a < 2; a++) {
+      const int d = a == 0 ? rs.fd : rs.ld;
+      if (pa[d] < f[NS_SKIN_LO + d] || pa[d] > f[NS_SKIN_HI + d]) return 0;
+    }
+    if (kind == NS_SKIN_POINT) {
+      const double dx = f[rs.fd] - pa[rs.fd], dy = f[rs.ld] - pa[rs.ld];
+      if (dx * dx + dy * dy > f[kR] * f[kR]) return 0;
+    }
+    double tt[2];
+    bool hit = rs.vc == 0 ? ray_quadric_f64<0>(f + NS_SKIN_Q, pa, tt)
+                          : (rs.vc == 1 ? ray_quadric_f64<1>(f + NS_SKIN_Q, pa, tt) : ray_quadric_f64<2>(f + NS_SKIN_Q, pa, tt));
+    if (!hit) return 0;
+    int out = 0;
+    for (int i = 0; i < 2; i++) {
+      double ip[3] = {pa[0], pa[1], pa[2]};
+      ip[rs.vc] += tt[i];
+      if (feasible_skin_f64(P.pool, first, cnt, ip)) t[out++] = tt[i] / box_dir;
+    }
+    return out;
+  }
   if (!candidate(f, rs, pa)) return 0;
   return intersect_f64(f, kind, first, cnt, P, rs, pa, dir, ray_dir, t);
 }
@@ -276,7 +326,7 @@ struct CandBatch {
   double cf[32], cl[32], lo_fd[32], hi_fd[32], lo_ld[32], hi_ld[32], r2[32], mn_fd[32], mn_ld[32], side[32],
       delta[32];
   int64_t nb[32], rbase[32], base[32];
-  int m0[32], m1[32], n0[32], ty[32], pid[32];
+  int m0[32], m1[32], n0[32], ty[32], pid[32], disc[32];
   int64_t gfirst[32], gend[32];
 };
 
@@ -296,12 +346,14 @@ __device__ __forceinline__ int cand_row(const CandBatch& q, int p, int row, int*
   const double lo_fd = q.lo_fd[p], hi_fd = q.hi_fd[p];
   const double dy = cl - pld;
   const double dy2 = dy * dy;
+  // skin cells other than Del0 have no equatorial-disc test (src/SkinSurface.cpp:3578-3587)
+  const bool disc = q.disc[p];
   int lo = q.m0[p], hi = q.m1[p] + 1;
   while (lo < hi) {
     const int mid = (lo + hi) >> 1;
     const double pa = (mn + (double)mid * side) + delta;
     const double dx = cf - pa;
-    const bool low = !(pa < lo_fd) && (dx < 0. || !(dx * dx + dy2 > r2));
+    const bool low = !(pa < lo_fd) && (!disc || dx < 0. || !(dx * dx + dy2 > r2));
     if (low) hi = mid;
     else lo = mid + 1;
   }
@@ -311,7 +363,7 @@ __device__ __forceinline__ int cand_row(const CandBatch& q, int p, int row, int*
     const int mid = (lo + hi) >> 1;
     const double pa = (mn + (double)mid * side) + delta;
     const double dx = cf - pa;
-    const bool high = !(pa > hi_fd) && (dx > 0. || !(dx * dx + dy2 > r2));
+    const bool high = !(pa > hi_fd) && (!disc || dx > 0. || !(dx * dx + dy2 > r2));
     if (!high) hi = mid;
     else lo = mid + 1;
   }
@@ -348,12 +400,15 @@ __global__ void __launch_bounds__(256) k_cand(TraceCtx C, CandOut co) {
         const RaySet rs = make_ray_set(C.set, g);
         const double* src = C.P.f64 + (int64_t)NS_PATCH_F64 * pid;
         const double cf = __ldg(src + rs.fd), cl = __ldg(src + rs.ld), r = __ldg(src + kR);
+        const int kind0 = C.P.i32[NS_PATCH_I32 * pid];
+        const bool skin = ns_is_skin(kind0);
         q.cf[lane] = cf;
         q.cl[lane] = cl;
-        q.lo_fd[lane] = cf - r;
-        q.hi_fd[lane] = cf + r;
-        q.lo_ld[lane] = cl - r;
-        q.hi_ld[lane] = cl + r;
+        q.lo_fd[lane] = skin ? __ldg(src + NS_SKIN_LO + rs.fd) : cf - r;
+        q.hi_fd[lane] = skin ? __ldg(src + NS_SKIN_HI + rs.fd) : cf + r;
+        q.lo_ld[lane] = skin ? __ldg(src + NS_SKIN_LO + rs.ld) : cl - r;
+        q.hi_ld[lane] = skin ? __ldg(src + NS_SKIN_HI + rs.ld) : cl + r;
+        q.disc[lane] = (!skin || kind0 == NS_SKIN_POINT) ? 1 : 0;
         q.r2[lane] = r * r;
         q.mn_fd[lane] = g.mn[rs.fd];
         q.mn_ld[lane] = g.mn[rs.ld];
@@ -472,15 +527,23 @@ template <int PN>
 void launch_isect(const TraceCtx& C, const CandOut& co, const HitStore& hs, int precision, const TuneParams& tp,
                   cudaStream_t s) {
   const int ig = sm_count() * tp.isect_bpsm, it = tp.isect_threads;
+  const bool ses = C.P.kind_mask & kSesKinds, skin = C.P.kind_mask & kSkinKinds;
   if (precision == 1) {
-    launch_isect_mixed<PN>(C, co, hs, tp, s);
+    if (ses) launch_isect_mixed<PN>(C, co, hs, tp, s);
+    if (skin) launch_isect_quad_mixed<PN>(C, co, hs, tp, s);
     // the deferred candidates, in double precision (few: a small grid)
     const CandOut dco{co.dsph, co.dtor, co.dcap, co.dcount, nullptr, nullptr, 0, nullptr};
-    k_isect<PN, false><<<sm_count(), 256, 0, s>>>(C, dco, hs);
-    k_isect<PN, true><<<sm_count(), 256, 0, s>>>(C, dco, hs);
+    if (ses) {
+      k_isect<PN, false><<<sm_count(), 256, 0, s>>>(C, dco, hs);
+      k_isect<PN, true><<<sm_count(), 256, 0, s>>>(C, dco, hs);
+    }
+    if (skin) k_isect_quad<PN><<<sm_count(), 256, 0, s>>>(C, dco, hs);
   } else {
-    k_isect<PN, false><<<ig, it, 0, s>>>(C, co, hs);
-    k_isect<PN, true><<<ig, it, 0, s>>>(C, co, hs);
+    if (ses) {
+      k_isect<PN, false><<<ig, it, 0, s>>>(C, co, hs);
+      k_isect<PN, true><<<ig, it, 0, s>>>(C, co, hs);
+    }
+    if (skin) k_isect_quad<PN><<<ig, it, 0, s>>>(C, co, hs);
   }
 }
 
@@ -792,7 +855,7 @@ __global__ void k_trace_overflow(TraceCtx C, const int64_t* __restrict__ tile_of
     for (int k = 0; k < NS_PATCH_F64; k++) f[k] = C.P.f64[(int64_t)NS_PATCH_F64 * pid + k];
     const int32_t* ir = C.P.i32 + NS_PATCH_I32 * pid;
     double t[4];
-    int k = ray_patch_f64(f, ir[0], ir[1], ir[2], C.P, rs, pa, dir, ray_dir, t);
+    int k = ray_patch_f64(f, ir[0], ir[1], ir[2], C.P, rs, pa, dir, ray_dir, S.box_dir[rs.vc], t);
     for (int i = 0; i < k; i++) {
       if (nh >= kOverflowCap) {
         atomicExch(C.out.error_flag, 4);
@@ -900,9 +963,15 @@ cudaError_t launch_windows(const PatchDev& P, int32_t* win, const BatchDev& B, c
   return cudaGetLastError();
 }
 
-cudaError_t launch_pool32(const PatchDev& P, float4* pool32, cudaStream_t s) {
+cudaError_t launch_pool32(const PatchDev& P, float4* pool32, float4* quad32, double4* quadl, cudaStream_t s) {
   if (P.n == 0) return cudaSuccess;
-  k_pool32<<<(unsigned)((P.n + 255) / 256), 256, 0, s>>>(P, pool32);
+  k_pool32<<<(unsigned)((P.n + 255) / 256), 256, 0, s>>>(P, pool32, quad32, quadl);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_kind_mask(const PatchDev& P, int* mask, cudaStream_t s) {
+  if (P.n == 0) return cudaSuccess;
+  k_kind_mask<<<(unsigned)((P.n + 255) / 256), 256, 0, s>>>(P, mask);
   return cudaGetLastError();
 }
 

@@ -12,6 +12,18 @@ void launch_isect_mixed(const TraceCtx& C, const CandOut& co, const HitStore& hs
   k_isect_mixed<PN, true><<<ig, it, 0, s>>>(C, co, hs);
 }
 
+template <int PN>
+void launch_isect_quad_mixed(const TraceCtx& C, const CandOut& co, const HitStore& hs, const TuneParams& tp,
+                             cudaStream_t s) {
+  k_isect_quad_mixed<PN><<<sm_count() * tp.isect_bpsm, tp.isect_threads, 0, s>>>(C, co, hs);
+}
+
+template void launch_isect_quad_mixed<0>(const TraceCtx&, const CandOut&, const HitStore&, const TuneParams&,
+                                         cudaStream_t);
+template void launch_isect_quad_mixed<1>(const TraceCtx&, const CandOut&, const HitStore&, const TuneParams&,
+                                         cudaStream_t);
+template void launch_isect_quad_mixed<2>(const TraceCtx&, const CandOut&, const HitStore&, const TuneParams&,
+                                         cudaStream_t);
 template void launch_isect_mixed<0>(const TraceCtx&, const CandOut&, const HitStore&, const TuneParams&, cudaStream_t);
 template void launch_isect_mixed<1>(const TraceCtx&, const CandOut&, const HitStore&, const TuneParams&, cudaStream_t);
 template void launch_isect_mixed<2>(const TraceCtx&, const CandOut&, const HitStore&, const TuneParams&, cudaStream_t);

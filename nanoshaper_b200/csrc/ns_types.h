@@ -22,8 +22,30 @@ enum NsPatchKind {
   NS_EDGE_REG = 1,
   NS_EDGE_SING = 2,
   NS_FACE_REG = 3,
-  NS_FACE_SING = 4
+  NS_FACE_SING = 4,
+  // Skin mixed cells (src/SkinSurface.h:18-105): a quadric patch inside a convex cell bounded by
+  // planes.  Del0Cell (reduced Voronoi cell of an atom), Del1Cell (Delaunay edge x Voronoi face),
+  // Del2Cell (Delaunay facet x Voronoi edge), Del3Cell (reduced tetrahedron).
+  NS_SKIN_POINT = 5,
+  NS_SKIN_EDGE = 6,
+  NS_SKIN_FACET = 7,
+  NS_SKIN_TETRA = 8
 };
+#define NS_KIND_COUNT 9
+
+// Skin cell record (NS_PATCH_F64 doubles):
+//   [0..2]  local origin: the atom centre (Del0), else the centre of the cell's bounding box
+//   [3]     atom radius (Del0, equatorial-disc culling), else half the box diagonal
+//   [4..13] quadric Q in the reference's coding (src/SkinSurface.cpp:4461):
+//           q11, q22, q33, q44, q12, q23, q34, q13, q24, q14 (x^T Q x = 0, x homogeneous)
+//   [14..16] bounding box low corner, [17..19] high corner (the reduced points' box, or the atom
+//           sphere's box for Del0), as the reference's culling computes them
+// Pool: the cell's planes (a, b, c, d); a point with a*x+b*y+c*z+d > 0 is outside the cell (the
+// planes of Del0 cells are stored negated, which flips the reference's "< 0" test exactly).
+#define NS_SKIN_Q 4
+#define NS_SKIN_LO 14
+#define NS_SKIN_HI 17
+NS_HD bool ns_is_skin(int kind) { return kind >= NS_SKIN_POINT; }
 
 // Per-patch double record (NS_PATCH_F64 doubles per patch).
 //   [0..2] bounding-sphere centre, [3] bounding-sphere radius

@@ -203,7 +203,8 @@ class DelPhiShared:
 class PatchSet:
     """Host copy of a patch set in the C-ABI layout (see include/nsgpu.h)."""
 
-    KINDS = ("point", "regular_edge", "singular_edge", "regular_facet", "singular_facet")
+    KINDS = ("point", "regular_edge", "singular_edge", "regular_facet", "singular_facet",
+             "skin_point", "skin_edge", "skin_facet", "skin_tetra")
 
     def __init__(self, f64: np.ndarray, i32: np.ndarray, pool: np.ndarray, pool_flag: np.ndarray, probe: float,
                  counts: tuple[int, ...] = (), atoms_of: np.ndarray | None = None,
@@ -213,7 +214,7 @@ class PatchSet:
         self.pool = np.ascontiguousarray(pool, np.float64).reshape(-1, 4)
         self.pool_flag = np.ascontiguousarray(pool_flag, np.int8).reshape(-1)
         self.probe = float(probe)
-        self.counts = tuple(counts) or tuple(int((self.i32[:, 0] == k).sum()) for k in range(5))
+        self.counts = tuple(counts) or tuple(int((self.i32[:, 0] == k).sum()) for k in range(len(self.KINDS)))
         # atoms each patch depends on (3 per patch, -1 unused) and the atoms the set was built
         # from (after jitter): the chain rule from patch parameters to atoms needs both
         self.atoms_of = None if atoms_of is None else np.ascontiguousarray(atoms_of, np.int32).reshape(-1, 3)
@@ -230,6 +231,8 @@ class PatchSet:
         npool = ctypes.c_int64()
         counts = (ctypes.c_int64 * 5)()
         N.check(L.nsg_patchset_info(handle, ctypes.byref(n), ctypes.byref(npool), counts), "patchset_info")
+        counts = (ctypes.c_int64 * len(cls.KINDS))()
+        N.check(L.nsg_patchset_kind_counts(handle, counts, len(cls.KINDS)), "patchset_kind_counts")
         f64 = np.zeros((n.value, 20))
         i32 = np.zeros((n.value, 4), np.int32)
         pool = np.zeros((npool.value, 4))
@@ -267,6 +270,24 @@ def build_ses_patches(atoms: np.ndarray, probe: float, threads: int = 0) -> Patc
         ps = PatchSet.from_native(h, probe)
         ps.degenerate = rc == -8
         ps.built_from = atoms.copy()
+        return ps
+    finally:
+        N.lib().nsg_patchset_free(h)
+
+
+def build_skin_patches(atoms: np.ndarray, shrink: float) -> PatchSet:
+    """Skin patch set (mixed cells of the weighted atoms: reduced Voronoi cells, edge and facet
+    prisms, reduced tetrahedra) of jittered atoms with shrink factor ``shrink``, built on the host."""
+    atoms = np.ascontiguousarray(atoms, np.float64)
+    h = ctypes.c_void_p()
+    rc = N.lib().nsg_skin_build(N.ptr(atoms), len(atoms), float(shrink), 0, ctypes.byref(h))
+    if rc not in (N.NSG_OK, -8):
+        N.check(rc, "skin patch construction")
+    try:
+        ps = PatchSet.from_native(h, 0.0)
+        ps.degenerate = rc == -8
+        ps.built_from = atoms.copy()
+        ps.shrink = float(shrink)
         return ps
     finally:
         N.lib().nsg_patchset_free(h)
@@ -524,6 +545,48 @@ class ConnollySurface(Surface):
         return True
 
 
+class SkinSurface(Surface):
+    """Skin surface of the weighted atoms, ``Surface = skin`` (src/SkinSurface.h): quadric patches
+    in the cells of the mixed complex, shrink factor ``Skin_Surface_Parameter``."""
+
+    name = "skin"
+    DEFAULT_S = 0.45
+
+    def __init__(self, cf: ConfigFile | None = None, delphi: DelPhiShared | None = None, device: int = 0):
+        super().__init__(cf, delphi, device)
+        cf = cf or ConfigFile()
+        self.setShrinking(cf.read("Skin_Surface_Parameter", self.DEFAULT_S, float))
+
+    def setShrinking(self, ss: float) -> None:
+        """The shrink factor s, accepted in [0.05, 0.95]; otherwise the default 0.45 is kept with a
+        warning, as SkinSurface::setShrinking does (src/SkinSurface.h)."""
+        e = 0.05
+        if e <= ss <= 1.0 - e:
+            self.s = float(ss)
+        else:
+            import warnings
+            warnings.warn(f"Cannot set {ss}. s parameter is in (0+e,1-e], where e is {e}. Setting {self.DEFAULT_S}")
+            self.s = self.DEFAULT_S
+
+    def getShrinking(self) -> float:
+        return self.s
+
+    def build(self) -> bool:
+        atoms = self.delphi.atoms
+        # the reference jitters the atoms inside its build (src/SkinSurface.cpp:1303-1311)
+        if self.randDisplacement > 0:
+            N.check(N.lib().nsg_jitter_atoms(N.ptr(atoms), len(atoms), self.randDisplacement, ctypes.byref(_seed)),
+                    "jitter")
+        self.patches = build_skin_patches(atoms, self.s)
+        return True
+
+    def getSurf(self, optimize_grids: bool = True, fill: bool = False, cav_vol: float = 0.0,
+                keep_hits: bool = False, download: bool = True, grad: bool = False) -> float:
+        if grad:
+            raise NotImplementedError("gradients are provided for the SES (and blobby) surfaces, not for skin")
+        return super().getSurf(optimize_grids, fill, cav_vol, keep_hits, download, grad)
+
+
 class SurfaceBatch:
     """Many built surfaces, each with its own grid and patch set, ray cast and triangulated in the
     same kernel launches: one ``getSurf`` + ``triangulateSurface`` per structure, batched.
@@ -689,6 +752,7 @@ class SurfaceFactory:
 
 _factory = SurfaceFactory()
 _factory.add("ses", lambda cf, ds, dev=0: ConnollySurface(cf, ds, dev))
+_factory.add("skin", lambda cf, ds, dev=0: SkinSurface(cf, ds, dev))
 
 
 def surfaceFactory() -> SurfaceFactory:

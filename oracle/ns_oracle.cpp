@@ -19,6 +19,9 @@
 //   * vertex assembly           assembleVerticesList (src/Surface.cpp:7415-7667)
 //   * marching cubes            triangulateSurface / getVertices / triangulationKernel / getTriangles
 //                               (src/Surface.cpp:9909-10300, 8002-8327, 9075-9318, 14526-14780)
+// For skin patch sets (mixed cells):
+//   * per-cell ray casting      SkinSurface::getPatchIntersectionData (src/SkinSurface.cpp:3422-3760),
+//                               rayQuadricIntersectionX/Y/Z (:4632-4709), isFeasible (:4374-4448)
 // Single-threaded by default so that volume and area are summed in the reference's serial order.
 // Compile without FMA contraction (-ffp-contract=off) so that every operation rounds as written.
 #include <math.h>
@@ -200,6 +203,47 @@ inline double dist2(const double* a, const double* b) {
 }
 inline double plane_test(const double* w, const double* p) { return (w[0] * p[0] + w[1] * p[1] + w[2] * p[2]) + w[3]; }
 
+// SkinSurface::isFeasible (src/SkinSurface.cpp:4374-4448): a point is outside the cell when a plane
+// test is positive (the planes of Del0 cells are stored negated, which turns the reference's
+// "val < 0" test of those cells into the same "> 0" test exactly).
+bool feasible_skin(const Patches& P, int64_t it, const double* p) {
+  const int32_t* ir = P.i32 + NS_PATCH_I32 * it;
+  const double* pool = P.pool + 4 * (int64_t)ir[1];
+  for (int q = 0; q < ir[2]; q++)
+    if (plane_test(pool + 4 * q, p) > 0) return false;
+  return true;
+}
+
+// rayQuadricIntersectionX/Y/Z with a unit direction along axis vc (src/SkinSurface.cpp:4632-4709);
+// Q in the reference's coding q11, q22, q33, q44, q12, q23, q34, q13, q24, q14.
+bool ray_quadric(const double* Q, int vc, const double* o, double t[2]) {
+  double q44 = Q[3], q33 = Q[2], q22 = Q[1], q11 = Q[0], q34 = Q[6], q24 = Q[8], q23 = Q[5], q14 = Q[9], q13 = Q[7],
+         q12 = Q[4];
+  double a, b;
+  if (vc == 0) {
+    a = q11;
+    if (a == 0) return false;
+    b = q14 + o[2] * q13 + o[1] * q12 + o[0] * q11;
+  } else if (vc == 1) {
+    a = q22;
+    if (a == 0) return false;
+    b = q24 + o[2] * q23 + o[1] * q22 + o[0] * q12;
+  } else {
+    a = q33;
+    if (a == 0) return false;
+    b = q34 + o[2] * q33 + o[1] * q23 + o[0] * q13;
+  }
+  double c = q44 + (o[2] + o[2]) * q34 + (o[2] * o[2]) * q33 + (o[1] + o[1]) * q24 + (2 * o[1] * o[2]) * q23 +
+             (o[1] * o[1]) * q22 + (o[0] + o[0]) * q14 + (2 * o[0] * o[2]) * q13 + (2 * o[0] * o[1]) * q12 +
+             (o[0] * o[0]) * q11;
+  double delta = b * b - a * c;
+  if (delta < 0) return false;
+  delta = sqrt(delta);
+  t[0] = (-b - delta) / a;
+  t[1] = (-b + delta) / a;
+  return true;
+}
+
 // isFeasible (src/ConnollySurface.cpp:4769-5019) over the patch-set encoding.
 bool feasible(const Patches& P, int64_t it, const double* p) {
   const int32_t* ir = P.i32 + NS_PATCH_I32 * it;
@@ -288,10 +332,75 @@ struct Oracle {
   double mind(int d) const { return d == 0 ? g.xmin : (d == 1 ? g.ymin : g.zmin); }
   double maxd(int d) const { return d == 0 ? g.xmax : (d == 1 ? g.ymax : g.zmax); }
 
+  // One skin cell (SkinSurface::getPatchIntersectionData, src/SkinSurface.cpp:3422-3760): the box
+  // of the cell culls the grid and the pixels, the atom disc culls Del0 pixels, rays of unit
+  // direction start at min + delta, hits are stored as t / (max - min).
+  void trace_skin(int64_t it, std::vector<Hit>& out) const {
+    const int32_t* ir = P.i32 + NS_PATCH_I32 * it;
+    const double* fr = P.f64 + NS_PATCH_F64 * it;
+    const int kind = ir[0];
+    const double* down = fr + NS_SKIN_LO;
+    const double* up = fr + NS_SKIN_HI;
+    const double* Q = fr + NS_SKIN_Q;
+    const double dacc = NS_DELTA;
+    for (int d = 0; d < 3; d++) if (down[d] > maxd(d) + NS_EPS_INT) return;
+    for (int d = 0; d < 3; d++) if (up[d] < mind(d) - (g.hside - dacc + NS_EPS_INT)) return;
+    int64_t i_start[3], i_end[3];
+    for (int d = 0; d < 3; d++) {
+      i_start[d] = (int64_t)rintp(fmax(0., (down[d] - mind(d))) * g.scale);
+      i_end[d] = (int64_t)rintp(fmax(0., up[d] - mind(d)) * g.scale);
+      if (i_end[d] >= Nd(d)) i_end[d] = Nd(d) - 1;
+    }
+    int64_t pixels[3] = {1 + i_end[0] - i_start[0], 1 + i_end[1] - i_start[1], 1 + i_end[2] - i_start[2]};
+    for (int phase = 0; phase < 2; phase++) {
+      if (panels[phase] == 0) continue;
+      double delta = (phase == 0) ? 0. : dacc - g.hside;
+      for (int panel = 0; panel < panels[phase]; panel++) {
+        int fd, ld, vc;
+        if (panel == 0) { fd = 1; ld = 2; vc = 0; }
+        else if (panel == 1) { fd = 0; ld = 1; vc = 2; }
+        else { fd = 0; ld = 2; vc = 1; }
+        double pa[3];
+        pa[vc] = mind(vc) + delta;
+        const double ray_dir = maxd(vc) - mind(vc);
+        int64_t npix = pixels[fd] * pixels[ld];
+        for (int64_t rp = 0; rp < npix; rp++) {
+          int64_t n = rp / pixels[fd];
+          int64_t m = rp - n * pixels[fd];
+          n += i_start[ld];
+          m += i_start[fd];
+          if (n < n_lo(Nd(ld)) || n >= n_hi(Nd(ld))) continue;
+          pa[fd] = coord(fd, m) + delta;
+          if (pa[fd] < down[fd] || pa[fd] > up[fd]) continue;
+          pa[ld] = coord(ld, n) + delta;
+          if (pa[ld] < down[ld] || pa[ld] > up[ld]) continue;
+          if (kind == NS_SKIN_POINT) {
+            double dx = fr[fd] - pa[fd];
+            double dy = fr[ld] - pa[ld];
+            if (dx * dx + dy * dy > fr[3] * fr[3]) continue;
+          }
+          double t[2];
+          if (!ray_quadric(Q, vc, pa, t)) continue;
+          for (int i = 0; i < 2; i++) {
+            double ip[3] = {pa[0], pa[1], pa[2]};
+            ip[vc] += t[i];
+            if (!feasible_skin(P, it, ip)) continue;
+            int64_t pid = (n * NMAX + m) * numPanels + (panels[0] * phase + panel);
+            out.push_back({pid, t[i] / ray_dir});
+          }
+        }
+      }
+    }
+  }
+
   void trace_patch(int64_t it, std::vector<Hit>& out) const {
     const int32_t* ir = P.i32 + NS_PATCH_I32 * it;
     const double* fr = P.f64 + NS_PATCH_F64 * it;
     int kind = ir[0];
+    if (ns_is_skin(kind)) {
+      trace_skin(it, out);
+      return;
+    }
     const double* sc = fr;
     double radius = fr[3];
     bool doTorus = (kind == NS_EDGE_REG || kind == NS_EDGE_SING);
@@ -351,6 +460,23 @@ struct Oracle {
     }
   }
 
+  // Runs f(lo, hi) over [a, b) split into contiguous blocks, one per thread.
+  template <class F>
+  void parallel_rows(int64_t a, int64_t b, F&& f) const {
+    const int nt = std::max(1, nthreads);
+    if (nt <= 1 || b - a < 2 * nt) {
+      f(a, b);
+      return;
+    }
+    std::vector<std::thread> th;
+    const int64_t step = (b - a + nt - 1) / nt;
+    for (int t = 0; t < nt; t++) {
+      const int64_t lo = a + t * step, hi = std::min(b, lo + step);
+      if (lo < hi) th.emplace_back([&f, lo, hi] { f(lo, hi); });
+    }
+    for (auto& x : th) x.join();
+  }
+
   void trace() {
     std::vector<std::vector<Hit>> per(std::max(1, nthreads));
     auto work = [&](int tid) {
@@ -404,35 +530,44 @@ struct Oracle {
     // phase 0: status map along x (only panel 0 when the status map is built)
     if (panels[0] > 0 && panel == 0) {
       flagsum++;
-      double pa[3], pb[3];
-      pa[0] = X(0); pb[0] = X(g.nx - 1);
-      rays_cast += (n_hi(na) - n_lo(na)) * nb;
-      for (int64_t n = n_lo(na); n < n_hi(na); n++) {
-        pa[2] = Z(n);
-        for (int64_t m = 0; m < nb; m++) {
-          int64_t id = (n * NMAX + m) * numPanels + panel;
-          pairs_of(id, pr);
-          if (pr.empty()) continue;
-          pa[1] = Y(m);
-          double dir = pb[0] - pa[0];
-          double lvi = 0.0;
-          for (auto& q : pr) {
-            double lim1 = pa[0] + dir * pix_t[q.first];
-            double lim2 = pa[0] + dir * pix_t[q.second];
-            lvi += lim2 - lim1;
-            int64_t i1 = (int64_t)rintp((lim1 - g.xmin) * g.scale);
-            int64_t i2 = (int64_t)rintp((lim2 - g.xmin) * g.scale);
-            i1 = i1 < 0 ? 0 : (i1 >= g.nx ? g.nx - 1 : i1);
-            i2 = i2 < 0 ? 0 : (i2 >= g.nx ? g.nx - 1 : i2);
-            if (i2 < i1) continue;
-            for (int64_t ix = i1; ix <= i2; ix++) {
-              double xx = X(ix);
-              if (xx <= lim2 && xx >= lim1) status[(n * g.ny + m) * g.nx + ix] = NS_STATUS_INSIDE;
+      const int64_t n0 = n_lo(na), n1 = n_hi(na);
+      rays_cast += (n1 - n0) * nb;
+      // rows are independent (each writes its own status row); the interval sums are kept per
+      // ray and added afterwards in the reference's serial ray order
+      std::vector<double> lv((size_t)(n1 - n0) * nb, 0.0);
+      auto rows = [&](int64_t nn0, int64_t nn1) {
+        std::vector<std::pair<int64_t, int64_t>> prl;
+        double pa[3], pb[3];
+        pa[0] = X(0); pb[0] = X(g.nx - 1);
+        for (int64_t n = nn0; n < nn1; n++) {
+          pa[2] = Z(n);
+          for (int64_t m = 0; m < nb; m++) {
+            int64_t id = (n * NMAX + m) * numPanels + panel;
+            pairs_of(id, prl);
+            if (prl.empty()) continue;
+            pa[1] = Y(m);
+            double dir = pb[0] - pa[0];
+            double lvi = 0.0;
+            for (auto& q : prl) {
+              double lim1 = pa[0] + dir * pix_t[q.first];
+              double lim2 = pa[0] + dir * pix_t[q.second];
+              lvi += lim2 - lim1;
+              int64_t i1 = (int64_t)rintp((lim1 - g.xmin) * g.scale);
+              int64_t i2 = (int64_t)rintp((lim2 - g.xmin) * g.scale);
+              i1 = i1 < 0 ? 0 : (i1 >= g.nx ? g.nx - 1 : i1);
+              i2 = i2 < 0 ? 0 : (i2 >= g.nx ? g.nx - 1 : i2);
+              if (i2 < i1) continue;
+              for (int64_t ix = i1; ix <= i2; ix++) {
+                double xx = X(ix);
+                if (xx <= lim2 && xx >= lim1) status[(n * g.ny + m) * g.nx + ix] = NS_STATUS_INSIDE;
+              }
             }
+            lv[(size_t)(n - n0) * nb + m] = lvi;
           }
-          volPanel[panel] += lvi;
         }
-      }
+      };
+      parallel_rows(n0, n1, rows);
+      for (double v : lv) volPanel[panel] += v;
     }
     if (!(flags & 2)) return;  // accurate triangulation rays
     flagsum++;
@@ -481,10 +616,12 @@ struct Oracle {
             int32_t t2[4] = {(int32_t)m, (int32_t)b, (int32_t)n, NS_Y_DIR};
             memcpy(e1, t1, sizeof e1); memcpy(e2, t2, sizeof e2);
           }
-          vert.insert(vert.end(), v1, v1 + 3);
-          vert_edge.insert(vert_edge.end(), e1, e1 + 4);
-          vert.insert(vert.end(), v2, v2 + 3);
-          vert_edge.insert(vert_edge.end(), e2, e2 + 4);
+          if (flags & 8) {  // analytic vertices are kept only for the triangulation
+            vert.insert(vert.end(), v1, v1 + 3);
+            vert_edge.insert(vert_edge.end(), e1, e1 + 4);
+            vert.insert(vert.end(), v2, v2 + 3);
+            vert_edge.insert(vert_edge.end(), e2, e2 + 4);
+          }
         }
         volPanel[panel] += lvi;
       }
@@ -726,9 +863,10 @@ struct Oracle {
     for (int panel = 0; panel < np; panel++) fill_panel(panel);
     volume = flagsum ? g.A * (volPanel[0] + volPanel[1] + volPanel[2]) / flagsum : 0;
     if ((flags & 4) && (flags & 1)) cavities();
-    if (flags & 2) {
+    // vertex assembly and marching cubes (the dense edge-index grids are needed only here)
+    if ((flags & 2) && (flags & 8)) {
       assemble();
-      if (flags & 8) triangulate();
+      triangulate();
     }
   }
 };

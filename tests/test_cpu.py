@@ -565,3 +565,109 @@ def test_reference_fixture_config_parses(native_lib):
     assert ns.scale == 2.0 and ns.perfil == 90.0
     ref_atoms = nb.read_xyzr(fx / "1crn.xyzr")
     np.testing.assert_array_equal(ns.ds.atoms, ref_atoms)
+
+
+def test_skin_predicates_signs(native_lib):
+    """Orientation and orthosphere-conflict predicates of the skin builder's triangulation on
+    integer points: the unit tetrahedron is positively oriented, a point inside its circumsphere
+    conflicts, a far point does not, and a point whose negative weight exceeds its power distance
+    to the orthosphere does not."""
+    import ctypes
+    from nanoshaper_b200 import _native as N
+    L = native_lib
+
+    def pred(p):
+        p = np.ascontiguousarray(p, np.int64)
+        o, c = ctypes.c_int(), ctypes.c_int()
+        assert L.nsg_skin_predicates(N.ptr(p), ctypes.byref(o), ctypes.byref(c)) == 0
+        return o.value, c.value
+
+    base = [[0, 0, 0, 0], [1000, 0, 0, 0], [0, 1000, 0, 0], [0, 0, 1000, 0]]
+    assert pred(base + [[250, 250, 250, 0]]) == (1, 1)
+    assert pred(base + [[3000, 3000, 3000, 0]]) == (1, 0)
+    assert pred(base + [[250, 250, 250, -10 ** 7]]) == (1, 0)
+    swapped = [base[1], base[0], base[2], base[3]]
+    assert pred(swapped + [[250, 250, 250, 0]])[0] == -1
+    # large coordinates: exact at the 2^33 bound of the snapped grid
+    big = np.array(base + [[250, 250, 250, 0]], np.int64)
+    big[:, :3] *= 2 ** 23
+    big[:, 3] *= 2 ** 46
+    assert pred(big) == (1, 1)
+
+
+def _skin(atoms, scale, perfil, s=0.45):
+    nb.reset_seed()
+    ds = nb.DelPhiShared(atoms, scale, perfil)
+    cf = nb.ConfigFile(text=f"Surface = skin\nSkin_Surface_Parameter = {s}\nAccurate_Triangulation = true\n")
+    surf = nb.surfaceFactory().create(cf, ds)
+    surf.build()
+    return ds, surf
+
+
+def test_skin_single_atom_is_its_sphere(native_lib, oracle_mod):
+    """One atom: a single Del0 cell without planes whose quadric is the atom sphere; the ray-cast
+    volume tends to 4/3 pi r^3."""
+    atoms = np.array([[0.0, 0.0, 0.0, 1.7]])
+    ds, surf = _skin(atoms, 6.0, 50.0)
+    p = surf.patches
+    assert p.n == 1 and p.i32[0, 0] == 5 and p.i32[0, 2] == 0
+    r = oracle_mod.run(ds.grid, p, flags=oracle_mod.STATUS)
+    exact = 4.0 / 3.0 * np.pi * 1.7 ** 3
+    assert abs(r.volume - exact) / exact < 0.01
+
+
+def test_skin_cells_tile_space_and_match_the_ray_cast(native_lib, oracle_mod):
+    """The mixed cells of a 30-atom globule: no grid node lies in two cells; at every node inside a
+    cell the sign of the cell's quadric (inside: < 0, > 0 for reduced tetrahedra) equals the
+    oracle's ray-cast status; every ray of the four ray sets has an even hit count."""
+    atoms = generator.rsa_globule(30, 1)
+    ds, surf = _skin(atoms, 3.0, 60.0)
+    p = surf.patches
+    r = oracle_mod.run(ds.grid, p, flags=oracle_mod.STATUS | oracle_mod.ACCURATE_TRIANGULATION)
+    for s in range(4):
+        cnt, _ = oracle_mod.ray_hits(r, s)
+        assert int((cnt % 2).sum()) == 0, f"ray set {s}: rays with odd hit counts"
+    zz, yy, xx = np.meshgrid(ds.z, ds.y, ds.x, indexing="ij")
+    X = np.stack([xx.ravel(), yy.ravel(), zz.ravel()], 1)
+    status_in = r.status.ravel() == -1
+    cell_in = np.zeros(len(X), bool)
+    covered = np.zeros(len(X), np.int32)
+    for i in range(p.n):
+        kind, first, cnt = p.i32[i, :3]
+        f = p.f64[i]
+        idx = np.nonzero(np.all((X >= f[14:17]) & (X <= f[17:20]), axis=1))[0]
+        if len(idx) == 0:
+            continue
+        Y = X[idx]
+        ok = np.ones(len(idx), bool)
+        for q in range(first, first + cnt):
+            ok &= (Y @ p.pool[q, :3] + p.pool[q, 3]) <= 0
+        idx, Y = idx[ok], Y[ok]
+        q11, q22, q33, q44, q12, q23, q34, q13, q24, q14 = f[4:14]
+        x, y, z = Y[:, 0], Y[:, 1], Y[:, 2]
+        v = (q11 * x * x + q22 * y * y + q33 * z * z + 2 * q12 * x * y + 2 * q23 * y * z + 2 * q13 * x * z +
+             2 * q14 * x + 2 * q24 * y + 2 * q34 * z + q44)
+        covered[idx] += 1
+        cell_in[idx] = v > 0 if kind == 8 else v < 0
+    assert covered.max() <= 1
+    cov = covered > 0
+    assert cov.sum() > 0.2 * len(X)
+    assert np.array_equal(cell_in[cov], status_in[cov])
+
+
+def test_skin_reference_fixture_1crn_is_watertight(native_lib, oracle_mod):
+    """The reference's 1crn skin fixture (its .prm through ConfigFile): the mixed complex ray casts
+    to an even hit count on every ray of the four ray sets."""
+    fx = Path(__file__).resolve().parent / "golden" / "fixtures"
+    cf = nb.ConfigFile(fx / "1crn_skin_conf.prm")
+    nb.reset_seed()
+    ns = nb.NanoShaper(config=cf)
+    assert ns.surf.name == "skin" and ns.surf.getShrinking() == 0.45
+    ns.buildAnalyticalSurface()
+    p = ns.surf.patches
+    assert p.counts[5] == 327
+    r = oracle_mod.run(ns.ds.grid, p, flags=oracle_mod.STATUS | oracle_mod.ACCURATE_TRIANGULATION)
+    for s in range(4):
+        cnt, _ = oracle_mod.ray_hits(r, s)
+        assert int((cnt % 2).sum()) == 0
+    assert r.volume > 0
