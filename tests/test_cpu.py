@@ -135,7 +135,7 @@ def test_rays_are_watertight(oracle_mod):
 def test_single_sphere_oracle_volume(oracle_mod):
     ds = nb.DelPhiShared(np.array([[0.0, 0.0, 0.0, 1.7]]), 4.0, 50.0)
     ps = nb.build_ses_patches(ds.atoms, 1.4)
-    assert ps.counts == (1, 0, 0, 0, 0)
+    assert ps.counts[:5] == (1, 0, 0, 0, 0)
     ref = oracle_mod.run(ds.grid, ps)
     assert abs(ref.volume - 4 / 3 * np.pi * 1.7 ** 3) / (4 / 3 * np.pi * 1.7 ** 3) < 0.02
     assert abs(ref.area - 4 * np.pi * 1.7 ** 2) / (4 * np.pi * 1.7 ** 2) < 0.05
@@ -145,7 +145,7 @@ def test_two_sphere_torus_patch(oracle_mod):
     """Two atoms closer than two probe diameters: one torus, two point cells, no probe patch."""
     atoms = np.array([[0.0, 0.0, 0.0, 1.7], [3.0, 0.0, 0.0, 1.7]])
     ps = nb.build_ses_patches(atoms, 1.4)
-    assert ps.counts == (2, 0, 1, 0, 0)
+    assert ps.counts[:5] == (2, 0, 1, 0, 0)
     # the torus: centre midway, major radius sqrt((r+p)^2 - (d/2)^2)
     tor = ps.f64[ps.i32[:, 0] == 2][0]
     np.testing.assert_allclose(tor[4:7], [1.5, 0, 0], atol=1e-12)
