@@ -198,6 +198,25 @@ int nsg_upload_atoms(nsg_ctx* ctx, const int64_t* atom_off, const double* atoms_
  * chained from the patch derivatives on the device; either pointer may be NULL. */
 int nsg_atom_grads(nsg_ctx* ctx, double* d_volume, double* d_area);
 
+/* ---- blobby surface (BlobbySurface, src/BlobbySurface.cpp:83-229) ----
+ * The atoms' Gaussian field sum exp(B (d^2/r^2 - 1)) (cut-off 6 A) on the context's grid, its
+ * marching-cubes mesh at iso level 1 (src/Surface.cpp:8143-8327, 9075-9318), one Laplacian
+ * smoothing pass (src/Surface.cpp:13089-13354) and the reference's OFF text round trip (vertices
+ * written "%.3f", read back as floats, src/MeshSurface.cpp:2350-2479), all on the device; the
+ * mesh's triangles (patch kind 9) become the context's patch set, ray cast like a MeshSurface
+ * (src/MeshSurface.cpp:1487-1855).  blobbyness < 0.  flags: NSG_BLOBBY_DIFFERENTIABLE skips the
+ * round trip (which is piecewise constant in the atoms) so that nsg_blobby_atom_grads applies. */
+#define NSG_BLOBBY_DIFFERENTIABLE 1
+int nsg_blobby_build(nsg_ctx* ctx, const double* atoms_xyzr, int64_t n_atoms, double blobbyness, int flags);
+/* The mesh of the last nsg_blobby_build: vertex and triangle counts, vertices (3 doubles) and
+ * triangles (3 ints); NULL buffers only report the counts. */
+int nsg_blobby_mesh(nsg_ctx* ctx, int64_t* n_vertices, int64_t* n_triangles, double* vertices, int32_t* triangles);
+/* d volume and d area of a NSG_BLOBBY_DIFFERENTIABLE blobby surface with respect to its atoms'
+ * x, y, z, r (n_atoms x 4 each), after nsg_raycast with NSG_RAYCAST_GRAD (and nsg_triangulate for
+ * the area): hit terms on the triangles, the smoothing, the interpolated vertices and the field,
+ * chained on the device (no counterpart in the reference); either pointer may be NULL. */
+int nsg_blobby_atom_grads(nsg_ctx* ctx, double* d_volume, double* d_area);
+
 /* ---- the hot path ---- */
 /* Ray casting of Surface::getSurf: getPatchIntersectionData (src/ConnollySurface.cpp:4319-4590),
  * pixel binning and sort (src/Surface.cpp:4766-5095), setVerticesAndGridsWithIntersectionData

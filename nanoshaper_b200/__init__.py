@@ -1,5 +1,6 @@
 """B200-native grid ray-casting molecular surface builder (NanoShaper-compatible interface)."""
 from .surface import (  # noqa: F401
+    BlobbySurface,
     ConfigFile,
     ConnollySurface,
     Context,

@@ -97,6 +97,9 @@ _SIGNATURES = {
     "nsg_patchset_kind_counts": ([_P, _P, _INT], _INT),
     "nsg_skin_build": ([_P, _I64, _D, _INT, ctypes.POINTER(_P)], _INT),
     "nsg_skin_predicates": ([_P, _P, _P], _INT),
+    "nsg_blobby_build": ([_P, _P, _I64, _D, _INT], _INT),
+    "nsg_blobby_mesh": ([_P, ctypes.POINTER(_I64), ctypes.POINTER(_I64), _P, _P], _INT),
+    "nsg_blobby_atom_grads": ([_P, _P, _P], _INT),
     "nsg_patchset_export": ([_P, _P, _P, _P, _P], _INT),
     "nsg_patchset_free": ([_P], None),
     "nsg_patchset_atoms": ([_P, _P], _INT),

@@ -18,6 +18,7 @@
 #include <cub/cub.cuh>
 
 #include "host/host_api.h"
+#include "kernels/blobby.h"
 #include "kernels/cavity.h"
 #include "kernels/mc.h"
 #include "kernels/pipeline.h"
@@ -134,6 +135,13 @@ struct nsg_ctx {
   int64_t n_vert = 0, n_analytic = 0, n_tri = 0, n_active = 0;
   double area = 0;
   DevBuf temp;  // cub temporary storage
+  // blobby surface: atoms, field, the field's marching-cubes mesh and its patches, adjoint scratch
+  DevBuf b_atoms, b_field, b_mask, b_nv, b_nt, b_voff, b_toff, b_vraw, b_verts, b_vkey, b_tris, b_inc_cnt, b_inc_off,
+      b_inc_cur, b_inc, b_patch_atoms, b_gpost, b_gpre, b_gfield, b_gatoms;
+  int64_t b_natoms = 0, b_nv_n = 0, b_nt_n = 0;
+  double b_B = -2.5;
+  int b_ng = 0;
+  bool b_valid = false, b_quantized = true;
   int64_t last_overflow_rays = 0;
   // timing: user events and per-stage kernel times (milliseconds, summed over calls)
   cudaEvent_t user_ev[8] = {};
@@ -443,7 +451,7 @@ int nsg_ctx_destroy(nsg_ctx* c) {
   if (!c) return NSG_ERR_ARG;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
-  DevBuf* bufs[] = {&c->f64, &c->i32, &c->pool, &c->flag, &c->win, &c->pool32, &c->quad32, &c->quadl, &c->kind_mask_d, &c->counters, &c->bin_area,
+  DevBuf* bufs[] = {&c->f64, &c->i32, &c->pool, &c->flag, &c->win, &c->pool32, &c->quad32, &c->quadl, &c->kind_mask_d, &c->b_atoms, &c->b_field, &c->b_mask, &c->b_nv, &c->b_nt, &c->b_voff, &c->b_toff, &c->b_vraw, &c->b_verts, &c->b_vkey, &c->b_tris, &c->b_inc_cnt, &c->b_inc_off, &c->b_inc_cur, &c->b_inc, &c->b_patch_atoms, &c->b_gpost, &c->b_gpre, &c->b_gfield, &c->b_gatoms, &c->counters, &c->bin_area,
                     &c->cand_sph, &c->cand_tor, &c->def_sph, &c->def_tor, &c->hit_t, &c->hit_cnt, &c->status, &c->bits, &c->pairs,
                     &c->ray_pair_off, &c->ray_pair_cnt, &c->cursors, &c->ovf_scratch, &c->err, &c->hits,
                     &c->hit_pid, &c->pair_pid, &c->ovf_pscratch, &c->gvol, &c->garea, &c->vpid, &c->vgrad,
@@ -508,6 +516,7 @@ static int upload_common(nsg_ctx* c, int64_t n, int64_t npool, double probe) {
   c->has_patches = true;
   c->pool32_valid = false;
   c->kind_mask_valid = false;
+  c->b_valid = false;
   c->patch_nstruct = 1;
   c->patch_struct_valid = false;
   c->patch_off.assign({0, n});
@@ -790,6 +799,139 @@ int nsg_bind_patches_device(nsg_ctx* c, int64_t n, const double* f64, const int3
   return upload_common(c, n, npool, probe);
 }
 
+// Blobby surface of the context's grid (BlobbySurface::build, src/BlobbySurface.cpp:83-229): the
+// atoms' Gaussian field, its marching-cubes mesh at iso level 1, one smoothing pass and (unless
+// NSG_BLOBBY_DIFFERENTIABLE) the OFF text round trip; the mesh's triangles become the context's
+// patch set.
+int nsg_blobby_build(nsg_ctx* c, const double* atoms_xyzr, int64_t n_atoms, double blobbyness, int flags) {
+  if (!c || !atoms_xyzr || n_atoms <= 0 || n_atoms >= ((int64_t)1 << 31) || !(blobbyness < 0))
+    return NSG_ERR_ARG;
+  if (!c->has_grid || c->nstruct != 1) return fail(NSG_ERR_STATE, "a single-structure grid must be set first");
+  CK(cudaSetDevice(c->device));
+  CK(nsg::blobby_init_tables());
+  const NsGrid& G = c->grid;
+  const nsg::GridDev g = grid_dev(G);
+  const int64_t nodes = G.nx * G.ny * G.nz;
+  const int64_t ncubes = (G.nx - 2) * (G.ny - 2) * (G.nz - 2);
+  cudaStream_t s = c->stream;
+  CK(c->b_atoms.ensure(n_atoms * 4 * sizeof(double)));
+  CK(cudaMemcpyAsync(c->b_atoms.p, atoms_xyzr, n_atoms * 4 * sizeof(double), cudaMemcpyHostToDevice, s));
+  // cut-off of 6 A in whole grid steps (DEFAULT_CUTOFF, src/BlobbySurface.h)
+  const int ng = (int)(6.0 / G.side + 0.5);
+  CK(c->b_field.ensure(nodes * sizeof(double)));
+  LAUNCH(nsg::launch_blobby_field(g, c->b_atoms.as<double>(), (int)n_atoms, blobbyness, ng, c->b_field.as<double>(), s));
+  const double iso = 1.0;
+  CK(c->b_mask.ensure(std::max<int64_t>(ncubes, 1)));
+  CK(c->b_nv.ensure(std::max<int64_t>(ncubes, 1) * sizeof(int32_t)));
+  CK(c->b_nt.ensure(std::max<int64_t>(ncubes, 1) * sizeof(int32_t)));
+  CK(c->b_voff.ensure((ncubes + 1) * sizeof(int64_t)));
+  CK(c->b_toff.ensure((ncubes + 1) * sizeof(int64_t)));
+  LAUNCH(nsg::launch_field_cubes(g, c->b_field.as<double>(), iso, ncubes, c->b_mask.as<uint8_t>(), c->b_nv.as<int32_t>(),
+                                 c->b_nt.as<int32_t>(), s));
+  int64_t nv = 0, nt = 0;
+  int rc = scan_counts(c, c->b_nv.as<int32_t>(), ncubes, c->b_voff.as<int64_t>(), &nv);
+  if (rc) return rc;
+  rc = scan_counts(c, c->b_nt.as<int32_t>(), ncubes, c->b_toff.as<int64_t>(), &nt);
+  if (rc) return rc;
+  if (nv >= ((int64_t)1 << 31) || nt >= ((int64_t)1 << 31)) return fail(NSG_ERR_CAPACITY, "mesh too large");
+  CK(c->b_vraw.ensure(std::max<int64_t>(nv, 1) * 3 * sizeof(double)));
+  CK(c->b_verts.ensure(std::max<int64_t>(nv, 1) * 3 * sizeof(double)));
+  CK(c->b_vkey.ensure(std::max<int64_t>(nv, 1) * sizeof(int4)));
+  CK(c->b_tris.ensure(std::max<int64_t>(nt, 1) * 3 * sizeof(int32_t)));
+  LAUNCH(nsg::launch_field_verts(g, c->b_field.as<double>(), iso, ncubes, c->b_mask.as<uint8_t>(),
+                                 c->b_voff.as<int64_t>(), c->b_vraw.as<double>(), c->b_vkey.as<int4>(), s));
+  LAUNCH(nsg::launch_field_tris(g, c->b_field.as<double>(), iso, ncubes, c->b_mask.as<uint8_t>(), c->b_voff.as<int64_t>(),
+                                c->b_toff.as<int64_t>(), c->b_nt.as<int32_t>(), c->b_tris.as<int32_t>(), s));
+  // smoothing: per-vertex incidence lists, then the triangle-ordered sums
+  CK(c->b_inc_cnt.ensure(std::max<int64_t>(nv, 1) * sizeof(int32_t)));
+  CK(c->b_inc_cur.ensure(std::max<int64_t>(nv, 1) * sizeof(int32_t)));
+  CK(c->b_inc_off.ensure((nv + 1) * sizeof(int64_t)));
+  CK(c->b_inc.ensure(std::max<int64_t>(3 * nt, 1) * sizeof(int32_t)));
+  CK(cudaMemsetAsync(c->b_inc_cnt.p, 0, std::max<int64_t>(nv, 1) * sizeof(int32_t), s));
+  CK(cudaMemsetAsync(c->b_inc_cur.p, 0, std::max<int64_t>(nv, 1) * sizeof(int32_t), s));
+  LAUNCH(nsg::launch_incidence(c->b_tris.as<int32_t>(), nt, 0, nullptr, c->b_inc_cnt.as<int32_t>(), nullptr, s));
+  int64_t ninc = 0;
+  if (nv > 0) {
+    rc = scan_counts(c, c->b_inc_cnt.as<int32_t>(), nv, c->b_inc_off.as<int64_t>(), &ninc);
+    if (rc) return rc;
+  }
+  LAUNCH(nsg::launch_incidence(c->b_tris.as<int32_t>(), nt, 1, c->b_inc_off.as<int64_t>(), c->b_inc_cur.as<int32_t>(),
+                               c->b_inc.as<int32_t>(), s));
+  LAUNCH(nsg::launch_smooth(c->b_vraw.as<double>(), nv, c->b_inc_off.as<int64_t>(), c->b_inc.as<int32_t>(),
+                            c->b_tris.as<int32_t>(), c->b_verts.as<double>(), s));
+  const bool quantize = !(flags & 1);
+  if (quantize) LAUNCH(nsg::launch_quantize(c->b_verts.as<double>(), 3 * nv, s));
+  // the triangles as the context's patch set
+  CK(c->f64.ensure(std::max<int64_t>(nt, 1) * NS_PATCH_F64 * sizeof(double)));
+  CK(c->i32.ensure(std::max<int64_t>(nt, 1) * NS_PATCH_I32 * sizeof(int32_t)));
+  CK(c->pool.ensure(4 * sizeof(double)));
+  CK(c->flag.ensure(1));
+  CK(c->b_patch_atoms.ensure(std::max<int64_t>(nt, 1) * 3 * sizeof(int32_t)));
+  LAUNCH(nsg::launch_tri_patches(c->b_verts.as<double>(), c->b_tris.as<int32_t>(), nt, c->f64.as<double>(),
+                                 c->i32.as<int32_t>(), c->b_patch_atoms.as<int32_t>(), s));
+  CK(cudaStreamSynchronize(s));
+  c->ext_f64 = nullptr; c->ext_i32 = nullptr; c->ext_pool = nullptr; c->ext_flag = nullptr;
+  rc = upload_common(c, nt, 0, 0.0);
+  if (rc) return rc;
+  c->b_natoms = n_atoms;
+  c->b_nv_n = nv;
+  c->b_nt_n = nt;
+  c->b_B = blobbyness;
+  c->b_ng = ng;
+  c->b_quantized = quantize;
+  c->b_valid = true;
+  return NSG_OK;
+}
+
+// The blobby mesh of the last nsg_blobby_build (vertices after smoothing and the OFF round trip,
+// triangles with the field's marching-cubes winding); NULL buffers only report the sizes.
+int nsg_blobby_mesh(nsg_ctx* c, int64_t* n_vertices, int64_t* n_triangles, double* vertices, int32_t* triangles) {
+  if (!c) return NSG_ERR_ARG;
+  if (!c->b_valid) return fail(NSG_ERR_STATE, "no blobby mesh built");
+  if (n_vertices) *n_vertices = c->b_nv_n;
+  if (n_triangles) *n_triangles = c->b_nt_n;
+  if (vertices && c->b_nv_n)
+    CK(cudaMemcpyAsync(vertices, c->b_verts.p, c->b_nv_n * 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (triangles && c->b_nt_n)
+    CK(cudaMemcpyAsync(triangles, c->b_tris.p, c->b_nt_n * 3 * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return NSG_OK;
+}
+
+// d volume and d area of a differentiable blobby surface with respect to its atoms (x, y, z, r per
+// atom, in the order given to nsg_blobby_build), after a gradient-mode nsg_raycast (and the
+// nsg_triangulate that followed it, for the area); either pointer may be NULL.
+int nsg_blobby_atom_grads(nsg_ctx* c, double* d_volume, double* d_area) {
+  if (!c) return NSG_ERR_ARG;
+  if (!c->b_valid) return fail(NSG_ERR_STATE, "no blobby mesh built");
+  if (c->b_quantized)
+    return fail(NSG_ERR_STATE, "the OFF round trip is piecewise constant: build with NSG_BLOBBY_DIFFERENTIABLE");
+  if ((d_volume && !c->have_gvol) || (d_area && !c->have_garea))
+    return fail(NSG_ERR_STATE, "no gradient-mode ray cast / triangulation to read");
+  CK(cudaSetDevice(c->device));
+  const NsGrid& G = c->grid;
+  const nsg::GridDev g = grid_dev(G);
+  CK(c->b_gpost.ensure(std::max<int64_t>(c->b_nv_n, 1) * 3 * sizeof(double)));
+  CK(c->b_gpre.ensure(std::max<int64_t>(c->b_nv_n, 1) * 3 * sizeof(double)));
+  CK(c->b_gfield.ensure(G.nx * G.ny * G.nz * sizeof(double)));
+  CK(c->b_gatoms.ensure(c->b_natoms * 4 * sizeof(double)));
+  nsg::BlobbyMeshDev M{c->b_nv_n, c->b_nt_n, c->b_verts.as<double>(), c->b_vkey.as<int4>(), c->b_tris.as<int32_t>(),
+                       c->f64.as<double>(), c->b_patch_atoms.as<int32_t>(), c->b_inc_cnt.as<int32_t>()};
+  for (int which = 0; which < 2; which++) {
+    double* dst = which == 0 ? d_volume : d_area;
+    if (!dst) continue;
+    CK(cudaMemsetAsync(c->b_gatoms.p, 0, c->b_natoms * 4 * sizeof(double), c->stream));
+    LAUNCH(nsg::launch_blobby_adjoint(g, c->b_atoms.as<double>(), (int)c->b_natoms, c->b_B, c->b_ng,
+                                      c->b_field.as<double>(), 1.0, M,
+                                      which == 0 ? c->gvol.as<double>() : c->garea.as<double>(), c->b_gpost.as<double>(),
+                                      c->b_gpre.as<double>(), c->b_gfield.as<double>(), c->b_gatoms.as<double>(),
+                                      c->stream));
+    CK(cudaMemcpyAsync(dst, c->b_gatoms.p, c->b_natoms * 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  }
+  return NSG_OK;
+}
+
 int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
   if (!c || !c->has_grid || !c->has_patches) return fail(NSG_ERR_STATE, "grid and patches must be set first");
   if (c->patch_nstruct != c->nstruct) return fail(NSG_ERR_STATE, "patches were uploaded for another batch layout");
@@ -816,7 +958,7 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
     c->kind_mask_valid = true;
   }
   if (grad && (c->kind_mask & nsg::kSkinKinds))
-    return fail(NSG_ERR_STATE, "gradients are provided for SES patch sets, not for skin cells");
+    return fail(NSG_ERR_STATE, "gradients are provided for SES and mesh patch sets, not for skin cells");
   c->grad_mode = grad;
   c->have_gvol = c->have_garea = false;
   c->flags = flags;

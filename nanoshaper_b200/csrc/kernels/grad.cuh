@@ -5,6 +5,7 @@
 //   sphere (atom or probe): F = |x - c|^2 - r^2,                 theta = (c, r)
 //   torus:                  F = S^2 - 4 R^2 (|y|^2 - z^2),      theta = (tc, u, R)
 //                           y = x - tc, z = u . y, S = |y|^2 + R^2 - probe^2
+//   mesh triangle:          F = n . (x - v0), n = (v1 - v0) x (v2 - v0), theta = (v0, v1, v2)
 // (the torus with the local z axis u = third row of the inverse frame, the surface rayTorus
 // solves, src/tools.cpp:907-1098).  A probe sphere's radius is the fixed probe, so its slot 3
 // stays 0.  Derivatives of the volume (interval ends) and of the marching-cubes area (analytic
@@ -42,6 +43,27 @@ __device__ __forceinline__ bool hit_grad(const double* __restrict__ P, int kind,
     g[4] = cu * y1;
     g[5] = cu * y2;
     g[6] = -(4.0 * S * R - 8.0 * R * (yy - z * z)) * inv;
+    return true;
+  }
+  if (kind == NS_MESH_TRI) {
+    // F = n . (x - v0), n = (v1 - v0) x (v2 - v0): moving corner k by dv moves the hit along the
+    // ray by b_k (n . dv) / n_vc (b the hit's barycentric weights); g[k] = b_k / n_vc, the factor n
+    // is applied per triangle by the chain rule to the mesh vertices
+    const double* n = P + NS_TRI_N;
+    const double nn = n[0] * n[0] + n[1] * n[1] + n[2] * n[2];
+    const double den = vc == 0 ? n[0] : (vc == 1 ? n[1] : n[2]);
+    if (!(fabs(den) > 1e-12 * sqrt(nn))) return false;
+    const double e1[3] = {P[3] - P[0], P[4] - P[1], P[5] - P[2]};
+    const double e2[3] = {P[6] - P[0], P[7] - P[1], P[8] - P[2]};
+    const double w[3] = {x[0] - P[0], x[1] - P[1], x[2] - P[2]};
+    const double c1[3] = {w[1] * e2[2] - w[2] * e2[1], w[2] * e2[0] - w[0] * e2[2], w[0] * e2[1] - w[1] * e2[0]};
+    const double c2[3] = {e1[1] * w[2] - e1[2] * w[1], e1[2] * w[0] - e1[0] * w[2], e1[0] * w[1] - e1[1] * w[0]};
+    const double b1 = (c1[0] * n[0] + c1[1] * n[1] + c1[2] * n[2]) / nn;
+    const double b2 = (c2[0] * n[0] + c2[1] * n[1] + c2[2] * n[2]) / nn;
+    const double inv = 1.0 / den;
+    g[0] = (1.0 - b1 - b2) * inv;
+    g[1] = b1 * inv;
+    g[2] = b2 * inv;
     return true;
   }
   const double d0 = x[0] - P[0], d1 = x[1] - P[1], d2 = x[2] - P[2];

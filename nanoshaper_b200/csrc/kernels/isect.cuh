@@ -197,7 +197,7 @@ __device__ __forceinline__ void isect_body(const TraceCtx& C, const CandOut& co,
     for (int k = 0; k < nf; k++) f[k] = __ldg(src + k);
     const int32_t* ir = C.P.i32 + NS_PATCH_I32 * pid;
     const int kind = ir[0], first = ir[1], cnt = ir[2];
-    if (!kTorus && ns_is_skin(kind)) continue;  // skin cells share the list; k_isect_quad takes them
+    if (!kTorus && ns_has_box(kind)) continue;  // skin cells and triangles share the list (k_isect_quad)
     double t[4];
     int k;
     if (kMixed) {
@@ -325,7 +325,55 @@ __device__ __forceinline__ int intersect_quadric_mixed(const double* f, int firs
   return out;
 }
 
-// One thread per skin candidate (a cell in the sphere list): intersection, feasibility, hit filing.
+// ---- mesh triangles: Moller-Trumbore ----
+
+// Double-precision triangle test of the ray-based mesh caster (MeshSurface::getRayIntersection,
+// src/MeshSurface.cpp:1756-1855): the reference's intersect_triangle with the ray from pa along
+// axis vc of length dirl; the hit is the ray parameter t.
+template <int PN>
+__device__ __forceinline__ int intersect_tri_f64(const double* f, const double* pa, double dirl, double* t) {
+  constexpr int vc = Ax<PN>::vc;
+  double dir[3] = {0.0, 0.0, 0.0};
+  dir[vc] = dirl;
+  double u, v;
+  return ray_triangle_f64(pa, dir, f, f + 3, f + 6, t, &u, &v) ? 1 : 0;
+}
+
+// Mixed-precision triangle test: the barycentric coordinates of the ray's foot in the triangle
+// from the transverse offsets in FP32 (with the ray along an axis they need only the triangle's
+// and the origin's transverse coordinates relative to v0); decisions within 1e-4 of a bound, and a
+// determinant near the reference's EPS cut, are taken by the double-precision test instead.  The
+// hit is v0 + u e1 + v e2 along the axis in FP64.
+template <int PN>
+__device__ __forceinline__ int intersect_tri_mixed(const double* f, const double* pa, double dirl, double* t) {
+  constexpr int vc = Ax<PN>::vc;
+  constexpr int a = vc == 0 ? 1 : (vc == 1 ? 2 : 0), b = vc == 0 ? 2 : (vc == 1 ? 0 : 1);
+  const float e1a = (float)(f[3 + a] - f[a]), e1b = (float)(f[3 + b] - f[b]);
+  const float e2a = (float)(f[6 + a] - f[a]), e2b = (float)(f[6 + b] - f[b]);
+  const float ta = (float)(pa[a] - f[a]), tb = (float)(pa[b] - f[b]);
+  const float D = e1b * e2a - e1a * e2b;
+  const float det = D * (float)dirl;
+  constexpr float kBand = 1e-4f;
+  bool undecided = fabsf(det) < 4e-5f;
+  float u = 0.f, v = 0.f;
+  if (!undecided) {
+    const float inv = 1.f / D;
+    u = (tb * e2a - ta * e2b) * inv;
+    v = (ta * e1b - tb * e1a) * inv;
+    const float w = 1.f - u - v;
+    const float lo = fminf(u, fminf(v, w));
+    if (lo < -kBand) return 0;
+    // the reference's bounds: u <= 1 and u + v <= 1 as well (implied by w >= 0 and v >= 0)
+    undecided = lo <= kBand;
+  }
+  if (undecided) return intersect_tri_f64<PN>(f, pa, dirl, t);
+  const double x = f[vc] + (double)u * (f[3 + vc] - f[vc]) + (double)v * (f[6 + vc] - f[vc]);
+  *t = (x - pa[vc]) / dirl;
+  return 1;
+}
+
+// One thread per skin or triangle candidate (in the sphere list): intersection, feasibility, hit
+// filing.
 template <int PN, bool kMixed>
 __device__ __forceinline__ void isect_quadric_body(const TraceCtx& C, const CandOut& co, const HitStore& hs) {
   constexpr int fd = Ax<PN>::fd, ld = Ax<PN>::ld, vc = Ax<PN>::vc;
@@ -338,7 +386,7 @@ __device__ __forceinline__ void isect_quadric_body(const TraceCtx& C, const Cand
     const int64_t rid = e.x, pid = e.y;
     const int32_t* ir = C.P.i32 + NS_PATCH_I32 * pid;
     const int kind = ir[0], first = ir[1], cnt = ir[2];
-    if (!ns_is_skin(kind)) continue;
+    if (!ns_has_box(kind)) continue;
     const StructDev& S = C.B.s[C.B.patch_struct[pid]];
     const GridDev& g = S.g;
     const double delta = C.set == 0 ? 0.0 : NS_DELTA - g.hside;
@@ -355,7 +403,12 @@ __device__ __forceinline__ void isect_quadric_body(const TraceCtx& C, const Cand
     for (int k = 0; k < NS_SKIN_Q + 10; k++) f[k] = __ldg(src + k);
     double t[2];
     int k;
-    if (kMixed) {
+    if (kind == NS_MESH_TRI) {
+      // the ray of the mesh caster runs from pa to pb = the last node (+ delta) of the axis
+      const double dirl = (gcoord(g, vc, g.n[vc] - 1) + delta) - (gcoord(g, vc, 0) + delta);
+      pa[vc] = gcoord(g, vc, 0) + delta;
+      k = kMixed ? intersect_tri_mixed<PN>(f, pa, dirl, t) : intersect_tri_f64<PN>(f, pa, dirl, t);
+    } else if (kMixed) {
       k = intersect_quadric_mixed<PN>(f, first, cnt, C.P, pid, pa, S.box_dir[vc], t, C.out.counters);
       const bool defer = k == kDefer;
       const unsigned am = __activemask();

@@ -176,6 +176,7 @@ struct PatchDev {
 constexpr int kSesKinds = (1 << NS_POINT) | (1 << NS_EDGE_REG) | (1 << NS_EDGE_SING) | (1 << NS_FACE_REG) |
                           (1 << NS_FACE_SING);
 constexpr int kSkinKinds = (1 << NS_SKIN_POINT) | (1 << NS_SKIN_EDGE) | (1 << NS_SKIN_FACET) | (1 << NS_SKIN_TETRA);
+constexpr int kBoxKinds = kSkinKinds | (1 << NS_MESH_TRI);
 
 // Streaming multiprocessors of the current device (queried once per device and cached); grids of
 // the grid-stride kernels are sized as multiples of it.

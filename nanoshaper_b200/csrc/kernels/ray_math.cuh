@@ -247,4 +247,34 @@ __device__ __forceinline__ bool feasible_skin_f64(const double4* __restrict__ po
   return true;
 }
 
+// MeshSurface::intersect_triangle (src/MeshSurface.cpp:1487-1553, the non-culling branch) for a
+// ray from orig with direction dir (the full ray, so t is the ray parameter), operation for
+// operation; EPS = 1e-5 (src/MeshSurface.h:21).  Returns the parameter t and the barycentric u, v.
+__device__ __forceinline__ bool ray_triangle_f64(const double* orig, const double* dir, const double* v0,
+                                                 const double* v1, const double* v2, double* t, double* uo,
+                                                 double* vo) {
+  constexpr double kEps = 1e-5;
+  double edge1[3], edge2[3], tvec[3], pvec[3], qvec[3];
+  edge1[0] = v1[0] - v0[0]; edge1[1] = v1[1] - v0[1]; edge1[2] = v1[2] - v0[2];
+  edge2[0] = v2[0] - v0[0]; edge2[1] = v2[1] - v0[1]; edge2[2] = v2[2] - v0[2];
+  pvec[0] = dir[1] * edge2[2] - dir[2] * edge2[1];
+  pvec[1] = dir[2] * edge2[0] - dir[0] * edge2[2];
+  pvec[2] = dir[0] * edge2[1] - dir[1] * edge2[0];
+  const double det = edge1[0] * pvec[0] + edge1[1] * pvec[1] + edge1[2] * pvec[2];
+  if (det > -kEps && det < kEps) return false;
+  const double inv_det = 1.0 / det;
+  tvec[0] = orig[0] - v0[0]; tvec[1] = orig[1] - v0[1]; tvec[2] = orig[2] - v0[2];
+  const double u = (tvec[0] * pvec[0] + tvec[1] * pvec[1] + tvec[2] * pvec[2]) * inv_det;
+  if (u < 0.0 || u > 1.0) return false;
+  qvec[0] = tvec[1] * edge1[2] - tvec[2] * edge1[1];
+  qvec[1] = tvec[2] * edge1[0] - tvec[0] * edge1[2];
+  qvec[2] = tvec[0] * edge1[1] - tvec[1] * edge1[0];
+  const double v = (dir[0] * qvec[0] + dir[1] * qvec[1] + dir[2] * qvec[2]) * inv_det;
+  if (v < 0.0 || u + v > 1.0) return false;
+  *t = (edge2[0] * qvec[0] + edge2[1] * qvec[1] + edge2[2] * qvec[2]) * inv_det;
+  *uo = u;
+  *vo = v;
+  return true;
+}
+
 }  // namespace nsg

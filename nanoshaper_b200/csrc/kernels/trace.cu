@@ -33,9 +33,10 @@ __global__ void k_windows(PatchDev P, int32_t* win, BatchDev B) {
   double r = f[3];
   double down[3], up[3];
   bool cull = false;
-  const bool skin = ns_is_skin(P.i32[NS_PATCH_I32 * p]);
+  const bool skin = ns_has_box(P.i32[NS_PATCH_I32 * p]);
   for (int d = 0; d < 3; d++) {
-    // SES: the bounding sphere's box; skin: the cell's box (src/SkinSurface.cpp:3470-3500)
+    // SES: the bounding sphere's box; skin cells and mesh triangles: their stored box
+    // (src/SkinSurface.cpp:3470-3500, src/MeshSurface.cpp:447-472)
     down[d] = skin ? f[NS_SKIN_LO + d] : f[d] - r;
     up[d] = skin ? f[NS_SKIN_HI + d] : f[d] + r;
     if (down[d] > g.mx[d] + NS_EPS_INT) cull = true;
@@ -160,7 +161,16 @@ __device__ __forceinline__ int intersect_f64(const double* f, int kind, int firs
 // Tests one (ray, patch) candidate and reports the feasible hits in t[0..n-1].
 __device__ __forceinline__ int ray_patch_f64(const double* f, int kind, int first, int cnt, const PatchDev& P,
                                              const RaySet& rs, const double* pa, const double* dir, double ray_dir,
-                                             double box_dir, double* t) {
+                                             double box_dir, double tri_dir, double* t) {
+  if (kind == NS_MESH_TRI) {
+    for (int a = 0; a < 2; a++) {
+      const int d = a == 0 ? rs.fd : rs.ld;
+      if (pa[d] < f[NS_SKIN_LO + d] || pa[d] > f[NS_SKIN_HI + d]) return 0;
+    }
+    double tdir[3] = {0.0, 0.0, 0.0}, u, v;
+    tdir[rs.vc] = tri_dir;
+    return ray_triangle_f64(pa, tdir, f, f + 3, f + 6, t, &u, &v) ? 1 : 0;
+  }
   if (ns_is_skin(kind)) {
     // the cell's box in the pixel axes, the atom disc for Del0 cells, then the ray-quadric test
     for (int a = 0; a < 2; a++) {
@@ -401,7 +411,7 @@ __global__ void __launch_bounds__(256) k_cand(TraceCtx C, CandOut co) {
         const double* src = C.P.f64 + (int64_t)NS_PATCH_F64 * pid;
         const double cf = __ldg(src + rs.fd), cl = __ldg(src + rs.ld), r = __ldg(src + kR);
         const int kind0 = C.P.i32[NS_PATCH_I32 * pid];
-        const bool skin = ns_is_skin(kind0);
+        const bool skin = ns_has_box(kind0);
         q.cf[lane] = cf;
         q.cl[lane] = cl;
         q.lo_fd[lane] = skin ? __ldg(src + NS_SKIN_LO + rs.fd) : cf - r;
@@ -422,7 +432,7 @@ __global__ void __launch_bounds__(256) k_cand(TraceCtx C, CandOut co) {
         const int h = w[3 + rs.ld] - w[rs.ld] + 1;
         H = (w[3 + rs.fd] >= w[rs.fd] && h > 0) ? h : 0;
         const int kind = C.P.i32[NS_PATCH_I32 * pid];
-        q.ty[lane] = (kind == NS_EDGE_REG || kind == NS_EDGE_SING) ? 1 : 0;
+        q.ty[lane] = (kind == NS_EDGE_REG || kind == NS_EDGE_SING) ? 1 : 0;  // skin, triangles: sphere list
       }
       q.gfirst[lane] = 0;
       q.gend[lane] = 0;
@@ -527,7 +537,7 @@ template <int PN>
 void launch_isect(const TraceCtx& C, const CandOut& co, const HitStore& hs, int precision, const TuneParams& tp,
                   cudaStream_t s) {
   const int ig = sm_count() * tp.isect_bpsm, it = tp.isect_threads;
-  const bool ses = C.P.kind_mask & kSesKinds, skin = C.P.kind_mask & kSkinKinds;
+  const bool ses = C.P.kind_mask & kSesKinds, skin = C.P.kind_mask & kBoxKinds;
   if (precision == 1) {
     if (ses) launch_isect_mixed<PN>(C, co, hs, tp, s);
     if (skin) launch_isect_quad_mixed<PN>(C, co, hs, tp, s);
@@ -855,7 +865,8 @@ __global__ void k_trace_overflow(TraceCtx C, const int64_t* __restrict__ tile_of
     for (int k = 0; k < NS_PATCH_F64; k++) f[k] = C.P.f64[(int64_t)NS_PATCH_F64 * pid + k];
     const int32_t* ir = C.P.i32 + NS_PATCH_I32 * pid;
     double t[4];
-    int k = ray_patch_f64(f, ir[0], ir[1], ir[2], C.P, rs, pa, dir, ray_dir, S.box_dir[rs.vc], t);
+    const double tri_dir = (gcoord(g, rs.vc, g.n[rs.vc] - 1) + rs.delta) - pa[rs.vc];
+    int k = ray_patch_f64(f, ir[0], ir[1], ir[2], C.P, rs, pa, dir, ray_dir, S.box_dir[rs.vc], tri_dir, t);
     for (int i = 0; i < k; i++) {
       if (nh >= kOverflowCap) {
         atomicExch(C.out.error_flag, 4);

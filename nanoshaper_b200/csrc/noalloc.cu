@@ -65,7 +65,7 @@ __global__ void k_status_noalloc(Geo g, int64_t np, const double* __restrict__ f
     bool ovf = false;
     for (int64_t p = 0; p < np && !ovf; p++) {
       const double* f = f64 + NS_PATCH_F64 * p;
-      if (ns_is_skin(i32[NS_PATCH_I32 * p])) {
+      if (ns_has_box(i32[NS_PATCH_I32 * p])) {
         err[0] = 2.0;  // SES patch sets only
         ovf = true;
         break;

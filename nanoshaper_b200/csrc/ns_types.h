@@ -29,9 +29,12 @@ enum NsPatchKind {
   NS_SKIN_POINT = 5,
   NS_SKIN_EDGE = 6,
   NS_SKIN_FACET = 7,
-  NS_SKIN_TETRA = 8
+  NS_SKIN_TETRA = 8,
+  // Triangle of a mesh surface (MeshSurface, src/MeshSurface.h): the blobby surface is ray cast as
+  // the triangle mesh of its scalar field (src/BlobbySurface.cpp:83-229).
+  NS_MESH_TRI = 9
 };
-#define NS_KIND_COUNT 9
+#define NS_KIND_COUNT 10
 
 // Skin cell record (NS_PATCH_F64 doubles):
 //   [0..2]  local origin: the atom centre (Del0), else the centre of the cell's bounding box
@@ -45,7 +48,15 @@ enum NsPatchKind {
 #define NS_SKIN_Q 4
 #define NS_SKIN_LO 14
 #define NS_SKIN_HI 17
-NS_HD bool ns_is_skin(int kind) { return kind >= NS_SKIN_POINT; }
+NS_HD bool ns_is_skin(int kind) { return kind >= NS_SKIN_POINT && kind <= NS_SKIN_TETRA; }
+
+// Mesh triangle record (NS_PATCH_F64 doubles): [0..2] vertex 0, [3..5] vertex 1, [6..8] vertex 2,
+// [9..11] the unnormalised normal (v1 - v0) x (v2 - v0), [14..16] / [17..19] the triangle's box
+// (the NS_SKIN_LO / NS_SKIN_HI slots).  No pool entries.  The patch's three "atoms" are its mesh
+// vertex indices.
+#define NS_TRI_N 9
+// Patches culled by a stored box (skin cells, mesh triangles) rather than their bounding sphere.
+NS_HD bool ns_has_box(int kind) { return kind >= NS_SKIN_POINT; }
 
 // Per-patch double record (NS_PATCH_F64 doubles per patch).
 //   [0..2] bounding-sphere centre, [3] bounding-sphere radius

@@ -587,6 +587,85 @@ class SkinSurface(Surface):
         return super().getSurf(optimize_grids, fill, cav_vol, keep_hits, download, grad)
 
 
+class BlobbySurface(Surface):
+    """Blobby surface, ``Surface = blobby`` (src/BlobbySurface.h): the triangle mesh of the atoms'
+    Gaussian field (blobbyness ``Blobbyness``, cut-off 6 A) at iso level 1, smoothed once and
+    passed through the reference's OFF text round trip, then ray cast as a mesh surface.  The
+    field, its marching cubes, the smoothing and the round trip run on the GPU (nsg_blobby_build);
+    the mesh stays in device memory as the context's patch set.
+
+    ``differentiable = True`` skips the OFF round trip (a rounding of every coordinate to 1e-3 A,
+    piecewise constant in the atoms) so that ``gradients`` can chain the ray-cast volume and area
+    back to the atoms."""
+
+    name = "blobby"
+    DEFAULT_BLOBBYNESS = -2.5
+
+    def __init__(self, cf: ConfigFile | None = None, delphi: DelPhiShared | None = None, device: int = 0):
+        super().__init__(cf, delphi, device)
+        cf = cf or ConfigFile()
+        self.setBlobbyness(cf.read("Blobbyness", self.DEFAULT_BLOBBYNESS, float))
+        self.differentiable = False
+        self.n_mesh_vertices = 0
+        self.n_mesh_triangles = 0
+
+    def setBlobbyness(self, b: float) -> None:
+        """B < 0; a non-negative value keeps the default -2.5 with a warning (setBlobbyness)."""
+        if b >= 0:
+            import warnings
+            warnings.warn(f"Blobbyness is always a stricly negative real: setting {self.DEFAULT_BLOBBYNESS}")
+            b = self.DEFAULT_BLOBBYNESS
+        self.B = float(b)
+
+    def getBlobbyness(self) -> float:
+        return self.B
+
+    def isPatchBasedRayTracingSupported(self) -> bool:
+        # the reference ray casts the blobby mesh ray by ray (BlobbySurface overrides this to false)
+        return False
+
+    def getNumPatches(self) -> int:
+        return 0
+
+    def build(self) -> bool:
+        if self.delphi is None:
+            raise RuntimeError("Cannot build without DelPhi environment")
+        c = self._context().handle
+        N.check(N.lib().nsg_set_grid(c, ctypes.byref(self.delphi.grid)), "set_grid")
+        atoms = np.ascontiguousarray(self.delphi.atoms, np.float64)
+        flags = 1 if self.differentiable else 0
+        N.check(N.lib().nsg_blobby_build(c, N.ptr(atoms), len(atoms), self.B, flags), "blobby build")
+        nv, nt = ctypes.c_int64(), ctypes.c_int64()
+        N.check(N.lib().nsg_blobby_mesh(c, ctypes.byref(nv), ctypes.byref(nt), None, None), "blobby mesh")
+        self.n_mesh_vertices, self.n_mesh_triangles = nv.value, nt.value
+        self.built_from = atoms.copy()
+        return True
+
+    def upload(self) -> None:
+        # the mesh patches are built in the context's device memory by build()
+        if self.ctx is None or self.n_mesh_triangles is None:
+            raise RuntimeError("Cannot get surface before build()")
+
+    def mesh(self) -> tuple[np.ndarray, np.ndarray]:
+        """The blobby mesh that is ray cast: vertices (n, 3) and triangles (m, 3)."""
+        c = self._context().handle
+        v = np.zeros((self.n_mesh_vertices, 3))
+        t = np.zeros((self.n_mesh_triangles, 3), np.int32)
+        N.check(N.lib().nsg_blobby_mesh(c, None, None, N.ptr(v), N.ptr(t)), "blobby mesh")
+        return v, t
+
+    def gradients(self, dvol: float = 1.0, darea: float = 0.0) -> np.ndarray:
+        """(n_atoms, 4) derivative of dvol * volume + darea * area with respect to the atoms' x, y,
+        z and radius, after a gradient-mode getSurf (and triangulateSurface when darea is nonzero)
+        of a differentiable blobby surface."""
+        c = self._context().handle
+        n = len(self.built_from)
+        gv = np.zeros((n, 4))
+        ga = np.zeros((n, 4)) if darea != 0.0 else None
+        N.check(N.lib().nsg_blobby_atom_grads(c, N.ptr(gv), None if ga is None else N.ptr(ga)), "blobby gradients")
+        return dvol * gv if ga is None else dvol * gv + darea * ga
+
+
 class SurfaceBatch:
     """Many built surfaces, each with its own grid and patch set, ray cast and triangulated in the
     same kernel launches: one ``getSurf`` + ``triangulateSurface`` per structure, batched.
@@ -753,6 +832,7 @@ class SurfaceFactory:
 _factory = SurfaceFactory()
 _factory.add("ses", lambda cf, ds, dev=0: ConnollySurface(cf, ds, dev))
 _factory.add("skin", lambda cf, ds, dev=0: SkinSurface(cf, ds, dev))
+_factory.add("blobby", lambda cf, ds, dev=0: BlobbySurface(cf, ds, dev))
 
 
 def surfaceFactory() -> SurfaceFactory:

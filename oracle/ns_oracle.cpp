@@ -22,6 +22,15 @@
 // For skin patch sets (mixed cells):
 //   * per-cell ray casting      SkinSurface::getPatchIntersectionData (src/SkinSurface.cpp:3422-3760),
 //                               rayQuadricIntersectionX/Y/Z (:4632-4709), isFeasible (:4374-4448)
+// For blobby surfaces:
+//   * field, marching cubes     BlobbySurface::build (src/BlobbySurface.cpp:83-229), getVertices
+//                               with a scalar field (src/Surface.cpp:8143-8327), triangulationKernel
+//                               (:9075-9318), vertexInterp (:14516-14523), classifyCube (:14526-14545)
+//   * smoothing                 smoothSurface (src/Surface.cpp:13089-13354)
+//   * OFF round trip            saveMesh "%.3f" (src/Surface.cpp:10857-10960), loadOFF "%f"
+//                               (src/MeshSurface.cpp:2350-2479), done here with snprintf / sscanf
+//   * ray casting               MeshSurface::getRayIntersection + intersect_triangle
+//                               (src/MeshSurface.cpp:1487-1553, 1756-1855)
 // Single-threaded by default so that volume and area are summed in the reference's serial order.
 // Compile without FMA contraction (-ffp-contract=off) so that every operation rounds as written.
 #include <math.h>
@@ -244,6 +253,33 @@ bool ray_quadric(const double* Q, int vc, const double* o, double t[2]) {
   return true;
 }
 
+// MeshSurface::intersect_triangle, non-culling branch (src/MeshSurface.cpp:1487-1553), EPS 1e-5.
+bool ray_triangle(const double* orig, const double* dir, const double* v0, const double* v1, const double* v2,
+                  double* t) {
+  const double EPS = 1e-5;
+  double edge1[3], edge2[3], tvec[3], pvec[3], qvec[3];
+  for (int k = 0; k < 3; k++) {
+    edge1[k] = v1[k] - v0[k];
+    edge2[k] = v2[k] - v0[k];
+  }
+  pvec[0] = dir[1] * edge2[2] - dir[2] * edge2[1];
+  pvec[1] = dir[2] * edge2[0] - dir[0] * edge2[2];
+  pvec[2] = dir[0] * edge2[1] - dir[1] * edge2[0];
+  double det = edge1[0] * pvec[0] + edge1[1] * pvec[1] + edge1[2] * pvec[2];
+  if (det > -EPS && det < EPS) return false;
+  double inv_det = 1.0 / det;
+  for (int k = 0; k < 3; k++) tvec[k] = orig[k] - v0[k];
+  double u = (tvec[0] * pvec[0] + tvec[1] * pvec[1] + tvec[2] * pvec[2]) * inv_det;
+  if (u < 0.0 || u > 1.0) return false;
+  qvec[0] = tvec[1] * edge1[2] - tvec[2] * edge1[1];
+  qvec[1] = tvec[2] * edge1[0] - tvec[0] * edge1[2];
+  qvec[2] = tvec[0] * edge1[1] - tvec[1] * edge1[0];
+  double v = (dir[0] * qvec[0] + dir[1] * qvec[1] + dir[2] * qvec[2]) * inv_det;
+  if (v < 0.0 || u + v > 1.0) return false;
+  *t = (edge2[0] * qvec[0] + edge2[1] * qvec[1] + edge2[2] * qvec[2]) * inv_det;
+  return true;
+}
+
 // isFeasible (src/ConnollySurface.cpp:4769-5019) over the patch-set encoding.
 bool feasible(const Patches& P, int64_t it, const double* p) {
   const int32_t* ir = P.i32 + NS_PATCH_I32 * it;
@@ -379,6 +415,19 @@ struct Oracle {
             double dy = fr[ld] - pa[ld];
             if (dx * dx + dy * dy > fr[3] * fr[3]) continue;
           }
+          if (kind == NS_MESH_TRI) {
+            // the mesh caster's ray runs from the first to the last node (+ delta) of the axis
+            double dir[3] = {0., 0., 0.};
+            dir[vc] = (coord(vc, Nd(vc) - 1) + delta) - (coord(vc, 0) + delta);
+            double o[3] = {pa[0], pa[1], pa[2]};
+            o[vc] = coord(vc, 0) + delta;
+            double tt;
+            if (ray_triangle(o, dir, fr, fr + 3, fr + 6, &tt)) {
+              int64_t pid = (n * NMAX + m) * numPanels + (panels[0] * phase + panel);
+              out.push_back({pid, tt});
+            }
+            continue;
+          }
           double t[2];
           if (!ray_quadric(Q, vc, pa, t)) continue;
           for (int i = 0; i < 2; i++) {
@@ -397,7 +446,7 @@ struct Oracle {
     const int32_t* ir = P.i32 + NS_PATCH_I32 * it;
     const double* fr = P.f64 + NS_PATCH_F64 * it;
     int kind = ir[0];
-    if (ns_is_skin(kind)) {
+    if (ns_has_box(kind)) {
       trace_skin(it, out);
       return;
     }
@@ -871,7 +920,178 @@ struct Oracle {
   }
 };
 
+// The blobby mesh: field, marching cubes at iso 1, smoothing, OFF round trip.
+struct BlobbyMesh {
+  std::vector<double> verts;  // 3 per vertex
+  std::vector<int32_t> vkey;  // 4 per vertex: grid edge (x, y, z, axis)
+  std::vector<int32_t> tris;  // 3 per triangle
+};
+
+BlobbyMesh blobby_mesh(const NsGrid& g, const double* atoms, int64_t na, double B, bool quantize) {
+  const int64_t NX = g.nx, NY = g.ny, NZ = g.nz;
+  auto X = [&](int64_t i) { return ns_coord(g.xmin, g.side, i); };
+  auto Y = [&](int64_t j) { return ns_coord(g.ymin, g.side, j); };
+  auto Z = [&](int64_t k) { return ns_coord(g.zmin, g.side, k); };
+  auto IX = [&](int64_t i, int64_t j, int64_t k) { return (k * NY + j) * NX + i; };
+  // BlobbySurface::build: atom by atom over its cube of +-numgrid nodes (cut-off 6 A)
+  const int numgrid = (int)(6.0 / g.side + 0.5);
+  std::vector<double> field(NX * NY * NZ, 0.0);
+  for (int64_t a = 0; a < na; a++) {
+    const double* pos = atoms + 4 * a;
+    const double r = atoms[4 * a + 3];
+    const double r2 = r * r;
+    const int ix = (int)rintp((pos[0] - g.xmin) * g.scale);
+    const int iy = (int)rintp((pos[1] - g.ymin) * g.scale);
+    const int iz = (int)rintp((pos[2] - g.zmin) * g.scale);
+    const int sx = std::max(0, ix - numgrid), sy = std::max(0, iy - numgrid), sz = std::max(0, iz - numgrid);
+    const int ex = std::min((int)NX, ix + numgrid), ey = std::min((int)NY, iy + numgrid), ez = std::min((int)NZ, iz + numgrid);
+    for (int kk = sz; kk < ez; kk++)
+      for (int jj = sy; jj < ey; jj++)
+        for (int ii = sx; ii < ex; ii++) {
+          double p[3] = {X(ii) - g.hside, Y(jj) - g.hside, Z(kk) - g.hside};
+          double dist2 = (p[0] - pos[0]) * (p[0] - pos[0]) + (p[1] - pos[1]) * (p[1] - pos[1]) +
+                         (p[2] - pos[2]) * (p[2] - pos[2]);
+          field[IX(ii, jj, kk)] += exp(B * (dist2 / r2 - 1));
+        }
+  }
+  const double iso = 1.0;
+  static const int ec[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6}, {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
+  auto cube = [&](int64_t i, int64_t j, int64_t k, double* v) {
+    v[0] = field[IX(i, j, k)]; v[1] = field[IX(i + 1, j, k)]; v[2] = field[IX(i + 1, j + 1, k)];
+    v[3] = field[IX(i, j + 1, k)]; v[4] = field[IX(i, j, k + 1)]; v[5] = field[IX(i + 1, j, k + 1)];
+    v[6] = field[IX(i + 1, j + 1, k + 1)]; v[7] = field[IX(i, j + 1, k + 1)];
+    int c = 0;
+    for (int q = 0; q < 8; q++)
+      if (v[q] < iso) c |= 1 << q;
+    return c;
+  };
+  auto emask = [&](int c) {
+    int m = 0;
+    for (int e = 0; e < 12; e++)
+      if (((c >> ec[e][0]) & 1) != ((c >> ec[e][1]) & 1)) m |= 1 << e;
+    return m;
+  };
+  BlobbyMesh M;
+  std::vector<int32_t> idx[3];
+  for (int d = 0; d < 3; d++) idx[d].assign(NX * NY * NZ, -1);
+  // getVertices: the own edges 5, 6, 10 of every active cube, in (k, j, i) order
+  for (int64_t k = 1; k < NZ - 1; k++)
+    for (int64_t j = 1; j < NY - 1; j++)
+      for (int64_t i = 1; i < NX - 1; i++) {
+        double v[8];
+        int c = cube(i, j, k, v);
+        int m = emask(c);
+        if (m == 0) continue;
+        double xg = X(i), yg = Y(j), zg = Z(k);
+        double tb[6] = {xg - g.hside, xg + g.hside, yg - g.hside, yg + g.hside, zg - g.hside, zg + g.hside};
+        static const int mul[8][3] = {{0, 2, 4}, {1, 2, 4}, {1, 3, 4}, {0, 2, 4}, {0, 2, 5}, {1, 2, 5}, {1, 3, 5}, {0, 3, 5}};
+        double pos[8][3];
+        for (int q = 0; q < 8; q++)
+          for (int d = 0; d < 3; d++) pos[q][d] = tb[mul[q][d]];
+        auto interp = [&](int a, int b, double* p) {
+          double mu = (iso - v[a]) / (v[b] - v[a]);
+          for (int d = 0; d < 3; d++) {
+            double tmp = pos[b][d] - pos[a][d];
+            p[d] = pos[a][d] + mu * tmp;
+          }
+        };
+        struct E { int bit, a, b, dir; int64_t x, y, z; };
+        const E es[3] = {{32, 5, 6, NS_Y_DIR, i + 1, j, k + 1}, {64, 6, 7, NS_X_DIR, i, j + 1, k + 1},
+                         {1024, 2, 6, NS_Z_DIR, i + 1, j + 1, k}};
+        for (const E& e : es) {
+          if (!(m & e.bit)) continue;
+          double p[3];
+          interp(e.a, e.b, p);
+          idx[e.dir][IX(e.x, e.y, e.z)] = (int32_t)(M.verts.size() / 3);
+          M.verts.insert(M.verts.end(), p, p + 3);
+          int32_t key[4] = {(int32_t)e.x, (int32_t)e.y, (int32_t)e.z, e.dir};
+          M.vkey.insert(M.vkey.end(), key, key + 4);
+        }
+      }
+  // triangulationKernel: triangles in the case table's order and winding
+  for (int64_t k = 1; k < NZ - 1; k++)
+    for (int64_t j = 1; j < NY - 1; j++)
+      for (int64_t i = 1; i < NX - 1; i++) {
+        double v[8];
+        int c = cube(i, j, k, v);
+        int m = emask(c);
+        if (m == 0) continue;
+        const int64_t ek[12][4] = {{i, j, k, 0}, {i + 1, j, k, 1}, {i, j + 1, k, 0}, {i, j, k, 1},
+                                   {i, j, k + 1, 0}, {i + 1, j, k + 1, 1}, {i, j + 1, k + 1, 0}, {i, j, k + 1, 1},
+                                   {i, j, k, 2}, {i + 1, j, k, 2}, {i + 1, j + 1, k, 2}, {i, j + 1, k, 2}};
+        int vl[12];
+        for (int e = 0; e < 12; e++) vl[e] = (m & (1 << e)) ? idx[ek[e][3]][IX(ek[e][0], ek[e][1], ek[e][2])] : -1;
+        const char* cs = kNsMcCases[c];
+        for (int q = 0; cs[q]; q += 3) {
+          int a = vl[cs[q] <= '9' ? cs[q] - '0' : cs[q] - 'a' + 10];
+          int b = vl[cs[q + 1] <= '9' ? cs[q + 1] - '0' : cs[q + 1] - 'a' + 10];
+          int cc = vl[cs[q + 2] <= '9' ? cs[q + 2] - '0' : cs[q + 2] - 'a' + 10];
+          if (a == -1 || b == -1 || cc == -1) continue;
+          M.tris.push_back(a);
+          M.tris.push_back(b);
+          M.tris.push_back(cc);
+        }
+      }
+  // smoothSurface: one Laplacian pass
+  const int64_t nv = (int64_t)M.verts.size() / 3, nt = (int64_t)M.tris.size() / 3;
+  std::vector<double> temp(3 * nv, 0.0);
+  std::vector<int> nn(nv, 0);
+  for (int64_t t = 0; t < nt; t++) {
+    int v1 = M.tris[3 * t], v2 = M.tris[3 * t + 1], v3 = M.tris[3 * t + 2];
+    for (int d = 0; d < 3; d++) {
+      temp[3 * v1 + d] += M.verts[3 * v2 + d] + M.verts[3 * v3 + d];
+      temp[3 * v2 + d] += M.verts[3 * v1 + d] + M.verts[3 * v3 + d];
+      temp[3 * v3 + d] += M.verts[3 * v1 + d] + M.verts[3 * v2 + d];
+    }
+    nn[v1] += 2;
+    nn[v2] += 2;
+    nn[v3] += 2;
+  }
+  for (int64_t v = 0; v < nv; v++) {
+    double scale = 1.0 / (double)nn[v];
+    for (int d = 0; d < 3; d++) M.verts[3 * v + d] = 0.5 * (M.verts[3 * v + d] + temp[3 * v + d] * scale);
+  }
+  // saveMesh writes "%.3f", loadOFF reads "%f" into floats
+  if (quantize)
+    for (auto& x : M.verts) {
+      char buf[64];
+      snprintf(buf, sizeof buf, "%.3f", x);
+      float f;
+      sscanf(buf, "%f", &f);
+      x = f;
+    }
+  return M;
+}
+
 }  // namespace
+
+extern "C" {
+
+// Blobby mesh of atoms on a grid (test infrastructure); read back with nso_size / nso_copy on
+// "verts", "vkeys", "tris", freed with nso_free_mesh.
+void* nso_blobby(const NsGrid* g, const double* atoms, int64_t n_atoms, double blobbyness, int quantize) {
+  return new BlobbyMesh(blobby_mesh(*g, atoms, n_atoms, blobbyness, quantize != 0));
+}
+int64_t nso_mesh_size(void* h, const char* what) {
+  BlobbyMesh* m = (BlobbyMesh*)h;
+  std::string w(what);
+  if (w == "verts") return (int64_t)m->verts.size();
+  if (w == "vkeys") return (int64_t)m->vkey.size();
+  if (w == "tris") return (int64_t)m->tris.size();
+  return -1;
+}
+int nso_mesh_copy(void* h, const char* what, void* dst) {
+  BlobbyMesh* m = (BlobbyMesh*)h;
+  std::string w(what);
+  if (w == "verts") memcpy(dst, m->verts.data(), m->verts.size() * sizeof(double));
+  else if (w == "vkeys") memcpy(dst, m->vkey.data(), m->vkey.size() * sizeof(int32_t));
+  else if (w == "tris") memcpy(dst, m->tris.data(), m->tris.size() * sizeof(int32_t));
+  else return -1;
+  return 0;
+}
+void nso_free_mesh(void* h) { delete (BlobbyMesh*)h; }
+
+}  // extern "C"
 
 extern "C" {
 

@@ -53,6 +53,13 @@ def lib() -> ctypes.CDLL:
         L.nso_run_slab.restype = P
         L.nso_run_slab.argtypes = [P, ctypes.c_int64, P, P, P, P, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                    ctypes.c_double, ctypes.c_double]
+        L.nso_blobby.restype = P
+        L.nso_blobby.argtypes = [P, P, ctypes.c_int64, ctypes.c_double, ctypes.c_int]
+        L.nso_mesh_size.restype = ctypes.c_int64
+        L.nso_mesh_size.argtypes = [P, ctypes.c_char_p]
+        L.nso_mesh_copy.restype = ctypes.c_int
+        L.nso_mesh_copy.argtypes = [P, ctypes.c_char_p, P]
+        L.nso_free_mesh.argtypes = [P]
         L.nso_ray_torus.restype = ctypes.c_int
         L.nso_ray_torus.argtypes = [P, P, P, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int, P, P, P]
         _lib = L
@@ -136,3 +143,41 @@ def time_slab(grid, patches, threads: int, slab_lo: float, slab_hi: float,
     rays = int(L.nso_scalar(h, b"rays_cast"))
     L.nso_free(h)
     return dt, rays
+
+
+def blobby_mesh(grid, atoms: np.ndarray, blobbyness: float = -2.5, quantize: bool = True):
+    """The oracle's blobby mesh (field, marching cubes, smoothing, OFF round trip): vertices (n, 3),
+    their grid edges (n, 4) and triangles (m, 3)."""
+    L = lib()
+    atoms = np.ascontiguousarray(atoms, np.float64)
+    h = L.nso_blobby(ctypes.byref(grid), atoms.ctypes.data, len(atoms), blobbyness, int(quantize))
+    try:
+        out = []
+        for name, dt, w in (("verts", np.float64, 3), ("vkeys", np.int32, 4), ("tris", np.int32, 3)):
+            n = L.nso_mesh_size(h, name.encode())
+            a = np.zeros(max(n, 0), dt)
+            if n > 0:
+                L.nso_mesh_copy(h, name.encode(), a.ctypes.data)
+            out.append(a.reshape(-1, w))
+        return tuple(out)
+    finally:
+        L.nso_free_mesh(h)
+
+
+class TrianglePatches:
+    """A mesh as the oracle's triangle patch set (kind 9): vertices, normal, box per triangle."""
+
+    def __init__(self, verts: np.ndarray, tris: np.ndarray):
+        p = verts[tris]  # (m, 3, 3)
+        self.n = len(tris)
+        f = np.zeros((self.n, 20))
+        f[:, 0:9] = p.reshape(-1, 9)
+        f[:, 9:12] = np.cross(p[:, 1] - p[:, 0], p[:, 2] - p[:, 0])
+        f[:, 14:17] = p.min(axis=1)
+        f[:, 17:20] = p.max(axis=1)
+        self.f64 = np.ascontiguousarray(f)
+        self.i32 = np.zeros((self.n, 4), np.int32)
+        self.i32[:, 0] = 9
+        self.pool = np.zeros((1, 4))
+        self.pool_flag = np.zeros(1, np.int8)
+        self.probe = 0.0

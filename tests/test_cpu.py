@@ -671,3 +671,33 @@ def test_skin_reference_fixture_1crn_is_watertight(native_lib, oracle_mod):
         cnt, _ = oracle_mod.ray_hits(r, s)
         assert int((cnt % 2).sum()) == 0
     assert r.volume > 0
+
+
+def test_blobby_oracle_mesh_is_closed_and_matches_field(native_lib, oracle_mod):
+    """The oracle's blobby mesh (field, marching cubes, smoothing, OFF round trip) of a 60-atom
+    globule: every vertex is used and finite, the coordinates carry the OFF text's 3 decimals, every
+    ray of the four ray sets has an even hit count, and the ray-cast volume is within 3% of the
+    field's inside-node count times side^3."""
+    atoms = generator.rsa_globule(60, 2)
+    ds = nb.DelPhiShared(atoms, 3.0, 70.0)
+    v, keys, t = oracle_mod.blobby_mesh(ds.grid, ds.atoms, -2.5, True)
+    used = np.zeros(len(v), bool)
+    used[t.ravel()] = True
+    assert used.all() and np.isfinite(v).all()
+    assert np.allclose(v, np.round(v.astype(np.float64), 3), atol=1e-5)
+    r = oracle_mod.run(ds.grid, oracle_mod.TrianglePatches(v, t),
+                       flags=oracle_mod.STATUS | oracle_mod.ACCURATE_TRIANGULATION)
+    for s in range(4):
+        cnt, _ = oracle_mod.ray_hits(r, s)
+        assert int((cnt % 2).sum()) == 0
+    g = ds.grid
+    xs = g.xmin + np.arange(g.nx) * g.side - g.hside
+    ys = g.ymin + np.arange(g.ny) * g.side - g.hside
+    zs = g.zmin + np.arange(g.nz) * g.side - g.hside
+    Z, Y, X = np.meshgrid(zs, ys, xs, indexing="ij")
+    f = np.zeros(X.shape)
+    for a in ds.atoms:
+        d2 = (X - a[0]) ** 2 + (Y - a[1]) ** 2 + (Z - a[2]) ** 2
+        f += np.exp(-2.5 * (d2 / a[3] ** 2 - 1))
+    vol_nodes = (f > 1.0).sum() * g.side ** 3
+    assert abs(r.volume - vol_nodes) <= 0.03 * vol_nodes

@@ -1,0 +1,146 @@
+"""GPU parity of the blobby surface against the oracle, and its adjoint against finite differences.
+
+* The mesh: the device's Gaussian field, marching cubes, smoothing and OFF round trip give the
+  oracle's vertices and triangles exactly (the field's exp may differ in its last bit, which the
+  round trip to 1e-3 A absorbs).
+* The ray cast of that mesh (the differentiation configuration: 2,000 atoms, blobbyness -2.5,
+  grid scale 3.0, perfil 80): every ray's hits, status map, insideness bits, vertices, triangles,
+  volume and area against the oracle in double precision; in mixed precision hits within 1e-5 A
+  with the same hit counts and maps.
+* Gradients of the ray-cast volume and area of the differentiable blobby surface (no OFF round
+  trip) with respect to atom x, y, z and radius, against central differences with h = 1e-4 A on
+  64 atoms, in double and mixed precision (the rule of tests/test_gpu_grad.py for non-smooth
+  components).
+"""
+import numpy as np
+import pytest
+import torch
+
+import nanoshaper_b200 as nb
+from nanoshaper_b200 import autograd as AG
+from nanoshaper_b200 import generator
+
+pytestmark = pytest.mark.gpu
+
+H = 1e-4
+RTOL = 1e-4
+
+
+def _blobby(atoms, scale, perfil, precision="fp64", grid=None, differentiable=False):
+    ds = nb.DelPhiShared(atoms, scale, perfil) if grid is None else nb.DelPhiShared(atoms, grid=grid)
+    cf = nb.ConfigFile(text="Surface = blobby\nBlobbyness = -2.5\nAccurate_Triangulation = true\n"
+                            f"Triangulation = true\nGpu_Precision = {precision}\n")
+    surf = nb.surfaceFactory().create(cf, ds)
+    surf.differentiable = differentiable
+    surf.build()
+    return ds, surf
+
+
+def test_blobby_mesh_matches_oracle(native_lib, oracle_mod):
+    atoms = generator.rsa_globule(300, 3)
+    ds, surf = _blobby(atoms, 3.0, 80.0)
+    v, t = surf.mesh()
+    vo, _, to = oracle_mod.blobby_mesh(ds.grid, ds.atoms, -2.5, True)
+    assert v.shape == vo.shape and t.shape == to.shape
+    np.testing.assert_array_equal(t, to)
+    np.testing.assert_array_equal(v, vo)
+    # without the round trip the vertices agree to the rounding of the field's exp
+    ds2, surf2 = _blobby(atoms, 3.0, 80.0, differentiable=True)
+    v2, t2 = surf2.mesh()
+    vo2, _, to2 = oracle_mod.blobby_mesh(ds2.grid, ds2.atoms, -2.5, False)
+    np.testing.assert_array_equal(t2, to2)
+    assert np.abs(v2 - vo2).max() <= 1e-9
+
+
+@pytest.fixture(scope="module")
+def atoms_2000():
+    return generator.rsa_globule(2000, 11)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_blobby_raycast_matches_oracle(precision, atoms_2000, native_lib, oracle_mod):
+    import compare
+    ds, surf = _blobby(atoms_2000, 3.0, 80.0, precision=precision)
+    surf.getSurf(True, True, 10.0, keep_hits=True)
+    surf.triangulateSurface()
+    v, t = surf.mesh()
+    patches = oracle_mod.TrianglePatches(v, t)
+    ref = oracle_mod.run(ds.grid, patches, cav_vol=10.0, threads=8)
+    g = ds.grid
+    lens = ((g.nx - 1) * g.side, (g.nx - 1) * g.side, (g.nz - 1) * g.side, (g.ny - 1) * g.side)
+    worst = 0.0
+    for s in range(4):
+        cnt_g, val_g = surf.hits(s)
+        cnt_o, val_o = oracle_mod.ray_hits(ref, s)
+        assert np.array_equal(cnt_g, cnt_o), f"ray set {s}: {(cnt_g != cnt_o).sum()} rays with other hit counts"
+        if len(val_o):
+            d = float(np.abs(val_g - val_o).max())
+            worst = max(worst, d * lens[s] if precision == "mixed" else d)
+    if precision == "fp64":
+        assert worst <= 1e-12
+        figs = compare.compare_surface(surf, ds, ref)
+    else:
+        assert worst <= 1e-5, f"max hit error {worst} A"
+        figs = compare.compare_surface(surf, ds, ref, rel_tol=1e-9, vert_tol=1e-5)
+    print(f"blobby 2000 {precision} ({len(t)} triangles, grid {ds.nx}^3): worst hit diff {worst:.3e}, {figs}")
+
+
+class BlobbyRunner:
+    """Volume / area / insideness of a differentiable blobby surface of perturbed atoms on one grid."""
+
+    def __init__(self, grid, precision):
+        self.grid, self.precision = grid, precision
+
+    def __call__(self, atoms):
+        ds, surf = _blobby(atoms, 0, 0, precision=self.precision, grid=self.grid, differentiable=True)
+        try:
+            v = surf.getSurf(True, False, 0.0, download=True)
+            a = surf.triangulateSurface(download=False)
+            return v, a, surf.insideness.copy()
+        finally:
+            surf.ctx.close()
+
+
+def _fd(run, atoms, i, d, h):
+    a1 = atoms.copy()
+    a1[i, d] += h
+    a2 = atoms.copy()
+    a2[i, d] -= h
+    v1, ar1, b1 = run(a1)
+    v2, ar2, b2 = run(a2)
+    return (v1 - v2) / (2 * h), (ar1 - ar2) / (2 * h), bool((b1 != b2).any())
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_blobby_gradients_match_fd(precision, atoms_2000, native_lib):
+    atoms = atoms_2000
+    grid = AG.grid_for(atoms, 3.0, 80.0)
+    x = torch.tensor(atoms, dtype=torch.float64, requires_grad=True)
+    out = AG.blobby_volume_area(x, -2.5, grid, precision=precision)
+    gv = torch.autograd.grad(out[0], x, retain_graph=True)[0].numpy()
+    ga = torch.autograd.grad(out[1], x)[0].numpy()
+    run = BlobbyRunner(grid, precision)
+    v0, a0, _ = run(atoms)
+    assert abs(v0 - out[0].item()) <= 1e-12 * abs(v0) and abs(a0 - out[1].item()) <= 1e-12 * abs(a0)
+    pick = np.random.default_rng(7).choice(len(atoms), size=64, replace=False)
+    floor_v, floor_a = 1e-6 * np.abs(gv).max(), 1e-6 * np.abs(ga).max()
+    bad, skipped, total = [], 0, 0
+    for i in pick:
+        for d in range(4):
+            fv, fa, jump = _fd(run, atoms, i, d, H)
+            fv2, fa2, jump2 = _fd(run, atoms, i, d, H / 10)
+            for name, g, f, f2, fl, disc in (("vol", gv[i, d], fv, fv2, floor_v, False),
+                                             ("area", ga[i, d], fa, fa2, floor_a, jump or jump2)):
+                total += 1
+                if disc:
+                    skipped += 1
+                    continue
+                tol = lambda ref: RTOL * abs(ref) + fl  # noqa: E731
+                if abs(g - f) <= tol(f):
+                    continue
+                if abs(f - f2) > tol(f2) and abs(g - f2) <= tol(f2):
+                    continue
+                bad.append((name, int(i), d, g, f, f2))
+    print(f"blobby {precision}: {total} components, {skipped} skipped as discontinuous, {len(bad)} off")
+    assert skipped <= 0.1 * total
+    assert not bad, f"{len(bad)} of {total} components off: {bad[:6]}"
