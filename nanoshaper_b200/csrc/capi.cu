@@ -77,7 +77,7 @@ struct nsg_ctx {
   std::vector<nsg::StructDev> sd;
   DevBuf d_sd, d_patch_struct, d_tile_struct[3], d_ray_base[4], d_mc_base, d_row_base, d_row_chunks;
   int64_t nchunks = 0;
-  int64_t tiles_tot[3] = {0, 0, 0}, rays_tot[4] = {0, 0, 0, 0}, mc_tot = 0, rows_tot = 0, words_tot = 0;
+  int64_t tiles_tot[3] = {0, 0, 0}, rays_tot[4] = {0, 0, 0, 0}, mc_tot = 0, rows_tot = 0, words_tot = 0, cubes_tot = 0;
   int32_t patch_nstruct = 0;  // structures the uploaded patches belong to
   bool patch_struct_valid = false;
   std::vector<double> volumes, areas;
@@ -98,9 +98,13 @@ struct nsg_ctx {
   DevBuf tile_cnt[3], tile_off[3], tile_list[3], bin_area;
   int64_t win_area[3] = {0, 0, 0};
   // wavefront tracing: candidate lists and the slot-major hit store
-  DevBuf cand_sph, cand_tor, hit_t, hit_cnt, def_sph, def_tor;
+  // per ray set (slot s when the ray sets run on their own streams, slot 0 otherwise)
+  DevBuf cand_sph[4], cand_tor[4], hit_t[4], hit_cnt[4], def_sph[4], def_tor[4], hit_pid[4];
+  bool concurrent_sets = true;
+  cudaStream_t set_stream[4] = {};
+  cudaEvent_t fork_ev = nullptr, join_ev[4] = {};
   // gradient mode: hit / pair / vertex patches and the per-patch derivatives of volume and area
-  DevBuf hit_pid, pair_pid, ovf_pscratch, gvol, garea, vpid, vgrad;
+  DevBuf pair_pid, ovf_pscratch, gvol, garea, vpid, vgrad;
   // atoms behind the patches (for the device chain rule) and the atom derivatives
   std::vector<int64_t> patch_off{0, 0};
   DevBuf d_atoms, d_patch_atoms, d_gatoms_vol, d_gatoms_area, d_bad, d_patch_off, d_pool_off, d_atom_off;
@@ -128,7 +132,7 @@ struct nsg_ctx {
   std::vector<double> cav_size;
   std::vector<int32_t> cav_filled;
   // mesh
-  DevBuf cube_vl;
+  DevBuf cube_vl, cube_map, vstruct;
   nsg::TuneParams tune;
   DevBuf surv_cnt, surv_off, vpos, vkey, row_act_cnt, row_mid_cnt, row_act_off, row_mid_off, act_rec, act_mid,
       tri_cnt, tri_off, tris, cube_area, red_out;
@@ -212,7 +216,7 @@ int batch_layout(nsg_ctx* c, const NsGrid* grids, int32_t n) {
   std::vector<int4> chunks;  // marching-cubes row chunks: structure, first row, row count
   constexpr int32_t kRowChunk = 64;
   for (int i = 0; i < 4; i++) rb[i].resize(n + 1);
-  int64_t tiles[3] = {0, 0, 0}, rays[4] = {0, 0, 0, 0}, mc = 0, rows = 0, words = 0;
+  int64_t tiles[3] = {0, 0, 0}, rays[4] = {0, 0, 0, 0}, mc = 0, rows = 0, words = 0, cubes = 0;
   for (int32_t b = 0; b < n; b++) {
     const NsGrid& G = grids[b];
     if (G.nx < 3 || G.ny < 3 || G.nz < 3) return fail(NSG_ERR_ARG, "grid must have at least 3 nodes per axis");
@@ -238,6 +242,8 @@ int batch_layout(nsg_ctx* c, const NsGrid* grids, int32_t n) {
     S.mc_base = mcb[b] = mc;
     mc += G.nz * G.ny + G.ny * G.nx + G.nz * G.nx;
     S.row_base = rowb[b] = rows;
+    S.cube_base = cubes;
+    cubes += (G.nx - 2) * (G.ny - 2) * (G.nz - 2);
     const int64_t srows = (G.ny - 2) * (G.nz - 2);
     for (int64_t r = 0; r < srows; r += kRowChunk)
       chunks.push_back(make_int4(b, (int32_t)r, (int32_t)std::min<int64_t>(kRowChunk, srows - r), 0));
@@ -271,6 +277,7 @@ int batch_layout(nsg_ctx* c, const NsGrid* grids, int32_t n) {
   c->mc_tot = mc;
   c->rows_tot = rows;
   c->words_tot = words;
+  c->cubes_tot = cubes;
   c->has_grid = true;
   c->have_status = c->have_bits = false;
   c->volumes.assign(n, 0.0);
@@ -452,10 +459,10 @@ int nsg_ctx_destroy(nsg_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   DevBuf* bufs[] = {&c->f64, &c->i32, &c->pool, &c->flag, &c->win, &c->pool32, &c->quad32, &c->quadl, &c->kind_mask_d, &c->b_atoms, &c->b_field, &c->b_mask, &c->b_nv, &c->b_nt, &c->b_voff, &c->b_toff, &c->b_vraw, &c->b_verts, &c->b_vkey, &c->b_tris, &c->b_inc_cnt, &c->b_inc_off, &c->b_inc_cur, &c->b_inc, &c->b_patch_atoms, &c->b_gpost, &c->b_gpre, &c->b_gfield, &c->b_gatoms, &c->counters, &c->bin_area,
-                    &c->cand_sph, &c->cand_tor, &c->def_sph, &c->def_tor, &c->hit_t, &c->hit_cnt, &c->status, &c->bits, &c->pairs,
+                    &c->status, &c->bits, &c->pairs,
                     &c->ray_pair_off, &c->ray_pair_cnt, &c->cursors, &c->ovf_scratch, &c->err, &c->hits,
-                    &c->hit_pid, &c->pair_pid, &c->ovf_pscratch, &c->gvol, &c->garea, &c->vpid, &c->vgrad,
-                    &c->d_atoms, &c->d_patch_atoms, &c->d_gatoms_vol, &c->d_gatoms_area, &c->d_bad, &c->cube_vl,
+                    &c->pair_pid, &c->ovf_pscratch, &c->gvol, &c->garea, &c->vpid, &c->vgrad,
+                    &c->d_atoms, &c->d_patch_atoms, &c->d_gatoms_vol, &c->d_gatoms_area, &c->d_bad, &c->cube_vl, &c->cube_map, &c->vstruct,
                     &c->d_patch_off, &c->d_pool_off, &c->d_atom_off,
                     &c->labels, &c->is_root, &c->sruns, &c->srun_off, &c->srun_cnt, &c->fr_cnt, &c->fr_off,
                     &c->fruns, &c->frow, &c->roots, &c->cc_count, &c->cc_desc, &c->cc_label_of,
@@ -471,6 +478,10 @@ int nsg_ctx_destroy(nsg_ctx* c) {
   for (int i = 0; i < 4; i++) c->d_ray_base[i].release();
   for (int i = 0; i < 4; i++) {
     c->vol_ray[i].release(); c->ovf_rays[i].release(); c->ray_hit_off[i].release(); c->ray_hit_cnt[i].release();
+    c->cand_sph[i].release(); c->cand_tor[i].release(); c->def_sph[i].release(); c->def_tor[i].release();
+    c->hit_t[i].release(); c->hit_cnt[i].release(); c->hit_pid[i].release();
+    if (c->set_stream[i]) cudaStreamDestroy(c->set_stream[i]);
+    if (c->join_ev[i]) cudaEventDestroy(c->join_ev[i]);
   }
   for (int i = 0; i < 8; i++)
     if (c->user_ev[i]) cudaEventDestroy(c->user_ev[i]);
@@ -725,6 +736,7 @@ int nsg_set_tuning(nsg_ctx* c, const int32_t* params, int n) {
   c->tune.isect_threads = it;
   c->tune.isect_bpsm = bpsm;
   c->tune.cand_threads = ct;
+  if (n >= 4) c->concurrent_sets = params[3] != 0;
   return NSG_OK;
 }
 
@@ -733,6 +745,7 @@ int nsg_get_tuning(nsg_ctx* c, int32_t* params, int n) {
   params[0] = c->tune.isect_threads;
   params[1] = c->tune.isect_bpsm;
   params[2] = c->tune.cand_threads;
+  if (n >= 4) params[3] = c->concurrent_sets ? 1 : 0;
   return NSG_OK;
 }
 
@@ -1002,15 +1015,31 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
     if (c->pair_cap == 0) c->pair_cap = std::max<int64_t>(4 * nrays_mc, 1 << 16);
   }
   CK(c->cursors.ensure(32 * sizeof(unsigned long long)));
+  // the ray sets run on their own streams (each with its own candidate lists and hit store) so
+  // that the double-precision intersection launches of one set overlap the integer-bound candidate
+  // and fill launches of another; or, with concurrent_sets off, one after another on the context's
+  // stream through slot 0
+  const bool conc = c->concurrent_sets && (do_mc ? 3 : 0) + (do_status ? 1 : 0) > 1;
+  const auto slot_of = [&](int set) { return conc ? set : 0; };
   {
     int64_t amax = std::max(c->win_area[0], std::max(c->win_area[1], c->win_area[2]));
     c->cand_cap = std::max<int64_t>(c->cand_cap, amax + 1024);
-    int64_t nr_max = std::max(std::max(c->rays_tot[0], c->rays_tot[1]), std::max(c->rays_tot[2], c->rays_tot[3]));
-    CK(c->hit_t.ensure((size_t)nr_max * nsg::kHitCap * sizeof(double)));
-    CK(c->hit_cnt.ensure(nr_max * sizeof(int32_t)));
-    if (grad) {
-      CK(c->hit_pid.ensure((size_t)nr_max * nsg::kHitCap * sizeof(int32_t)));
-      CK(c->gvol.ensure(std::max<int64_t>(c->np, 1) * NS_GRAD_PER_PATCH * sizeof(double)));
+    for (int set = 0; set < 4; set++) {
+      if ((set == 0 && !do_status) || (set > 0 && !do_mc)) continue;
+      const int sl = slot_of(set);
+      const int64_t nr = conc ? c->rays_tot[set]
+                              : std::max(std::max(c->rays_tot[0], c->rays_tot[1]), std::max(c->rays_tot[2], c->rays_tot[3]));
+      CK(c->hit_t[sl].ensure((size_t)nr * nsg::kHitCap * sizeof(double)));
+      CK(c->hit_cnt[sl].ensure(nr * sizeof(int32_t)));
+      if (grad) CK(c->hit_pid[sl].ensure((size_t)nr * nsg::kHitCap * sizeof(int32_t)));
+    }
+    if (grad) CK(c->gvol.ensure(std::max<int64_t>(c->np, 1) * NS_GRAD_PER_PATCH * sizeof(double)));
+    if (conc) {
+      if (!c->fork_ev) CK(cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming));
+      for (int set = 0; set < 4; set++) {
+        if (!c->set_stream[set]) CK(cudaStreamCreateWithFlags(&c->set_stream[set], cudaStreamNonBlocking));
+        if (!c->join_ev[set]) CK(cudaEventCreateWithFlags(&c->join_ev[set], cudaEventDisableTiming));
+      }
     }
   }
   CK(c->err.ensure(sizeof(int32_t)));
@@ -1020,12 +1049,16 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
     if (do_mc && grad) CK(c->pair_pid.ensure(c->pair_cap * sizeof(int2)));
     if (grad)
       CK(cudaMemsetAsync(c->gvol.p, 0, std::max<int64_t>(c->np, 1) * NS_GRAD_PER_PATCH * sizeof(double), c->stream));
-    CK(c->cand_sph.ensure(c->cand_cap * sizeof(int2)));
-    CK(c->cand_tor.ensure(c->cand_cap * sizeof(int2)));
-    if (precision == NSG_PRECISION_MIXED) {
-      c->def_cap = std::max<int64_t>(c->def_cap, c->cand_cap / 16 + (1 << 16));
-      CK(c->def_sph.ensure(c->def_cap * sizeof(int2)));
-      CK(c->def_tor.ensure(c->def_cap * sizeof(int2)));
+    if (precision == NSG_PRECISION_MIXED) c->def_cap = std::max<int64_t>(c->def_cap, c->cand_cap / 16 + (1 << 16));
+    for (int set = 0; set < 4; set++) {
+      if ((set == 0 && !do_status) || (set > 0 && !do_mc)) continue;
+      const int sl = slot_of(set);
+      CK(c->cand_sph[sl].ensure(c->cand_cap * sizeof(int2)));
+      CK(c->cand_tor[sl].ensure(c->cand_cap * sizeof(int2)));
+      if (precision == NSG_PRECISION_MIXED) {
+        CK(c->def_sph[sl].ensure(c->def_cap * sizeof(int2)));
+        CK(c->def_tor[sl].ensure(c->def_cap * sizeof(int2)));
+      }
     }
     if (do_status) {
       CK(c->sruns.ensure(c->srun_cap * sizeof(int2)));
@@ -1049,8 +1082,14 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
       CK(cudaMemsetAsync(c->counters.p, 0, 8 * sizeof(unsigned long long), c->stream));
     }
     stage_begin(c, kStageTrace);
+    if (conc) CK(cudaEventRecord(c->fork_ev, c->stream));
     for (int si = 0; si < nsets; si++) {
       int s = sets[si];
+      cudaStream_t st = c->stream;
+      if (conc) {
+        st = c->set_stream[s];
+        CK(cudaStreamWaitEvent(st, c->fork_ev, 0));
+      }
       int panel = s == 0 ? 0 : s - 1;
       int64_t nr = c->rays_tot[s];
       CK(c->vol_ray[s].ensure(nr * sizeof(double)));
@@ -1081,7 +1120,7 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
       if (keep_hits) {
         CK(c->ray_hit_off[s].ensure(nr * sizeof(int64_t)));
         CK(c->ray_hit_cnt[s].ensure(nr * sizeof(int32_t)));
-        CK(cudaMemsetAsync(c->ray_hit_cnt[s].p, 0, nr * sizeof(int32_t), c->stream));
+        CK(cudaMemsetAsync(c->ray_hit_cnt[s].p, 0, nr * sizeof(int32_t), st));
         o.hits = c->hits.as<double>();
         o.hit_cap = c->hit_cap;
         o.hit_cursor = cur + 1;
@@ -1089,10 +1128,12 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
         o.ray_hit_cnt = c->ray_hit_cnt[s].as<int32_t>();
       }
       outs[s] = o;
-      nsg::CandOut co{c->cand_sph.as<int2>(), c->cand_tor.as<int2>(), c->cand_cap, cur + 8 + 2 * s,
-                      c->def_sph.as<int2>(), c->def_tor.as<int2>(), c->def_cap, cur + 16 + 2 * s};
-      nsg::HitStore hs{c->hit_t.as<double>(), c->hit_cnt.as<int32_t>(), nr, grad ? c->hit_pid.as<int32_t>() : nullptr};
-      CK(cudaMemsetAsync(c->hit_cnt.p, 0, nr * sizeof(int32_t), c->stream));
+      const int sl = slot_of(s);
+      nsg::CandOut co{c->cand_sph[sl].as<int2>(), c->cand_tor[sl].as<int2>(), c->cand_cap, cur + 8 + 2 * s,
+                      c->def_sph[sl].as<int2>(), c->def_tor[sl].as<int2>(), c->def_cap, cur + 16 + 2 * s};
+      nsg::HitStore hs{c->hit_t[sl].as<double>(), c->hit_cnt[sl].as<int32_t>(), nr,
+                       grad ? c->hit_pid[sl].as<int32_t>() : nullptr};
+      CK(cudaMemsetAsync(c->hit_cnt[sl].p, 0, nr * sizeof(int32_t), st));
       c->launches += precision == NSG_PRECISION_MIXED ? 6 : 4;
       cudaEvent_t* ev = nullptr;
       if (c->profile) {
@@ -1100,8 +1141,11 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
           if (!c->sub_ev[s][q]) CK(cudaEventCreate(&c->sub_ev[s][q]));
         ev = c->sub_ev[s];
       }
-      CK(nsg::launch_trace(P, B, s, c->tiles_tot[panel], o, co, hs, precision, c->tune, c->stream, ev));
+      CK(nsg::launch_trace(P, B, s, c->tiles_tot[panel], o, co, hs, precision, c->tune, st, ev));
+      if (conc) CK(cudaEventRecord(c->join_ev[s], st));
     }
+    if (conc)
+      for (int si = 0; si < nsets; si++) CK(cudaStreamWaitEvent(c->stream, c->join_ev[sets[si]], 0));
     stage_end(c, kStageTrace);
     if (c->profile) {
       // candidate, intersection and fill kernels of every ray set (stage_end synchronised the stream)
@@ -1348,6 +1392,8 @@ int nsg_triangulate(nsg_ctx* c, double* area_out, int64_t* nverts, int64_t* ntri
   CK(c->vpos.ensure(std::max<int64_t>(n_an, 1) * 3 * sizeof(double)));
   V.vpos = c->vpos.as<double>();
   V.vkey = c->vkey.as<int4>();
+  CK(c->vstruct.ensure(std::max<int64_t>(n_an, 1) * sizeof(int32_t)));
+  V.vstruct = c->vstruct.as<int32_t>();
   const bool grad = c->grad_mode && c->have_gvol;
   if (grad) {
     CK(c->vpid.ensure(std::max<int64_t>(n_an, 1) * sizeof(int32_t)));
@@ -1359,6 +1405,7 @@ int nsg_triangulate(nsg_ctx* c, double* area_out, int64_t* nverts, int64_t* ntri
   stage_begin(c, kStageMC);
   M.vpos = c->vpos.as<double>();
   M.vkey = c->vkey.as<int4>();
+  M.vstruct = c->vstruct.as<int32_t>();
   // active cubes
   LAUNCH(nsg::launch_mc_rows(M, 0, c->stream));
   int64_t n_act = 0, n_mid = 0;
@@ -1374,7 +1421,15 @@ int nsg_triangulate(nsg_ctx* c, double* area_out, int64_t* nverts, int64_t* ntri
   M.mid_cnt = c->row_mid_cnt.as<int32_t>();
   M.mid_off = c->row_mid_off.as<int64_t>();
   M.n_active = n_act;
+  // the dense cube -> active-cube map (entries of inactive cubes are never read, so it is not
+  // cleared) and the vertex of every cut edge of every active cube, filled by the vertices
+  CK(c->cube_map.ensure(std::max<int64_t>(c->cubes_tot, 1) * sizeof(int32_t)));
+  CK(c->cube_vl.ensure(std::max<int64_t>(n_act, 1) * 12 * sizeof(int32_t)));
+  M.cube_map = c->cube_map.as<int32_t>();
+  M.cube_vl = c->cube_vl.as<int32_t>();
+  CK(cudaMemsetAsync(c->cube_vl.p, 0xff, std::max<int64_t>(n_act, 1) * 12 * sizeof(int32_t), c->stream));
   LAUNCH(nsg::launch_mc_rows(M, 1, c->stream));
+  LAUNCH(nsg::launch_mc_push(M, 0, n_an, c->stream));
   // midpoint vertices of cut edges without an analytic vertex
   LAUNCH(nsg::launch_mc_mid(M, 0, c->stream));
   rc = scan_counts(c, c->row_mid_cnt.as<int32_t>(), n_act, c->row_mid_off.as<int64_t>(), &n_mid);
@@ -1394,16 +1449,24 @@ int nsg_triangulate(nsg_ctx* c, double* area_out, int64_t* nverts, int64_t* ntri
     c->vkey = nk;
     c->vpos = np_;
   }
+  if ((size_t)n_v * sizeof(int32_t) > c->vstruct.cap) {
+    DevBuf ns;
+    CK(ns.ensure(n_v * sizeof(int32_t)));
+    if (n_an) CK(cudaMemcpyAsync(ns.p, c->vstruct.p, n_an * sizeof(int32_t), cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->vstruct.release();
+    c->vstruct = ns;
+  }
   M.vpos = c->vpos.as<double>();
   M.vkey = c->vkey.as<int4>();
+  M.vstruct = c->vstruct.as<int32_t>();
   LAUNCH(nsg::launch_mc_mid(M, 1, c->stream));
+  LAUNCH(nsg::launch_mc_push(M, n_an, n_v, c->stream));
   M.n_active = n_act;
   CK(c->tri_cnt.ensure(std::max<int64_t>(n_act, 1) * sizeof(int32_t)));
   CK(c->tri_off.ensure((n_act + 1) * sizeof(int64_t)));
   CK(c->cube_area.ensure(std::max<int64_t>(n_act, 1) * sizeof(double)));
   M.tri_cnt = c->tri_cnt.as<int32_t>();
-  CK(c->cube_vl.ensure(std::max<int64_t>(n_act, 1) * 12 * sizeof(int32_t)));
-  M.cube_vl = c->cube_vl.as<int32_t>();
   M.cube_area = c->cube_area.as<double>();
   if (grad) {
     const nsg::PatchDev P = patch_dev(c);

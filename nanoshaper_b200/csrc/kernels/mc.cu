@@ -4,9 +4,10 @@
 // vertices on the grid edges that contain the interval ends; a vertex is dropped when the two
 // end nodes of its edge have the same final insideness, and the first vertex of an edge wins
 // (assembleVerticesList src/Surface.cpp:7415-7667).  Vertices keep the reference order: panel 0
-// rays (z-major), panel 1 rays (y-major), panel 2 rays (z-major), pairs in ray order.  Because a
-// ray's surviving vertices are sorted along the ray, the vertex of a grid edge is found by a
-// binary search over that one ray's survivors, so no dense edge-index grids are needed.
+// rays (z-major), panel 1 rays (y-major), panel 2 rays (z-major), pairs in ray order.  Each vertex
+// writes its id into the slots of the (up to four) active cubes that share its grid edge
+// (atomicMin: the first vertex of an edge wins), through a dense cube -> active-cube map written
+// by the classification pass, so the triangle passes read every cut edge's vertex directly.
 //
 // Marching cubes: cubes (i,j,k) in [1, N-2]^3 are classified from the 8 insideness bits; active
 // cubes add an edge-midpoint vertex to their own edges 5, 6, 10 that carry no analytic vertex,
@@ -107,6 +108,7 @@ __global__ void k_vert(VertArgs A, int emit) {
       A.vpos[3 * o + 1] = p[1];
       A.vpos[3 * o + 2] = p[2];
       A.vkey[o] = e;
+      A.vstruct[o] = (int32_t)(&S - A.B.s);
       if (A.vpid) {
         const int2 pp = A.pair_pid[A.ray_pair_off[r] + (q >> 1)];
         A.vpid[o] = (q & 1) ? pp.y : pp.x;
@@ -116,42 +118,13 @@ __global__ void k_vert(VertArgs A, int emit) {
   }
 }
 
-// Index of the analytic vertex on edge (dir, i, j, k), -1 if none.
-__device__ __forceinline__ int64_t analytic_vertex(const MCArgs& A, const StructDev& S, int dir, int64_t i, int64_t j,
-                                                   int64_t k) {
-  const GridDev& g = S.g;
-  const int64_t NX = g.n[0], NY = g.n[1], NZ = g.n[2];
-  int64_t r, e;
-  if (dir == NS_X_DIR) { r = k * NY + j; e = i; }
-  else if (dir == NS_Z_DIR) { r = NZ * NY + j * NX + i; e = k; }
-  else { r = NZ * NY + NY * NX + k * NX + i; e = j; }
-  r += S.mc_base;
-  int cnt = A.surv_cnt[r];
-  if (cnt == 0) return -1;
-  // the ray's survivors are sorted along the ray: first one at position >= e
-  const int64_t off = A.surv_off[r];
-  const int* kv = (const int*)(A.vkey + off) + (dir == NS_X_DIR ? 0 : (dir == NS_Y_DIR ? 1 : 2));
-  int lo = 0, hi = cnt;
-  while (lo < hi) {
-    int mid = (lo + hi) >> 1;
-    if (kv[4 * mid] < e) lo = mid + 1;
-    else hi = mid;
-  }
-  return (lo < cnt && kv[4 * lo] == e) ? off + lo : -1;
-}
-
-// Midpoint vertices a cube creates on its own edges 5 (y), 6 (x), 10 (z): bit 0, 1, 2.
-__device__ __forceinline__ int own_midpoints(const MCArgs& A, const StructDev& S, int64_t i, int64_t j, int64_t k,
-                                             int em) {
-  int mm = 0;
-  if ((em & 32) && analytic_vertex(A, S, NS_Y_DIR, i + 1, j, k + 1) < 0) mm |= 1;
-  if ((em & 64) && analytic_vertex(A, S, NS_X_DIR, i, j + 1, k + 1) < 0) mm |= 2;
-  if ((em & 1024) && analytic_vertex(A, S, NS_Z_DIR, i + 1, j + 1, k) < 0) mm |= 4;
-  return mm;
-}
-
 __device__ __forceinline__ int rec_struct(int w) { return (int)((unsigned)w >> 11); }
 
+
+// Local index of cube (i, j, k) in its structure's dense cube map.
+__device__ __forceinline__ int64_t cube_local(const GridDev& g, int64_t i, int64_t j, int64_t k) {
+  return ((k - 1) * (g.n[1] - 2) + (j - 1)) * (g.n[0] - 2) + (i - 1);
+}
 
 // The 32 bits of the flat bit grid starting at bit f (missing words read as outside), and in *next
 // the 32 bits starting at f + 1, from the same two words.
@@ -234,6 +207,7 @@ __global__ void k_mc_rows(MCArgs A, int emit) {
             int cs = 0;
 #pragma unroll
             for (int q = 0; q < 8; q++) cs |= ((c[q] >> bit) & 1u) << q;
+            A.cube_map[S.cube_base + cube_local(S.g, ic + bit, j, k)] = (int32_t)slot;
             A.act_rec[slot++] = make_int4((int)(ic + bit), j, k, cs | (C.x << 11));
           }
         }
@@ -259,7 +233,13 @@ __global__ void k_mc_mid(MCArgs A, int emit) {
     const StructDev& S = A.B.s[rec_struct(rec.w)];
     const GridDev& g = S.g;
     if (!emit) {
-      int mm = own_midpoints(A, S, i, j, k, s_emask[rec.w & 255]);
+      // own edges 5 (y), 6 (x), 10 (z) that are cut and carry no analytic vertex
+      const int em = s_emask[rec.w & 255];
+      const int32_t* cv = A.cube_vl + 12 * a;
+      int mm = 0;
+      if ((em & 32) && cv[5] < 0) mm |= 1;
+      if ((em & 64) && cv[6] < 0) mm |= 2;
+      if ((em & 1024) && cv[10] < 0) mm |= 4;
       A.act_rec[a].w = (rec.w & ~(7 << 8)) | (mm << 8);
       A.mid_cnt[a] = __popc(mm);
       continue;
@@ -267,6 +247,7 @@ __global__ void k_mc_mid(MCArgs A, int emit) {
     int mm = (rec.w >> 8) & 7;
     int64_t v = A.n_analytic + A.mid_off[a];
     A.act_mid[a] = (int32_t)v;
+    for (int q = 0; q < __popc(mm); q++) A.vstruct[v + q] = rec_struct(rec.w);
     if (mm & 1) {
       A.vpos[3 * v] = gcoord(g, 0, i + 1) - g.hside; A.vpos[3 * v + 1] = gcoord(g, 1, j);
       A.vpos[3 * v + 2] = gcoord(g, 2, k + 1) - g.hside;
@@ -287,57 +268,39 @@ __global__ void k_mc_mid(MCArgs A, int emit) {
   }
 }
 
-// Midpoint vertex created by the cube that owns edge (dir, ex, ey, ez), -1 if none.
-__device__ __forceinline__ int64_t midpoint_vertex(const MCArgs& A, const StructDev& S, int dir, int64_t ex, int64_t ey,
-                                                   int64_t ez) {
-  const int64_t NX = S.g.n[0], NY = S.g.n[1], NZ = S.g.n[2];
-  int64_t oi = ex, oj = ey, ok = ez;
-  int bit;
-  if (dir == NS_Y_DIR) { oi = ex - 1; ok = ez - 1; bit = 0; }
-  else if (dir == NS_X_DIR) { oj = ey - 1; ok = ez - 1; bit = 1; }
-  else { oi = ex - 1; oj = ey - 1; bit = 2; }
-  if (oi < 1 || oj < 1 || ok < 1 || oi > NX - 2 || oj > NY - 2 || ok > NZ - 2) return -1;
-  int64_t row = S.row_base + (ok - 1) * (NY - 2) + (oj - 1);
-  int64_t lo = A.row_act_off[row], hi = A.row_act_off[row + 1];
-  while (lo < hi) {
-    int64_t mid = (lo + hi) >> 1;
-    if (A.act_rec[mid].x < oi) lo = mid + 1;
-    else hi = mid;
+// One thread per vertex: the cubes that share its grid edge (x, y, z, axis) and the edge's number
+// in each of them; the vertex id goes into their slots, the smallest id of an edge winning.
+__global__ void k_mc_push(MCArgs A, int64_t v0, int64_t v1) {
+  for (int64_t v = v0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < v1; v += (int64_t)gridDim.x * blockDim.x) {
+    const int4 e = A.vkey[v];
+    const StructDev& S = A.B.s[A.vstruct[v]];
+    const GridDev& g = S.g;
+    // cube offsets and the edge's number in each cube: an x edge at (x, y, z) is edge 0 of cube
+    // (x, y, z), 2 of (x, y-1, z), 4 of (x, y, z-1) and 6 of (x, y-1, z-1); y and z edges alike
+    int t[4][4];
+    if (e.w == NS_X_DIR) {
+      const int u[4][4] = {{0, 0, 0, 0}, {0, -1, 0, 2}, {0, 0, -1, 4}, {0, -1, -1, 6}};
+      memcpy(t, u, sizeof t);
+    } else if (e.w == NS_Y_DIR) {
+      const int u[4][4] = {{0, 0, 0, 3}, {-1, 0, 0, 1}, {0, 0, -1, 7}, {-1, 0, -1, 5}};
+      memcpy(t, u, sizeof t);
+    } else {
+      const int u[4][4] = {{0, 0, 0, 8}, {-1, 0, 0, 9}, {0, -1, 0, 11}, {-1, -1, 0, 10}};
+      memcpy(t, u, sizeof t);
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int64_t i = e.x + t[q][0], j = e.y + t[q][1], k = e.z + t[q][2];
+      if (i < 1 || j < 1 || k < 1 || i > g.n[0] - 2 || j > g.n[1] - 2 || k > g.n[2] - 2) continue;
+      const int32_t a = A.cube_map[S.cube_base + cube_local(g, i, j, k)];
+      atomicMin((unsigned int*)(A.cube_vl + 12 * (int64_t)a + t[q][3]), (unsigned int)v);
+    }
   }
-  if (lo >= A.row_act_off[row + 1] || A.act_rec[lo].x != oi) return -1;
-  int mm = (A.act_rec[lo].w >> 8) & 7;
-  if (!(mm & (1 << bit))) return -1;
-  return A.act_mid[lo] + __popc(mm & ((1 << bit) - 1));
 }
 
-__device__ __forceinline__ int64_t edge_vertex(const MCArgs& A, const StructDev& S, int e, int64_t i, int64_t j,
-                                               int64_t k) {
-  // cube edge -> grid edge (dir, ex, ey, ez)
-  int dir;
-  int64_t x = i, y = j, z = k;
-  switch (e) {
-    case 0: dir = NS_X_DIR; break;
-    case 1: dir = NS_Y_DIR; x = i + 1; break;
-    case 2: dir = NS_X_DIR; y = j + 1; break;
-    case 3: dir = NS_Y_DIR; break;
-    case 4: dir = NS_X_DIR; z = k + 1; break;
-    case 5: dir = NS_Y_DIR; x = i + 1; z = k + 1; break;
-    case 6: dir = NS_X_DIR; y = j + 1; z = k + 1; break;
-    case 7: dir = NS_Y_DIR; z = k + 1; break;
-    case 8: dir = NS_Z_DIR; break;
-    case 9: dir = NS_Z_DIR; x = i + 1; break;
-    case 10: dir = NS_Z_DIR; x = i + 1; y = j + 1; break;
-    default: dir = NS_Z_DIR; y = j + 1; break;
-  }
-  int64_t v = analytic_vertex(A, S, dir, x, y, z);
-  if (v >= 0) return v;
-  return midpoint_vertex(A, S, dir, x, y, z);
-}
-
-
-// One thread per active cube.  Pass 0 finds the vertex of every cut edge, counts the triangles
-// and sums their areas (and, in gradient mode, their derivatives with respect to the analytic
-// vertices); pass 1 writes the triangles at their offsets from the stored vertex ids.
+// One thread per active cube, the vertex of every cut edge read from its slots.  Pass 0 counts the
+// triangles whose three edges have vertices; pass 1 writes them at their offsets and sums their
+// areas (and, in gradient mode, their derivatives with respect to the analytic vertices).
 __global__ void __launch_bounds__(128, 8) k_mc_tris(MCArgs A, int emit) {
   __shared__ int8_t s_tri[256][16];
   __shared__ uint16_t s_emask[256];
@@ -353,18 +316,9 @@ __global__ void __launch_bounds__(128, 8) k_mc_tris(MCArgs A, int emit) {
     int c = rec.w & 255;
     int64_t i = rec.x, j = rec.y, k = rec.z;
     const StructDev& S = A.B.s[rec_struct(rec.w)];
-    int em = s_emask[c];
-    int32_t* cv = A.cube_vl + 12 * a;
-    if (!emit) {
-      // the edge -> vertex searches run once; the emit pass reads their results
-      for (int e = 0; e < 12; e++) {
-        const int32_t v = (em >> e) & 1 ? (int32_t)edge_vertex(A, S, e, i, j, k) : -1;
-        vl[e * 128] = v;
-        cv[e] = v;
-      }
-    } else {
-      for (int e = 0; e < 12; e++) vl[e * 128] = cv[e];
-    }
+    (void)i; (void)j; (void)k; (void)S;
+    const int32_t* cv = A.cube_vl + 12 * a;
+    for (int e = 0; e < 12; e++) vl[e * 128] = cv[e];
     int cnt = 0;
     int64_t o = emit ? A.tri_off[a] : 0;
     double area = 0.0;
@@ -372,11 +326,14 @@ __global__ void __launch_bounds__(128, 8) k_mc_tris(MCArgs A, int emit) {
       const int e0 = s_tri[c][q], e1 = s_tri[c][q + 1], e2 = s_tri[c][q + 2];
       const int32_t v0 = vl[e0 * 128], v1 = vl[e1 * 128], v2 = vl[e2 * 128];
       if (v0 < 0 || v1 < 0 || v2 < 0) continue;
-      if (emit) {
-        A.tris[3 * (o + cnt) + 0] = (int32_t)v2;
-        A.tris[3 * (o + cnt) + 1] = (int32_t)v1;
-        A.tris[3 * (o + cnt) + 2] = (int32_t)v0;
-      } else {
+      if (!emit) {
+        cnt++;
+        continue;
+      }
+      A.tris[3 * (o + cnt) + 0] = (int32_t)v2;
+      A.tris[3 * (o + cnt) + 1] = (int32_t)v1;
+      A.tris[3 * (o + cnt) + 2] = (int32_t)v0;
+      {
         const double* P0 = A.vpos + 3 * (int64_t)v0;
         const double* P1 = A.vpos + 3 * (int64_t)v1;
         const double* P2 = A.vpos + 3 * (int64_t)v2;
@@ -415,10 +372,8 @@ __global__ void __launch_bounds__(128, 8) k_mc_tris(MCArgs A, int emit) {
       }
       cnt++;
     }
-    if (!emit) {
-      A.tri_cnt[a] = cnt;
-      A.cube_area[a] = area;
-    }
+    if (!emit) A.tri_cnt[a] = cnt;
+    else A.cube_area[a] = area;
   }
 }
 
@@ -497,6 +452,12 @@ cudaError_t launch_mc_mid(const MCArgs& A, int emit, cudaStream_t s) {
 cudaError_t launch_mc_tris(const MCArgs& A, int emit, cudaStream_t s) {
   if (A.n_active <= 0) return cudaSuccess;
   k_mc_tris<<<grid_for(A.n_active, 128), 128, 0, s>>>(A, emit);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mc_push(const MCArgs& A, int64_t v0, int64_t v1, cudaStream_t s) {
+  if (v1 <= v0) return cudaSuccess;
+  k_mc_push<<<grid_for(v1 - v0, 256), 256, 0, s>>>(A, v0, v1);
   return cudaGetLastError();
 }
 

@@ -20,6 +20,7 @@ struct VertArgs {
   const int64_t* surv_off;       // exclusive scan of surv_cnt
   double* vpos;                  // 3 per vertex
   int4* vkey;                    // ix, iy, iz, dir per vertex
+  int32_t* vstruct;              // structure of every vertex
   const int2* pair_pid;          // gradient mode: patches of the pair ends, else null
   int32_t* vpid;                 // gradient mode: patch of every analytic vertex
 };
@@ -32,6 +33,7 @@ struct MCArgs {
   int64_t n_analytic;
   double* vpos;
   int4* vkey;
+  int32_t* vstruct;              // structure of every vertex
   int64_t nrows;                 // cube rows, (NY-2)*(NZ-2) per structure
   const int4* row_chunks;        // structure, first local row, row count (consecutive rows)
   int64_t nchunks;
@@ -43,7 +45,8 @@ struct MCArgs {
   int32_t* act_mid;              // index of the first midpoint vertex of the cube
   int64_t n_active;
   int32_t* tri_cnt;
-  int32_t* cube_vl;              // 12 per active cube: vertex of each cut edge (-1 none), pass 0 -> 1
+  int32_t* cube_vl;              // 12 per active cube: vertex of each cut edge (-1 none)
+  int32_t* cube_map;             // dense per structure (cube_base): active index of every active cube
   const int64_t* tri_off;
   int32_t* tris;
   double* cube_area;
@@ -62,6 +65,9 @@ cudaError_t launch_vert(const VertArgs& A, int emit, cudaStream_t s);
 cudaError_t launch_mc_rows(const MCArgs& A, int emit, cudaStream_t s);
 cudaError_t launch_mc_mid(const MCArgs& A, int emit, cudaStream_t s);
 cudaError_t launch_mc_tris(const MCArgs& A, int emit, cudaStream_t s);
+// Every vertex in [v0, v1) writes its id into the cube_vl slots of the (up to four) active cubes
+// that share its grid edge; the smallest id of an edge wins (atomicMin).
+cudaError_t launch_mc_push(const MCArgs& A, int64_t v0, int64_t v1, cudaStream_t s);
 // d area / d patch parameters from the per-vertex derivatives (gradient mode).
 cudaError_t launch_grad_vert(const MCArgs& A, cudaStream_t s);
 

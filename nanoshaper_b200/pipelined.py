@@ -147,3 +147,178 @@ class PipelinedBatches:
     def close(self) -> None:
         for c in self.ctxs:
             c.close()
+
+
+class AtomsPipeline:
+    """Volume, area and their atom derivatives of every structure of an ensemble, starting from
+    the atoms: per step each structure's grid is built (buildGrid), its atoms jittered with the
+    process-wide generator in structure order (as one ConnollySurface::build per structure would),
+    its SES patches built on the host, and the chunks ray cast, triangulated and differentiated
+    on two contexts as in PipelinedBatches.  The host work overlaps the device work: structures are
+    built on a pool of host threads (one single-threaded patch build per structure), each chunk's
+    patch sets are exported straight into its pinned buffers, and a chunk goes to the GPU as soon
+    as it is complete while the pool builds the next."""
+
+    def __init__(self, atoms: list, probe: float = 1.4, scale: float = 2.0, perfil: float = 80.0, n_chunks: int = 8,
+                 device: int = 0, precision: str = "mixed", tuning: list[int] | None = None, threads: int = 0):
+        import os
+        if not atoms:
+            raise ValueError("empty ensemble")
+        self.atoms = [np.ascontiguousarray(a, np.float64) for a in atoms]
+        self.probe, self.scale, self.perfil = probe, scale, perfil
+        self.bounds = chunk_bounds(len(atoms), n_chunks)
+        self.prec = S.PRECISIONS[precision]
+        self.flags = N.STATUS | N.ACCURATE_TRIANGULATION | N.GRAD
+        self.threads = threads or (os.cpu_count() or 1)
+        self.ctxs = [S.Context(device), S.Context(device)]
+        self._upload_lock = threading.Lock()
+        if tuning is not None:
+            p = np.ascontiguousarray(tuning, np.int32)
+            for c in self.ctxs:
+                N.check(N.lib().nsg_set_tuning(c.handle, N.ptr(p), len(p)), "set tuning")
+        self._pinned: dict = {}
+        self.h2d_bytes = 0
+        self.d2h_bytes = 0
+        self.volumes = np.zeros(len(atoms))
+        self.areas = np.zeros(len(atoms))
+
+    def _pin(self, key, nbytes: int) -> torch.Tensor:
+        t = self._pinned.get(key)
+        if t is None or t.numel() < nbytes:
+            t = torch.empty(max(nbytes, 64), dtype=torch.uint8, pin_memory=True)
+            self._pinned[key] = t
+        return t
+
+    def _build_one(self, b: int, jittered: np.ndarray):
+        h = ctypes.c_void_p()
+        rc = N.lib().nsg_ses_build(N.ptr(jittered), len(jittered), self.probe, 1, ctypes.byref(h))
+        if rc not in (N.NSG_OK, -8):
+            N.check(rc, "SES patch construction")
+        n = ctypes.c_int64()
+        npool = ctypes.c_int64()
+        N.check(N.lib().nsg_patchset_info(h, ctypes.byref(n), ctypes.byref(npool), None), "patchset_info")
+        return h, n.value, npool.value
+
+    def _host_chunk(self, ci: int, pool, grids, jittered):
+        """Builds chunk ci's patch sets on the pool and exports them into its pinned buffers."""
+        lo, hi = int(self.bounds[ci]), int(self.bounds[ci + 1])
+        built = list(pool.map(lambda b: self._build_one(b, jittered[b]), range(lo, hi)))
+        m = hi - lo
+        patch_off = np.zeros(m + 1, np.int64)
+        pool_off = np.zeros(m + 1, np.int64)
+        atom_off = np.zeros(m + 1, np.int64)
+        patch_off[1:] = np.cumsum([x[1] for x in built])
+        pool_off[1:] = np.cumsum([x[2] for x in built])
+        atom_off[1:] = np.cumsum([len(jittered[b]) for b in range(lo, hi)])
+        npat, npool, nat = int(patch_off[-1]), int(pool_off[-1]), int(atom_off[-1])
+        pin = {"f64": self._pin((ci, "f64"), npat * 160), "i32": self._pin((ci, "i32"), npat * 16),
+               "pool": self._pin((ci, "pool"), max(npool, 1) * 32), "flag": self._pin((ci, "flag"), max(npool, 1)),
+               "atoms": self._pin((ci, "atoms"), nat * 32), "patch_atoms": self._pin((ci, "pa"), npat * 12),
+               "gvol": self._pin((ci, "gvol"), nat * 32), "garea": self._pin((ci, "garea"), nat * 32)}
+        L = N.lib()
+
+        def export(q: int) -> None:
+            h = built[q][0]
+            try:
+                po, qo, ao = int(patch_off[q]), int(pool_off[q]), int(atom_off[q])
+                N.check(L.nsg_patchset_export(h, pin["f64"].data_ptr() + po * 160, pin["i32"].data_ptr() + po * 16,
+                                              pin["pool"].data_ptr() + qo * 32, pin["flag"].data_ptr() + qo),
+                        "patchset_export")
+                N.check(L.nsg_patchset_atoms(h, pin["patch_atoms"].data_ptr() + po * 12), "patchset_atoms")
+                a = jittered[lo + q]
+                ctypes.memmove(pin["atoms"].data_ptr() + ao * 32, a.ctypes.data, a.nbytes)
+            finally:
+                L.nsg_patchset_free(h)
+
+        list(pool.map(export, range(m)))
+        if npool == 0:
+            pin["flag"].zero_()
+        g = (N.NsGrid * m)(*grids[lo:hi])
+        return dict(lo=lo, hi=hi, patch_off=patch_off, pool_off=pool_off, atom_off=atom_off, pin=pin, grids=g,
+                    h2d=npat * 188 + max(npool, 1) * 33 + nat * 32, d2h=16 * m + 64 * nat)
+
+    def _gpu_chunk(self, c, ch) -> None:
+        L = N.lib()
+        pin = ch["pin"]
+        m = ch["hi"] - ch["lo"]
+        with self._upload_lock:
+            N.check(L.nsg_set_batch(c, m, ch["grids"]), "set_batch")
+            N.check(L.nsg_upload_batch(c, N.ptr(ch["patch_off"]), pin["f64"].data_ptr(), pin["i32"].data_ptr(),
+                                       N.ptr(ch["pool_off"]), pin["pool"].data_ptr(), pin["flag"].data_ptr(),
+                                       self.probe), "upload_batch")
+            N.check(L.nsg_upload_atoms(c, N.ptr(ch["atom_off"]), pin["atoms"].data_ptr(), pin["patch_atoms"].data_ptr()),
+                    "upload atoms")
+        v = ctypes.c_double()
+        N.check(L.nsg_raycast(c, self.flags, self.prec, ctypes.byref(v)), "raycast")
+        a = ctypes.c_double()
+        nv = ctypes.c_int64()
+        nt = ctypes.c_int64()
+        N.check(L.nsg_triangulate(c, ctypes.byref(a), ctypes.byref(nv), ctypes.byref(nt)), "triangulate")
+        rc = L.nsg_atom_grads(c, pin["gvol"].data_ptr(), pin["garea"].data_ptr())
+        if rc not in (N.NSG_OK, -8):
+            N.check(rc, "atom gradients")
+        vols = np.zeros(m)
+        areas = np.zeros(m)
+        N.check(L.nsg_batch_results(c, N.ptr(vols), N.ptr(areas)), "batch results")
+        self.volumes[ch["lo"]:ch["hi"]] = vols
+        self.areas[ch["lo"]:ch["hi"]] = areas
+
+    def run(self) -> tuple[np.ndarray, np.ndarray]:
+        """One pass over the ensemble from its atoms; returns the per-structure volumes and areas."""
+        import queue
+        from concurrent.futures import ThreadPoolExecutor
+        L = N.lib()
+        # grids from the loaded atoms, then the jitter in structure order (process-wide generator)
+        grids = []
+        jittered = []
+        S.reset_seed()
+        for a in self.atoms:
+            g = N.NsGrid()
+            N.check(L.nsg_grid_build(N.ptr(a), len(a), self.scale, self.perfil, ctypes.byref(g)), "buildGrid")
+            grids.append(g)
+            j = a.copy()
+            N.check(L.nsg_jitter_atoms(N.ptr(j), len(j), S.RAND_DISPLACEMENT, ctypes.byref(S._seed)), "jitter")
+            jittered.append(j)
+        ready: "queue.Queue" = queue.Queue()
+        errors: list[BaseException] = []
+        n_chunks = len(self.bounds) - 1
+        h2d = [0]
+        d2h = [0]
+
+        def producer() -> None:
+            try:
+                with ThreadPoolExecutor(self.threads) as pool:
+                    for ci in range(n_chunks):
+                        ch = self._host_chunk(ci, pool, grids, jittered)
+                        h2d[0] += ch["h2d"]
+                        d2h[0] += ch["d2h"]
+                        ready.put(ch)
+            except BaseException as e:
+                errors.append(e)
+            finally:
+                for _ in range(2):
+                    ready.put(None)
+
+        def worker(w: int) -> None:
+            try:
+                while True:
+                    ch = ready.get()
+                    if ch is None:
+                        return
+                    self._gpu_chunk(self.ctxs[w].handle, ch)
+            except BaseException as e:
+                errors.append(e)
+
+        threads = [threading.Thread(target=producer)] + [threading.Thread(target=worker, args=(w,)) for w in range(2)]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        if errors:
+            raise errors[0]
+        self.h2d_bytes, self.d2h_bytes = h2d[0], d2h[0]
+        return self.volumes.copy(), self.areas.copy()
+
+    def close(self) -> None:
+        for c in self.ctxs:
+            c.close()

@@ -117,3 +117,30 @@ def test_pipelined_batches_match_one_batch(native_lib):
         assert np.abs(gv - rv).max() <= 1e-10 * np.abs(gv).max()
         assert np.abs(ga - ra).max() <= 1e-10 * np.abs(ga).max()
     runner.close()
+
+
+def test_atoms_pipeline_matches_batch(native_lib):
+    """AtomsPipeline (grids, jitter and patch builds on host threads, overlapped with the device)
+    gives the per-structure volumes and areas of the same ensemble built structure by structure
+    and run as one batch."""
+    from nanoshaper_b200.pipelined import AtomsPipeline
+    atoms = generator.ensemble(2, 4, 300, 900, 0.3, 3)
+    nb.reset_seed()
+    surfs = []
+    for a in atoms:
+        ds = nb.DelPhiShared(a, 2.0, 80.0)
+        cf = nb.ConfigFile(text="Surface = ses\nProbe_Radius = 1.4\nAccurate_Triangulation = true\n"
+                                "Gpu_Precision = mixed\n")
+        sf = nb.surfaceFactory().create(cf, ds)
+        sf.build()
+        surfs.append(sf)
+    batch = nb.SurfaceBatch(surfs, precision="mixed")
+    vol = batch.getSurf(grad=True)
+    area = batch.triangulateSurface()
+    batch.close()
+    ap = AtomsPipeline(atoms, n_chunks=3, precision="mixed", threads=4)
+    for _ in range(2):
+        v2, a2 = ap.run()
+        np.testing.assert_allclose(v2, vol, rtol=1e-12, atol=0)
+        np.testing.assert_allclose(a2, area, rtol=1e-12, atol=0)
+    ap.close()
