@@ -32,6 +32,7 @@ extern "C" {
 #define NSG_RAYCAST_TRIANGULATION 2     /* accurate-triangulation rays: Accurate_Triangulation = true */
 #define NSG_RAYCAST_KEEP_HITS 16        /* keep per-ray sorted hits for nsg_download_hits */
 #define NSG_RAYCAST_GRAD 32             /* adjoint: d volume (and d area of the next nsg_triangulate) / d patch */
+#define NSG_RAYCAST_NORMALS 64          /* keep the hits' patches for analytic vertex normals (Compute_Vertex_Normals) */
 
 /* Gradient slots per patch (nsg_patch_grads): point (cx, cy, cz, r), facet (px, py, pz),
  * edge (tcx, tcy, tcz, ux, uy, uz, R); unused slots are 0. */
@@ -231,6 +232,16 @@ int nsg_cavity_order(int32_t n_regions, const uint32_t* desc_key, int32_t* label
 int nsg_triangulate(nsg_ctx* ctx, double* area, int64_t* n_vertices, int64_t* n_triangles);
 
 /* ---- results into caller-owned host buffers ---- */
+/* Vertex normals of the last nsg_triangulate (after nsg_raycast with NSG_RAYCAST_NORMALS or
+ * NSG_RAYCAST_GRAD), 3 doubles per vertex: analytic vertices get their patch's normal
+ * (ConnollySurface::getNormal, src/ConnollySurface.cpp:5736-5819; the skin quadric's gradient,
+ * src/SkinSurface.cpp:3684-3712), the others the triangle average of approximateNormals
+ * (src/Surface.cpp:10420-10460, 10588-10735). */
+int nsg_vertex_normals(nsg_ctx* ctx, double* normals);
+/* Host: the vertices whose normal is (0, 0, 0) get the triangle-averaged normal (approximateNormals
+ * for the listed vertices, src/Surface.cpp:10660-10735). */
+int nsg_fill_zero_normals(const double* vertices, int64_t n_vertices, const int32_t* triangles, int64_t n_triangles,
+                          double* normals);
 /* Status map, flat int32 k*ny*nx + j*nx + i (read3DVector layout, src/tools.h:549-575). */
 int nsg_download_status(nsg_ctx* ctx, int32_t* dst);
 /* 32x-packed insideness bits, bit = 1 outside (src/tools.h:1324-1414); ceil(nx/32)*ny*nz words. */

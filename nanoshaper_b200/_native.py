@@ -31,6 +31,7 @@ STATUS = 1
 ACCURATE_TRIANGULATION = 2
 KEEP_HITS = 16
 GRAD = 32
+NORMALS = 64
 
 
 class NsGrid(ctypes.Structure):
@@ -100,6 +101,8 @@ _SIGNATURES = {
     "nsg_blobby_build": ([_P, _P, _I64, _D, _INT], _INT),
     "nsg_blobby_mesh": ([_P, ctypes.POINTER(_I64), ctypes.POINTER(_I64), _P, _P], _INT),
     "nsg_blobby_atom_grads": ([_P, _P, _P], _INT),
+    "nsg_vertex_normals": ([_P, _P], _INT),
+    "nsg_fill_zero_normals": ([_P, _I64, _P, _I64, _P], _INT),
     "nsg_patchset_export": ([_P, _P, _P, _P, _P], _INT),
     "nsg_patchset_free": ([_P], None),
     "nsg_patchset_atoms": ([_P, _P], _INT),

@@ -110,7 +110,7 @@ struct nsg_ctx {
   DevBuf d_atoms, d_patch_atoms, d_gatoms_vol, d_gatoms_area, d_bad, d_patch_off, d_pool_off, d_atom_off;
   int64_t n_atoms = 0;
   bool have_atoms = false;
-  bool grad_mode = false, have_gvol = false, have_garea = false;
+  bool grad_mode = false, have_gvol = false, have_garea = false, have_pids = false;
   int64_t cand_cap = 0, def_cap = 0;
   // trace outputs
   DevBuf status, bits, vol_ray[4];
@@ -960,6 +960,8 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
   const bool do_mc = flags & 2;
   const bool keep_hits = flags & 16;
   const bool grad = flags & 32;
+  // the patches of the hits are kept for the gradients and for the analytic vertex normals
+  const bool pids = grad || (flags & 64);
   if (!c->kind_mask_valid) {
     // which patch kinds are present (SES and / or skin cells) selects the intersection kernels
     CK(c->kind_mask_d.ensure(sizeof(int)));
@@ -1031,7 +1033,7 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
                               : std::max(std::max(c->rays_tot[0], c->rays_tot[1]), std::max(c->rays_tot[2], c->rays_tot[3]));
       CK(c->hit_t[sl].ensure((size_t)nr * nsg::kHitCap * sizeof(double)));
       CK(c->hit_cnt[sl].ensure(nr * sizeof(int32_t)));
-      if (grad) CK(c->hit_pid[sl].ensure((size_t)nr * nsg::kHitCap * sizeof(int32_t)));
+      if (pids) CK(c->hit_pid[sl].ensure((size_t)nr * nsg::kHitCap * sizeof(int32_t)));
     }
     if (grad) CK(c->gvol.ensure(std::max<int64_t>(c->np, 1) * NS_GRAD_PER_PATCH * sizeof(double)));
     if (conc) {
@@ -1046,7 +1048,7 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
   const int ovf_cap = 1 << 16;
   for (int attempt = 0; attempt < 4; attempt++) {
     if (do_mc) CK(c->pairs.ensure(c->pair_cap * 2 * sizeof(double)));
-    if (do_mc && grad) CK(c->pair_pid.ensure(c->pair_cap * sizeof(int2)));
+    if (do_mc && pids) CK(c->pair_pid.ensure(c->pair_cap * sizeof(int2)));
     if (grad)
       CK(cudaMemsetAsync(c->gvol.p, 0, std::max<int64_t>(c->np, 1) * NS_GRAD_PER_PATCH * sizeof(double), c->stream));
     if (precision == NSG_PRECISION_MIXED) c->def_cap = std::max<int64_t>(c->def_cap, c->cand_cap / 16 + (1 << 16));
@@ -1112,9 +1114,9 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
       o.ovf_count = ovf_count + s;
       o.error_flag = c->err.as<int32_t>();
       o.counters = c->profile ? c->counters.as<unsigned long long>() : nullptr;
+      if (pids) o.pair_pid = c->pair_pid.as<int2>();
       if (grad) {
         o.gvol = c->gvol.as<double>();
-        o.pair_pid = c->pair_pid.as<int2>();
         o.grad_scale = 1.0 / (double)((do_status ? 1 : 0) + (do_mc ? 3 : 0));
       }
       if (keep_hits) {
@@ -1132,7 +1134,7 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
       nsg::CandOut co{c->cand_sph[sl].as<int2>(), c->cand_tor[sl].as<int2>(), c->cand_cap, cur + 8 + 2 * s,
                       c->def_sph[sl].as<int2>(), c->def_tor[sl].as<int2>(), c->def_cap, cur + 16 + 2 * s};
       nsg::HitStore hs{c->hit_t[sl].as<double>(), c->hit_cnt[sl].as<int32_t>(), nr,
-                       grad ? c->hit_pid[sl].as<int32_t>() : nullptr};
+                       pids ? c->hit_pid[sl].as<int32_t>() : nullptr};
       CK(cudaMemsetAsync(c->hit_cnt[sl].p, 0, nr * sizeof(int32_t), st));
       c->launches += precision == NSG_PRECISION_MIXED ? 6 : 4;
       cudaEvent_t* ev = nullptr;
@@ -1177,10 +1179,10 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
         tiles_built[panel] = true;
       }
       CK(c->ovf_scratch.ensure((size_t)n * nsg::kOverflowCap * sizeof(double)));
-      if (grad) CK(c->ovf_pscratch.ensure((size_t)n * nsg::kOverflowCap * sizeof(int32_t)));
+      if (pids) CK(c->ovf_pscratch.ensure((size_t)n * nsg::kOverflowCap * sizeof(int32_t)));
       LAUNCH(nsg::launch_trace_overflow(P, B, s, c->tile_off[panel].as<int64_t>(), c->tile_list[panel].as<int32_t>(),
                                         outs[s], n, c->ovf_scratch.as<double>(),
-                                        grad ? c->ovf_pscratch.as<int32_t>() : nullptr, precision, c->stream));
+                                        pids ? c->ovf_pscratch.as<int32_t>() : nullptr, precision, c->stream));
       CK(cudaStreamSynchronize(c->stream));
     }
     stage_end(c, kStageOverflow);
@@ -1239,6 +1241,7 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
   }
   c->status_dense = false;
   c->have_gvol = grad;
+  c->have_pids = pids && do_mc;
   c->have_status = do_status;
   c->have_bits = do_mc;
   c->n_vert = c->n_tri = 0;
@@ -1395,7 +1398,7 @@ int nsg_triangulate(nsg_ctx* c, double* area_out, int64_t* nverts, int64_t* ntri
   CK(c->vstruct.ensure(std::max<int64_t>(n_an, 1) * sizeof(int32_t)));
   V.vstruct = c->vstruct.as<int32_t>();
   const bool grad = c->grad_mode && c->have_gvol;
-  if (grad) {
+  if (c->have_pids) {
     CK(c->vpid.ensure(std::max<int64_t>(n_an, 1) * sizeof(int32_t)));
     V.pair_pid = c->pair_pid.as<int2>();
     V.vpid = c->vpid.as<int32_t>();
@@ -1510,6 +1513,33 @@ int nsg_triangulate(nsg_ctx* c, double* area_out, int64_t* nverts, int64_t* ntri
   if (nverts) *nverts = n_v;
   if (ntris) *ntris = n_tri;
   return NSG_OK;
+}
+
+// Vertex normals of the last triangulation (Compute_Vertex_Normals): for a surface with analytic
+// normals the normal of each analytic vertex's patch at the vertex (ConnollySurface::getNormal,
+// src/ConnollySurface.cpp:5736-5819; the skin quadric's gradient, src/SkinSurface.cpp:3684-3712),
+// the others (midpoint vertices, mesh surfaces) by triangle averaging as approximateNormals does
+// for the vertices whose normal is zero (src/Surface.cpp:10420-10460, 10588-10735).
+int nsg_vertex_normals(nsg_ctx* c, double* normals) {
+  if (!c || !normals) return NSG_ERR_ARG;
+  if (!c->have_pids) return fail(NSG_ERR_STATE, "ray cast with NSG_RAYCAST_NORMALS (or NSG_RAYCAST_GRAD) first");
+  const int64_t nv = c->n_vert, nt = c->n_tri;
+  if (nv == 0) return NSG_OK;
+  CK(cudaSetDevice(c->device));
+  DevBuf dn;
+  CK(dn.ensure(nv * 3 * sizeof(double)));
+  CK(cudaMemsetAsync(dn.p, 0, nv * 3 * sizeof(double), c->stream));
+  const nsg::PatchDev P = patch_dev(c);
+  LAUNCH(nsg::launch_vertex_normals(c->vpos.as<double>(), c->vpid.as<int32_t>(), c->n_analytic, P.f64, P.i32, P.probe,
+                                    dn.as<double>(), c->stream));
+  std::vector<double> verts(nv * 3);
+  std::vector<int32_t> tris(std::max<int64_t>(nt, 1) * 3);
+  CK(cudaMemcpyAsync(normals, dn.p, nv * 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(verts.data(), c->vpos.p, nv * 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (nt) CK(cudaMemcpyAsync(tris.data(), c->tris.p, nt * 3 * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  dn.release();
+  return nsg_fill_zero_normals(verts.data(), nv, tris.data(), nt, normals);
 }
 
 int nsg_download_status(nsg_ctx* c, int32_t* dst) {

@@ -180,6 +180,22 @@ int nsg_mesh_normals(const double* vertices, int64_t n_vertices, const int32_t* 
   return NSG_OK;
 }
 
+// The vertices whose normal is (0, 0, 0) get the triangle-averaged normal (approximateNormals for
+// the listed vertices, src/Surface.cpp:10420-10460, 10660-10735); the others keep theirs.
+int nsg_fill_zero_normals(const double* vertices, int64_t n_vertices, const int32_t* triangles, int64_t n_triangles,
+                          double* normals) {
+  if (n_vertices < 0 || (n_vertices && (!vertices || !normals))) return NSG_ERR_ARG;
+  std::vector<double> avg(3 * (size_t)n_vertices);
+  int rc = nsg_mesh_normals(vertices, n_vertices, triangles, n_triangles, avg.data());
+  if (rc) return rc;
+  for (int64_t v = 0; v < n_vertices; v++) {
+    double* nv = normals + 3 * v;
+    if (nv[0] == 0 && nv[1] == 0 && nv[2] == 0)
+      for (int q = 0; q < 3; q++) nv[q] = avg[3 * v + q];
+  }
+  return NSG_OK;
+}
+
 // Nearest atom of every vertex, as vdwAccessible picks it (src/Surface.cpp:16663-16715): the atom of
 // least power distance |p - c|^2 - r^2 (ties: the lower index).  The reference searches the atoms
 // binned in the grid cells around the vertex; here a uniform grid of cells is searched in growing

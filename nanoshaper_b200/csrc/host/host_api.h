@@ -48,6 +48,11 @@ int nsg_write_cavities(const char* cavities_path, const char* sizes_path, const 
 int nsg_write_mesh(const char* root, int format, const double* vertices, int64_t n_vertices, const int32_t* triangles,
                    int64_t n_triangles, int revert);
 
+int nsg_mesh_normals(const double* vertices, int64_t n_vertices, const int32_t* triangles, int64_t n_triangles,
+                     double* normals);
+int nsg_fill_zero_normals(const double* vertices, int64_t n_vertices, const int32_t* triangles, int64_t n_triangles,
+                          double* normals);
+
 int nsg_ses_chain_grad(const double* atoms_xyzr, int64_t n_atoms, double probe, int64_t n_patches,
                        const int32_t* i32, const double* f64, const int32_t* patch_atoms, const double* gpatch,
                        double* grad_atoms);

@@ -404,6 +404,47 @@ __global__ void k_grad_vert(MCArgs A) {
   }
 }
 
+// The patch normal at a vertex: ConnollySurface::getNormal (src/ConnollySurface.cpp:5736-5819) for
+// atom spheres (y - c) / r, probe spheres (c - y) / probe and tori (getNormalToTorus, with the
+// frame's transpose for Rot); for skin cells the quadric's gradient times 2 (-2 for reduced
+// tetrahedra), as SkinSurface::getPatchIntersectionData stores it (src/SkinSurface.cpp:3684-3712).
+__global__ void k_vertex_normals(const double* __restrict__ vpos, const int32_t* __restrict__ vpid, int64_t n,
+                                 const double* __restrict__ f64, const int32_t* __restrict__ i32, double probe,
+                                 double* out) {
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t pid = vpid[v];
+    if (pid < 0) continue;
+    const double* f = f64 + (int64_t)NS_PATCH_F64 * pid;
+    const int kind = i32[NS_PATCH_I32 * pid];
+    const double y[3] = {vpos[3 * v], vpos[3 * v + 1], vpos[3 * v + 2]};
+    double nrm[3] = {0.0, 0.0, 0.0};
+    if (kind == NS_FACE_REG || kind == NS_FACE_SING) {
+      for (int d = 0; d < 3; d++) nrm[d] = (f[d] - y[d]) / probe;
+    } else if (kind == NS_POINT) {
+      for (int d = 0; d < 3; d++) nrm[d] = (y[d] - f[d]) / f[3];
+    } else if (kind == NS_EDGE_REG || kind == NS_EDGE_SING) {
+      const double* inv = f + 9;
+      const double t[3] = {y[0] - f[4], y[1] - f[5], y[2] - f[6]};
+      double C[3];
+      for (int i = 0; i < 3; i++) C[i] = inv[3 * i] * t[0] + inv[3 * i + 1] * t[1] + inv[3 * i + 2] * t[2];
+      double dd = C[0] * C[0] + C[1] * C[1];
+      const double rm1 = f[7] / sqrt(dd) - 1.;
+      dd = sqrt(dd * rm1 * rm1 + C[2] * C[2]);
+      C[0] *= rm1 / dd;
+      C[1] *= rm1 / dd;
+      C[2] /= -dd;
+      for (int i = 0; i < 3; i++) nrm[i] = inv[i] * C[0] + inv[3 + i] * C[1] + inv[6 + i] * C[2];
+    } else if (ns_is_skin(kind)) {
+      const double* Q = f + NS_SKIN_Q;
+      const double sg = kind == NS_SKIN_TETRA ? -2.0 : 2.0;
+      nrm[0] = sg * (Q[0] * y[0] + Q[4] * y[1] + Q[7] * y[2] + Q[9]);
+      nrm[1] = sg * (Q[4] * y[0] + Q[1] * y[1] + Q[5] * y[2] + Q[8]);
+      nrm[2] = sg * (Q[7] * y[0] + Q[5] * y[1] + Q[2] * y[2] + Q[6]);
+    }
+    for (int d = 0; d < 3; d++) out[3 * v + d] = nrm[d];
+  }
+}
+
 int grid_for(int64_t n, int threads) {
   int64_t b = (n + threads - 1) / threads;
   const int64_t cap = (int64_t)sm_count() * 32;
@@ -452,6 +493,13 @@ cudaError_t launch_mc_mid(const MCArgs& A, int emit, cudaStream_t s) {
 cudaError_t launch_mc_tris(const MCArgs& A, int emit, cudaStream_t s) {
   if (A.n_active <= 0) return cudaSuccess;
   k_mc_tris<<<grid_for(A.n_active, 128), 128, 0, s>>>(A, emit);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_vertex_normals(const double* vpos, const int32_t* vpid, int64_t n_analytic, const double* f64,
+                                  const int32_t* i32, double probe, double* normals, cudaStream_t s) {
+  if (n_analytic <= 0) return cudaSuccess;
+  k_vertex_normals<<<grid_for(n_analytic, 256), 256, 0, s>>>(vpos, vpid, n_analytic, f64, i32, probe, normals);
   return cudaGetLastError();
 }
 

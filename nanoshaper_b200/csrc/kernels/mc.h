@@ -68,6 +68,10 @@ cudaError_t launch_mc_tris(const MCArgs& A, int emit, cudaStream_t s);
 // Every vertex in [v0, v1) writes its id into the cube_vl slots of the (up to four) active cubes
 // that share its grid edge; the smallest id of an edge wins (atomicMin).
 cudaError_t launch_mc_push(const MCArgs& A, int64_t v0, int64_t v1, cudaStream_t s);
+// Analytic normal of every analytic vertex v < n_analytic from its patch vpid[v] (zero for patch
+// kinds without one, e.g. mesh triangles); 3 doubles per vertex.
+cudaError_t launch_vertex_normals(const double* vpos, const int32_t* vpid, int64_t n_analytic, const double* f64,
+                                  const int32_t* i32, double probe, double* normals, cudaStream_t s);
 // d area / d patch parameters from the per-vertex derivatives (gradient mode).
 cudaError_t launch_grad_vert(const MCArgs& A, cudaStream_t s);
 

@@ -634,7 +634,7 @@ __global__ void __launch_bounds__(kTraceThreads, 6) k_fill(TraceCtx C, HitStore 
   double vol = 0.0;
   int np = 0;
   const auto slot_pid = [&](uint8_t sl) { return hs.pid[(int64_t)sl * hs.nrays + rid]; };
-  if (kGrad) {
+  if (kGrad && C.out.gvol) {
     // d volume / d patch parameters, interval end by interval end (the pairing rule of
     // make_pairs), summed over runs of lanes on the same patch before the atomics
     const double W = S.A * C.out.grad_scale;
@@ -697,6 +697,9 @@ __global__ void __launch_bounds__(kTraceThreads, 6) k_fill(TraceCtx C, HitStore 
         for (int c3 = 0; c3 < NS_GRAD_PER_PATCH; c3++) gk[c3] = 0.0;
       warp_add_grad(pid, gk, C.out.gvol);
     }
+  }
+  if (kGrad) {
+    // the hits' patches follow their pairs (gradients, analytic normals)
     if (valid && !ovf)
       np = make_pairs(col, kThreads, nh, pa_vc, dirl, g.mn[rs.vc], g.scale, mc, &vol, pcol, (GradCtx*)nullptr,
                       slot_pid);
@@ -912,7 +915,7 @@ __global__ void k_trace_overflow(TraceCtx C, const int64_t* __restrict__ tile_of
   gc.x[rs.vc] = 0.0;
   gc.vc = rs.vc;
   gc.gvol = C.out.gvol;
-  int np = make_pairs(col, 1, nh, pa_vc, dirl, g.mn[rs.vc], g.scale, mc, &vol, pcol, pcol ? &gc : nullptr);
+  int np = make_pairs(col, 1, nh, pa_vc, dirl, g.mn[rs.vc], g.scale, mc, &vol, pcol, (pcol && gc.gvol) ? &gc : nullptr);
   C.out.vol_ray[rid] = vol;
   const int64_t NX = g.n[0], NY = g.n[1];
   if (!mc) {
@@ -1018,7 +1021,7 @@ cudaError_t launch_trace(const PatchDev& P, const BatchDev& B, int set, int64_t 
   else if (panel == 1) launch_isect<1>(C, co, hs, precision, tp, s);
   else launch_isect<2>(C, co, hs, precision, tp, s);
   if (ev) cudaEventRecord(ev[2], s);
-  if (out.gvol) k_fill<true><<<(unsigned)ntiles, kTraceThreads, 0, s>>>(C, hs);
+  if (hs.pid) k_fill<true><<<(unsigned)ntiles, kTraceThreads, 0, s>>>(C, hs);
   else k_fill<false><<<(unsigned)ntiles, kTraceThreads, 0, s>>>(C, hs);
   if (ev) cudaEventRecord(ev[3], s);
   return cudaGetLastError();

@@ -384,12 +384,15 @@ class Surface:
             flags |= N.KEEP_HITS
         if grad:
             flags |= N.GRAD
+        if self.computeNormals and self.providesAnalyticalNormals and self.accurateTriangulation:
+            flags |= N.NORMALS
         prec = PRECISIONS.get(self.precision)
         if prec is None:
             raise ValueError(f"unknown Gpu_Precision {self.precision}")
         vol = ctypes.c_double()
         N.check(N.lib().nsg_raycast(c, flags, prec, ctypes.byref(vol)), "ray casting")
         self.volume = vol.value
+        self._analytic_normals = bool(flags & (N.NORMALS | N.GRAD))
         if fill:
             if not self.delphi.buildStatus:
                 raise RuntimeError("Cannot do cavity detection without a status map (Build_status_map = true)")
@@ -449,6 +452,22 @@ class Surface:
         N.check(N.lib().nsg_vertex_atoms(N.ptr(v), len(v), N.ptr(a), len(a), N.ptr(out)), "vertex atoms")
         return out
 
+    # surfaces whose patches give a normal at every hit (the reference's providesAnalyticalNormals)
+    providesAnalyticalNormals = True
+
+    def vertexNormals(self) -> np.ndarray:
+        """Vertex normals of the last triangulation, as the reference outputs them with
+        Compute_Vertex_Normals: the patch normal at each analytic vertex and the triangle average for
+        the others (nsg_vertex_normals); by triangle averaging alone when the surface has no analytic
+        normals or the ray cast did not keep its hits' patches."""
+        if self.vertices is None:
+            raise RuntimeError("no mesh: call triangulateSurface() first")
+        if not (self.providesAnalyticalNormals and getattr(self, "_analytic_normals", False)):
+            return self.approximateNormals()
+        out = np.zeros((len(self.vertices), 3))
+        N.check(N.lib().nsg_vertex_normals(self._context().handle, N.ptr(out)), "vertex normals")
+        return out
+
     def approximateNormals(self) -> np.ndarray:
         """Vertex normals of the last triangulation by triangle averaging (the reference's
         approximateNormals for surfaces without analytic normals, src/Surface.cpp:10588-10660);
@@ -473,7 +492,7 @@ class Surface:
         t = np.ascontiguousarray(self.triangles, np.int32)
         if name in self.ATTR_MESH_FORMATS:
             fmt = self.ATTR_MESH_FORMATS[name]
-            nrm = np.ascontiguousarray(self.approximateNormals(), np.float64) if fmt != 2 else None
+            nrm = np.ascontiguousarray(self.vertexNormals(), np.float64) if fmt != 2 else None
             ato = self.vertexAtoms() if fmt >= 2 else None
             N.check(N.lib().nsg_write_mesh_attrs(str(fileName).encode(), fmt, N.ptr(v),
                                                  None if nrm is None else N.ptr(nrm),
@@ -600,6 +619,7 @@ class BlobbySurface(Surface):
 
     name = "blobby"
     DEFAULT_BLOBBYNESS = -2.5
+    providesAnalyticalNormals = False
 
     def __init__(self, cf: ConfigFile | None = None, delphi: DelPhiShared | None = None, device: int = 0):
         super().__init__(cf, delphi, device)

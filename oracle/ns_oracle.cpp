@@ -324,6 +324,7 @@ bool feasible(const Patches& P, int64_t it, const double* p) {
 struct Hit {
   int64_t pixel;
   double t;
+  int32_t patch;
 };
 
 struct Oracle {
@@ -338,6 +339,7 @@ struct Oracle {
   // products
   std::vector<int64_t> pix_off;  // pixel -> first hit
   std::vector<double> pix_t;
+  std::vector<int32_t> pix_pid;  // patch of every hit
   std::vector<int32_t> status;
   std::vector<uint32_t> bits;
   double volPanel[3] = {0, 0, 0};
@@ -345,6 +347,9 @@ struct Oracle {
   double volume = 0;
   std::vector<double> vert;        // analytic vertices before assembly: x y z
   std::vector<int32_t> vert_edge;  // ix iy iz dir
+  std::vector<int32_t> vert_pid;   // patch of every analytic vertex
+  std::vector<int32_t> vpid;       // patch of every assembled analytic vertex
+  std::vector<double> normals;     // vertex normals (Compute_Vertex_Normals)
   std::vector<double> vlist;       // assembled vertex list
   std::vector<int32_t> vkey;       // edge of every assembled vertex (ix iy iz dir)
   std::vector<int32_t> tris;
@@ -424,7 +429,7 @@ struct Oracle {
             double tt;
             if (ray_triangle(o, dir, fr, fr + 3, fr + 6, &tt)) {
               int64_t pid = (n * NMAX + m) * numPanels + (panels[0] * phase + panel);
-              out.push_back({pid, tt});
+              out.push_back({pid, tt, (int32_t)it});
             }
             continue;
           }
@@ -435,7 +440,7 @@ struct Oracle {
             ip[vc] += t[i];
             if (!feasible_skin(P, it, ip)) continue;
             int64_t pid = (n * NMAX + m) * numPanels + (panels[0] * phase + panel);
-            out.push_back({pid, t[i] / ray_dir});
+            out.push_back({pid, t[i] / ray_dir, (int32_t)it});
           }
         }
       }
@@ -502,7 +507,7 @@ struct Oracle {
             ip[vc] += t[i] * ray_dir;
             if (!feasible(P, it, ip)) continue;
             int64_t pid = (n * NMAX + m) * numPanels + (panels[0] * phase + panel);
-            out.push_back({pid, t[i]});
+            out.push_back({pid, t[i], (int32_t)it});
           }
         }
       }
@@ -544,11 +549,27 @@ struct Oracle {
     for (int64_t i = 0; i < npix; i++) pix_off[i + 1] += pix_off[i];
     n_hits = pix_off[npix];
     pix_t.resize(n_hits);
+    pix_pid.resize(n_hits);
     std::vector<int64_t> fill(pix_off.begin(), pix_off.end() - 1);
     for (auto& v : per)
-      for (auto& h : v) pix_t[fill[h.pixel]++] = h.t;
-    for (int64_t i = 0; i < npix; i++)
-      std::sort(pix_t.begin() + pix_off[i], pix_t.begin() + pix_off[i + 1]);
+      for (auto& h : v) {
+        pix_pid[fill[h.pixel]] = h.patch;
+        pix_t[fill[h.pixel]++] = h.t;
+      }
+    // per pixel by t (the patch of each hit follows it; equal t keep their patch order)
+    std::vector<std::pair<double, int32_t>> tmp;
+    for (int64_t i = 0; i < npix; i++) {
+      const int64_t a = pix_off[i], b = pix_off[i + 1];
+      if (b - a < 2) continue;
+      tmp.clear();
+      for (int64_t q = a; q < b; q++) tmp.push_back({pix_t[q], pix_pid[q]});
+      std::stable_sort(tmp.begin(), tmp.end(), [](const std::pair<double, int32_t>& x,
+                                                  const std::pair<double, int32_t>& y) { return x.first < y.first; });
+      for (int64_t q = a; q < b; q++) {
+        pix_t[q] = tmp[q - a].first;
+        pix_pid[q] = tmp[q - a].second;
+      }
+    }
   }
 
   // 32x compressed bit grid accessors (src/tools.h:1364-1413); bit = 1 means outside.
@@ -668,8 +689,10 @@ struct Oracle {
           if (flags & 8) {  // analytic vertices are kept only for the triangulation
             vert.insert(vert.end(), v1, v1 + 3);
             vert_edge.insert(vert_edge.end(), e1, e1 + 4);
+            vert_pid.push_back(pix_pid[q.first]);
             vert.insert(vert.end(), v2, v2 + 3);
             vert_edge.insert(vert_edge.end(), e2, e2 + 4);
+            vert_pid.push_back(pix_pid[q.second]);
           }
         }
         volPanel[panel] += lvi;
@@ -794,6 +817,70 @@ struct Oracle {
       slot = (int32_t)(vlist.size() / 3);
       vlist.insert(vlist.end(), &vert[3 * v], &vert[3 * v] + 3);
       vkey.insert(vkey.end(), e, e + 4);
+      vpid.push_back(vert_pid[v]);
+    }
+  }
+
+  // Compute_Vertex_Normals: the patch normal at each analytic vertex (ConnollySurface::getNormal,
+  // src/ConnollySurface.cpp:5736-5819, evaluated at the vertex; the skin quadric's gradient
+  // times 2, -2 for reduced tetrahedra, src/SkinSurface.cpp:3684-3712), zero for the others, which
+  // then get the mean of their triangles' plane3points normals, normalised (approximateNormals,
+  // src/Surface.cpp:10420-10460, 10660-10735).
+  void vertex_normals() {
+    const int64_t nv = (int64_t)vlist.size() / 3, nan = (int64_t)vpid.size();
+    normals.assign(3 * nv, 0.0);
+    for (int64_t v = 0; v < nan; v++) {
+      const int32_t pid = vpid[v];
+      const double* f = P.f64 + NS_PATCH_F64 * (int64_t)pid;
+      const int kind = P.i32[NS_PATCH_I32 * (int64_t)pid];
+      const double* y = &vlist[3 * v];
+      double* n = &normals[3 * v];
+      if (kind == NS_FACE_REG || kind == NS_FACE_SING) {
+        for (int d = 0; d < 3; d++) n[d] = (f[d] - y[d]) / P.probe;
+      } else if (kind == NS_POINT) {
+        for (int d = 0; d < 3; d++) n[d] = (y[d] - f[d]) / f[3];
+      } else if (kind == NS_EDGE_REG || kind == NS_EDGE_SING) {
+        const double* inv = f + 9;
+        double t[3] = {y[0] - f[4], y[1] - f[5], y[2] - f[6]}, C[3];
+        for (int i = 0; i < 3; i++) C[i] = inv[3 * i] * t[0] + inv[3 * i + 1] * t[1] + inv[3 * i + 2] * t[2];
+        double d = C[0] * C[0] + C[1] * C[1];
+        double rm1 = f[7] / sqrt(d) - 1.;
+        d = sqrt(d * rm1 * rm1 + C[2] * C[2]);
+        C[0] *= rm1 / d;
+        C[1] *= rm1 / d;
+        C[2] /= -d;
+        for (int i = 0; i < 3; i++) n[i] = inv[i] * C[0] + inv[3 + i] * C[1] + inv[6 + i] * C[2];
+      } else if (ns_is_skin(kind)) {
+        const double* Q = f + NS_SKIN_Q;
+        const double sg = kind == NS_SKIN_TETRA ? -2.0 : 2.0;
+        n[0] = sg * (Q[0] * y[0] + Q[4] * y[1] + Q[7] * y[2] + Q[9]);
+        n[1] = sg * (Q[4] * y[0] + Q[1] * y[1] + Q[5] * y[2] + Q[8]);
+        n[2] = sg * (Q[7] * y[0] + Q[5] * y[1] + Q[2] * y[2] + Q[6]);
+      }
+    }
+    std::vector<char> app(nv, 0);
+    for (int64_t v = 0; v < nv; v++) app[v] = normals[3 * v] == 0 && normals[3 * v + 1] == 0 && normals[3 * v + 2] == 0;
+    std::vector<double> mean(3 * nv, 0.0);
+    const int64_t nt = (int64_t)tris.size() / 3;
+    for (int64_t t = 0; t < nt; t++) {
+      const double* p1 = &vlist[3 * (int64_t)tris[3 * t]];
+      const double* p2 = &vlist[3 * (int64_t)tris[3 * t + 1]];
+      const double* p3 = &vlist[3 * (int64_t)tris[3 * t + 2]];
+      double w[3];
+      w[0] = p1[1] * (p2[2] - p3[2]) + p2[1] * (p3[2] - p1[2]) + p3[1] * (p1[2] - p2[2]);
+      w[1] = p1[2] * (p2[0] - p3[0]) + p2[2] * (p3[0] - p1[0]) + p3[2] * (p1[0] - p2[0]);
+      w[2] = p1[0] * (p2[1] - p3[1]) + p2[0] * (p3[1] - p1[1]) + p3[0] * (p1[1] - p2[1]);
+      for (int q = 0; q < 3; q++) {
+        const int32_t v = tris[3 * t + q];
+        if (!app[v]) continue;
+        for (int d = 0; d < 3; d++) mean[3 * v + d] = mean[3 * v + d] + w[d];
+      }
+    }
+    for (int64_t v = 0; v < nv; v++) {
+      if (!app[v]) continue;
+      double* m = &mean[3 * v];
+      double len = sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+      for (int d = 0; d < 3; d++) normals[3 * v + d] = m[d] / len;
     }
   }
 
@@ -916,6 +1003,7 @@ struct Oracle {
     if ((flags & 2) && (flags & 8)) {
       assemble();
       triangulate();
+      if (flags & 16) vertex_normals();
     }
   }
 };
@@ -1096,7 +1184,7 @@ void nso_free_mesh(void* h) { delete (BlobbyMesh*)h; }
 extern "C" {
 
 // flags: 1 status map, 2 accurate-triangulation rays + insideness, 4 cavity detection/filling,
-//        8 marching cubes.
+//        8 marching cubes, 16 vertex normals (Compute_Vertex_Normals).
 void* nso_run(const NsGrid* g, int64_t n_patches, const double* f64, const int32_t* i32, const double* pool,
               const int8_t* pool_flag, double probe, int flags, double cav_vol, int nthreads) {
   Oracle* o = new Oracle();
@@ -1134,6 +1222,7 @@ int64_t nso_size(void* h, const char* what) {
   if (w == "cav_size") return (int64_t)o->cav_size.size();
   if (w == "pix_off") return (int64_t)o->pix_off.size();
   if (w == "pix_t") return (int64_t)o->pix_t.size();
+  if (w == "normals") return (int64_t)o->normals.size();
   return -1;
 }
 
@@ -1149,6 +1238,7 @@ int nso_copy(void* h, const char* what, void* dst) {
   else if (w == "cav_filled") memcpy(dst, o->cav_filled.data(), o->cav_filled.size() * 4);
   else if (w == "pix_off") memcpy(dst, o->pix_off.data(), o->pix_off.size() * 8);
   else if (w == "pix_t") memcpy(dst, o->pix_t.data(), o->pix_t.size() * 8);
+  else if (w == "normals") memcpy(dst, o->normals.data(), o->normals.size() * 8);
   else return -1;
   return 0;
 }

@@ -18,6 +18,7 @@ STATUS = 1
 ACCURATE_TRIANGULATION = 2
 CAVITIES = 4
 TRIANGULATE = 8
+NORMALS = 16
 
 _lib = None
 
@@ -97,6 +98,7 @@ class OracleResult:
         if n > 0:
             L.nso_copy(handle, b"cav_filled", fl.ctypes.data)
         self.cav_filled = fl
+        self.normals = arr("normals", np.float64).reshape(-1, 3)
         self.pix_off = arr("pix_off", np.int64)
         self.pix_t = arr("pix_t", np.float64)
 

@@ -46,9 +46,10 @@ def test_reference_fixture_1crn_ses(native_lib, oracle_mod):
     surf, ds = ns.surf, ns.ds
     surf.getSurf(True, fill, cav_vol, keep_hits=True)
     surf.triangulateSurface()
+    assert surf.computeNormals  # the fixture asks for Compute_Vertex_Normals
     ref = oracle_mod.run(ds.grid, surf.patches, cav_vol=cav_vol if fill else 0.0,
                          flags=oracle_mod.STATUS | oracle_mod.ACCURATE_TRIANGULATION | oracle_mod.TRIANGULATE |
-                         (oracle_mod.CAVITIES if fill else 0))
+                         oracle_mod.NORMALS | (oracle_mod.CAVITIES if fill else 0))
     worst = 0.0
     for s in range(4):
         cnt_g, val_g = surf.hits(s)
@@ -58,7 +59,12 @@ def test_reference_fixture_1crn_ses(native_lib, oracle_mod):
             worst = max(worst, float(np.abs(val_g - val_o).max()))
     assert worst <= HIT_TOL
     figs = compare.compare_surface(surf, ds, ref)
-    print(f"1crn ses (grid {ds.nx}x{ds.ny}x{ds.nz}, {surf.patches.n} patches): worst hit diff {worst:.2e}, {figs}")
+    # analytic vertex normals (patch normal at every analytic vertex, triangle average elsewhere)
+    nrm = surf.vertexNormals()
+    dn = float(np.abs(nrm - ref.normals).max())
+    assert dn <= 1e-9, f"vertex normals differ by {dn}"
+    print(f"1crn ses (grid {ds.nx}x{ds.ny}x{ds.nz}, {surf.patches.n} patches): worst hit diff {worst:.2e}, "
+          f"normals within {dn:.1e}, {figs}")
 
 
 def test_ses_100k_maps_match_oracle(native_lib, oracle_mod):

@@ -63,11 +63,15 @@ def test_skin_fixture_1crn_fp64(native_lib, oracle_mod):
     surf, ds = ns.surf, ns.ds
     surf.getSurf(True, False, 0.0, keep_hits=True)
     surf.triangulateSurface()
-    ref = oracle_mod.run(ds.grid, surf.patches)
+    ref = oracle_mod.run(ds.grid, surf.patches, flags=oracle_mod.STATUS | oracle_mod.ACCURATE_TRIANGULATION |
+                         oracle_mod.TRIANGULATE | oracle_mod.NORMALS)
     worst = _compare_hits(surf, ref, oracle_mod)
     assert worst <= HIT_TOL
     figs = compare.compare_surface(surf, ds, ref)
-    print(f"1crn skin ({surf.patches.n} cells, grid {ds.nx}^3): worst hit diff {worst:.2e}, {figs}")
+    nrm = surf.vertexNormals()
+    dn = float(np.abs(nrm - ref.normals).max() / max(np.abs(ref.normals).max(), 1.0))
+    assert dn <= 1e-9, f"vertex normals differ by {dn} (relative)"
+    print(f"1crn skin ({surf.patches.n} cells, grid {ds.nx}^3): worst hit diff {worst:.2e}, normals {dn:.1e}, {figs}")
 
 
 @pytest.fixture(scope="module")
