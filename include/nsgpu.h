@@ -30,6 +30,7 @@ extern "C" {
 /* nsg_raycast flags */
 #define NSG_RAYCAST_STATUS 1            /* status map: Build_status_map = true */
 #define NSG_RAYCAST_TRIANGULATION 2     /* accurate-triangulation rays: Accurate_Triangulation = true */
+#define NSG_RAYCAST_EPSMAP 4            /* epsilon and ideb maps: Build_epsilon_maps = true (node rays of all three panels) */
 #define NSG_RAYCAST_KEEP_HITS 16        /* keep per-ray sorted hits for nsg_download_hits */
 #define NSG_RAYCAST_GRAD 32             /* adjoint: d volume (and d area of the next nsg_triangulate) / d patch */
 #define NSG_RAYCAST_NORMALS 64          /* keep the hits' patches for analytic vertex normals (Compute_Vertex_Normals) */
@@ -251,8 +252,32 @@ int nsg_download_insideness(nsg_ctx* ctx, uint32_t* dst);
 int nsg_download_mesh(nsg_ctx* ctx, double* vertices, int32_t* vertex_edges, int32_t* triangles);
 /* cavitiesSize / cavitiesFlag of DelPhiShared (src/DelphiShared.h:160-213). */
 int nsg_download_cavities(nsg_ctx* ctx, double* sizes, int32_t* filled);
-/* Sorted hit parameters per ray of one ray set (tests). */
+/* Sorted hit parameters per ray of one ray set (tests); sets 0 status, 1..3 accurate triangulation,
+ * 4 and 5 the epsilon-map node rays along z and y. */
 int nsg_download_hits(nsg_ctx* ctx, int ray_set, int32_t* counts, double* dst, int64_t dst_capacity);
+
+/* ---- epsilon maps and boundary grid points (Build_epsilon_maps, Project_boundary_grid_points) ---- */
+/* Epsilon map of the last nsg_raycast with NSG_RAYCAST_EPSMAP (single structure), cavity-filled
+ * when nsg_cavities ran after it: DelPhiShared::epsmap, int32 ((k*ny + j)*nx + i)*3 + axis, the
+ * code of the grid edge from node (i, j, k) to its neighbour along the axis: 0 outside, 5 inside
+ * (the node-ray fill of src/Surface.cpp:6645-6680, 6786-6795, 6887-6896; fillCavities
+ * src/Surface.cpp:2400-2417). */
+int nsg_download_epsmap(nsg_ctx* ctx, int32_t* dst);
+/* ideb map (DelPhiShared::idebmap), 1 byte per node, (k*ny + j)*nx + i: 0 inside the surface or in
+ * a filled cavity, 1 elsewhere (src/Surface.cpp:6655-6663, 2416). */
+int nsg_download_idebmap(nsg_ctx* ctx, uint8_t* dst);
+/* Boundary grid points of the epsilon map (src/Surface.cpp:1488-1546: nodes whose six edge codes
+ * differ, scan order z, y, x) and, with project != 0, the projection of the external ones onto an
+ * SES (Surface::projector, src/Surface.cpp:4657-4676; ConnollySurface::getProjection,
+ * src/ConnollySurface.cpp:5822-5912, over the auxiliary grid of buildAuxiliaryGrid,
+ * src/ConnollySurface.cpp:3666-3900, aux_max_dim = Max_ses_patches_auxiliary_grid_size, 50 by
+ * default).  Internal points (different dielectrics) do not arise with one inside code. */
+int nsg_bgp(nsg_ctx* ctx, int project, int32_t aux_max_dim, int64_t* n_bgp, int64_t* n_external);
+/* The points of the last nsg_bgp: ibgp (ix, iy, iz), type (1 external, 0 internal), scspos /
+ * scsnor (3 doubles; the reference leaves an external point's normal at 0) and the projection flag
+ * (0 projected, 1 no feasible projection among the cell's patches: the point is kept, 2 empty
+ * auxiliary cell, 3 internal); any pointer may be NULL. */
+int nsg_download_bgp(nsg_ctx* ctx, int32_t* ibgp, int32_t* type, double* scspos, double* scsnor, int32_t* flag);
 
 /* ---- allocation-free status ray cast ----
  * No counterpart in the reference: an addition for callers that may not allocate device memory

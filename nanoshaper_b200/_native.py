@@ -29,6 +29,7 @@ ERRORS = {
 # raycast flags
 STATUS = 1
 ACCURATE_TRIANGULATION = 2
+EPSMAP = 4
 KEEP_HITS = 16
 GRAD = 32
 NORMALS = 64
@@ -78,6 +79,10 @@ _SIGNATURES = {
     "nsg_download_mesh": ([_P, _P, _P, _P], _INT),
     "nsg_download_cavities": ([_P, _P, _P], _INT),
     "nsg_download_hits": ([_P, _INT, _P, _P, _I64], _INT),
+    "nsg_download_epsmap": ([_P, _P], _INT),
+    "nsg_download_idebmap": ([_P, _P], _INT),
+    "nsg_bgp": ([_P, _INT, ctypes.c_int32, _P, _P], _INT),
+    "nsg_download_bgp": ([_P, _P, _P, _P, _P, _P], _INT),
     "nsg_stats": ([_P, _P, _INT], _INT),
     "nsg_event_record": ([_P, _INT], _INT),
     "nsg_event_elapsed": ([_P, _INT, _INT, ctypes.POINTER(_D)], _INT),

@@ -20,6 +20,7 @@
 #include "host/host_api.h"
 #include "kernels/blobby.h"
 #include "kernels/cavity.h"
+#include "kernels/epsmap.h"
 #include "kernels/mc.h"
 #include "kernels/pipeline.h"
 
@@ -75,9 +76,9 @@ struct nsg_ctx {
   int32_t nstruct = 0;
   std::vector<NsGrid> grids;
   std::vector<nsg::StructDev> sd;
-  DevBuf d_sd, d_patch_struct, d_tile_struct[3], d_ray_base[4], d_mc_base, d_row_base, d_row_chunks;
+  DevBuf d_sd, d_patch_struct, d_tile_struct[3], d_ray_base[nsg::kRaySets], d_mc_base, d_row_base, d_row_chunks;
   int64_t nchunks = 0;
-  int64_t tiles_tot[3] = {0, 0, 0}, rays_tot[4] = {0, 0, 0, 0}, mc_tot = 0, rows_tot = 0, words_tot = 0, cubes_tot = 0;
+  int64_t tiles_tot[3] = {0, 0, 0}, rays_tot[nsg::kRaySets] = {0, 0, 0, 0, 0, 0}, mc_tot = 0, rows_tot = 0, words_tot = 0, cubes_tot = 0;
   int32_t patch_nstruct = 0;  // structures the uploaded patches belong to
   bool patch_struct_valid = false;
   std::vector<double> volumes, areas;
@@ -99,10 +100,11 @@ struct nsg_ctx {
   int64_t win_area[3] = {0, 0, 0};
   // wavefront tracing: candidate lists and the slot-major hit store
   // per ray set (slot s when the ray sets run on their own streams, slot 0 otherwise)
-  DevBuf cand_sph[4], cand_tor[4], hit_t[4], hit_cnt[4], def_sph[4], def_tor[4], hit_pid[4];
+  DevBuf cand_sph[nsg::kRaySets], cand_tor[nsg::kRaySets], hit_t[nsg::kRaySets], hit_cnt[nsg::kRaySets],
+      def_sph[nsg::kRaySets], def_tor[nsg::kRaySets], hit_pid[nsg::kRaySets];
   bool concurrent_sets = true;
-  cudaStream_t set_stream[4] = {};
-  cudaEvent_t fork_ev = nullptr, join_ev[4] = {};
+  cudaStream_t set_stream[nsg::kRaySets] = {};
+  cudaEvent_t fork_ev = nullptr, join_ev[nsg::kRaySets] = {};
   // gradient mode: hit / pair / vertex patches and the per-patch derivatives of volume and area
   DevBuf pair_pid, ovf_pscratch, gvol, garea, vpid, vgrad;
   // atoms behind the patches (for the device chain rule) and the atom derivatives
@@ -113,9 +115,9 @@ struct nsg_ctx {
   bool grad_mode = false, have_gvol = false, have_garea = false, have_pids = false;
   int64_t cand_cap = 0, def_cap = 0;
   // trace outputs
-  DevBuf status, bits, vol_ray[4];
-  DevBuf pairs, ray_pair_off, ray_pair_cnt, cursors, ovf_rays[4], ovf_scratch, err;
-  DevBuf hits, ray_hit_off[4], ray_hit_cnt[4];
+  DevBuf status, bits, vol_ray[nsg::kRaySets], epsmap;
+  DevBuf pairs, ray_pair_off, ray_pair_cnt, cursors, ovf_rays[nsg::kRaySets], ovf_scratch, err;
+  DevBuf hits, ray_hit_off[nsg::kRaySets], ray_hit_cnt[nsg::kRaySets];
   int64_t pair_cap = 0, hit_cap = 0;
   int flags = 0;
   int precision = 0;
@@ -126,6 +128,13 @@ struct nsg_ctx {
   DevBuf sruns, srun_off, srun_cnt, fr_cnt, fr_off, fruns, frow;
   int64_t srun_cap = 0, n_fruns = 0;
   bool status_dense = false;
+  bool have_eps = false;     // the last ray cast built the epsilon maps
+  bool eps_filled = false;   // cavity filling has been applied to them
+  // ideb map and boundary grid points (node index, ibgp, type, projection, projection flag), the
+  // auxiliary grid of the projection
+  DevBuf ideb, bgp_node, bgp_ibgp, bgp_type, bgp_pos, bgp_nor, bgp_flag, bgp_n, aux_cnt, aux_off, aux_list;
+  int64_t n_bgp = 0, n_bgp_ext = 0;
+  bool have_bgp = false, bgp_projected = false;
   // cavities
   DevBuf labels, is_root, roots, cc_count, cc_desc, cc_label_of, cc_fill_of, nroots_d;
   int ncav = 0;
@@ -153,7 +162,7 @@ struct nsg_ctx {
   cudaEvent_t st_ev[2 * 12] = {};
   double stage_ms[12] = {};
   int64_t stage_calls[12] = {};
-  cudaEvent_t sub_ev[4][4] = {};  // per ray set: before candidates, after candidates / intersections / fill
+  cudaEvent_t sub_ev[nsg::kRaySets][4] = {};  // per ray set: before candidates, after candidates / intersections / fill
   int64_t launches = 0;
   DevBuf counters;
   unsigned long long counter_host[8] = {};
@@ -194,7 +203,7 @@ nsg::BatchDev batch_dev(nsg_ctx* c) {
   B.s = c->d_sd.as<nsg::StructDev>();
   B.patch_struct = c->d_patch_struct.as<int32_t>();
   for (int i = 0; i < 3; i++) B.tile_struct[i] = c->d_tile_struct[i].as<int32_t>();
-  for (int i = 0; i < 4; i++) B.ray_base[i] = c->d_ray_base[i].as<int64_t>();
+  for (int i = 0; i < nsg::kRaySets; i++) B.ray_base[i] = c->d_ray_base[i].as<int64_t>();
   B.mc_base = c->d_mc_base.as<int64_t>();
   B.row_base = c->d_row_base.as<int64_t>();
   return B;
@@ -211,12 +220,12 @@ cudaError_t upload_vec(DevBuf& d, const std::vector<T>& h, cudaStream_t s) {
 // rows and bit words, and the reverse maps tile -> structure.
 int batch_layout(nsg_ctx* c, const NsGrid* grids, int32_t n) {
   std::vector<nsg::StructDev> sd(n);
-  std::vector<int64_t> rb[4], mcb(n + 1), rowb(n + 1);
+  std::vector<int64_t> rb[nsg::kRaySets], mcb(n + 1), rowb(n + 1);
   std::vector<int32_t> ts[3];
   std::vector<int4> chunks;  // marching-cubes row chunks: structure, first row, row count
   constexpr int32_t kRowChunk = 64;
-  for (int i = 0; i < 4; i++) rb[i].resize(n + 1);
-  int64_t tiles[3] = {0, 0, 0}, rays[4] = {0, 0, 0, 0}, mc = 0, rows = 0, words = 0, cubes = 0;
+  for (int i = 0; i < nsg::kRaySets; i++) rb[i].resize(n + 1);
+  int64_t tiles[3] = {0, 0, 0}, rays[nsg::kRaySets] = {0, 0, 0, 0, 0, 0}, mc = 0, rows = 0, words = 0, cubes = 0;
   for (int32_t b = 0; b < n; b++) {
     const NsGrid& G = grids[b];
     if (G.nx < 3 || G.ny < 3 || G.nz < 3) return fail(NSG_ERR_ARG, "grid must have at least 3 nodes per axis");
@@ -234,7 +243,7 @@ int batch_layout(nsg_ctx* c, const NsGrid* grids, int32_t n) {
       ts[panel].insert(ts[panel].end(), nt, b);
       tiles[panel] += nt;
     }
-    for (int set = 0; set < 4; set++) {
+    for (int set = 0; set < nsg::kRaySets; set++) {
       nsg::RaySet rs = nsg::make_ray_set(set, S.g);
       S.ray_base[set] = rb[set][b] = rays[set];
       rays[set] += rs.nb * rs.na;
@@ -254,7 +263,7 @@ int batch_layout(nsg_ctx* c, const NsGrid* grids, int32_t n) {
       S.box_dir[d] = S.g.mx[d] - S.g.mn[d];
     }
   }
-  for (int i = 0; i < 4; i++) {
+  for (int i = 0; i < nsg::kRaySets; i++) {
     rb[i][n] = rays[i];
     if (rays[i] >= (int64_t)1 << 31) return fail(NSG_ERR_CAPACITY, "more than 2^31 rays in one ray set of a batch");
   }
@@ -262,7 +271,7 @@ int batch_layout(nsg_ctx* c, const NsGrid* grids, int32_t n) {
   rowb[n] = rows;
   CK(upload_vec(c->d_sd, sd, c->stream));
   for (int i = 0; i < 3; i++) CK(upload_vec(c->d_tile_struct[i], ts[i], c->stream));
-  for (int i = 0; i < 4; i++) CK(upload_vec(c->d_ray_base[i], rb[i], c->stream));
+  for (int i = 0; i < nsg::kRaySets; i++) CK(upload_vec(c->d_ray_base[i], rb[i], c->stream));
   CK(upload_vec(c->d_mc_base, mcb, c->stream));
   CK(upload_vec(c->d_row_base, rowb, c->stream));
   CK(upload_vec(c->d_row_chunks, chunks, c->stream));
@@ -273,7 +282,7 @@ int batch_layout(nsg_ctx* c, const NsGrid* grids, int32_t n) {
   c->sd = sd;
   c->grid = grids[0];
   for (int i = 0; i < 3; i++) c->tiles_tot[i] = tiles[i];
-  for (int i = 0; i < 4; i++) c->rays_tot[i] = rays[i];
+  for (int i = 0; i < nsg::kRaySets; i++) c->rays_tot[i] = rays[i];
   c->mc_tot = mc;
   c->rows_tot = rows;
   c->words_tot = words;
@@ -459,7 +468,8 @@ int nsg_ctx_destroy(nsg_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   DevBuf* bufs[] = {&c->f64, &c->i32, &c->pool, &c->flag, &c->win, &c->pool32, &c->quad32, &c->quadl, &c->kind_mask_d, &c->b_atoms, &c->b_field, &c->b_mask, &c->b_nv, &c->b_nt, &c->b_voff, &c->b_toff, &c->b_vraw, &c->b_verts, &c->b_vkey, &c->b_tris, &c->b_inc_cnt, &c->b_inc_off, &c->b_inc_cur, &c->b_inc, &c->b_patch_atoms, &c->b_gpost, &c->b_gpre, &c->b_gfield, &c->b_gatoms, &c->counters, &c->bin_area,
-                    &c->status, &c->bits, &c->pairs,
+                    &c->status, &c->bits, &c->epsmap, &c->ideb, &c->bgp_node, &c->bgp_ibgp, &c->bgp_type,
+                    &c->bgp_pos, &c->bgp_nor, &c->bgp_flag, &c->bgp_n, &c->aux_cnt, &c->aux_off, &c->aux_list, &c->pairs,
                     &c->ray_pair_off, &c->ray_pair_cnt, &c->cursors, &c->ovf_scratch, &c->err, &c->hits,
                     &c->pair_pid, &c->ovf_pscratch, &c->gvol, &c->garea, &c->vpid, &c->vgrad,
                     &c->d_atoms, &c->d_patch_atoms, &c->d_gatoms_vol, &c->d_gatoms_area, &c->d_bad, &c->cube_vl, &c->cube_map, &c->vstruct,
@@ -475,8 +485,8 @@ int nsg_ctx_destroy(nsg_ctx* c) {
   c->d_row_chunks.release();
   c->vol_struct.release(); c->area_struct.release(); c->seg_part.release();
   for (int i = 0; i < 3; i++) c->d_tile_struct[i].release();
-  for (int i = 0; i < 4; i++) c->d_ray_base[i].release();
-  for (int i = 0; i < 4; i++) {
+  for (int i = 0; i < nsg::kRaySets; i++) c->d_ray_base[i].release();
+  for (int i = 0; i < nsg::kRaySets; i++) {
     c->vol_ray[i].release(); c->ovf_rays[i].release(); c->ray_hit_off[i].release(); c->ray_hit_cnt[i].release();
     c->cand_sph[i].release(); c->cand_tor[i].release(); c->def_sph[i].release(); c->def_tor[i].release();
     c->hit_t[i].release(); c->hit_cnt[i].release(); c->hit_pid[i].release();
@@ -487,7 +497,7 @@ int nsg_ctx_destroy(nsg_ctx* c) {
     if (c->user_ev[i]) cudaEventDestroy(c->user_ev[i]);
   for (int i = 0; i < 24; i++)
     if (c->st_ev[i]) cudaEventDestroy(c->st_ev[i]);
-  for (int i = 0; i < 4; i++)
+  for (int i = 0; i < nsg::kRaySets; i++)
     for (int q = 0; q < 4; q++)
       if (c->sub_ev[i][q]) cudaEventDestroy(c->sub_ev[i][q]);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -960,6 +970,10 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
   const bool do_mc = flags & 2;
   const bool keep_hits = flags & 16;
   const bool grad = flags & 32;
+  // epsilon maps: the node rays of panels 1 and 2 besides the status rays (Build_epsilon_maps)
+  const bool do_eps = flags & NSG_RAYCAST_EPSMAP;
+  if (do_eps && c->nstruct != 1) return fail(NSG_ERR_STATE, "epsilon maps are built for a single structure");
+  const auto cast = [&](int set) { return set == 0 ? (do_status || do_eps) : (set <= 3 ? do_mc : do_eps); };
   // the patches of the hits are kept for the gradients and for the analytic vertex normals
   const bool pids = grad || (flags & 64);
   if (!c->kind_mask_valid) {
@@ -994,8 +1008,8 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
   stage_begin(c, kStageBin);
   LAUNCH(nsg::launch_windows(P, c->win.as<int32_t>(), B, c->stream));
   for (int panel = 0; panel < 3; panel++) {
-    if (panel == 0 && !(do_status || do_mc)) continue;
-    if (panel > 0 && !do_mc) continue;
+    if (panel == 0 && !(do_status || do_eps || do_mc)) continue;
+    if (panel > 0 && !(do_mc || do_eps)) continue;
     int rc = panel_area(c, panel);
     if (rc) return rc;
   }
@@ -1003,7 +1017,7 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
   const int64_t nwords = c->words_tot;
   const int64_t nrays_mc = c->mc_tot;
   const int64_t nrows = c->rays_tot[0];
-  if (do_status) {
+  if (do_status || do_eps) {
     CK(c->srun_off.ensure(nrows * sizeof(int64_t)));
     CK(c->srun_cnt.ensure(nrows * sizeof(int32_t)));
     if (c->srun_cap == 0) c->srun_cap = std::max<int64_t>(4 * nrows, 1 << 16);
@@ -1021,16 +1035,18 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
   // that the double-precision intersection launches of one set overlap the integer-bound candidate
   // and fill launches of another; or, with concurrent_sets off, one after another on the context's
   // stream through slot 0
-  const bool conc = c->concurrent_sets && (do_mc ? 3 : 0) + (do_status ? 1 : 0) > 1;
+  const bool conc = c->concurrent_sets && (do_mc ? 3 : 0) + ((do_status || do_eps) ? 1 : 0) + (do_eps ? 2 : 0) > 1;
   const auto slot_of = [&](int set) { return conc ? set : 0; };
   {
     int64_t amax = std::max(c->win_area[0], std::max(c->win_area[1], c->win_area[2]));
     c->cand_cap = std::max<int64_t>(c->cand_cap, amax + 1024);
-    for (int set = 0; set < 4; set++) {
-      if ((set == 0 && !do_status) || (set > 0 && !do_mc)) continue;
+    int64_t nr_all = 0;
+    for (int set = 0; set < nsg::kRaySets; set++)
+      if (cast(set)) nr_all = std::max(nr_all, c->rays_tot[set]);
+    for (int set = 0; set < nsg::kRaySets; set++) {
+      if (!cast(set)) continue;
       const int sl = slot_of(set);
-      const int64_t nr = conc ? c->rays_tot[set]
-                              : std::max(std::max(c->rays_tot[0], c->rays_tot[1]), std::max(c->rays_tot[2], c->rays_tot[3]));
+      const int64_t nr = conc ? c->rays_tot[set] : nr_all;
       CK(c->hit_t[sl].ensure((size_t)nr * nsg::kHitCap * sizeof(double)));
       CK(c->hit_cnt[sl].ensure(nr * sizeof(int32_t)));
       if (pids) CK(c->hit_pid[sl].ensure((size_t)nr * nsg::kHitCap * sizeof(int32_t)));
@@ -1038,7 +1054,7 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
     if (grad) CK(c->gvol.ensure(std::max<int64_t>(c->np, 1) * NS_GRAD_PER_PATCH * sizeof(double)));
     if (conc) {
       if (!c->fork_ev) CK(cudaEventCreateWithFlags(&c->fork_ev, cudaEventDisableTiming));
-      for (int set = 0; set < 4; set++) {
+      for (int set = 0; set < nsg::kRaySets; set++) {
         if (!c->set_stream[set]) CK(cudaStreamCreateWithFlags(&c->set_stream[set], cudaStreamNonBlocking));
         if (!c->join_ev[set]) CK(cudaEventCreateWithFlags(&c->join_ev[set], cudaEventDisableTiming));
       }
@@ -1052,8 +1068,8 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
     if (grad)
       CK(cudaMemsetAsync(c->gvol.p, 0, std::max<int64_t>(c->np, 1) * NS_GRAD_PER_PATCH * sizeof(double), c->stream));
     if (precision == NSG_PRECISION_MIXED) c->def_cap = std::max<int64_t>(c->def_cap, c->cand_cap / 16 + (1 << 16));
-    for (int set = 0; set < 4; set++) {
-      if ((set == 0 && !do_status) || (set > 0 && !do_mc)) continue;
+    for (int set = 0; set < nsg::kRaySets; set++) {
+      if (!cast(set)) continue;
       const int sl = slot_of(set);
       CK(c->cand_sph[sl].ensure(c->cand_cap * sizeof(int2)));
       CK(c->cand_tor[sl].ensure(c->cand_cap * sizeof(int2)));
@@ -1062,23 +1078,32 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
         CK(c->def_tor[sl].ensure(c->def_cap * sizeof(int2)));
       }
     }
-    if (do_status) {
+    if (do_status || do_eps) {
       CK(c->sruns.ensure(c->srun_cap * sizeof(int2)));
       CK(cudaMemsetAsync(c->srun_cnt.p, 0, nrows * sizeof(int32_t), c->stream));
     }
     if (keep_hits) {
-      if (c->hit_cap == 0) c->hit_cap = std::max<int64_t>(8 * (nrays_mc + c->rays_tot[0]), 1 << 16);
+      if (c->hit_cap == 0)
+        c->hit_cap = std::max<int64_t>(8 * (nrays_mc + c->rays_tot[0] + (do_eps ? c->rays_tot[4] + c->rays_tot[5] : 0)),
+                                       1 << 16);
       CK(c->hits.ensure(c->hit_cap * sizeof(double)));
     }
     CK(cudaMemsetAsync(c->cursors.p, 0, 32 * sizeof(unsigned long long), c->stream));
     CK(cudaMemsetAsync(c->err.p, 0, sizeof(int32_t), c->stream));
     if (do_mc) CK(cudaMemsetAsync(c->bits.p, 0xff, nwords * sizeof(uint32_t), c->stream));
+    // cursors: 0 pairs, 1 kept hits, 2 status runs, 4..6 the overflow counts of the six ray sets
+    // (int32), 8 + 2 s the candidate counts of set s (spheres, tori), 20 + 2 s its deferred counts
     unsigned long long* cur = c->cursors.as<unsigned long long>();
-    int32_t* ovf_count = (int32_t*)(cur + 4);  // 4 int32 counters
-    int sets[4], nsets = 0;
-    if (do_status) sets[nsets++] = 0;
-    if (do_mc) { sets[nsets++] = 1; sets[nsets++] = 2; sets[nsets++] = 3; }
-    nsg::TraceOut outs[4];
+    int32_t* ovf_count = (int32_t*)(cur + 4);
+    int sets[nsg::kRaySets], nsets = 0;
+    for (int set = 0; set < nsg::kRaySets; set++)
+      if (cast(set)) sets[nsets++] = set;
+    nsg::TraceOut outs[nsg::kRaySets];
+    if (do_eps) {
+      const size_t eb = (size_t)c->grid.nx * c->grid.ny * c->grid.nz * 3 * sizeof(int32_t);
+      CK(c->epsmap.ensure(eb));
+      CK(cudaMemsetAsync(c->epsmap.p, 0, eb, c->stream));
+    }
     if (c->profile) {
       CK(c->counters.ensure(8 * sizeof(unsigned long long)));
       CK(cudaMemsetAsync(c->counters.p, 0, 8 * sizeof(unsigned long long), c->stream));
@@ -1092,7 +1117,7 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
         st = c->set_stream[s];
         CK(cudaStreamWaitEvent(st, c->fork_ev, 0));
       }
-      int panel = s == 0 ? 0 : s - 1;
+      int panel = nsg::ray_set_panel(s);
       int64_t nr = c->rays_tot[s];
       CK(c->vol_ray[s].ensure(nr * sizeof(double)));
       CK(c->ovf_rays[s].ensure(ovf_cap * sizeof(int32_t)));
@@ -1114,10 +1139,14 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
       o.ovf_count = ovf_count + s;
       o.error_flag = c->err.as<int32_t>();
       o.counters = c->profile ? c->counters.as<unsigned long long>() : nullptr;
+      if (do_eps && (s == 0 || s >= 4)) {
+        o.epsmap = c->epsmap.as<int32_t>();
+        o.eps_inside = NS_EPS_INSIDE;
+      }
       if (pids) o.pair_pid = c->pair_pid.as<int2>();
       if (grad) {
         o.gvol = c->gvol.as<double>();
-        o.grad_scale = 1.0 / (double)((do_status ? 1 : 0) + (do_mc ? 3 : 0));
+        o.grad_scale = 1.0 / (double)nsets;
       }
       if (keep_hits) {
         CK(c->ray_hit_off[s].ensure(nr * sizeof(int64_t)));
@@ -1132,7 +1161,7 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
       outs[s] = o;
       const int sl = slot_of(s);
       nsg::CandOut co{c->cand_sph[sl].as<int2>(), c->cand_tor[sl].as<int2>(), c->cand_cap, cur + 8 + 2 * s,
-                      c->def_sph[sl].as<int2>(), c->def_tor[sl].as<int2>(), c->def_cap, cur + 16 + 2 * s};
+                      c->def_sph[sl].as<int2>(), c->def_tor[sl].as<int2>(), c->def_cap, cur + 20 + 2 * s};
       nsg::HitStore hs{c->hit_t[sl].as<double>(), c->hit_cnt[sl].as<int32_t>(), nr,
                        pids ? c->hit_pid[sl].as<int32_t>() : nullptr};
       CK(cudaMemsetAsync(c->hit_cnt[sl].p, 0, nr * sizeof(int32_t), st));
@@ -1161,8 +1190,8 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
         }
       }
     }
-    int32_t novf[4] = {0, 0, 0, 0};
-    CK(cudaMemcpyAsync(novf, ovf_count, 4 * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    int32_t novf[nsg::kRaySets] = {0, 0, 0, 0, 0, 0};
+    CK(cudaMemcpyAsync(novf, ovf_count, nsg::kRaySets * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     int64_t tot_ovf = 0;
     bool tiles_built[3] = {false, false, false};
@@ -1172,7 +1201,7 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
       int n = std::min(novf[s], ovf_cap);
       tot_ovf += n;
       if (n == 0) continue;
-      const int panel = s == 0 ? 0 : s - 1;
+      const int panel = nsg::ray_set_panel(s);
       if (!tiles_built[panel]) {
         int rc = bin_panel(c, panel);
         if (rc) return rc;
@@ -1190,8 +1219,9 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
     if (c->profile) {
       CK(cudaMemcpyAsync(c->counter_host, c->counters.p, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                          c->stream));
-      unsigned long long cand[8];
-      CK(cudaMemcpyAsync(cand, cur + 8, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
+      unsigned long long cand[2 * nsg::kRaySets];
+      CK(cudaMemcpyAsync(cand, cur + 8, 2 * nsg::kRaySets * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                         c->stream));
       CK(cudaStreamSynchronize(c->stream));
       // candidate pairs (spheres + tori) and torus pairs of all ray sets
       c->counter_host[nsg::kCntCandidates] = 0;
@@ -1222,8 +1252,8 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
   int flag_sum = 0;
   CK(c->vol_struct.ensure(nb * sizeof(double)));
   CK(c->seg_part.ensure((size_t)nb * nsg::kSegParts * sizeof(double)));
-  for (int s = 0; s < 4; s++) {
-    if ((s == 0 && !do_status) || (s > 0 && !do_mc)) continue;
+  for (int s = 0; s < nsg::kRaySets; s++) {
+    if (!cast(s)) continue;
     LAUNCH(nsg::launch_segment_sums(c->vol_ray[s].as<double>(), B.ray_base[s], nullptr, nb,
                                     c->vol_struct.as<double>(), c->seg_part.as<double>(), flag_sum > 0, c->stream));
     flag_sum++;
@@ -1235,14 +1265,17 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
   for (int32_t b = 0; b < nb; b++) c->volumes[b] = flag_sum ? c->grids[b].A * vsum[b] / flag_sum : 0.0;
   c->volume = c->volumes[0];
   if (volume) *volume = c->volume;
-  if (do_status && nb == 1) {
+  if ((do_status || do_eps) && nb == 1) {
     int rc = build_free_runs(c);
     if (rc) return rc;
   }
   c->status_dense = false;
   c->have_gvol = grad;
   c->have_pids = pids && do_mc;
-  c->have_status = do_status;
+  c->have_status = do_status || do_eps;
+  c->have_eps = do_eps;
+  c->eps_filled = false;
+  c->have_bgp = c->bgp_projected = false;
   c->have_bits = do_mc;
   c->n_vert = c->n_tri = 0;
   return NSG_OK;
@@ -1346,6 +1379,11 @@ int nsg_cavities(nsg_ctx* c, double cav_vol, int* ncav_out) {
   CK(cudaMemcpyAsync(c->cc_fill_of.p, fill_of.data(), nroots, cudaMemcpyHostToDevice, c->stream));
   if (c->have_bits)
     LAUNCH(nsg::run_fill(A, c->cc_fill_of.as<uint8_t>(), c->bits.as<uint32_t>(), nwords_of(g), c->stream));
+  if (c->have_eps) {
+    LAUNCH(nsg::eps_fill_cavities(A, c->cc_fill_of.as<uint8_t>(), c->epsmap.as<int32_t>(), NS_EPS_INSIDE, c->stream));
+    c->eps_filled = true;
+    c->have_bgp = false;
+  }
   int rc = materialize_status(c, c->cc_label_of.as<int32_t>());
   if (rc) return rc;
   stage_end(c, kStageCavity);
@@ -1582,10 +1620,169 @@ int nsg_download_cavities(nsg_ctx* c, double* sizes, int32_t* filled) {
   return NSG_OK;
 }
 
+// Epsilon map in the reference's layout ((k*ny + j)*nx + i)*3 + axis (DelPhiShared::epsmap), after
+// cavity filling when nsg_cavities ran on this ray cast.
+int nsg_download_epsmap(nsg_ctx* c, int32_t* dst) {
+  if (!c || !dst) return NSG_ERR_ARG;
+  if (!c->have_eps) return fail(NSG_ERR_STATE, "no epsilon maps: ray cast with NSG_RAYCAST_EPSMAP");
+  CK(cudaSetDevice(c->device));
+  const NsGrid& g = c->grid;
+  CK(cudaMemcpyAsync(dst, c->epsmap.p, (size_t)g.nx * g.ny * g.nz * 3 * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                     c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return NSG_OK;
+}
+
+// ideb map (DelPhiShared::idebmap), 1 byte per node, (k*ny + j)*nx + i.
+int nsg_download_idebmap(nsg_ctx* c, uint8_t* dst) {
+  if (!c || !dst) return NSG_ERR_ARG;
+  if (!c->have_eps) return fail(NSG_ERR_STATE, "no ideb map: ray cast with NSG_RAYCAST_EPSMAP");
+  CK(cudaSetDevice(c->device));
+  const NsGrid& g = c->grid;
+  const size_t nn = (size_t)g.nx * g.ny * g.nz;
+  CK(c->ideb.ensure(nn));
+  nsg::RunArgs A = run_args(c);
+  LAUNCH(nsg::ideb_write(A, c->eps_filled ? c->cc_fill_of.as<uint8_t>() : nullptr, c->ideb.as<uint8_t>(), c->stream));
+  CK(cudaMemcpyAsync(dst, c->ideb.p, nn, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return NSG_OK;
+}
+
+// Auxiliary grid of the SES projection (ConnollySurface::buildAuxiliaryGrid,
+// src/ConnollySurface.cpp:3681-3726): the smallest odd multiplier gridMul >= 1 that brings the
+// node count igrid (an odd count of gridMul-wide cells covering nx nodes) to at most max_dim,
+// centred on the grid's barycentre.
+nsg::AuxGrid aux_grid_of(const NsGrid& g, int64_t max_dim) {
+  int64_t igrid = g.nx, mul = 1;
+  while (igrid > max_dim) {
+    mul += 2;
+    int64_t digrid = g.nx;
+    while (true) {
+      const int64_t fixed_point = (digrid + (mul - 1)) / mul;
+      igrid = fixed_point * mul;
+      if (igrid % 2 == 0) {
+        digrid = igrid + 1;
+      } else {
+        igrid = fixed_point;
+        break;
+      }
+    }
+  }
+  nsg::AuxGrid a;
+  a.n = igrid;
+  a.scale = g.scale / (double)mul;
+  const double side = (double)mul / g.scale;
+  a.mn[0] = g.baricenter[0] - (igrid - 1) * 0.5 * side;
+  a.mn[1] = g.baricenter[1] - (igrid - 1) * 0.5 * side;
+  a.mn[2] = g.baricenter[2] - (igrid - 1) * 0.5 * side;
+  return a;
+}
+
+// Boundary grid points of the epsilon map (src/Surface.cpp:1488-1546) and, with project != 0,
+// the projection of the external ones onto the SES (Surface::projector with
+// ConnollySurface::getProjection); aux_max_dim is Max_ses_patches_auxiliary_grid_size (50).
+int nsg_bgp(nsg_ctx* c, int project, int32_t aux_max_dim, int64_t* n_bgp, int64_t* n_external) {
+  if (!c) return NSG_ERR_ARG;
+  if (!c->have_eps) return fail(NSG_ERR_STATE, "boundary grid points need the epsilon maps (NSG_RAYCAST_EPSMAP)");
+  if (project && (c->kind_mask & ~nsg::kSesKinds))
+    return fail(NSG_ERR_STATE, "boundary grid point projection is provided for SES patch sets");
+  if (project && aux_max_dim < 1) return fail(NSG_ERR_ARG, "auxiliary grid size must be positive");
+  CK(cudaSetDevice(c->device));
+  const NsGrid& g = c->grid;
+  const int32_t* eps = c->epsmap.as<int32_t>();
+  CK(c->bgp_n.ensure(2 * sizeof(int64_t)));
+  int32_t* cnt_d = c->bgp_n.as<int32_t>();
+  size_t tb = 0;
+  CK(nsg::bgp_select(eps, g.nx, g.ny, g.nz, nullptr, cnt_d, nullptr, &tb, c->stream));
+  CK(c->temp.ensure(tb));
+  tb = c->temp.cap;
+  c->launches++;
+  CK(nsg::bgp_select(eps, g.nx, g.ny, g.nz, nullptr, cnt_d, c->temp.p, &tb, c->stream));
+  int32_t n = 0;
+  CK(cudaMemcpyAsync(&n, cnt_d, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  const size_t ncap = std::max<int32_t>(n, 1);
+  CK(c->bgp_node.ensure(ncap * sizeof(int32_t)));
+  CK(c->bgp_ibgp.ensure(3 * ncap * sizeof(int32_t)));
+  CK(c->bgp_type.ensure(ncap * sizeof(int32_t)));
+  tb = 0;
+  CK(nsg::bgp_select(eps, g.nx, g.ny, g.nz, c->bgp_node.as<int32_t>(), cnt_d, nullptr, &tb, c->stream));
+  CK(c->temp.ensure(tb));
+  tb = c->temp.cap;
+  c->launches++;
+  CK(nsg::bgp_select(eps, g.nx, g.ny, g.nz, c->bgp_node.as<int32_t>(), cnt_d, c->temp.p, &tb, c->stream));
+  LAUNCH(nsg::bgp_expand(eps, g.nx, g.ny, g.nz, c->bgp_node.as<int32_t>(), n, c->bgp_ibgp.as<int32_t>(),
+                         c->bgp_type.as<int32_t>(), c->stream));
+  int64_t n_ext = 0;
+  if (n > 0) {
+    int64_t* ext_d = c->bgp_n.as<int64_t>() + 1;
+    tb = 0;
+    CK(nsg::sum_i32(c->bgp_type.as<int32_t>(), n, ext_d, nullptr, &tb, c->stream));
+    CK(c->temp.ensure(tb));
+    tb = c->temp.cap;
+    c->launches++;
+    CK(nsg::sum_i32(c->bgp_type.as<int32_t>(), n, ext_d, c->temp.p, &tb, c->stream));
+    CK(cudaMemcpyAsync(&n_ext, ext_d, sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  c->n_bgp = n;
+  c->n_bgp_ext = n_ext;
+  c->have_bgp = true;
+  c->bgp_projected = false;
+  if (project && n > 0) {
+    const nsg::AuxGrid a = aux_grid_of(g, aux_max_dim);
+    const int64_t ncell = a.n * a.n * a.n;
+    CK(c->aux_cnt.ensure(ncell * sizeof(int32_t)));
+    CK(c->aux_off.ensure((ncell + 1) * sizeof(int64_t)));
+    CK(cudaMemsetAsync(c->aux_cnt.p, 0, ncell * sizeof(int32_t), c->stream));
+    nsg::PatchDev P = patch_dev(c);
+    LAUNCH(nsg::aux_count(P, a, c->aux_cnt.as<int32_t>(), c->stream));
+    int64_t total = 0;
+    int rc = scan_counts(c, c->aux_cnt.as<int32_t>(), ncell, c->aux_off.as<int64_t>(), &total);
+    if (rc) return rc;
+    CK(c->aux_list.ensure(std::max<int64_t>(total, 1) * sizeof(int32_t)));
+    CK(cudaMemsetAsync(c->aux_cnt.p, 0, ncell * sizeof(int32_t), c->stream));
+    LAUNCH(nsg::aux_fill(P, a, c->aux_off.as<int64_t>(), c->aux_cnt.as<int32_t>(), c->aux_list.as<int32_t>(),
+                         c->stream));
+    CK(c->bgp_pos.ensure(3 * ncap * sizeof(double)));
+    CK(c->bgp_nor.ensure(3 * ncap * sizeof(double)));
+    CK(c->bgp_flag.ensure(ncap * sizeof(int32_t)));
+    LAUNCH(nsg::bgp_project(P, a, c->aux_off.as<int64_t>(), c->aux_list.as<int32_t>(), grid_dev(g), c->bgp_ibgp.as<int32_t>(),
+                            c->bgp_type.as<int32_t>(), n, c->bgp_pos.as<double>(), c->bgp_nor.as<double>(),
+                            c->bgp_flag.as<int32_t>(), c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->bgp_projected = true;
+  }
+  if (n_bgp) *n_bgp = n;
+  if (n_external) *n_external = n_ext;
+  return NSG_OK;
+}
+
+// The boundary grid points of the last nsg_bgp: ibgp (3 int32 per point), type (EXTERNAL 1 /
+// INTERNAL 0), and when projected scspos / scsnor (3 doubles per point) and the projection flag
+// (0 projected, 1 no feasible projection, 2 empty auxiliary cell, 3 internal point); any pointer
+// may be NULL.
+int nsg_download_bgp(nsg_ctx* c, int32_t* ibgp, int32_t* type, double* scspos, double* scsnor, int32_t* flag) {
+  if (!c) return NSG_ERR_ARG;
+  if (!c->have_bgp) return fail(NSG_ERR_STATE, "no boundary grid points: call nsg_bgp first");
+  if ((scspos || scsnor || flag) && !c->bgp_projected) return fail(NSG_ERR_STATE, "boundary grid points not projected");
+  CK(cudaSetDevice(c->device));
+  const size_t n = (size_t)c->n_bgp;
+  if (n) {
+    if (ibgp) CK(cudaMemcpyAsync(ibgp, c->bgp_ibgp.p, 3 * n * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    if (type) CK(cudaMemcpyAsync(type, c->bgp_type.p, n * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    if (scspos) CK(cudaMemcpyAsync(scspos, c->bgp_pos.p, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (scsnor) CK(cudaMemcpyAsync(scsnor, c->bgp_nor.p, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (flag) CK(cudaMemcpyAsync(flag, c->bgp_flag.p, n * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  return NSG_OK;
+}
+
 // Per-ray sorted hit parameters of one ray set (raycast with flag 16): counts are indexed by
 // n*nb + m of the set; hits are gathered in that order into dst.
 int nsg_download_hits(nsg_ctx* c, int set, int32_t* counts, double* dst, int64_t dst_cap) {
-  if (!c || set < 0 || set > 3 || !(c->flags & 16)) return NSG_ERR_STATE;
+  if (!c || set < 0 || set >= nsg::kRaySets || !(c->flags & 16)) return NSG_ERR_STATE;
   int64_t nr = c->rays_tot[set];
   std::vector<int64_t> off(nr);
   std::vector<int32_t> cnt(nr);

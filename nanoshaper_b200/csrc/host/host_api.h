@@ -19,6 +19,8 @@
 #define NSG_PRECISION_FP64 0
 #define NSG_PRECISION_MIXED 1
 
+#define NSG_RAYCAST_EPSMAP 4
+
 #ifdef __cplusplus
 extern "C" {
 #endif

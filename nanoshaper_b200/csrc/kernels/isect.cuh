@@ -180,7 +180,7 @@ __device__ __forceinline__ void isect_body(const TraceCtx& C, const CandOut& co,
     const int64_t rid = e.x, pid = e.y;
     const StructDev& S = C.B.s[C.B.patch_struct[pid]];
     const GridDev& g = S.g;
-    const double delta = C.set == 0 ? 0.0 : NS_DELTA - g.hside;
+    const double delta = ray_set_shifted(C.set) ? NS_DELTA - g.hside : 0.0;
     const double ray_dir = S.ray_dir[vc];
     const double inv_dir = S.inv_dir[vc];
     const int64_t nb = g.n[fd];
@@ -389,7 +389,7 @@ __device__ __forceinline__ void isect_quadric_body(const TraceCtx& C, const Cand
     if (!ns_has_box(kind)) continue;
     const StructDev& S = C.B.s[C.B.patch_struct[pid]];
     const GridDev& g = S.g;
-    const double delta = C.set == 0 ? 0.0 : NS_DELTA - g.hside;
+    const double delta = ray_set_shifted(C.set) ? NS_DELTA - g.hside : 0.0;
     const int64_t nb = g.n[fd];
     const int64_t lr = rid - S.ray_base[C.set];
     const int64_t m = lr % nb, n = lr / nb;

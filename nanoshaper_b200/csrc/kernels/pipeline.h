@@ -21,9 +21,12 @@ constexpr int kHitCap = 32;
 constexpr int kOverflowCap = 2048;
 
 // Ray sets: 0 = status rays along x (panel 0, through grid nodes); 1..3 = accurate
-// triangulation rays of panels 0 (x), 1 (z), 2 (y), shifted by DELTA - hside.
+// triangulation rays of panels 0 (x), 1 (z), 2 (y), shifted by DELTA - hside; 4, 5 = the node rays
+// of panels 1 (z) and 2 (y) that the epsilon maps add (the reference's node-ray pass over all
+// three panels when Build_epsilon_maps is set, src/Surface.cpp:6318-6340).
+constexpr int kRaySets = 6;
 struct RaySet {
-  int set;      // 0..3
+  int set;      // 0..5
   int panel;    // 0..2
   int fd, ld, vc;  // first pixel axis (m), second pixel axis (n), ray axis
   int64_t nb, na;  // pixel counts along m and n
@@ -45,7 +48,7 @@ struct StructDev {
   int64_t nwords;        // words of its 32x-packed insideness bit grid
   int64_t word_base;     // first word in the batch's bit array
   int64_t tile_base[3];  // first tile of each panel in the panel's tile arrays
-  int64_t ray_base[4];   // first ray of each ray set in the set's ray arrays
+  int64_t ray_base[kRaySets];  // first ray of each ray set in the set's ray arrays
   int64_t mc_base;       // first accurate-triangulation ray ordinal (its 3 panels are contiguous)
   int64_t row_base;      // first marching-cubes row ((NY-2)*(NZ-2) rows per structure)
   int64_t cube_base;     // first entry of its dense cube map ((NX-2)*(NY-2)*(NZ-2) cubes)
@@ -62,7 +65,7 @@ struct BatchDev {
   const StructDev* s;
   const int32_t* patch_struct;    // structure of every patch
   const int32_t* tile_struct[3];  // structure of every tile of each panel
-  const int64_t* ray_base[4];     // n+1 per ray set
+  const int64_t* ray_base[kRaySets];  // n+1 per ray set
   const int64_t* mc_base;         // n+1
   const int64_t* row_base;        // n+1
 };
@@ -78,22 +81,26 @@ __device__ __forceinline__ int find_struct(const int64_t* __restrict__ base, int
   return lo;
 }
 
+// Panel of a ray set, and whether its origins are shifted off the grid nodes.
+__host__ __device__ inline int ray_set_panel(int set) { return set == 0 ? 0 : (set <= 3 ? set - 1 : set - 3); }
+__host__ __device__ inline bool ray_set_shifted(int set) { return set >= 1 && set <= 3; }
+
 __host__ __device__ inline RaySet make_ray_set(int set, const GridDev& g) {
   RaySet r;
   r.set = set;
-  r.panel = set == 0 ? 0 : set - 1;
+  r.panel = ray_set_panel(set);
   if (r.panel == 0) { r.fd = 1; r.ld = 2; r.vc = 0; }
   else if (r.panel == 1) { r.fd = 0; r.ld = 1; r.vc = 2; }
   else { r.fd = 0; r.ld = 2; r.vc = 1; }
   r.nb = g.n[r.fd];
   r.na = g.n[r.ld];
-  r.delta = set == 0 ? 0.0 : NS_DELTA - g.hside;
+  r.delta = ray_set_shifted(set) ? NS_DELTA - g.hside : 0.0;
   // accurate triangulation ray order: panel 0 rays (n over z, m over y), panel 1 (n over y,
   // m over x), panel 2 (n over z, m over x)
   int64_t b = 0;
   if (r.panel >= 1) b += g.n[2] * g.n[1];
   if (r.panel >= 2) b += g.n[1] * g.n[0];
-  r.ordinal_base = set == 0 ? 0 : b;
+  r.ordinal_base = ray_set_shifted(set) ? b : 0;
   return r;
 }
 
@@ -129,6 +136,11 @@ struct TraceOut {
   double* gvol;
   int2* pair_pid;
   double grad_scale;
+  // epsilon maps (null otherwise): the reference's 4-D layout ((k*ny + j)*nx + i)*3 + l, l the axis
+  // of the grid edge from node (i, j, k) to its +1 neighbour; set 0 writes l = 0, set 4 l = 2,
+  // set 5 l = 1; eps_inside is the code of the inside medium
+  int32_t* epsmap;
+  int32_t eps_inside;
   // optional event counters (profiling): candidates, torus candidates, mixed-precision fallbacks
   // (near-tangent sphere, quartic isolation, root polish / root boundary), FP64 re-evaluations of
   // feasibility tests

@@ -278,6 +278,32 @@ __device__ __forceinline__ void status_node_range(const GridDev& g, double lim1,
   *ib = b;
 }
 
+// Epsilon-map entries of one interval [lim1, lim2] of a node ray (sets 0, 4, 5): the reference takes
+// the clamped rintp node range [c1, c2] of the interval and marks the grid edges that start at a
+// node c with coord(c) <= lim2 - hside (src/Surface.cpp:6645-6680 for x, inclusive of c2;
+// :6786-6795 for z and :6887-6896 for y, exclusive of c2).  m, n are the ray's pixel indices.
+__device__ __forceinline__ void eps_fill(const GridDev& g, const RaySet& rs, int64_t m, int64_t n, double lim1,
+                                         double lim2, int32_t* __restrict__ eps, int32_t inside) {
+  const int vc = rs.vc;
+  const int64_t N = g.n[vc];
+  int64_t c1 = (int64_t)rintp((lim1 - g.mn[vc]) * g.scale);
+  int64_t c2 = (int64_t)rintp((lim2 - g.mn[vc]) * g.scale);
+  c1 = c1 < 0 ? 0 : (c1 >= N ? N - 1 : c1);
+  c2 = c2 < 0 ? 0 : (c2 >= N ? N - 1 : c2);
+  if (c2 < c1) return;
+  int64_t e = vc == 0 ? c2 : c2 - 1;
+  const double lim = lim2 - g.hside;
+  while (e >= c1 && gcoord(g, vc, e) > lim) e--;
+  const int64_t NX = g.n[0], NY = g.n[1];
+  // node (i, j, k) of position c along the ray; l = the component of this ray set
+  int64_t base, step;
+  int l;
+  if (vc == 0) { base = (n * NY + m) * NX; step = 1; l = 0; }
+  else if (vc == 2) { base = n * NX + m; step = NX * NY; l = 2; }
+  else { base = n * NY * NX + m; step = NX; l = 1; }
+  for (int64_t c = c1; c <= e; c++) eps[(base + c * step) * 3 + l] = inside;
+}
+
 // Warp-aggregated append of this lane's `cnt` records to a shared store; returns the lane's first
 // slot, or -1 when the store is full (the error flag is then set to `code`).
 __device__ __forceinline__ int64_t warp_append(unsigned long long* cursor, int64_t cap, int cnt, int32_t* error_flag,
@@ -564,7 +590,7 @@ void launch_isect(const TraceCtx& C, const CandOut& co, const HitStore& hs, int 
 template <bool kGrad>
 __global__ void __launch_bounds__(kTraceThreads, 6) k_fill(TraceCtx C, HitStore hs) {
   constexpr int kThreads = kTraceThreads;
-  const int panel = C.set == 0 ? 0 : C.set - 1;
+  const int panel = ray_set_panel(C.set);
   const int64_t tile = blockIdx.x;
   const StructDev& S = C.B.s[C.B.tile_struct[panel][tile]];
   const GridDev g = S.g;
@@ -621,9 +647,9 @@ __global__ void __launch_bounds__(kTraceThreads, 6) k_fill(TraceCtx C, HitStore 
     }
   }
   // interval ends
-  const bool mc = rs.set != 0;
+  const bool mc = ray_set_shifted(rs.set);
   double pa_vc, dirl;
-  if (!mc) {
+  if (rs.set == 0) {
     pa_vc = gcoord(g, 0, 0);
     dirl = gcoord(g, 0, g.n[0] - 1) - pa_vc;
   } else {
@@ -709,11 +735,20 @@ __global__ void __launch_bounds__(kTraceThreads, 6) k_fill(TraceCtx C, HitStore 
   if (valid && !ovf) C.out.vol_ray[rid] = vol;
   __syncwarp();
   const int64_t NX = g.n[0], NY = g.n[1];
+  if (rs.set >= 4) {
+    // epsilon-map node rays of panels 1 and 2
+    if (valid && !ovf && C.out.epsmap)
+      for (int q = 0; q < np; q++)
+        eps_fill(g, rs, m, n, col[(2 * q) * kThreads], col[(2 * q + 1) * kThreads], C.out.epsmap, C.out.eps_inside);
+    return;
+  }
   if (!mc) {
     // status row (., j = m, k = n): runs of inside nodes
     int nr = 0;
     if (valid && !ovf)
       for (int q = 0; q < np; q++) {
+        if (C.out.epsmap)
+          eps_fill(g, rs, m, n, col[(2 * q) * kThreads], col[(2 * q + 1) * kThreads], C.out.epsmap, C.out.eps_inside);
         int64_t ia, ib;
         status_node_range(g, col[(2 * q) * kThreads], col[(2 * q + 1) * kThreads], &ia, &ib);
         if (ia > ib) continue;
@@ -895,9 +930,9 @@ __global__ void k_trace_overflow(TraceCtx C, const int64_t* __restrict__ tile_of
       atomicExch(C.out.error_flag, 2);
     }
   }
-  const bool mc = rs.set != 0;
+  const bool mc = ray_set_shifted(rs.set);
   double pa_vc, dirl;
-  if (!mc) {
+  if (rs.set == 0) {
     pa_vc = gcoord(g, 0, 0);
     dirl = gcoord(g, 0, g.n[0] - 1) - pa_vc;
   } else {
@@ -918,9 +953,15 @@ __global__ void k_trace_overflow(TraceCtx C, const int64_t* __restrict__ tile_of
   int np = make_pairs(col, 1, nh, pa_vc, dirl, g.mn[rs.vc], g.scale, mc, &vol, pcol, (pcol && gc.gvol) ? &gc : nullptr);
   C.out.vol_ray[rid] = vol;
   const int64_t NX = g.n[0], NY = g.n[1];
+  if (rs.set >= 4) {
+    if (C.out.epsmap)
+      for (int q = 0; q < np; q++) eps_fill(g, rs, m, n, col[2 * q], col[2 * q + 1], C.out.epsmap, C.out.eps_inside);
+    return;
+  }
   if (!mc) {
     int nr = 0;
     for (int q = 0; q < np; q++) {
+      if (C.out.epsmap) eps_fill(g, rs, m, n, col[2 * q], col[2 * q + 1], C.out.epsmap, C.out.eps_inside);
       int64_t ia, ib;
       status_node_range(g, col[2 * q], col[2 * q + 1], &ia, &ib);
       if (ia > ib) continue;
@@ -1008,7 +1049,7 @@ cudaError_t launch_trace(const PatchDev& P, const BatchDev& B, int set, int64_t 
                          cudaEvent_t* ev) {
   if (ntiles <= 0) return cudaSuccess;
   TraceCtx C{P, B, set, out};
-  const int panel = set == 0 ? 0 : set - 1;
+  const int panel = ray_set_panel(set);
   if (ev) cudaEventRecord(ev[0], s);
   if (P.n > 0) {
     const int wpb = tp.cand_threads / 32;

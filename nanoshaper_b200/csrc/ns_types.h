@@ -86,6 +86,14 @@ NS_HD bool ns_has_box(int kind) { return kind >= NS_SKIN_POINT; }
 #define NS_STATUS_OUT 3
 #define NS_STATUS_FIRST_CAV 4
 
+// Epsilon-map code of the inside medium: every surface type sets inside = 5
+// (src/ConnollySurface.cpp:214, src/SkinSurface.cpp:200, src/BlobbySurface.cpp:18,
+// src/MeshSurface.cpp:188); outside edges keep 0.
+#define NS_EPS_INSIDE 5
+// Boundary grid point types (src/Surface.h:294-295).
+#define NS_INTERNAL_BGP 0
+#define NS_EXTERNAL_BGP 1
+
 // Tolerances of the reference (src/Surface.h:285-291).
 #define NS_EPS_INT 1e-8
 #define NS_DELTA 1e-10

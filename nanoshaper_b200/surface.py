@@ -147,8 +147,6 @@ class DelPhiShared:
             raise ValueError("Cannot build grid with no atoms!")
         self.buildStatus = build_status
         self.buildEpsMap = build_eps_map
-        if build_eps_map:
-            raise NotImplementedError("epsilon maps are not built by this implementation")
         self.grid = N.NsGrid()
         if grid is None:
             self.buildGrid(scale, perfil)
@@ -159,6 +157,19 @@ class DelPhiShared:
         self.status: np.ndarray | None = None
         self.cavitiesSize: list[float] = []
         self.cavitiesFlag: list[bool] = []
+        # epsilon and ideb maps (Build_epsilon_maps): epsmap[k, j, i, axis] is the code of the grid
+        # edge from node (i, j, k) along the axis (0 outside, 5 inside), idebmap[k, j, i] is False
+        # inside the surface and in filled cavities
+        self.epsmap: np.ndarray | None = None
+        self.idebmap: np.ndarray | None = None
+        # boundary grid points (Project_boundary_grid_points): nodes (ix, iy, iz), their type
+        # (1 external, 0 internal), projections onto the surface and normals
+        self.nbgp = 0
+        self.ibgp: np.ndarray | None = None
+        self.bgp_type: np.ndarray | None = None
+        self.scspos: np.ndarray | None = None
+        self.scsnor: np.ndarray | None = None
+        self.bgp_flag: np.ndarray | None = None
 
     def saveStatus(self, fname: str | Path = "") -> None:
         """``fname.status.txt`` and the cavity files (DelPhiShared::saveStatus / saveCavities)."""
@@ -330,6 +341,8 @@ class Surface:
         self.forceSerialBuild = cf.read("Force_Serial_Build", False, bool)
         self.numThreads = cf.read("Number_thread", 0, int)
         self.precision = cf.read("Gpu_Precision", "fp64", str).strip().lower()
+        self.projBGP = cf.read("Project_boundary_grid_points", False, bool)
+        self.auxGridDim = cf.read("Max_ses_patches_auxiliary_grid_size", 50, int)
         self.randDisplacement = RAND_DISPLACEMENT
         self.device = device
         self.ctx: Context | None = None
@@ -380,6 +393,10 @@ class Surface:
             flags |= N.STATUS
         if self.accurateTriangulation:
             flags |= N.ACCURATE_TRIANGULATION
+        if self.delphi.buildEpsMap:
+            flags |= N.EPSMAP
+        elif self.projBGP:
+            raise RuntimeError("Cannot project boundary grid points without an epsilon map (Build_epsilon_maps = true)")
         if keep_hits:
             flags |= N.KEEP_HITS
         if grad:
@@ -416,7 +433,39 @@ class Surface:
                 bits = np.empty(words, np.uint32)
                 N.check(N.lib().nsg_download_insideness(c, N.ptr(bits)), "download insideness")
                 self.insideness = bits
+            if self.delphi.buildEpsMap:
+                eps = np.empty(g.nx * g.ny * g.nz * 3, np.int32)
+                N.check(N.lib().nsg_download_epsmap(c, N.ptr(eps)), "download epsilon map")
+                self.delphi.epsmap = eps.reshape(g.nz, g.ny, g.nx, 3)
+                ideb = np.empty(g.nx * g.ny * g.nz, np.uint8)
+                N.check(N.lib().nsg_download_idebmap(c, N.ptr(ideb)), "download ideb map")
+                self.delphi.idebmap = ideb.reshape(g.nz, g.ny, g.nx).astype(bool)
+        if self.projBGP:
+            self.projectBoundaryGridPoints()
         return self.volume
+
+    def projectBoundaryGridPoints(self) -> int:
+        """Boundary grid points of the epsilon map and their projection onto the surface (the
+        projBGP phase of Surface::getSurf, src/Surface.cpp:1473-1678); fills the DelPhiShared's
+        ibgp, bgp_type, scspos, scsnor (and bgp_flag: 0 projected, 1 no feasible projection among
+        the auxiliary cell's patches, the point kept; 2 empty cell).  Returns the point count."""
+        if self.name != "ses":
+            raise NotImplementedError("boundary grid point projection is provided for the SES")
+        c = self._context().handle
+        n = ctypes.c_int64()
+        ne = ctypes.c_int64()
+        N.check(N.lib().nsg_bgp(c, 1, int(self.auxGridDim), ctypes.byref(n), ctypes.byref(ne)), "boundary grid points")
+        d = self.delphi
+        d.nbgp = n.value
+        d.ibgp = np.zeros((d.nbgp, 3), np.int32)
+        d.bgp_type = np.zeros(d.nbgp, np.int32)
+        d.scspos = np.zeros((d.nbgp, 3))
+        d.scsnor = np.zeros((d.nbgp, 3))
+        d.bgp_flag = np.zeros(d.nbgp, np.int32)
+        if d.nbgp:
+            N.check(N.lib().nsg_download_bgp(c, N.ptr(d.ibgp), N.ptr(d.bgp_type), N.ptr(d.scspos), N.ptr(d.scsnor),
+                                             N.ptr(d.bgp_flag)), "download boundary grid points")
+        return d.nbgp
 
     def triangulateSurface(self, outputMesh: bool = False, fileName: str = "triangulatedSurf",
                            download: bool = True) -> float:
@@ -510,7 +559,7 @@ class Surface:
         """Per-ray sorted hit parameters of one ray set from the last keep_hits ray cast."""
         c = self._context().handle
         g = self.delphi.grid
-        nb, na = ((g.ny, g.nz), (g.ny, g.nz), (g.nx, g.ny), (g.nx, g.nz))[ray_set]
+        nb, na = ((g.ny, g.nz), (g.ny, g.nz), (g.nx, g.ny), (g.nx, g.nz), (g.nx, g.ny), (g.nx, g.nz))[ray_set]
         counts = np.zeros(nb * na, np.int32)
         total = N.lib().nsg_download_hits(c, ray_set, N.ptr(counts), None, 0)
         if total < 0:
@@ -889,7 +938,8 @@ class NanoShaper:
         self.cf = cf
         self.scale = cf.read("Grid_scale", scale, float)
         self.perfil = cf.read("Grid_perfil", perfil, float)
-        self.ds = DelPhiShared(atoms, self.scale, self.perfil, build_status=cf.read("Build_status_map", True, bool))
+        self.ds = DelPhiShared(atoms, self.scale, self.perfil, build_status=cf.read("Build_status_map", True, bool),
+                               build_eps_map=cf.read("Build_epsilon_maps", False, bool))
         self.surf = surfaceFactory().create(cf, self.ds, device)
 
     def buildAnalyticalSurface(self, randDisplacement: float = -1) -> bool:

@@ -58,3 +58,37 @@ def compare_surface(surf, ds, ref, rel_tol=1e-12, vert_tol=1e-9):
         out["area_rel"] = abs(surf.area - ref.area) / abs(ref.area)
         assert out["area_rel"] <= rel_tol
     return out
+
+
+def near_threshold_eps(gpu_eps, ref, grid, near=1e-6):
+    """(#mismatching epsilon-map entries, #of them near a threshold of the oracle).
+
+    Edge (node c, axis a) of a node ray is inside when its midpoint coord(c) + hside lies in an
+    interval [lim1, lim2]; an entry counts as near when an oracle interval end of its ray lies
+    within ``near`` of that midpoint or of coord(c) - hside (the rintp rounding of lim1)."""
+    import oracle as O
+    mism = np.argwhere(gpu_eps != ref.epsmap)
+    if len(mism) == 0:
+        return 0, 0
+    mins = (grid.xmin, grid.ymin, grid.zmin)
+    ns = (grid.nx, grid.ny, grid.nz)
+    # axis -> (ray set, axis of m, axis of n)
+    sets = {0: (0, 1, 2), 2: (4, 0, 1), 1: (5, 0, 2)}
+    cache = {}
+    n_near = 0
+    for k, j, i, a in mism:
+        s, fa, la = sets[int(a)]
+        if s not in cache:
+            cnt, vals = O.ray_hits(ref, s)
+            cache[s] = (cnt, vals, np.concatenate([[0], np.cumsum(cnt.ravel())]))
+        cnt, vals, offs = cache[s]
+        idx = (i, j, k)
+        m, n = idx[fa], idx[la]
+        r = n * cnt.shape[1] + m
+        t = vals[offs[r]:offs[r + 1]]
+        x0 = mins[a]
+        lims = x0 + ((x0 + (ns[a] - 1) * grid.side) - x0) * t
+        c = mins[a] + idx[a] * grid.side
+        if len(lims) and min(np.min(np.abs(lims - (c + grid.hside))), np.min(np.abs(lims - (c - grid.hside)))) < near:
+            n_near += 1
+    return len(mism), n_near

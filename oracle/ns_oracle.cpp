@@ -342,6 +342,14 @@ struct Oracle {
   std::vector<int32_t> pix_pid;  // patch of every hit
   std::vector<int32_t> status;
   std::vector<uint32_t> bits;
+  // epsilon map ((k*ny + j)*nx + i)*3 + axis and ideb map (flag 32); boundary grid points and their
+  // projection (flag 64)
+  std::vector<int32_t> eps;
+  std::vector<uint8_t> ideb;
+  std::vector<int32_t> ibgp, bgp_type, bgp_flag;
+  std::vector<double> scspos, scsnor;
+  int aux_max_dim = 50;
+  bool eps_on() const { return (flags & 32) != 0; }
   double volPanel[3] = {0, 0, 0};
   int flagsum = 0;
   double volume = 0;
@@ -597,6 +605,45 @@ struct Oracle {
     else if (panel == 1) { na = g.ny; nb = g.nx; }
     else { na = g.nz; nb = g.nx; }
     std::vector<std::pair<int64_t, int64_t>> pr;
+    // phase 0 of panels 1 and 2: the epsilon map's node rays along z and y (src/Surface.cpp:6698-6898)
+    if (eps_on() && panel > 0) {
+      flagsum++;
+      const int vc = panel == 1 ? 2 : 1;
+      const int64_t n0 = n_lo(na), n1 = n_hi(na);
+      rays_cast += (n1 - n0) * nb;
+      double pa[3], pb[3];
+      pa[vc] = coord(vc, 0);
+      pb[vc] = coord(vc, Nd(vc) - 1);
+      for (int64_t n = n0; n < n1; n++) {
+        if (panel == 1) pa[1] = Y(n);
+        else pa[2] = Z(n);
+        for (int64_t m = 0; m < nb; m++) {
+          int64_t id = (n * NMAX + m) * numPanels + panel;
+          pairs_of(id, pr);
+          if (pr.empty()) continue;
+          pa[0] = X(m);
+          double dir = pb[vc] - pa[vc];
+          double lvi = 0.0;
+          for (auto& q : pr) {
+            double lim1 = pa[vc] + dir * pix_t[q.first];
+            double lim2 = pa[vc] + dir * pix_t[q.second];
+            lvi += lim2 - lim1;
+            int64_t c1 = (int64_t)rintp((lim1 - mind(vc)) * g.scale);
+            int64_t c2 = (int64_t)rintp((lim2 - mind(vc)) * g.scale);
+            c1 = c1 < 0 ? 0 : (c1 >= Nd(vc) ? Nd(vc) - 1 : c1);
+            c2 = c2 < 0 ? 0 : (c2 >= Nd(vc) ? Nd(vc) - 1 : c2);
+            if (c2 < c1) continue;
+            for (int64_t c = c1; c < c2; c++) {
+              if (coord(vc, c) <= lim2 - g.hside) {
+                if (panel == 1) eps[3 * ((c * g.ny + n) * g.nx + m) + 2] = NS_EPS_INSIDE;
+                else eps[3 * ((n * g.ny + c) * g.nx + m) + 1] = NS_EPS_INSIDE;
+              }
+            }
+          }
+          volPanel[panel] += lvi;
+        }
+      }
+    }
     // phase 0: status map along x (only panel 0 when the status map is built)
     if (panels[0] > 0 && panel == 0) {
       flagsum++;
@@ -629,7 +676,12 @@ struct Oracle {
               if (i2 < i1) continue;
               for (int64_t ix = i1; ix <= i2; ix++) {
                 double xx = X(ix);
-                if (xx <= lim2 && xx >= lim1) status[(n * g.ny + m) * g.nx + ix] = NS_STATUS_INSIDE;
+                const int64_t f = (n * g.ny + m) * g.nx + ix;
+                if (eps_on() && xx <= lim2 - g.hside) eps[3 * f] = NS_EPS_INSIDE;
+                if (xx <= lim2 && xx >= lim1) {
+                  status[f] = NS_STATUS_INSIDE;
+                  if (eps_on()) ideb[f] = 0;
+                }
               }
             }
             lv[(size_t)(n - n0) * nb + m] = lvi;
@@ -783,6 +835,14 @@ struct Oracle {
       cav_size[c] = cv;
       if (cv <= cav_vol) {
         cav_filled[c] = 1;
+        if (eps_on())
+          for (int64_t f : cav_nodes[c]) {
+            for (int a = 0; a < 3; a++) eps[3 * f + a] = NS_EPS_INSIDE;
+            eps[3 * (f - 1)] = NS_EPS_INSIDE;
+            eps[3 * (f - g.nx) + 1] = NS_EPS_INSIDE;
+            eps[3 * (f - plane) + 2] = NS_EPS_INSIDE;
+            ideb[f] = 0;
+          }
         if (flags & 2)
           for (int64_t f : cav_nodes[c]) {
             int64_t k = f / plane, j = (f % plane) / g.nx, i = f % g.nx;
@@ -791,6 +851,139 @@ struct Oracle {
                 for (int di = 0; di < 2; di++) clear_bit(i + di, j + dj, k + dk);
           }
       }
+    }
+  }
+
+  // projectToSphere (src/tools.cpp:1112-1120)
+  static double project_sphere(const double* y, const double* c, double r, double* proj) {
+    double dist = sqrt((y[0] - c[0]) * (y[0] - c[0]) + (y[1] - c[1]) * (y[1] - c[1]) + (y[2] - c[2]) * (y[2] - c[2]));
+    dist = r / dist;
+    for (int d = 0; d < 3; d++) proj[d] = y[d] - c[d];
+    for (int d = 0; d < 3; d++) proj[d] = c[d] + dist * proj[d];
+    return sqrt((proj[0] - y[0]) * (proj[0] - y[0]) + (proj[1] - y[1]) * (proj[1] - y[1]) +
+                (proj[2] - y[2]) * (proj[2] - y[2]));
+  }
+  // projectToCircle (src/ConnollySurface.cpp:5693-5703) with point2plane (src/tools.cpp:277-287)
+  static void project_circle(const double* p, double radius, const double* c, const double* w, double* proj) {
+    const double den = w[0] * w[0] + w[1] * w[1] + w[2] * w[2];
+    const double val = (w[0] * p[0] + w[1] * p[1] + w[2] * p[2]) + w[3];
+    const double cc = val / den;
+    for (int d = 0; d < 3; d++) proj[d] = p[d] - w[d] * cc;
+    for (int d = 0; d < 3; d++) proj[d] = proj[d] - c[d];
+    radius /= sqrt(proj[0] * proj[0] + proj[1] * proj[1] + proj[2] * proj[2]);
+    for (int d = 0; d < 3; d++) proj[d] = c[d] + radius * proj[d];
+  }
+  // projectToTorus (src/ConnollySurface.cpp:5705-5733); the rotation back is the transpose of the
+  // stored inverse frame
+  static double project_torus(const double* y, const double* f, double probe, double* proj) {
+    const double* inv = f + 9;
+    const double* tc = f + 4;
+    double temp[3], pp[3];
+    for (int d = 0; d < 3; d++) temp[d] = y[d] - tc[d];
+    for (int i = 0; i < 3; i++) pp[i] = inv[3 * i] * temp[0] + inv[3 * i + 1] * temp[1] + inv[3 * i + 2] * temp[2];
+    const double zero3[3] = {0., 0., 0.};
+    const double torus_plane[4] = {0., 0., 1., 0.};
+    double major[3];
+    project_circle(pp, f[7], zero3, torus_plane, major);
+    // plane3points (src/tools.cpp:258-274), normalised
+    const double p2[3] = {0., 0., 1.}, p3[3] = {0., 0., -1.};
+    double w[4];
+    w[0] = major[1] * (p2[2] - p3[2]) + p2[1] * (p3[2] - major[2]) + p3[1] * (major[2] - p2[2]);
+    w[1] = major[2] * (p2[0] - p3[0]) + p2[2] * (p3[0] - major[0]) + p3[2] * (major[0] - p2[0]);
+    w[2] = major[0] * (p2[1] - p3[1]) + p2[0] * (p3[1] - major[1]) + p3[0] * (major[1] - p2[1]);
+    w[3] = -(w[0] * major[0] + w[1] * major[1] + w[2] * major[2]);
+    const double nrm = sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+    for (int d = 0; d < 4; d++) w[d] /= nrm;
+    double loc[3];
+    project_circle(pp, probe, major, w, loc);
+    for (int i = 0; i < 3; i++) pp[i] = inv[i] * loc[0] + inv[3 + i] * loc[1] + inv[6 + i] * loc[2];
+    for (int d = 0; d < 3; d++) proj[d] = pp[d] + tc[d];
+    return sqrt((proj[0] - y[0]) * (proj[0] - y[0]) + (proj[1] - y[1]) * (proj[1] - y[1]) +
+                (proj[2] - y[2]) * (proj[2] - y[2]));
+  }
+
+  // Boundary grid points (src/Surface.cpp:1488-1546) and the projection of the external ones
+  // (Surface::projector, src/Surface.cpp:4657-4676; ConnollySurface::getProjection,
+  // src/ConnollySurface.cpp:5822-5912) over the auxiliary grid of buildAuxiliaryGrid
+  // (src/ConnollySurface.cpp:3681-3870).  A point without a feasible projection keeps its own
+  // coordinates (flag 1; the reference's sampled-circle retry for self-intersecting edges is not
+  // restated), one in an empty cell too (flag 2).
+  void boundary_points() {
+    const int64_t NX = g.nx, NY = g.ny, NZ = g.nz;
+    auto E = [&](int64_t i, int64_t j, int64_t k, int l) { return eps[3 * ((k * NY + j) * NX + i) + l]; };
+    for (int64_t iz = 1; iz < NZ; iz++)
+      for (int64_t iy = 1; iy < NY; iy++)
+        for (int64_t ix = 1; ix < NX; ix++) {
+          const int32_t k0 = E(ix, iy, iz, 0);
+          if (k0 != E(ix, iy, iz, 1) || k0 != E(ix, iy, iz, 2) || k0 != E(ix - 1, iy, iz, 0) ||
+              k0 != E(ix, iy - 1, iz, 1) || k0 != E(ix, iy, iz - 1, 2)) {
+            ibgp.push_back((int32_t)ix);
+            ibgp.push_back((int32_t)iy);
+            ibgp.push_back((int32_t)iz);
+            const bool ext = E(ix, iy, iz, 0) == 0 || E(ix, iy, iz, 1) == 0 || E(ix, iy, iz, 2) == 0 ||
+                             E(ix - 1, iy, iz, 0) == 0 || E(ix, iy - 1, iz, 1) == 0 || E(ix, iy, iz - 1, 2) == 0;
+            bgp_type.push_back(ext ? NS_EXTERNAL_BGP : NS_INTERNAL_BGP);
+          }
+        }
+    // auxiliary grid
+    int64_t igrid = NX, mul = 1;
+    while (igrid > aux_max_dim) {
+      mul += 2;
+      int64_t digrid = NX;
+      while (true) {
+        const int64_t fp = (digrid + (mul - 1)) / mul;
+        igrid = fp * mul;
+        if (igrid % 2 == 0) digrid = igrid + 1;
+        else { igrid = fp; break; }
+      }
+    }
+    const double ascale = g.scale / (double)mul, aside = (double)mul / g.scale;
+    const double amin[3] = {g.baricenter[0] - (igrid - 1) * 0.5 * aside, g.baricenter[1] - (igrid - 1) * 0.5 * aside,
+                            g.baricenter[2] - (igrid - 1) * 0.5 * aside};
+    std::vector<std::vector<int32_t>> cells((size_t)(igrid * igrid * igrid));
+    for (int64_t it = 0; it < P.n; it++) {
+      const double* f = P.f64 + NS_PATCH_F64 * it;
+      int64_t lo[3], hi[3];
+      for (int d = 0; d < 3; d++) {
+        lo[d] = (int64_t)rintp(fmax(0., (f[d] - f[3]) - amin[d]) * ascale);
+        hi[d] = (int64_t)rintp(fmax(0., (f[d] + f[3]) - amin[d]) * ascale);
+        if (lo[d] >= igrid) lo[d] = igrid - 1;
+        if (hi[d] >= igrid) hi[d] = igrid - 1;
+      }
+      for (int64_t iz = lo[2]; iz <= hi[2]; iz++)
+        for (int64_t iy = lo[1]; iy <= hi[1]; iy++)
+          for (int64_t ix = lo[0]; ix <= hi[0]; ix++) cells[(iz * igrid + iy) * igrid + ix].push_back((int32_t)it);
+    }
+    const size_t n = bgp_type.size();
+    scspos.assign(3 * n, 0.0);
+    scsnor.assign(3 * n, 0.0);
+    bgp_flag.assign(n, 0);
+    for (size_t q = 0; q < n; q++) {
+      const double y[3] = {X(ibgp[3 * q]), Y(ibgp[3 * q + 1]), Z(ibgp[3 * q + 2])};
+      for (int d = 0; d < 3; d++) scspos[3 * q + d] = y[d];
+      if (bgp_type[q] != NS_EXTERNAL_BGP) { bgp_flag[q] = 3; continue; }
+      int64_t ic[3];
+      bool in = true;
+      for (int d = 0; d < 3; d++) {
+        ic[d] = (int64_t)rintp((y[d] - amin[d]) * ascale);
+        in = in && ic[d] >= 0 && ic[d] < igrid;
+      }
+      if (!in || cells[(ic[2] * igrid + ic[1]) * igrid + ic[0]].empty()) { bgp_flag[q] = 2; continue; }
+      double best = INFINITY;
+      for (int32_t it : cells[(ic[2] * igrid + ic[1]) * igrid + ic[0]]) {
+        const double* f = P.f64 + NS_PATCH_F64 * (int64_t)it;
+        const int kind = P.i32[NS_PATCH_I32 * (int64_t)it];
+        double proj[3], dist;
+        if (kind == NS_POINT) dist = project_sphere(y, f, f[3], proj);
+        else if (kind == NS_FACE_REG || kind == NS_FACE_SING) dist = project_sphere(y, f, P.probe, proj);
+        else dist = project_torus(y, f, P.probe, proj);
+        if (!feasible(P, it, proj)) continue;
+        if (dist < best) {
+          best = dist;
+          for (int d = 0; d < 3; d++) scspos[3 * q + d] = proj[d];
+        }
+      }
+      bgp_flag[q] = best == INFINITY ? 1 : 0;
     }
   }
 
@@ -983,10 +1176,14 @@ struct Oracle {
 
   void run() {
     NMAX = std::max(g.nx, std::max(g.ny, g.nz));
-    panels[0] = (flags & 1) ? 1 : 0;
+    panels[0] = eps_on() ? 3 : ((flags & 1) ? 1 : 0);
     panels[1] = (flags & 2) ? 3 : 0;
     numPanels = panels[0] + panels[1];
-    if (flags & 1) status.assign(g.nx * g.ny * g.nz, NS_STATUS_TEMPORARY_OUT);
+    if (flags & (1 | 32)) status.assign(g.nx * g.ny * g.nz, NS_STATUS_TEMPORARY_OUT);
+    if (eps_on()) {
+      eps.assign(3 * g.nx * g.ny * g.nz, 0);
+      ideb.assign(g.nx * g.ny * g.nz, 1);
+    }
     if (flags & 2) {
       int64_t cnx = (g.nx + 31) >> 5;
       bits.assign(cnx * g.ny * g.nz, ~0u);
@@ -995,10 +1192,11 @@ struct Oracle {
     else {
       pix_off.assign(NMAX * NMAX * std::max(1, numPanels) + 1, 0);
     }
-    int np = (flags & 2) ? 3 : ((flags & 1) ? 1 : 0);
+    int np = ((flags & 2) || eps_on()) ? 3 : ((flags & 1) ? 1 : 0);
     for (int panel = 0; panel < np; panel++) fill_panel(panel);
     volume = flagsum ? g.A * (volPanel[0] + volPanel[1] + volPanel[2]) / flagsum : 0;
-    if ((flags & 4) && (flags & 1)) cavities();
+    if ((flags & 4) && (flags & (1 | 32))) cavities();
+    if (eps_on() && (flags & 64)) boundary_points();
     // vertex assembly and marching cubes (the dense edge-index grids are needed only here)
     if ((flags & 2) && (flags & 8)) {
       assemble();
@@ -1184,7 +1382,8 @@ void nso_free_mesh(void* h) { delete (BlobbyMesh*)h; }
 extern "C" {
 
 // flags: 1 status map, 2 accurate-triangulation rays + insideness, 4 cavity detection/filling,
-//        8 marching cubes, 16 vertex normals (Compute_Vertex_Normals).
+//        8 marching cubes, 16 vertex normals (Compute_Vertex_Normals), 32 epsilon and ideb maps
+//        (Build_epsilon_maps), 64 boundary grid points and their projection (with 32).
 void* nso_run(const NsGrid* g, int64_t n_patches, const double* f64, const int32_t* i32, const double* pool,
               const int8_t* pool_flag, double probe, int flags, double cav_vol, int nthreads) {
   Oracle* o = new Oracle();
@@ -1223,6 +1422,9 @@ int64_t nso_size(void* h, const char* what) {
   if (w == "pix_off") return (int64_t)o->pix_off.size();
   if (w == "pix_t") return (int64_t)o->pix_t.size();
   if (w == "normals") return (int64_t)o->normals.size();
+  if (w == "eps") return (int64_t)o->eps.size();
+  if (w == "ideb") return (int64_t)o->ideb.size();
+  if (w == "bgp_type") return (int64_t)o->bgp_type.size();
   return -1;
 }
 
@@ -1239,6 +1441,13 @@ int nso_copy(void* h, const char* what, void* dst) {
   else if (w == "pix_off") memcpy(dst, o->pix_off.data(), o->pix_off.size() * 8);
   else if (w == "pix_t") memcpy(dst, o->pix_t.data(), o->pix_t.size() * 8);
   else if (w == "normals") memcpy(dst, o->normals.data(), o->normals.size() * 8);
+  else if (w == "eps") memcpy(dst, o->eps.data(), o->eps.size() * 4);
+  else if (w == "ideb") memcpy(dst, o->ideb.data(), o->ideb.size());
+  else if (w == "ibgp") memcpy(dst, o->ibgp.data(), o->ibgp.size() * 4);
+  else if (w == "bgp_type") memcpy(dst, o->bgp_type.data(), o->bgp_type.size() * 4);
+  else if (w == "bgp_flag") memcpy(dst, o->bgp_flag.data(), o->bgp_flag.size() * 4);
+  else if (w == "scspos") memcpy(dst, o->scspos.data(), o->scspos.size() * 8);
+  else if (w == "scsnor") memcpy(dst, o->scsnor.data(), o->scsnor.size() * 8);
   else return -1;
   return 0;
 }

@@ -19,6 +19,8 @@ ACCURATE_TRIANGULATION = 2
 CAVITIES = 4
 TRIANGULATE = 8
 NORMALS = 16
+EPSMAP = 32
+BGP = 64
 
 _lib = None
 
@@ -70,9 +72,10 @@ def lib() -> ctypes.CDLL:
 class OracleResult:
     """Products of one oracle run (arrays copied out, native handle freed)."""
 
-    def __init__(self, handle, grid):
+    def __init__(self, handle, grid, flags: int = 0):
         L = lib()
         self.grid = grid
+        self.flags = flags
 
         def arr(name, dtype):
             n = L.nso_size(handle, name.encode())
@@ -101,6 +104,27 @@ class OracleResult:
         self.normals = arr("normals", np.float64).reshape(-1, 3)
         self.pix_off = arr("pix_off", np.int64)
         self.pix_t = arr("pix_t", np.float64)
+        # epsilon / ideb maps and boundary grid points
+        self.epsmap = arr("eps", np.int32)
+        if len(self.epsmap):
+            self.epsmap = self.epsmap.reshape(grid.nz, grid.ny, grid.nx, 3)
+        ideb = arr("ideb", np.uint8)
+        self.idebmap = ideb.reshape(grid.nz, grid.ny, grid.nx).astype(bool) if len(ideb) else ideb
+        nb = max(L.nso_size(handle, b"bgp_type"), 0)
+        self.nbgp = nb
+
+        def fixed(name, dtype, k):
+            a = np.zeros(nb * k, dtype)
+            if nb:
+                L.nso_copy(handle, name.encode(), a.ctypes.data)
+            return a.reshape(nb, k) if k > 1 else a
+
+        self.ibgp = fixed("ibgp", np.int32, 3)
+        self.bgp_type = fixed("bgp_type", np.int32, 1)
+        if flags & BGP:
+            self.scspos = fixed("scspos", np.float64, 3)
+            self.scsnor = fixed("scsnor", np.float64, 3)
+            self.bgp_flag = fixed("bgp_flag", np.int32, 1)
 
 
 def run(grid, patches, flags: int = STATUS | ACCURATE_TRIANGULATION | CAVITIES | TRIANGULATE, cav_vol: float = 0.0,
@@ -111,7 +135,7 @@ def run(grid, patches, flags: int = STATUS | ACCURATE_TRIANGULATION | CAVITIES |
     h = L.nso_run(ctypes.byref(grid), p.n, p.f64.ctypes.data, p.i32.ctypes.data, p.pool.ctypes.data,
                   p.pool_flag.ctypes.data, p.probe, flags, cav_vol, threads)
     try:
-        return OracleResult(h, grid)
+        return OracleResult(h, grid, flags)
     finally:
         L.nso_free(h)
 
@@ -120,9 +144,13 @@ def ray_hits(res: OracleResult, ray_set: int) -> tuple[np.ndarray, np.ndarray]:
     """Per-ray sorted hits of one ray set, laid out like the GPU dump: (counts[na, nb], values)."""
     g = res.grid
     nmax = max(g.nx, g.ny, g.nz)
-    nb, na = ((g.ny, g.nz), (g.ny, g.nz), (g.nx, g.ny), (g.nx, g.nz))[ray_set]
+    nb, na = ((g.ny, g.nz), (g.ny, g.nz), (g.nx, g.ny), (g.nx, g.nz), (g.nx, g.ny), (g.nx, g.nz))[ray_set]
     npan = (len(res.pix_off) - 1) // (nmax * nmax)
-    panel_idx = ray_set if npan == 4 else ray_set - 1
+    # oracle panel order: the node-ray panels (1, or 3 with the epsilon maps), then the three
+    # accurate-triangulation panels
+    node_panels = 3 if res.flags & EPSMAP else (1 if res.flags & STATUS else 0)
+    panel_idx = {0: 0, 4: 1, 5: 2}[ray_set] if ray_set in (0, 4, 5) else node_panels + ray_set - 1
+    assert panel_idx < npan, "ray set not cast by this oracle run"
     n_idx = np.arange(na)[:, None]
     m_idx = np.arange(nb)[None, :]
     pid = (n_idx * nmax + m_idx) * npan + panel_idx

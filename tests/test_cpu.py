@@ -701,3 +701,76 @@ def test_blobby_oracle_mesh_is_closed_and_matches_field(native_lib, oracle_mod):
         f += np.exp(-2.5 * (d2 / a[3] ** 2 - 1))
     vol_nodes = (f > 1.0).sum() * g.side ** 3
     assert abs(r.volume - vol_nodes) <= 0.03 * vol_nodes
+
+
+def test_oracle_epsilon_map_rules(oracle_mod):
+    """Epsilon map of the oracle against the rule it restates, checked from the oracle's own ray
+    hits: the edge from node c along an axis is inside exactly when its midpoint coord(c) + hside
+    lies in an interval of its node ray (src/Surface.cpp:6645-6680, 6786-6795, 6887-6896); the ideb
+    map is the complement of the status map's inside nodes; the boundary grid points are the nodes
+    whose six edge codes differ (src/Surface.cpp:1488-1546), all external with one inside code."""
+    atoms, ds, surf = _surface(60, 3, 2.0, 70.0)
+    O = oracle_mod
+    ref = O.run(ds.grid, surf.patches, flags=O.STATUS | O.EPSMAP | O.BGP)
+    g = ds.grid
+    eps = ref.epsmap
+    assert set(np.unique(eps).tolist()) == {0, 5}
+    mins = (g.xmin, g.ymin, g.zmin)
+    ns = (g.nx, g.ny, g.nz)
+    n_checked = n_tie = 0
+    for axis, s, fa, la in ((0, 0, 1, 2), (2, 4, 0, 1), (1, 5, 0, 2)):
+        cnt, vals = O.ray_hits(ref, s)
+        offs = np.concatenate([[0], np.cumsum(cnt.ravel())])
+        mid = mins[axis] + np.arange(ns[axis]) * g.side + g.hside
+        x0 = mins[axis]
+        dirl = (x0 + (ns[axis] - 1) * g.side) - x0
+        for n in range(cnt.shape[0]):
+            for m in range(cnt.shape[1]):
+                r = n * cnt.shape[1] + m
+                t = vals[offs[r]:offs[r + 1]]
+                want = np.zeros(ns[axis], bool)
+                near = np.zeros(ns[axis], bool)
+                if len(t) and len(t) % 2 == 0:
+                    for q in range(0, len(t), 2):
+                        if abs(t[q + 1] - t[q]) < 1e-8:
+                            continue
+                        l1, l2 = x0 + dirl * t[q], x0 + dirl * t[q + 1]
+                        want |= (mid >= l1) & (mid <= l2)
+                        near |= (np.abs(mid - l1) < 1e-9) | (np.abs(mid - l2) < 1e-9)
+                idx = [0, 0, 0]
+                idx[fa], idx[la] = m, n
+                line = [slice(None)] * 3
+                line[2 - fa], line[2 - la] = m, n  # eps is indexed [k, j, i]
+                got = eps[tuple(line) + (axis,)] == 5
+                ok = (got == want) | near
+                assert ok.all(), f"axis {axis} ray (m={m}, n={n}): {np.flatnonzero(~ok)}"
+                n_checked += len(got)
+                n_tie += int(near.sum())
+    assert n_checked == 3 * g.nx * g.ny * g.nz and n_tie < 10
+    # ideb: the complement of the inside nodes (no cavity filled here)
+    np.testing.assert_array_equal(ref.idebmap, ref.status != -1)
+    # boundary grid points: the nodes whose six edge codes differ, in (z, y, x) scan order
+    e = eps
+    c0 = e[1:, 1:, 1:, 0]
+    diff = (c0 != e[1:, 1:, 1:, 1]) | (c0 != e[1:, 1:, 1:, 2]) | (c0 != e[1:, 1:, :-1, 0]) | \
+           (c0 != e[1:, :-1, 1:, 1]) | (c0 != e[:-1, 1:, 1:, 2])
+    kji = np.argwhere(diff) + 1
+    np.testing.assert_array_equal(ref.ibgp, kji[:, ::-1])
+    assert (ref.bgp_type == 1).all() and ref.nbgp > 0
+
+
+def test_oracle_bgp_projection_single_atom(oracle_mod):
+    """One atom: the SES is its sphere, and every boundary grid point projects radially onto it."""
+    O = oracle_mod
+    ds = nb.DelPhiShared(np.array([[0.3, -0.2, 0.1, 1.7]]), 4.0, 50.0)
+    ps = nb.build_ses_patches(ds.atoms, 1.4)
+    ref = O.run(ds.grid, ps, flags=O.STATUS | O.EPSMAP | O.BGP)
+    assert ref.nbgp > 0 and (ref.bgp_flag == 0).all()
+    c = ds.atoms[0, :3]
+    y = np.stack([ds.x[ref.ibgp[:, 0]], ds.y[ref.ibgp[:, 1]], ds.z[ref.ibgp[:, 2]]], 1)
+    np.testing.assert_allclose(np.linalg.norm(ref.scspos - c, axis=1), 1.7, atol=1e-12)
+    u = (y - c) / np.linalg.norm(y - c, axis=1)[:, None]
+    np.testing.assert_allclose(ref.scspos, c + 1.7 * u, atol=1e-12)
+    assert not ref.scsnor.any()
+    # every point lies within one grid diagonal of the sphere
+    assert np.abs(np.linalg.norm(y - c, axis=1) - 1.7).max() <= np.sqrt(3) * ds.side
