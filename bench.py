@@ -425,10 +425,14 @@ def run_ensemble(args, world: int, rank: int, local: int) -> None:
         return nv.value, nt.value
 
     def timed(precision: int, steps: int) -> float:
+        # an NVTX range per timed region ("timed_fp64" / "timed_mixed") lets a profiler capture
+        # exactly the timed launches (ncu --nvtx --nvtx-include "timed_mixed/")
+        torch.cuda.nvtx.range_push("timed_" + ("fp64" if precision == 0 else "mixed"))
         N.check(L.nsg_event_record(ctx, 0), "event")
         for _ in range(steps):
             step(precision)
         N.check(L.nsg_event_record(ctx, 1), "event")
+        torch.cuda.nvtx.range_pop()
         ms = ctypes.c_double()
         N.check(L.nsg_event_elapsed(ctx, 0, 1, ctypes.byref(ms)), "elapsed")
         return ms.value / steps

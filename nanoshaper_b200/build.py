@@ -20,7 +20,7 @@ LIB_DIR = PKG / "lib"
 BUILD_DIR = PKG / "_build"
 LIB = LIB_DIR / "libnsgpu.so"
 
-CU_SOURCES = ["capi.cu", "kernels/trace.cu", "kernels/trace_mixed.cu", "kernels/cavity.cu", "kernels/mc.cu", "kernels/reduce.cu", "kernels/chain.cu", "kernels/blobby.cu", "kernels/epsmap.cu", "noalloc.cu"]
+CU_SOURCES = ["capi.cu", "kernels/trace.cu", "kernels/trace_mixed.cu", "kernels/trace_mixed_torus.cu", "kernels/cavity.cu", "kernels/mc.cu", "kernels/reduce.cu", "kernels/chain.cu", "kernels/blobby.cu", "kernels/epsmap.cu", "noalloc.cu"]
 CPP_SOURCES = ["host/grid.cpp", "host/ses_builder.cpp", "host/skin_builder.cpp", "host/grad.cpp", "host/formats.cpp"]
 
 NVCC_FLAGS = [

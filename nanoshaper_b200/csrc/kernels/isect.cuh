@@ -29,6 +29,10 @@ struct TraceCtx {
 template <int PN>
 void launch_isect_mixed(const TraceCtx& C, const CandOut& co, const HitStore& hs, const TuneParams& tp,
                         cudaStream_t s);
+// The torus launch of launch_isect_mixed (trace_mixed_torus.cu, built without fused multiply-adds).
+template <int PN>
+void launch_isect_mixed_torus(const TraceCtx& C, const CandOut& co, const HitStore& hs, const TuneParams& tp,
+                              cudaStream_t s);
 // Mixed-precision skin cell launch of one panel (trace_mixed.cu).
 template <int PN>
 void launch_isect_quad_mixed(const TraceCtx& C, const CandOut& co, const HitStore& hs, const TuneParams& tp,
@@ -104,19 +108,20 @@ __device__ __forceinline__ int intersect_mixed(const double* f, int kind, int fi
     if (ctr) atomicAdd(ctr + kCntFbSphere, 1ull);
     return kDefer;
   }
-  float s32 = sqrtf(disc);
-  double disc64 = r * r - dx64 * dx64 - dy64 * dy64;
-  double sd = (double)s32;
-  sd = sd + (disc64 - sd * sd) * (double)(0.5f / s32);
-  double xs[4];
+  double xs[4], ts[4];
   int nx = 0;
   const double cv = f[vc];
   if (kTorus) {
-    const double x_in = cv - sd;
-    double orig1[3];
-    orig1[fd] = pa[fd];
-    orig1[ld] = pa[ld];
-    orig1[vc] = x_in;
+    // the double-precision path's clipping-sphere entry and quartic, operation for operation (the
+    // torus kernels are built without fused multiply-adds, trace_mixed_torus.cu), so that an
+    // undeferred root is the FP64 path's to the bit: the reference's solver is ill-conditioned
+    // for some rays (its resolvent approximations), where a different rounding moves a root by
+    // up to 1e-4 A
+    double tsph[2];
+    if (!ray_sphere_axis<vc>(pa, ray_dir, f, r, &tsph[0], &tsph[1])) return 0;
+    const double t0 = tsph[0];
+    double orig1[3] = {pa[0], pa[1], pa[2]};
+    orig1[vc] += t0 * ray_dir;
     double B, C, D, E;
     torus_coeffs_f64(f, P.probe, vc, orig1, &B, &C, &D, &E);
     double roots[4];
@@ -133,18 +138,30 @@ __device__ __forceinline__ int intersect_mixed(const double* f, int kind, int fi
         return kDefer;
       }
       if (root < 0) continue;
-      double px = x_in + root;
-      double e0 = f[fd] - pa[fd], e1 = f[ld] - pa[ld], e2 = cv - px;
-      double dd = e0 * e0 + e1 * e1 + e2 * e2;
+      double point[3] = {orig1[0], orig1[1], orig1[2]};
+      point[vc] += root;
+      double dd = (f[0] - point[0]) * (f[0] - point[0]) + (f[1] - point[1]) * (f[1] - point[1]) +
+                  (f[2] - point[2]) * (f[2] - point[2]);
       if (fabs(dd - r2) < 1e-9) {
         if (ctr) atomicAdd(ctr + kCntFbRoot, 1ull);
         return kDefer;
       }
-      if (dd < r2) xs[nx++] = px;
+      if (dd < r2) {
+        ts[nx] = t0 + root / ray_dir;
+        xs[nx] = pa[vc] + ts[nx] * ray_dir;
+        nx++;
+      }
     }
   } else {
+    // the chord half-length in FP32, one FP64 Newton correction against the FP64 discriminant
+    const float s32 = sqrtf(disc);
+    const double disc64 = r * r - dx64 * dx64 - dy64 * dy64;
+    double sd = (double)s32;
+    sd = sd + (disc64 - sd * sd) * (double)(0.5f / s32);
     xs[0] = cv - sd;
     xs[1] = cv + sd;
+    ts[0] = (xs[0] - pa[vc]) * inv_dir;
+    ts[1] = (xs[1] - pa[vc]) * inv_dir;
     nx = 2;
   }
   int out = 0;
@@ -157,8 +174,7 @@ __device__ __forceinline__ int intersect_mixed(const double* f, int kind, int fi
     p64[fd] = pa[fd];
     p64[ld] = pa[ld];
     p64[vc] = xs[i];
-    if (feasible_mixed<kTorus>(f, kind, first, cnt, P.pool, P.pool32, P.flag, pl, p64))
-      t[out++] = (xs[i] - pa[vc]) * inv_dir;
+    if (feasible_mixed<kTorus>(f, kind, first, cnt, P.pool, P.pool32, P.flag, pl, p64)) t[out++] = ts[i];
   }
   return out;
 }
@@ -341,9 +357,10 @@ __device__ __forceinline__ int intersect_tri_f64(const double* f, const double* 
 
 // Mixed-precision triangle test: the barycentric coordinates of the ray's foot in the triangle
 // from the transverse offsets in FP32 (with the ray along an axis they need only the triangle's
-// and the origin's transverse coordinates relative to v0); decisions within 1e-4 of a bound, and a
-// determinant near the reference's EPS cut, are taken by the double-precision test instead.  The
-// hit is v0 + u e1 + v e2 along the axis in FP64.
+// and the origin's transverse coordinates relative to v0) reject the candidates that miss by more
+// than 1e-4 (in barycentric units); every other candidate, and every one with a determinant near
+// the reference's EPS cut, is tested in double precision, so that no FP32 rounding reaches an
+// accepted hit (which keeps the ray-cast volume and area smooth in the vertices).
 template <int PN>
 __device__ __forceinline__ int intersect_tri_mixed(const double* f, const double* pa, double dirl, double* t) {
   constexpr int vc = Ax<PN>::vc;
@@ -354,22 +371,15 @@ __device__ __forceinline__ int intersect_tri_mixed(const double* f, const double
   const float D = e1b * e2a - e1a * e2b;
   const float det = D * (float)dirl;
   constexpr float kBand = 1e-4f;
-  bool undecided = fabsf(det) < 4e-5f;
-  float u = 0.f, v = 0.f;
-  if (!undecided) {
+  if (fabsf(det) >= 4e-5f) {
     const float inv = 1.f / D;
-    u = (tb * e2a - ta * e2b) * inv;
-    v = (ta * e1b - tb * e1a) * inv;
+    const float u = (tb * e2a - ta * e2b) * inv;
+    const float v = (ta * e1b - tb * e1a) * inv;
     const float w = 1.f - u - v;
-    const float lo = fminf(u, fminf(v, w));
-    if (lo < -kBand) return 0;
     // the reference's bounds: u <= 1 and u + v <= 1 as well (implied by w >= 0 and v >= 0)
-    undecided = lo <= kBand;
+    if (fminf(u, fminf(v, w)) < -kBand) return 0;
   }
-  if (undecided) return intersect_tri_f64<PN>(f, pa, dirl, t);
-  const double x = f[vc] + (double)u * (f[3 + vc] - f[vc]) + (double)v * (f[6 + vc] - f[vc]);
-  *t = (x - pa[vc]) / dirl;
-  return 1;
+  return intersect_tri_f64<PN>(f, pa, dirl, t);
 }
 
 // One thread per skin or triangle candidate (in the sphere list): intersection, feasibility, hit

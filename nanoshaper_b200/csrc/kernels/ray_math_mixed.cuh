@@ -4,11 +4,13 @@
 //   * sphere hits: the discriminant and square root in FP32 on local offsets, then one FP64
 //     Newton correction of the square root against the FP64 discriminant; near-tangent rays
 //     (|disc| below a threshold) fall back to the double-precision test;
-//   * torus hits: the clipping-sphere entry as for spheres; the quartic root isolation stays in
-//     FP64 (the double-precision solver, its decisions guarded: a discriminant, resolvent root or
-//     square-root argument within rounding of its threshold defers the candidate); measured on
-//     B200, an FP32 isolation followed by FP64 Newton polishing costs more FP64 issue than the
-//     FP64 solver itself;
+//   * torus hits: the FP32 discriminant only screens near-tangent rays; the clipping-sphere entry
+//     and the quartic are the double-precision path's operations (built without fused
+//     multiply-adds, its decisions guarded: a discriminant, resolvent root or square-root argument
+//     within rounding of its threshold defers the candidate), because the reference's solver is
+//     ill-conditioned for some rays and another rounding would move their roots by up to 1e-4 A;
+//     measured on B200, an FP32 isolation followed by FP64 Newton polishing costs more FP64 issue
+//     than the FP64 solver itself;
 //   * feasibility: plane and sphere tests in FP32 on local coordinates; a test whose FP32 value is
 //     within a tolerance of zero is re-evaluated in FP64 from the double-precision pool.
 // Hit points therefore carry FP64 accuracy and the accept/reject decisions equal the

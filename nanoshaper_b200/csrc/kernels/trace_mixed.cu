@@ -1,5 +1,6 @@
-// Mixed-precision ray-patch intersection kernels, compiled with fused multiply-adds (the build
-// gives this file --fmad=true; every other device file is compiled with --fmad=false).
+// Mixed-precision ray-patch intersection kernels of spheres and skin cells, compiled with fused
+// multiply-adds (the build gives this file --fmad=true; every other device file, the mixed torus
+// kernels of trace_mixed_torus.cu included, is compiled with --fmad=false).
 #include "isect.cuh"
 
 namespace nsg {
@@ -9,7 +10,7 @@ void launch_isect_mixed(const TraceCtx& C, const CandOut& co, const HitStore& hs
                         cudaStream_t s) {
   const int ig = sm_count() * tp.isect_bpsm, it = tp.isect_threads;
   k_isect_mixed<PN, false><<<ig, it, 0, s>>>(C, co, hs);
-  k_isect_mixed<PN, true><<<ig, it, 0, s>>>(C, co, hs);
+  launch_isect_mixed_torus<PN>(C, co, hs, tp, s);
 }
 
 template <int PN>

@@ -1384,6 +1384,19 @@ extern "C" {
 // flags: 1 status map, 2 accurate-triangulation rays + insideness, 4 cavity detection/filling,
 //        8 marching cubes, 16 vertex normals (Compute_Vertex_Normals), 32 epsilon and ideb maps
 //        (Build_epsilon_maps), 64 boundary grid points and their projection (with 32).
+void* nso_run_ex(const NsGrid* g, int64_t n_patches, const double* f64, const int32_t* i32, const double* pool,
+                 const int8_t* pool_flag, double probe, int flags, double cav_vol, int nthreads, int aux_max_dim) {
+  Oracle* o = new Oracle();
+  o->g = *g;
+  o->P = {n_patches, f64, i32, pool, pool_flag, probe};
+  o->flags = flags;
+  o->cav_vol = cav_vol;
+  o->nthreads = nthreads;
+  o->aux_max_dim = aux_max_dim;
+  o->run();
+  return o;
+}
+
 void* nso_run(const NsGrid* g, int64_t n_patches, const double* f64, const int32_t* i32, const double* pool,
               const int8_t* pool_flag, double probe, int flags, double cav_vol, int nthreads) {
   Oracle* o = new Oracle();
@@ -1421,6 +1434,7 @@ int64_t nso_size(void* h, const char* what) {
   if (w == "cav_size") return (int64_t)o->cav_size.size();
   if (w == "pix_off") return (int64_t)o->pix_off.size();
   if (w == "pix_t") return (int64_t)o->pix_t.size();
+  if (w == "pix_pid") return (int64_t)o->pix_pid.size();
   if (w == "normals") return (int64_t)o->normals.size();
   if (w == "eps") return (int64_t)o->eps.size();
   if (w == "ideb") return (int64_t)o->ideb.size();
@@ -1440,6 +1454,7 @@ int nso_copy(void* h, const char* what, void* dst) {
   else if (w == "cav_filled") memcpy(dst, o->cav_filled.data(), o->cav_filled.size() * 4);
   else if (w == "pix_off") memcpy(dst, o->pix_off.data(), o->pix_off.size() * 8);
   else if (w == "pix_t") memcpy(dst, o->pix_t.data(), o->pix_t.size() * 8);
+  else if (w == "pix_pid") memcpy(dst, o->pix_pid.data(), o->pix_pid.size() * 4);
   else if (w == "normals") memcpy(dst, o->normals.data(), o->normals.size() * 8);
   else if (w == "eps") memcpy(dst, o->eps.data(), o->eps.size() * 4);
   else if (w == "ideb") memcpy(dst, o->ideb.data(), o->ideb.size());

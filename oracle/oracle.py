@@ -40,6 +40,9 @@ def lib() -> ctypes.CDLL:
         L.nso_run.restype = P
         L.nso_run.argtypes = [P, ctypes.c_int64, P, P, P, P, ctypes.c_double, ctypes.c_int, ctypes.c_double,
                               ctypes.c_int]
+        L.nso_run_ex.restype = P
+        L.nso_run_ex.argtypes = [P, ctypes.c_int64, P, P, P, P, ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                                 ctypes.c_int, ctypes.c_int]
         L.nso_scalar.restype = ctypes.c_double
         L.nso_scalar.argtypes = [P, ctypes.c_char_p]
         L.nso_size.restype = ctypes.c_int64
@@ -104,6 +107,7 @@ class OracleResult:
         self.normals = arr("normals", np.float64).reshape(-1, 3)
         self.pix_off = arr("pix_off", np.int64)
         self.pix_t = arr("pix_t", np.float64)
+        self.pix_pid = arr("pix_pid", np.int32)
         # epsilon / ideb maps and boundary grid points
         self.epsmap = arr("eps", np.int32)
         if len(self.epsmap):
@@ -128,12 +132,13 @@ class OracleResult:
 
 
 def run(grid, patches, flags: int = STATUS | ACCURATE_TRIANGULATION | CAVITIES | TRIANGULATE, cav_vol: float = 0.0,
-        threads: int = 1) -> OracleResult:
-    """Runs the CPU restatement on a grid (NsGrid ctypes struct) and a PatchSet."""
+        threads: int = 1, aux_grid_dim: int = 50) -> OracleResult:
+    """Runs the CPU restatement on a grid (NsGrid ctypes struct) and a PatchSet; aux_grid_dim is
+    Max_ses_patches_auxiliary_grid_size of the boundary-point projection."""
     L = lib()
     p = patches
-    h = L.nso_run(ctypes.byref(grid), p.n, p.f64.ctypes.data, p.i32.ctypes.data, p.pool.ctypes.data,
-                  p.pool_flag.ctypes.data, p.probe, flags, cav_vol, threads)
+    h = L.nso_run_ex(ctypes.byref(grid), p.n, p.f64.ctypes.data, p.i32.ctypes.data, p.pool.ctypes.data,
+                     p.pool_flag.ctypes.data, p.probe, flags, cav_vol, threads, aux_grid_dim)
     try:
         return OracleResult(h, grid, flags)
     finally:

@@ -59,7 +59,7 @@ def test_epsmap_fixture_1crn_fp64(native_lib, oracle_mod):
     surf, ds = ns.surf, ns.ds
     assert surf.auxGridDim == 1000
     surf.getSurf(True, True, 30.0)
-    ref = oracle_mod.run(ds.grid, surf.patches, cav_vol=30.0,
+    ref = oracle_mod.run(ds.grid, surf.patches, cav_vol=30.0, aux_grid_dim=1000,
                          flags=oracle_mod.STATUS | oracle_mod.ACCURATE_TRIANGULATION | oracle_mod.CAVITIES |
                          oracle_mod.EPSMAP | oracle_mod.BGP)
     figs = _check(surf, ds, ref)
@@ -84,7 +84,7 @@ def test_epsmap_2000_matches_oracle(precision, atoms_2000, native_lib, oracle_mo
     surf.build()
     assert surf.auxGridDim == 50
     surf.getSurf(True, True, 10.0, keep_hits=True)
-    ref = oracle_mod.run(ds.grid, surf.patches, cav_vol=10.0, threads=8,
+    ref = oracle_mod.run(ds.grid, surf.patches, cav_vol=10.0, threads=8, aux_grid_dim=50,
                          flags=oracle_mod.STATUS | oracle_mod.ACCURATE_TRIANGULATION | oracle_mod.CAVITIES |
                          oracle_mod.EPSMAP | oracle_mod.BGP)
     # the node rays of the epsilon map (ray sets 4, 5): same hit counts as the oracle
