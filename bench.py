@@ -64,6 +64,13 @@ STAGES = ("bin", "trace", "overflow", "cavity", "vertex", "mc", "cand", "isect",
 # (smsp__sass_thread_inst_executed_op_{dadd,dmul,dfma,fadd,fmul,ffma}_pred_on.sum) on the
 # 64-structure conformer ensemble and divided by its candidate counts.
 FLOPS_PER_CANDIDATE = {"torus": {"fp64": 312.0, "fp32": 35.0}, "sphere": {"fp64": 26.0, "fp32": 74.0}}
+# Algorithmic operations per candidate: the oracle's operation model (oracle/oracle.py OP_MODEL:
+# adds and multiplies of doubles, FMA = 2; square roots, divisions and the resolvent's cube roots,
+# arccos and cos apart) summed over the branches the double-precision path takes, per candidate of
+# each kind, on 16 structures of the 64-structure ensemble (10.0 M torus and 9.8 M sphere
+# candidates; the model is frozen here, the ncu instruction counts above are reported next to it).
+OPS_PER_CANDIDATE = {"torus": {"flops": 180.0, "sqrt": 5.10, "div": 4.81, "cbrt": 1.37, "acos": 0.20, "cos": 0.20},
+                     "sphere": {"flops": 73.8, "sqrt": 1.0, "div": 2.0}}
 # DRAM bytes (read + written) of the mixed intersection launches per candidate, from an ncu capture
 # of the 64-structure ensemble (the ray set of panel 1: 283 MB for the sphere launch, 224 MB for the
 # torus launch, 5 MB for the deferred ones, over its 19.9 M candidates)
@@ -449,8 +456,14 @@ def run_ensemble(args, world: int, rank: int, local: int) -> None:
     # double-precision batch: reference numbers for the volume / area comparison
     step(0)
     vol64, area64 = results()
-    # per-stage kernel times of the measured precision from one profiled pass
+    # per-stage kernel times of the measured precision from one profiled pass, with the ray sets
+    # one after another so that each kernel's event interval holds that kernel alone
     step(prec)
+    tun = (ctypes.c_int32 * 5)()
+    N.check(L.nsg_get_tuning(ctx, tun, 5), "tuning")
+    serial = (ctypes.c_int32 * 5)(*tun)
+    serial[3] = 0
+    N.check(L.nsg_set_tuning(ctx, serial, 5), "tuning")
     N.check(L.nsg_profile(ctx, 1), "profile")
     step(prec)
     stage_ms = np.zeros(12)
@@ -459,6 +472,7 @@ def run_ensemble(args, world: int, rank: int, local: int) -> None:
     counters = np.zeros(8, np.int64)
     L.nsg_trace_counters(ctx, counters.ctypes.data, 8)
     N.check(L.nsg_profile(ctx, 0), "profile")
+    N.check(L.nsg_set_tuning(ctx, tun, 5), "tuning")
 
     for _ in range(args.warmup):
         nv, nt = step(prec)
@@ -560,10 +574,14 @@ def run_ensemble(args, world: int, rank: int, local: int) -> None:
     peaks = load_peaks()
     stage_times = {STAGES[i]: float(stage_ms[i]) for i in range(len(STAGES))}
     # The dominant kernels are the intersection kernels (the largest share of the trace stage),
-    # bound by FP64 arithmetic: achieved = operation model x candidates / their event-timed time,
-    # against the FP64 rate of this GPU measured live with FMA chains.
+    # bound by FP64 arithmetic: achieved = the algorithmic operation model (OPS_PER_CANDIDATE) x
+    # candidates / their event-timed time, against the FP64 rate of this GPU measured live with FMA
+    # chains; the executed-instruction count from ncu (FLOPS_PER_CANDIDATE) is reported beside it.
     n_tor = int(counters[1])
     n_sph = int(counters[0]) - n_tor
+    flops_model = n_tor * OPS_PER_CANDIDATE["torus"]["flops"] + n_sph * OPS_PER_CANDIDATE["sphere"]["flops"]
+    special = {k: n_tor * OPS_PER_CANDIDATE["torus"].get(k, 0.0) + n_sph * OPS_PER_CANDIDATE["sphere"].get(k, 0.0)
+               for k in ("sqrt", "div", "cbrt", "acos", "cos")}
     flops64 = n_tor * FLOPS_PER_CANDIDATE["torus"]["fp64"] + n_sph * FLOPS_PER_CANDIDATE["sphere"]["fp64"]
     flops32 = n_tor * FLOPS_PER_CANDIDATE["torus"]["fp32"] + n_sph * FLOPS_PER_CANDIDATE["sphere"]["fp32"]
     isect_s = stage_times["isect"] / 1000.0
@@ -572,12 +590,18 @@ def run_ensemble(args, world: int, rank: int, local: int) -> None:
     N.check(L.nsg_fp_peak(pctx.handle, 0, ctypes.byref(pk64)), "fp64 peak")
     N.check(L.nsg_fp_peak(pctx.handle, 1, ctypes.byref(pk32)), "fp32 peak")
     pctx.close()
+    ach_model = flops_model / isect_s / 1e12 if isect_s > 0 else 0.0
     ach64 = flops64 / isect_s / 1e12 if isect_s > 0 else 0.0
     ach32 = flops32 / isect_s / 1e12 if isect_s > 0 else 0.0
     # the memory-side figure of the trace stage's fill kernel (bit grids, interval sums, pairs)
     fill_bytes = 3 * 2 * 4 * nwords + 8 * rays + 16 * nv
-    roofline = {"bound": "fp64", "kernel": "k_isect (ray-patch intersection, 4 ray sets)", "achieved": ach64,
-                "peak": pk64.value / 1e12, "unit": "TFLOP/s", "frac": ach64 / (pk64.value / 1e12),
+    roofline = {"bound": "fp64", "kernel": "k_isect (ray-patch intersection, 4 ray sets)", "achieved": ach_model,
+                "peak": pk64.value / 1e12, "unit": "TFLOP/s", "frac": ach_model / (pk64.value / 1e12),
+                "work": "algorithmic operation model of the oracle (OPS_PER_CANDIDATE) x the step's candidates; "
+                        "isect time from the profiled pass with the ray sets run one after another",
+                "ops_per_step": {"flops": flops_model, **special},
+                "executed": {"note": "ncu-counted FP64/FP32 instructions per candidate (FLOPS_PER_CANDIDATE)",
+                             "fp64_tflops": ach64, "fp64_frac": ach64 / (pk64.value / 1e12)},
                 "traffic": (n_tor + n_sph) * ISECT_DRAM_BYTES_PER_CANDIDATE,
                 "traffic_note": "DRAM bytes of the step's intersection launches: ncu-measured bytes per candidate "
                                 "on the 64-structure ensemble x this step's candidates",

@@ -180,8 +180,11 @@ int nsg_batch_results(nsg_ctx* ctx, double* volumes, double* areas);
 
 /* ---- launch-shape tuning (no counterpart in the reference) ----
  * params: [intersection threads per block (64..256), intersection blocks per SM (1..64),
- * candidate-kernel threads per block (32..256)].  nsg_autotune times `reps` ray casts of the
- * current batch per candidate shape and keeps the fastest in the context. */
+ * candidate-kernel threads per block (32..256), and optionally (n >= 4) the ray sets on concurrent
+ * streams (1, default) or not, and (n >= 5) the torus candidates split by resolvent branch before
+ * the solve (1, default) or not; results do not depend on any of them].  nsg_autotune times
+ * `reps` ray casts of the current batch per candidate shape and keeps the fastest in the
+ * context. */
 int nsg_set_tuning(nsg_ctx* ctx, const int32_t* params, int n);
 int nsg_get_tuning(nsg_ctx* ctx, int32_t* params, int n);
 int nsg_autotune(nsg_ctx* ctx, int flags, int precision, int reps, double* best_ms);

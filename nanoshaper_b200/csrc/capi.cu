@@ -101,7 +101,8 @@ struct nsg_ctx {
   // wavefront tracing: candidate lists and the slot-major hit store
   // per ray set (slot s when the ray sets run on their own streams, slot 0 otherwise)
   DevBuf cand_sph[nsg::kRaySets], cand_tor[nsg::kRaySets], hit_t[nsg::kRaySets], hit_cnt[nsg::kRaySets],
-      def_sph[nsg::kRaySets], def_tor[nsg::kRaySets], hit_pid[nsg::kRaySets];
+      def_sph[nsg::kRaySets], def_tor[nsg::kRaySets], hit_pid[nsg::kRaySets], tsplit_a[nsg::kRaySets],
+      tsplit_b[nsg::kRaySets];
   bool concurrent_sets = true;
   cudaStream_t set_stream[nsg::kRaySets] = {};
   cudaEvent_t fork_ev = nullptr, join_ev[nsg::kRaySets] = {};
@@ -144,7 +145,7 @@ struct nsg_ctx {
   DevBuf cube_vl, cube_map, vstruct;
   nsg::TuneParams tune;
   DevBuf surv_cnt, surv_off, vpos, vkey, row_act_cnt, row_mid_cnt, row_act_off, row_mid_off, act_rec, act_mid,
-      tri_cnt, tri_off, tris, cube_area, red_out;
+      tri_cnt, tri_off, tris, cube_area, red_out, bnd_list, bnd_cursor;
   int64_t n_vert = 0, n_analytic = 0, n_tri = 0, n_active = 0;
   double area = 0;
   DevBuf temp;  // cub temporary storage
@@ -478,7 +479,8 @@ int nsg_ctx_destroy(nsg_ctx* c) {
                     &c->fruns, &c->frow, &c->roots, &c->cc_count, &c->cc_desc, &c->cc_label_of,
                     &c->cc_fill_of, &c->nroots_d, &c->surv_cnt, &c->surv_off, &c->vpos, &c->vkey,
                     &c->row_act_cnt, &c->row_mid_cnt, &c->row_act_off, &c->row_mid_off, &c->act_rec,
-                    &c->act_mid, &c->tri_cnt, &c->tri_off, &c->tris, &c->cube_area, &c->red_out, &c->temp};
+                    &c->act_mid, &c->tri_cnt, &c->tri_off, &c->tris, &c->cube_area, &c->red_out, &c->bnd_list,
+                    &c->bnd_cursor, &c->temp};
   for (DevBuf* b : bufs) b->release();
   for (int i = 0; i < 3; i++) { c->tile_cnt[i].release(); c->tile_off[i].release(); c->tile_list[i].release(); }
   c->d_sd.release(); c->d_patch_struct.release(); c->d_mc_base.release(); c->d_row_base.release();
@@ -490,6 +492,7 @@ int nsg_ctx_destroy(nsg_ctx* c) {
     c->vol_ray[i].release(); c->ovf_rays[i].release(); c->ray_hit_off[i].release(); c->ray_hit_cnt[i].release();
     c->cand_sph[i].release(); c->cand_tor[i].release(); c->def_sph[i].release(); c->def_tor[i].release();
     c->hit_t[i].release(); c->hit_cnt[i].release(); c->hit_pid[i].release();
+    c->tsplit_a[i].release(); c->tsplit_b[i].release();
     if (c->set_stream[i]) cudaStreamDestroy(c->set_stream[i]);
     if (c->join_ev[i]) cudaEventDestroy(c->join_ev[i]);
   }
@@ -747,6 +750,7 @@ int nsg_set_tuning(nsg_ctx* c, const int32_t* params, int n) {
   c->tune.isect_bpsm = bpsm;
   c->tune.cand_threads = ct;
   if (n >= 4) c->concurrent_sets = params[3] != 0;
+  if (n >= 5) c->tune.torus_split = params[4] != 0;
   return NSG_OK;
 }
 
@@ -756,6 +760,7 @@ int nsg_get_tuning(nsg_ctx* c, int32_t* params, int n) {
   params[1] = c->tune.isect_bpsm;
   params[2] = c->tune.cand_threads;
   if (n >= 4) params[3] = c->concurrent_sets ? 1 : 0;
+  if (n >= 5) params[4] = c->tune.torus_split;
   return NSG_OK;
 }
 
@@ -1030,12 +1035,14 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
     CK(cudaMemsetAsync(c->ray_pair_cnt.p, 0, nrays_mc * sizeof(int32_t), c->stream));
     if (c->pair_cap == 0) c->pair_cap = std::max<int64_t>(4 * nrays_mc, 1 << 16);
   }
-  CK(c->cursors.ensure(32 * sizeof(unsigned long long)));
+  CK(c->cursors.ensure(64 * sizeof(unsigned long long)));
   // the ray sets run on their own streams (each with its own candidate lists and hit store) so
   // that the double-precision intersection launches of one set overlap the integer-bound candidate
   // and fill launches of another; or, with concurrent_sets off, one after another on the context's
   // stream through slot 0
   const bool conc = c->concurrent_sets && (do_mc ? 3 : 0) + ((do_status || do_eps) ? 1 : 0) + (do_eps ? 2 : 0) > 1;
+  // torus candidates split by resolvent branch (SES patch sets)
+  const bool split = c->tune.torus_split && (c->kind_mask & nsg::kSesKinds);
   const auto slot_of = [&](int set) { return conc ? set : 0; };
   {
     int64_t amax = std::max(c->win_area[0], std::max(c->win_area[1], c->win_area[2]));
@@ -1073,6 +1080,10 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
       const int sl = slot_of(set);
       CK(c->cand_sph[sl].ensure(c->cand_cap * sizeof(int2)));
       CK(c->cand_tor[sl].ensure(c->cand_cap * sizeof(int2)));
+      if (split) {
+        CK(c->tsplit_a[sl].ensure(c->cand_cap * sizeof(int2)));
+        CK(c->tsplit_b[sl].ensure(c->cand_cap * sizeof(int2)));
+      }
       if (precision == NSG_PRECISION_MIXED) {
         CK(c->def_sph[sl].ensure(c->def_cap * sizeof(int2)));
         CK(c->def_tor[sl].ensure(c->def_cap * sizeof(int2)));
@@ -1088,11 +1099,12 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
                                        1 << 16);
       CK(c->hits.ensure(c->hit_cap * sizeof(double)));
     }
-    CK(cudaMemsetAsync(c->cursors.p, 0, 32 * sizeof(unsigned long long), c->stream));
+    CK(cudaMemsetAsync(c->cursors.p, 0, 64 * sizeof(unsigned long long), c->stream));
     CK(cudaMemsetAsync(c->err.p, 0, sizeof(int32_t), c->stream));
     if (do_mc) CK(cudaMemsetAsync(c->bits.p, 0xff, nwords * sizeof(uint32_t), c->stream));
     // cursors: 0 pairs, 1 kept hits, 2 status runs, 4..6 the overflow counts of the six ray sets
-    // (int32), 8 + 2 s the candidate counts of set s (spheres, tori), 20 + 2 s its deferred counts
+    // (int32), 8 + 2 s the candidate counts of set s (spheres, tori), 20 + 2 s its deferred counts,
+    // 32 + 4 s its split torus counts (at +1 and +3)
     unsigned long long* cur = c->cursors.as<unsigned long long>();
     int32_t* ovf_count = (int32_t*)(cur + 4);
     int sets[nsg::kRaySets], nsets = 0;
@@ -1161,7 +1173,9 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
       outs[s] = o;
       const int sl = slot_of(s);
       nsg::CandOut co{c->cand_sph[sl].as<int2>(), c->cand_tor[sl].as<int2>(), c->cand_cap, cur + 8 + 2 * s,
-                      c->def_sph[sl].as<int2>(), c->def_tor[sl].as<int2>(), c->def_cap, cur + 20 + 2 * s};
+                      c->def_sph[sl].as<int2>(), c->def_tor[sl].as<int2>(), c->def_cap, cur + 20 + 2 * s,
+                      split ? c->tsplit_a[sl].as<int2>() : nullptr, split ? c->tsplit_b[sl].as<int2>() : nullptr,
+                      split ? cur + 32 + 4 * s : nullptr};
       nsg::HitStore hs{c->hit_t[sl].as<double>(), c->hit_cnt[sl].as<int32_t>(), nr,
                        pids ? c->hit_pid[sl].as<int32_t>() : nullptr};
       CK(cudaMemsetAsync(c->hit_cnt[sl].p, 0, nr * sizeof(int32_t), st));
@@ -1469,6 +1483,15 @@ int nsg_triangulate(nsg_ctx* c, double* area_out, int64_t* nverts, int64_t* ntri
   M.cube_map = c->cube_map.as<int32_t>();
   M.cube_vl = c->cube_vl.as<int32_t>();
   CK(cudaMemsetAsync(c->cube_vl.p, 0xff, std::max<int64_t>(n_act, 1) * 12 * sizeof(int32_t), c->stream));
+  // triangle counts per active cube: the case table's for interior cubes (written by the
+  // classification), a count over the vertex slots for the listed low-face cubes
+  CK(c->tri_cnt.ensure(std::max<int64_t>(n_act, 1) * sizeof(int32_t)));
+  CK(c->bnd_list.ensure(std::max<int64_t>(n_act, 1) * sizeof(int32_t)));
+  CK(c->bnd_cursor.ensure(sizeof(unsigned long long)));
+  CK(cudaMemsetAsync(c->bnd_cursor.p, 0, sizeof(unsigned long long), c->stream));
+  M.tri_cnt = c->tri_cnt.as<int32_t>();
+  M.bnd_list = c->bnd_list.as<int32_t>();
+  M.bnd_cursor = c->bnd_cursor.as<unsigned long long>();
   LAUNCH(nsg::launch_mc_rows(M, 1, c->stream));
   LAUNCH(nsg::launch_mc_push(M, 0, n_an, c->stream));
   // midpoint vertices of cut edges without an analytic vertex
@@ -1504,7 +1527,6 @@ int nsg_triangulate(nsg_ctx* c, double* area_out, int64_t* nverts, int64_t* ntri
   LAUNCH(nsg::launch_mc_mid(M, 1, c->stream));
   LAUNCH(nsg::launch_mc_push(M, n_an, n_v, c->stream));
   M.n_active = n_act;
-  CK(c->tri_cnt.ensure(std::max<int64_t>(n_act, 1) * sizeof(int32_t)));
   CK(c->tri_off.ensure((n_act + 1) * sizeof(int64_t)));
   CK(c->cube_area.ensure(std::max<int64_t>(n_act, 1) * sizeof(double)));
   M.tri_cnt = c->tri_cnt.as<int32_t>();
@@ -1522,7 +1544,7 @@ int nsg_triangulate(nsg_ctx* c, double* area_out, int64_t* nverts, int64_t* ntri
     M.i32 = P.i32;
     M.probe = P.probe;
   }
-  LAUNCH(nsg::launch_mc_tris(M, 0, c->stream));
+  LAUNCH(nsg::launch_mc_tris_bnd(M, c->stream));
   int64_t n_tri = 0;
   rc = scan_counts(c, c->tri_cnt.as<int32_t>(), n_act, c->tri_off.as<int64_t>(), &n_tri);
   if (rc) return rc;

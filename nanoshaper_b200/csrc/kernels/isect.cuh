@@ -24,12 +24,12 @@ struct TraceCtx {
   TraceOut out;
 };
 
-// Mixed-precision intersection launches of one panel (trace_mixed.cu): the sphere and torus
-// candidate lists of co, with the deferred candidates appended to co's deferred lists.
+// Mixed-precision intersection launches of one panel: the sphere candidate list of co
+// (trace_mixed.cu) and the torus list (trace_mixed_torus.cu, built without fused multiply-adds),
+// with the deferred candidates appended to co's deferred lists.
 template <int PN>
-void launch_isect_mixed(const TraceCtx& C, const CandOut& co, const HitStore& hs, const TuneParams& tp,
-                        cudaStream_t s);
-// The torus launch of launch_isect_mixed (trace_mixed_torus.cu, built without fused multiply-adds).
+void launch_isect_mixed_sphere(const TraceCtx& C, const CandOut& co, const HitStore& hs, const TuneParams& tp,
+                               cudaStream_t s);
 template <int PN>
 void launch_isect_mixed_torus(const TraceCtx& C, const CandOut& co, const HitStore& hs, const TuneParams& tp,
                               cudaStream_t s);

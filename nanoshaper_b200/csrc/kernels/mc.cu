@@ -28,6 +28,7 @@ namespace {
 
 __constant__ int8_t c_tri[256][16];  // triangle edge lists, -1 terminated
 __constant__ uint16_t c_emask[256];  // cut-edge mask per case
+__constant__ uint8_t c_ntri[256];    // case-table triangles per case
 
 __device__ __forceinline__ double gcoord(const GridDev& g, int d, int64_t i) { return g.mn[d] + (double)i * g.side; }
 
@@ -146,6 +147,9 @@ __device__ __forceinline__ uint32_t bits32_pair(const uint32_t* __restrict__ bit
 // the row in blocks of 32 words.  Pass 0 counts the active cubes of each row, pass 1 writes them
 // in i order at the row's offset.
 __global__ void k_mc_rows(MCArgs A, int emit) {
+  __shared__ uint8_t s_ntri[256];
+  for (int t = threadIdx.x; t < 256; t += blockDim.x) s_ntri[t] = c_ntri[t];
+  __syncthreads();
   const int lane = threadIdx.x & 31;
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t ch = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); ch < A.nchunks; ch += warps) {
@@ -208,6 +212,17 @@ __global__ void k_mc_rows(MCArgs A, int emit) {
 #pragma unroll
             for (int q = 0; q < 8; q++) cs |= ((c[q] >> bit) & 1u) << q;
             A.cube_map[S.cube_base + cube_local(S.g, ic + bit, j, k)] = (int32_t)slot;
+            // every cut edge of a cube with i, j, k >= 2 has a vertex (an analytic one, or the
+            // midpoint its owner cube adds), so its triangles are the case table's; a cube on the
+            // low faces of the cube range may lack vertices on edges whose owner lies outside the
+            // range, and is counted after the vertices are in place (k_mc_tris_bnd)
+            if (ic + bit >= 2 && j >= 2 && k >= 2) {
+              A.tri_cnt[slot] = s_ntri[cs];
+            } else {
+              A.tri_cnt[slot] = 0;
+              const unsigned long long q = atomicAdd(A.bnd_cursor, 1ull);
+              A.bnd_list[q] = (int32_t)slot;
+            }
             A.act_rec[slot++] = make_int4((int)(ic + bit), j, k, cs | (C.x << 11));
           }
         }
@@ -298,9 +313,25 @@ __global__ void k_mc_push(MCArgs A, int64_t v0, int64_t v1) {
   }
 }
 
-// One thread per active cube, the vertex of every cut edge read from its slots.  Pass 0 counts the
-// triangles whose three edges have vertices; pass 1 writes them at their offsets and sums their
-// areas (and, in gradient mode, their derivatives with respect to the analytic vertices).
+// Triangle counts of the active cubes on the low faces of the cube range (listed by k_mc_rows): the
+// case-table triangles whose three edges have vertices.
+__global__ void k_mc_tris_bnd(MCArgs A) {
+  const int64_t n = (int64_t)*A.bnd_cursor;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t a = A.bnd_list[q];
+    const int c = A.act_rec[a].w & 255;
+    const int32_t* cv = A.cube_vl + 12 * (int64_t)a;
+    int cnt = 0;
+    for (int t = 0; t < 16 && c_tri[c][t] >= 0; t += 3)
+      if (cv[c_tri[c][t]] >= 0 && cv[c_tri[c][t + 1]] >= 0 && cv[c_tri[c][t + 2]] >= 0) cnt++;
+    A.tri_cnt[a] = cnt;
+  }
+}
+
+// One thread per active cube, the vertex of every cut edge read from its slots: writes the
+// triangles whose three edges have vertices at the cube's offset and sums their areas (and, in
+// gradient mode, their derivatives with respect to the analytic vertices).  (Pass 0, the count of
+// those triangles, is kept for tests; the pipeline takes the counts from the classification.)
 __global__ void __launch_bounds__(128, 8) k_mc_tris(MCArgs A, int emit) {
   __shared__ int8_t s_tri[256][16];
   __shared__ uint16_t s_emask[256];
@@ -456,6 +487,7 @@ int grid_for(int64_t n, int threads) {
 cudaError_t mc_init_tables() {
   int8_t tri[256][16];
   uint16_t em[256];
+  uint8_t nt[256];
   static const int ec[12][2] = {{0, 1}, {1, 2}, {2, 3}, {3, 0}, {4, 5}, {5, 6}, {6, 7}, {7, 4}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
   for (int c = 0; c < 256; c++) {
     int m = 0;
@@ -465,9 +497,11 @@ cudaError_t mc_init_tables() {
     const char* s = kNsMcCases[c];
     int q = 0;
     for (; s[q] && q < 16; q++) tri[c][q] = (int8_t)(s[q] <= '9' ? s[q] - '0' : s[q] - 'a' + 10);
+    nt[c] = (uint8_t)(q / 3);
     for (; q < 16; q++) tri[c][q] = -1;
   }
   cudaError_t err = cudaMemcpyToSymbol(c_tri, tri, sizeof tri);
+  if (err == cudaSuccess) err = cudaMemcpyToSymbol(c_ntri, nt, sizeof nt);
   if (err != cudaSuccess) return err;
   return cudaMemcpyToSymbol(c_emask, em, sizeof em);
 }
@@ -500,6 +534,12 @@ cudaError_t launch_vertex_normals(const double* vpos, const int32_t* vpid, int64
                                   const int32_t* i32, double probe, double* normals, cudaStream_t s) {
   if (n_analytic <= 0) return cudaSuccess;
   k_vertex_normals<<<grid_for(n_analytic, 256), 256, 0, s>>>(vpos, vpid, n_analytic, f64, i32, probe, normals);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mc_tris_bnd(const MCArgs& A, cudaStream_t s) {
+  if (A.n_active <= 0) return cudaSuccess;
+  k_mc_tris_bnd<<<sm_count() * 4, 256, 0, s>>>(A);
   return cudaGetLastError();
 }
 

@@ -44,7 +44,9 @@ struct MCArgs {
   const int64_t* mid_off;        // exclusive scan of mid_cnt
   int32_t* act_mid;              // index of the first midpoint vertex of the cube
   int64_t n_active;
-  int32_t* tri_cnt;
+  int32_t* tri_cnt;               // triangles per active cube (interior cubes: from the classification)
+  int32_t* bnd_list;             // active cubes on the low faces of the cube range
+  unsigned long long* bnd_cursor;
   int32_t* cube_vl;              // 12 per active cube: vertex of each cut edge (-1 none)
   int32_t* cube_map;             // dense per structure (cube_base): active index of every active cube
   const int64_t* tri_off;
@@ -65,6 +67,8 @@ cudaError_t launch_vert(const VertArgs& A, int emit, cudaStream_t s);
 cudaError_t launch_mc_rows(const MCArgs& A, int emit, cudaStream_t s);
 cudaError_t launch_mc_mid(const MCArgs& A, int emit, cudaStream_t s);
 cudaError_t launch_mc_tris(const MCArgs& A, int emit, cudaStream_t s);
+// Triangle counts of the listed low-face cubes, once every vertex is in its cube slots.
+cudaError_t launch_mc_tris_bnd(const MCArgs& A, cudaStream_t s);
 // Every vertex in [v0, v1) writes its id into the cube_vl slots of the (up to four) active cubes
 // that share its grid edge; the smallest id of an edge wins (atomicMin).
 cudaError_t launch_mc_push(const MCArgs& A, int64_t v0, int64_t v1, cudaStream_t s);

@@ -161,6 +161,12 @@ struct CandOut {
   int2* dtor;
   int64_t dcap;
   unsigned long long* dcount;  // 2 counters
+  // torus candidates split by the branch their resolvent cubic takes (null: no split): the
+  // cube-root branch (and the rare approximate ones) in tsa, the arccos branch in tsb, each of
+  // capacity cap; counts at tscount[1] and tscount[3]
+  int2* tsa;
+  int2* tsb;
+  unsigned long long* tscount;
 };
 
 // Slot-major hit store of one ray set: hit i of ray r at t[i * nrays + r]; cnt[r] counts the
@@ -200,6 +206,7 @@ struct TuneParams {
   int isect_threads = 256;  // threads per block of the intersection kernels (64..256)
   int isect_bpsm = 16;      // their blocks per SM (grid = SMs * isect_bpsm, grid-stride)
   int cand_threads = 256;   // threads per block of the candidate kernel (one warp per patch)
+  int torus_split = 1;      // torus candidates solved in two launches, one per resolvent branch
 };
 
 // trace.cu: every launch covers all structures of the batch; `set` is the ray set (0..3) and

@@ -559,13 +559,112 @@ __global__ void __launch_bounds__(256) k_cand(TraceCtx C, CandOut co) {
   }
 }
 
+// Branch class of a torus candidate, from the operations of the double-precision path up to the
+// resolvent cubic (ray_sphere_axis, torus_coeffs_f64, the head of quartic_f64 and of
+// real_cubic_f64, the same operations in the same order): -1 when the path returns no hit there
+// (no clipping-sphere hit, or no real quartic root), 1 for the resolvent's arccos branch, 0 for
+// the cube-root branch and the rare others.
+template <int PN>
+__device__ __forceinline__ int torus_class(const double* f, double probe, const double* pa, double ray_dir) {
+  constexpr int vc = Ax<PN>::vc;
+  double t0, t1;
+  if (!ray_sphere_axis<vc>(pa, ray_dir, f, f[kR], &t0, &t1)) return -1;
+  double orig1[3] = {pa[0], pa[1], pa[2]};
+  orig1[vc] += t0 * ray_dir;
+  double b, c, d, e;
+  torus_coeffs_f64(f, probe, vc, orig1, &b, &c, &d, &e);
+  const double b_2 = 0.5 * b;
+  const double b_4 = 0.25 * b;
+  const double p = c - 1.5 * (b_2 * b_2);
+  const double q = d + b_2 * (b_2 * b_2 - c);
+  const double r = e + b_4 * (b_4 * (c - 3.0 * b_4 * b_4) - d);
+  const double ff = p * p - 4. * r;
+  const double delta =
+      4. * ff * (4. * r * (p * p) - p * (q * q) - 16. * (r * r)) + (q * q) * (128. * p * r - 27. * (q * q));
+  if (e != 0. && (fabs(p) > 3.E+3 || fabs(r) > 3.E+3 || fabs(q) > 3.E+3 || fabs(delta) > 1.E+14)) return 0;
+  if (!(delta < 0. || (delta == 0. && (p >= 0. || ff < 0.))) && !((p < 0. && ff > 0.) || (delta == 0. && p == 0. && r == 0.)))
+    return -1;
+  // the resolvent cubic x^3 + cb x^2 + cc x + cd
+  const double cb = p, cc = 0.25 * (p * p) - r, cd = (-0.125) * (q * q);
+  if (fabs(cc) < cb * cb * 1.E-6 && fabs(cd) < fabs(cb) * 1.E-6) return 0;
+  if (fabs(cd / cc) < 4.E-4) return 0;
+  const double pc = -(1.0 / 3.0) * cb * cb + cc;
+  const double qc = (2. / 27.) * cb * cb * cb - (1. / 3.) * cb * cc + cd;
+  const double D3p = (1. / 27.) * pc * pc * pc;
+  const double D3 = D3p + 0.25 * qc * qc;
+  return D3 >= 0. ? 0 : 1;
+}
+
+// One thread per torus candidate: its branch class; candidates with no hit are dropped, the
+// others appended (warp-aggregated) to the list of their class, so that each solve launch runs
+// with the lanes of a warp on one branch of the solver.
+template <int PN>
+__global__ void __launch_bounds__(256) k_torus_split(TraceCtx C, CandOut co) {
+  constexpr int fd = Ax<PN>::fd, ld = Ax<PN>::ld, vc = Ax<PN>::vc;
+  const int64_t ncand = co.count[1];
+  const int64_t nlim = ncand < co.cap ? ncand : co.cap;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int lane = threadIdx.x & 31;
+  const int64_t c0 = blockIdx.x * (int64_t)blockDim.x + (threadIdx.x & ~31);
+  for (int64_t cb = c0; cb < nlim; cb += stride) {
+    const int64_t c = cb + lane;
+    int cls = -1;
+    int2 e = make_int2(0, 0);
+    if (c < nlim) {
+      e = co.tor[c];
+      const int64_t rid = e.x, pid = e.y;
+      const StructDev& S = C.B.s[C.B.patch_struct[pid]];
+      const GridDev& g = S.g;
+      const double delta = ray_set_shifted(C.set) ? NS_DELTA - g.hside : 0.0;
+      const int64_t nb = g.n[fd];
+      const int64_t lr = rid - S.ray_base[C.set];
+      const int64_t m = lr % nb, n = lr / nb;
+      double pa[3];
+      pa[fd] = gcoord(g, fd, m) + delta;
+      pa[ld] = gcoord(g, ld, n) + delta;
+      pa[vc] = gcoord(g, vc, 0) + delta;
+      double f[18];
+      const double* src = C.P.f64 + (int64_t)NS_PATCH_F64 * pid;
+#pragma unroll
+      for (int k = 0; k < 18; k++) f[k] = __ldg(src + k);
+      cls = torus_class<PN>(f, C.P.probe, pa, S.ray_dir[vc]);
+    }
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+      const unsigned m = __ballot_sync(0xffffffffu, cls == k);
+      if (!m) continue;
+      unsigned long long base = 0;
+      if (lane == 0) base = atomicAdd(co.tscount + 1 + 2 * k, (unsigned long long)__popc(m));
+      base = __shfl_sync(0xffffffffu, base, 0);
+      if (cls == k) {
+        const unsigned long long slot = base + __popc(m & ((1u << lane) - 1u));
+        (k == 0 ? co.tsa : co.tsb)[slot] = e;
+      }
+    }
+  }
+}
+
 template <int PN>
 void launch_isect(const TraceCtx& C, const CandOut& co, const HitStore& hs, int precision, const TuneParams& tp,
                   cudaStream_t s) {
   const int ig = sm_count() * tp.isect_bpsm, it = tp.isect_threads;
   const bool ses = C.P.kind_mask & kSesKinds, skin = C.P.kind_mask & kBoxKinds;
+  // the torus candidates, split by resolvent branch into two lists solved one after the other
+  const bool split = tp.torus_split && co.tsa && co.tsb && co.tscount;
+  CandOut ca = co, cb = co;
+  if (split) {
+    k_torus_split<PN><<<ig, 256, 0, s>>>(C, co);
+    ca.tor = co.tsa;
+    ca.count = co.tscount;
+    cb.tor = co.tsb;
+    cb.count = co.tscount + 2;
+  }
   if (precision == 1) {
-    if (ses) launch_isect_mixed<PN>(C, co, hs, tp, s);
+    if (ses) {
+      launch_isect_mixed_sphere<PN>(C, co, hs, tp, s);
+      launch_isect_mixed_torus<PN>(C, ca, hs, tp, s);
+      if (split) launch_isect_mixed_torus<PN>(C, cb, hs, tp, s);
+    }
     if (skin) launch_isect_quad_mixed<PN>(C, co, hs, tp, s);
     // the deferred candidates, in double precision (few: a small grid)
     const CandOut dco{co.dsph, co.dtor, co.dcap, co.dcount, nullptr, nullptr, 0, nullptr};
@@ -577,7 +676,8 @@ void launch_isect(const TraceCtx& C, const CandOut& co, const HitStore& hs, int 
   } else {
     if (ses) {
       k_isect<PN, false><<<ig, it, 0, s>>>(C, co, hs);
-      k_isect<PN, true><<<ig, it, 0, s>>>(C, co, hs);
+      k_isect<PN, true><<<ig, it, 0, s>>>(C, ca, hs);
+      if (split) k_isect<PN, true><<<ig, it, 0, s>>>(C, cb, hs);
     }
     if (skin) k_isect_quad<PN><<<ig, it, 0, s>>>(C, co, hs);
   }

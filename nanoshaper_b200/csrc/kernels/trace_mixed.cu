@@ -6,11 +6,9 @@
 namespace nsg {
 
 template <int PN>
-void launch_isect_mixed(const TraceCtx& C, const CandOut& co, const HitStore& hs, const TuneParams& tp,
-                        cudaStream_t s) {
-  const int ig = sm_count() * tp.isect_bpsm, it = tp.isect_threads;
-  k_isect_mixed<PN, false><<<ig, it, 0, s>>>(C, co, hs);
-  launch_isect_mixed_torus<PN>(C, co, hs, tp, s);
+void launch_isect_mixed_sphere(const TraceCtx& C, const CandOut& co, const HitStore& hs, const TuneParams& tp,
+                               cudaStream_t s) {
+  k_isect_mixed<PN, false><<<sm_count() * tp.isect_bpsm, tp.isect_threads, 0, s>>>(C, co, hs);
 }
 
 template <int PN>
@@ -25,8 +23,11 @@ template void launch_isect_quad_mixed<1>(const TraceCtx&, const CandOut&, const 
                                          cudaStream_t);
 template void launch_isect_quad_mixed<2>(const TraceCtx&, const CandOut&, const HitStore&, const TuneParams&,
                                          cudaStream_t);
-template void launch_isect_mixed<0>(const TraceCtx&, const CandOut&, const HitStore&, const TuneParams&, cudaStream_t);
-template void launch_isect_mixed<1>(const TraceCtx&, const CandOut&, const HitStore&, const TuneParams&, cudaStream_t);
-template void launch_isect_mixed<2>(const TraceCtx&, const CandOut&, const HitStore&, const TuneParams&, cudaStream_t);
+template void launch_isect_mixed_sphere<0>(const TraceCtx&, const CandOut&, const HitStore&, const TuneParams&,
+                                           cudaStream_t);
+template void launch_isect_mixed_sphere<1>(const TraceCtx&, const CandOut&, const HitStore&, const TuneParams&,
+                                           cudaStream_t);
+template void launch_isect_mixed_sphere<2>(const TraceCtx&, const CandOut&, const HitStore&, const TuneParams&,
+                                           cudaStream_t);
 
 }  // namespace nsg

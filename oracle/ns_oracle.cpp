@@ -79,6 +79,25 @@ bool ray_sphere(const double* orig, const double* dir, const double* c, double r
   return true;
 }
 
+// Branch counters of the torus path (the op model of the bench's roofline and the candidates'
+// branch mix): torus candidates, clipping-sphere misses, quartic outcomes, resolvent-cubic branches.
+enum {
+  kOpTorusCand, kOpTorusNoSphere, kOpQuarticNone, kOpQuarticM0, kOpQuartic2, kOpQuartic4, kOpQuarticRecip,
+  kOpCubicSmallC, kOpCubicRatioSqrt, kOpCubicRatioEps, kOpCubicCbrt, kOpCubicAcos, kOpSphereCand,
+  kOpSphereMiss, kOpRootTest, kOpRootIn, kOpFeasTest, kOpPlaneTest, kOpClipTest, kOpSirTest,
+  kOpCount
+};
+std::atomic<uint64_t> g_ops[kOpCount];
+thread_local uint64_t t_ops[kOpCount];
+inline void op_count(int k) { t_ops[k]++; }
+// Adds this thread's counts to the totals (end of a tracing worker).
+inline void op_flush() {
+  for (int k = 0; k < kOpCount; k++) {
+    g_ops[k].fetch_add(t_ops[k], std::memory_order_relaxed);
+    t_ops[k] = 0;
+  }
+}
+
 // realCubicSolution (src/tools.cpp:350-391)
 double real_cubic(double b, double c, double d) {
   double p = -(1.0 / 3.0) * b * b + c;
@@ -86,22 +105,27 @@ double real_cubic(double b, double c, double d) {
   double D3p = (1. / 27.) * p * p * p;
   double D3 = D3p + 0.25 * q * q;
   if (fabs(c) < b * b * 1.E-6 && fabs(d) < fabs(b) * 1.E-6) {
+    op_count(kOpCubicSmallC);
     return c / b - b - d / (b * b);
   } else if (fabs(d / c) < 4.E-4) {
     double ratio = d / c;
     if (D3 <= 0.) {
+      op_count(kOpCubicRatioSqrt);
       return 0.5 * (ratio - b + sqrt((b - ratio) * (b - ratio) - 4. * (c - ratio * (b - ratio))));
     } else {
+      op_count(kOpCubicRatioEps);
       double eps = -ratio * ratio * (b - ratio) / (3. * ratio * ratio - 2. * b * ratio + c);
       return eps - ratio;
     }
   } else {
     if (D3 >= 0.) {
+      op_count(kOpCubicCbrt);
       double radD3 = sqrt(D3);
       double A = cbrt(radD3 - 0.5 * q);
       double psu3A = cbrt(radD3 + 0.5 * q);
       return A - psu3A - (1. / 3.) * b;
     } else {
+      op_count(kOpCubicAcos);
       double Aarg = acos(-0.5 * q / sqrt(-D3p));
       return 2. * sqrt(-(1. / 3.) * p) * cos((1. / 3.) * Aarg) - (1. / 3.) * b;
     }
@@ -119,6 +143,7 @@ void quartic(double roots[4], double b, double c, double d, double e, int* num_s
   double delta = 4. * f * (4. * r * (p * p) - p * (q * q) - 16. * (r * r)) + (q * q) * (128. * p * r - 27. * (q * q));
   bool change_variant = false;
   if (e != 0. && (fabs(p) > 3.E+3 || fabs(r) > 3.E+3 || fabs(q) > 3.E+3 || fabs(delta) > 1.E+14)) {
+    op_count(kOpQuarticRecip);
     double dsu2e = 0.5 * d / e;
     change_variant = true;
     p = -1.5 * dsu2e * dsu2e + c / e;
@@ -132,11 +157,14 @@ void quartic(double roots[4], double b, double c, double d, double e, int* num_s
   else if ((p < 0. && f > 0.) || (delta == 0. && p == 0. && r == 0.))
     *num_sol = 4;
   else {
+    op_count(kOpQuarticNone);
     *num_sol = 0;
     return;
   }
+  op_count(*num_sol == 2 ? kOpQuartic2 : kOpQuartic4);
   double m = real_cubic(p, 0.25 * (p * p) - r, (-0.125) * (q * q));
   if (m <= 0) {
+    op_count(kOpQuarticM0);
     *num_sol = 0;
     return;
   }
@@ -198,11 +226,15 @@ bool ray_torus(const double* invrot, const double* tc, const double* sc, double 
   numInt = 0;
   for (int i = 0; i < numroots; i++) {
     if (roots[i] < 0) continue;
+    op_count(kOpRootTest);
     double point[3] = {orig1[0], orig1[1], orig1[2]};
     point[vc] += roots[i];
     double dd = (sc[0] - point[0]) * (sc[0] - point[0]) + (sc[1] - point[1]) * (sc[1] - point[1]) +
                 (sc[2] - point[2]) * (sc[2] - point[2]);
-    if (dd < radius * radius) t[numInt++] = t0 + roots[i] / ray_dir;
+    if (dd < radius * radius) {
+      op_count(kOpRootIn);
+      t[numInt++] = t0 + roots[i] / ray_dir;
+    }
   }
   return numInt != 0;
 }
@@ -288,13 +320,17 @@ bool feasible(const Patches& P, int64_t it, const double* p) {
   const double* pool = P.pool + 4 * (int64_t)ir[1];
   const int8_t* flg = P.flag + ir[1];
   int cnt = ir[2];
+  op_count(kOpFeasTest);
   if (kind == NS_FACE_REG || kind == NS_FACE_SING) {
-    for (int q = 0; q < cnt; q++)
+    for (int q = 0; q < cnt; q++) {
+      op_count(kOpPlaneTest);
       if (plane_test(pool + 4 * q, p) > 0) return false;
+    }
     return true;
   }
   if (kind == NS_POINT) {
     for (int q = 0; q < cnt; q++) {
+      op_count(kOpClipTest);
       double dd = dist2(pool + 4 * q, p);
       dd -= pool[4 * q + 3];
       if (dd < 0) return false;
@@ -303,18 +339,22 @@ bool feasible(const Patches& P, int64_t it, const double* p) {
   }
   double r = fr[8];
   if (r >= 0.) {
+    op_count(kOpSirTest);
     double dd = dist2(fr + 4, p);
     if (dd < r * r) return false;
   }
   if (cnt == 0) return true;
   for (int q = 0; q + 1 < cnt; q += 2) {
+    op_count(kOpPlaneTest);
     double t0 = plane_test(pool + 4 * q, p);
     if (flg[q]) {
       if (t0 > 0) continue;
+      op_count(kOpPlaneTest);
       if (plane_test(pool + 4 * (q + 1), p) > 0) continue;
       return true;
     } else {
       if (t0 <= 0) return true;
+      op_count(kOpPlaneTest);
       if (plane_test(pool + 4 * (q + 1), p) <= 0) return true;
     }
   }
@@ -506,7 +546,11 @@ struct Oracle {
           double dy = sc[ld] - pa[ld];
           if (dx * dx + dy * dy > radius * radius) continue;
           double t[4];
-          if (!ray_sphere(pa, dir, sc, radius, &t[0], &t[1])) continue;
+          op_count(doTorus ? kOpTorusCand : kOpSphereCand);
+          if (!ray_sphere(pa, dir, sc, radius, &t[0], &t[1])) {
+            op_count(doTorus ? kOpTorusNoSphere : kOpSphereMiss);
+            continue;
+          }
           int numInt = 0;
           if (!doTorus) numInt = 2;
           else ray_torus(fr + 9, fr + 4, sc, P.probe, fr[7], radius, vc, pa, dir, t, numInt);
@@ -543,6 +587,7 @@ struct Oracle {
     std::vector<std::vector<Hit>> per(std::max(1, nthreads));
     auto work = [&](int tid) {
       for (int64_t it = tid; it < P.n; it += std::max(1, nthreads)) trace_patch(it, per[tid]);
+      op_flush();
     };
     if (nthreads <= 1) work(0);
     else {
@@ -1175,6 +1220,7 @@ struct Oracle {
   }
 
   void run() {
+    for (int k = 0; k < kOpCount; k++) g_ops[k].store(0);
     NMAX = std::max(g.nx, std::max(g.ny, g.nz));
     panels[0] = eps_on() ? 3 : ((flags & 1) ? 1 : 0);
     panels[1] = (flags & 2) ? 3 : 0;
@@ -1420,6 +1466,13 @@ double nso_scalar(void* h, const char* what) {
   if (w == "vol_panel0") return o->volPanel[0];
   if (w == "vol_panel1") return o->volPanel[1];
   if (w == "vol_panel2") return o->volPanel[2];
+  static const char* kOpNames[kOpCount] = {"torus_cand", "torus_no_sphere", "quartic_none", "quartic_m0", "quartic_2",
+                                           "quartic_4", "quartic_recip", "cubic_small_c", "cubic_ratio_sqrt",
+                                           "cubic_ratio_eps", "cubic_cbrt", "cubic_acos", "sphere_cand",
+                                           "sphere_miss", "root_test", "root_in", "feas_test", "plane_test",
+                                           "clip_test", "sir_test"};
+  for (int k = 0; k < kOpCount; k++)
+    if (w == std::string("op_") + kOpNames[k]) return (double)g_ops[k].load();
   return NAN;
 }
 

@@ -216,3 +216,60 @@ class TrianglePatches:
         self.pool = np.zeros((1, 4))
         self.pool_flag = np.zeros(1, np.int8)
         self.probe = 0.0
+
+
+OP_NAMES = ("torus_cand", "torus_no_sphere", "quartic_none", "quartic_m0", "quartic_2", "quartic_4", "quartic_recip",
+            "cubic_small_c", "cubic_ratio_sqrt", "cubic_ratio_eps", "cubic_cbrt", "cubic_acos", "sphere_cand",
+            "sphere_miss", "root_test", "root_in", "feas_test", "plane_test", "clip_test", "sir_test")
+
+# Operation model of the ray-patch tests (adds, subtractions and multiplications of doubles counted
+# as one flop each, so a fused multiply-add is two; square roots, divisions, cube roots, arccos and
+# cos counted apart), per executed block of the restated code:
+#   ray-sphere (raySphere on an axis ray): 15 flops, +2 flops, 1 sqrt and 2 divisions on a hit
+#   torus: the entry point 2, the coefficients 53, the quartic head 38, then (with roots) the
+#     resolvent's arguments 5 and head 19 + 1 division; the resolvent branch: cube roots 7 + 1 sqrt
+#     + 2 cbrt; arccos 7 + 2 sqrt + 1 division + acos + cos; the two approximations 9 + 1 sqrt and
+#     10 + 1 division; the small-coefficient one 3 + 2 divisions; the quartic tail 16 + 1 division
+#     + 3 sqrt for 2 roots, 25 + 1 division + 4 sqrt for 4; per non-negative root 10, per root in
+#     the clipping sphere 1 + 1 division
+#   feasibility: 2 per tested point, a plane 6, a clipping sphere 9, the spindle sphere 9
+OP_MODEL = {
+    "sphere_cand": {"flops": 15}, "sphere_hit": {"flops": 2, "sqrt": 1, "div": 2},
+    "torus_entry": {"flops": 2 + 53 + 38},
+    "cubic_head": {"flops": 5 + 19, "div": 1},
+    "cubic_cbrt": {"flops": 7, "sqrt": 1, "cbrt": 2},
+    "cubic_acos": {"flops": 7, "sqrt": 2, "div": 1, "acos": 1, "cos": 1},
+    "cubic_ratio_sqrt": {"flops": 9, "sqrt": 1},
+    "cubic_ratio_eps": {"flops": 10, "div": 1},
+    "cubic_small_c": {"flops": 3, "div": 2},
+    "quartic_2": {"flops": 16, "div": 1, "sqrt": 3},
+    "quartic_4": {"flops": 25, "div": 1, "sqrt": 4},
+    "root_test": {"flops": 10}, "root_in": {"flops": 1, "div": 1},
+    "feas_test": {"flops": 2}, "plane_test": {"flops": 6}, "clip_test": {"flops": 9}, "sir_test": {"flops": 9},
+}
+
+
+def op_counts(handle) -> dict:
+    """The branch counters of the last oracle run (a native handle of nso_run*)."""
+    L = lib()
+    return {n: L.nso_scalar(handle, ("op_" + n).encode()) for n in OP_NAMES}
+
+
+def op_model(c: dict) -> dict:
+    """Operations of a run's ray-patch tests from its branch counters (OP_MODEL)."""
+    blocks = {
+        "sphere_cand": c["sphere_cand"] + c["torus_cand"],
+        "sphere_hit": c["sphere_cand"] - c["sphere_miss"] + c["torus_cand"] - c["torus_no_sphere"],
+        "torus_entry": c["torus_cand"] - c["torus_no_sphere"],
+        "cubic_head": c["quartic_2"] + c["quartic_4"],
+        "cubic_cbrt": c["cubic_cbrt"], "cubic_acos": c["cubic_acos"], "cubic_ratio_sqrt": c["cubic_ratio_sqrt"],
+        "cubic_ratio_eps": c["cubic_ratio_eps"], "cubic_small_c": c["cubic_small_c"],
+        "quartic_2": c["quartic_2"], "quartic_4": c["quartic_4"],
+        "root_test": c["root_test"], "root_in": c["root_in"], "feas_test": c["feas_test"],
+        "plane_test": c["plane_test"], "clip_test": c["clip_test"], "sir_test": c["sir_test"],
+    }
+    out = {}
+    for b, n in blocks.items():
+        for k, v in OP_MODEL[b].items():
+            out[k] = out.get(k, 0.0) + n * v
+    return out

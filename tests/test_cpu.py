@@ -774,3 +774,41 @@ def test_oracle_bgp_projection_single_atom(oracle_mod):
     assert not ref.scsnor.any()
     # every point lies within one grid diagonal of the sphere
     assert np.abs(np.linalg.norm(y - c, axis=1) - 1.7).max() <= np.sqrt(3) * ds.side
+
+
+def test_oracle_operation_counters_are_consistent(oracle_mod):
+    """The oracle's branch counters (the bench's operation model) add up: every torus candidate
+    with a clipping-sphere hit leaves the quartic's head with 0, 2 or 4 roots, every quartic with
+    roots takes exactly one resolvent branch, and the model's totals follow the counts."""
+    import ctypes
+    atoms, ds, surf = _surface(300, 1, 2.0, 70.0)
+    O = oracle_mod
+    p = surf.patches
+    L = O.lib()
+    h = L.nso_run_ex(ctypes.byref(ds.grid), p.n, p.f64.ctypes.data, p.i32.ctypes.data, p.pool.ctypes.data,
+                     p.pool_flag.ctypes.data, p.probe, O.STATUS | O.ACCURATE_TRIANGULATION, 0.0, 4, 50)
+    c = O.op_counts(h)
+    L.nso_free(h)
+    assert c["torus_cand"] > 0 and c["sphere_cand"] > 0
+    assert c["quartic_none"] + c["quartic_2"] + c["quartic_4"] == c["torus_cand"] - c["torus_no_sphere"]
+    branches = c["cubic_small_c"] + c["cubic_ratio_sqrt"] + c["cubic_ratio_eps"] + c["cubic_cbrt"] + c["cubic_acos"]
+    assert branches == c["quartic_2"] + c["quartic_4"]
+    assert c["root_in"] <= c["root_test"]
+    m = O.op_model(c)
+    assert m["flops"] >= 15 * (c["torus_cand"] + c["sphere_cand"])
+    assert m["cbrt"] == 2 * c["cubic_cbrt"] and m["acos"] == c["cubic_acos"]
+
+
+def test_cxx_surface_binding_compiles_and_links(native_lib, tmp_path):
+    """The reference-side Surface subclass of the integration notes (tests/cxx/gpu_ses_surface.h)
+    compiles against a stand-in of the reference's interface and links against libnsgpu.so."""
+    import shutil
+    if shutil.which("g++") is None:
+        pytest.skip("no C++ compiler")
+    from nanoshaper_b200 import build as B
+    out = tmp_path / "gss"
+    cmd = ["g++", "-std=c++17", "-Wall", "-Wextra", "-Werror", "-I", str(ROOT / "include"),
+           "-I", str(ROOT / "tests" / "cxx" / "reference_stub"), "-I", str(ROOT / "tests" / "cxx"),
+           str(ROOT / "tests" / "cxx" / "gpu_ses_surface_main.cpp"), "-L", str(B.LIB_DIR), "-lnsgpu", "-o", str(out)]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    assert res.returncode == 0, res.stderr

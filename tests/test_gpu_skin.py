@@ -37,10 +37,21 @@ def _compare_hits(surf, ref, oracle_mod, angstrom=False):
     for s in range(4):
         cnt_g, val_g = surf.hits(s)
         cnt_o, val_o = oracle_mod.ray_hits(ref, s)
-        assert np.array_equal(cnt_g, cnt_o), f"ray set {s}: {(cnt_g != cnt_o).sum()} rays with other hit counts"
+        if not np.array_equal(cnt_g, cnt_o):
+            bad = np.argwhere(cnt_g != cnt_o)[:4]
+            og = np.concatenate([[0], np.cumsum(cnt_g.ravel())])
+            oo = np.concatenate([[0], np.cumsum(cnt_o.ravel())])
+            det = []
+            for n, m in bad:
+                r = n * cnt_g.shape[1] + m
+                det.append((int(n), int(m), val_g[og[r]:og[r + 1]].tolist(), val_o[oo[r]:oo[r + 1]].tolist()))
+            raise AssertionError(f"ray set {s}: {(cnt_g != cnt_o).sum()} rays with other hit counts: {det}")
         if len(val_o):
-            d = float(np.abs(val_g - val_o).max())
-            worst = max(worst, d * _ray_len(g, s) if angstrom else d)
+            d = np.abs(val_g - val_o)
+            k = int(d.argmax())
+            if d[k] > HIT_TOL:
+                print(f"ray set {s}: largest hit difference {d[k]:.3e} at hit {k}: {val_g[k]!r} vs {val_o[k]!r}")
+            worst = max(worst, float(d[k]) * _ray_len(g, s) if angstrom else float(d[k]))
     return worst
 
 
@@ -114,11 +125,14 @@ def test_skin_fixture_6xm4_maps(native_lib, oracle_mod, tmp_path):
     assert len(ns.ds.atoms) == 48519
     ns.buildAnalyticalSurface()
     surf, ds = ns.surf, ns.ds
-    vol = surf.getSurf(True, False, 0.0)
+    vol = surf.getSurf(True, False, 0.0, keep_hits=True)
     ref = oracle_mod.run(ds.grid, surf.patches, flags=oracle_mod.STATUS | oracle_mod.ACCURATE_TRIANGULATION,
                          threads=8)
+    worst = _compare_hits(surf, ref, oracle_mod)
+    assert worst <= HIT_TOL
     n_mis, n_near = compare.near_node_status(ds.status, ref, ds.grid)
     assert n_mis == n_near
     assert np.array_equal(surf.insideness, ref.bits)
-    assert abs(vol - ref.volume) <= 1e-12 * abs(ref.volume)
-    print(f"6xm4 skin ({surf.patches.n} cells, grid {ds.nx}^3): status mismatches {n_mis} (near-node {n_near})")
+    assert abs(vol - ref.volume) <= 1e-12 * abs(ref.volume), f"volume {vol} vs {ref.volume}"
+    print(f"6xm4 skin ({surf.patches.n} cells, grid {ds.nx}^3): status mismatches {n_mis} (near-node {n_near}), "
+          f"worst hit diff {worst:.2e}")
