@@ -182,7 +182,8 @@ int nsg_batch_results(nsg_ctx* ctx, double* volumes, double* areas);
  * params: [intersection threads per block (64..256), intersection blocks per SM (1..64),
  * candidate-kernel threads per block (32..256), and optionally (n >= 4) the ray sets on concurrent
  * streams (1, default) or not, and (n >= 5) the torus candidates split by resolvent branch before
- * the solve (1, default) or not; results do not depend on any of them].  nsg_autotune times
+ * the solve (1) or not (0, default: measured slower on the ensemble); results do not depend on
+ * any of them].  nsg_autotune times
  * `reps` ray casts of the current batch per candidate shape and keeps the fastest in the
  * context. */
 int nsg_set_tuning(nsg_ctx* ctx, const int32_t* params, int n);
