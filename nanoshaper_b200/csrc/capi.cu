@@ -78,7 +78,7 @@ struct nsg_ctx {
   std::vector<nsg::StructDev> sd;
   DevBuf d_sd, d_patch_struct, d_tile_struct[3], d_ray_base[nsg::kRaySets], d_mc_base, d_row_base, d_row_chunks;
   int64_t nchunks = 0;
-  int64_t tiles_tot[3] = {0, 0, 0}, rays_tot[nsg::kRaySets] = {0, 0, 0, 0, 0, 0}, mc_tot = 0, rows_tot = 0, words_tot = 0, cubes_tot = 0;
+  int64_t tiles_tot[3] = {0, 0, 0}, rays_tot[nsg::kRaySets] = {0, 0, 0, 0, 0, 0}, mc_tot = 0, rows_tot = 0, words_tot = 0, awords_tot = 0;
   int32_t patch_nstruct = 0;  // structures the uploaded patches belong to
   bool patch_struct_valid = false;
   std::vector<double> volumes, areas;
@@ -142,7 +142,7 @@ struct nsg_ctx {
   std::vector<double> cav_size;
   std::vector<int32_t> cav_filled;
   // mesh
-  DevBuf cube_vl, cube_map, vstruct;
+  DevBuf amap, valong, vstruct;
   nsg::TuneParams tune;
   DevBuf surv_cnt, surv_off, vpos, vkey, row_act_cnt, row_mid_cnt, row_act_off, row_mid_off, act_rec, act_mid,
       tri_cnt, tri_off, tris, cube_area, red_out, bnd_list, bnd_cursor;
@@ -226,7 +226,7 @@ int batch_layout(nsg_ctx* c, const NsGrid* grids, int32_t n) {
   std::vector<int4> chunks;  // marching-cubes row chunks: structure, first row, row count
   constexpr int32_t kRowChunk = 64;
   for (int i = 0; i < nsg::kRaySets; i++) rb[i].resize(n + 1);
-  int64_t tiles[3] = {0, 0, 0}, rays[nsg::kRaySets] = {0, 0, 0, 0, 0, 0}, mc = 0, rows = 0, words = 0, cubes = 0;
+  int64_t tiles[3] = {0, 0, 0}, rays[nsg::kRaySets] = {0, 0, 0, 0, 0, 0}, mc = 0, rows = 0, words = 0, awords = 0;
   for (int32_t b = 0; b < n; b++) {
     const NsGrid& G = grids[b];
     if (G.nx < 3 || G.ny < 3 || G.nz < 3) return fail(NSG_ERR_ARG, "grid must have at least 3 nodes per axis");
@@ -252,8 +252,8 @@ int batch_layout(nsg_ctx* c, const NsGrid* grids, int32_t n) {
     S.mc_base = mcb[b] = mc;
     mc += G.nz * G.ny + G.ny * G.nx + G.nz * G.nx;
     S.row_base = rowb[b] = rows;
-    S.cube_base = cubes;
-    cubes += (G.nx - 2) * (G.ny - 2) * (G.nz - 2);
+    S.aword_base = awords;
+    awords += ((G.nx - 2 + 31) / 32) * (G.ny - 2) * (G.nz - 2);
     const int64_t srows = (G.ny - 2) * (G.nz - 2);
     for (int64_t r = 0; r < srows; r += kRowChunk)
       chunks.push_back(make_int4(b, (int32_t)r, (int32_t)std::min<int64_t>(kRowChunk, srows - r), 0));
@@ -287,7 +287,7 @@ int batch_layout(nsg_ctx* c, const NsGrid* grids, int32_t n) {
   c->mc_tot = mc;
   c->rows_tot = rows;
   c->words_tot = words;
-  c->cubes_tot = cubes;
+  c->awords_tot = awords;
   c->has_grid = true;
   c->have_status = c->have_bits = false;
   c->volumes.assign(n, 0.0);
@@ -473,7 +473,7 @@ int nsg_ctx_destroy(nsg_ctx* c) {
                     &c->bgp_pos, &c->bgp_nor, &c->bgp_flag, &c->bgp_n, &c->aux_cnt, &c->aux_off, &c->aux_list, &c->pairs,
                     &c->ray_pair_off, &c->ray_pair_cnt, &c->cursors, &c->ovf_scratch, &c->err, &c->hits,
                     &c->pair_pid, &c->ovf_pscratch, &c->gvol, &c->garea, &c->vpid, &c->vgrad,
-                    &c->d_atoms, &c->d_patch_atoms, &c->d_gatoms_vol, &c->d_gatoms_area, &c->d_bad, &c->cube_vl, &c->cube_map, &c->vstruct,
+                    &c->d_atoms, &c->d_patch_atoms, &c->d_gatoms_vol, &c->d_gatoms_area, &c->d_bad, &c->amap, &c->valong, &c->vstruct,
                     &c->d_patch_off, &c->d_pool_off, &c->d_atom_off,
                     &c->labels, &c->is_root, &c->sruns, &c->srun_off, &c->srun_cnt, &c->fr_cnt, &c->fr_off,
                     &c->fruns, &c->frow, &c->roots, &c->cc_count, &c->cc_desc, &c->cc_label_of,
@@ -1445,7 +1445,9 @@ int nsg_triangulate(nsg_ctx* c, double* area_out, int64_t* nverts, int64_t* ntri
   // analytic vertices first (the midpoint pass needs their edge keys)
   CK(c->vkey.ensure(std::max<int64_t>(n_an, 1) * sizeof(int4)));
   CK(c->vpos.ensure(std::max<int64_t>(n_an, 1) * 3 * sizeof(double)));
+  CK(c->valong.ensure(std::max<int64_t>(n_an, 1) * sizeof(double)));
   V.vpos = c->vpos.as<double>();
+  V.valong = c->valong.as<double>();
   V.vkey = c->vkey.as<int4>();
   CK(c->vstruct.ensure(std::max<int64_t>(n_an, 1) * sizeof(int32_t)));
   V.vstruct = c->vstruct.as<int32_t>();
@@ -1459,6 +1461,7 @@ int nsg_triangulate(nsg_ctx* c, double* area_out, int64_t* nverts, int64_t* ntri
   stage_end(c, kStageVertex);
   stage_begin(c, kStageMC);
   M.vpos = c->vpos.as<double>();
+  M.valong = c->valong.as<double>();
   M.vkey = c->vkey.as<int4>();
   M.vstruct = c->vstruct.as<int32_t>();
   // active cubes
@@ -1476,13 +1479,9 @@ int nsg_triangulate(nsg_ctx* c, double* area_out, int64_t* nverts, int64_t* ntri
   M.mid_cnt = c->row_mid_cnt.as<int32_t>();
   M.mid_off = c->row_mid_off.as<int64_t>();
   M.n_active = n_act;
-  // the dense cube -> active-cube map (entries of inactive cubes are never read, so it is not
-  // cleared) and the vertex of every cut edge of every active cube, filled by the vertices
-  CK(c->cube_map.ensure(std::max<int64_t>(c->cubes_tot, 1) * sizeof(int32_t)));
-  CK(c->cube_vl.ensure(std::max<int64_t>(n_act, 1) * 12 * sizeof(int32_t)));
-  M.cube_map = c->cube_map.as<int32_t>();
-  M.cube_vl = c->cube_vl.as<int32_t>();
-  CK(cudaMemsetAsync(c->cube_vl.p, 0xff, std::max<int64_t>(n_act, 1) * 12 * sizeof(int32_t), c->stream));
+  // the active-cube map: per 32 cubes of a row, their active bits and the first one's index
+  CK(c->amap.ensure(std::max<int64_t>(c->awords_tot, 1) * sizeof(int2)));
+  M.amap = c->amap.as<int2>();
   // triangle counts per active cube: the case table's for interior cubes (written by the
   // classification), a count over the vertex slots for the listed low-face cubes
   CK(c->tri_cnt.ensure(std::max<int64_t>(n_act, 1) * sizeof(int32_t)));
@@ -1493,7 +1492,6 @@ int nsg_triangulate(nsg_ctx* c, double* area_out, int64_t* nverts, int64_t* ntri
   M.bnd_list = c->bnd_list.as<int32_t>();
   M.bnd_cursor = c->bnd_cursor.as<unsigned long long>();
   LAUNCH(nsg::launch_mc_rows(M, 1, c->stream));
-  LAUNCH(nsg::launch_mc_push(M, 0, n_an, c->stream));
   // midpoint vertices of cut edges without an analytic vertex
   LAUNCH(nsg::launch_mc_mid(M, 0, c->stream));
   rc = scan_counts(c, c->row_mid_cnt.as<int32_t>(), n_act, c->row_mid_off.as<int64_t>(), &n_mid);
@@ -1525,7 +1523,6 @@ int nsg_triangulate(nsg_ctx* c, double* area_out, int64_t* nverts, int64_t* ntri
   M.vkey = c->vkey.as<int4>();
   M.vstruct = c->vstruct.as<int32_t>();
   LAUNCH(nsg::launch_mc_mid(M, 1, c->stream));
-  LAUNCH(nsg::launch_mc_push(M, n_an, n_v, c->stream));
   M.n_active = n_act;
   CK(c->tri_off.ensure((n_act + 1) * sizeof(int64_t)));
   CK(c->cube_area.ensure(std::max<int64_t>(n_act, 1) * sizeof(double)));
@@ -1551,7 +1548,7 @@ int nsg_triangulate(nsg_ctx* c, double* area_out, int64_t* nverts, int64_t* ntri
   CK(c->tris.ensure(std::max<int64_t>(n_tri, 1) * 3 * sizeof(int32_t)));
   M.tri_off = c->tri_off.as<int64_t>();
   M.tris = c->tris.as<int32_t>();
-  LAUNCH(nsg::launch_mc_tris(M, 1, c->stream));
+  LAUNCH(nsg::launch_mc_tris(M, c->stream));
   if (grad) LAUNCH(nsg::launch_grad_vert(M, c->stream));
   c->have_garea = grad;
   // per-structure areas in an order fixed by the structure alone (independent of the batch)

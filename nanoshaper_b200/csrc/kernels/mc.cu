@@ -4,18 +4,20 @@
 // vertices on the grid edges that contain the interval ends; a vertex is dropped when the two
 // end nodes of its edge have the same final insideness, and the first vertex of an edge wins
 // (assembleVerticesList src/Surface.cpp:7415-7667).  Vertices keep the reference order: panel 0
-// rays (z-major), panel 1 rays (y-major), panel 2 rays (z-major), pairs in ray order.  Each vertex
-// writes its id into the slots of the (up to four) active cubes that share its grid edge
-// (atomicMin: the first vertex of an edge wins), through a dense cube -> active-cube map written
-// by the classification pass, so the triangle passes read every cut edge's vertex directly.
+// rays (z-major), panel 1 rays (y-major), panel 2 rays (z-major), pairs in ray order.  An edge's
+// vertices all come from the one ray that runs along it, so the vertex of a cut edge is found by
+// scanning that ray's (few) surviving vertices for the first on the edge; no per-cube vertex
+// table is built.
 //
-// Marching cubes: cubes (i,j,k) in [1, N-2]^3 are classified from the 8 insideness bits; active
-// cubes add an edge-midpoint vertex to their own edges 5, 6, 10 that carry no analytic vertex,
-// in (k, j, i, edge) order, appended after the analytic ones (getVertices :8002-8327); a second
-// pass emits the case-table triangles with reversed winding and sums their areas (the reference
-// sums Heron areas; here |cross product| / 2, the same quantity)
-// (triangulationKernel :9075-9318, getTriangles :14559-14780).  Triangles with an edge without a
-// vertex are skipped, as the reference does.
+// Marching cubes: cubes (i,j,k) in [1, N-2]^3 are classified from the 8 insideness bits; the
+// classification writes the active cubes in (k, j, i) order and, per 32 cubes of a row, their
+// active bits and the index of the first (the active-cube map, 8 bytes per 32 cubes, which finds
+// the active index of any active cube).  Active cubes add an edge-midpoint vertex to their own
+// edges 5, 6, 10 that carry no analytic vertex, in (k, j, i, edge) order, appended after the
+// analytic ones (getVertices :8002-8327); the triangle pass emits the case-table triangles with
+// reversed winding and sums their areas (the reference sums Heron areas; here |cross product| / 2,
+// the same quantity) (triangulationKernel :9075-9318, getTriangles :14559-14780).  Triangles
+// with an edge without a vertex are skipped, as the reference does.
 #include <cub/cub.cuh>
 
 #include "../mc_cases.h"
@@ -30,7 +32,14 @@ __constant__ int8_t c_tri[256][16];  // triangle edge lists, -1 terminated
 __constant__ uint16_t c_emask[256];  // cut-edge mask per case
 __constant__ uint8_t c_ntri[256];    // case-table triangles per case
 
+// Node coordinate, and the grid edge a point on a ray along axis d lies on: the nearest node after
+// the half-side shift, floor((p - min) * scale + 0.5).  Each operation is rounded on its own (the
+// file is built without contraction), so every kernel here that places or finds a vertex gets the
+// same doubles.
 __device__ __forceinline__ double gcoord(const GridDev& g, int d, int64_t i) { return g.mn[d] + (double)i * g.side; }
+__device__ __forceinline__ int64_t edge_index(const GridDev& g, int d, double p) {
+  return (int64_t)floor((p - g.mn[d]) * g.scale + 0.5);
+}
 
 __device__ __forceinline__ int rbit(const uint32_t* __restrict__ bits, int64_t nwords, int64_t f) {
   if (f < 0 || (f >> 5) >= nwords) return 1;
@@ -59,6 +68,17 @@ __device__ __forceinline__ int4 edge_key(const RayId& id, int64_t a) {
   return make_int4((int)id.m, (int)a, (int)id.n, NS_Y_DIR);
 }
 
+// The accurate-triangulation ray (batch-wide ordinal) that runs along grid edge (axis, x, y, z),
+// the inverse of ray_of / edge_key; *a = the edge's index along the ray.
+__device__ __forceinline__ int64_t edge_ray(const StructDev& S, int axis, int64_t x, int64_t y, int64_t z,
+                                            int64_t* a) {
+  const int64_t NX = S.g.n[0], NY = S.g.n[1], NZ = S.g.n[2];
+  if (axis == NS_X_DIR) { *a = x; return S.mc_base + z * NY + y; }
+  if (axis == NS_Z_DIR) { *a = z; return S.mc_base + NZ * NY + y * NX + x; }
+  *a = y;
+  return S.mc_base + NZ * NY + NY * NX + z * NX + x;
+}
+
 __device__ __forceinline__ bool keeps(const GridDev& g, const uint32_t* bits, int64_t nwords, int4 e) {
   const int64_t NX = g.n[0], NY = g.n[1];
   int64_t f = ((int64_t)e.z * NY + e.y) * NX + e.x;
@@ -78,10 +98,8 @@ __global__ void k_vert(VertArgs A, int emit) {
         RayId id = ray_of(g, r - S.mc_base);
         int vc = id.panel == 0 ? 0 : (id.panel == 1 ? 2 : 1);
         const double* pr = A.pairs + 2 * A.ray_pair_off[r];
-        for (int q = 0; q < 2 * np; q++) {
-          int64_t a = (int64_t)floor((pr[q] - g.mn[vc]) * g.scale + 0.5);
-          if (keeps(g, bits, S.nwords, edge_key(id, a))) cnt++;
-        }
+        for (int q = 0; q < 2 * np; q++)
+          if (keeps(g, bits, S.nwords, edge_key(id, edge_index(g, vc, pr[q])))) cnt++;
       }
       A.surv_cnt[r] = cnt;
       continue;
@@ -100,14 +118,14 @@ __global__ void k_vert(VertArgs A, int emit) {
     else { base[0] = gcoord(g, 0, id.m) + delta; base[2] = gcoord(g, 2, id.n) + delta; }
     int64_t o = A.surv_off[r];
     for (int q = 0; q < 2 * np; q++) {
-      int64_t a = (int64_t)floor((pr[q] - g.mn[vc]) * g.scale + 0.5);
-      int4 e = edge_key(id, a);
+      int4 e = edge_key(id, edge_index(g, vc, pr[q]));
       if (!keeps(g, bits, S.nwords, e)) continue;
       double p[3] = {base[0], base[1], base[2]};
       p[vc] = pr[q];
       A.vpos[3 * o + 0] = p[0];
       A.vpos[3 * o + 1] = p[1];
       A.vpos[3 * o + 2] = p[2];
+      A.valong[o] = pr[q];
       A.vkey[o] = e;
       A.vstruct[o] = (int32_t)(&S - A.B.s);
       if (A.vpid) {
@@ -121,10 +139,89 @@ __global__ void k_vert(VertArgs A, int emit) {
 
 __device__ __forceinline__ int rec_struct(int w) { return (int)((unsigned)w >> 11); }
 
+// Cube edge e (the case table's corner numbering): its axis and the offset of its grid-edge key
+// from the cube (i, j, k), packed as axis | dx << 2 | dy << 3 | dz << 4, 5 bits per edge:
+// edges 0, 2, 4, 6 along x at (i, j, k), (i, j+1, k), (i, j, k+1), (i, j+1, k+1); 3, 1, 7, 5 along
+// y at (i, j, k), (i+1, j, k), (i, j, k+1), (i+1, j, k+1); 8, 9, 11, 10 along z at (i, j, k),
+// (i+1, j, k), (i, j+1, k), (i+1, j+1, k).
+constexpr unsigned long long kCubeEdges = (0ull << 0) | (5ull << 5) | (8ull << 10) | (1ull << 15) | (16ull << 20) |
+                                          (21ull << 25) | (24ull << 30) | (17ull << 35) | (2ull << 40) |
+                                          (6ull << 45) | (14ull << 50) | (10ull << 55);
+__device__ __forceinline__ int cube_edge(int e) { return (int)((kCubeEdges >> (5 * e)) & 31); }
 
-// Local index of cube (i, j, k) in its structure's dense cube map.
-__device__ __forceinline__ int64_t cube_local(const GridDev& g, int64_t i, int64_t j, int64_t k) {
-  return ((k - 1) * (g.n[1] - 2) + (j - 1)) * (g.n[0] - 2) + (i - 1);
+// Active index of the active cube (i, j, k) of structure S, from the active-cube map.
+__device__ __forceinline__ int32_t active_index(const int2* __restrict__ amap, const StructDev& S, int64_t i,
+                                                int64_t j, int64_t k) {
+  const int64_t W = (S.g.n[0] - 2 + 31) >> 5;
+  const int64_t b = i - 1;
+  const int2 w = amap[S.aword_base + ((k - 1) * (S.g.n[1] - 2) + (j - 1)) * W + (b >> 5)];
+  return w.y + __popc((unsigned)w.x & ((1u << (b & 31)) - 1u));
+}
+
+// The first analytic vertex among ray vertices [lo, hi) whose edge index is a: its id, and its
+// coordinate along the ray in *along; -1 if none.
+__device__ __forceinline__ int32_t scan_ray(const double* __restrict__ valong, const GridDev& g, int axis, int64_t lo,
+                                            int64_t hi, int64_t a, double* along) {
+  for (int64_t v = lo; v < hi; v++) {
+    const double p = valong[v];
+    if (edge_index(g, axis, p) == a) {
+      *along = p;
+      return (int32_t)v;
+    }
+  }
+  return -1;
+}
+
+// The analytic vertex of grid edge (axis, x, y, z): -1 if none.
+__device__ __forceinline__ int32_t analytic_vertex(const MCArgs& A, const StructDev& S, int axis, int64_t x,
+                                                   int64_t y, int64_t z, double* along) {
+  int64_t a;
+  const int64_t r = edge_ray(S, axis, x, y, z, &a);
+  const int64_t lo = A.surv_off[r];
+  return scan_ray(A.valong, S.g, axis, lo, lo + A.surv_cnt[r], a, along);
+}
+
+// The midpoint vertex of grid edge (axis, x, y, z), added by the cube that has it as its edge 6
+// (x), 5 (y) or 10 (z): -1 if that cube lies outside the cube range or added none.  Only for cut
+// edges, whose four cubes are all active.
+__device__ __forceinline__ int32_t mid_vertex(const MCArgs& A, const StructDev& S, int axis, int64_t x, int64_t y,
+                                              int64_t z) {
+  int64_t i = x, j = y, k = z;
+  int bit;
+  if (axis == NS_X_DIR) { j--; k--; bit = 1; }
+  else if (axis == NS_Y_DIR) { i--; k--; bit = 0; }
+  else { i--; j--; bit = 2; }
+  if (i < 1 || j < 1 || k < 1 || i > S.g.n[0] - 2 || j > S.g.n[1] - 2 || k > S.g.n[2] - 2) return -1;
+  const int32_t o = active_index(A.amap, S, i, j, k);
+  const int mm = (reinterpret_cast<const int*>(A.act_rec + o)[3] >> 8) & 7;
+  if (!((mm >> bit) & 1)) return -1;
+  return A.act_mid[o] + __popc(mm & ((1 << bit) - 1));
+}
+
+// Vertex of cut edge e of cube (i, j, k): the analytic one, else the midpoint one; its coordinate
+// along the edge's axis in *along.
+__device__ __forceinline__ int32_t cube_edge_vertex(const MCArgs& A, const StructDev& S, int64_t i, int64_t j,
+                                                    int64_t k, int e, double* along) {
+  const int ce = cube_edge(e), ax = ce & 3;
+  const int64_t kx = i + ((ce >> 2) & 1), ky = j + ((ce >> 3) & 1), kz = k + ((ce >> 4) & 1);
+  int32_t v = analytic_vertex(A, S, ax, kx, ky, kz, along);
+  if (v < 0) {
+    v = mid_vertex(A, S, ax, kx, ky, kz);
+    *along = gcoord(S.g, ax, ax == 0 ? kx : (ax == 1 ? ky : kz));
+  }
+  return v;
+}
+
+// Position of the vertex of cube edge e of cube (i, j, k) from its coordinate along the edge: the
+// other two coordinates are those of the edge's ray (node + DELTA - side/2) for an analytic
+// vertex, node - side/2 for a midpoint one (as k_vert and k_mc_mid write them).
+__device__ __forceinline__ void vertex_pos(const GridDev& g, int64_t i, int64_t j, int64_t k, int e, bool analytic,
+                                           double along, double p[3]) {
+  const int ce = cube_edge(e), ax = ce & 3;
+  const double sh = analytic ? NS_DELTA - g.hside : -g.hside;
+  p[0] = ax == 0 ? along : gcoord(g, 0, i + ((ce >> 2) & 1)) + sh;
+  p[1] = ax == 1 ? along : gcoord(g, 1, j + ((ce >> 3) & 1)) + sh;
+  p[2] = ax == 2 ? along : gcoord(g, 2, k + ((ce >> 4) & 1)) + sh;
 }
 
 // The 32 bits of the flat bit grid starting at bit f (missing words read as outside), and in *next
@@ -145,7 +242,7 @@ __device__ __forceinline__ uint32_t bits32_pair(const uint32_t* __restrict__ bit
 // (corner inside = bit 0): a cube is active unless its 8 corners agree.  A row needs
 // W = ceil((NX-2)/32) lanes; when W <= 32 the warp packs 32/W rows side by side, otherwise it walks
 // the row in blocks of 32 words.  Pass 0 counts the active cubes of each row, pass 1 writes them
-// in i order at the row's offset.
+// in i order at the row's offset, and the row's words of the active-cube map.
 __global__ void k_mc_rows(MCArgs A, int emit) {
   __shared__ uint8_t s_ntri[256];
   for (int t = threadIdx.x; t < 256; t += blockDim.x) s_ntri[t] = c_ntri[t];
@@ -204,18 +301,18 @@ __global__ void k_mc_rows(MCArgs A, int emit) {
         }
         const int head_excl = __shfl_sync(0xffffffffu, incl - na, head);
         const int row_total = __shfl_sync(0xffffffffu, incl, tail) - head_excl;
-        if (emit && na) {
+        if (emit && row_ok && word < W) {
           int64_t slot = act_base + run + (incl - na - head_excl);
+          A.amap[S.aword_base + (int64_t)lr * W + word] = make_int2((int)act, (int)slot);
           for (uint32_t m = act; m; m &= m - 1) {
             int bit = __ffs(m) - 1;
             int cs = 0;
 #pragma unroll
             for (int q = 0; q < 8; q++) cs |= ((c[q] >> bit) & 1u) << q;
-            A.cube_map[S.cube_base + cube_local(S.g, ic + bit, j, k)] = (int32_t)slot;
             // every cut edge of a cube with i, j, k >= 2 has a vertex (an analytic one, or the
             // midpoint its owner cube adds), so its triangles are the case table's; a cube on the
             // low faces of the cube range may lack vertices on edges whose owner lies outside the
-            // range, and is counted after the vertices are in place (k_mc_tris_bnd)
+            // range, and is counted after the midpoint vertices are in place (k_mc_tris_bnd)
             if (ic + bit >= 2 && j >= 2 && k >= 2) {
               A.tri_cnt[slot] = s_ntri[cs];
             } else {
@@ -248,13 +345,14 @@ __global__ void k_mc_mid(MCArgs A, int emit) {
     const StructDev& S = A.B.s[rec_struct(rec.w)];
     const GridDev& g = S.g;
     if (!emit) {
-      // own edges 5 (y), 6 (x), 10 (z) that are cut and carry no analytic vertex
+      // own edges 5 (y at (i+1, j, k+1)), 6 (x at (i, j+1, k+1)), 10 (z at (i+1, j+1, k)) that are
+      // cut and carry no analytic vertex
       const int em = s_emask[rec.w & 255];
-      const int32_t* cv = A.cube_vl + 12 * a;
+      double al;
       int mm = 0;
-      if ((em & 32) && cv[5] < 0) mm |= 1;
-      if ((em & 64) && cv[6] < 0) mm |= 2;
-      if ((em & 1024) && cv[10] < 0) mm |= 4;
+      if ((em & 32) && analytic_vertex(A, S, NS_Y_DIR, i + 1, j, k + 1, &al) < 0) mm |= 1;
+      if ((em & 64) && analytic_vertex(A, S, NS_X_DIR, i, j + 1, k + 1, &al) < 0) mm |= 2;
+      if ((em & 1024) && analytic_vertex(A, S, NS_Z_DIR, i + 1, j + 1, k, &al) < 0) mm |= 4;
       A.act_rec[a].w = (rec.w & ~(7 << 8)) | (mm << 8);
       A.mid_cnt[a] = __popc(mm);
       continue;
@@ -283,128 +381,208 @@ __global__ void k_mc_mid(MCArgs A, int emit) {
   }
 }
 
-// One thread per vertex: the cubes that share its grid edge (x, y, z, axis) and the edge's number
-// in each of them; the vertex id goes into their slots, the smallest id of an edge winning.
-__global__ void k_mc_push(MCArgs A, int64_t v0, int64_t v1) {
-  for (int64_t v = v0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < v1; v += (int64_t)gridDim.x * blockDim.x) {
-    const int4 e = A.vkey[v];
-    const StructDev& S = A.B.s[A.vstruct[v]];
-    const GridDev& g = S.g;
-    // cube offsets and the edge's number in each cube: an x edge at (x, y, z) is edge 0 of cube
-    // (x, y, z), 2 of (x, y-1, z), 4 of (x, y, z-1) and 6 of (x, y-1, z-1); y and z edges alike
-    int t[4][4];
-    if (e.w == NS_X_DIR) {
-      const int u[4][4] = {{0, 0, 0, 0}, {0, -1, 0, 2}, {0, 0, -1, 4}, {0, -1, -1, 6}};
-      memcpy(t, u, sizeof t);
-    } else if (e.w == NS_Y_DIR) {
-      const int u[4][4] = {{0, 0, 0, 3}, {-1, 0, 0, 1}, {0, 0, -1, 7}, {-1, 0, -1, 5}};
-      memcpy(t, u, sizeof t);
-    } else {
-      const int u[4][4] = {{0, 0, 0, 8}, {-1, 0, 0, 9}, {0, -1, 0, 11}, {-1, -1, 0, 10}};
-      memcpy(t, u, sizeof t);
-    }
-#pragma unroll
-    for (int q = 0; q < 4; q++) {
-      const int64_t i = e.x + t[q][0], j = e.y + t[q][1], k = e.z + t[q][2];
-      if (i < 1 || j < 1 || k < 1 || i > g.n[0] - 2 || j > g.n[1] - 2 || k > g.n[2] - 2) continue;
-      const int32_t a = A.cube_map[S.cube_base + cube_local(g, i, j, k)];
-      atomicMin((unsigned int*)(A.cube_vl + 12 * (int64_t)a + t[q][3]), (unsigned int)v);
-    }
-  }
-}
-
 // Triangle counts of the active cubes on the low faces of the cube range (listed by k_mc_rows): the
 // case-table triangles whose three edges have vertices.
 __global__ void k_mc_tris_bnd(MCArgs A) {
   const int64_t n = (int64_t)*A.bnd_cursor;
   for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
     const int32_t a = A.bnd_list[q];
-    const int c = A.act_rec[a].w & 255;
-    const int32_t* cv = A.cube_vl + 12 * (int64_t)a;
+    const int4 rec = A.act_rec[a];
+    const int c = rec.w & 255;
+    const StructDev& S = A.B.s[rec_struct(rec.w)];
+    const int em = c_emask[c];
+    unsigned has = 0;
+    for (int e = 0; e < 12; e++) {
+      double al;
+      if (((em >> e) & 1) && cube_edge_vertex(A, S, rec.x, rec.y, rec.z, e, &al) >= 0) has |= 1u << e;
+    }
     int cnt = 0;
     for (int t = 0; t < 16 && c_tri[c][t] >= 0; t += 3)
-      if (cv[c_tri[c][t]] >= 0 && cv[c_tri[c][t + 1]] >= 0 && cv[c_tri[c][t + 2]] >= 0) cnt++;
+      if (((has >> c_tri[c][t]) & 1) && ((has >> c_tri[c][t + 1]) & 1) && ((has >> c_tri[c][t + 2]) & 1)) cnt++;
     A.tri_cnt[a] = cnt;
   }
 }
 
-// One thread per active cube, the vertex of every cut edge read from its slots: writes the
-// triangles whose three edges have vertices at the cube's offset and sums their areas (and, in
-// gradient mode, their derivatives with respect to the analytic vertices).  (Pass 0, the count of
-// those triangles, is kept for tests; the pipeline takes the counts from the classification.)
-__global__ void __launch_bounds__(128, 8) k_mc_tris(MCArgs A, int emit) {
-  __shared__ int8_t s_tri[256][16];
-  __shared__ uint16_t s_emask[256];
-  // vertex of cut edge e of this thread's cube at [e][thread]: the case table indexes it at run
-  // time, which a register array cannot serve
-  __shared__ int32_t s_vl[12][128];
+constexpr int kTrisThreads = 256;
+constexpr int kTrisWarps = kTrisThreads / 32;
+constexpr int kMaxCubeTris = 5;  // the most triangles of a case
+
+// Triangles, 32 active cubes per warp.  Every lane finds the vertices of its cube's cut edges (the
+// first vertex on the edge's ray, else the midpoint of the edge's owner cube): first the ray
+// ranges of all cut edges, then each range's first vertex, both as independent loads across the
+// edges, then the remaining scans and midpoint lookups.  The warp's triangles (tri_cnt per cube,
+// at tri_off) are then spread over the lanes, one per lane: it writes the triangle with reversed
+// winding and its area (and, in gradient mode, the area's derivatives with respect to its
+// analytic vertices); each cube's area is the sum of its triangles' in case-table order.
+struct TrisShared {
+  // per warp, per cube edge, per lane: the vertex of the cut edge; its coordinate along the edge
+  // (before that, the ray's vertex range); the areas of the warp's triangles
+  double s_alo[kTrisWarps][12][32];
+  double s_area[kTrisWarps][kMaxCubeTris * 32];
+  int32_t s_vid[kTrisWarps][12][32];
+  int8_t s_tri[256][16];
+  uint16_t s_emask[256];
+};
+
+__global__ void __launch_bounds__(kTrisThreads, 4) k_mc_tris(MCArgs A) {
+  extern __shared__ __align__(16) unsigned char s_raw[];
+  TrisShared& sh = *reinterpret_cast<TrisShared*>(s_raw);
+  auto& s_alo = sh.s_alo;
+  auto& s_area = sh.s_area;
+  auto& s_vid = sh.s_vid;
+  auto& s_tri = sh.s_tri;
+  auto& s_emask = sh.s_emask;
   for (int t = threadIdx.x; t < 256 * 16; t += blockDim.x) (&s_tri[0][0])[t] = (&c_tri[0][0])[t];
   for (int t = threadIdx.x; t < 256; t += blockDim.x) s_emask[t] = c_emask[t];
   __syncthreads();
-  int32_t* vl = &s_vl[0][threadIdx.x];
-  for (int64_t a = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; a < A.n_active; a += (int64_t)gridDim.x * blockDim.x) {
-    int4 rec = A.act_rec[a];
-    int c = rec.w & 255;
-    int64_t i = rec.x, j = rec.y, k = rec.z;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  int32_t* const vid = &s_vid[w][0][lane];
+  double* const alo = &s_alo[w][0][lane];
+  for (int64_t base = ((int64_t)blockIdx.x * kTrisWarps + w) * 32; base < A.n_active;
+       base += (int64_t)gridDim.x * kTrisThreads) {
+    const int64_t a = base + lane;
+    const bool valid = a < A.n_active;
+    const int4 rec = valid ? A.act_rec[a] : make_int4(1, 1, 1, 0);
     const StructDev& S = A.B.s[rec_struct(rec.w)];
-    (void)i; (void)j; (void)k; (void)S;
-    const int32_t* cv = A.cube_vl + 12 * a;
-    for (int e = 0; e < 12; e++) vl[e * 128] = cv[e];
-    int cnt = 0;
-    int64_t o = emit ? A.tri_off[a] : 0;
-    double area = 0.0;
-    for (int q = 0; q < 16 && s_tri[c][q] >= 0; q += 3) {
-      const int e0 = s_tri[c][q], e1 = s_tri[c][q + 1], e2 = s_tri[c][q + 2];
-      const int32_t v0 = vl[e0 * 128], v1 = vl[e1 * 128], v2 = vl[e2 * 128];
-      if (v0 < 0 || v1 < 0 || v2 < 0) continue;
-      if (!emit) {
-        cnt++;
-        continue;
+    const GridDev& g = S.g;
+    const int em = s_emask[rec.w & 255];
+    // ray vertex ranges of the cut edges
+#pragma unroll
+    for (int e = 0; e < 12; e++) {
+      int2 r = make_int2(0, 0);
+      if ((em >> e) & 1) {
+        const int ce = cube_edge(e);
+        int64_t ak;
+        const int64_t ray = edge_ray(S, ce & 3, rec.x + ((ce >> 2) & 1), rec.y + ((ce >> 3) & 1),
+                                     rec.z + ((ce >> 4) & 1), &ak);
+        const int32_t lo = (int32_t)A.surv_off[ray];
+        r = make_int2(lo, lo + A.surv_cnt[ray]);
       }
-      A.tris[3 * (o + cnt) + 0] = (int32_t)v2;
-      A.tris[3 * (o + cnt) + 1] = (int32_t)v1;
-      A.tris[3 * (o + cnt) + 2] = (int32_t)v0;
-      {
-        const double* P0 = A.vpos + 3 * (int64_t)v0;
-        const double* P1 = A.vpos + 3 * (int64_t)v1;
-        const double* P2 = A.vpos + 3 * (int64_t)v2;
-        const double p0[3] = {P0[0], P0[1], P0[2]}, p1[3] = {P1[0], P1[1], P1[2]}, p2[3] = {P2[0], P2[1], P2[2]};
-        // area = |n| / 2, n = (P1 - P0) x (P2 - P0): the area the reference computes with Heron's
-        // formula (getTriangles, src/Surface.cpp:14559-14780), with one square root instead of four
-        const double f1[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
-        const double f2[3] = {p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2]};
-        double nn[3] = {f1[1] * f2[2] - f1[2] * f2[1], f1[2] * f2[0] - f1[0] * f2[2], f1[0] * f2[1] - f1[1] * f2[0]};
-        const double nl = sqrt(nn[0] * nn[0] + nn[1] * nn[1] + nn[2] * nn[2]);
-        if (nl > 0) {
-          area += 0.5 * nl;
-          if (A.vgrad) {
-            // d area / d P0 = (P1 - P2) x n / (2 |n|), cyclic
-            {
-              const double h = 0.5 / nl;
-              nn[0] *= h;
-              nn[1] *= h;
-              nn[2] *= h;
-              // d area / d (position of vertex vv along the axis of its cube edge ev, which is
-              // the ray an analytic vertex moves on): ((Pa - Pb) x n / (2 |n|)) along that axis
-              const auto add = [&](int32_t vv, int ev, double dx, double dy, double dz) {
-                if (vv >= A.n_analytic) return;
-                double comp;
-                if (ev >= 8) comp = dx * nn[1] - dy * nn[0];        // z
-                else if (ev & 1) comp = dz * nn[0] - dx * nn[2];    // y
-                else comp = dy * nn[2] - dz * nn[1];                // x
-                if (comp != 0.0) atomicAdd(A.vgrad + vv, comp);
-              };
-              add(v0, e0, p1[0] - p2[0], p1[1] - p2[1], p1[2] - p2[2]);
-              add(v1, e1, p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2]);
-              add(v2, e2, p0[0] - p1[0], p0[1] - p1[1], p0[2] - p1[2]);
-            }
+      *reinterpret_cast<int2*>(alo + 32 * e) = r;
+    }
+    // the first vertex of each range: the edge's vertex when it lies on the edge (-2: scan on)
+#pragma unroll
+    for (int e = 0; e < 12; e++) {
+      int32_t v = -1;
+      if ((em >> e) & 1) {
+        const int2 r = *reinterpret_cast<const int2*>(alo + 32 * e);
+        if (r.x < r.y) {
+          const double p = A.valong[r.x];
+          const int ce = cube_edge(e), ax = ce & 3;
+          const int64_t ka = ax == 0 ? rec.x + ((ce >> 2) & 1) : (ax == 1 ? rec.y + ((ce >> 3) & 1) : rec.z + ((ce >> 4) & 1));
+          if (edge_index(g, ax, p) == ka) {
+            v = r.x;
+            alo[32 * e] = p;
+          } else if (r.y - r.x > 1) {
+            v = -2;
           }
         }
       }
-      cnt++;
+      vid[32 * e] = v;
     }
-    if (!emit) A.tri_cnt[a] = cnt;
-    else A.cube_area[a] = area;
+    // the rest of the scans, and midpoint vertices
+    for (int m = em; m; m &= m - 1) {
+      const int e = __ffs(m) - 1;
+      int32_t v = vid[32 * e];
+      if (v >= 0) continue;
+      const int ce = cube_edge(e), ax = ce & 3;
+      const int64_t kx = rec.x + ((ce >> 2) & 1), ky = rec.y + ((ce >> 3) & 1), kz = rec.z + ((ce >> 4) & 1);
+      const int64_t ka = ax == 0 ? kx : (ax == 1 ? ky : kz);
+      double p = 0.0;
+      if (v == -2) {
+        const int2 r = *reinterpret_cast<const int2*>(alo + 32 * e);
+        v = scan_ray(A.valong, g, ax, r.x + 1, r.y, ka, &p);
+      }
+      if (v < 0) {
+        v = mid_vertex(A, S, ax, kx, ky, kz);
+        p = gcoord(g, ax, ka);
+      }
+      vid[32 * e] = v;
+      alo[32 * e] = p;
+    }
+    // the warp's triangles
+    const int cnt = valid ? A.tri_cnt[a] : 0;
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int x = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += x;
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    const int64_t tbase = A.tri_off[base];
+    __syncwarp();
+    for (int t0 = 0; t0 < total; t0 += 32) {
+      const int t = t0 + lane;
+      // the cube of triangle t: the first lane whose inclusive count exceeds t
+      int l = 0;
+#pragma unroll
+      for (int step = 16; step; step >>= 1) {
+        const int x = __shfl_sync(0xffffffffu, incl, l + step - 1);
+        if (x <= t) l += step;
+      }
+      const int ll = l < 31 ? l : 31;
+      const int first = __shfl_sync(0xffffffffu, incl - cnt, ll);
+      const int ci = __shfl_sync(0xffffffffu, rec.x, ll), cj = __shfl_sync(0xffffffffu, rec.y, ll);
+      const int ck = __shfl_sync(0xffffffffu, rec.z, ll), cw = __shfl_sync(0xffffffffu, rec.w, ll);
+      if (t >= total) continue;
+      const int q = t - first;
+      const int c = cw & 255;
+      const GridDev& gt = A.B.s[rec_struct(cw)].g;
+      const int32_t* lv = &s_vid[w][0][ll];
+      const double* la = &s_alo[w][0][ll];
+      // the q-th case triangle whose three edges have vertices
+      int e0 = 0, e1 = 0, e2 = 0;
+      for (int qq = 0, seen = 0; qq < 15 && s_tri[c][qq] >= 0; qq += 3) {
+        e0 = s_tri[c][qq];
+        e1 = s_tri[c][qq + 1];
+        e2 = s_tri[c][qq + 2];
+        if (lv[32 * e0] >= 0 && lv[32 * e1] >= 0 && lv[32 * e2] >= 0) {
+          if (seen == q) break;
+          seen++;
+        }
+      }
+      const int32_t v0 = lv[32 * e0], v1 = lv[32 * e1], v2 = lv[32 * e2];
+      A.tris[3 * (tbase + t) + 0] = v2;
+      A.tris[3 * (tbase + t) + 1] = v1;
+      A.tris[3 * (tbase + t) + 2] = v0;
+      double p0[3], p1[3], p2[3];
+      vertex_pos(gt, ci, cj, ck, e0, v0 < A.n_analytic, la[32 * e0], p0);
+      vertex_pos(gt, ci, cj, ck, e1, v1 < A.n_analytic, la[32 * e1], p1);
+      vertex_pos(gt, ci, cj, ck, e2, v2 < A.n_analytic, la[32 * e2], p2);
+      // area = |n| / 2, n = (P1 - P0) x (P2 - P0): the area the reference computes with Heron's
+      // formula (getTriangles, src/Surface.cpp:14559-14780), with one square root instead of four
+      const double f1[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
+      const double f2[3] = {p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2]};
+      double nn[3] = {f1[1] * f2[2] - f1[2] * f2[1], f1[2] * f2[0] - f1[0] * f2[2], f1[0] * f2[1] - f1[1] * f2[0]};
+      const double nl = sqrt(nn[0] * nn[0] + nn[1] * nn[1] + nn[2] * nn[2]);
+      s_area[w][t] = nl > 0 ? 0.5 * nl : 0.0;
+      if (nl > 0 && A.vgrad) {
+        // d area / d (position of vertex vv along the axis of its cube edge ev, which is the ray
+        // an analytic vertex moves on): ((Pa - Pb) x n / (2 |n|)) along that axis
+        const double h = 0.5 / nl;
+        nn[0] *= h;
+        nn[1] *= h;
+        nn[2] *= h;
+        const auto add = [&](int32_t vv, int ev, double dx, double dy, double dz) {
+          if (vv >= A.n_analytic) return;
+          double comp;
+          if (ev >= 8) comp = dx * nn[1] - dy * nn[0];        // z
+          else if (ev & 1) comp = dz * nn[0] - dx * nn[2];    // y
+          else comp = dy * nn[2] - dz * nn[1];                // x
+          if (comp != 0.0) atomicAdd(A.vgrad + vv, comp);
+        };
+        add(v0, e0, p1[0] - p2[0], p1[1] - p2[1], p1[2] - p2[2]);
+        add(v1, e1, p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2]);
+        add(v2, e2, p0[0] - p1[0], p0[1] - p1[1], p0[2] - p1[2]);
+      }
+    }
+    __syncwarp();
+    if (valid) {
+      double area = 0.0;
+      for (int q = 0; q < cnt; q++) area += s_area[w][incl - cnt + q];
+      A.cube_area[a] = area;
+    }
+    __syncwarp();
   }
 }
 
@@ -524,9 +702,22 @@ cudaError_t launch_mc_mid(const MCArgs& A, int emit, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_mc_tris(const MCArgs& A, int emit, cudaStream_t s) {
+cudaError_t launch_mc_tris(const MCArgs& A, cudaStream_t s) {
   if (A.n_active <= 0) return cudaSuccess;
-  k_mc_tris<<<grid_for(A.n_active, 128), 128, 0, s>>>(A, emit);
+  // the shared block is above the 48 KB of a static allocation: opt in once per device
+  static bool opted[64] = {false};
+  int dev = 0;
+  cudaError_t err = cudaGetDevice(&dev);
+  if (err != cudaSuccess) return err;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  if (!opted[dev]) {
+    err = cudaFuncSetAttribute(k_mc_tris, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TrisShared));
+    if (err != cudaSuccess) return err;
+    opted[dev] = true;
+  }
+  int64_t b = (A.n_active + kTrisThreads - 1) / kTrisThreads;
+  const int64_t cap = (int64_t)sm_count() * 4 * 8;
+  k_mc_tris<<<(unsigned)(b < cap ? b : cap), kTrisThreads, sizeof(TrisShared), s>>>(A);
   return cudaGetLastError();
 }
 
@@ -540,12 +731,6 @@ cudaError_t launch_vertex_normals(const double* vpos, const int32_t* vpid, int64
 cudaError_t launch_mc_tris_bnd(const MCArgs& A, cudaStream_t s) {
   if (A.n_active <= 0) return cudaSuccess;
   k_mc_tris_bnd<<<sm_count() * 4, 256, 0, s>>>(A);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_mc_push(const MCArgs& A, int64_t v0, int64_t v1, cudaStream_t s) {
-  if (v1 <= v0) return cudaSuccess;
-  k_mc_push<<<grid_for(v1 - v0, 256), 256, 0, s>>>(A, v0, v1);
   return cudaGetLastError();
 }
 

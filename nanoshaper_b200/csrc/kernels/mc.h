@@ -19,6 +19,7 @@ struct VertArgs {
   int32_t* surv_cnt;             // surviving vertices per ray
   const int64_t* surv_off;       // exclusive scan of surv_cnt
   double* vpos;                  // 3 per vertex
+  double* valong;                // per analytic vertex: its coordinate along its ray
   int4* vkey;                    // ix, iy, iz, dir per vertex
   int32_t* vstruct;              // structure of every vertex
   const int2* pair_pid;          // gradient mode: patches of the pair ends, else null
@@ -31,6 +32,7 @@ struct MCArgs {
   const int32_t* surv_cnt;
   const int64_t* surv_off;
   int64_t n_analytic;
+  const double* valong;          // coordinate of every analytic vertex along its ray
   double* vpos;
   int4* vkey;
   int32_t* vstruct;              // structure of every vertex
@@ -47,8 +49,10 @@ struct MCArgs {
   int32_t* tri_cnt;               // triangles per active cube (interior cubes: from the classification)
   int32_t* bnd_list;             // active cubes on the low faces of the cube range
   unsigned long long* bnd_cursor;
-  int32_t* cube_vl;              // 12 per active cube: vertex of each cut edge (-1 none)
-  int32_t* cube_map;             // dense per structure (cube_base): active index of every active cube
+  // active-cube map, one entry per 32 cubes of a cube row (W = ceil((NX-2)/32) per row, rows of a
+  // structure from its aword_base): the cubes' active bits and the active index of the first
+  // active cube of the word
+  int2* amap;
   const int64_t* tri_off;
   int32_t* tris;
   double* cube_area;
@@ -66,12 +70,9 @@ cudaError_t mc_init_tables();
 cudaError_t launch_vert(const VertArgs& A, int emit, cudaStream_t s);
 cudaError_t launch_mc_rows(const MCArgs& A, int emit, cudaStream_t s);
 cudaError_t launch_mc_mid(const MCArgs& A, int emit, cudaStream_t s);
-cudaError_t launch_mc_tris(const MCArgs& A, int emit, cudaStream_t s);
-// Triangle counts of the listed low-face cubes, once every vertex is in its cube slots.
+cudaError_t launch_mc_tris(const MCArgs& A, cudaStream_t s);
+// Triangle counts of the listed low-face cubes, once the midpoint vertices are in place.
 cudaError_t launch_mc_tris_bnd(const MCArgs& A, cudaStream_t s);
-// Every vertex in [v0, v1) writes its id into the cube_vl slots of the (up to four) active cubes
-// that share its grid edge; the smallest id of an edge wins (atomicMin).
-cudaError_t launch_mc_push(const MCArgs& A, int64_t v0, int64_t v1, cudaStream_t s);
 // Analytic normal of every analytic vertex v < n_analytic from its patch vpid[v] (zero for patch
 // kinds without one, e.g. mesh triangles); 3 doubles per vertex.
 cudaError_t launch_vertex_normals(const double* vpos, const int32_t* vpid, int64_t n_analytic, const double* f64,

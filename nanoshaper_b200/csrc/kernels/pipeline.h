@@ -51,7 +51,7 @@ struct StructDev {
   int64_t ray_base[kRaySets];  // first ray of each ray set in the set's ray arrays
   int64_t mc_base;       // first accurate-triangulation ray ordinal (its 3 panels are contiguous)
   int64_t row_base;      // first marching-cubes row ((NY-2)*(NZ-2) rows per structure)
-  int64_t cube_base;     // first entry of its dense cube map ((NX-2)*(NY-2)*(NZ-2) cubes)
+  int64_t aword_base;    // first entry of its active-cube map (ceil((NX-2)/32) per cube row)
   double A;              // side^2: the area of one pixel, volume weight of an interval length
   double ray_dir[3];     // ray length along each axis: coordinate of the last node minus the first
   double inv_dir[3];     // 1 / ray_dir

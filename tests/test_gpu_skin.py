@@ -8,8 +8,9 @@
   precision (FP32 ray-quadric and plane tests with FP64 refinement): every ray's hit count equal,
   hits within 1e-5 A, status map and insideness bits equal except at nodes whose oracle hit lies
   within 1e-6 A of the node (counted).
-* The reference's 6xm4 skin fixture (48,519 atoms, scale 2, perfil 90): status map and insideness
-  bits in double precision.
+* The reference's 6xm4 skin fixture (48,519 atoms, scale 2, perfil 90, Build_epsilon_maps on) in
+  double precision: every ray's hits over all six ray sets (the epsilon map's node rays included),
+  status map, insideness bits, epsilon and ideb maps, and the volume averaged over the six sets.
 """
 import gzip
 import shutil
@@ -28,13 +29,14 @@ HIT_TOL = 1e-12
 
 
 def _ray_len(g, s):
-    return ((g.nx - 1) * g.side, (g.nx - 1) * g.side, (g.nz - 1) * g.side, (g.ny - 1) * g.side)[s]
+    return ((g.nx - 1) * g.side, (g.nx - 1) * g.side, (g.nz - 1) * g.side, (g.ny - 1) * g.side,
+            (g.nz - 1) * g.side, (g.ny - 1) * g.side)[s]
 
 
-def _compare_hits(surf, ref, oracle_mod, angstrom=False):
+def _compare_hits(surf, ref, oracle_mod, angstrom=False, sets=range(4)):
     worst = 0.0
     g = surf.delphi.grid
-    for s in range(4):
+    for s in sets:
         cnt_g, val_g = surf.hits(s)
         cnt_o, val_o = oracle_mod.ray_hits(ref, s)
         if not np.array_equal(cnt_g, cnt_o):
@@ -125,14 +127,19 @@ def test_skin_fixture_6xm4_maps(native_lib, oracle_mod, tmp_path):
     assert len(ns.ds.atoms) == 48519
     ns.buildAnalyticalSurface()
     surf, ds = ns.surf, ns.ds
+    # the fixture builds the epsilon map: six ray sets, the volume averaged over all six
+    assert ds.buildEpsMap
     vol = surf.getSurf(True, False, 0.0, keep_hits=True)
-    ref = oracle_mod.run(ds.grid, surf.patches, flags=oracle_mod.STATUS | oracle_mod.ACCURATE_TRIANGULATION,
-                         threads=8)
-    worst = _compare_hits(surf, ref, oracle_mod)
+    ref = oracle_mod.run(ds.grid, surf.patches, threads=8,
+                         flags=oracle_mod.STATUS | oracle_mod.ACCURATE_TRIANGULATION | oracle_mod.EPSMAP)
+    worst = _compare_hits(surf, ref, oracle_mod, sets=range(6))
     assert worst <= HIT_TOL
     n_mis, n_near = compare.near_node_status(ds.status, ref, ds.grid)
     assert n_mis == n_near
     assert np.array_equal(surf.insideness, ref.bits)
+    e_mis, e_near = compare.near_threshold_eps(ds.epsmap, ref, ds.grid)
+    assert e_mis == 0, f"{e_mis} epsilon-map entries differ ({e_near} near a threshold)"
+    assert np.array_equal(ds.idebmap, ref.idebmap)
     assert abs(vol - ref.volume) <= 1e-12 * abs(ref.volume), f"volume {vol} vs {ref.volume}"
     print(f"6xm4 skin ({surf.patches.n} cells, grid {ds.nx}^3): status mismatches {n_mis} (near-node {n_near}), "
-          f"worst hit diff {worst:.2e}")
+          f"worst hit diff {worst:.2e}, epsilon map exact")
