@@ -123,6 +123,11 @@ int nsg_write_status(const char* path, const int32_t* status, int64_t nx, int64_
 /* DelPhiShared::saveCavities (src/DelphiShared.cpp:1889-1946): cavities.txt and cavitiesSize.txt. */
 int nsg_write_cavities(const char* cavities_path, const char* sizes_path, const int32_t* status, const NsGrid* grid,
                        int32_t n_cavities, const double* sizes, const int32_t* filled);
+/* DelPhiShared::saveCavities' cavAtomsSerials.txt (src/DelphiShared.cpp:1946-1962): one line per
+ * cavity, its atoms' serials ("%d " each; the atom index + 1 unless serials gives a positive
+ * serial), cavities with skip[c] != 0 left out (skip may be NULL: onlySaveNonFilled = false). */
+int nsg_write_cavity_atoms(const char* path, int32_t n_cavities, const int32_t* offsets, const int32_t* atoms,
+                           const int32_t* serials, int64_t n_atoms, const int32_t* skip);
 /* Surface::saveMesh (src/Surface.cpp:10857-11052): format 0 = root.off + roottriangleAreas.txt,
  * 1 = root.ply (binary); revert writes every triangle in the opposite winding. */
 int nsg_write_mesh(const char* root, int format, const double* vertices, int64_t n_vertices, const int32_t* triangles,
@@ -181,9 +186,10 @@ int nsg_batch_results(nsg_ctx* ctx, double* volumes, double* areas);
 /* ---- launch-shape tuning (no counterpart in the reference) ----
  * params: [intersection threads per block (64..256), intersection blocks per SM (1..64),
  * candidate-kernel threads per block (32..256), and optionally (n >= 4) the ray sets on concurrent
- * streams (1, default) or not, and (n >= 5) the torus candidates split by resolvent branch before
- * the solve (1) or not (0, default: measured slower on the ensemble); results do not depend on
- * any of them].  nsg_autotune times
+ * streams (1, default) or not, (n >= 5) the torus candidates split by resolvent branch before
+ * the solve (1) or not (0, default: measured slower on the ensemble), and (n >= 6) the blocks per
+ * SM of the marching-cubes triangle kernel (3, default, or 4); results do not depend on any of
+ * them].  nsg_autotune times
  * `reps` ray casts of the current batch per candidate shape and keeps the fastest in the
  * context. */
 int nsg_set_tuning(nsg_ctx* ctx, const int32_t* params, int n);
@@ -256,6 +262,18 @@ int nsg_download_insideness(nsg_ctx* ctx, uint32_t* dst);
 int nsg_download_mesh(nsg_ctx* ctx, double* vertices, int32_t* vertex_edges, int32_t* triangles);
 /* cavitiesSize / cavitiesFlag of DelPhiShared (src/DelphiShared.h:160-213). */
 int nsg_download_cavities(nsg_ctx* ctx, double* sizes, int32_t* filled);
+/* Atoms lining each cavity of the last nsg_cavities: DelPhiShared::cav2atoms as
+ * Surface::getCavitiesAtomsWithBilevelStatusMap fills it (src/Surface.cpp:2249-2346).  Every node
+ * of cavity c (status 4 + c) with a 6-neighbour of another status (outside the grid counts as
+ * status 2) contributes the atom of least |a - x|^2 - r^2 among the atoms of the 27 cells around
+ * it in the reference's atom grid (buildAtomsMap, src/Surface.cpp:1695-1749: side 2 r_max, halved
+ * until it spans 1.3 rmaxdim in at most 100 cells, centred on the grid's barycentre), the first
+ * of equal ones in cell order, or -1 when those cells hold no atom.  atoms_xyzr: the structure's
+ * atoms (x, y, z, radius).  Per cavity, its distinct atoms ascending (std::set order, -1 first) at
+ * offsets[c] .. offsets[c + 1] of atoms (n_cav + 1 offsets); with atoms == NULL only *n_total is
+ * set.  The result is kept until the next cast or cavity detection. */
+int nsg_cavity_atoms(nsg_ctx* ctx, const double* atoms_xyzr, int64_t n_atoms, int32_t* offsets, int32_t* atoms,
+                     int64_t* n_total);
 /* Sorted hit parameters per ray of one ray set (tests); sets 0 status, 1..3 accurate triangulation,
  * 4 and 5 the epsilon-map node rays along z and y. */
 int nsg_download_hits(nsg_ctx* ctx, int ray_set, int32_t* counts, double* dst, int64_t dst_capacity);

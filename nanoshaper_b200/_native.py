@@ -78,6 +78,7 @@ _SIGNATURES = {
     "nsg_download_insideness": ([_P, _P], _INT),
     "nsg_download_mesh": ([_P, _P, _P, _P], _INT),
     "nsg_download_cavities": ([_P, _P, _P], _INT),
+    "nsg_cavity_atoms": ([_P, _P, _I64, _P, _P, ctypes.POINTER(_I64)], _INT),
     "nsg_download_hits": ([_P, _INT, _P, _P, _I64], _INT),
     "nsg_download_epsmap": ([_P, _P], _INT),
     "nsg_download_idebmap": ([_P, _P], _INT),
@@ -114,6 +115,7 @@ _SIGNATURES = {
     "nsg_write_status": ([ctypes.c_char_p, _P, _I64, _I64, _I64], _INT),
     "nsg_write_cavities": ([ctypes.c_char_p, ctypes.c_char_p, _P, ctypes.POINTER(NsGrid), ctypes.c_int32, _P, _P],
                            _INT),
+    "nsg_write_cavity_atoms": ([ctypes.c_char_p, ctypes.c_int32, _P, _P, _P, _I64, _P], _INT),
     "nsg_write_mesh": ([ctypes.c_char_p, _INT, _P, _I64, _P, _I64, _INT], _INT),
     "nsg_mesh_normals": ([_P, _I64, _P, _I64, _P], _INT),
     "nsg_vertex_atoms": ([_P, _I64, _P, _I64, _P], _INT),

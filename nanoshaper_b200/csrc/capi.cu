@@ -141,8 +141,13 @@ struct nsg_ctx {
   int ncav = 0;
   std::vector<double> cav_size;
   std::vector<int32_t> cav_filled;
+  int64_t cav_nodes = 0;                       // nodes of all cavities (labels >= 4)
+  bool cav_detected = false;                   // nsg_cavities ran on the last cast
+  bool have_cav_atoms = false;
+  std::vector<int32_t> cav_atom_off, cav_atom_list;
+  DevBuf ca_atoms, ca_cell_off, ca_cell_atoms, ca_pairs, ca_alt, ca_count;
   // mesh
-  DevBuf amap, valong, vstruct;
+  DevBuf amap, cube_vl, vstruct;
   nsg::TuneParams tune;
   DevBuf surv_cnt, surv_off, vpos, vkey, row_act_cnt, row_mid_cnt, row_act_off, row_mid_off, act_rec, act_mid,
       tri_cnt, tri_off, tris, cube_area, red_out, bnd_list, bnd_cursor;
@@ -224,7 +229,7 @@ int batch_layout(nsg_ctx* c, const NsGrid* grids, int32_t n) {
   std::vector<int64_t> rb[nsg::kRaySets], mcb(n + 1), rowb(n + 1);
   std::vector<int32_t> ts[3];
   std::vector<int4> chunks;  // marching-cubes row chunks: structure, first row, row count
-  constexpr int32_t kRowChunk = 64;
+  constexpr int32_t kRowChunk = 32;  // cube rows per chunk: one warp, one row per lane
   for (int i = 0; i < nsg::kRaySets; i++) rb[i].resize(n + 1);
   int64_t tiles[3] = {0, 0, 0}, rays[nsg::kRaySets] = {0, 0, 0, 0, 0, 0}, mc = 0, rows = 0, words = 0, awords = 0;
   for (int32_t b = 0; b < n; b++) {
@@ -317,14 +322,15 @@ void stage_begin(nsg_ctx* c, int id) {
   cudaEventRecord(c->st_ev[2 * id], c->stream);
 }
 
-void stage_end(nsg_ctx* c, int id) {
+// A stage may be timed in several intervals per call; the last one passes count = true.
+void stage_end(nsg_ctx* c, int id, bool count = true) {
   if (!c->profile) return;
   cudaEventRecord(c->st_ev[2 * id + 1], c->stream);
   cudaEventSynchronize(c->st_ev[2 * id + 1]);
   float ms = 0;
   cudaEventElapsedTime(&ms, c->st_ev[2 * id], c->st_ev[2 * id + 1]);
   c->stage_ms[id] += ms;
-  c->stage_calls[id]++;
+  if (count) c->stage_calls[id]++;
 }
 
 #define LAUNCH(call)  \
@@ -473,7 +479,7 @@ int nsg_ctx_destroy(nsg_ctx* c) {
                     &c->bgp_pos, &c->bgp_nor, &c->bgp_flag, &c->bgp_n, &c->aux_cnt, &c->aux_off, &c->aux_list, &c->pairs,
                     &c->ray_pair_off, &c->ray_pair_cnt, &c->cursors, &c->ovf_scratch, &c->err, &c->hits,
                     &c->pair_pid, &c->ovf_pscratch, &c->gvol, &c->garea, &c->vpid, &c->vgrad,
-                    &c->d_atoms, &c->d_patch_atoms, &c->d_gatoms_vol, &c->d_gatoms_area, &c->d_bad, &c->amap, &c->valong, &c->vstruct,
+                    &c->d_atoms, &c->d_patch_atoms, &c->d_gatoms_vol, &c->d_gatoms_area, &c->d_bad, &c->amap, &c->cube_vl, &c->vstruct, &c->ca_atoms, &c->ca_cell_off, &c->ca_cell_atoms, &c->ca_pairs, &c->ca_alt, &c->ca_count,
                     &c->d_patch_off, &c->d_pool_off, &c->d_atom_off,
                     &c->labels, &c->is_root, &c->sruns, &c->srun_off, &c->srun_cnt, &c->fr_cnt, &c->fr_off,
                     &c->fruns, &c->frow, &c->roots, &c->cc_count, &c->cc_desc, &c->cc_label_of,
@@ -751,6 +757,10 @@ int nsg_set_tuning(nsg_ctx* c, const int32_t* params, int n) {
   c->tune.cand_threads = ct;
   if (n >= 4) c->concurrent_sets = params[3] != 0;
   if (n >= 5) c->tune.torus_split = params[4] != 0;
+  if (n >= 6) {
+    if (params[5] != 3 && params[5] != 4) return fail(NSG_ERR_ARG, "tuning parameter 5 is 3 or 4");
+    c->tune.mc_tris_bpsm = params[5];
+  }
   return NSG_OK;
 }
 
@@ -761,6 +771,7 @@ int nsg_get_tuning(nsg_ctx* c, int32_t* params, int n) {
   params[2] = c->tune.cand_threads;
   if (n >= 4) params[3] = c->concurrent_sets ? 1 : 0;
   if (n >= 5) params[4] = c->tune.torus_split;
+  if (n >= 6) params[5] = c->tune.mc_tris_bpsm;
   return NSG_OK;
 }
 
@@ -1284,6 +1295,7 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
     if (rc) return rc;
   }
   c->status_dense = false;
+  c->cav_detected = c->have_cav_atoms = false;
   c->have_gvol = grad;
   c->have_pids = pids && do_mc;
   c->have_status = do_status || do_eps;
@@ -1331,6 +1343,8 @@ int nsg_cavities(nsg_ctx* c, double cav_vol, int* ncav_out) {
   const int64_t nr = c->n_fruns;
   c->cav_size.clear();
   c->cav_filled.clear();
+  c->cav_nodes = 0;
+  c->cav_detected = c->have_cav_atoms = false;
   stage_begin(c, kStageCavity);
   CK(c->labels.ensure(std::max<int64_t>(nr, 1) * sizeof(int32_t)));
   CK(c->is_root.ensure(std::max<int64_t>(nr, 1)));
@@ -1355,6 +1369,7 @@ int nsg_cavities(nsg_ctx* c, double cav_vol, int* ncav_out) {
     int rc = materialize_status(c, nullptr);
     if (rc) return rc;
     stage_end(c, kStageCavity);
+    c->cav_detected = true;
     if (ncav_out) *ncav_out = 0;
     return NSG_OK;
   }
@@ -1381,6 +1396,7 @@ int nsg_cavities(nsg_ctx* c, double cav_vol, int* ncav_out) {
     int lab = label_of[r];
     if (lab < NS_STATUS_FIRST_CAV) continue;
     double v = (double)cnt[r] * cube;
+    c->cav_nodes += (int64_t)cnt[r];
     c->cav_size[lab - NS_STATUS_FIRST_CAV] = v;
     if (v <= cav_vol) {
       c->cav_filled[lab - NS_STATUS_FIRST_CAV] = 1;
@@ -1402,6 +1418,7 @@ int nsg_cavities(nsg_ctx* c, double cav_vol, int* ncav_out) {
   if (rc) return rc;
   stage_end(c, kStageCavity);
   CK(cudaStreamSynchronize(c->stream));
+  c->cav_detected = true;
   if (ncav_out) *ncav_out = c->ncav;
   c->n_vert = c->n_tri = 0;
   return NSG_OK;
@@ -1442,12 +1459,47 @@ int nsg_triangulate(nsg_ctx* c, double* area_out, int64_t* nverts, int64_t* ntri
   M.n_analytic = n_an;
   M.nrows = nrows;
   M.row_act_cnt = c->row_act_cnt.as<int64_t>();
-  // analytic vertices first (the midpoint pass needs their edge keys)
+  stage_end(c, kStageVertex, false);
+  stage_begin(c, kStageMC);
+  // active cubes, their map and vertex slots (the vertex pass writes into the slots)
+  LAUNCH(nsg::launch_mc_rows(M, 0, c->stream));
+  int64_t n_act = 0, n_mid = 0;
+  rc = scan_counts(c, c->row_act_cnt.as<int64_t>(), nrows, c->row_act_off.as<int64_t>(), &n_act);
+  if (rc) return rc;
+  if (n_act >= ((int64_t)1 << 31) / 12) return fail(NSG_ERR_CAPACITY, "too many active cubes in one batch");
+  M.row_act_off = c->row_act_off.as<int64_t>();
+  CK(c->act_rec.ensure(std::max<int64_t>(n_act, 1) * sizeof(int4)));
+  CK(c->act_mid.ensure(std::max<int64_t>(n_act, 1) * sizeof(int32_t)));
+  CK(c->row_mid_cnt.ensure(std::max<int64_t>(n_act, 1) * sizeof(int32_t)));
+  CK(c->row_mid_off.ensure((n_act + 1) * sizeof(int64_t)));
+  M.act_rec = c->act_rec.as<int4>();
+  M.act_mid = c->act_mid.as<int32_t>();
+  M.mid_cnt = c->row_mid_cnt.as<int32_t>();
+  M.mid_off = c->row_mid_off.as<int64_t>();
+  M.n_active = n_act;
+  // the active-cube map (per 32 cubes of a row: their active bits and the first one's index) and
+  // 12 vertex slots per active cube; only the slots a cube reads are written (the low-face cubes'
+  // all start at -1), so they are not cleared
+  CK(c->amap.ensure(std::max<int64_t>(c->awords_tot, 1) * sizeof(int2)));
+  CK(c->cube_vl.ensure(std::max<int64_t>(n_act, 1) * 12 * sizeof(int32_t)));
+  M.amap = c->amap.as<int2>();
+  M.cube_vl = c->cube_vl.as<int32_t>();
+  // triangle counts per active cube: the case table's for interior cubes (written by the
+  // classification), a count over the vertex slots for the listed low-face cubes
+  CK(c->tri_cnt.ensure(std::max<int64_t>(n_act, 1) * sizeof(int32_t)));
+  CK(c->bnd_list.ensure(std::max<int64_t>(n_act, 1) * sizeof(int32_t)));
+  CK(c->bnd_cursor.ensure(sizeof(unsigned long long)));
+  CK(cudaMemsetAsync(c->bnd_cursor.p, 0, sizeof(unsigned long long), c->stream));
+  M.tri_cnt = c->tri_cnt.as<int32_t>();
+  M.bnd_list = c->bnd_list.as<int32_t>();
+  M.bnd_cursor = c->bnd_cursor.as<unsigned long long>();
+  LAUNCH(nsg::launch_mc_rows(M, 1, c->stream));
+  stage_end(c, kStageMC, false);
+  // analytic vertices, then each first vertex of an edge into the slots of the edge's cubes
+  stage_begin(c, kStageVertex);
   CK(c->vkey.ensure(std::max<int64_t>(n_an, 1) * sizeof(int4)));
   CK(c->vpos.ensure(std::max<int64_t>(n_an, 1) * 3 * sizeof(double)));
-  CK(c->valong.ensure(std::max<int64_t>(n_an, 1) * sizeof(double)));
   V.vpos = c->vpos.as<double>();
-  V.valong = c->valong.as<double>();
   V.vkey = c->vkey.as<int4>();
   CK(c->vstruct.ensure(std::max<int64_t>(n_an, 1) * sizeof(int32_t)));
   V.vstruct = c->vstruct.as<int32_t>();
@@ -1461,37 +1513,9 @@ int nsg_triangulate(nsg_ctx* c, double* area_out, int64_t* nverts, int64_t* ntri
   stage_end(c, kStageVertex);
   stage_begin(c, kStageMC);
   M.vpos = c->vpos.as<double>();
-  M.valong = c->valong.as<double>();
   M.vkey = c->vkey.as<int4>();
   M.vstruct = c->vstruct.as<int32_t>();
-  // active cubes
-  LAUNCH(nsg::launch_mc_rows(M, 0, c->stream));
-  int64_t n_act = 0, n_mid = 0;
-  rc = scan_counts(c, c->row_act_cnt.as<int64_t>(), nrows, c->row_act_off.as<int64_t>(), &n_act);
-  if (rc) return rc;
-  M.row_act_off = c->row_act_off.as<int64_t>();
-  CK(c->act_rec.ensure(std::max<int64_t>(n_act, 1) * sizeof(int4)));
-  CK(c->act_mid.ensure(std::max<int64_t>(n_act, 1) * sizeof(int32_t)));
-  CK(c->row_mid_cnt.ensure(std::max<int64_t>(n_act, 1) * sizeof(int32_t)));
-  CK(c->row_mid_off.ensure((n_act + 1) * sizeof(int64_t)));
-  M.act_rec = c->act_rec.as<int4>();
-  M.act_mid = c->act_mid.as<int32_t>();
-  M.mid_cnt = c->row_mid_cnt.as<int32_t>();
-  M.mid_off = c->row_mid_off.as<int64_t>();
-  M.n_active = n_act;
-  // the active-cube map: per 32 cubes of a row, their active bits and the first one's index
-  CK(c->amap.ensure(std::max<int64_t>(c->awords_tot, 1) * sizeof(int2)));
-  M.amap = c->amap.as<int2>();
-  // triangle counts per active cube: the case table's for interior cubes (written by the
-  // classification), a count over the vertex slots for the listed low-face cubes
-  CK(c->tri_cnt.ensure(std::max<int64_t>(n_act, 1) * sizeof(int32_t)));
-  CK(c->bnd_list.ensure(std::max<int64_t>(n_act, 1) * sizeof(int32_t)));
-  CK(c->bnd_cursor.ensure(sizeof(unsigned long long)));
-  CK(cudaMemsetAsync(c->bnd_cursor.p, 0, sizeof(unsigned long long), c->stream));
-  M.tri_cnt = c->tri_cnt.as<int32_t>();
-  M.bnd_list = c->bnd_list.as<int32_t>();
-  M.bnd_cursor = c->bnd_cursor.as<unsigned long long>();
-  LAUNCH(nsg::launch_mc_rows(M, 1, c->stream));
+  LAUNCH(nsg::launch_mc_push(M, 0, n_an, c->stream));
   // midpoint vertices of cut edges without an analytic vertex
   LAUNCH(nsg::launch_mc_mid(M, 0, c->stream));
   rc = scan_counts(c, c->row_mid_cnt.as<int32_t>(), n_act, c->row_mid_off.as<int64_t>(), &n_mid);
@@ -1548,7 +1572,7 @@ int nsg_triangulate(nsg_ctx* c, double* area_out, int64_t* nverts, int64_t* ntri
   CK(c->tris.ensure(std::max<int64_t>(n_tri, 1) * 3 * sizeof(int32_t)));
   M.tri_off = c->tri_off.as<int64_t>();
   M.tris = c->tris.as<int32_t>();
-  LAUNCH(nsg::launch_mc_tris(M, c->stream));
+  LAUNCH(nsg::launch_mc_tris(M, c->tune.mc_tris_bpsm, c->stream));
   if (grad) LAUNCH(nsg::launch_grad_vert(M, c->stream));
   c->have_garea = grad;
   // per-structure areas in an order fixed by the structure alone (independent of the batch)
@@ -1641,6 +1665,134 @@ int nsg_download_cavities(nsg_ctx* c, double* sizes, int32_t* filled) {
 
 // Epsilon map in the reference's layout ((k*ny + j)*nx + i)*3 + axis (DelPhiShared::epsmap), after
 // cavity filling when nsg_cavities ran on this ray cast.
+int nsg_cavity_atoms(nsg_ctx* c, const double* atoms_xyzr, int64_t n_atoms, int32_t* offsets, int32_t* atoms,
+                     int64_t* n_total) {
+  if (!c || (n_atoms > 0 && !atoms_xyzr) || n_atoms < 0 || (atoms && !offsets)) return NSG_ERR_ARG;
+  if (!c->cav_detected || !c->status_dense || c->nstruct != 1)
+    return fail(NSG_ERR_STATE, "cavity atoms need nsg_cavities after the cast");
+  if (!c->have_cav_atoms) {
+    CK(cudaSetDevice(c->device));
+    const NsGrid& g = c->grid;
+    c->cav_atom_off.assign(c->ncav + 1, 0);
+    c->cav_atom_list.clear();
+    if (c->ncav > 0 && c->cav_nodes > 0) {
+      if (c->cav_nodes >= ((int64_t)1 << 31)) return fail(NSG_ERR_CAPACITY, "more than 2^31 cavity nodes");
+      // the reference's atom grid (buildAtomsMap)
+      double rmax = 0;
+      for (int64_t a = 0; a < n_atoms; a++) rmax = std::max(atoms_xyzr[4 * a + 3], rmax);
+      if (!(rmax > 0)) return fail(NSG_ERR_ARG, "cavity atoms need atoms of positive radius");
+      double gscale = 0.5 / rmax;
+      unsigned int ggrid = 1;
+      for (int it = 0; it < 4096; it++) {
+        ggrid = (unsigned int)floor(gscale * 1.3 * g.rmaxdim);
+        if (ggrid <= 100) {
+          if (ggrid <= 0) gscale *= 2.0;
+          else break;
+        } else {
+          gscale *= 0.5;
+        }
+      }
+      if (ggrid == 0 || ggrid > 100) return fail(NSG_ERR_ARG, "atom grid size out of range");
+      const double gside = 1. / gscale;
+      const int64_t gn = ggrid, ncell = gn * gn * gn;
+      double gmn[3];
+      for (int d = 0; d < 3; d++) gmn[d] = g.baricenter[d] - (ggrid - 1) * 0.5 * gside;
+      std::vector<int32_t> cell_of(n_atoms), cell_off(ncell + 1, 0), cell_atoms(n_atoms);
+      for (int64_t a = 0; a < n_atoms; a++) {
+        int64_t ix[3];
+        for (int d = 0; d < 3; d++) ix[d] = (int64_t)floor((atoms_xyzr[4 * a + d] - gmn[d]) * gscale + 0.5);
+        if (ix[0] < 0 || ix[1] < 0 || ix[2] < 0 || ix[0] >= gn || ix[1] >= gn || ix[2] >= gn)
+          return fail(NSG_ERR_ARG, "an atom lies outside the atom grid (atoms of another structure?)");
+        cell_of[a] = (int32_t)((ix[2] * gn + ix[1]) * gn + ix[0]);
+        cell_off[cell_of[a] + 1]++;
+      }
+      for (int64_t q = 0; q < ncell; q++) cell_off[q + 1] += cell_off[q];
+      {
+        std::vector<int32_t> cur(cell_off.begin(), cell_off.end() - 1);
+        for (int64_t a = 0; a < n_atoms; a++) cell_atoms[cur[cell_of[a]]++] = (int32_t)a;
+      }
+      const int64_t cap = c->cav_nodes;
+      CK(c->ca_atoms.ensure(std::max<int64_t>(n_atoms, 1) * 4 * sizeof(double)));
+      CK(c->ca_cell_off.ensure((ncell + 1) * sizeof(int32_t)));
+      CK(c->ca_cell_atoms.ensure(std::max<int64_t>(n_atoms, 1) * sizeof(int32_t)));
+      CK(c->ca_pairs.ensure(cap * sizeof(unsigned long long)));
+      CK(c->ca_alt.ensure(cap * sizeof(unsigned long long)));
+      CK(c->ca_count.ensure(2 * sizeof(unsigned long long)));
+      if (n_atoms)
+        CK(cudaMemcpyAsync(c->ca_atoms.p, atoms_xyzr, n_atoms * 4 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+      CK(cudaMemcpyAsync(c->ca_cell_off.p, cell_off.data(), (ncell + 1) * sizeof(int32_t), cudaMemcpyHostToDevice,
+                         c->stream));
+      if (n_atoms)
+        CK(cudaMemcpyAsync(c->ca_cell_atoms.p, cell_atoms.data(), n_atoms * sizeof(int32_t), cudaMemcpyHostToDevice,
+                           c->stream));
+      CK(cudaMemsetAsync(c->ca_count.p, 0, 2 * sizeof(unsigned long long), c->stream));
+      CK(cudaMemsetAsync(c->err.p, 0, sizeof(int32_t), c->stream));
+      nsg::CavAtomArgs A{};
+      A.status = c->status.as<int32_t>();
+      A.nx = g.nx;
+      A.ny = g.ny;
+      A.nz = g.nz;
+      A.mn[0] = g.xmin;
+      A.mn[1] = g.ymin;
+      A.mn[2] = g.zmin;
+      A.side = g.side;
+      A.gn = gn;
+      for (int d = 0; d < 3; d++) A.gmn[d] = gmn[d];
+      A.gscale = gscale;
+      A.cell_off = c->ca_cell_off.as<int32_t>();
+      A.cell_atoms = c->ca_cell_atoms.as<int32_t>();
+      A.atoms = c->ca_atoms.as<double>();
+      A.pairs = c->ca_pairs.as<unsigned long long>();
+      A.count = c->ca_count.as<unsigned long long>();
+      A.cap = cap;
+      A.err = c->err.as<int32_t>();
+      LAUNCH(nsg::cavity_atom_pairs(A, c->stream));
+      unsigned long long npairs = 0;
+      int32_t errflag = 0;
+      CK(cudaMemcpyAsync(&npairs, c->ca_count.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaMemcpyAsync(&errflag, c->err.p, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+      if (errflag) return fail(NSG_ERR_CAPACITY, "cavity boundary nodes exceed the cavity node count");
+      int64_t nu = 0;
+      if (npairs > 0) {
+        size_t tb = 0;
+        int64_t* d_nu = reinterpret_cast<int64_t*>(c->ca_count.as<unsigned long long>() + 1);
+        CK(nsg::sort_unique_u64(A.pairs, c->ca_alt.as<unsigned long long>(), (int64_t)npairs, d_nu, nullptr, &tb,
+                                c->stream));
+        CK(c->temp.ensure(tb));
+        tb = c->temp.cap;
+        c->launches += 2;
+        CK(nsg::sort_unique_u64(A.pairs, c->ca_alt.as<unsigned long long>(), (int64_t)npairs, d_nu, c->temp.p, &tb,
+                                c->stream));
+        CK(cudaMemcpyAsync(&nu, d_nu, sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+      }
+      std::vector<unsigned long long> keys(nu);
+      if (nu) {
+        CK(cudaMemcpyAsync(keys.data(), c->ca_pairs.p, nu * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                           c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+      }
+      c->cav_atom_list.resize(nu);
+      for (int64_t q = 0; q < nu; q++) {
+        const int64_t cav = (int64_t)(keys[q] >> 32);
+        if (cav < 0 || cav >= c->ncav) return fail(NSG_ERR_STATE, "cavity index out of range");
+        c->cav_atom_list[q] = (int32_t)(uint32_t)(keys[q] & 0xffffffffu) - 1;
+        c->cav_atom_off[cav + 1]++;
+      }
+      for (int q = 0; q < c->ncav; q++) c->cav_atom_off[q + 1] += c->cav_atom_off[q];
+    }
+    c->have_cav_atoms = true;
+  }
+  if (n_total) *n_total = (int64_t)c->cav_atom_list.size();
+  if (atoms) {
+    memcpy(offsets, c->cav_atom_off.data(), c->cav_atom_off.size() * sizeof(int32_t));
+    if (!c->cav_atom_list.empty())
+      memcpy(atoms, c->cav_atom_list.data(), c->cav_atom_list.size() * sizeof(int32_t));
+  }
+  return NSG_OK;
+}
+
 int nsg_download_epsmap(nsg_ctx* c, int32_t* dst) {
   if (!c || !dst) return NSG_ERR_ARG;
   if (!c->have_eps) return fail(NSG_ERR_STATE, "no epsilon maps: ray cast with NSG_RAYCAST_EPSMAP");

@@ -103,6 +103,24 @@ static int write_triangle_areas(const std::string& base, const double* vertices,
 
 // format: 0 OFF (+ triangleAreas.txt), 1 PLY (binary little endian).  root is the path without
 // extension; the reference's file names are root + ".off" / ".ply" and root + "triangleAreas.txt".
+int nsg_write_cavity_atoms(const char* path, int32_t n_cav, const int32_t* offsets, const int32_t* atoms,
+                           const int32_t* serials, int64_t n_atoms, const int32_t* skip) {
+  if (!path || n_cav < 0 || (n_cav > 0 && (!offsets || !atoms))) return NSG_ERR_ARG;
+  FILE* fp = fopen(path, "w");
+  if (!fp) return NSG_ERR_IO;
+  for (int32_t c = 0; c < n_cav; c++) {
+    if (skip && skip[c]) continue;
+    for (int32_t q = offsets[c]; q < offsets[c + 1]; q++) {
+      const int32_t a = atoms[q];
+      int32_t serial = a + 1;
+      if (serials && a >= 0 && a < n_atoms && serials[a] > 0) serial = serials[a];
+      fprintf(fp, "%d ", serial);
+    }
+    fprintf(fp, "\n");
+  }
+  return fclose(fp) == 0 ? NSG_OK : NSG_ERR_IO;
+}
+
 int nsg_write_mesh(const char* root, int format, const double* vertices, int64_t n_vertices, const int32_t* triangles,
                    int64_t n_triangles, int revert) {
   if (!root || n_vertices < 0 || n_triangles < 0 || (n_vertices && !vertices) || (n_triangles && !triangles))

@@ -192,6 +192,56 @@ __global__ void k_status_write(RunArgs A, const int32_t* __restrict__ label_of, 
   }
 }
 
+// The 27 cells around a cell, in the reference's order (shift_map, src/tools.h:35-64).
+__constant__ int8_t c_shift27[27][3] = {
+    {0, 0, 0},   {0, 0, -1},  {0, 0, 1},   {0, 1, 0},   {0, 1, -1},  {0, 1, 1},   {0, -1, 0},  {0, -1, -1}, {0, -1, 1},
+    {1, 0, 0},   {1, 0, -1},  {1, 0, 1},   {1, 1, 0},   {1, 1, -1},  {1, 1, 1},   {1, -1, 0},  {1, -1, -1}, {1, -1, 1},
+    {-1, 0, 0},  {-1, 0, -1}, {-1, 0, 1},  {-1, 1, 0},  {-1, 1, -1}, {-1, 1, 1},  {-1, -1, 0}, {-1, -1, -1}, {-1, -1, 1}};
+
+__device__ __forceinline__ int32_t status_at(const CavAtomArgs& A, int64_t i, int64_t j, int64_t k) {
+  if (i < 0 || j < 0 || k < 0 || i >= A.nx || j >= A.ny || k >= A.nz) return NS_STATUS_TEMPORARY_OUT;
+  return A.status[(k * A.ny + j) * A.nx + i];
+}
+
+// One thread per node (the status map is read once, coalesced); cavity boundary nodes search the
+// atom grid and append their pair.
+__global__ void k_cav_atoms(CavAtomArgs A) {
+  const int64_t n = A.nx * A.ny * A.nz;
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t s = A.status[v];
+    if (s < NS_STATUS_FIRST_CAV) continue;
+    const int64_t i = v % A.nx, j = (v / A.nx) % A.ny, k = v / (A.nx * A.ny);
+    if (status_at(A, i + 1, j, k) == s && status_at(A, i - 1, j, k) == s && status_at(A, i, j + 1, k) == s &&
+        status_at(A, i, j - 1, k) == s && status_at(A, i, j, k + 1) == s && status_at(A, i, j, k - 1) == s)
+      continue;
+    const double p[3] = {A.mn[0] + (double)i * A.side, A.mn[1] + (double)j * A.side, A.mn[2] + (double)k * A.side};
+    int64_t c[3];
+    for (int d = 0; d < 3; d++) c[d] = (int64_t)floor((p[d] - A.gmn[d]) * A.gscale + 0.5);
+    double best = INFINITY;
+    int32_t first = -1;
+    for (int q = 0; q < 27; q++) {
+      const int64_t cx = c[0] + c_shift27[q][0], cy = c[1] + c_shift27[q][1], cz = c[2] + c_shift27[q][2];
+      if (cx >= A.gn || cy >= A.gn || cz >= A.gn || cx < 0 || cy < 0 || cz < 0) continue;
+      const int64_t cell = (cz * A.gn + cy) * A.gn + cx;
+      for (int32_t t = A.cell_off[cell]; t < A.cell_off[cell + 1]; t++) {
+        const int32_t a = A.cell_atoms[t];
+        const double* at = A.atoms + 4 * (int64_t)a;
+        double d = (at[0] - p[0]) * (at[0] - p[0]) + (at[1] - p[1]) * (at[1] - p[1]) + (at[2] - p[2]) * (at[2] - p[2]);
+        d -= at[3] * at[3];
+        if (d < best) {
+          best = d;
+          first = a;
+        }
+      }
+    }
+    const unsigned long long slot = atomicAdd(A.count, 1ull);
+    if ((int64_t)slot < A.cap)
+      A.pairs[slot] = ((unsigned long long)(uint32_t)(s - NS_STATUS_FIRST_CAV) << 32) | (uint32_t)(first + 1);
+    else
+      atomicExch(A.err, 1);
+  }
+}
+
 int grid_for(int64_t n, int threads = 256) {
   int64_t b = (n + threads - 1) / threads;
   const int64_t cap = (int64_t)sm_count() * 32;
@@ -237,6 +287,30 @@ cudaError_t status_write(const RunArgs& A, const int32_t* label_of, int32_t* sta
   if (A.nrows <= 0) return cudaSuccess;
   k_status_write<<<grid_for(A.nrows * 32), 256, 0, s>>>(A, label_of, status);
   return cudaGetLastError();
+}
+
+cudaError_t cavity_atom_pairs(const CavAtomArgs& A, cudaStream_t s) {
+  const int64_t n = A.nx * A.ny * A.nz;
+  if (n <= 0) return cudaSuccess;
+  k_cav_atoms<<<grid_for(n), 256, 0, s>>>(A);
+  return cudaGetLastError();
+}
+
+cudaError_t sort_unique_u64(unsigned long long* keys, unsigned long long* keys_alt, int64_t n, int64_t* n_unique,
+                            void* temp, size_t* temp_bytes, cudaStream_t s) {
+  // sorted keys land in keys_alt, the unique ones back in keys; n_unique is a device counter
+  size_t t1 = 0, t2 = 0;
+  cudaError_t e = cub::DeviceRadixSort::SortKeys(nullptr, t1, keys, keys_alt, (int)n, 0, 64, s);
+  if (e != cudaSuccess) return e;
+  e = cub::DeviceSelect::Unique(nullptr, t2, keys_alt, keys, n_unique, (int)n, s);
+  if (e != cudaSuccess) return e;
+  if (!temp) {
+    *temp_bytes = t1 > t2 ? t1 : t2;
+    return cudaSuccess;
+  }
+  e = cub::DeviceRadixSort::SortKeys(temp, t1, keys, keys_alt, (int)n, 0, 64, s);
+  if (e != cudaSuccess) return e;
+  return cub::DeviceSelect::Unique(temp, t2, keys_alt, keys, n_unique, (int)n, s);
 }
 
 }  // namespace nsg

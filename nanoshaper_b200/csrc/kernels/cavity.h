@@ -37,4 +37,31 @@ cudaError_t run_fill(const RunArgs& A, const uint8_t* fill_of, uint32_t* bits, i
 // Dense status map from the runs; label_of == nullptr writes TEMPORARY_OUT for free nodes.
 cudaError_t status_write(const RunArgs& A, const int32_t* label_of, int32_t* status, cudaStream_t s);
 
+// Atoms lining the cavities (getCavitiesAtomsWithBilevelStatusMap, src/Surface.cpp:2249-2346), on
+// the dense status map after cavity detection and the reference's atom grid (buildAtomsMap,
+// src/Surface.cpp:1695-1749): gn^3 cells of side 1/gscale from gmn, cell (x, y, z) at
+// (z*gn + y)*gn + x, its atoms in ascending index order at cell_off.
+struct CavAtomArgs {
+  const int32_t* status;
+  int64_t nx, ny, nz;
+  double mn[3], side;
+  int64_t gn;
+  double gmn[3], gscale;
+  const int32_t* cell_off;    // gn^3 + 1
+  const int32_t* cell_atoms;
+  const double* atoms;        // x, y, z, r per atom
+  unsigned long long* pairs;  // (cavity << 32) | (atom + 1), one per cavity boundary node
+  unsigned long long* count;
+  int64_t cap;
+  int32_t* err;               // set to 1 when the pairs overflow cap
+};
+// One pair per node of cavity c (status FIRST_CAV + c) that has a 6-neighbour of another status
+// (TEMPORARY_OUT outside the grid): c and the atom of least |a - x|^2 - r^2 over the 27 cells
+// around the node, in the reference's cell order, the first of equal ones; atom -1 when the cells
+// hold no atom.
+cudaError_t cavity_atom_pairs(const CavAtomArgs& A, cudaStream_t s);
+// Sorts the n pairs and keeps one of each; pass temp == nullptr to query temp_bytes.
+cudaError_t sort_unique_u64(unsigned long long* keys, unsigned long long* keys_alt, int64_t n, int64_t* n_unique,
+                            void* temp, size_t* temp_bytes, cudaStream_t s);
+
 }  // namespace nsg

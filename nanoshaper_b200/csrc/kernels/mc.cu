@@ -4,20 +4,22 @@
 // vertices on the grid edges that contain the interval ends; a vertex is dropped when the two
 // end nodes of its edge have the same final insideness, and the first vertex of an edge wins
 // (assembleVerticesList src/Surface.cpp:7415-7667).  Vertices keep the reference order: panel 0
-// rays (z-major), panel 1 rays (y-major), panel 2 rays (z-major), pairs in ray order.  An edge's
-// vertices all come from the one ray that runs along it, so the vertex of a cut edge is found by
-// scanning that ray's (few) surviving vertices for the first on the edge; no per-cube vertex
-// table is built.
+// rays (z-major), panel 1 rays (y-major), panel 2 rays (z-major), pairs in ray order.
 //
 // Marching cubes: cubes (i,j,k) in [1, N-2]^3 are classified from the 8 insideness bits; the
 // classification writes the active cubes in (k, j, i) order and, per 32 cubes of a row, their
-// active bits and the index of the first (the active-cube map, 8 bytes per 32 cubes, which finds
-// the active index of any active cube).  Active cubes add an edge-midpoint vertex to their own
-// edges 5, 6, 10 that carry no analytic vertex, in (k, j, i, edge) order, appended after the
-// analytic ones (getVertices :8002-8327); the triangle pass emits the case-table triangles with
-// reversed winding and sums their areas (the reference sums Heron areas; here |cross product| / 2,
-// the same quantity) (triangulationKernel :9075-9318, getTriangles :14559-14780).  Triangles
-// with an edge without a vertex are skipped, as the reference does.
+// active bits and the index of the first (the active-cube map, 8 bytes per 32 cubes, from which
+// the active index of any active cube follows).  Every active cube has 12 vertex slots (cube_vl).
+// The vertex pass writes each vertex that is the first of its grid edge into the slots of the
+// (up to four) cubes that share the edge: a ray's vertices are sorted along it, so the vertices
+// of an edge have consecutive ids, the first of them is the one whose predecessor has another
+// edge key, and a slot is written once, with a plain store.  Active cubes add an edge-midpoint vertex to their own edges 5, 6, 10
+// that carry no analytic vertex, in (k, j, i, edge) order, appended after the analytic ones
+// (getVertices :8002-8327), and write it into the slots in the same way.  The triangle pass emits
+// the case-table triangles with reversed winding and sums their areas (the reference sums Heron
+// areas; here |cross product| / 2, the same quantity) (triangulationKernel :9075-9318,
+// getTriangles :14559-14780).  Triangles with an edge without a vertex are skipped, as the
+// reference does.
 #include <cub/cub.cuh>
 
 #include "../mc_cases.h"
@@ -86,7 +88,45 @@ __device__ __forceinline__ bool keeps(const GridDev& g, const uint32_t* bits, in
   return rbit(bits, nwords, f) != rbit(bits, nwords, f + step);
 }
 
-__global__ void k_vert(VertArgs A, int emit) {
+__device__ __forceinline__ int rec_struct(int w) { return (int)((unsigned)w >> 11); }
+
+// Active index of the active cube (i, j, k) of structure S, from the active-cube map (a structure
+// has fewer than 2^31 cubes, so the offsets within it fit 32 bits).
+__device__ __forceinline__ int32_t active_index(const int2* __restrict__ amap, const StructDev& S, int i, int j,
+                                                int k) {
+  const int W = ((int)S.g.n[0] - 2 + 31) >> 5;
+  const int b = i - 1;
+  const int2 w = amap[S.aword_base + ((k - 1) * ((int)S.g.n[1] - 2) + (j - 1)) * W + (b >> 5)];
+  return w.y + __popc((unsigned)w.x & ((1u << (b & 31)) - 1u));
+}
+
+// Writes vertex v into the slots of the active cubes (up to four, those inside the cube range)
+// that share grid edge (axis, x, y, z).  An x edge at (x, y, z) is edge 0 of cube (x, y, z), 2 of
+// (x, y-1, z), 4 of (x, y, z-1), 6 of (x, y-1, z-1); a y edge is 3 of (x, y, z), 1 of (x-1, y, z),
+// 7 of (x, y, z-1), 5 of (x-1, y, z-1); a z edge 8 of (x, y, z), 9 of (x-1, y, z), 11 of
+// (x, y-1, z), 10 of (x-1, y-1, z).  A cut edge's cubes are all active.
+__device__ __forceinline__ void push_vertex(const int2* __restrict__ amap, int32_t* cube_vl, const StructDev& S,
+                                            int axis, int x, int y, int z, int32_t v) {
+  // per axis: the two offset axes of the four cubes and the slots of (0,0), (1,0), (0,1), (1,1)
+  const int u = axis == NS_X_DIR ? 1 : 0, w = axis == NS_Z_DIR ? 1 : 2;
+  const int s00 = axis == NS_X_DIR ? 0 : (axis == NS_Y_DIR ? 3 : 8);
+  const int s10 = axis == NS_X_DIR ? 2 : (axis == NS_Y_DIR ? 1 : 9);
+  const int s01 = axis == NS_X_DIR ? 4 : (axis == NS_Y_DIR ? 7 : 11);
+  const int s11 = axis == NS_X_DIR ? 6 : (axis == NS_Y_DIR ? 5 : 10);
+  const int nx = (int)S.g.n[0] - 2, ny = (int)S.g.n[1] - 2, nz = (int)S.g.n[2] - 2;
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    int c[3] = {x, y, z};
+    if (q & 1) c[u]--;
+    if (q & 2) c[w]--;
+    if (c[0] < 1 || c[1] < 1 || c[2] < 1 || c[0] > nx || c[1] > ny || c[2] > nz) continue;
+    const int slot = q == 0 ? s00 : (q == 1 ? s10 : (q == 2 ? s01 : s11));
+    cube_vl[12 * (int64_t)active_index(amap, S, c[0], c[1], c[2]) + slot] = v;
+  }
+}
+
+template <bool emit>
+__global__ void k_vert(VertArgs A) {
   for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < A.nrays; r += (int64_t)gridDim.x * blockDim.x) {
     int np = A.ray_pair_cnt[r];
     if (!emit) {
@@ -125,7 +165,6 @@ __global__ void k_vert(VertArgs A, int emit) {
       A.vpos[3 * o + 0] = p[0];
       A.vpos[3 * o + 1] = p[1];
       A.vpos[3 * o + 2] = p[2];
-      A.valong[o] = pr[q];
       A.vkey[o] = e;
       A.vstruct[o] = (int32_t)(&S - A.B.s);
       if (A.vpid) {
@@ -137,98 +176,12 @@ __global__ void k_vert(VertArgs A, int emit) {
   }
 }
 
-__device__ __forceinline__ int rec_struct(int w) { return (int)((unsigned)w >> 11); }
-
-// Cube edge e (the case table's corner numbering): its axis and the offset of its grid-edge key
-// from the cube (i, j, k), packed as axis | dx << 2 | dy << 3 | dz << 4, 5 bits per edge:
-// edges 0, 2, 4, 6 along x at (i, j, k), (i, j+1, k), (i, j, k+1), (i, j+1, k+1); 3, 1, 7, 5 along
-// y at (i, j, k), (i+1, j, k), (i, j, k+1), (i+1, j, k+1); 8, 9, 11, 10 along z at (i, j, k),
-// (i+1, j, k), (i, j+1, k), (i+1, j+1, k).
-constexpr unsigned long long kCubeEdges = (0ull << 0) | (5ull << 5) | (8ull << 10) | (1ull << 15) | (16ull << 20) |
-                                          (21ull << 25) | (24ull << 30) | (17ull << 35) | (2ull << 40) |
-                                          (6ull << 45) | (14ull << 50) | (10ull << 55);
-__device__ __forceinline__ int cube_edge(int e) { return (int)((kCubeEdges >> (5 * e)) & 31); }
-
-// Active index of the active cube (i, j, k) of structure S, from the active-cube map.
-__device__ __forceinline__ int32_t active_index(const int2* __restrict__ amap, const StructDev& S, int64_t i,
-                                                int64_t j, int64_t k) {
-  const int64_t W = (S.g.n[0] - 2 + 31) >> 5;
-  const int64_t b = i - 1;
-  const int2 w = amap[S.aword_base + ((k - 1) * (S.g.n[1] - 2) + (j - 1)) * W + (b >> 5)];
-  return w.y + __popc((unsigned)w.x & ((1u << (b & 31)) - 1u));
-}
-
-// The first analytic vertex among ray vertices [lo, hi) whose edge index is a: its id, and its
-// coordinate along the ray in *along; -1 if none.
-__device__ __forceinline__ int32_t scan_ray(const double* __restrict__ valong, const GridDev& g, int axis, int64_t lo,
-                                            int64_t hi, int64_t a, double* along) {
-  for (int64_t v = lo; v < hi; v++) {
-    const double p = valong[v];
-    if (edge_index(g, axis, p) == a) {
-      *along = p;
-      return (int32_t)v;
-    }
-  }
-  return -1;
-}
-
-// The analytic vertex of grid edge (axis, x, y, z): -1 if none.
-__device__ __forceinline__ int32_t analytic_vertex(const MCArgs& A, const StructDev& S, int axis, int64_t x,
-                                                   int64_t y, int64_t z, double* along) {
-  int64_t a;
-  const int64_t r = edge_ray(S, axis, x, y, z, &a);
-  const int64_t lo = A.surv_off[r];
-  return scan_ray(A.valong, S.g, axis, lo, lo + A.surv_cnt[r], a, along);
-}
-
-// The midpoint vertex of grid edge (axis, x, y, z), added by the cube that has it as its edge 6
-// (x), 5 (y) or 10 (z): -1 if that cube lies outside the cube range or added none.  Only for cut
-// edges, whose four cubes are all active.
-__device__ __forceinline__ int32_t mid_vertex(const MCArgs& A, const StructDev& S, int axis, int64_t x, int64_t y,
-                                              int64_t z) {
-  int64_t i = x, j = y, k = z;
-  int bit;
-  if (axis == NS_X_DIR) { j--; k--; bit = 1; }
-  else if (axis == NS_Y_DIR) { i--; k--; bit = 0; }
-  else { i--; j--; bit = 2; }
-  if (i < 1 || j < 1 || k < 1 || i > S.g.n[0] - 2 || j > S.g.n[1] - 2 || k > S.g.n[2] - 2) return -1;
-  const int32_t o = active_index(A.amap, S, i, j, k);
-  const int mm = (reinterpret_cast<const int*>(A.act_rec + o)[3] >> 8) & 7;
-  if (!((mm >> bit) & 1)) return -1;
-  return A.act_mid[o] + __popc(mm & ((1 << bit) - 1));
-}
-
-// Vertex of cut edge e of cube (i, j, k): the analytic one, else the midpoint one; its coordinate
-// along the edge's axis in *along.
-__device__ __forceinline__ int32_t cube_edge_vertex(const MCArgs& A, const StructDev& S, int64_t i, int64_t j,
-                                                    int64_t k, int e, double* along) {
-  const int ce = cube_edge(e), ax = ce & 3;
-  const int64_t kx = i + ((ce >> 2) & 1), ky = j + ((ce >> 3) & 1), kz = k + ((ce >> 4) & 1);
-  int32_t v = analytic_vertex(A, S, ax, kx, ky, kz, along);
-  if (v < 0) {
-    v = mid_vertex(A, S, ax, kx, ky, kz);
-    *along = gcoord(S.g, ax, ax == 0 ? kx : (ax == 1 ? ky : kz));
-  }
-  return v;
-}
-
-// Position of the vertex of cube edge e of cube (i, j, k) from its coordinate along the edge: the
-// other two coordinates are those of the edge's ray (node + DELTA - side/2) for an analytic
-// vertex, node - side/2 for a midpoint one (as k_vert and k_mc_mid write them).
-__device__ __forceinline__ void vertex_pos(const GridDev& g, int64_t i, int64_t j, int64_t k, int e, bool analytic,
-                                           double along, double p[3]) {
-  const int ce = cube_edge(e), ax = ce & 3;
-  const double sh = analytic ? NS_DELTA - g.hside : -g.hside;
-  p[0] = ax == 0 ? along : gcoord(g, 0, i + ((ce >> 2) & 1)) + sh;
-  p[1] = ax == 1 ? along : gcoord(g, 1, j + ((ce >> 3) & 1)) + sh;
-  p[2] = ax == 2 ? along : gcoord(g, 2, k + ((ce >> 4) & 1)) + sh;
-}
-
 // The 32 bits of the flat bit grid starting at bit f (missing words read as outside), and in *next
-// the 32 bits starting at f + 1, from the same two words.
-__device__ __forceinline__ uint32_t bits32_pair(const uint32_t* __restrict__ bits, int64_t nwords, int64_t f,
+// the 32 bits starting at f + 1, from the same two words.  A structure's grid has fewer than 2^31
+// nodes, so its bit indices fit 32 bits.
+__device__ __forceinline__ uint32_t bits32_pair(const uint32_t* __restrict__ bits, int32_t nwords, int32_t f,
                                                 uint32_t* next) {
-  const int64_t w = f >> 5;
+  const int32_t w = f >> 5;
   const int s = (int)(f & 31);
   const uint32_t lo = w < nwords ? bits[w] : 0xffffffffu;
   const uint32_t hi = (w + 1) < nwords ? bits[w + 1] : 0xffffffffu;
@@ -237,13 +190,26 @@ __device__ __forceinline__ uint32_t bits32_pair(const uint32_t* __restrict__ bit
   return x;
 }
 
-// Cube rows (j, k) in chunks of consecutive rows of one structure, one warp per chunk.  Every
-// lane classifies 32 consecutive cubes of a row at once from the four bit rows the cubes touch
-// (corner inside = bit 0): a cube is active unless its 8 corners agree.  A row needs
-// W = ceil((NX-2)/32) lanes; when W <= 32 the warp packs 32/W rows side by side, otherwise it walks
-// the row in blocks of 32 words.  Pass 0 counts the active cubes of each row, pass 1 writes them
-// in i order at the row's offset, and the row's words of the active-cube map.
-__global__ void k_mc_rows(MCArgs A, int emit) {
+// The analytic vertex of grid edge (axis, x, y, z), as the vertex pass files it: whether the edge's
+// ray holds a surviving vertex with the edge's index.
+__device__ __forceinline__ bool has_analytic(const MCArgs& A, const StructDev& S, int axis, int64_t x, int64_t y,
+                                             int64_t z) {
+  int64_t a;
+  const int64_t r = edge_ray(S, axis, x, y, z, &a);
+  const int64_t lo = A.surv_off[r], hi = lo + A.surv_cnt[r];
+  for (int64_t v = lo; v < hi; v++)
+    if (edge_index(S.g, axis, A.vpos[3 * v + axis]) == a) return true;
+  return false;
+}
+
+// Cube rows (j, k), one thread per row; a warp takes a chunk of consecutive rows of one structure.
+// The thread walks its row 32 cubes at a time: the cubes' corners come from the four bit rows
+// they touch (corner inside = bit 0), one pair of words per bit row, and a cube is active unless
+// its 8 corners agree.  Pass 0 counts the active cubes of the row; pass 1 writes them in i order
+// at the row's offset, the row's words of the active-cube map, and -1 into every vertex slot of
+// the low-face cubes (the other cubes get a vertex in every slot they read).
+template <bool emit>
+__global__ void k_mc_rows(MCArgs A) {
   __shared__ uint8_t s_ntri[256];
   for (int t = threadIdx.x; t < 256; t += blockDim.x) s_ntri[t] = c_ntri[t];
   __syncthreads();
@@ -254,86 +220,70 @@ __global__ void k_mc_rows(MCArgs A, int emit) {
     const StructDev& S = A.B.s[C.x];
     const int NX = (int)S.g.n[0], NY = (int)S.g.n[1];
     const uint32_t* bits = A.bits + S.word_base;
-    const int64_t nwords = S.nwords;
+    const int32_t nwords = (int32_t)S.nwords;
     const int W = (NX - 2 + 31) >> 5;
-    const int WB = W < 32 ? W : 32;
-    const int R = 32 / WB;
-    const int NB = (W + 31) >> 5;
-    const int sub = lane / WB, wl = lane - sub * WB;
-    const int head = sub * WB;
-    const int tail = head + WB - 1 < 31 ? head + WB - 1 : 31;
-    for (int r0 = 0; r0 < C.z; r0 += R) {
-      const bool row_ok = sub < R && r0 + sub < C.z;
-      const int lr = C.y + r0 + (row_ok ? sub : 0);
+    for (int rr = lane; rr < C.z; rr += 32) {
+      const int lr = C.y + rr;
       const int j = 1 + lr % (NY - 2), k = 1 + lr / (NY - 2);
       const int64_t grow = S.row_base + lr;
-      const int64_t b00 = ((int64_t)k * NY + j) * NX, b10 = b00 + NX, b01 = b00 + (int64_t)NX * NY, b11 = b01 + NX;
-      const int64_t act_base = (emit && row_ok) ? A.row_act_off[grow] : 0;
-      int64_t run = 0;
-      for (int wb = 0; wb < NB; wb++) {
-        const int word = wb * 32 + wl;
-        const int64_t ic = 1 + 32 * (int64_t)word;
-        uint32_t act = 0;
-        uint32_t c[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-        if (row_ok && word < W) {
-          int64_t nvalid = NX - 1 - ic;
-          uint32_t vm = nvalid >= 32 ? 0xffffffffu : ((1u << nvalid) - 1u);
-          // corners i and i + 1 of each of the four bit rows from one pair of words per row
-          uint32_t n0, n1, n2, n3;
-          c[0] = ~bits32_pair(bits, nwords, b00 + ic, &n0);
-          c[1] = ~n0;
-          c[3] = ~bits32_pair(bits, nwords, b10 + ic, &n1);
-          c[2] = ~n1;
-          c[4] = ~bits32_pair(bits, nwords, b01 + ic, &n2);
-          c[5] = ~n2;
-          c[7] = ~bits32_pair(bits, nwords, b11 + ic, &n3);
-          c[6] = ~n3;
-          uint32_t d = 0;
+      const int32_t b00 = (k * NY + j) * NX, b10 = b00 + NX, b01 = b00 + NX * NY, b11 = b01 + NX;
+      int64_t slot = emit ? A.row_act_off[grow] : 0;
+      int32_t run = 0;
+      for (int word = 0; word < W; word++) {
+        const int32_t ic = 1 + 32 * word;
+        const int32_t nvalid = NX - 1 - ic;
+        const uint32_t vm = nvalid >= 32 ? 0xffffffffu : ((1u << nvalid) - 1u);
+        // corners i and i + 1 of each of the four bit rows from one pair of words per row
+        uint32_t c[8], n0, n1, n2, n3;
+        c[0] = ~bits32_pair(bits, nwords, b00 + ic, &n0);
+        c[1] = ~n0;
+        c[3] = ~bits32_pair(bits, nwords, b10 + ic, &n1);
+        c[2] = ~n1;
+        c[4] = ~bits32_pair(bits, nwords, b01 + ic, &n2);
+        c[5] = ~n2;
+        c[7] = ~bits32_pair(bits, nwords, b11 + ic, &n3);
+        c[6] = ~n3;
+        uint32_t d = 0;
 #pragma unroll
-          for (int q = 1; q < 8; q++) d |= c[0] ^ c[q];
-          act = d & vm;
+        for (int q = 1; q < 8; q++) d |= c[0] ^ c[q];
+        const uint32_t act = d & vm;
+        if (!emit) {
+          run += __popc(act);
+          continue;
         }
-        const int na = __popc(act);
-        int incl = na;
-        for (int o = 1; o < 32; o <<= 1) {
-          int v = __shfl_up_sync(0xffffffffu, incl, o);
-          if (lane >= o) incl += v;
-        }
-        const int head_excl = __shfl_sync(0xffffffffu, incl - na, head);
-        const int row_total = __shfl_sync(0xffffffffu, incl, tail) - head_excl;
-        if (emit && row_ok && word < W) {
-          int64_t slot = act_base + run + (incl - na - head_excl);
-          A.amap[S.aword_base + (int64_t)lr * W + word] = make_int2((int)act, (int)slot);
-          for (uint32_t m = act; m; m &= m - 1) {
-            int bit = __ffs(m) - 1;
-            int cs = 0;
+        A.amap[S.aword_base + (int64_t)lr * W + word] = make_int2((int)act, (int)slot);
+        for (uint32_t m = act; m; m &= m - 1) {
+          const int bit = __ffs(m) - 1;
+          int cs = 0;
 #pragma unroll
-            for (int q = 0; q < 8; q++) cs |= ((c[q] >> bit) & 1u) << q;
-            // every cut edge of a cube with i, j, k >= 2 has a vertex (an analytic one, or the
-            // midpoint its owner cube adds), so its triangles are the case table's; a cube on the
-            // low faces of the cube range may lack vertices on edges whose owner lies outside the
-            // range, and is counted after the midpoint vertices are in place (k_mc_tris_bnd)
-            if (ic + bit >= 2 && j >= 2 && k >= 2) {
-              A.tri_cnt[slot] = s_ntri[cs];
-            } else {
-              A.tri_cnt[slot] = 0;
-              const unsigned long long q = atomicAdd(A.bnd_cursor, 1ull);
-              A.bnd_list[q] = (int32_t)slot;
-            }
-            A.act_rec[slot++] = make_int4((int)(ic + bit), j, k, cs | (C.x << 11));
+          for (int q = 0; q < 8; q++) cs |= ((c[q] >> bit) & 1u) << q;
+          // every cut edge of a cube with i, j, k >= 2 has a vertex (an analytic one, or the
+          // midpoint its owner cube adds), so its triangles are the case table's; a cube on the
+          // low faces of the cube range may lack vertices on edges whose owner lies outside the
+          // range, and is counted after the midpoint vertices are in place (k_mc_tris_bnd)
+          if (ic + bit >= 2 && j >= 2 && k >= 2) {
+            A.tri_cnt[slot] = s_ntri[cs];
+          } else {
+            A.tri_cnt[slot] = 0;
+            const unsigned long long q = atomicAdd(A.bnd_cursor, 1ull);
+            A.bnd_list[q] = (int32_t)slot;
+            int4* cv = reinterpret_cast<int4*>(A.cube_vl + 12 * slot);
+            cv[0] = cv[1] = cv[2] = make_int4(-1, -1, -1, -1);
           }
+          A.act_rec[slot++] = make_int4(ic + bit, j, k, cs | (C.x << 11));
         }
-        run += row_total;
       }
-      if (!emit && row_ok && wl == 0) A.row_act_cnt[grow] = run;
+      if (!emit) A.row_act_cnt[grow] = run;
     }
   }
 }
 
 // One thread per active cube.  Pass 0: which of the cube's own edges 5, 6, 10 need a midpoint
 // vertex (cut edge without an analytic vertex); the mask goes to bits 8..10 of the record and the
-// count to mid_cnt.  Pass 1: writes those vertices at their final indices (act_mid).
-__global__ void k_mc_mid(MCArgs A, int emit) {
+// count to mid_cnt.  Pass 1: writes those vertices at their final indices (act_mid) and into the
+// slots of the cubes that share their edges.
+template <bool emit>
+__global__ void k_mc_mid(MCArgs A) {
   // case tables in shared memory: a constant-bank read with a different index per lane is
   // serialised across the warp
   __shared__ uint16_t s_emask[256];
@@ -341,18 +291,17 @@ __global__ void k_mc_mid(MCArgs A, int emit) {
   __syncthreads();
   for (int64_t a = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; a < A.n_active; a += (int64_t)gridDim.x * blockDim.x) {
     int4 rec = A.act_rec[a];
-    const int64_t i = rec.x, j = rec.y, k = rec.z;
+    const int i = rec.x, j = rec.y, k = rec.z;
     const StructDev& S = A.B.s[rec_struct(rec.w)];
     const GridDev& g = S.g;
     if (!emit) {
       // own edges 5 (y at (i+1, j, k+1)), 6 (x at (i, j+1, k+1)), 10 (z at (i+1, j+1, k)) that are
       // cut and carry no analytic vertex
       const int em = s_emask[rec.w & 255];
-      double al;
       int mm = 0;
-      if ((em & 32) && analytic_vertex(A, S, NS_Y_DIR, i + 1, j, k + 1, &al) < 0) mm |= 1;
-      if ((em & 64) && analytic_vertex(A, S, NS_X_DIR, i, j + 1, k + 1, &al) < 0) mm |= 2;
-      if ((em & 1024) && analytic_vertex(A, S, NS_Z_DIR, i + 1, j + 1, k, &al) < 0) mm |= 4;
+      if ((em & 32) && !has_analytic(A, S, NS_Y_DIR, i + 1, j, k + 1)) mm |= 1;
+      if ((em & 64) && !has_analytic(A, S, NS_X_DIR, i, j + 1, k + 1)) mm |= 2;
+      if ((em & 1024) && !has_analytic(A, S, NS_Z_DIR, i + 1, j + 1, k)) mm |= 4;
       A.act_rec[a].w = (rec.w & ~(7 << 8)) | (mm << 8);
       A.mid_cnt[a] = __popc(mm);
       continue;
@@ -364,20 +313,38 @@ __global__ void k_mc_mid(MCArgs A, int emit) {
     if (mm & 1) {
       A.vpos[3 * v] = gcoord(g, 0, i + 1) - g.hside; A.vpos[3 * v + 1] = gcoord(g, 1, j);
       A.vpos[3 * v + 2] = gcoord(g, 2, k + 1) - g.hside;
-      A.vkey[v] = make_int4((int)(i + 1), (int)j, (int)(k + 1), NS_Y_DIR);
+      A.vkey[v] = make_int4(i + 1, j, k + 1, NS_Y_DIR);
+      push_vertex(A.amap, A.cube_vl, S, NS_Y_DIR, i + 1, j, k + 1, (int32_t)v);
       v++;
     }
     if (mm & 2) {
       A.vpos[3 * v] = gcoord(g, 0, i); A.vpos[3 * v + 1] = gcoord(g, 1, j + 1) - g.hside;
       A.vpos[3 * v + 2] = gcoord(g, 2, k + 1) - g.hside;
-      A.vkey[v] = make_int4((int)i, (int)(j + 1), (int)(k + 1), NS_X_DIR);
+      A.vkey[v] = make_int4(i, j + 1, k + 1, NS_X_DIR);
+      push_vertex(A.amap, A.cube_vl, S, NS_X_DIR, i, j + 1, k + 1, (int32_t)v);
       v++;
     }
     if (mm & 4) {
       A.vpos[3 * v] = gcoord(g, 0, i + 1) - g.hside; A.vpos[3 * v + 1] = gcoord(g, 1, j + 1) - g.hside;
       A.vpos[3 * v + 2] = gcoord(g, 2, k);
-      A.vkey[v] = make_int4((int)(i + 1), (int)(j + 1), (int)k, NS_Z_DIR);
+      A.vkey[v] = make_int4(i + 1, j + 1, k, NS_Z_DIR);
+      push_vertex(A.amap, A.cube_vl, S, NS_Z_DIR, i + 1, j + 1, k, (int32_t)v);
     }
+  }
+}
+
+// One thread per analytic vertex: the first vertex of each grid edge goes into the slots of the
+// edge's cubes.  A ray's vertices are sorted along it and an edge's vertices all lie on one ray,
+// so they have consecutive ids: vertex v is the first of its edge unless vertex v - 1 has the same
+// edge key.  Each slot is written once, with a plain store.
+__global__ void k_mc_push(MCArgs A, int64_t v0, int64_t v1) {
+  for (int64_t v = v0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < v1; v += (int64_t)gridDim.x * blockDim.x) {
+    const int4 e = A.vkey[v];
+    if (v > v0) {
+      const int4 p = A.vkey[v - 1];
+      if (p.x == e.x && p.y == e.y && p.z == e.z && p.w == e.w) continue;
+    }
+    push_vertex(A.amap, A.cube_vl, A.B.s[A.vstruct[v]], e.w, e.x, e.y, e.z, (int32_t)v);
   }
 }
 
@@ -387,18 +354,11 @@ __global__ void k_mc_tris_bnd(MCArgs A) {
   const int64_t n = (int64_t)*A.bnd_cursor;
   for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
     const int32_t a = A.bnd_list[q];
-    const int4 rec = A.act_rec[a];
-    const int c = rec.w & 255;
-    const StructDev& S = A.B.s[rec_struct(rec.w)];
-    const int em = c_emask[c];
-    unsigned has = 0;
-    for (int e = 0; e < 12; e++) {
-      double al;
-      if (((em >> e) & 1) && cube_edge_vertex(A, S, rec.x, rec.y, rec.z, e, &al) >= 0) has |= 1u << e;
-    }
+    const int c = A.act_rec[a].w & 255;
+    const int32_t* cv = A.cube_vl + 12 * (int64_t)a;
     int cnt = 0;
     for (int t = 0; t < 16 && c_tri[c][t] >= 0; t += 3)
-      if (((has >> c_tri[c][t]) & 1) && ((has >> c_tri[c][t + 1]) & 1) && ((has >> c_tri[c][t + 2]) & 1)) cnt++;
+      if (cv[c_tri[c][t]] >= 0 && cv[c_tri[c][t + 1]] >= 0 && cv[c_tri[c][t + 2]] >= 0) cnt++;
     A.tri_cnt[a] = cnt;
   }
 }
@@ -407,100 +367,34 @@ constexpr int kTrisThreads = 256;
 constexpr int kTrisWarps = kTrisThreads / 32;
 constexpr int kMaxCubeTris = 5;  // the most triangles of a case
 
-// Triangles, 32 active cubes per warp.  Every lane finds the vertices of its cube's cut edges (the
-// first vertex on the edge's ray, else the midpoint of the edge's owner cube): first the ray
-// ranges of all cut edges, then each range's first vertex, both as independent loads across the
-// edges, then the remaining scans and midpoint lookups.  The warp's triangles (tri_cnt per cube,
-// at tri_off) are then spread over the lanes, one per lane: it writes the triangle with reversed
-// winding and its area (and, in gradient mode, the area's derivatives with respect to its
+// Triangles, 32 active cubes per warp: the lanes load their cubes' 12 vertex slots into shared
+// memory, then the warp's triangles (tri_cnt per cube, at tri_off) are spread over the lanes, one
+// per lane, whatever the cubes' cases.  Each writes its triangle with reversed winding (coalesced
+// across the warp) and its area (and, in gradient mode, the area's derivatives with respect to its
 // analytic vertices); each cube's area is the sum of its triangles' in case-table order.
-struct TrisShared {
-  // per warp, per cube edge, per lane: the vertex of the cut edge; its coordinate along the edge
-  // (before that, the ray's vertex range); the areas of the warp's triangles
-  double s_alo[kTrisWarps][12][32];
-  double s_area[kTrisWarps][kMaxCubeTris * 32];
-  int32_t s_vid[kTrisWarps][12][32];
-  int8_t s_tri[256][16];
-  uint16_t s_emask[256];
-};
-
-__global__ void __launch_bounds__(kTrisThreads, 4) k_mc_tris(MCArgs A) {
-  extern __shared__ __align__(16) unsigned char s_raw[];
-  TrisShared& sh = *reinterpret_cast<TrisShared*>(s_raw);
-  auto& s_alo = sh.s_alo;
-  auto& s_area = sh.s_area;
-  auto& s_vid = sh.s_vid;
-  auto& s_tri = sh.s_tri;
-  auto& s_emask = sh.s_emask;
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kTrisThreads, kMinBlocks) k_mc_tris(MCArgs A) {
+  __shared__ int8_t s_tri[256][16];
+  __shared__ uint8_t s_ntri[256];
+  // per warp: each cube's vertex slots ([slot][lane]) and the areas of the warp's triangles
+  __shared__ int32_t s_vid[kTrisWarps][12][32];
+  __shared__ double s_area[kTrisWarps][kMaxCubeTris * 32];
   for (int t = threadIdx.x; t < 256 * 16; t += blockDim.x) (&s_tri[0][0])[t] = (&c_tri[0][0])[t];
-  for (int t = threadIdx.x; t < 256; t += blockDim.x) s_emask[t] = c_emask[t];
+  for (int t = threadIdx.x; t < 256; t += blockDim.x) s_ntri[t] = c_ntri[t];
   __syncthreads();
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  int32_t* const vid = &s_vid[w][0][lane];
-  double* const alo = &s_alo[w][0][lane];
   for (int64_t base = ((int64_t)blockIdx.x * kTrisWarps + w) * 32; base < A.n_active;
        base += (int64_t)gridDim.x * kTrisThreads) {
     const int64_t a = base + lane;
     const bool valid = a < A.n_active;
-    const int4 rec = valid ? A.act_rec[a] : make_int4(1, 1, 1, 0);
-    const StructDev& S = A.B.s[rec_struct(rec.w)];
-    const GridDev& g = S.g;
-    const int em = s_emask[rec.w & 255];
-    // ray vertex ranges of the cut edges
-#pragma unroll
-    for (int e = 0; e < 12; e++) {
-      int2 r = make_int2(0, 0);
-      if ((em >> e) & 1) {
-        const int ce = cube_edge(e);
-        int64_t ak;
-        const int64_t ray = edge_ray(S, ce & 3, rec.x + ((ce >> 2) & 1), rec.y + ((ce >> 3) & 1),
-                                     rec.z + ((ce >> 4) & 1), &ak);
-        const int32_t lo = (int32_t)A.surv_off[ray];
-        r = make_int2(lo, lo + A.surv_cnt[ray]);
-      }
-      *reinterpret_cast<int2*>(alo + 32 * e) = r;
+    const int cw = valid ? A.act_rec[a].w : 0;
+    if (valid) {
+      const int4* cv = reinterpret_cast<const int4*>(A.cube_vl + 12 * a);
+      const int4 v0 = cv[0], v1 = cv[1], v2 = cv[2];
+      s_vid[w][0][lane] = v0.x; s_vid[w][1][lane] = v0.y; s_vid[w][2][lane] = v0.z; s_vid[w][3][lane] = v0.w;
+      s_vid[w][4][lane] = v1.x; s_vid[w][5][lane] = v1.y; s_vid[w][6][lane] = v1.z; s_vid[w][7][lane] = v1.w;
+      s_vid[w][8][lane] = v2.x; s_vid[w][9][lane] = v2.y; s_vid[w][10][lane] = v2.z; s_vid[w][11][lane] = v2.w;
     }
-    // the first vertex of each range: the edge's vertex when it lies on the edge (-2: scan on)
-#pragma unroll
-    for (int e = 0; e < 12; e++) {
-      int32_t v = -1;
-      if ((em >> e) & 1) {
-        const int2 r = *reinterpret_cast<const int2*>(alo + 32 * e);
-        if (r.x < r.y) {
-          const double p = A.valong[r.x];
-          const int ce = cube_edge(e), ax = ce & 3;
-          const int64_t ka = ax == 0 ? rec.x + ((ce >> 2) & 1) : (ax == 1 ? rec.y + ((ce >> 3) & 1) : rec.z + ((ce >> 4) & 1));
-          if (edge_index(g, ax, p) == ka) {
-            v = r.x;
-            alo[32 * e] = p;
-          } else if (r.y - r.x > 1) {
-            v = -2;
-          }
-        }
-      }
-      vid[32 * e] = v;
-    }
-    // the rest of the scans, and midpoint vertices
-    for (int m = em; m; m &= m - 1) {
-      const int e = __ffs(m) - 1;
-      int32_t v = vid[32 * e];
-      if (v >= 0) continue;
-      const int ce = cube_edge(e), ax = ce & 3;
-      const int64_t kx = rec.x + ((ce >> 2) & 1), ky = rec.y + ((ce >> 3) & 1), kz = rec.z + ((ce >> 4) & 1);
-      const int64_t ka = ax == 0 ? kx : (ax == 1 ? ky : kz);
-      double p = 0.0;
-      if (v == -2) {
-        const int2 r = *reinterpret_cast<const int2*>(alo + 32 * e);
-        v = scan_ray(A.valong, g, ax, r.x + 1, r.y, ka, &p);
-      }
-      if (v < 0) {
-        v = mid_vertex(A, S, ax, kx, ky, kz);
-        p = gcoord(g, ax, ka);
-      }
-      vid[32 * e] = v;
-      alo[32 * e] = p;
-    }
-    // the warp's triangles
     const int cnt = valid ? A.tri_cnt[a] : 0;
     int incl = cnt;
 #pragma unroll
@@ -522,33 +416,34 @@ __global__ void __launch_bounds__(kTrisThreads, 4) k_mc_tris(MCArgs A) {
       }
       const int ll = l < 31 ? l : 31;
       const int first = __shfl_sync(0xffffffffu, incl - cnt, ll);
-      const int ci = __shfl_sync(0xffffffffu, rec.x, ll), cj = __shfl_sync(0xffffffffu, rec.y, ll);
-      const int ck = __shfl_sync(0xffffffffu, rec.z, ll), cw = __shfl_sync(0xffffffffu, rec.w, ll);
+      const int lcnt = __shfl_sync(0xffffffffu, cnt, ll);
+      const int lw = __shfl_sync(0xffffffffu, cw, ll);
       if (t >= total) continue;
       const int q = t - first;
-      const int c = cw & 255;
-      const GridDev& gt = A.B.s[rec_struct(cw)].g;
+      const int c = lw & 255;
       const int32_t* lv = &s_vid[w][0][ll];
-      const double* la = &s_alo[w][0][ll];
-      // the q-th case triangle whose three edges have vertices
-      int e0 = 0, e1 = 0, e2 = 0;
-      for (int qq = 0, seen = 0; qq < 15 && s_tri[c][qq] >= 0; qq += 3) {
-        e0 = s_tri[c][qq];
-        e1 = s_tri[c][qq + 1];
-        e2 = s_tri[c][qq + 2];
-        if (lv[32 * e0] >= 0 && lv[32 * e1] >= 0 && lv[32 * e2] >= 0) {
-          if (seen == q) break;
-          seen++;
+      // the q-th case triangle whose three edges have vertices: the q-th of the case when the cube
+      // keeps all of them (every cube off the low faces), else found by a scan
+      int e0 = s_tri[c][3 * q], e1 = s_tri[c][3 * q + 1], e2 = s_tri[c][3 * q + 2];
+      if (lcnt != s_ntri[c]) {
+        for (int qq = 0, seen = 0; qq < 15 && s_tri[c][qq] >= 0; qq += 3) {
+          e0 = s_tri[c][qq];
+          e1 = s_tri[c][qq + 1];
+          e2 = s_tri[c][qq + 2];
+          if (lv[32 * e0] >= 0 && lv[32 * e1] >= 0 && lv[32 * e2] >= 0) {
+            if (seen == q) break;
+            seen++;
+          }
         }
       }
       const int32_t v0 = lv[32 * e0], v1 = lv[32 * e1], v2 = lv[32 * e2];
       A.tris[3 * (tbase + t) + 0] = v2;
       A.tris[3 * (tbase + t) + 1] = v1;
       A.tris[3 * (tbase + t) + 2] = v0;
-      double p0[3], p1[3], p2[3];
-      vertex_pos(gt, ci, cj, ck, e0, v0 < A.n_analytic, la[32 * e0], p0);
-      vertex_pos(gt, ci, cj, ck, e1, v1 < A.n_analytic, la[32 * e1], p1);
-      vertex_pos(gt, ci, cj, ck, e2, v2 < A.n_analytic, la[32 * e2], p2);
+      const double* P0 = A.vpos + 3 * (int64_t)v0;
+      const double* P1 = A.vpos + 3 * (int64_t)v1;
+      const double* P2 = A.vpos + 3 * (int64_t)v2;
+      const double p0[3] = {P0[0], P0[1], P0[2]}, p1[3] = {P1[0], P1[1], P1[2]}, p2[3] = {P2[0], P2[1], P2[2]};
       // area = |n| / 2, n = (P1 - P0) x (P2 - P0): the area the reference computes with Heron's
       // formula (getTriangles, src/Surface.cpp:14559-14780), with one square root instead of four
       const double f1[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
@@ -686,45 +581,48 @@ cudaError_t mc_init_tables() {
 
 cudaError_t launch_vert(const VertArgs& A, int emit, cudaStream_t s) {
   if (A.nrays == 0) return cudaSuccess;
-  k_vert<<<grid_for(A.nrays, 256), 256, 0, s>>>(A, emit);
+  if (emit) k_vert<true><<<grid_for(A.nrays, 256), 256, 0, s>>>(A);
+  else k_vert<false><<<grid_for(A.nrays, 256), 256, 0, s>>>(A);
   return cudaGetLastError();
 }
 
 cudaError_t launch_mc_rows(const MCArgs& A, int emit, cudaStream_t s) {
   if (A.nchunks <= 0) return cudaSuccess;
-  k_mc_rows<<<grid_for(A.nchunks * 32, 256), 256, 0, s>>>(A, emit);
+  if (emit) k_mc_rows<true><<<grid_for(A.nchunks * 32, 256), 256, 0, s>>>(A);
+  else k_mc_rows<false><<<grid_for(A.nchunks * 32, 256), 256, 0, s>>>(A);
   return cudaGetLastError();
 }
 
 cudaError_t launch_mc_mid(const MCArgs& A, int emit, cudaStream_t s) {
   if (A.n_active <= 0) return cudaSuccess;
-  k_mc_mid<<<grid_for(A.n_active, 256), 256, 0, s>>>(A, emit);
+  if (emit) k_mc_mid<true><<<grid_for(A.n_active, 256), 256, 0, s>>>(A);
+  else k_mc_mid<false><<<grid_for(A.n_active, 256), 256, 0, s>>>(A);
   return cudaGetLastError();
 }
 
-cudaError_t launch_mc_tris(const MCArgs& A, cudaStream_t s) {
-  if (A.n_active <= 0) return cudaSuccess;
-  // the shared block is above the 48 KB of a static allocation: opt in once per device
-  static bool opted[64] = {false};
-  int dev = 0;
-  cudaError_t err = cudaGetDevice(&dev);
-  if (err != cudaSuccess) return err;
-  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-  if (!opted[dev]) {
-    err = cudaFuncSetAttribute(k_mc_tris, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TrisShared));
-    if (err != cudaSuccess) return err;
-    opted[dev] = true;
-  }
+template <int kMinBlocks>
+cudaError_t launch_tris(const MCArgs& A, cudaStream_t s) {
   int64_t b = (A.n_active + kTrisThreads - 1) / kTrisThreads;
-  const int64_t cap = (int64_t)sm_count() * 4 * 8;
-  k_mc_tris<<<(unsigned)(b < cap ? b : cap), kTrisThreads, sizeof(TrisShared), s>>>(A);
+  const int64_t cap = (int64_t)sm_count() * kMinBlocks * 8;
+  k_mc_tris<kMinBlocks><<<(unsigned)(b < cap ? b : cap), kTrisThreads, 0, s>>>(A);
   return cudaGetLastError();
+}
+
+cudaError_t launch_mc_tris(const MCArgs& A, int blocks_per_sm, cudaStream_t s) {
+  if (A.n_active <= 0) return cudaSuccess;
+  return blocks_per_sm >= 4 ? launch_tris<4>(A, s) : launch_tris<3>(A, s);
 }
 
 cudaError_t launch_vertex_normals(const double* vpos, const int32_t* vpid, int64_t n_analytic, const double* f64,
                                   const int32_t* i32, double probe, double* normals, cudaStream_t s) {
   if (n_analytic <= 0) return cudaSuccess;
   k_vertex_normals<<<grid_for(n_analytic, 256), 256, 0, s>>>(vpos, vpid, n_analytic, f64, i32, probe, normals);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mc_push(const MCArgs& A, int64_t v0, int64_t v1, cudaStream_t s) {
+  if (v1 <= v0) return cudaSuccess;
+  k_mc_push<<<grid_for(v1 - v0, 256), 256, 0, s>>>(A, v0, v1);
   return cudaGetLastError();
 }
 

@@ -19,7 +19,6 @@ struct VertArgs {
   int32_t* surv_cnt;             // surviving vertices per ray
   const int64_t* surv_off;       // exclusive scan of surv_cnt
   double* vpos;                  // 3 per vertex
-  double* valong;                // per analytic vertex: its coordinate along its ray
   int4* vkey;                    // ix, iy, iz, dir per vertex
   int32_t* vstruct;              // structure of every vertex
   const int2* pair_pid;          // gradient mode: patches of the pair ends, else null
@@ -32,7 +31,6 @@ struct MCArgs {
   const int32_t* surv_cnt;
   const int64_t* surv_off;
   int64_t n_analytic;
-  const double* valong;          // coordinate of every analytic vertex along its ray
   double* vpos;
   int4* vkey;
   int32_t* vstruct;              // structure of every vertex
@@ -53,6 +51,7 @@ struct MCArgs {
   // structure from its aword_base): the cubes' active bits and the active index of the first
   // active cube of the word
   int2* amap;
+  int32_t* cube_vl;              // 12 per active cube: the vertex of each cut edge it reads
   const int64_t* tri_off;
   int32_t* tris;
   double* cube_area;
@@ -70,7 +69,11 @@ cudaError_t mc_init_tables();
 cudaError_t launch_vert(const VertArgs& A, int emit, cudaStream_t s);
 cudaError_t launch_mc_rows(const MCArgs& A, int emit, cudaStream_t s);
 cudaError_t launch_mc_mid(const MCArgs& A, int emit, cudaStream_t s);
-cudaError_t launch_mc_tris(const MCArgs& A, cudaStream_t s);
+// blocks_per_sm: 4 (64 registers a thread) or 3 (80 registers).
+cudaError_t launch_mc_tris(const MCArgs& A, int blocks_per_sm, cudaStream_t s);
+// Analytic vertices [v0, v1): the first vertex of each grid edge is written into the vertex slots
+// of the (up to four) active cubes that share the edge.
+cudaError_t launch_mc_push(const MCArgs& A, int64_t v0, int64_t v1, cudaStream_t s);
 // Triangle counts of the listed low-face cubes, once the midpoint vertices are in place.
 cudaError_t launch_mc_tris_bnd(const MCArgs& A, cudaStream_t s);
 // Analytic normal of every analytic vertex v < n_analytic from its patch vpid[v] (zero for patch

@@ -207,6 +207,7 @@ struct TuneParams {
   int isect_bpsm = 16;      // their blocks per SM (grid = SMs * isect_bpsm, grid-stride)
   int cand_threads = 256;   // threads per block of the candidate kernel (one warp per patch)
   int torus_split = 0;      // torus candidates solved in two launches, one per resolvent branch
+  int mc_tris_bpsm = 3;     // blocks per SM of the marching-cubes triangle kernel (3 or 4)
 };
 
 // trace.cu: every launch covers all structures of the batch; `set` is the ray set (0..3) and

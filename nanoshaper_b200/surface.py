@@ -157,6 +157,9 @@ class DelPhiShared:
         self.status: np.ndarray | None = None
         self.cavitiesSize: list[float] = []
         self.cavitiesFlag: list[bool] = []
+        # atoms lining each cavity (cav2atoms), ascending atom indices, -1 for a boundary node with
+        # no atom in its 27 atom-grid cells
+        self.cav2atoms: list[list[int]] = []
         # epsilon and ideb maps (Build_epsilon_maps): epsmap[k, j, i, axis] is the code of the grid
         # edge from node (i, j, k) along the axis (0 outside, 5 inside), idebmap[k, j, i] is False
         # inside the surface and in filled cavities
@@ -192,6 +195,13 @@ class DelPhiShared:
                                            N.ptr(st), ctypes.byref(self.grid), len(sizes),
                                            N.ptr(sizes) if len(sizes) else None, N.ptr(flags) if len(flags) else None),
                 "saveCavities")
+        # cavAtomsSerials.txt: every cavity's atoms (onlySaveNonFilled = false)
+        off = np.zeros(len(self.cav2atoms) + 1, np.int32)
+        off[1:] = np.cumsum([len(a) for a in self.cav2atoms]) if self.cav2atoms else []
+        lst = np.ascontiguousarray([a for cav in self.cav2atoms for a in cav] or [0], np.int32)
+        N.check(N.lib().nsg_write_cavity_atoms(str(d / "cavAtomsSerials.txt").encode(), len(self.cav2atoms),
+                                               N.ptr(off), N.ptr(lst), None, len(self.atoms), None),
+                "saveCavities (atoms)")
 
     def buildGrid(self, scale: float, perfil: float) -> bool:
         N.check(N.lib().nsg_grid_build(N.ptr(self.atoms), len(self.atoms), scale, perfil, ctypes.byref(self.grid)),
@@ -379,6 +389,22 @@ class Surface:
         N.check(N.lib().nsg_upload_patches(c, p.n, N.ptr(p.f64), N.ptr(p.i32), len(p.pool), N.ptr(p.pool),
                                            N.ptr(p.pool_flag), p.probe), "upload_patches")
 
+    def getCavitiesAtoms(self) -> list[list[int]]:
+        """Atoms lining each cavity of the last cavity detection (getCavitiesAtomsWithBilevelStatusMap,
+        src/Surface.cpp:2249-2346), into ``delphi.cav2atoms``: per cavity the ascending indices of
+        the atoms nearest (least power distance, in the reference's atom grid) to the cavity's
+        boundary nodes; -1 where a boundary node has no atom in its 27 grid cells."""
+        c = self._context().handle
+        atoms = np.ascontiguousarray(self.delphi.atoms, np.float64)
+        n = ctypes.c_int64()
+        N.check(N.lib().nsg_cavity_atoms(c, N.ptr(atoms), len(atoms), None, None, ctypes.byref(n)), "cavity atoms")
+        off = np.zeros(max(self.ncav, 0) + 1, np.int32)
+        lst = np.zeros(max(n.value, 1), np.int32)
+        N.check(N.lib().nsg_cavity_atoms(c, N.ptr(atoms), len(atoms), N.ptr(off), N.ptr(lst), ctypes.byref(n)),
+                "cavity atoms")
+        self.delphi.cav2atoms = [lst[off[i]:off[i + 1]].tolist() for i in range(max(self.ncav, 0))]
+        return self.delphi.cav2atoms
+
     def getSurf(self, optimize_grids: bool = True, fill: bool = False, cav_vol: float = 0.0,
                 keep_hits: bool = False, download: bool = True, grad: bool = False) -> float:
         """Ray casts the grid: status map, insideness bits, volume; optional cavity filling.
@@ -422,6 +448,7 @@ class Surface:
                 N.check(N.lib().nsg_download_cavities(c, N.ptr(sizes), N.ptr(flagv)), "download cavities")
             self.delphi.cavitiesSize = sizes.tolist()
             self.delphi.cavitiesFlag = [bool(f) for f in flagv]
+            self.getCavitiesAtoms()
         if download:
             g = self.delphi.grid
             if self.delphi.buildStatus:

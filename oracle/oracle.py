@@ -273,3 +273,84 @@ def op_model(c: dict) -> dict:
         for k, v in OP_MODEL[b].items():
             out[k] = out.get(k, 0.0) + n * v
     return out
+
+
+# The 27 cells around a cell in the reference's order (shift_map, src/tools.h:35-64).
+SHIFT27 = ((0, 0, 0), (0, 0, -1), (0, 0, 1), (0, 1, 0), (0, 1, -1), (0, 1, 1), (0, -1, 0), (0, -1, -1), (0, -1, 1),
+           (1, 0, 0), (1, 0, -1), (1, 0, 1), (1, 1, 0), (1, 1, -1), (1, 1, 1), (1, -1, 0), (1, -1, -1), (1, -1, 1),
+           (-1, 0, 0), (-1, 0, -1), (-1, 0, 1), (-1, 1, 0), (-1, 1, -1), (-1, 1, 1), (-1, -1, 0), (-1, -1, -1),
+           (-1, -1, 1))
+
+
+def atom_grid(grid, atoms: np.ndarray):
+    """The reference's atom grid (Surface::buildAtomsMap, src/Surface.cpp:1695-1749): cell side
+    2 r_max, halved or doubled until 1.3 rmaxdim spans 1..100 cells, centred on the grid's
+    barycentre; the atoms of each cell in ascending index order.  Returns (ggrid, gmin, gscale,
+    cells: dict flat cell index -> atom indices)."""
+    rmax = 0.0
+    for r in atoms[:, 3]:
+        rmax = max(float(r), rmax)
+    gscale = 0.5 / rmax
+    while True:
+        ggrid = int(np.floor(gscale * 1.3 * grid.rmaxdim))
+        if ggrid <= 100:
+            if ggrid <= 0:
+                gscale *= 2.0
+            else:
+                break
+        else:
+            gscale *= 0.5
+    gside = 1. / gscale
+    gmin = np.array([grid.baricenter[d] - (ggrid - 1) * 0.5 * gside for d in range(3)])
+    idx = np.floor((atoms[:, :3] - gmin) * gscale + 0.5).astype(np.int64)
+    flat = (idx[:, 2] * ggrid + idx[:, 1]) * ggrid + idx[:, 0]
+    cells: dict[int, list[int]] = {}
+    for a, f in enumerate(flat.tolist()):
+        cells.setdefault(f, []).append(a)
+    return ggrid, gmin, gscale, cells
+
+
+def cavity_atoms(grid, status: np.ndarray, ncav: int, atoms: np.ndarray) -> list[list[int]]:
+    """cav2atoms as Surface::getCavitiesAtomsWithBilevelStatusMap fills it
+    (src/Surface.cpp:2249-2346): for every node of cavity c (status 4 + c) with a 6-neighbour of
+    another status (TEMPORARY_OUT = 2 outside the grid), the atom of least |a - x|^2 - r^2 over the
+    27 atom-grid cells around the node, scanned in shift_map order and ascending atom order with a
+    strict comparison (the first of equal ones wins), -1 when those cells are empty; per cavity the
+    distinct atoms ascending (std::set order).  Vectorised over the boundary nodes: one pass per
+    (cell shift, slot within the cell) keeps the scan order of the reference's loops."""
+    nz, ny, nx = status.shape
+    pad = np.pad(status, 1, constant_values=2)
+    s = pad[1:-1, 1:-1, 1:-1]
+    same = ((pad[1:-1, 1:-1, 2:] == s) & (pad[1:-1, 1:-1, :-2] == s) & (pad[1:-1, 2:, 1:-1] == s) &
+            (pad[1:-1, :-2, 1:-1] == s) & (pad[2:, 1:-1, 1:-1] == s) & (pad[:-2, 1:-1, 1:-1] == s))
+    k, j, i = np.nonzero((status >= 4) & ~same)
+    out: list[set] = [set() for _ in range(ncav)]
+    if len(i) == 0:
+        return [sorted(x) for x in out]
+    ggrid, gmin, gscale, cells = atom_grid(grid, atoms)
+    p = np.stack([grid.xmin + i * grid.side, grid.ymin + j * grid.side, grid.zmin + k * grid.side], 1)
+    c = np.floor((p - gmin) * gscale + 0.5).astype(np.int64)
+    maxper = max(len(v) for v in cells.values())
+    table = np.full((ggrid ** 3, maxper), -1, np.int64)
+    for f, lst in cells.items():
+        table[f, :len(lst)] = lst
+    best = np.full(len(i), np.inf)
+    first = np.full(len(i), -1, np.int64)
+    for sx, sy, sz in SHIFT27:
+        cx, cy, cz = c[:, 0] + sx, c[:, 1] + sy, c[:, 2] + sz
+        ok = (cx >= 0) & (cy >= 0) & (cz >= 0) & (cx < ggrid) & (cy < ggrid) & (cz < ggrid)
+        f = np.where(ok, (cz * ggrid + cy) * ggrid + cx, 0)
+        for slot in range(maxper):
+            a = np.where(ok, table[f, slot], -1)
+            has = a >= 0
+            at = atoms[np.maximum(a, 0)]
+            d = ((at[:, 0] - p[:, 0]) * (at[:, 0] - p[:, 0]) + (at[:, 1] - p[:, 1]) * (at[:, 1] - p[:, 1]) +
+                 (at[:, 2] - p[:, 2]) * (at[:, 2] - p[:, 2]))
+            d = d - at[:, 3] * at[:, 3]
+            better = has & (d < best)
+            best = np.where(better, d, best)
+            first = np.where(better, a, first)
+    cav = status[k, j, i] - 4
+    for cc, a in zip(cav.tolist(), first.tolist()):
+        out[cc].add(a)
+    return [sorted(x) for x in out]

@@ -812,3 +812,65 @@ def test_cxx_surface_binding_compiles_and_links(native_lib, tmp_path):
            str(ROOT / "tests" / "cxx" / "gpu_ses_surface_main.cpp"), "-L", str(B.LIB_DIR), "-lnsgpu", "-o", str(out)]
     res = subprocess.run(cmd, capture_output=True, text=True)
     assert res.returncode == 0, res.stderr
+
+
+def test_oracle_cavity_atoms_against_loops(oracle_mod):
+    """The oracle's vectorised cavity atoms (getCavitiesAtomsWithBilevelStatusMap) equal a direct
+    loop transcription of the reference's scan: boundary nodes of each cavity, the 27 atom-grid
+    cells in shift_map order, atoms in cell order, strict power-distance minimum, -1 for empty
+    neighbourhoods.  Synthetic status map: two box cavities and one cavity touching the grid edge
+    (its nodes on the grid boundary see TEMPORARY_OUT outside)."""
+    atoms, ds, surf = _surface(120, 3, 2.0, 70.0)
+    g = ds.grid
+    O = oracle_mod
+    st = np.full((g.nz, g.ny, g.nx), -1, np.int32)
+    st[:2, :, :] = 3
+    st[5:9, 6:10, 7:12] = 4
+    st[12:15, 4:7, 9:11] = 5
+    st[g.nz - 3:, g.ny - 4:, : 3] = 6
+    ncav = 3
+    got = O.cavity_atoms(g, st, ncav, ds.atoms)
+    ggrid, gmin, gscale, cells = O.atom_grid(g, ds.atoms)
+    want = [set() for _ in range(ncav)]
+    nz, ny, nx = st.shape
+
+    def at(i, j, k):
+        return st[k, j, i] if 0 <= i < nx and 0 <= j < ny and 0 <= k < nz else 2
+
+    for k, j, i in zip(*[v.tolist() for v in np.nonzero(st >= 4)]):
+        s = st[k, j, i]
+        if all(at(*q) == s for q in ((i + 1, j, k), (i - 1, j, k), (i, j + 1, k), (i, j - 1, k),
+                                     (i, j, k + 1), (i, j, k - 1))):
+            continue
+        p = (g.xmin + i * g.side, g.ymin + j * g.side, g.zmin + k * g.side)
+        c = [int(np.floor((p[d] - gmin[d]) * gscale + 0.5)) for d in range(3)]
+        best, first = np.inf, -1
+        for sx, sy, sz in O.SHIFT27:
+            cx, cy, cz = c[0] + sx, c[1] + sy, c[2] + sz
+            if not (0 <= cx < ggrid and 0 <= cy < ggrid and 0 <= cz < ggrid):
+                continue
+            for a in cells.get((cz * ggrid + cy) * ggrid + cx, []):
+                x = ds.atoms[a]
+                d = (x[0] - p[0]) * (x[0] - p[0]) + (x[1] - p[1]) * (x[1] - p[1]) + (x[2] - p[2]) * (x[2] - p[2])
+                d -= x[3] * x[3]
+                if d < best:
+                    best, first = d, a
+        want[s - 4].add(first)
+    assert got == [sorted(w) for w in want]
+    assert all(len(x) > 0 for x in got)
+
+
+def test_write_cavity_atoms_layout(native_lib, tmp_path):
+    """cavAtomsSerials.txt: one line per cavity, "%d " per atom serial (index + 1, or the given
+    serial), -1 written as 0, skipped cavities left out (DelPhiShared::saveCavities)."""
+    from nanoshaper_b200 import _native as N
+    off = np.array([0, 3, 3, 5], np.int32)
+    lst = np.array([-1, 4, 9, 0, 2], np.int32)
+    p = tmp_path / "cavAtomsSerials.txt"
+    N.check(N.lib().nsg_write_cavity_atoms(str(p).encode(), 3, N.ptr(off), N.ptr(lst), None, 10, None), "write")
+    assert p.read_text() == "0 5 10 \n\n1 3 \n"
+    serials = np.arange(100, 110, dtype=np.int32)
+    skip = np.array([0, 1, 0], np.int32)
+    N.check(N.lib().nsg_write_cavity_atoms(str(p).encode(), 3, N.ptr(off), N.ptr(lst), N.ptr(serials), 10,
+                                           N.ptr(skip)), "write")
+    assert p.read_text() == "0 104 109 \n100 102 \n"
