@@ -263,11 +263,19 @@ struct SesBuilder {
     return d2 > dr * dr && d2 < rs * rs;
   }
 
-  bool buried_point(const double* p, int64_t i, int64_t j, int64_t k) const {
+  // Whether point p (a probe placement touching the expanded spheres of i, j, k) lies inside the
+  // expanded sphere of another neighbour of i.  *hint is the neighbour that buried the previous
+  // placement tested from i; neighbouring placements are mostly buried by the same sphere, so it
+  // is tried first (the answer does not depend on the order).
+  bool buried_point(const double* p, int64_t i, int64_t j, int64_t k, int64_t* hint = nullptr) const {
+    if (hint && *hint >= 0 && *hint != j && *hint != k && dist2(p, C(*hint)) < W[*hint]) return true;
     for (int64_t s = nb_off[i]; s < nb_off[i + 1]; s++) {
       int64_t l = nb[s];
       if (l == j || l == k) continue;
-      if (dist2(p, C(l)) < W[l]) return true;
+      if (dist2(p, C(l)) < W[l]) {
+        if (hint) *hint = l;
+        return true;
+      }
     }
     return false;
   }
@@ -332,6 +340,7 @@ struct SesBuilder {
     std::vector<std::vector<Facet>> per_atom(n);
     parallel_for(n, nthreads, [&](int64_t i, int) {
       std::vector<Facet>& out = per_atom[i];
+      int64_t hint = -1;
       const int32_t* ni = nb.data() + nb_off[i];
       int64_t nni = nb_off[i + 1] - nb_off[i];
       for (int64_t a = 0; a < nni; a++) {
@@ -350,8 +359,8 @@ struct SesBuilder {
           if (!probe_pair(C(i), C(j), C(k), W[i], W[j], W[k], Q, nn, &coeff)) continue;
           double pp[3], pm[3];
           for (int d = 0; d < 3; d++) { pp[d] = Q[d] + coeff * nn[d]; pm[d] = Q[d] - coeff * nn[d]; }
-          bool fp = !buried_point(pp, i, j, k);
-          bool fm = !buried_point(pm, i, j, k);
+          bool fp = !buried_point(pp, i, j, k, &hint);
+          bool fm = !buried_point(pm, i, j, k, &hint);
           if (fp && fm) {
             Facet f1, f2;
             make_facet(f1, pp, C(i), C(j), C(k), true, (int)i, (int)j, (int)k);
@@ -455,11 +464,48 @@ struct SesBuilder {
   // alpha complex.  Used for fully buried circles only.
   bool power_face_meets_disc(int64_t i, int64_t j, const TorusGeom& g) const {
     double r = g.rcoi;
-    std::vector<double> poly = {-r, -r, r, -r, r, r, -r, r}, next;
     const int32_t* ni = nb.data() + nb_off[i];
     int64_t nni = nb_off[i + 1] - nb_off[i];
     const int32_t* nj = nb.data() + nb_off[j];
     int64_t nnj = nb_off[j + 1] - nb_off[j];
+    {
+      // the disc centre (the origin of the disc plane) inside every neighbour's half-plane, by a
+      // margin well above rounding: it then lies inside the clipped polygon, which the full
+      // clipping below would find too
+      bool centre_in = true;
+      int64_t b = 0, c = 0;
+      while (centre_in && b < nni && c < nnj) {
+        if (ni[b] < nj[c]) { b++; continue; }
+        if (ni[b] > nj[c]) { c++; continue; }
+        const int64_t k = ni[b];
+        b++; c++;
+        double e[3];
+        sub3(e, g.tc, C(k));
+        const double ee = dot3(e, e);
+        const double ga = ee - W[k] + r * r;
+        if (!(ga > 1e-9 * (ee + W[k] + r * r))) centre_in = false;
+      }
+      if (centre_in) return true;
+    }
+    // the clipped polygon: each clip adds at most one vertex, so 4 + (common neighbours) bound it;
+    // two fixed buffers serve every call that fits, a heap pair the rest
+    constexpr size_t kStack = 512;
+    double sbuf[2][kStack];
+    std::vector<double> hbuf[2];
+    const int64_t nmax = 2 * (4 + std::min(nb_off[i + 1] - nb_off[i], nb_off[j + 1] - nb_off[j]) + 2);
+    double* polyp = sbuf[0];
+    double* nextp = sbuf[1];
+    if (nmax > (int64_t)kStack) {
+      hbuf[0].resize(nmax);
+      hbuf[1].resize(nmax);
+      polyp = hbuf[0].data();
+      nextp = hbuf[1].data();
+    }
+    size_t plen = 8, nlen = 0;
+    {
+      const double init[8] = {-r, -r, r, -r, r, r, -r, r};
+      for (int q = 0; q < 8; q++) polyp[q] = init[q];
+    }
     int64_t b = 0, c = 0;
     while (b < nni && c < nnj) {
       if (ni[b] < nj[c]) { b++; continue; }
@@ -470,24 +516,26 @@ struct SesBuilder {
       sub3(e, g.tc, C(k));
       double al = -2 * dot3(g.u, e), be = -2 * dot3(g.v, e);
       double ga = dot3(e, e) - W[k] + r * r;
-      next.clear();
-      size_t m = poly.size() / 2;
+      nlen = 0;
+      size_t m = plen / 2;
       for (size_t q = 0; q < m; q++) {
-        double ax = poly[2 * q], ay = poly[2 * q + 1];
-        double bx = poly[2 * ((q + 1) % m)], by = poly[2 * ((q + 1) % m) + 1];
+        double ax = polyp[2 * q], ay = polyp[2 * q + 1];
+        double bx = polyp[2 * ((q + 1) % m)], by = polyp[2 * ((q + 1) % m) + 1];
         double fa = al * ax + be * ay - ga, fb = al * bx + be * by - ga;
-        if (fa <= 0) { next.push_back(ax); next.push_back(ay); }
+        if (fa <= 0) { nextp[nlen++] = ax; nextp[nlen++] = ay; }
         if ((fa <= 0) != (fb <= 0)) {
           double t = fa / (fa - fb);
-          next.push_back(ax + t * (bx - ax));
-          next.push_back(ay + t * (by - ay));
+          nextp[nlen++] = ax + t * (bx - ax);
+          nextp[nlen++] = ay + t * (by - ay);
         }
       }
-      poly.swap(next);
-      if (poly.size() < 6) return false;
+      std::swap(polyp, nextp);
+      plen = nlen;
+      if (plen < 6) return false;
     }
+    const double* poly = polyp;
     // distance from the disc centre to the clipped polygon
-    size_t m = poly.size() / 2;
+    size_t m = plen / 2;
     bool inside = true;
     double best = INFINITY;
     for (size_t q = 0; q < m; q++) {
@@ -532,13 +580,18 @@ struct SesBuilder {
     std::vector<std::vector<Buried>> per_atom_b(n);
     std::vector<int64_t> errs(std::max(1, nthreads), 0);
     parallel_for(n, nthreads, [&](int64_t i, int tid) {
+      // the incidence entries of atom i's pairs (i, j > i) are contiguous and ascending in j, as
+      // are i's neighbours: one search, then a forward walk
+      auto it = std::lower_bound(inc.begin(), inc.end(), std::make_pair(i * n, -1));
+      std::vector<int> fcv;
       for (int64_t s = nb_off[i]; s < nb_off[i + 1]; s++) {
         int64_t j = nb[s];
-        if (j <= i || !proper(i, j)) continue;
-        int64_t key = i * n + j;
-        auto lo = std::lower_bound(inc.begin(), inc.end(), std::make_pair(key, -1));
-        std::vector<int> fcv;
-        for (auto it = lo; it != inc.end() && it->first == key; ++it) fcv.push_back(it->second);
+        if (j <= i) continue;
+        const int64_t key = i * n + j;
+        while (it != inc.end() && it->first < key) ++it;
+        if (!proper(i, j)) continue;
+        fcv.clear();
+        for (auto jt = it; jt != inc.end() && jt->first == key; ++jt) fcv.push_back(jt->second);
         TorusGeom g;
         torus_geom(C(i), W[i], at[4 * i + 3], C(j), W[j], &g);
         if (fcv.empty()) {
