@@ -1478,10 +1478,10 @@ int nsg_triangulate(nsg_ctx* c, double* area_out, int64_t* nverts, int64_t* ntri
   M.mid_off = c->row_mid_off.as<int64_t>();
   M.n_active = n_act;
   // the active-cube map (per 32 cubes of a row: their active bits and the first one's index) and
-  // 12 vertex slots per active cube; only the slots a cube reads are written (the low-face cubes'
-  // all start at -1), so they are not cleared
+  // 12 vertex slots per active cube, all -1 until the vertices are written into them
   CK(c->amap.ensure(std::max<int64_t>(c->awords_tot, 1) * sizeof(int2)));
   CK(c->cube_vl.ensure(std::max<int64_t>(n_act, 1) * 12 * sizeof(int32_t)));
+  CK(cudaMemsetAsync(c->cube_vl.p, 0xff, std::max<int64_t>(n_act, 1) * 12 * sizeof(int32_t), c->stream));
   M.amap = c->amap.as<int2>();
   M.cube_vl = c->cube_vl.as<int32_t>();
   // triangle counts per active cube: the case table's for interior cubes (written by the

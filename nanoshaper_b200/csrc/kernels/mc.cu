@@ -13,7 +13,7 @@
 // The vertex pass writes each vertex that is the first of its grid edge into the slots of the
 // (up to four) cubes that share the edge: a ray's vertices are sorted along it, so the vertices
 // of an edge have consecutive ids, the first of them is the one whose predecessor has another
-// edge key, and a slot is written once, with a plain store.  Active cubes add an edge-midpoint vertex to their own edges 5, 6, 10
+// edge key, and a slot is written once, with a plain store (the slots start at -1).  Active cubes add an edge-midpoint vertex to their own edges 5, 6, 10
 // that carry no analytic vertex, in (k, j, i, edge) order, appended after the analytic ones
 // (getVertices :8002-8327), and write it into the slots in the same way.  The triangle pass emits
 // the case-table triangles with reversed winding and sums their areas (the reference sums Heron
@@ -190,24 +190,11 @@ __device__ __forceinline__ uint32_t bits32_pair(const uint32_t* __restrict__ bit
   return x;
 }
 
-// The analytic vertex of grid edge (axis, x, y, z), as the vertex pass files it: whether the edge's
-// ray holds a surviving vertex with the edge's index.
-__device__ __forceinline__ bool has_analytic(const MCArgs& A, const StructDev& S, int axis, int64_t x, int64_t y,
-                                             int64_t z) {
-  int64_t a;
-  const int64_t r = edge_ray(S, axis, x, y, z, &a);
-  const int64_t lo = A.surv_off[r], hi = lo + A.surv_cnt[r];
-  for (int64_t v = lo; v < hi; v++)
-    if (edge_index(S.g, axis, A.vpos[3 * v + axis]) == a) return true;
-  return false;
-}
-
 // Cube rows (j, k), one thread per row; a warp takes a chunk of consecutive rows of one structure.
 // The thread walks its row 32 cubes at a time: the cubes' corners come from the four bit rows
 // they touch (corner inside = bit 0), one pair of words per bit row, and a cube is active unless
 // its 8 corners agree.  Pass 0 counts the active cubes of the row; pass 1 writes them in i order
-// at the row's offset, the row's words of the active-cube map, and -1 into every vertex slot of
-// the low-face cubes (the other cubes get a vertex in every slot they read).
+// at the row's offset and the row's words of the active-cube map.
 template <bool emit>
 __global__ void k_mc_rows(MCArgs A) {
   __shared__ uint8_t s_ntri[256];
@@ -267,8 +254,6 @@ __global__ void k_mc_rows(MCArgs A) {
             A.tri_cnt[slot] = 0;
             const unsigned long long q = atomicAdd(A.bnd_cursor, 1ull);
             A.bnd_list[q] = (int32_t)slot;
-            int4* cv = reinterpret_cast<int4*>(A.cube_vl + 12 * slot);
-            cv[0] = cv[1] = cv[2] = make_int4(-1, -1, -1, -1);
           }
           A.act_rec[slot++] = make_int4(ic + bit, j, k, cs | (C.x << 11));
         }
@@ -296,12 +281,14 @@ __global__ void k_mc_mid(MCArgs A) {
     const GridDev& g = S.g;
     if (!emit) {
       // own edges 5 (y at (i+1, j, k+1)), 6 (x at (i, j+1, k+1)), 10 (z at (i+1, j+1, k)) that are
-      // cut and carry no analytic vertex
+      // cut and carry no analytic vertex: their slots are still empty after the analytic push
       const int em = s_emask[rec.w & 255];
+      const int4 s47 = reinterpret_cast<const int4*>(A.cube_vl + 12 * a)[1];
+      const int s10 = A.cube_vl[12 * a + 10];
       int mm = 0;
-      if ((em & 32) && !has_analytic(A, S, NS_Y_DIR, i + 1, j, k + 1)) mm |= 1;
-      if ((em & 64) && !has_analytic(A, S, NS_X_DIR, i, j + 1, k + 1)) mm |= 2;
-      if ((em & 1024) && !has_analytic(A, S, NS_Z_DIR, i + 1, j + 1, k)) mm |= 4;
+      if ((em & 32) && s47.y < 0) mm |= 1;
+      if ((em & 64) && s47.z < 0) mm |= 2;
+      if ((em & 1024) && s10 < 0) mm |= 4;
       A.act_rec[a].w = (rec.w & ~(7 << 8)) | (mm << 8);
       A.mid_cnt[a] = __popc(mm);
       continue;
