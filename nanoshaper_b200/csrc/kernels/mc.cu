@@ -323,16 +323,24 @@ __global__ void k_mc_mid(MCArgs A) {
 // One thread per analytic vertex: the first vertex of each grid edge goes into the slots of the
 // edge's cubes.  A ray's vertices are sorted along it and an edge's vertices all lie on one ray,
 // so they have consecutive ids: vertex v is the first of its edge unless vertex v - 1 has the same
-// edge key.  Each slot is written once, with a plain store.
+// edge key in the same structure.  Each slot is written once, with a plain store.
 __global__ void k_mc_push(MCArgs A, int64_t v0, int64_t v1) {
   for (int64_t v = v0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < v1; v += (int64_t)gridDim.x * blockDim.x) {
     const int4 e = A.vkey[v];
+    const int32_t sv = A.vstruct[v];
     if (v > v0) {
       const int4 p = A.vkey[v - 1];
-      if (p.x == e.x && p.y == e.y && p.z == e.z && p.w == e.w) continue;
+      if (p.x == e.x && p.y == e.y && p.z == e.z && p.w == e.w && A.vstruct[v - 1] == sv) continue;
     }
-    push_vertex(A.amap, A.cube_vl, A.B.s[A.vstruct[v]], e.w, e.x, e.y, e.z, (int32_t)v);
+    push_vertex(A.amap, A.cube_vl, A.B.s[sv], e.w, e.x, e.y, e.z, (int32_t)v);
   }
+}
+
+// dst[q] = src[idx[q]]: per-structure offsets out of batch-wide prefix sums.
+__global__ void k_gather_i64(const int64_t* __restrict__ src, const int64_t* __restrict__ idx, int64_t n,
+                             int64_t* dst) {
+  const int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (q < n) dst[q] = src[idx[q]];
 }
 
 // Triangle counts of the active cubes on the low faces of the cube range (listed by k_mc_rows): the
@@ -604,6 +612,12 @@ cudaError_t launch_vertex_normals(const double* vpos, const int32_t* vpid, int64
                                   const int32_t* i32, double probe, double* normals, cudaStream_t s) {
   if (n_analytic <= 0) return cudaSuccess;
   k_vertex_normals<<<grid_for(n_analytic, 256), 256, 0, s>>>(vpos, vpid, n_analytic, f64, i32, probe, normals);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gather_i64(const int64_t* src, const int64_t* idx, int64_t n, int64_t* dst, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_gather_i64<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(src, idx, n, dst);
   return cudaGetLastError();
 }
 

@@ -71,6 +71,8 @@ cudaError_t launch_mc_rows(const MCArgs& A, int emit, cudaStream_t s);
 cudaError_t launch_mc_mid(const MCArgs& A, int emit, cudaStream_t s);
 // blocks_per_sm: 4 (64 registers a thread) or 3 (80 registers).
 cudaError_t launch_mc_tris(const MCArgs& A, int blocks_per_sm, cudaStream_t s);
+// dst[q] = src[idx[q]] for q < n (per-structure offsets out of batch-wide prefix sums).
+cudaError_t launch_gather_i64(const int64_t* src, const int64_t* idx, int64_t n, int64_t* dst, cudaStream_t s);
 // Analytic vertices [v0, v1): the first vertex of each grid edge is written into the vertex slots
 // of the (up to four) active cubes that share the edge.
 cudaError_t launch_mc_push(const MCArgs& A, int64_t v0, int64_t v1, cudaStream_t s);
