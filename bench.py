@@ -537,6 +537,20 @@ def run_ensemble(args, world: int, rank: int, local: int) -> None:
     from nanoshaper_b200.pipelined import PipelinedBatches
     runner = PipelinedBatches(surfs, n_chunks=6, device=local, precision=args.precision, tuning=tuning)
     h2d, d2h = runner.h2d_bytes, runner.d2h_bytes
+    # the host link's copy rate (pinned host to device, the largest chunk's patch records, event
+    # timed): with it the step's inputs give the transfer floor of the e2e figure
+    big = max(runner.chunks, key=lambda ch: ch.pin["f64"].numel()).pin["f64"]
+    link_dst = torch.empty(big.numel(), dtype=torch.uint8, device=f"cuda:{local}")
+    link_dst.copy_(big, non_blocking=True)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(3):
+        link_dst.copy_(big, non_blocking=True)
+    ev1.record()
+    torch.cuda.synchronize()
+    link_gbs = 3 * big.numel() / (ev0.elapsed_time(ev1) / 1000.0) / 1e9
+    del link_dst
     runner.run()
     barrier()
     e2e_steps = max(2, min(args.steps, 5))
@@ -657,6 +671,7 @@ def run_ensemble(args, world: int, rank: int, local: int) -> None:
                     "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms,
                     "method": "6 chunks (the first half-size) on 2 contexts, one upload at a time, copies "
                               "overlapped with compute (PipelinedBatches)",
+                    "h2d_link_gbs": link_gbs, "transfer_floor_ms": h2d / link_gbs / 1e6,
                     "results_match_resident_run": e2e_matches},
             "e2e_from_atoms": {"value": world * nstruct * 1000.0 / ap_ms, "unit": "structures/s", "ms_per_step": ap_ms,
                                "h2d_bytes_per_step": int(ap_h2d), "d2h_bytes_per_step": int(ap_d2h),

@@ -992,6 +992,8 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
   const auto cast = [&](int set) { return set == 0 ? (do_status || do_eps) : (set <= 3 ? do_mc : do_eps); };
   // the patches of the hits are kept for the gradients and for the analytic vertex normals
   const bool pids = grad || (flags & 64);
+  // the marching-cubes vertices carry their patch index in 29 bits (vpid_pack, mc.cu)
+  if (pids && c->np >= ((int64_t)1 << 29)) return fail(NSG_ERR_CAPACITY, "more than 2^29 patches with patch ids");
   if (!c->kind_mask_valid) {
     // which patch kinds are present (SES and / or skin cells) selects the intersection kernels
     CK(c->kind_mask_d.ensure(sizeof(int)));

@@ -90,6 +90,14 @@ __device__ __forceinline__ bool keeps(const GridDev& g, const uint32_t* bits, in
 
 __device__ __forceinline__ int rec_struct(int w) { return (int)((unsigned)w >> 11); }
 
+// vpid of an analytic vertex: its patch, and in bits 29-30 the axis of its ray (the gradient pass
+// reads the axis from here rather than from the 16-byte edge key); -1 without a patch.
+constexpr int kVpidAxisShift = 29;
+constexpr int32_t kVpidPatchMask = (1 << kVpidAxisShift) - 1;
+__device__ __forceinline__ int32_t vpid_pack(int32_t pid, int axis) {
+  return pid < 0 ? -1 : (pid | (axis << kVpidAxisShift));
+}
+
 // Active index of the active cube (i, j, k) of structure S, from the active-cube map (a structure
 // has fewer than 2^31 cubes, so the offsets within it fit 32 bits).
 __device__ __forceinline__ int32_t active_index(const int2* __restrict__ amap, const StructDev& S, int i, int j,
@@ -169,7 +177,7 @@ __global__ void k_vert(VertArgs A) {
       A.vstruct[o] = (int32_t)(&S - A.B.s);
       if (A.vpid) {
         const int2 pp = A.pair_pid[A.ray_pair_off[r] + (q >> 1)];
-        A.vpid[o] = (q & 1) ? pp.y : pp.x;
+        A.vpid[o] = vpid_pack((q & 1) ? pp.y : pp.x, e.w);
       }
       o++;
     }
@@ -488,8 +496,10 @@ __global__ void k_grad_vert(MCArgs A) {
     const double gv = v < A.n_analytic ? A.vgrad[v] : 0.0;
     if (gv != 0.0) {
       const double x[3] = {A.vpos[3 * v], A.vpos[3 * v + 1], A.vpos[3 * v + 2]};
-      pid = A.vpid[v];
-      if (hit_grad(A.f64 + (int64_t)NS_PATCH_F64 * pid, A.i32[NS_PATCH_I32 * pid], A.probe, x, A.vkey[v].w, g)) {
+      const int32_t vp = A.vpid[v];
+      pid = vp & kVpidPatchMask;
+      if (vp >= 0 &&
+          hit_grad(A.f64 + (int64_t)NS_PATCH_F64 * pid, A.i32[NS_PATCH_I32 * pid], A.probe, x, vp >> kVpidAxisShift, g)) {
 #pragma unroll
         for (int k = 0; k < NS_GRAD_PER_PATCH; k++) g[k] *= gv;
       } else {
@@ -511,8 +521,9 @@ __global__ void k_vertex_normals(const double* __restrict__ vpos, const int32_t*
                                  const double* __restrict__ f64, const int32_t* __restrict__ i32, double probe,
                                  double* out) {
   for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
-    const int32_t pid = vpid[v];
-    if (pid < 0) continue;
+    const int32_t vp = vpid[v];
+    if (vp < 0) continue;
+    const int32_t pid = vp & kVpidPatchMask;
     const double* f = f64 + (int64_t)NS_PATCH_F64 * pid;
     const int kind = i32[NS_PATCH_I32 * pid];
     const double y[3] = {vpos[3 * v], vpos[3 * v + 1], vpos[3 * v + 2]};
