@@ -535,7 +535,8 @@ def run_ensemble(args, world: int, rank: int, local: int) -> None:
     # volumes, areas and atom derivatives back to the host
     batch.close()
     from nanoshaper_b200.pipelined import PipelinedBatches
-    runner = PipelinedBatches(surfs, n_chunks=6, device=local, precision=args.precision, tuning=tuning)
+    runner = PipelinedBatches(surfs, n_chunks=8, device=local, precision=args.precision, tuning=tuning,
+                              n_contexts=4)
     h2d, d2h = runner.h2d_bytes, runner.d2h_bytes
     # the host link's copy rate (pinned host to device, the largest chunk's patch records, event
     # timed): with it the step's inputs give the transfer floor of the e2e figure
@@ -669,7 +670,7 @@ def run_ensemble(args, world: int, rank: int, local: int) -> None:
             "clocks": clocks,
             "e2e": {"value": world * nstruct * 1000.0 / e2e_ms, "unit": "structures/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms,
-                    "method": "6 chunks (the first half-size) on 2 contexts, one upload at a time, copies "
+                    "method": "8 chunks (the first half-size) on 4 contexts, one upload at a time, copies "
                               "overlapped with compute (PipelinedBatches)",
                     "h2d_link_gbs": link_gbs, "transfer_floor_ms": h2d / link_gbs / 1e6,
                     "results_match_resident_run": e2e_matches},

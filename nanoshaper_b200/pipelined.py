@@ -2,9 +2,10 @@
 
 An ensemble whose patch sets live in host memory spends a large share of its time in the
 host-to-device copy (about 0.9 GB per 1,000 structures of ~4,000 atoms).  ``PipelinedBatches``
-splits the ensemble into chunks, keeps every chunk's inputs in pinned host buffers, and drives two
-libnsgpu contexts (two CUDA streams) from two host threads.  While one context computes a chunk,
-the other copies the next, so the copy engines and the SMs work at the same time.  Each chunk is
+splits the ensemble into chunks, keeps every chunk's inputs in pinned host buffers, and drives
+several libnsgpu contexts (two by default, each with its own CUDA stream) from as many host threads.
+While one context computes a chunk, another copies the next, so the copy engines and the SMs work
+at the same time.  Each chunk is
 one batch (``nsg_set_batch`` / ``nsg_upload_batch`` / ``nsg_upload_atoms``, then the ray cast,
 the triangulation and the atom derivatives).  The results are the same as one batch of the whole
 ensemble.
@@ -67,7 +68,7 @@ class PipelinedBatches:
     on two contexts with overlapped transfers."""
 
     def __init__(self, surfaces: list, n_chunks: int = 4, device: int = 0, precision: str = "mixed",
-                 tuning: list[int] | None = None):
+                 tuning: list[int] | None = None, n_contexts: int = 2):
         if not surfaces:
             raise ValueError("empty ensemble")
         bounds = chunk_bounds(len(surfaces), n_chunks)
@@ -77,7 +78,7 @@ class PipelinedBatches:
         self.prec = S.PRECISIONS[precision]
         s0 = surfaces[0]
         self.flags = (N.STATUS if s0.delphi.buildStatus else 0) | N.ACCURATE_TRIANGULATION | N.GRAD
-        self.ctxs = [S.Context(device), S.Context(device)]
+        self.ctxs = [S.Context(device) for _ in range(max(1, n_contexts))]
         self._upload_lock = threading.Lock()
         if tuning is not None:
             p = np.ascontiguousarray(tuning, np.int32)
@@ -117,14 +118,16 @@ class PipelinedBatches:
         derivatives are in ``gradients()``)."""
         errors: list[BaseException] = []
 
+        nw = len(self.ctxs)
+
         def worker(w: int) -> None:
             try:
-                for ch in self.chunks[w::2]:
+                for ch in self.chunks[w::nw]:
                     self._run_chunk(self.ctxs[w].handle, ch)
-            except BaseException as e:  # reported after both workers joined
+            except BaseException as e:  # reported after all workers joined
                 errors.append(e)
 
-        threads = [threading.Thread(target=worker, args=(w,)) for w in range(2)]
+        threads = [threading.Thread(target=worker, args=(w,)) for w in range(nw)]
         for t in threads:
             t.start()
         for t in threads:
