@@ -100,8 +100,8 @@ def test_autotune_keeps_results(native_lib):
 
 
 def test_pipelined_batches_match_one_batch(native_lib):
-    """Chunked, two-context processing with overlapped copies gives the same per-structure
-    volumes and areas as one batch, and the same atom derivatives (1e-10 relative)."""
+    """Chunked processing on two and on three contexts, with overlapped copies, gives the same
+    per-structure volumes and areas as one batch, and the same atom derivatives (1e-10 relative)."""
     from nanoshaper_b200.pipelined import PipelinedBatches
     surfs = _structures(SPECS)
     batch = nb.SurfaceBatch(surfs, precision="mixed")
@@ -109,14 +109,15 @@ def test_pipelined_batches_match_one_batch(native_lib):
     a = batch.triangulateSurface().copy()
     g = batch.atom_gradients()
     batch.close()
-    runner = PipelinedBatches(surfs, n_chunks=3, precision="mixed")
-    for _ in range(2):
-        pv, pa = runner.run()
-        assert np.array_equal(pv, v) and np.array_equal(pa, a)
-    for (gv, ga), (rv, ra) in zip(g, runner.gradients()):
-        assert np.abs(gv - rv).max() <= 1e-10 * np.abs(gv).max()
-        assert np.abs(ga - ra).max() <= 1e-10 * np.abs(ga).max()
-    runner.close()
+    for n_chunks, n_contexts in ((3, 2), (4, 3)):
+        runner = PipelinedBatches(surfs, n_chunks=n_chunks, precision="mixed", n_contexts=n_contexts)
+        for _ in range(2):
+            pv, pa = runner.run()
+            assert np.array_equal(pv, v) and np.array_equal(pa, a)
+        for (gv, ga), (rv, ra) in zip(g, runner.gradients()):
+            assert np.abs(gv - rv).max() <= 1e-10 * np.abs(gv).max()
+            assert np.abs(ga - ra).max() <= 1e-10 * np.abs(ga).max()
+        runner.close()
 
 
 def test_atoms_pipeline_matches_batch(native_lib):
