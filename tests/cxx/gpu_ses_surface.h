@@ -3,6 +3,7 @@
 // stand-in of the reference's interface (reference_stub/Surface.h).
 #pragma once
 #include <cstdint>
+#include <set>
 #include <vector>
 
 #include "Surface.h"
@@ -28,6 +29,10 @@ class GpuSesSurface : public Surface {
     }
     int64_t seed = 1234;
     if (nsg_jitter_atoms(xyzr.data(), (int64_t)delphi->atoms.size(), 1e-4, &seed) != NSG_OK) return false;
+    // the reference jitters DelPhiShared's atoms in place; cavity atoms use them
+    for (size_t i = 0; i < delphi->atoms.size(); i++)
+      for (int d = 0; d < 3; d++) delphi->atoms[i].pos[d] = xyzr[4 * i + d];
+    atoms_xyzr = xyzr;
     if (patches) nsg_patchset_free(patches);
     patches = nullptr;
     return nsg_ses_build(xyzr.data(), (int64_t)delphi->atoms.size(), probe_radius, 0, &patches) == NSG_OK;
@@ -61,6 +66,15 @@ class GpuSesSurface : public Surface {
       std::vector<int32_t> filled(ncav);
       if (ncav > 0 && nsg_download_cavities(ctx, delphi->cavitiesSize.data(), filled.data()) != NSG_OK) return false;
       delphi->cavitiesFlag.assign(filled.begin(), filled.end());
+      // getCavitiesAtomsWithBilevelStatusMap: cav2atoms, one set per cavity
+      int64_t total = 0;
+      const int64_t na = (int64_t)atoms_xyzr.size() / 4;
+      if (nsg_cavity_atoms(ctx, atoms_xyzr.data(), na, nullptr, nullptr, &total) != NSG_OK) return false;
+      std::vector<int32_t> off(ncav + 1), lst(total > 0 ? total : 1);
+      if (nsg_cavity_atoms(ctx, atoms_xyzr.data(), na, off.data(), lst.data(), &total) != NSG_OK) return false;
+      for (auto* st : delphi->cav2atoms) delete st;
+      delphi->cav2atoms.assign(ncav, nullptr);
+      for (int cv = 0; cv < ncav; cv++) delphi->cav2atoms[cv] = new std::set<int>(&lst[off[cv]], &lst[off[cv + 1]]);
     }
     if (delphi->buildStatus && delphi->status && nsg_download_status(ctx, delphi->status) != NSG_OK) return false;
     return true;
@@ -80,6 +94,7 @@ class GpuSesSurface : public Surface {
  private:
   nsg_ctx* ctx = nullptr;
   NsPatchSet* patches = nullptr;
+  std::vector<double> atoms_xyzr;  // the jittered atoms (x, y, z, r)
   double probe_radius;
   int precision_;
 };

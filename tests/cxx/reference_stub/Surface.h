@@ -5,6 +5,7 @@
 // reference's header.
 #pragma once
 #include <cstdint>
+#include <set>
 #include <string>
 #include <vector>
 
@@ -27,6 +28,10 @@ class DelPhiShared {
   std::vector<Atom> atoms;
   vector<double> cavitiesSize;
   vector<bool> cavitiesFlag;
+  vector<std::set<int>*> cav2atoms;
+  ~DelPhiShared() {
+    for (auto* s : cav2atoms) delete s;
+  }
 };
 
 struct packet;
