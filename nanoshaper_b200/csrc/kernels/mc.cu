@@ -10,10 +10,12 @@
 // classification writes the active cubes in (k, j, i) order and, per 32 cubes of a row, their
 // active bits and the index of the first (the active-cube map, 8 bytes per 32 cubes, from which
 // the active index of any active cube follows).  Every active cube has 12 vertex slots (cube_vl).
-// The vertex pass writes each vertex that is the first of its grid edge into the slots of the
-// (up to four) cubes that share the edge: a ray's vertices are sorted along it, so the vertices
-// of an edge have consecutive ids, the first of them is the one whose predecessor has another
-// edge key, and a slot is written once, with a plain store (the slots start at -1).  Active cubes add an edge-midpoint vertex to their own edges 5, 6, 10
+// The push pass (k_mc_push) writes each vertex that is the first of its grid edge into the slots
+// of the (up to four) cubes that share the edge: a ray's vertices are sorted along it, so the
+// vertices of an edge have consecutive ids, the first of them is the one whose predecessor has
+// another edge key, and a slot is written once, with a plain store (the slots start at -1; the
+// host clears and fills them structure chunk by structure chunk, so that a chunk's slots stay in
+// L2 between the two).  Active cubes add an edge-midpoint vertex to their own edges 5, 6, 10
 // that carry no analytic vertex, in (k, j, i, edge) order, appended after the analytic ones
 // (getVertices :8002-8327), and write it into the slots in the same way.  The triangle pass emits
 // the case-table triangles with reversed winding and sums their areas (the reference sums Heron
@@ -68,17 +70,6 @@ __device__ __forceinline__ int4 edge_key(const RayId& id, int64_t a) {
   if (id.panel == 0) return make_int4((int)a, (int)id.m, (int)id.n, NS_X_DIR);
   if (id.panel == 1) return make_int4((int)id.m, (int)id.n, (int)a, NS_Z_DIR);
   return make_int4((int)id.m, (int)a, (int)id.n, NS_Y_DIR);
-}
-
-// The accurate-triangulation ray (batch-wide ordinal) that runs along grid edge (axis, x, y, z),
-// the inverse of ray_of / edge_key; *a = the edge's index along the ray.
-__device__ __forceinline__ int64_t edge_ray(const StructDev& S, int axis, int64_t x, int64_t y, int64_t z,
-                                            int64_t* a) {
-  const int64_t NX = S.g.n[0], NY = S.g.n[1], NZ = S.g.n[2];
-  if (axis == NS_X_DIR) { *a = x; return S.mc_base + z * NY + y; }
-  if (axis == NS_Z_DIR) { *a = z; return S.mc_base + NZ * NY + y * NX + x; }
-  *a = y;
-  return S.mc_base + NZ * NY + NY * NX + z * NX + x;
 }
 
 __device__ __forceinline__ bool keeps(const GridDev& g, const uint32_t* bits, int64_t nwords, int4 e) {
