@@ -236,6 +236,17 @@ int nsg_blobby_atom_grads(nsg_ctx* ctx, double* d_volume, double* d_area);
 int nsg_raycast(nsg_ctx* ctx, int flags, int precision, double* volume);
 /* getCavitiesWithBilevelStatusMap + fillCavities (src/Surface.cpp:1994-2126, 2355-2484). */
 int nsg_cavities(nsg_ctx* ctx, double cavity_volume, int* n_cavities);
+/* Water-shape filter of the cavities that nsg_cavities kept, Keep_Water_Shaped_Cavities
+ * (filterCavitiesWithBilevelStatusMap, src/Surface.cpp:3011-3290; called by getSurf at
+ * src/Surface.cpp:1128-1139): the nodes of a cavity that no probe sphere of radius probe_radius
+ * fitting inside the cavity covers are removed, i.e. their insideness bits, epsilon and ideb
+ * entries filled as fillCavities does.  The status map takes the reference's codes: -(4 + c) for
+ * the support nodes of cavity c, 4 + c for the covered ones, and for the removed ones
+ * STATUS_POINT_INSIDE when modify_status is set, else -3 (SHAPE_UNDER_CHECK) or -2 (SHAPE_OK,
+ * inside a support sphere of a later cavity).  A cavity whose nodes are all removed becomes
+ * filled (nsg_download_cavities); nsg_cavity_atoms keeps the cavity membership from before the
+ * filter.  Once per nsg_cavities; n_removed (may be NULL) receives the removed node count. */
+int nsg_filter_cavities(nsg_ctx* ctx, double probe_radius, int modify_status, int64_t* n_removed);
 /* Label order of the alternating-z seed scan of getCavitiesWithBilevelStatusMap
  * (src/Surface.cpp:2044-2116) over regions sorted by first node; host only. */
 int nsg_cavity_order(int32_t n_regions, const uint32_t* desc_key, int32_t* label_out);

@@ -144,6 +144,11 @@ struct nsg_ctx {
   int64_t cav_nodes = 0;                       // nodes of all cavities (labels >= 4)
   bool cav_detected = false;                   // nsg_cavities ran on the last cast
   bool have_cav_atoms = false;
+  std::vector<int64_t> cav_count;              // nodes per cavity
+  // water-shape filter: the labels before it, per-node support / removed / later flags
+  DevBuf cav_label, sh_support, sh_removed[2], sh_later, sh_filled, sh_nrem, sh_changed;
+  bool shape_filtered = false;
+  bool ideb_ready = false;                     // ideb holds the map (after a shape filter)
   std::vector<int32_t> cav_atom_off, cav_atom_list;
   DevBuf ca_atoms, ca_cell_off, ca_cell_atoms, ca_pairs, ca_alt, ca_count;
   // mesh
@@ -1298,6 +1303,7 @@ int nsg_raycast(nsg_ctx* c, int flags, int precision, double* volume) {
   }
   c->status_dense = false;
   c->cav_detected = c->have_cav_atoms = false;
+  c->shape_filtered = c->ideb_ready = false;
   c->have_gvol = grad;
   c->have_pids = pids && do_mc;
   c->have_status = do_status || do_eps;
@@ -1345,8 +1351,10 @@ int nsg_cavities(nsg_ctx* c, double cav_vol, int* ncav_out) {
   const int64_t nr = c->n_fruns;
   c->cav_size.clear();
   c->cav_filled.clear();
+  c->cav_count.clear();
   c->cav_nodes = 0;
   c->cav_detected = c->have_cav_atoms = false;
+  c->shape_filtered = c->ideb_ready = false;
   stage_begin(c, kStageCavity);
   CK(c->labels.ensure(std::max<int64_t>(nr, 1) * sizeof(int32_t)));
   CK(c->is_root.ensure(std::max<int64_t>(nr, 1)));
@@ -1394,11 +1402,13 @@ int nsg_cavities(nsg_ctx* c, double cav_vol, int* ncav_out) {
   c->ncav = id - NS_STATUS_OUT;
   c->cav_size.assign(c->ncav, 0.0);
   c->cav_filled.assign(c->ncav, 0);
+  c->cav_count.assign(c->ncav, 0);
   for (int32_t r = 0; r < nroots; r++) {
     int lab = label_of[r];
     if (lab < NS_STATUS_FIRST_CAV) continue;
     double v = (double)cnt[r] * cube;
     c->cav_nodes += (int64_t)cnt[r];
+    c->cav_count[lab - NS_STATUS_FIRST_CAV] = (int64_t)cnt[r];
     c->cav_size[lab - NS_STATUS_FIRST_CAV] = v;
     if (v <= cav_vol) {
       c->cav_filled[lab - NS_STATUS_FIRST_CAV] = 1;
@@ -1423,6 +1433,94 @@ int nsg_cavities(nsg_ctx* c, double cav_vol, int* ncav_out) {
   c->cav_detected = true;
   if (ncav_out) *ncav_out = c->ncav;
   c->n_vert = c->n_tri = 0;
+  return NSG_OK;
+}
+
+int nsg_filter_cavities(nsg_ctx* c, double probe_radius, int modify_status, int64_t* n_removed) {
+  if (!c || !(probe_radius > 0)) return NSG_ERR_ARG;
+  if (!c->cav_detected || !c->status_dense || c->nstruct != 1)
+    return fail(NSG_ERR_STATE, "the shape filter needs nsg_cavities after the cast");
+  if (c->shape_filtered) return fail(NSG_ERR_STATE, "the shape filter runs once per cavity detection");
+  if (n_removed) *n_removed = 0;
+  if (c->ncav == 0) return NSG_OK;
+  CK(cudaSetDevice(c->device));
+  const NsGrid& g = c->grid;
+  const int64_t nn = g.nx * g.ny * g.nz;
+  const int ncav = c->ncav;
+  CK(c->cav_label.ensure(nn * sizeof(int32_t)));
+  CK(c->sh_support.ensure(nn));
+  CK(c->sh_removed[0].ensure(nn));
+  CK(c->sh_removed[1].ensure(nn));
+  CK(c->sh_later.ensure(nn));
+  CK(c->sh_filled.ensure(ncav));
+  CK(c->sh_nrem.ensure(ncav * sizeof(unsigned long long)));
+  CK(c->sh_changed.ensure(sizeof(int32_t)));
+  std::vector<uint8_t> filled(ncav);
+  for (int q = 0; q < ncav; q++) filled[q] = c->cav_filled[q] ? 1 : 0;
+  CK(cudaMemcpyAsync(c->cav_label.p, c->status.p, nn * sizeof(int32_t), cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->sh_filled.p, filled.data(), ncav, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemsetAsync(c->sh_nrem.p, 0, ncav * sizeof(unsigned long long), c->stream));
+  if (c->have_eps && !c->ideb_ready) {
+    CK(c->ideb.ensure(nn));
+    nsg::RunArgs R = run_args(c);
+    LAUNCH(nsg::ideb_write(R, c->eps_filled ? c->cc_fill_of.as<uint8_t>() : nullptr, c->ideb.as<uint8_t>(),
+                           c->stream));
+  }
+  nsg::ShapeArgs A{};
+  A.status = c->status.as<int32_t>();
+  A.label = c->cav_label.as<int32_t>();
+  A.nx = g.nx;
+  A.ny = g.ny;
+  A.nz = g.nz;
+  A.mn[0] = g.xmin;
+  A.mn[1] = g.ymin;
+  A.mn[2] = g.zmin;
+  A.side = g.side;
+  A.scale = g.scale;
+  A.r = probe_radius;
+  A.filled = c->sh_filled.as<uint8_t>();
+  A.mod_status = modify_status ? 1 : 0;
+  A.support = c->sh_support.as<uint8_t>();
+  A.later = c->sh_later.as<uint8_t>();
+  A.changed = c->sh_changed.as<int32_t>();
+  A.bits = c->have_bits ? c->bits.as<uint32_t>() : nullptr;
+  A.nwords = nwords_of(g);
+  A.eps = c->have_eps ? c->epsmap.as<int32_t>() : nullptr;
+  A.ideb = c->have_eps ? c->ideb.as<uint8_t>() : nullptr;
+  A.n_removed = c->sh_nrem.as<unsigned long long>();
+  // pass t is exact for cavities 0..t; a pass that changes no removed flag is the fixed point
+  // (a modified status map turns removed nodes inside at once: one pass)
+  int cur = 0;
+  for (int pass = 0; pass <= ncav; pass++) {
+    A.removed = c->sh_removed[cur].as<uint8_t>();
+    A.removed_prev = pass ? c->sh_removed[cur ^ 1].as<uint8_t>() : nullptr;
+    CK(cudaMemsetAsync(c->sh_changed.p, 0, sizeof(int32_t), c->stream));
+    c->launches += 2;
+    CK(nsg::shape_pass(A, c->stream));
+    if (modify_status) break;
+    int32_t changed = 0;
+    CK(cudaMemcpyAsync(&changed, c->sh_changed.p, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (pass && !changed) break;
+    if (pass == ncav) return fail(NSG_ERR_STATE, "the shape filter did not settle");
+    cur ^= 1;
+  }
+  LAUNCH(nsg::shape_apply(A, c->stream));
+  std::vector<unsigned long long> nrem(ncav);
+  CK(cudaMemcpyAsync(nrem.data(), c->sh_nrem.p, ncav * sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  int64_t tot = 0;
+  for (int q = 0; q < ncav; q++) {
+    tot += (int64_t)nrem[q];
+    // partially filled cavities stay open; completely filled ones are flagged
+    if (!c->cav_filled[q] && nrem[q] > 0 && (int64_t)nrem[q] == c->cav_count[q]) c->cav_filled[q] = 1;
+  }
+  c->shape_filtered = true;
+  c->ideb_ready = c->have_eps;
+  c->have_cav_atoms = false;
+  if (c->have_eps) c->have_bgp = c->bgp_projected = false;
+  c->n_vert = c->n_tri = 0;
+  if (n_removed) *n_removed = tot;
   return NSG_OK;
 }
 
@@ -1688,8 +1786,6 @@ int nsg_download_cavities(nsg_ctx* c, double* sizes, int32_t* filled) {
   return NSG_OK;
 }
 
-// Epsilon map in the reference's layout ((k*ny + j)*nx + i)*3 + axis (DelPhiShared::epsmap), after
-// cavity filling when nsg_cavities ran on this ray cast.
 int nsg_cavity_atoms(nsg_ctx* c, const double* atoms_xyzr, int64_t n_atoms, int32_t* offsets, int32_t* atoms,
                      int64_t* n_total) {
   if (!c || (n_atoms > 0 && !atoms_xyzr) || n_atoms < 0 || (atoms && !offsets)) return NSG_ERR_ARG;
@@ -1754,6 +1850,7 @@ int nsg_cavity_atoms(nsg_ctx* c, const double* atoms_xyzr, int64_t n_atoms, int3
       CK(cudaMemsetAsync(c->err.p, 0, sizeof(int32_t), c->stream));
       nsg::CavAtomArgs A{};
       A.status = c->status.as<int32_t>();
+      A.label = c->shape_filtered ? c->cav_label.as<int32_t>() : nullptr;
       A.nx = g.nx;
       A.ny = g.ny;
       A.nz = g.nz;
@@ -1818,6 +1915,8 @@ int nsg_cavity_atoms(nsg_ctx* c, const double* atoms_xyzr, int64_t n_atoms, int3
   return NSG_OK;
 }
 
+// Epsilon map in the reference's layout ((k*ny + j)*nx + i)*3 + axis (DelPhiShared::epsmap), after
+// cavity filling when nsg_cavities ran on this ray cast.
 int nsg_download_epsmap(nsg_ctx* c, int32_t* dst) {
   if (!c || !dst) return NSG_ERR_ARG;
   if (!c->have_eps) return fail(NSG_ERR_STATE, "no epsilon maps: ray cast with NSG_RAYCAST_EPSMAP");
@@ -1836,9 +1935,12 @@ int nsg_download_idebmap(nsg_ctx* c, uint8_t* dst) {
   CK(cudaSetDevice(c->device));
   const NsGrid& g = c->grid;
   const size_t nn = (size_t)g.nx * g.ny * g.nz;
-  CK(c->ideb.ensure(nn));
-  nsg::RunArgs A = run_args(c);
-  LAUNCH(nsg::ideb_write(A, c->eps_filled ? c->cc_fill_of.as<uint8_t>() : nullptr, c->ideb.as<uint8_t>(), c->stream));
+  if (!c->ideb_ready) {
+    CK(c->ideb.ensure(nn));
+    nsg::RunArgs A = run_args(c);
+    LAUNCH(nsg::ideb_write(A, c->eps_filled ? c->cc_fill_of.as<uint8_t>() : nullptr, c->ideb.as<uint8_t>(),
+                           c->stream));
+  }
   CK(cudaMemcpyAsync(dst, c->ideb.p, nn, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return NSG_OK;

@@ -208,8 +208,9 @@ __device__ __forceinline__ int32_t status_at(const CavAtomArgs& A, int64_t i, in
 __global__ void k_cav_atoms(CavAtomArgs A) {
   const int64_t n = A.nx * A.ny * A.nz;
   for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t lab = A.label ? A.label[v] : A.status[v];
+    if (lab < NS_STATUS_FIRST_CAV) continue;
     const int32_t s = A.status[v];
-    if (s < NS_STATUS_FIRST_CAV) continue;
     const int64_t i = v % A.nx, j = (v / A.nx) % A.ny, k = v / (A.nx * A.ny);
     if (status_at(A, i + 1, j, k) == s && status_at(A, i - 1, j, k) == s && status_at(A, i, j + 1, k) == s &&
         status_at(A, i, j - 1, k) == s && status_at(A, i, j, k + 1) == s && status_at(A, i, j, k - 1) == s)
@@ -236,9 +237,156 @@ __global__ void k_cav_atoms(CavAtomArgs A) {
     }
     const unsigned long long slot = atomicAdd(A.count, 1ull);
     if ((int64_t)slot < A.cap)
-      A.pairs[slot] = ((unsigned long long)(uint32_t)(s - NS_STATUS_FIRST_CAV) << 32) | (uint32_t)(first + 1);
+      A.pairs[slot] = ((unsigned long long)(uint32_t)(lab - NS_STATUS_FIRST_CAV) << 32) | (uint32_t)(first + 1);
     else
       atomicExch(A.err, 1);
+  }
+}
+
+// Water-shape filter.  The reference walks the kept cavities in order; within one cavity the
+// support test reads only whether each node of the probe box is in the cavity's in-set
+// (SHAPE_UNDER_CHECK, SHAPE_OK or -cavityId), a set that the walk does not change, so the supports
+// do not depend on the order of the cavity's points.  Across cavities, the removed nodes of an
+// earlier kept cavity stay SHAPE_UNDER_CHECK (or become SHAPE_OK inside a later support sphere)
+// when the status map is not modified, and count as in-set nodes of every later cavity.  The
+// passes below solve that lower-triangular dependency by fixed-point iteration: pass t takes the
+// removed set of pass t-1 for the earlier cavities, so cavity t is exact after pass t and a pass
+// that changes nothing is the reference's result.
+
+// The reference's probe box around node q along one axis (rintp of the shifted coordinates,
+// clamped to the grid).
+__device__ __forceinline__ void shape_axis(double mn, double side, double scale, double r, int64_t n, int64_t q,
+                                           int64_t* lo, int64_t* hi) {
+  const double x = mn + (double)q * side;
+  int64_t s = (int64_t)floor(((x - r) - mn) * scale + 0.5);
+  int64_t e = (int64_t)floor(((x + r) - mn) * scale + 0.5);
+  *lo = s < 0 ? 0 : (s >= n ? n - 1 : s);
+  *hi = e < 0 ? 0 : (e >= n ? n - 1 : e);
+}
+
+// |x_u - x_v|^2 with the grid coordinates min + i*side, as the reference evaluates it.
+__device__ __forceinline__ double shape_d2(const ShapeArgs& A, int64_t ui, int64_t uj, int64_t uk, int64_t vi,
+                                           int64_t vj, int64_t vk) {
+  const double a = (A.mn[0] + (double)ui * A.side) - (A.mn[0] + (double)vi * A.side);
+  const double b = (A.mn[1] + (double)uj * A.side) - (A.mn[1] + (double)vj * A.side);
+  const double c = (A.mn[2] + (double)uk * A.side) - (A.mn[2] + (double)vk * A.side);
+  return a * a + b * b + c * c;
+}
+
+__device__ __forceinline__ bool shape_kept(const ShapeArgs& A, int32_t lab) {
+  return lab >= NS_STATUS_FIRST_CAV && !A.filled[lab - NS_STATUS_FIRST_CAV];
+}
+
+// A node of a kept cavity is a support when no node of its probe sphere lies outside the in-set.
+__global__ void k_shape_support(ShapeArgs A) {
+  const int64_t n = A.nx * A.ny * A.nz;
+  const double r2 = A.r * A.r;
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t lab = A.label[v];
+    if (!shape_kept(A, lab)) continue;
+    const int64_t i = v % A.nx, j = (v / A.nx) % A.ny, k = v / (A.nx * A.ny);
+    int64_t lo[3], hi[3];
+    shape_axis(A.mn[0], A.side, A.scale, A.r, A.nx, i, &lo[0], &hi[0]);
+    shape_axis(A.mn[1], A.side, A.scale, A.r, A.ny, j, &lo[1], &hi[1]);
+    shape_axis(A.mn[2], A.side, A.scale, A.r, A.nz, k, &lo[2], &hi[2]);
+    bool ok = true;
+    for (int64_t z = lo[2]; z <= hi[2] && ok; z++)
+      for (int64_t y = lo[1]; y <= hi[1] && ok; y++)
+        for (int64_t x = lo[0]; x <= hi[0]; x++) {
+          if (shape_d2(A, x, y, z, i, j, k) > r2) continue;
+          const int64_t u = (z * A.ny + y) * A.nx + x;
+          const int32_t lu = A.label[u];
+          if (lu == lab) continue;
+          if (A.removed_prev && A.removed_prev[u] && lu >= NS_STATUS_FIRST_CAV && lu < lab) continue;
+          ok = false;
+          break;
+        }
+    A.support[v] = ok ? 1 : 0;
+  }
+}
+
+// A node of a kept cavity is removed when no support of its own cavity has it in its probe
+// sphere; `later` records a support sphere of a later cavity (which only reaches removed nodes).
+// Gathered from the node's side: the supports whose probe box can hold it lie within its own box
+// widened by one node, and each is tested with the support's own box and distance.
+__global__ void k_shape_cover(ShapeArgs A) {
+  const int64_t n = A.nx * A.ny * A.nz;
+  const double r2 = A.r * A.r;
+  for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < n; u += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t lab = A.label[u];
+    if (!shape_kept(A, lab)) continue;
+    const int64_t i = u % A.nx, j = (u / A.nx) % A.ny, k = u / (A.nx * A.ny);
+    int64_t lo[3], hi[3];
+    shape_axis(A.mn[0], A.side, A.scale, A.r, A.nx, i, &lo[0], &hi[0]);
+    shape_axis(A.mn[1], A.side, A.scale, A.r, A.ny, j, &lo[1], &hi[1]);
+    shape_axis(A.mn[2], A.side, A.scale, A.r, A.nz, k, &lo[2], &hi[2]);
+    const int64_t nn[3] = {A.nx, A.ny, A.nz};
+    for (int d = 0; d < 3; d++) {
+      lo[d] = lo[d] > 0 ? lo[d] - 1 : 0;
+      hi[d] = hi[d] < nn[d] - 1 ? hi[d] + 1 : nn[d] - 1;
+    }
+    bool own = false, later = false;
+    for (int64_t z = lo[2]; z <= hi[2] && !own; z++)
+      for (int64_t y = lo[1]; y <= hi[1] && !own; y++)
+        for (int64_t x = lo[0]; x <= hi[0]; x++) {
+          const int64_t v = (z * A.ny + y) * A.nx + x;
+          if (!A.support[v]) continue;
+          const int32_t lv = A.label[v];
+          if (lv < lab || (lv > lab && later)) continue;
+          int64_t a0, a1, b0, b1, c0, c1;
+          shape_axis(A.mn[0], A.side, A.scale, A.r, A.nx, x, &a0, &a1);
+          shape_axis(A.mn[1], A.side, A.scale, A.r, A.ny, y, &b0, &b1);
+          shape_axis(A.mn[2], A.side, A.scale, A.r, A.nz, z, &c0, &c1);
+          if (i < a0 || i > a1 || j < b0 || j > b1 || k < c0 || k > c1) continue;
+          if (shape_d2(A, i, j, k, x, y, z) > r2) continue;
+          if (lv == lab) {
+            own = true;
+            break;
+          }
+          later = true;
+        }
+    const uint8_t rm = own ? 0 : 1;
+    A.removed[u] = rm;
+    A.later[u] = later ? 1 : 0;
+    if (A.removed_prev && A.removed_prev[u] != rm) atomicExch(A.changed, 1);
+  }
+}
+
+__global__ void k_shape_apply(ShapeArgs A) {
+  const int64_t n = A.nx * A.ny * A.nz;
+  const int64_t plane = A.nx * A.ny;
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < n; v += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t lab = A.label[v];
+    if (!shape_kept(A, lab)) continue;
+    if (A.support[v]) {
+      A.status[v] = -lab;
+      continue;
+    }
+    if (!A.removed[v]) {
+      A.status[v] = lab;
+      continue;
+    }
+    A.status[v] = A.mod_status ? NS_STATUS_INSIDE : (A.later[v] ? NS_STATUS_SHAPE_OK : NS_STATUS_SHAPE_UNDER_CHECK);
+    atomicAdd(A.n_removed + (lab - NS_STATUS_FIRST_CAV), 1ull);
+    const int64_t i = v % A.nx, j = (v / A.nx) % A.ny, k = v / plane;
+    if (A.bits) {
+      // the 8 corners of the node's cube (a cavity never touches the grid's last planes)
+      for (int dk = 0; dk < 2; dk++)
+        for (int dj = 0; dj < 2; dj++)
+          for (int di = 0; di < 2; di++) {
+            const int64_t f = v + dk * plane + dj * A.nx + di;
+            if ((f >> 5) < A.nwords) atomicAnd(A.bits + (f >> 5), ~(1u << (f & 31)));
+          }
+    }
+    if (A.eps) {
+      A.eps[3 * v] = NS_EPS_INSIDE;
+      A.eps[3 * v + 1] = NS_EPS_INSIDE;
+      A.eps[3 * v + 2] = NS_EPS_INSIDE;
+      if (i > 0) A.eps[3 * (v - 1)] = NS_EPS_INSIDE;
+      if (j > 0) A.eps[3 * (v - A.nx) + 1] = NS_EPS_INSIDE;
+      if (k > 0) A.eps[3 * (v - plane) + 2] = NS_EPS_INSIDE;
+    }
+    if (A.ideb) A.ideb[v] = 0;
   }
 }
 
@@ -293,6 +441,21 @@ cudaError_t cavity_atom_pairs(const CavAtomArgs& A, cudaStream_t s) {
   const int64_t n = A.nx * A.ny * A.nz;
   if (n <= 0) return cudaSuccess;
   k_cav_atoms<<<grid_for(n), 256, 0, s>>>(A);
+  return cudaGetLastError();
+}
+
+cudaError_t shape_pass(const ShapeArgs& A, cudaStream_t s) {
+  const int64_t n = A.nx * A.ny * A.nz;
+  if (n <= 0) return cudaSuccess;
+  k_shape_support<<<grid_for(n), 256, 0, s>>>(A);
+  k_shape_cover<<<grid_for(n), 256, 0, s>>>(A);
+  return cudaGetLastError();
+}
+
+cudaError_t shape_apply(const ShapeArgs& A, cudaStream_t s) {
+  const int64_t n = A.nx * A.ny * A.nz;
+  if (n <= 0) return cudaSuccess;
+  k_shape_apply<<<grid_for(n), 256, 0, s>>>(A);
   return cudaGetLastError();
 }
 

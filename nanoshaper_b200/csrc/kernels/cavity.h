@@ -43,6 +43,7 @@ cudaError_t status_write(const RunArgs& A, const int32_t* label_of, int32_t* sta
 // (z*gn + y)*gn + x, its atoms in ascending index order at cell_off.
 struct CavAtomArgs {
   const int32_t* status;
+  const int32_t* label;       // cavity membership (the labels before a shape filter); nullptr: status
   int64_t nx, ny, nz;
   double mn[3], side;
   int64_t gn;
@@ -60,6 +61,36 @@ struct CavAtomArgs {
 // around the node, in the reference's cell order, the first of equal ones; atom -1 when the cells
 // hold no atom.
 cudaError_t cavity_atom_pairs(const CavAtomArgs& A, cudaStream_t s);
+
+// Water-shape filter of the cavities that filling kept (filterCavitiesWithBilevelStatusMap,
+// src/Surface.cpp:3011-3290), on the dense status map after cavity detection.  A node of cavity c
+// is a support when every grid node within the probe radius of it (inside the reference's
+// rounded box) belongs to the filter's in-set of c: the nodes of c, and the removed nodes of the
+// kept cavities before c, which the reference leaves as SHAPE_UNDER_CHECK / SHAPE_OK when the
+// status map is not modified.  A node of c outside every support sphere of c is removed.
+struct ShapeArgs {
+  int32_t* status;              // labels in, filtered codes out
+  const int32_t* label;         // the labels (FIRST_CAV + c for cavity c) before the filter
+  int64_t nx, ny, nz;
+  double mn[3], side, scale, r;
+  const uint8_t* filled;        // per cavity: filled by the volume threshold (skipped)
+  int mod_status;               // removed nodes become STATUS_POINT_INSIDE
+  uint8_t* support;             // per node
+  uint8_t* removed;             // per node, this pass
+  const uint8_t* removed_prev;  // per node, the pass before; nullptr on the first pass
+  uint8_t* later;               // per node: inside a support sphere of a later cavity
+  int32_t* changed;             // set when removed differs from removed_prev
+  uint32_t* bits;               // insideness bits or nullptr
+  int64_t nwords;
+  int32_t* eps;                 // epsilon map or nullptr
+  uint8_t* ideb;                // ideb map or nullptr
+  unsigned long long* n_removed;  // per cavity
+};
+// One pass: supports from the removed set of the pass before, then the removed set.
+cudaError_t shape_pass(const ShapeArgs& A, cudaStream_t s);
+// Filtered status codes; the removed nodes' insideness bits, epsilon and ideb entries.
+cudaError_t shape_apply(const ShapeArgs& A, cudaStream_t s);
+
 // Sorts the n pairs and keeps one of each; pass temp == nullptr to query temp_bytes.
 cudaError_t sort_unique_u64(unsigned long long* keys, unsigned long long* keys_alt, int64_t n, int64_t* n_unique,
                             void* temp, size_t* temp_bytes, cudaStream_t s);

@@ -85,6 +85,9 @@ NS_HD bool ns_has_box(int kind) { return kind >= NS_SKIN_POINT; }
 #define NS_STATUS_TEMPORARY_OUT 2
 #define NS_STATUS_OUT 3
 #define NS_STATUS_FIRST_CAV 4
+// water-shape filter codes (src/DelphiShared.h:22-23)
+#define NS_STATUS_SHAPE_UNDER_CHECK (-3)
+#define NS_STATUS_SHAPE_OK (-2)
 
 // Epsilon-map code of the inside medium: every surface type sets inside = 5
 // (src/ConnollySurface.cpp:214, src/SkinSurface.cpp:200, src/BlobbySurface.cpp:18,

@@ -353,6 +353,7 @@ class Surface:
         self.precision = cf.read("Gpu_Precision", "fp64", str).strip().lower()
         self.projBGP = cf.read("Project_boundary_grid_points", False, bool)
         self.auxGridDim = cf.read("Max_ses_patches_auxiliary_grid_size", 50, int)
+        self.keepWellShapedCavities = cf.read("Keep_Water_Shaped_Cavities", False, bool)
         self.randDisplacement = RAND_DISPLACEMENT
         self.device = device
         self.ctx: Context | None = None
@@ -388,6 +389,25 @@ class Surface:
         N.check(N.lib().nsg_set_grid(c, ctypes.byref(self.delphi.grid)), "set_grid")
         N.check(N.lib().nsg_upload_patches(c, p.n, N.ptr(p.f64), N.ptr(p.i32), len(p.pool), N.ptr(p.pool),
                                            N.ptr(p.pool_flag), p.probe), "upload_patches")
+
+    def setKeepWellShapedCavities(self, flag: bool) -> None:
+        self.keepWellShapedCavities = bool(flag)
+
+    def filterCavities(self, modStatus: bool = False) -> int:
+        """Water-shape filter of the cavities kept by the last cavity detection
+        (filterCavitiesWithBilevelStatusMap, src/Surface.cpp:3011-3290) with a probe of
+        ``probe_radius``: the nodes of a cavity that no probe sphere inside the cavity covers are
+        filled; a cavity filled completely is flagged in ``delphi.cavitiesFlag``.  Returns the
+        number of filled nodes."""
+        c = self._context().handle
+        nrem = ctypes.c_int64()
+        N.check(N.lib().nsg_filter_cavities(c, float(self.probe_radius), int(bool(modStatus)), ctypes.byref(nrem)),
+                "cavity shape filter")
+        flagv = np.zeros(max(self.ncav, 0), np.int32)
+        if self.ncav > 0:
+            N.check(N.lib().nsg_download_cavities(c, None, N.ptr(flagv)), "download cavities")
+        self.delphi.cavitiesFlag = [bool(f) for f in flagv]
+        return nrem.value
 
     def getCavitiesAtoms(self) -> list[list[int]]:
         """Atoms lining each cavity of the last cavity detection (getCavitiesAtomsWithBilevelStatusMap,
@@ -448,6 +468,8 @@ class Surface:
                 N.check(N.lib().nsg_download_cavities(c, N.ptr(sizes), N.ptr(flagv)), "download cavities")
             self.delphi.cavitiesSize = sizes.tolist()
             self.delphi.cavitiesFlag = [bool(f) for f in flagv]
+            if self.keepWellShapedCavities:
+                self.filterCavities()
             self.getCavitiesAtoms()
         if download:
             g = self.delphi.grid

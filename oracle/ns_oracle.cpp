@@ -1427,6 +1427,111 @@ void nso_free_mesh(void* h) { delete (BlobbyMesh*)h; }
 
 extern "C" {
 
+// Water-shape filter of the kept cavities, Keep_Water_Shaped_Cavities
+// (Surface::filterCavitiesWithBilevelStatusMap, src/Surface.cpp:3011-3290), restated loop for
+// loop: cavity by cavity, each of its points marked SHAPE_UNDER_CHECK, then every point whose
+// probe sphere (the rintp box, clamped, and dist^2 <= r^2 on the grid coordinates) holds no node
+// outside {SHAPE_UNDER_CHECK, SHAPE_OK, -cavityId} becomes a support (-cavityId) and marks the
+// sphere SHAPE_OK; the points left SHAPE_UNDER_CHECK are removed (epsilon, ideb and insideness
+// entries as fillCavities writes them) and become STATUS_POINT_INSIDE when mod_status is set,
+// the SHAPE_OK ones return to cavityId.  status holds the labels after cavity detection and is
+// modified in place; filled (per cavity) is the fillCavities flag, updated as the reference
+// updates cavitiesFlag.  The points of a cavity are taken in ascending node order rather than in
+// the flood fill's order: the support test reads only membership of the set above, which the
+// walk over one cavity does not change.  Returns the number of removed points.
+int64_t nso_shape_filter(const NsGrid* gp, int32_t* status, int ncav, int32_t* filled, uint32_t* bits, int64_t nwords,
+                         int32_t* eps, uint8_t* ideb, double probe, int mod_status) {
+  const NsGrid& g = *gp;
+  const int64_t NX = g.nx, NY = g.ny, NZ = g.nz, plane = NX * NY, n = plane * NZ;
+  std::vector<std::vector<int64_t>> pts(ncav);
+  for (int64_t f = 0; f < n; f++)
+    if (status[f] >= NS_STATUS_FIRST_CAV && status[f] - NS_STATUS_FIRST_CAV < ncav)
+      pts[status[f] - NS_STATUS_FIRST_CAV].push_back(f);
+  std::vector<double> X(NX), Y(NY), Z(NZ);
+  for (int64_t i = 0; i < NX; i++) X[i] = g.xmin + i * g.side;
+  for (int64_t i = 0; i < NY; i++) Y[i] = g.ymin + i * g.side;
+  for (int64_t i = 0; i < NZ; i++) Z[i] = g.zmin + i * g.side;
+  auto box = [&](double c, double mn, int64_t N, int64_t& lo, int64_t& hi) {
+    lo = (int64_t)floor(((c - probe) - mn) * g.scale + 0.5);
+    hi = (int64_t)floor(((c + probe) - mn) * g.scale + 0.5);
+    if (lo < 0) lo = 0;
+    if (hi < 0) hi = 0;
+    if (hi >= N) hi = N - 1;
+    if (lo >= N) lo = N - 1;
+  };
+  const double dist2ref = probe * probe;
+  int64_t total = 0;
+  for (int c = 0; c < ncav; c++) {
+    if (filled[c]) continue;
+    const int cid = c + NS_STATUS_FIRST_CAV;
+    for (int64_t f : pts[c]) status[f] = NS_STATUS_SHAPE_UNDER_CHECK;
+    for (int64_t f : pts[c]) {
+      const int64_t vk = f / plane, vj = (f % plane) / NX, vi = f % NX;
+      int64_t x0, x1, y0, y1, z0, z1;
+      box(X[vi], g.xmin, NX, x0, x1);
+      box(Y[vj], g.ymin, NY, y0, y1);
+      box(Z[vk], g.zmin, NZ, z0, z1);
+      bool go_out = false;
+      for (int64_t iz = z0; iz <= z1 && !go_out; iz++)
+        for (int64_t iy = y0; iy <= y1 && !go_out; iy++)
+          for (int64_t ix = x0; ix <= x1; ix++) {
+            const double a = X[ix] - X[vi], b = Y[iy] - Y[vj], cc = Z[iz] - Z[vk];
+            if (a * a + b * b + cc * cc > dist2ref) continue;
+            const int32_t val = status[(iz * NY + iy) * NX + ix];
+            if (val != NS_STATUS_SHAPE_UNDER_CHECK && val != NS_STATUS_SHAPE_OK && val != -cid) {
+              go_out = true;
+              break;
+            }
+          }
+      if (go_out) continue;
+      for (int64_t iz = z0; iz <= z1; iz++)
+        for (int64_t iy = y0; iy <= y1; iy++)
+          for (int64_t ix = x0; ix <= x1; ix++) {
+            const double a = X[ix] - X[vi], b = Y[iy] - Y[vj], cc = Z[iz] - Z[vk];
+            if (a * a + b * b + cc * cc > dist2ref) continue;
+            int32_t& val = status[(iz * NY + iy) * NX + ix];
+            if (val != -cid) val = NS_STATUS_SHAPE_OK;
+          }
+      status[f] = -cid;
+    }
+    int64_t removed = 0;
+    for (int64_t f : pts[c]) {
+      if (status[f] == NS_STATUS_SHAPE_UNDER_CHECK) {
+        removed++;
+        const int64_t vk = f / plane, vj = (f % plane) / NX;
+        if (eps) {
+          for (int a = 0; a < 3; a++) eps[3 * f + a] = NS_EPS_INSIDE;
+          if (f % NX > 0) eps[3 * (f - 1)] = NS_EPS_INSIDE;
+          if (vj > 0) eps[3 * (f - NX) + 1] = NS_EPS_INSIDE;
+          if (vk > 0) eps[3 * (f - plane) + 2] = NS_EPS_INSIDE;
+        }
+        if (ideb) ideb[f] = 0;
+        if (bits)
+          for (int dk = 0; dk < 2; dk++)
+            for (int dj = 0; dj < 2; dj++)
+              for (int di = 0; di < 2; di++) {
+                const int64_t q = f + dk * plane + dj * NX + di;
+                if ((q >> 5) < nwords) bits[q >> 5] &= ~(1u << (q & 31));
+              }
+      }
+      if (mod_status && status[f] == NS_STATUS_SHAPE_UNDER_CHECK)
+        status[f] = NS_STATUS_INSIDE;
+      else if (status[f] == NS_STATUS_SHAPE_OK)
+        status[f] = cid;
+    }
+    if (removed && removed != (int64_t)pts[c].size())
+      filled[c] = 0;
+    else if (removed && removed == (int64_t)pts[c].size())
+      filled[c] = 1;
+    total += removed;
+  }
+  return total;
+}
+
+}  // extern "C"
+
+extern "C" {
+
 // flags: 1 status map, 2 accurate-triangulation rays + insideness, 4 cavity detection/filling,
 //        8 marching cubes, 16 vertex normals (Compute_Vertex_Normals), 32 epsilon and ideb maps
 //        (Build_epsilon_maps), 64 boundary grid points and their projection (with 32).

@@ -66,6 +66,8 @@ def lib() -> ctypes.CDLL:
         L.nso_mesh_copy.restype = ctypes.c_int
         L.nso_mesh_copy.argtypes = [P, ctypes.c_char_p, P]
         L.nso_free_mesh.argtypes = [P]
+        L.nso_shape_filter.restype = ctypes.c_int64
+        L.nso_shape_filter.argtypes = [P, P, ctypes.c_int, P, P, ctypes.c_int64, P, P, ctypes.c_double, ctypes.c_int]
         L.nso_ray_torus.restype = ctypes.c_int
         L.nso_ray_torus.argtypes = [P, P, P, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int, P, P, P]
         _lib = L
@@ -310,20 +312,41 @@ def atom_grid(grid, atoms: np.ndarray):
     return ggrid, gmin, gscale, cells
 
 
-def cavity_atoms(grid, status: np.ndarray, ncav: int, atoms: np.ndarray) -> list[list[int]]:
+def shape_filter(grid, status: np.ndarray, ncav: int, filled, bits=None, eps=None, ideb=None, probe: float = 1.4,
+                 mod_status: bool = False):
+    """Keep_Water_Shaped_Cavities on copies of the maps after cavity detection
+    (nso_shape_filter in ns_oracle.cpp).  Returns (status, filled, bits, eps, ideb, removed)."""
+    L = lib()
+    st = np.ascontiguousarray(status, np.int32).copy()
+    fl = np.ascontiguousarray(filled, np.int32).copy()
+    b = None if bits is None else np.ascontiguousarray(bits, np.uint32).copy()
+    e = None if eps is None else np.ascontiguousarray(eps, np.int32).copy()
+    d = None if ideb is None else np.ascontiguousarray(ideb, np.uint8).copy()
+
+    def ptr(a):
+        return None if a is None else a.ctypes.data
+    n = L.nso_shape_filter(ctypes.byref(grid), st.ctypes.data, int(ncav), ptr(fl), ptr(b), 0 if b is None else b.size,
+                           ptr(e), ptr(d), float(probe), int(bool(mod_status)))
+    return st, fl, b, e, None if d is None else d.astype(bool), int(n)
+
+
+def cavity_atoms(grid, status: np.ndarray, ncav: int, atoms: np.ndarray, label: np.ndarray | None = None) -> list[list[int]]:
     """cav2atoms as Surface::getCavitiesAtomsWithBilevelStatusMap fills it
     (src/Surface.cpp:2249-2346): for every node of cavity c (status 4 + c) with a 6-neighbour of
     another status (TEMPORARY_OUT = 2 outside the grid), the atom of least |a - x|^2 - r^2 over the
     27 atom-grid cells around the node, scanned in shift_map order and ascending atom order with a
     strict comparison (the first of equal ones wins), -1 when those cells are empty; per cavity the
-    distinct atoms ascending (std::set order).  Vectorised over the boundary nodes: one pass per
+    distinct atoms ascending (std::set order).  After a shape filter the cavities' points are
+    those of ``label`` (the labels before it) and the comparisons read the filtered ``status``.
+    Vectorised over the boundary nodes: one pass per
     (cell shift, slot within the cell) keeps the scan order of the reference's loops."""
     nz, ny, nx = status.shape
     pad = np.pad(status, 1, constant_values=2)
     s = pad[1:-1, 1:-1, 1:-1]
     same = ((pad[1:-1, 1:-1, 2:] == s) & (pad[1:-1, 1:-1, :-2] == s) & (pad[1:-1, 2:, 1:-1] == s) &
             (pad[1:-1, :-2, 1:-1] == s) & (pad[2:, 1:-1, 1:-1] == s) & (pad[:-2, 1:-1, 1:-1] == s))
-    k, j, i = np.nonzero((status >= 4) & ~same)
+    lab = status if label is None else np.asarray(label).reshape(status.shape)
+    k, j, i = np.nonzero((lab >= 4) & ~same)
     out: list[set] = [set() for _ in range(ncav)]
     if len(i) == 0:
         return [sorted(x) for x in out]
@@ -350,7 +373,7 @@ def cavity_atoms(grid, status: np.ndarray, ncav: int, atoms: np.ndarray) -> list
             better = has & (d < best)
             best = np.where(better, d, best)
             first = np.where(better, a, first)
-    cav = status[k, j, i] - 4
+    cav = lab[k, j, i] - 4
     for cc, a in zip(cav.tolist(), first.tolist()):
         out[cc].add(a)
     return [sorted(x) for x in out]

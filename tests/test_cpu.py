@@ -874,3 +874,99 @@ def test_write_cavity_atoms_layout(native_lib, tmp_path):
     N.check(N.lib().nsg_write_cavity_atoms(str(p).encode(), 3, N.ptr(off), N.ptr(lst), N.ptr(serials), 10,
                                            N.ptr(skip)), "write")
     assert p.read_text() == "0 104 109 \n100 102 \n"
+
+
+def _box_grid(n: int, scale: float):
+    from nanoshaper_b200 import _native as N
+    g = N.NsGrid()
+    g.nx = g.ny = g.nz = n
+    g.xmin = g.ymin = g.zmin = -3.0
+    g.xmax = g.ymax = g.zmax = -3.0 + (n - 1) / scale
+    g.scale, g.side, g.hside = scale, 1.0 / scale, 0.5 / scale
+    return g
+
+
+def _shape_fixed_point(g, lab, filled, r, mod):
+    """The device formulation of the water-shape filter, restated in Python: supports read the
+    removed set of the pass before for the earlier cavities, passes repeat until the removed set
+    settles; then the status codes."""
+    nz, ny, nx = lab.shape
+    X = [g.xmin + i * g.side for i in range(nx)]
+
+    def box(q, n):
+        x = g.xmin + q * g.side
+        lo = int(np.floor(((x - r) - g.xmin) * g.scale + 0.5))
+        hi = int(np.floor(((x + r) - g.xmin) * g.scale + 0.5))
+        return min(max(lo, 0), n - 1), min(max(hi, 0), n - 1)
+
+    def sphere(k, j, i):
+        (z0, z1), (y0, y1), (x0, x1) = box(k, nz), box(j, ny), box(i, nx)
+        for z in range(z0, z1 + 1):
+            for y in range(y0, y1 + 1):
+                for x in range(x0, x1 + 1):
+                    a, b, c = X[x] - X[i], X[y] - X[j], X[z] - X[k]
+                    if a * a + b * b + c * c <= r * r:
+                        yield z, y, x
+
+    nodes = [tuple(v) for v in np.argwhere(lab >= 4) if not filled[lab[tuple(v)] - 4]]
+    prev = None
+    for t in range(len(filled) + 1):
+        sup = {v for v in nodes if all(lab[u] == lab[v] or (prev is not None and u in prev and 4 <= lab[u] < lab[v])
+                                       for u in sphere(*v))}
+        own, later = set(), set()
+        for v in sup:
+            for u in sphere(*v):
+                (own if lab[u] == lab[v] else later).add(u)
+        removed = {v for v in nodes if v not in own}
+        if mod or (t > 0 and removed == prev):
+            break
+        prev = removed
+    st = lab.copy()
+    for v in nodes:
+        L = lab[v]
+        st[v] = -L if v in sup else (L if v not in removed else (-1 if mod else (-2 if v in later else -3)))
+    return st, removed
+
+
+def test_oracle_shape_filter_known_cube(oracle_mod):
+    """An 8^3 block cavity at scale 1 with a 1.4 A probe: the probe sphere is a node and its six
+    face neighbours, so the 6^3 interior nodes are supports and the 12 edges (with the corners,
+    80 nodes) are removed; the cavity stays open."""
+    g = _box_grid(14, 1.0)
+    lab = np.full((14, 14, 14), -1, np.int32)
+    lab[:2] = 3
+    lab[3:11, 3:11, 3:11] = 4
+    st, fl, _b, _e, _d, nrem = oracle_mod.shape_filter(g, lab, 1, [0], probe=1.4)
+    assert nrem == 80 and fl.tolist() == [0]
+    assert (st == -4).sum() == 216 and (st == 4).sum() == 512 - 216 - 80 and (st == -3).sum() == 80
+    st2, fl2, *_rest, nrem2 = oracle_mod.shape_filter(g, lab, 1, [0], probe=1.4, mod_status=True)
+    assert nrem2 == 80 and (st2 == -1).sum() == (lab == -1).sum() + 80
+
+
+def test_oracle_shape_filter_matches_fixed_point(oracle_mod):
+    """The oracle's cavity-by-cavity loops equal the device's fixed-point formulation on touching
+    cavities with ragged walls (the removed nodes of an earlier cavity count for a later one when
+    the status map is kept), a thin cavity removed completely (flagged filled) and a filled one
+    (skipped)."""
+    g = _box_grid(26, 2.0)
+    rng = np.random.default_rng(7)
+    lab = np.full((26, 26, 26), -1, np.int32)
+    lab[:2] = 3
+    lab[3:13, 3:20, 3:20] = 4
+    lab[13:22, 3:20, 3:20] = 5
+    lab[6:9, 22:24, 4:20] = 6           # two nodes thick: no probe sphere fits
+    lab[18:22, 21:24, 21:24] = 7        # filled by the volume threshold
+    noise = rng.random(lab.shape) < 0.04
+    lab[noise & (lab >= 4) & (lab <= 5)] = -1
+    filled = [0, 0, 0, 1]
+    cross = False
+    for mod in (False, True):
+        st, fl, _b, _e, _d, nrem = oracle_mod.shape_filter(g, lab, 4, filled, probe=1.4, mod_status=mod)
+        want, removed = _shape_fixed_point(g, lab, filled, 1.4, mod)
+        np.testing.assert_array_equal(st, want)
+        assert nrem == len(removed)
+        assert fl.tolist()[2:] == [1, 1] and fl.tolist()[:2] == [0, 0]
+        if not mod:
+            own_only, _ = _shape_fixed_point(g, lab, filled, 1.4, True)
+            cross = bool(((want == -4 - 1) != (own_only == -4 - 1)).any())
+    assert cross, "the case should exercise removed nodes of cavity 4 inside supports of cavity 5"
