@@ -247,6 +247,20 @@ int nsg_cavities(nsg_ctx* ctx, double cavity_volume, int* n_cavities);
  * filled (nsg_download_cavities); nsg_cavity_atoms keeps the cavity membership from before the
  * filter.  Once per nsg_cavities; n_removed (may be NULL) receives the removed node count. */
 int nsg_filter_cavities(nsg_ctx* ctx, double probe_radius, int modify_status, int64_t* n_removed);
+/* Pocket detection by difference, the step `(*surf1) -= (*surf2)` of pocket mode followed by
+ * fillCavities (src/main.cpp:1533, 1586; Surface::operator-= src/Surface.cpp:15556-15619).
+ * ctx holds the fat-probe surface and small the small-probe one, both ray cast on the same grid
+ * (cavity detection on either is optional: its cavities then count as inside, as the reference's
+ * cavity codes do).  Surface::difference (src/Surface.cpp:11471-11717) marks the nodes inside the
+ * fat surface and outside the small one as one cavity and every other node inside; the water-shape
+ * filter with a 1.4 A probe and the status map modified (nsg_filter_cavities) keeps the part a
+ * water molecule fits in; cav2out returns it to TEMPORARY_OUT, and its 6-connected regions become
+ * the pockets 4, 5, ... in the reference's alternating-z seed order; pockets of at most
+ * fill_volume A^3 are filled.  Afterwards ctx is in the state nsg_cavities leaves (pocket sizes and
+ * flags from nsg_download_cavities, nsg_cavity_atoms, nsg_download_status, insideness bits).
+ * The epsilon and ideb maps are left as the reference leaves them (not differenced).  Linking of
+ * split pockets (linkCavities) is not part of this call. */
+int nsg_pocket_difference(nsg_ctx* ctx, nsg_ctx* small, double fill_volume, int* n_pockets);
 /* Label order of the alternating-z seed scan of getCavitiesWithBilevelStatusMap
  * (src/Surface.cpp:2044-2116) over regions sorted by first node; host only. */
 int nsg_cavity_order(int32_t n_regions, const uint32_t* desc_key, int32_t* label_out);

@@ -73,6 +73,7 @@ _SIGNATURES = {
     "nsg_fp_peak": ([_P, _INT, ctypes.POINTER(_D)], _INT),
     "nsg_cavities": ([_P, _D, ctypes.POINTER(_INT)], _INT),
     "nsg_filter_cavities": ([_P, _D, _INT, ctypes.POINTER(ctypes.c_int64)], _INT),
+    "nsg_pocket_difference": ([_P, _P, _D, ctypes.POINTER(_INT)], _INT),
     "nsg_cavity_order": ([ctypes.c_int32, _P, _P], _INT),
     "nsg_triangulate": ([_P, ctypes.POINTER(_D), ctypes.POINTER(_I64), ctypes.POINTER(_I64)], _INT),
     "nsg_download_status": ([_P, _P], _INT),

@@ -1343,10 +1343,14 @@ int nsg_cavity_order(int32_t n, const uint32_t* desc_key, int32_t* label_out) {
   return NSG_OK;
 }
 
-int nsg_cavities(nsg_ctx* c, double cav_vol, int* ncav_out) {
-  if (!c || !c->have_status) return fail(NSG_ERR_STATE, "cavity detection needs the status map");
-  if (c->nstruct != 1) return fail(NSG_ERR_STATE, "cavity detection runs on a single structure");
-  CK(cudaSetDevice(c->device));
+}  // extern "C"
+
+namespace {
+
+// Region labelling of the context's free runs and conditional filling.  With `pockets` every
+// region is a cavity (getCavitiesWithBilevelStatusMap with idStart = STATUS_POINT_OUT, as the
+// difference map is labelled), else the first region found is the outside.
+int detect_cavities(nsg_ctx* c, double cav_vol, bool pockets, int* ncav_out) {
   const NsGrid& g = c->grid;
   const int64_t nr = c->n_fruns;
   c->cav_size.clear();
@@ -1397,7 +1401,9 @@ int nsg_cavities(nsg_ctx* c, double cav_vol, int* ncav_out) {
   std::vector<int32_t> label_of(nroots, 0);
   std::vector<uint8_t> fill_of(nroots, 0);
   nsg_cavity_order(nroots, desc.data(), label_of.data());
-  const int32_t id = NS_STATUS_TEMPORARY_OUT + nroots;
+  if (pockets)
+    for (auto& l : label_of) l++;
+  const int32_t id = NS_STATUS_TEMPORARY_OUT + nroots + (pockets ? 1 : 0);
   const double cube = g.side * g.side * g.side;
   c->ncav = id - NS_STATUS_OUT;
   c->cav_size.assign(c->ncav, 0.0);
@@ -1434,6 +1440,77 @@ int nsg_cavities(nsg_ctx* c, double cav_vol, int* ncav_out) {
   if (ncav_out) *ncav_out = c->ncav;
   c->n_vert = c->n_tri = 0;
   return NSG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int nsg_cavities(nsg_ctx* c, double cav_vol, int* ncav_out) {
+  if (!c || !c->have_status) return fail(NSG_ERR_STATE, "cavity detection needs the status map");
+  if (c->nstruct != 1) return fail(NSG_ERR_STATE, "cavity detection runs on a single structure");
+  CK(cudaSetDevice(c->device));
+  return detect_cavities(c, cav_vol, false, ncav_out);
+}
+
+int nsg_filter_cavities(nsg_ctx* c, double probe_radius, int modify_status, int64_t* n_removed);
+
+int nsg_pocket_difference(nsg_ctx* c, nsg_ctx* small, double fill_volume, int* n_pockets) {
+  if (!c || !small || c == small) return NSG_ERR_ARG;
+  if (!c->have_status || !small->have_status) return fail(NSG_ERR_STATE, "the difference needs both status maps");
+  if (c->nstruct != 1 || small->nstruct != 1) return fail(NSG_ERR_STATE, "the difference runs on single structures");
+  if (c->device != small->device) return fail(NSG_ERR_ARG, "both surfaces must live on one device");
+  const NsGrid& g = c->grid;
+  const NsGrid& h = small->grid;
+  if (g.nx != h.nx || g.ny != h.ny || g.nz != h.nz) return fail(NSG_ERR_ARG, "the two grids differ");
+  CK(cudaSetDevice(c->device));
+  const int64_t nn = g.nx * g.ny * g.nz;
+  if (!c->status_dense) {
+    int rc = materialize_status(c, nullptr);
+    if (rc) return rc;
+  }
+  if (!small->status_dense) {
+    int rc = materialize_status(small, nullptr);
+    if (rc) return rc;
+  }
+  CK(cudaStreamSynchronize(small->stream));
+  stage_begin(c, kStageCavity);
+  CK(c->ca_count.ensure(2 * sizeof(unsigned long long)));
+  CK(cudaMemsetAsync(c->ca_count.p, 0, sizeof(unsigned long long), c->stream));
+  LAUNCH(nsg::pocket_difference(c->status.as<int32_t>(), small->status.as<int32_t>(), nn,
+                                c->have_bits ? c->bits.as<uint32_t>() : nullptr, c->ca_count.as<unsigned long long>(),
+                                c->stream));
+  unsigned long long ndiff = 0;
+  CK(cudaMemcpyAsync(&ndiff, c->ca_count.p, sizeof(unsigned long long), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  // the difference is one cavity, kept, for the Connolly filter with a 1.4 A probe
+  c->ncav = 1;
+  c->cav_count.assign(1, (int64_t)ndiff);
+  c->cav_size.assign(1, (double)ndiff * g.side * g.side * g.side);
+  c->cav_filled.assign(1, 0);
+  c->cav_nodes = (int64_t)ndiff;
+  c->status_dense = c->cav_detected = true;
+  c->shape_filtered = c->have_cav_atoms = false;
+  c->eps_filled = false;
+  int rc = ndiff ? nsg_filter_cavities(c, 1.4, 1, nullptr) : NSG_OK;
+  if (rc) return rc;
+  if (ndiff) LAUNCH(nsg::pocket_cav2out(c->status.as<int32_t>(), c->cav_label.as<int32_t>(), nn, c->stream));
+  // the filtered map's free runs replace the cast's, then the regions are labelled as pockets
+  const int64_t nrows = g.ny * g.nz;
+  CK(c->fr_cnt.ensure(nrows * sizeof(int32_t)));
+  CK(c->fr_off.ensure((nrows + 1) * sizeof(int64_t)));
+  nsg::RunArgs A = run_args(c);
+  LAUNCH(nsg::dense_free_runs(A, c->status.as<int32_t>(), 0, c->stream));
+  int64_t nr = 0;
+  rc = scan_counts(c, c->fr_cnt.as<int32_t>(), nrows, c->fr_off.as<int64_t>(), &nr);
+  if (rc) return rc;
+  CK(c->fruns.ensure(std::max<int64_t>(nr, 1) * sizeof(int2)));
+  CK(c->frow.ensure(std::max<int64_t>(nr, 1) * sizeof(int32_t)));
+  c->n_fruns = nr;
+  A = run_args(c);
+  LAUNCH(nsg::dense_free_runs(A, c->status.as<int32_t>(), 1, c->stream));
+  stage_end(c, kStageCavity);
+  return detect_cavities(c, fill_volume, true, n_pockets);
 }
 
 int nsg_filter_cavities(nsg_ctx* c, double probe_radius, int modify_status, int64_t* n_removed) {

@@ -390,6 +390,66 @@ __global__ void k_shape_apply(ShapeArgs A) {
   }
 }
 
+// One warp per 32 consecutive nodes, so that each insideness word is formed by one ballot.
+__global__ void k_pocket_diff(int32_t* st1, const int32_t* st2, int64_t n, uint32_t* bits,
+                              unsigned long long* count) {
+  const int lane = threadIdx.x & 31;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  unsigned long long mine = 0;
+  for (int64_t f0 = blockIdx.x * (int64_t)blockDim.x + (threadIdx.x & ~31); f0 < n; f0 += stride) {
+    const int64_t f = f0 + lane;
+    bool pk = false;
+    if (f < n) {
+      const int32_t s1 = st1[f], s2 = st2[f];
+      pk = (s1 != NS_STATUS_TEMPORARY_OUT && s1 != NS_STATUS_OUT) &&
+           (s2 == NS_STATUS_TEMPORARY_OUT || s2 == NS_STATUS_OUT);
+      st1[f] = pk ? NS_STATUS_FIRST_CAV : NS_STATUS_INSIDE;
+    }
+    const uint32_t m = __ballot_sync(0xffffffffu, pk);
+    if (lane == 0) {
+      mine += __popc(m);
+      if (bits) {
+        const int64_t valid = n - f0 < 32 ? n - f0 : 32;
+        const uint32_t vm = valid == 32 ? 0xffffffffu : ((1u << valid) - 1u);
+        uint32_t* w = bits + (f0 >> 5);
+        *w = (*w & ~vm) | m;
+      }
+    }
+  }
+  if (lane == 0 && mine) atomicAdd(count, mine);
+}
+
+__global__ void k_pocket_cav2out(int32_t* status, const int32_t* __restrict__ label, int64_t n) {
+  for (int64_t f = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; f < n; f += (int64_t)gridDim.x * blockDim.x) {
+    if (label[f] != NS_STATUS_FIRST_CAV) continue;
+    const int32_t v = status[f];
+    if (v >= NS_STATUS_FIRST_CAV || v <= -NS_STATUS_FIRST_CAV) status[f] = NS_STATUS_TEMPORARY_OUT;
+  }
+}
+
+// One thread per x-row of the dense map.
+__global__ void k_dense_free_runs(RunArgs A, const int32_t* __restrict__ status, int emit) {
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < A.nrows; r += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t* row = status + r * A.nx;
+    int nf = 0;
+    int64_t o = emit ? A.fr_off[r] : 0;
+    int64_t start = -1;
+    for (int64_t i = 0; i <= A.nx; i++) {
+      const bool fr = i < A.nx && row[i] == NS_STATUS_TEMPORARY_OUT;
+      if (fr && start < 0) start = i;
+      if (!fr && start >= 0) {
+        if (emit) {
+          A.fruns[o + nf] = make_int2((int)start, (int)(i - 1));
+          A.frow[o + nf] = (int32_t)r;
+        }
+        nf++;
+        start = -1;
+      }
+    }
+    if (!emit) A.fr_cnt[r] = nf;
+  }
+}
+
 int grid_for(int64_t n, int threads = 256) {
   int64_t b = (n + threads - 1) / threads;
   const int64_t cap = (int64_t)sm_count() * 32;
@@ -456,6 +516,25 @@ cudaError_t shape_apply(const ShapeArgs& A, cudaStream_t s) {
   const int64_t n = A.nx * A.ny * A.nz;
   if (n <= 0) return cudaSuccess;
   k_shape_apply<<<grid_for(n), 256, 0, s>>>(A);
+  return cudaGetLastError();
+}
+
+cudaError_t pocket_difference(int32_t* st1, const int32_t* st2, int64_t n, uint32_t* bits, unsigned long long* count,
+                              cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_pocket_diff<<<grid_for(n), 256, 0, s>>>(st1, st2, n, bits, count);
+  return cudaGetLastError();
+}
+
+cudaError_t pocket_cav2out(int32_t* status, const int32_t* label, int64_t n, cudaStream_t s) {
+  if (n <= 0) return cudaSuccess;
+  k_pocket_cav2out<<<grid_for(n), 256, 0, s>>>(status, label, n);
+  return cudaGetLastError();
+}
+
+cudaError_t dense_free_runs(const RunArgs& A, const int32_t* status, int emit, cudaStream_t s) {
+  if (A.nrows <= 0) return cudaSuccess;
+  k_dense_free_runs<<<grid_for(A.nrows), 256, 0, s>>>(A, status, emit);
   return cudaGetLastError();
 }
 

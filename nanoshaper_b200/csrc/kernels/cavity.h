@@ -91,6 +91,19 @@ cudaError_t shape_pass(const ShapeArgs& A, cudaStream_t s);
 // Filtered status codes; the removed nodes' insideness bits, epsilon and ideb entries.
 cudaError_t shape_apply(const ShapeArgs& A, cudaStream_t s);
 
+// Pocket difference (Surface::difference, src/Surface.cpp:11471-11717), on the dense maps of the
+// fat-probe (st1, in/out) and small-probe (st2) surfaces: a node inside-or-cavity in st1 and
+// TEMPORARY_OUT / OUT in st2 becomes FIRST_CAV, every other node STATUS_POINT_INSIDE; its
+// insideness bit becomes the same predicate (the last of the reference's 8-corner writes to a
+// node is the node's own).  count receives the number of difference nodes.
+cudaError_t pocket_difference(int32_t* st1, const int32_t* st2, int64_t n, uint32_t* bits, unsigned long long* count,
+                              cudaStream_t s);
+// cav2outWithBilevelStatusMap (src/Surface.cpp:2691-2748) for the one difference cavity: its
+// nodes (label FIRST_CAV) still at a cavity or support code return to TEMPORARY_OUT.
+cudaError_t pocket_cav2out(int32_t* status, const int32_t* label, int64_t n, cudaStream_t s);
+// Free runs (TEMPORARY_OUT runs per x-row) of a dense status map; count pass then emit pass.
+cudaError_t dense_free_runs(const RunArgs& A, const int32_t* status, int emit, cudaStream_t s);
+
 // Sorts the n pairs and keeps one of each; pass temp == nullptr to query temp_bytes.
 cudaError_t sort_unique_u64(unsigned long long* keys, unsigned long long* keys_alt, int64_t n, int64_t* n_unique,
                             void* temp, size_t* temp_bytes, cudaStream_t s);

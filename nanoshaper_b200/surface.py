@@ -409,6 +409,36 @@ class Surface:
         self.delphi.cavitiesFlag = [bool(f) for f in flagv]
         return nrem.value
 
+    def difference(self, small: "Surface", fill_volume: float = 0.0) -> int:
+        """Pocket detection by difference, pocket mode's ``(*surf1) -= (*surf2)`` followed by
+        ``fillCavities`` (src/main.cpp:1533, 1586; Surface::operator-=, src/Surface.cpp:15556-15619):
+        this surface holds the fat-probe cast and ``small`` the small-probe cast of the same grid.
+        The nodes inside this surface and outside ``small`` that a 1.4 A water probe fits in become
+        the pockets (``ncav``, ``delphi.cavitiesSize`` / ``cavitiesFlag``, the status map with the
+        pocket labels); pockets of at most ``fill_volume`` A^3 are filled.  Returns the pocket
+        count."""
+        c = self._context().handle
+        n = ctypes.c_int()
+        N.check(N.lib().nsg_pocket_difference(c, small._context().handle, float(fill_volume), ctypes.byref(n)),
+                "pocket difference")
+        self.ncav = n.value
+        sizes = np.zeros(max(self.ncav, 0))
+        flagv = np.zeros(max(self.ncav, 0), np.int32)
+        if self.ncav > 0:
+            N.check(N.lib().nsg_download_cavities(c, N.ptr(sizes), N.ptr(flagv)), "download cavities")
+        self.delphi.cavitiesSize = sizes.tolist()
+        self.delphi.cavitiesFlag = [bool(f) for f in flagv]
+        g = self.delphi.grid
+        if self.delphi.buildStatus:
+            st = np.empty(g.nx * g.ny * g.nz, np.int32)
+            N.check(N.lib().nsg_download_status(c, N.ptr(st)), "download status")
+            self.delphi.status = st.reshape(g.nz, g.ny, g.nx)
+        if self.accurateTriangulation:
+            bits = np.empty(((g.nx + 31) >> 5) * g.ny * g.nz, np.uint32)
+            N.check(N.lib().nsg_download_insideness(c, N.ptr(bits)), "download insideness")
+            self.insideness = bits
+        return self.ncav
+
     def getCavitiesAtoms(self) -> list[list[int]]:
         """Atoms lining each cavity of the last cavity detection (getCavitiesAtomsWithBilevelStatusMap,
         src/Surface.cpp:2249-2346), into ``delphi.cav2atoms``: per cavity the ascending indices of

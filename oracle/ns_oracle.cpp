@@ -1528,6 +1528,102 @@ int64_t nso_shape_filter(const NsGrid* gp, int32_t* status, int ncav, int32_t* f
   return total;
 }
 
+
+// Pocket detection by difference: Surface::difference (flat status map, src/Surface.cpp:11471-11717)
+// loop for loop with its insideness writes, then operator-= (src/Surface.cpp:15556-15619): the
+// water-shape filter of the one difference cavity with a 1.4 A probe and the status map modified,
+// cav2out (src/Surface.cpp:2649-2689), getCavities(STATUS_POINT_OUT) (src/Surface.cpp:1877-1992:
+// the seed scan alternates ascending and descending z; each seed's TEMPORARY_OUT region is the next
+// pocket, here flooded breadth-first since only its node set matters), then fillCavities(fill_vol)
+// (src/Surface.cpp:2355-2484) on the insideness bits.  st1 (fat probe) is modified in place; sizes
+// and filled receive up to cap pockets.  Returns the number of pockets, -1 past cap.
+int nso_pocket_difference(const NsGrid* gp, int32_t* st1, const int32_t* st2, uint32_t* bits, int64_t nwords,
+                          double fill_vol, double* sizes, int32_t* filled, int cap) {
+  const NsGrid& g = *gp;
+  const int64_t NX = g.nx, NY = g.ny, NZ = g.nz, plane = NX * NY, n = plane * NZ;
+  auto setb = [&](int64_t i, int64_t j, int64_t k, bool v) {
+    const int64_t f = k * plane + j * NX + i;
+    if (!bits || (f >> 5) >= nwords) return;
+    if (v) bits[f >> 5] |= 1u << (f & 31);
+    else bits[f >> 5] &= ~(1u << (f & 31));
+  };
+  std::vector<int64_t> diff;
+  for (int64_t k = 0; k < NZ; k++)
+    for (int64_t j = 0; j < NY; j++)
+      for (int64_t i = 0; i < NX; i++) {
+        const int64_t f = k * plane + j * NX + i;
+        const int32_t s1 = st1[f], s2 = st2[f];
+        if ((s1 != NS_STATUS_TEMPORARY_OUT && s1 != NS_STATUS_OUT) &&
+            (s2 == NS_STATUS_TEMPORARY_OUT || s2 == NS_STATUS_OUT)) {
+          st1[f] = NS_STATUS_FIRST_CAV;
+          diff.push_back(f);
+          for (int dk = 0; dk < 2; dk++)
+            for (int dj = 0; dj < 2; dj++)
+              for (int di = 0; di < 2; di++) setb(i + di, j + dj, k + dk, true);
+        } else {
+          st1[f] = NS_STATUS_INSIDE;
+          for (int dk = 0; dk < 2; dk++)
+            for (int dj = 0; dj < 2; dj++)
+              for (int di = 0; di < 2; di++)
+                if (i + di < NX && j + dj < NY && k + dk < NZ) setb(i + di, j + dj, k + dk, false);
+        }
+      }
+  if (!diff.empty()) {
+    int32_t fl0 = 0;
+    nso_shape_filter(gp, st1, 1, &fl0, bits, nwords, nullptr, nullptr, 1.4, 1);
+    for (int64_t f : diff)
+      if (st1[f] >= NS_STATUS_FIRST_CAV || st1[f] <= -NS_STATUS_FIRST_CAV) st1[f] = NS_STATUS_TEMPORARY_OUT;
+  }
+  int id = NS_STATUS_OUT, times = 0;
+  std::vector<std::vector<int64_t>> regions;
+  std::vector<int64_t> queue;
+  while (true) {
+    int64_t seed = -1;
+    for (int64_t kk = 0; kk < NZ && seed < 0; kk++) {
+      const int64_t k = (times % 2 == 0) ? kk : NZ - 1 - kk;
+      for (int64_t q = k * plane; q < (k + 1) * plane; q++)
+        if (st1[q] == NS_STATUS_TEMPORARY_OUT) { seed = q; break; }
+    }
+    times++;
+    if (seed < 0) break;
+    id++;
+    std::vector<int64_t> nodes;
+    queue.assign(1, seed);
+    st1[seed] = id;
+    for (size_t h = 0; h < queue.size(); h++) {
+      const int64_t f = queue[h];
+      nodes.push_back(f);
+      const int64_t k = f / plane, j = (f % plane) / NX, i = f % NX;
+      const int64_t nb[6][3] = {{i + 1, j, k}, {i - 1, j, k}, {i, j + 1, k}, {i, j - 1, k}, {i, j, k + 1}, {i, j, k - 1}};
+      for (auto& b : nb) {
+        if (b[0] < 0 || b[1] < 0 || b[2] < 0 || b[0] >= NX || b[1] >= NY || b[2] >= NZ) continue;
+        const int64_t u = b[2] * plane + b[1] * NX + b[0];
+        if (st1[u] != NS_STATUS_TEMPORARY_OUT) continue;
+        st1[u] = id;
+        queue.push_back(u);
+      }
+    }
+    regions.push_back(std::move(nodes));
+  }
+  const int ncav = (int)regions.size();
+  if (ncav > cap) return -1;
+  const double cube = g.side * g.side * g.side;
+  for (int c = 0; c < ncav; c++) {
+    const double vol = regions[c].size() * cube;
+    sizes[c] = vol;
+    filled[c] = vol <= fill_vol ? 1 : 0;
+    if (filled[c] && bits)
+      for (int64_t f : regions[c]) {
+        const int64_t k = f / plane, j = (f % plane) / NX, i = f % NX;
+        for (int dk = 0; dk < 2; dk++)
+          for (int dj = 0; dj < 2; dj++)
+            for (int di = 0; di < 2; di++) setb(i + di, j + dj, k + dk, false);
+      }
+  }
+  (void)n;
+  return ncav;
+}
+
 }  // extern "C"
 
 extern "C" {

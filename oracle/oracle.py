@@ -68,6 +68,8 @@ def lib() -> ctypes.CDLL:
         L.nso_free_mesh.argtypes = [P]
         L.nso_shape_filter.restype = ctypes.c_int64
         L.nso_shape_filter.argtypes = [P, P, ctypes.c_int, P, P, ctypes.c_int64, P, P, ctypes.c_double, ctypes.c_int]
+        L.nso_pocket_difference.restype = ctypes.c_int
+        L.nso_pocket_difference.argtypes = [P, P, P, P, ctypes.c_int64, ctypes.c_double, P, P, ctypes.c_int]
         L.nso_ray_torus.restype = ctypes.c_int
         L.nso_ray_torus.argtypes = [P, P, P, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int, P, P, P]
         _lib = L
@@ -328,6 +330,23 @@ def shape_filter(grid, status: np.ndarray, ncav: int, filled, bits=None, eps=Non
     n = L.nso_shape_filter(ctypes.byref(grid), st.ctypes.data, int(ncav), ptr(fl), ptr(b), 0 if b is None else b.size,
                            ptr(e), ptr(d), float(probe), int(bool(mod_status)))
     return st, fl, b, e, None if d is None else d.astype(bool), int(n)
+
+
+def pocket_difference(grid, status_fat: np.ndarray, status_small: np.ndarray, bits=None, fill_volume: float = 0.0):
+    """Pocket mode's difference step on copies of two status maps after their casts
+    (nso_pocket_difference in ns_oracle.cpp).  Returns (status, bits, sizes, filled)."""
+    L = lib()
+    st = np.ascontiguousarray(status_fat, np.int32).copy()
+    s2 = np.ascontiguousarray(status_small, np.int32)
+    b = None if bits is None else np.ascontiguousarray(bits, np.uint32).copy()
+    cap = st.size
+    sizes = np.zeros(cap)
+    filled = np.zeros(cap, np.int32)
+    n = L.nso_pocket_difference(ctypes.byref(grid), st.ctypes.data, s2.ctypes.data, None if b is None else b.ctypes.data,
+                                0 if b is None else b.size, float(fill_volume), sizes.ctypes.data, filled.ctypes.data,
+                                cap)
+    assert n >= 0
+    return st, b, sizes[:n].copy(), filled[:n].copy()
 
 
 def cavity_atoms(grid, status: np.ndarray, ncav: int, atoms: np.ndarray, label: np.ndarray | None = None) -> list[list[int]]:

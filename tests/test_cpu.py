@@ -970,3 +970,27 @@ def test_oracle_shape_filter_matches_fixed_point(oracle_mod):
             own_only, _ = _shape_fixed_point(g, lab, filled, 1.4, True)
             cross = bool(((want == -4 - 1) != (own_only == -4 - 1)).any())
     assert cross, "the case should exercise removed nodes of cavity 4 inside supports of cavity 5"
+
+
+def test_oracle_pocket_difference_known(oracle_mod):
+    """Pocket difference on synthetic maps at scale 1: a solid block for the fat surface and, for
+    the small one, the same block with a 7^3 pit and a 2^3 pit.  The 7^3 difference keeps its
+    5^3 core and faces after the 1.4 A water filter (the 68 edge and corner nodes go), one pocket
+    of 275 A^3; the 2^3 pit holds no water probe and vanishes.  A filling threshold of 300 A^3
+    fills it and clears its insideness bits."""
+    g = _box_grid(30, 1.0)
+    st1 = np.full((30, 30, 30), 3, np.int32)
+    st1[2:28, 2:28, 2:28] = -1
+    st2 = st1.copy()
+    st2[4:11, 5:12, 5:12] = 2
+    st2[15:17, 15:17, 15:17] = 2
+    words = ((30 + 31) >> 5) * 30 * 30
+    bits = np.zeros(words, np.uint32)
+    st, b, sizes, filled = oracle_mod.pocket_difference(g, st1, st2, bits, fill_volume=0.0)
+    assert sizes.tolist() == [275.0] and filled.tolist() == [0]
+    assert (st == 4).sum() == 275 and set(np.unique(st).tolist()) == {-1, 4}
+    node_bits = np.unpackbits(b.view(np.uint8), bitorder="little")[:30 ** 3].reshape(30, 30, 30)
+    assert 0 < node_bits[4:11, 5:12, 5:12].sum() == node_bits.sum() < 343
+    assert node_bits[15:17, 15:17, 15:17].sum() == 0
+    st_f, b_f, sizes_f, filled_f = oracle_mod.pocket_difference(g, st1, st2, bits, fill_volume=300.0)
+    assert filled_f.tolist() == [1] and int(np.unpackbits(b_f.view(np.uint8)).sum()) == 0
