@@ -2,10 +2,11 @@
 ``fillCavities``, src/main.cpp:1411-1586) against the oracle's loop-for-loop restatement applied
 to the oracle's own status maps and insideness bits of the two casts.
 
-A 2,000-atom SES at scale 2.0: the fat surface with a 3.0 A probe and the small one with 1.4 A,
-both with cavity detection and every cavity filled (as pocket mode casts them); pockets of at most
-22.8 A^3 (two water molecules) filled.  Status map with the pocket labels, insideness bits,
-pocket sizes and flags, and the pockets' atoms equal the oracle's.
+SES of 2,000 atoms (pockets of at most 22.8 A^3, two water molecules, filled) and of 10,000 atoms
+(no pocket filled) at scale 2.0: the fat surface with a 3.0 A probe and the small one with 1.4 A,
+both with cavity detection and every cavity filled (as pocket mode casts them).  Status map with
+the pocket labels, insideness bits, pocket sizes and flags, and the pockets' atoms equal the
+oracle's.
 """
 import math
 
@@ -28,8 +29,9 @@ def _cast(atoms, probe):
     return ds, surf
 
 
-def test_pocket_difference_2000(native_lib, oracle_mod):
-    atoms = generator.rsa_globule(2000, 5)
+@pytest.mark.parametrize("n_atoms,seed,fill", [(2000, 5, 22.8), (10000, 2, 0.0)])
+def test_pocket_difference(n_atoms, seed, fill, native_lib, oracle_mod):
+    atoms = generator.rsa_globule(n_atoms, seed)
     ds1, fat = _cast(atoms, 3.0)
     ds2, small = _cast(atoms, 1.4)
     flags = oracle_mod.STATUS | oracle_mod.ACCURATE_TRIANGULATION | oracle_mod.CAVITIES
@@ -37,8 +39,8 @@ def test_pocket_difference_2000(native_lib, oracle_mod):
     r2 = oracle_mod.run(ds2.grid, small.patches, flags=flags, cav_vol=math.inf, threads=8)
     np.testing.assert_array_equal(ds1.status, r1.status)
     np.testing.assert_array_equal(ds2.status, r2.status)
-    n = fat.difference(small, 22.8)
-    st, bits, sizes, filled = oracle_mod.pocket_difference(ds1.grid, r1.status, r2.status, r1.bits, 22.8)
+    n = fat.difference(small, fill)
+    st, bits, sizes, filled = oracle_mod.pocket_difference(ds1.grid, r1.status, r2.status, r1.bits, fill)
     assert n == len(sizes) and n > 0
     np.testing.assert_array_equal(ds1.status.reshape(-1), st.reshape(-1))
     np.testing.assert_array_equal(fat.insideness, bits)
@@ -46,5 +48,5 @@ def test_pocket_difference_2000(native_lib, oracle_mod):
     assert ds1.cavitiesFlag == [bool(f) for f in filled]
     got = fat.getCavitiesAtoms()
     assert got == oracle_mod.cavity_atoms(ds1.grid, st.reshape(r1.status.shape), n, ds1.atoms)
-    print(f"ses 2000 pockets (probes 3.0 / 1.4): {n} pockets, {int(sum(filled))} filled, "
+    print(f"ses {n_atoms} pockets (probes 3.0 / 1.4): {n} pockets, {int(sum(filled))} filled, "
           f"largest {max(sizes):.2f} A^3")
