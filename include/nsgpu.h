@@ -318,12 +318,18 @@ int nsg_download_idebmap(nsg_ctx* ctx, uint8_t* dst);
  * SES (Surface::projector, src/Surface.cpp:4657-4676; ConnollySurface::getProjection,
  * src/ConnollySurface.cpp:5822-5912, over the auxiliary grid of buildAuxiliaryGrid,
  * src/ConnollySurface.cpp:3666-3900, aux_max_dim = Max_ses_patches_auxiliary_grid_size, 50 by
- * default).  Internal points (different dielectrics) do not arise with one inside code. */
+ * default), or onto a mesh surface (the blobby surface's triangles: MeshSurface::getProjection,
+ * src/MeshSurface.cpp:2045-2141, point2triangle :1864-2008, over the triangles' vertex boxes on
+ * the auxiliary grid of MeshSurface::buildAuxiliaryGrid :729-935, aux_max_dim =
+ * Max_mesh_auxiliary_grid_size, 100 by default).  Skin cells are not projected (NSG_ERR_STATE).
+ * Internal points (different dielectrics) do not arise with one inside code. */
 int nsg_bgp(nsg_ctx* ctx, int project, int32_t aux_max_dim, int64_t* n_bgp, int64_t* n_external);
 /* The points of the last nsg_bgp: ibgp (ix, iy, iz), type (1 external, 0 internal), scspos /
- * scsnor (3 doubles; the reference leaves an external point's normal at 0) and the projection flag
- * (0 projected, 1 no feasible projection among the cell's patches: the point is kept, 2 empty
- * auxiliary cell, 3 internal); any pointer may be NULL. */
+ * scsnor (3 doubles; the reference leaves an external SES point's normal at 0, a mesh point gets
+ * its triangle's normal) and the projection flag (0 projected, 1 for the SES no feasible
+ * projection among the cell's patches: the point is kept, for a mesh the nearest point lies on a
+ * triangle's edge or corner (the reference's getProjection returns false; the point is still
+ * projected), 2 empty auxiliary cell, 3 internal); any pointer may be NULL. */
 int nsg_download_bgp(nsg_ctx* ctx, int32_t* ibgp, int32_t* type, double* scspos, double* scsnor, int32_t* flag);
 
 /* ---- allocation-free status ray cast ----

@@ -2059,8 +2059,8 @@ nsg::AuxGrid aux_grid_of(const NsGrid& g, int64_t max_dim) {
 int nsg_bgp(nsg_ctx* c, int project, int32_t aux_max_dim, int64_t* n_bgp, int64_t* n_external) {
   if (!c) return NSG_ERR_ARG;
   if (!c->have_eps) return fail(NSG_ERR_STATE, "boundary grid points need the epsilon maps (NSG_RAYCAST_EPSMAP)");
-  if (project && (c->kind_mask & ~nsg::kSesKinds))
-    return fail(NSG_ERR_STATE, "boundary grid point projection is provided for SES patch sets");
+  if (project && (c->kind_mask & ~nsg::kSesKinds) && c->kind_mask != (1 << NS_MESH_TRI))
+    return fail(NSG_ERR_STATE, "boundary grid point projection is provided for SES and mesh patch sets");
   if (project && aux_max_dim < 1) return fail(NSG_ERR_ARG, "auxiliary grid size must be positive");
   CK(cudaSetDevice(c->device));
   const NsGrid& g = c->grid;

@@ -109,11 +109,27 @@ __device__ __forceinline__ void aux_box(const double* f, const AuxGrid& a, int64
   }
 }
 
+// Cell range of a mesh triangle: its vertices' box (MeshSurface::buildAuxiliaryGrid,
+// src/MeshSurface.cpp:867-929); the reference stops on a box outside the grid, here it is clamped.
+__device__ __forceinline__ void aux_box_tri(const double* f, const AuxGrid& a, int64_t lo[3], int64_t hi[3]) {
+  for (int d = 0; d < 3; d++) {
+    double dn = 1e20, up = -1e20;
+    for (int v = 0; v < 3; v++) {
+      dn = f[3 * v + d] < dn ? f[3 * v + d] : dn;
+      up = f[3 * v + d] > up ? f[3 * v + d] : up;
+    }
+    const int64_t l = (int64_t)rintp((dn - a.mn[d]) * a.scale), h = (int64_t)rintp((up - a.mn[d]) * a.scale);
+    lo[d] = l < 0 ? 0 : (l >= a.n ? a.n - 1 : l);
+    hi[d] = h < 0 ? 0 : (h >= a.n ? a.n - 1 : h);
+  }
+}
+
 __global__ void k_aux_bin(PatchDev P, AuxGrid a, int32_t* cnt, const int64_t* __restrict__ off, int32_t* cursor,
                           int32_t* list) {
   for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < P.n; p += (int64_t)gridDim.x * blockDim.x) {
     int64_t lo[3], hi[3];
-    aux_box(P.f64 + (int64_t)NS_PATCH_F64 * p, a, lo, hi);
+    if (P.i32[NS_PATCH_I32 * p] == NS_MESH_TRI) aux_box_tri(P.f64 + (int64_t)NS_PATCH_F64 * p, a, lo, hi);
+    else aux_box(P.f64 + (int64_t)NS_PATCH_F64 * p, a, lo, hi);
     for (int64_t iz = lo[2]; iz <= hi[2]; iz++)
       for (int64_t iy = lo[1]; iy <= hi[1]; iy++)
         for (int64_t ix = lo[0]; ix <= hi[0]; ix++) {
@@ -122,6 +138,88 @@ __global__ void k_aux_bin(PatchDev P, AuxGrid a, int32_t* cnt, const int64_t* __
           else list[off[c] + atomicAdd(cursor + c, 1)] = (int32_t)p;
         }
   }
+}
+
+// MeshSurface::point2triangle (src/MeshSurface.cpp:1864-2008) with the triangle's plane as
+// preProcessTriangles stores it (plane3points, normalised, offset from the triple product,
+// :674-684), point2plane (:2034-2044) and inTriangle (:2010-2032, whose barycentric test
+// multiplies by the denominator).  Outside the triangle the nearest of the three clamped edge
+// projections wins, with the reference's edge "normal" S + T t normalised.  Returns whether the
+// plane projection fell inside the triangle.
+__device__ __forceinline__ double dot3(const double* x, const double* y) { return x[0] * y[0] + x[1] * y[1] + x[2] * y[2]; }
+
+__device__ bool project_tri(const double* P, const double* f, double* proj, double* dist, double* normal) {
+  const double *A = f, *B = f + 3, *C = f + 6;
+  double w[4];
+  w[0] = A[1] * (B[2] - C[2]) + B[1] * (C[2] - A[2]) + C[1] * (A[2] - B[2]);
+  w[1] = A[2] * (B[0] - C[0]) + B[2] * (C[0] - A[0]) + C[2] * (A[0] - B[0]);
+  w[2] = A[0] * (B[1] - C[1]) + B[0] * (C[1] - A[1]) + C[0] * (A[1] - B[1]);
+  const double norm = sqrt(dot3(w, w));
+  for (int d = 0; d < 3; d++) w[d] /= norm;
+  w[3] = -(A[0] * (B[1] * C[2] - C[1] * B[2]) + B[0] * (C[1] * A[2] - A[1] * C[2]) + C[0] * (A[1] * B[2] - B[1] * A[2]));
+  w[3] /= norm;
+  const double den = dot3(w, w);
+  const double val = dot3(w, P) + w[3];
+  for (int d = 0; d < 3; d++) proj[d] = P[d] - w[d] * (val / den);
+  *dist = fabs(val / sqrt(den));
+  double v0[3], v1[3], v2[3];
+  for (int d = 0; d < 3; d++) {
+    v0[d] = C[d] - A[d];
+    v1[d] = B[d] - A[d];
+    v2[d] = proj[d] - A[d];
+  }
+  const double d00 = dot3(v0, v0), d01 = dot3(v0, v1), d02 = dot3(v0, v2), d11 = dot3(v1, v1), d12 = dot3(v1, v2);
+  const double den2 = d00 * d11 - d01 * d01;
+  const double u = (d11 * d02 - d01 * d12) * den2, v = (d00 * d12 - d01 * d02) * den2;
+  if (u > 0 && v > 0 && u + v < 1) {
+    for (int d = 0; d < 3; d++) normal[d] = w[d];
+    return true;
+  }
+  double bd = 0, bt = 0, bres[3] = {0, 0, 0};
+  int be = -1;
+  for (int e = 0; e < 3; e++) {
+    const double* S = e == 2 ? B : A;
+    const double* T = e == 0 ? B : C;
+    double t2[3], t1[3], res[3], de;
+    for (int d = 0; d < 3; d++) {
+      t2[d] = T[d] - S[d];
+      t1[d] = proj[d] - S[d];
+    }
+    const double l2 = dot3(t2, t2);
+    double t = dot3(t1, t2);
+    if (t < 0.0) {
+      for (int d = 0; d < 3; d++) t1[d] = P[d] - S[d];
+      de = sqrt(dot3(t1, t1));
+      for (int d = 0; d < 3; d++) res[d] = S[d];
+      t = 0.0;
+    } else if (t > l2) {
+      for (int d = 0; d < 3; d++) t1[d] = P[d] - T[d];
+      de = sqrt(dot3(t1, t1));
+      for (int d = 0; d < 3; d++) res[d] = T[d];
+      t = 1.0;
+    } else {
+      t /= l2;
+      for (int d = 0; d < 3; d++) res[d] = S[d] + t2[d] * t;
+      for (int d = 0; d < 3; d++) t1[d] = res[d] - P[d];
+      de = sqrt(dot3(t1, t1));
+    }
+    // the reference's choice (d0 <= d1 && d0 <= d2, then d1 <= d0 && d1 <= d2, else d2) is the
+    // first smallest: keep an edge only when strictly nearer than the ones before it
+    if (be < 0 || de < bd) {
+      be = e;
+      bd = de;
+      bt = t;
+      for (int d = 0; d < 3; d++) bres[d] = res[d];
+    }
+  }
+  const double* S = be == 2 ? B : A;
+  const double* T = be == 0 ? B : C;
+  for (int d = 0; d < 3; d++) proj[d] = bres[d];
+  *dist = bd;
+  for (int d = 0; d < 3; d++) normal[d] = S[d] + T[d] * bt;
+  const double nn = sqrt(dot3(normal, normal));
+  for (int d = 0; d < 3; d++) normal[d] /= nn;
+  return false;
 }
 
 // projectToSphere (src/tools.cpp:1112-1120), operation for operation.
@@ -203,12 +301,28 @@ __global__ void k_bgp_project(PatchDev P, AuxGrid a, const int64_t* __restrict__
     double best = INFINITY;
     int32_t best_p = INT32_MAX;
     double bp[3] = {y[0], y[1], y[2]};
+    double bn[3] = {0.0, 0.0, 0.0};
+    int best_in = 0;
     for (int64_t u = b + lane; u < e; u += 32) {
       const int32_t p = list[u];
       const double* f = P.f64 + (int64_t)NS_PATCH_F64 * p;
       const int32_t* ir = P.i32 + NS_PATCH_I32 * (int64_t)p;
       const int kind = ir[0];
       double proj[3], dist;
+      if (kind == NS_MESH_TRI) {
+        double nrm[3];
+        const bool in_tri = project_tri(y, f, proj, &dist, nrm);
+        if (dist < best || (dist == best && p < best_p)) {
+          best = dist;
+          best_p = p;
+          best_in = in_tri ? 1 : 0;
+          for (int d = 0; d < 3; d++) {
+            bp[d] = proj[d];
+            bn[d] = nrm[d];
+          }
+        }
+        continue;
+      }
       if (kind == NS_POINT) dist = project_sphere(y, f, f[3], proj);
       else if (kind == NS_FACE_REG || kind == NS_FACE_SING) dist = project_sphere(y, f, P.probe, proj);
       else dist = project_torus(y, f, P.probe, proj);
@@ -228,21 +342,30 @@ __global__ void k_bgp_project(PatchDev P, AuxGrid a, const int64_t* __restrict__
       const double o0 = __shfl_xor_sync(0xffffffffu, bp[0], o);
       const double o1 = __shfl_xor_sync(0xffffffffu, bp[1], o);
       const double o2 = __shfl_xor_sync(0xffffffffu, bp[2], o);
+      const double n0 = __shfl_xor_sync(0xffffffffu, bn[0], o);
+      const double n1 = __shfl_xor_sync(0xffffffffu, bn[1], o);
+      const double n2 = __shfl_xor_sync(0xffffffffu, bn[2], o);
+      const int oi = __shfl_xor_sync(0xffffffffu, best_in, o);
       if (od < best || (od == best && op < best_p)) {
         best = od;
         best_p = op;
         bp[0] = o0;
         bp[1] = o1;
         bp[2] = o2;
+        bn[0] = n0;
+        bn[1] = n1;
+        bn[2] = n2;
+        best_in = oi;
       }
     }
     if (lane == 0) {
       const bool ok = best_p != INT32_MAX;
+      const bool mesh = ok && P.i32[NS_PATCH_I32 * (int64_t)best_p] == NS_MESH_TRI;
       for (int d = 0; d < 3; d++) {
         pos[3 * q + d] = ok ? bp[d] : y[d];
-        nor[3 * q + d] = 0.0;
+        nor[3 * q + d] = mesh ? bn[d] : 0.0;
       }
-      flag[q] = e == b ? 2 : (ok ? 0 : 1);
+      flag[q] = e == b ? 2 : (mesh ? (best_in ? 0 : 1) : (ok ? 0 : 1));
     }
   }
 }

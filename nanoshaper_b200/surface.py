@@ -526,10 +526,13 @@ class Surface:
     def projectBoundaryGridPoints(self) -> int:
         """Boundary grid points of the epsilon map and their projection onto the surface (the
         projBGP phase of Surface::getSurf, src/Surface.cpp:1473-1678); fills the DelPhiShared's
-        ibgp, bgp_type, scspos, scsnor (and bgp_flag: 0 projected, 1 no feasible projection among
-        the auxiliary cell's patches, the point kept; 2 empty cell).  Returns the point count."""
-        if self.name != "ses":
-            raise NotImplementedError("boundary grid point projection is provided for the SES")
+        ibgp, bgp_type, scspos, scsnor (and bgp_flag: 0 projected; 1 for the SES no feasible
+        projection among the auxiliary cell's patches, the point kept, for the blobby mesh the
+        nearest point on a triangle's edge or corner; 2 empty cell).  The blobby surface projects
+        onto its triangles as MeshSurface::getProjection (src/MeshSurface.cpp:2045-2141) does.
+        Returns the point count."""
+        if self.name not in ("ses", "blobby"):
+            raise NotImplementedError("boundary grid point projection is provided for the SES and blobby surfaces")
         c = self._context().handle
         n = ctypes.c_int64()
         ne = ctypes.c_int64()
@@ -753,6 +756,8 @@ class BlobbySurface(Surface):
         super().__init__(cf, delphi, device)
         cf = cf or ConfigFile()
         self.setBlobbyness(cf.read("Blobbyness", self.DEFAULT_BLOBBYNESS, float))
+        # the projection runs on the mesh's auxiliary grid (MeshSurface::init, src/MeshSurface.cpp:179)
+        self.auxGridDim = cf.read("Max_mesh_auxiliary_grid_size", 100, int)
         self.differentiable = False
         self.n_mesh_vertices = 0
         self.n_mesh_triangles = 0

@@ -947,6 +947,86 @@ struct Oracle {
                 (proj[2] - y[2]) * (proj[2] - y[2]));
   }
 
+  // Mesh surfaces (MeshSurface, src/MeshSurface.cpp): the projection plane of a triangle
+  // (plane3points src/tools.cpp:258-274, normalised and its offset recomputed as in
+  // preProcessTriangles :674-684), point2plane (:2034-2044), inTriangle (:2010-2032, the
+  // denominator multiplied rather than divided, as there) and point2triangle (:1864-2008: the
+  // nearest of the three edge projections when the plane projection falls outside; its "normal"
+  // is A + B t normalised, as there).  Returns whether the plane projection fell inside.
+  static void mesh_plane(const double* f, double w[4]) {
+    const double *a = f, *b = f + 3, *c = f + 6;
+    w[0] = a[1] * (b[2] - c[2]) + b[1] * (c[2] - a[2]) + c[1] * (a[2] - b[2]);
+    w[1] = a[2] * (b[0] - c[0]) + b[2] * (c[0] - a[0]) + c[2] * (a[0] - b[0]);
+    w[2] = a[0] * (b[1] - c[1]) + b[0] * (c[1] - a[1]) + c[0] * (a[1] - b[1]);
+    const double norm = sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+    w[0] /= norm;
+    w[1] /= norm;
+    w[2] /= norm;
+    w[3] = -(a[0] * (b[1] * c[2] - c[1] * b[2]) + b[0] * (c[1] * a[2] - a[1] * c[2]) + c[0] * (a[1] * b[2] - b[1] * a[2]));
+    w[3] /= norm;
+  }
+  static bool mesh_project(const double* P, const double* f, double* proj, double* dist, double* normal) {
+    const double *A = f, *B = f + 3, *C = f + 6;
+    double w[4];
+    mesh_plane(f, w);
+    const double den = w[0] * w[0] + w[1] * w[1] + w[2] * w[2];
+    const double dd = sqrt(den);
+    const double val = (w[0] * P[0] + w[1] * P[1] + w[2] * P[2]) + w[3];
+    for (int d = 0; d < 3; d++) proj[d] = P[d] - w[d] * (val / den);
+    *dist = fabs(val / dd);
+    double v0[3], v1[3], v2[3];
+    for (int d = 0; d < 3; d++) {
+      v0[d] = C[d] - A[d];
+      v1[d] = B[d] - A[d];
+      v2[d] = proj[d] - A[d];
+    }
+    auto dot = [](const double* x, const double* y) { return x[0] * y[0] + x[1] * y[1] + x[2] * y[2]; };
+    const double d00 = dot(v0, v0), d01 = dot(v0, v1), d02 = dot(v0, v2), d11 = dot(v1, v1), d12 = dot(v1, v2);
+    const double inv = d00 * d11 - d01 * d01;
+    const double u = (d11 * d02 - d01 * d12) * inv, v = (d00 * d12 - d01 * d02) * inv;
+    if (u > 0 && v > 0 && u + v < 1) {
+      for (int d = 0; d < 3; d++) normal[d] = w[d];
+      return true;
+    }
+    // edges AB, AC, BC: clamp the plane projection's parameter, distance from P
+    const double* E[3][2] = {{A, B}, {A, C}, {B, C}};
+    double res[3][3], de[3], tt[3];
+    for (int e = 0; e < 3; e++) {
+      const double *S = E[e][0], *T = E[e][1];
+      double t2[3], t1[3];
+      for (int d = 0; d < 3; d++) {
+        t2[d] = T[d] - S[d];
+        t1[d] = proj[d] - S[d];
+      }
+      const double l2 = dot(t2, t2);
+      double t = dot(t1, t2);
+      if (t < 0.0) {
+        for (int d = 0; d < 3; d++) t1[d] = P[d] - S[d];
+        de[e] = sqrt(dot(t1, t1));
+        for (int d = 0; d < 3; d++) res[e][d] = S[d];
+        t = 0.0;
+      } else if (t > l2) {
+        for (int d = 0; d < 3; d++) t1[d] = P[d] - T[d];
+        de[e] = sqrt(dot(t1, t1));
+        for (int d = 0; d < 3; d++) res[e][d] = T[d];
+        t = 1.0;
+      } else {
+        t /= l2;
+        for (int d = 0; d < 3; d++) res[e][d] = S[d] + t2[d] * t;
+        for (int d = 0; d < 3; d++) t1[d] = res[e][d] - P[d];
+        de[e] = sqrt(dot(t1, t1));
+      }
+      tt[e] = t;
+    }
+    const int k = (de[0] <= de[1] && de[0] <= de[2]) ? 0 : ((de[1] <= de[0] && de[1] <= de[2]) ? 1 : 2);
+    for (int d = 0; d < 3; d++) proj[d] = res[k][d];
+    *dist = de[k];
+    for (int d = 0; d < 3; d++) normal[d] = E[k][0][d] + E[k][1][d] * tt[k];
+    const double nn = sqrt(dot(normal, normal));
+    for (int d = 0; d < 3; d++) normal[d] /= nn;
+    return false;
+  }
+
   // Boundary grid points (src/Surface.cpp:1488-1546) and the projection of the external ones
   // (Surface::projector, src/Surface.cpp:4657-4676; ConnollySurface::getProjection,
   // src/ConnollySurface.cpp:5822-5912) over the auxiliary grid of buildAuxiliaryGrid
@@ -989,6 +1069,18 @@ struct Oracle {
     for (int64_t it = 0; it < P.n; it++) {
       const double* f = P.f64 + NS_PATCH_F64 * it;
       int64_t lo[3], hi[3];
+      if (P.i32[NS_PATCH_I32 * it] == NS_MESH_TRI) {
+        // the triangle's vertex box (MeshSurface::buildAuxiliaryGrid, src/MeshSurface.cpp:867-929)
+        for (int d = 0; d < 3; d++) {
+          double dn = 1e20, up = -1e20;
+          for (int v = 0; v < 3; v++) {
+            dn = f[3 * v + d] < dn ? f[3 * v + d] : dn;
+            up = f[3 * v + d] > up ? f[3 * v + d] : up;
+          }
+          lo[d] = std::min<int64_t>(std::max<int64_t>((int64_t)rintp((dn - amin[d]) * ascale), 0), igrid - 1);
+          hi[d] = std::min<int64_t>(std::max<int64_t>((int64_t)rintp((up - amin[d]) * ascale), 0), igrid - 1);
+        }
+      } else
       for (int d = 0; d < 3; d++) {
         lo[d] = (int64_t)rintp(fmax(0., (f[d] - f[3]) - amin[d]) * ascale);
         hi[d] = (int64_t)rintp(fmax(0., (f[d] + f[3]) - amin[d]) * ascale);
@@ -1015,10 +1107,26 @@ struct Oracle {
       }
       if (!in || cells[(ic[2] * igrid + ic[1]) * igrid + ic[0]].empty()) { bgp_flag[q] = 2; continue; }
       double best = INFINITY;
-      for (int32_t it : cells[(ic[2] * igrid + ic[1]) * igrid + ic[0]]) {
+      std::vector<int32_t> cand = cells[(ic[2] * igrid + ic[1]) * igrid + ic[0]];
+      std::sort(cand.begin(), cand.end());
+      bool inside_best = false;
+      for (int32_t it : cand) {
         const double* f = P.f64 + NS_PATCH_F64 * (int64_t)it;
         const int kind = P.i32[NS_PATCH_I32 * (int64_t)it];
         double proj[3], dist;
+        if (kind == NS_MESH_TRI) {
+          double nrm[3];
+          const bool in_tri = mesh_project(y, f, proj, &dist, nrm);
+          if (dist < best) {
+            best = dist;
+            inside_best = in_tri;
+            for (int d = 0; d < 3; d++) {
+              scspos[3 * q + d] = proj[d];
+              scsnor[3 * q + d] = nrm[d];
+            }
+          }
+          continue;
+        }
         if (kind == NS_POINT) dist = project_sphere(y, f, f[3], proj);
         else if (kind == NS_FACE_REG || kind == NS_FACE_SING) dist = project_sphere(y, f, P.probe, proj);
         else dist = project_torus(y, f, P.probe, proj);
@@ -1028,7 +1136,8 @@ struct Oracle {
           for (int d = 0; d < 3; d++) scspos[3 * q + d] = proj[d];
         }
       }
-      bgp_flag[q] = best == INFINITY ? 1 : 0;
+      const bool mesh = P.i32[NS_PATCH_I32 * (int64_t)cand[0]] == NS_MESH_TRI;
+      bgp_flag[q] = mesh ? (inside_best ? 0 : 1) : (best == INFINITY ? 1 : 0);
     }
   }
 
@@ -1537,6 +1646,11 @@ int64_t nso_shape_filter(const NsGrid* gp, int32_t* status, int ncav, int32_t* f
 // pocket, here flooded breadth-first since only its node set matters), then fillCavities(fill_vol)
 // (src/Surface.cpp:2355-2484) on the insideness bits.  st1 (fat probe) is modified in place; sizes
 // and filled receive up to cap pockets.  Returns the number of pockets, -1 past cap.
+// The mesh projection of one point onto one triangle (9 doubles: A, B, C), for tests.
+int nso_mesh_project(const double* P, const double* tri, double* proj, double* dist, double* normal) {
+  return Oracle::mesh_project(P, tri, proj, dist, normal) ? 1 : 0;
+}
+
 int nso_pocket_difference(const NsGrid* gp, int32_t* st1, const int32_t* st2, uint32_t* bits, int64_t nwords,
                           double fill_vol, double* sizes, int32_t* filled, int cap) {
   const NsGrid& g = *gp;

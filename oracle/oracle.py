@@ -70,6 +70,8 @@ def lib() -> ctypes.CDLL:
         L.nso_shape_filter.argtypes = [P, P, ctypes.c_int, P, P, ctypes.c_int64, P, P, ctypes.c_double, ctypes.c_int]
         L.nso_pocket_difference.restype = ctypes.c_int
         L.nso_pocket_difference.argtypes = [P, P, P, P, ctypes.c_int64, ctypes.c_double, P, P, ctypes.c_int]
+        L.nso_mesh_project.restype = ctypes.c_int
+        L.nso_mesh_project.argtypes = [P, P, P, P, P]
         L.nso_ray_torus.restype = ctypes.c_int
         L.nso_ray_torus.argtypes = [P, P, P, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int, P, P, P]
         _lib = L
@@ -330,6 +332,19 @@ def shape_filter(grid, status: np.ndarray, ncav: int, filled, bits=None, eps=Non
     n = L.nso_shape_filter(ctypes.byref(grid), st.ctypes.data, int(ncav), ptr(fl), ptr(b), 0 if b is None else b.size,
                            ptr(e), ptr(d), float(probe), int(bool(mod_status)))
     return st, fl, b, e, None if d is None else d.astype(bool), int(n)
+
+
+def mesh_project(point, tri):
+    """MeshSurface::point2triangle of one point onto one triangle (nso_mesh_project):
+    (inside the triangle, projection, distance, normal)."""
+    L = lib()
+    p = np.ascontiguousarray(point, np.float64)
+    t = np.ascontiguousarray(tri, np.float64).reshape(9)
+    proj = np.zeros(3)
+    nrm = np.zeros(3)
+    dist = ctypes.c_double()
+    ins = L.nso_mesh_project(p.ctypes.data, t.ctypes.data, proj.ctypes.data, ctypes.byref(dist), nrm.ctypes.data)
+    return bool(ins), proj, dist.value, nrm
 
 
 def pocket_difference(grid, status_fat: np.ndarray, status_small: np.ndarray, bits=None, fill_volume: float = 0.0):

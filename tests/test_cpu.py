@@ -994,3 +994,14 @@ def test_oracle_pocket_difference_known(oracle_mod):
     assert node_bits[15:17, 15:17, 15:17].sum() == 0
     st_f, b_f, sizes_f, filled_f = oracle_mod.pocket_difference(g, st1, st2, bits, fill_volume=300.0)
     assert filled_f.tolist() == [1] and int(np.unpackbits(b_f.view(np.uint8)).sum()) == 0
+
+
+def test_oracle_mesh_projection_known(oracle_mod):
+    """MeshSurface::point2triangle on the unit right triangle: a point above the interior drops
+    to its foot with the plane normal; a point beyond the corner B goes to B through the first
+    edge (AB) and gets the reference's edge "normal" A + B t normalised, here (1, 0, 0)."""
+    tri = [0, 0, 0, 1, 0, 0, 0, 1, 0]
+    ins, proj, dist, nrm = oracle_mod.mesh_project([0.2, 0.2, 1.0], tri)
+    assert ins and proj.tolist() == [0.2, 0.2, 0.0] and dist == 1.0 and nrm.tolist() == [0.0, 0.0, 1.0]
+    ins, proj, dist, nrm = oracle_mod.mesh_project([2.0, -1.0, 0.5], tri)
+    assert not ins and proj.tolist() == [1.0, 0.0, 0.0] and dist == 1.5 and nrm.tolist() == [1.0, 0.0, 0.0]

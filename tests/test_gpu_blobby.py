@@ -177,3 +177,32 @@ def test_blobby_gradients_match_fd(precision, atoms_2000, native_lib):
     assert not loose, f"{len(loose)} of {total - skipped} compared components off by more than 1e-2: {loose[:8]}"
     assert len(bad) <= 0.05 * (total - skipped), f"{len(bad)} of {total - skipped} compared components off: {bad[:8]}"
     assert total - skipped >= 0.2 * total, f"only {total - skipped} of {total} components compared"
+
+
+def test_blobby_bgp_projection_matches_oracle(atoms_2000, native_lib, oracle_mod):
+    """Boundary grid points of the blobby surface projected onto its triangles
+    (MeshSurface::getProjection, src/MeshSurface.cpp:2045-2141, over the triangles' vertex boxes on
+    the 100-cell auxiliary grid): points, types, flags (0 inside a triangle, 1 on an edge or
+    corner), projections and normals against the oracle on the same mesh, FP64."""
+    import compare
+    ds = nb.DelPhiShared(atoms_2000, 2.0, 80.0, build_eps_map=True)
+    cf = nb.ConfigFile(text="Surface = blobby\nBlobbyness = -2.5\nAccurate_Triangulation = true\n"
+                            "Project_boundary_grid_points = true\n")
+    surf = nb.surfaceFactory().create(cf, ds)
+    surf.build()
+    surf.getSurf(True, True, 10.0)
+    v, t = surf.mesh()
+    ref = oracle_mod.run(ds.grid, oracle_mod.TrianglePatches(v, t), cav_vol=10.0, threads=8, aux_grid_dim=100,
+                         flags=oracle_mod.STATUS | oracle_mod.ACCURATE_TRIANGULATION | oracle_mod.CAVITIES |
+                         oracle_mod.EPSMAP | oracle_mod.BGP)
+    n_mis, n_near = compare.near_threshold_eps(ds.epsmap, ref, ds.grid)
+    assert n_mis == 0, f"{n_mis} epsilon-map entries differ ({n_near} near a threshold)"
+    np.testing.assert_array_equal(ds.ibgp, ref.ibgp)
+    np.testing.assert_array_equal(ds.bgp_type, ref.bgp_type)
+    np.testing.assert_array_equal(ds.bgp_flag, ref.bgp_flag)
+    dp = float(np.abs(ds.scspos - ref.scspos).max())
+    dn = float(np.abs(ds.scsnor - ref.scsnor).max())
+    assert dp <= 1e-12 and dn <= 1e-12, f"projections differ by {dp} A, normals by {dn}"
+    n_edge = int((ds.bgp_flag == 1).sum())
+    assert ds.nbgp > 0 and n_edge < ds.nbgp
+    print(f"blobby 2000 bgp: {ds.nbgp} points, {n_edge} on edges or corners, projections {dp:.1e}, normals {dn:.1e}")
